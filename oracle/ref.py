@@ -1,0 +1,278 @@
+"""Test infrastructure only: ctypes access to the reference's OWN RI code.
+
+``oracle/_ref/librrref.so`` is the reference's unmodified RI sources compiled by
+``oracle/Makefile`` (see ``ref_bridge.cpp`` for the entry points and the reference
+file:line each one calls).  Only tests/, tests/golden/make_golden.py and bench.py's
+CPU-baseline leg import this module; the product library never does.
+
+All arrays are row-major numpy float64 / complex128 (interleaved), exactly the
+reference's ``Matrix<T>`` layout.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "_ref" / "librrref.so"
+_lib = None
+
+_i64 = ctypes.c_int64
+_dp = ctypes.POINTER(ctypes.c_double)
+_lp = ctypes.POINTER(ctypes.c_int64)
+
+
+class ScfResult(ctypes.Structure):
+    _fields_ = [("electronic_energy", ctypes.c_double), ("iterations", ctypes.c_int64),
+                ("converged", ctypes.c_int64)]
+
+
+def available() -> bool:
+    return LIB_PATH.exists()
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"reference oracle not built: {LIB_PATH} (run `make -C oracle`)")
+        _lib = ctypes.CDLL(str(LIB_PATH))
+        _lib.rrref_last_error.restype = ctypes.c_char_p
+        set_threads(int(os.environ.get("RRREF_THREADS", os.cpu_count() or 1)))
+    return _lib
+
+
+def set_threads(n: int) -> None:
+    lib_ = _lib if _lib is not None else lib()
+    lib_.rrref_set_threads(ctypes.c_int(n))
+
+
+def _p(a):
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "arrays must be C-contiguous"
+    if a.dtype == np.int64:
+        return a.ctypes.data_as(_lp)
+    return a.ctypes.data_as(_dp)
+
+
+def _d(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _c(a):
+    return np.ascontiguousarray(a, dtype=np.complex128)
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise RuntimeError(lib().rrref_last_error().decode())
+
+
+def nonrel_fock(h, B, D, S, X):
+    n = h.shape[0]
+    naux = B.shape[0]
+    F = np.empty((n, n))
+    B, h, D, S, X = _d(B), _d(h), _d(D), _d(S), _d(X)
+    _check(lib().rrref_nonrel_fock(_i64(n), _i64(naux), _p(B), _p(h), _p(D), _p(S), _p(X), _i64(X.shape[1]), _p(F)))
+    return F
+
+
+def x2c_fock(h, B, P, S, X):
+    n = h.shape[0]
+    nl = n // 2
+    F = np.empty((n, n), dtype=np.complex128)
+    B, h, P, S, X = _d(B), _c(h), _c(P), _c(S), _c(X)
+    _check(lib().rrref_x2c_fock(_i64(nl), _i64(B.shape[0]), _p(B), _p(h), _p(P), _p(S), _p(X), _i64(X.shape[1]),
+                                _p(F)))
+    return F
+
+
+def ukb_two_electron(nl, ns, B_LL, B_SS, P_ukb, C_occ, occ):
+    nu = 2 * nl + 2 * ns
+    G = np.empty((nu, nu), dtype=np.complex128)
+    B_LL, B_SS, P_ukb, C_occ, occ = _d(B_LL), _d(B_SS), _c(P_ukb), _c(C_occ), _d(occ)
+    _check(lib().rrref_ukb_two_electron(_i64(nl), _i64(ns), _i64(B_LL.shape[0]), _p(B_LL), _p(B_SS), _p(P_ukb),
+                                        _p(C_occ), _i64(C_occ.shape[1]), _p(occ), _p(G)))
+    return G
+
+
+def rkb_fock(h, nl, ns, B_LL, B_SS, v_total, s_full, x_full, P):
+    n_rkb = h.shape[0]
+    F = np.empty((n_rkb, n_rkb), dtype=np.complex128)
+    B_LL, B_SS, v_total, s_full, x_full, h, P = _d(B_LL), _d(B_SS), _c(v_total), _c(s_full), _c(x_full), _c(h), _c(P)
+    _check(lib().rrref_rkb_fock(_i64(nl), _i64(ns), _i64(B_LL.shape[0]), _p(B_LL), _p(B_SS), _p(v_total),
+                                _i64(n_rkb), _p(s_full), _p(x_full), _i64(x_full.shape[1]), _p(h), _p(P), _p(F)))
+    return F
+
+
+def nonrel_mo_build(B, C):
+    n = C.shape[0]
+    out = np.empty((B.shape[0], n * n))
+    B, C = _d(B), _d(C)
+    _check(lib().rrref_nonrel_mo_build(_i64(n), _i64(B.shape[0]), _p(B), _p(C), _p(out)))
+    return out
+
+
+def nonrel_mo_rotated(Bmo, n, U):
+    out = np.empty_like(Bmo, dtype=np.float64)
+    Bmo, U = _d(Bmo), _d(U)
+    _check(lib().rrref_nonrel_mo_rotated(_i64(n), _i64(Bmo.shape[0]), _p(Bmo), _p(U), _p(out)))
+    return out
+
+
+def nonrel_mo_embedded(Bmo, n):
+    out = np.empty((Bmo.shape[0], 4 * n * n))
+    Bmo = _d(Bmo)
+    _check(lib().rrref_nonrel_mo_embedded(_i64(n), _i64(Bmo.shape[0]), _p(Bmo), _p(out)))
+    return out
+
+
+def nonrel_mo_eri(Bmo, n, abcd):
+    abcd = np.ascontiguousarray(abcd, dtype=np.int64).reshape(-1, 4)
+    out = np.empty(abcd.shape[0])
+    Bmo = _d(Bmo)
+    _check(lib().rrref_nonrel_mo_eri(_i64(n), _i64(Bmo.shape[0]), _p(Bmo), _i64(abcd.shape[0]), _p(abcd), _p(out)))
+    return out
+
+
+def ri_mo_build(nl, ns, B_LL, B_SS, c_ukb):
+    n_total = c_ukb.shape[1]
+    out = np.empty((B_LL.shape[0], n_total * n_total), dtype=np.complex128)
+    B_LL, B_SS, c_ukb = _d(B_LL), _d(B_SS), _c(c_ukb)
+    _check(lib().rrref_ri_mo_build(_i64(nl), _i64(ns), _i64(B_LL.shape[0]), _p(B_LL), _p(B_SS), _p(c_ukb),
+                                   _i64(n_total), _p(out)))
+    return out
+
+
+def ri_mo_rotated(Bmo, n, U):
+    out = np.empty_like(Bmo, dtype=np.complex128)
+    Bmo, U = _c(Bmo), _c(U)
+    _check(lib().rrref_ri_mo_rotated(_i64(n), _i64(Bmo.shape[0]), _p(Bmo), _p(U), _p(out)))
+    return out
+
+
+def ri_mo_positive(Bmo, n, off):
+    m = n - off
+    out = np.empty((Bmo.shape[0], m * m), dtype=np.complex128)
+    Bmo = _c(Bmo)
+    _check(lib().rrref_ri_mo_positive(_i64(n), _i64(Bmo.shape[0]), _p(Bmo), _i64(off), _p(out)))
+    return out
+
+
+def ri_mo_eri(Bmo, n, abcd):
+    abcd = np.ascontiguousarray(abcd, dtype=np.int64).reshape(-1, 4)
+    out = np.empty(abcd.shape[0], dtype=np.complex128)
+    Bmo = _c(Bmo)
+    _check(lib().rrref_ri_mo_eri(_i64(n), _i64(Bmo.shape[0]), _p(Bmo), _i64(abcd.shape[0]), _p(abcd), _p(out)))
+    return out
+
+
+def hx_fock_nonrel(Bmo_spatial, n_sp, h, occ, h2, x2, pair_of=None, l1=None, l2=None, use_reference=False):
+    n = 2 * n_sp
+    F = np.empty((n, n))
+    args = [_d(Bmo_spatial), _d(h), _d(occ), _d(h2), _d(x2)]
+    po = None if pair_of is None else np.ascontiguousarray(pair_of, dtype=np.int64)
+    L1 = None if pair_of is None else _d(l1)
+    L2 = None if pair_of is None else _d(l2)
+    _check(lib().rrref_hx_fock_nonrel(_i64(n_sp), _i64(args[0].shape[0]), *[_p(a) for a in args], _p(po), _p(L1),
+                                      _p(L2), ctypes.c_int(1 if use_reference else 0), _p(F)))
+    return F
+
+
+def hx_fock_complex(Bmo, n, h, occ, h2, x2, pair_of=None, l1=None, l2=None, use_reference=False):
+    F = np.empty((n, n), dtype=np.complex128)
+    args = [_c(Bmo), _c(h), _d(occ), _d(h2), _d(x2)]
+    po = None if pair_of is None else np.ascontiguousarray(pair_of, dtype=np.int64)
+    L1 = None if pair_of is None else _d(l1)
+    L2 = None if pair_of is None else _d(l2)
+    _check(lib().rrref_hx_fock_complex(_i64(n), _i64(args[0].shape[0]), *[_p(a) for a in args], _p(po), _p(L1),
+                                       _p(L2), ctypes.c_int(1 if use_reference else 0), _p(F)))
+    return F
+
+
+def commutator_error(F, P, S):
+    n = F.shape[0]
+    if np.iscomplexobj(F) or np.iscomplexobj(P) or np.iscomplexobj(S):
+        E = np.empty((n, n), dtype=np.complex128)
+        _check(lib().rrref_commutator_error_complex(_i64(n), _p(_c(F)), _p(_c(P)), _p(_c(S)), _p(E)))
+    else:
+        E = np.empty((n, n))
+        _check(lib().rrref_commutator_error_real(_i64(n), _p(_d(F)), _p(_d(P)), _p(_d(S)), _p(E)))
+    return E
+
+
+def diis_sequence(max_vectors, errors, values):
+    """Feed (errors[t], values[t]) into one reference Diis object; returns (outputs, weight counts)."""
+    is_c = np.iscomplexobj(errors) or np.iscomplexobj(values)
+    conv = _c if is_c else _d
+    errors, values = conv(errors), conv(values)
+    steps = errors.shape[0]
+    size = errors[0].size
+    out = np.empty_like(values)
+    wc = np.empty(steps, dtype=np.int64)
+    _check(lib().rrref_diis_sequence(ctypes.c_int(1 if is_c else 0), _i64(max_vectors), _i64(steps), _i64(size),
+                                     _p(errors), _p(values), _p(out), _p(wc)))
+    return out, wc
+
+
+def canonical_orth(S, thr=1e-10):
+    n = S.shape[0]
+    n_eff = _i64(0)
+    if np.iscomplexobj(S):
+        X = np.zeros((n * n,), dtype=np.complex128)
+        _check(lib().rrref_canonical_orth_hermitian(_i64(n), _p(_c(S)), ctypes.c_double(thr), _p(X),
+                                                    ctypes.byref(n_eff)))
+    else:
+        X = np.zeros((n * n,))
+        _check(lib().rrref_canonical_orth(_i64(n), _p(_d(S)), ctypes.c_double(thr), _p(X), ctypes.byref(n_eff)))
+    return X[: n * n_eff.value].reshape(n, n_eff.value)
+
+
+def nonrel_scf(sysd, diis_size=5, max_iter=100, e_tol=1e-8, d_tol=1e-6):
+    n, B = sysd["n"], _d(sysd["B"])
+    X = _d(sysd["X"])
+    res = ScfResult()
+    P = np.empty((n, n))
+    hist = np.full(max_iter, np.nan)
+    _check(lib().rrref_nonrel_scf(_i64(n), _i64(B.shape[0]), _p(B), _p(_d(sysd["h"])), _p(X), _i64(X.shape[1]),
+                                  _p(_d(sysd["S"])), _p(_d(sysd["D0"])), ctypes.c_int(sysd["n_electrons"]),
+                                  ctypes.c_int(diis_size), ctypes.c_int(max_iter), ctypes.c_double(e_tol),
+                                  ctypes.c_double(d_tol), ctypes.byref(res), _p(P), _p(hist)))
+    return dict(energy=res.electronic_energy, iterations=res.iterations, converged=bool(res.converged), P=P,
+                history=hist[: res.iterations].copy())
+
+
+def x2c_scf(sysd, diis_size=5, max_iter=100, e_tol=1e-8, d_tol=1e-6, kramers=True):
+    nl, B = sysd["nl"], _d(sysd["B"])
+    X = _c(sysd["X"])
+    res = ScfResult()
+    P = np.empty((2 * nl, 2 * nl), dtype=np.complex128)
+    hist = np.full(max_iter, np.nan)
+    _check(lib().rrref_x2c_scf(_i64(nl), _i64(B.shape[0]), _p(B), _p(_c(sysd["h"])), _p(X), _i64(X.shape[1]),
+                               _p(_c(sysd["S"])), _p(_c(sysd["P0"])), ctypes.c_int(sysd["n_electrons"]),
+                               ctypes.c_int(diis_size), ctypes.c_int(max_iter), ctypes.c_double(e_tol),
+                               ctypes.c_double(d_tol), ctypes.c_int(1 if kramers else 0), ctypes.byref(res), _p(P),
+                               _p(hist)))
+    return dict(energy=res.electronic_energy, iterations=res.iterations, converged=bool(res.converged), P=P,
+                history=hist[: res.iterations].copy())
+
+
+def dhf_scf(sysd, diis_size=5, max_iter=100, e_tol=1e-8, d_tol=1e-6, kramers=True):
+    nl, ns = sysd["nl"], sysd["ns"]
+    n_rkb = sysd["n_rkb"]
+    x_full = _c(sysd["x_full"])
+    res = ScfResult()
+    P = np.empty((n_rkb, n_rkb), dtype=np.complex128)
+    hist = np.full(max_iter, np.nan)
+    _check(lib().rrref_dhf_scf(_i64(nl), _i64(ns), _i64(sysd["B_LL"].shape[0]), _p(_d(sysd["B_LL"])),
+                               _p(_d(sysd["B_SS"])), _p(_c(sysd["v_total"])), _i64(n_rkb), _p(_c(sysd["s_full"])),
+                               _p(x_full), _i64(x_full.shape[1]), _p(_c(sysd["h"])), _p(_c(sysd["P0"])),
+                               ctypes.c_int(sysd["n_electrons"]), ctypes.c_int(diis_size), ctypes.c_int(max_iter),
+                               ctypes.c_double(e_tol), ctypes.c_double(d_tol), ctypes.c_int(1 if kramers else 0),
+                               ctypes.byref(res), _p(P), _p(hist)))
+    return dict(energy=res.electronic_energy, iterations=res.iterations, converged=bool(res.converged), P=P,
+                history=hist[: res.iterations].copy())

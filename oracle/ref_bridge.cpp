@@ -1,0 +1,436 @@
+// Test infrastructure only: a C-ABI bridge onto the reference's OWN RI functions, compiled
+// unmodified from the reference source tree by oracle/Makefile into oracle/_ref/librrref.so.
+// Only tests/, tests/golden/make_golden.py and bench.py's CPU-baseline leg load it; the product
+// library never links it.  Every entry point copies plain row-major buffers into the reference's
+// Matrix<T> value types, calls the reference function named in its comment, and copies the result
+// back.  Complex buffers are interleaved (re, im) doubles, i.e. std::complex<double> layout.
+// Errors (std::exception) are caught and reported as return code 1; 0 means success.
+#include <omp.h>
+
+#include <complex>
+#include <cstdint>
+#include <cstring>
+#include <deque>
+#include <exception>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "C4_DHF.h"
+#include "DIIS.h"
+#include "LinearAlgebra.h"
+#include "NonRelFockMatrixRi.h"
+#include "NonRelHartreeFock.h"
+#include "NonRelSpinRiMoEri.h"
+#include "RiGemmFock.h"
+#include "RiSigmaGemm.h"
+#include "RiMoEri.h"
+#include "UkbFockMatrixRi.h"
+#include "X2C_FockMatrixRi.h"
+#include "X2C_HF.h"
+#include "JkOnlyFock.h"
+#include "HartreeExchangeGradient.h"
+
+extern "C" void scipy_openblas_set_num_threads(int n);
+
+using rerdmft::Matrix;
+using C = std::complex<double>;
+using i64 = std::int64_t;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <typename T>
+Matrix<T> toMatrix(const T* p, i64 rows, i64 cols) {
+  Matrix<T> m(static_cast<std::size_t>(rows), static_cast<std::size_t>(cols));
+  if (rows * cols > 0) std::memcpy(m.data(), p, sizeof(T) * static_cast<std::size_t>(rows * cols));
+  return m;
+}
+Matrix<C> toCMatrix(const double* p, i64 rows, i64 cols) {
+  return toMatrix<C>(reinterpret_cast<const C*>(p), rows, cols);
+}
+template <typename T>
+void fromMatrix(const Matrix<T>& m, T* out) {
+  if (m.rows() * m.cols() > 0) std::memcpy(out, m.data(), sizeof(T) * m.rows() * m.cols());
+}
+void fromCMatrix(const Matrix<C>& m, double* out) { fromMatrix<C>(m, reinterpret_cast<C*>(out)); }
+
+template <typename F>
+int guard(F&& f) {
+  try {
+    f();
+    return 0;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return 1;
+  }
+}
+
+}  // namespace
+
+// ---- Stubs for the non-RI overloads the SCF-loop translation units reference but the RI path
+// never calls (their real definitions need libcint, which is absent).  Each one throws. ----
+namespace rerdmft {
+[[noreturn]] static void notBuilt(const char* what) {
+  throw std::runtime_error(std::string(what) + ": non-RI two-electron path is not built into the oracle");
+}
+Matrix<double> nonRelFockMatrix(const Matrix<double>&, const AoCholesky&, const Matrix<double>&) {
+  notBuilt("nonRelFockMatrix(AoCholesky)");
+}
+Matrix<C> x2cFockMatrix(const Matrix<C>&, const AoCholesky&, const Matrix<C>&) { notBuilt("x2cFockMatrix"); }
+Matrix<C> x2cFockMatrix(const Matrix<C>&, const PackedTwoElectronTensor&, const Matrix<C>&) {
+  notBuilt("x2cFockMatrix");
+}
+Matrix<C> x2cFockMatrix(const Matrix<C>&, const Tensor4<double>&, const Matrix<C>&) { notBuilt("x2cFockMatrix"); }
+Matrix<C> rkbFockMatrix(const Matrix<C>&, const RkbCholesky&, const Matrix<C>&) { notBuilt("rkbFockMatrix"); }
+Matrix<C> rkbFockMatrix(const Matrix<C>&, const SymmetricEri<C>&, const Matrix<C>&) { notBuilt("rkbFockMatrix"); }
+Matrix<C> rkbFockMatrix(const Matrix<C>&, const UkbDirectEriSource&, const Matrix<C>&) {
+  notBuilt("rkbFockMatrix");
+}
+template <>
+double CholeskyEri<double>::operator()(std::size_t, std::size_t, std::size_t, std::size_t) const {
+  notBuilt("CholeskyEri");
+}
+template <>
+C CholeskyEri<C>::operator()(std::size_t, std::size_t, std::size_t, std::size_t) const { notBuilt("CholeskyEri"); }
+}  // namespace rerdmft
+
+extern "C" {
+
+const char* rrref_last_error() { return g_last_error.c_str(); }
+
+// OpenMP threads for the reference's parallel loops; BLAS stays serial inside them, exactly as
+// the reference expects (src/Utils/BlasThreads.h).
+void rrref_set_threads(int n) {
+  scipy_openblas_set_num_threads(1);
+  omp_set_num_threads(n > 0 ? n : 1);
+}
+
+// src/NON_REL/NonRelFockMatrixRi.cpp:71 nonRelFockMatrix(h, RiNonRelEriSource, D)
+int rrref_nonrel_fock(i64 n, i64 naux, const double* B, const double* h, const double* D, const double* S,
+                      const double* X, i64 n_eff, double* F) {
+  return guard([&] {
+    rerdmft::RiNonRelEriSource src;
+    src.nl = static_cast<std::size_t>(n);
+    src.eri3_L = toMatrix(B, naux, n * n);
+    src.x_large = toMatrix(X, n, n_eff);
+    src.overlap = toMatrix(S, n, n);
+    fromMatrix(rerdmft::nonRelFockMatrix(toMatrix(h, n, n), src, toMatrix(D, n, n)), F);
+  });
+}
+
+// src/X2C_DHF/X2C_FockMatrixRi.cpp:79 x2cFockMatrix(h_x2c, RiX2cEriSource, P); complex 2nl x 2nl.
+int rrref_x2c_fock(i64 nl, i64 naux, const double* B, const double* h, const double* P, const double* S,
+                   const double* X, i64 n_eff, double* F) {
+  return guard([&] {
+    rerdmft::RiX2cEriSource src;
+    src.nl = static_cast<std::size_t>(nl);
+    src.eri3_L = toMatrix(B, naux, nl * nl);
+    src.x_large = toCMatrix(X, 2 * nl, n_eff);
+    src.overlap = toCMatrix(S, 2 * nl, 2 * nl);
+    fromCMatrix(rerdmft::x2cFockMatrix(toCMatrix(h, 2 * nl, 2 * nl), src, toCMatrix(P, 2 * nl, 2 * nl)), F);
+  });
+}
+
+// src/UKB/UkbFockMatrixRi.cpp:35 riFockTwoElectronDirect(nl, ns, B_LL, B_SS, P_ukb, C_occ_ukb, occ)
+int rrref_ukb_two_electron(i64 nl, i64 ns, i64 naux, const double* B_LL, const double* B_SS, const double* P_ukb,
+                           const double* C_occ, i64 n_occ, const double* occ, double* G) {
+  return guard([&] {
+    const i64 nu = 2 * nl + 2 * ns;
+    std::vector<double> o(occ, occ + n_occ);
+    fromCMatrix(rerdmft::riFockTwoElectronDirect(static_cast<std::size_t>(nl), static_cast<std::size_t>(ns),
+                                                 toMatrix(B_LL, naux, nl * nl), toMatrix(B_SS, naux, ns * ns),
+                                                 toCMatrix(P_ukb, nu, nu), toCMatrix(C_occ, nu, n_occ), o),
+                G);
+  });
+}
+
+static rerdmft::RiDirectEriSource makeDirect(i64 nl, i64 ns, i64 naux, const double* B_LL, const double* B_SS,
+                                             const double* v_total, i64 n_rkb, const double* s_full,
+                                             const double* x_full, i64 n_eff) {
+  rerdmft::RiDirectEriSource src;
+  src.nl = static_cast<std::size_t>(nl);
+  src.ns = static_cast<std::size_t>(ns);
+  src.eri3_LL = toMatrix(B_LL, naux, nl * nl);
+  src.eri3_SS = toMatrix(B_SS, naux, ns * ns);
+  const i64 nu = 2 * nl + 2 * ns;
+  if (v_total) src.v_total = toCMatrix(v_total, nu, n_rkb);
+  if (s_full) src.s_full = toCMatrix(s_full, n_rkb, n_rkb);
+  if (x_full) src.x_full = toCMatrix(x_full, n_rkb, n_eff);
+  return src;
+}
+
+// src/UKB/UkbFockMatrixRi.cpp:185 rkbFockMatrix(h_rkb, RiDirectEriSource, P)
+int rrref_rkb_fock(i64 nl, i64 ns, i64 naux, const double* B_LL, const double* B_SS, const double* v_total,
+                   i64 n_rkb, const double* s_full, const double* x_full, i64 n_eff, const double* h,
+                   const double* P, double* F) {
+  return guard([&] {
+    auto src = makeDirect(nl, ns, naux, B_LL, B_SS, v_total, n_rkb, s_full, x_full, n_eff);
+    fromCMatrix(rerdmft::rkbFockMatrix(toCMatrix(h, n_rkb, n_rkb), src, toCMatrix(P, n_rkb, n_rkb)), F);
+  });
+}
+
+// src/NON_REL/NonRelSpinRiMoEri.cpp:13 buildRiNonRelSpinMoEri(B, n, C)
+int rrref_nonrel_mo_build(i64 n, i64 naux, const double* B, const double* Cs, double* out) {
+  return guard([&] {
+    auto eri = rerdmft::buildRiNonRelSpinMoEri(toMatrix(B, naux, n * n), static_cast<std::size_t>(n),
+                                               toMatrix(Cs, n, n));
+    fromMatrix(eri.b(), out);
+  });
+}
+
+// src/NON_REL/NonRelSpinRiMoEri.cpp:45 RiNonRelSpinMoEri::rotated(U), U is 2n x 2n
+int rrref_nonrel_mo_rotated(i64 n, i64 naux, const double* Bmo, const double* U, double* out) {
+  return guard([&] {
+    rerdmft::RiNonRelSpinMoEri eri(static_cast<std::size_t>(n), toMatrix(Bmo, naux, n * n));
+    fromMatrix(eri.rotated(toMatrix(U, 2 * n, 2 * n)).b(), out);
+  });
+}
+
+// src/NON_REL/NonRelSpinRiMoEri.h:77 embeddedB()
+int rrref_nonrel_mo_embedded(i64 n, i64 naux, const double* Bmo, double* out) {
+  return guard([&] {
+    rerdmft::RiNonRelSpinMoEri eri(static_cast<std::size_t>(n), toMatrix(Bmo, naux, n * n));
+    fromMatrix(eri.embeddedB(), out);
+  });
+}
+
+// src/NON_REL/NonRelSpinRiMoEri.h:40 operator()(a,b,c,d) over `count` index quadruples.
+int rrref_nonrel_mo_eri(i64 n, i64 naux, const double* Bmo, i64 count, const i64* abcd, double* out) {
+  return guard([&] {
+    rerdmft::RiNonRelSpinMoEri eri(static_cast<std::size_t>(n), toMatrix(Bmo, naux, n * n));
+    for (i64 t = 0; t < count; ++t)
+      out[t] = eri(static_cast<std::size_t>(abcd[4 * t]), static_cast<std::size_t>(abcd[4 * t + 1]),
+                   static_cast<std::size_t>(abcd[4 * t + 2]), static_cast<std::size_t>(abcd[4 * t + 3]));
+  });
+}
+
+// src/UKB/RiMoEri.cpp:64 buildRiMoEri(RiDirectEriSource, c_ukb); c_ukb is n_ukb x n_total complex.
+int rrref_ri_mo_build(i64 nl, i64 ns, i64 naux, const double* B_LL, const double* B_SS, const double* c_ukb,
+                      i64 n_total, double* out) {
+  return guard([&] {
+    auto src = makeDirect(nl, ns, naux, B_LL, B_SS, nullptr, 0, nullptr, nullptr, 0);
+    fromCMatrix(rerdmft::buildRiMoEri(src, toCMatrix(c_ukb, 2 * nl + 2 * ns, n_total)).b(), out);
+  });
+}
+
+// src/UKB/RiMoEri.cpp:88 RiMoEri::rotated(U)
+int rrref_ri_mo_rotated(i64 n, i64 naux, const double* Bmo, const double* U, double* out) {
+  return guard([&] {
+    rerdmft::RiMoEri eri(static_cast<std::size_t>(n), toCMatrix(Bmo, naux, n * n));
+    fromCMatrix(eri.rotated(toCMatrix(U, n, n)).b(), out);
+  });
+}
+
+// src/UKB/RiMoEri.cpp:112 RiMoEri::positiveBlock(off)
+int rrref_ri_mo_positive(i64 n, i64 naux, const double* Bmo, i64 off, double* out) {
+  return guard([&] {
+    rerdmft::RiMoEri eri(static_cast<std::size_t>(n), toCMatrix(Bmo, naux, n * n));
+    fromCMatrix(eri.positiveBlock(static_cast<std::size_t>(off)).b(), out);
+  });
+}
+
+// src/UKB/RiMoEri.h:50 operator()(a,b,c,d) over `count` quadruples; out is complex.
+int rrref_ri_mo_eri(i64 n, i64 naux, const double* Bmo, i64 count, const i64* abcd, double* out) {
+  return guard([&] {
+    rerdmft::RiMoEri eri(static_cast<std::size_t>(n), toCMatrix(Bmo, naux, n * n));
+    C* o = reinterpret_cast<C*>(out);
+    for (i64 t = 0; t < count; ++t)
+      o[t] = eri(static_cast<std::size_t>(abcd[4 * t]), static_cast<std::size_t>(abcd[4 * t + 1]),
+                 static_cast<std::size_t>(abcd[4 * t + 2]), static_cast<std::size_t>(abcd[4 * t + 3]));
+  });
+}
+
+static std::vector<std::size_t> pairVec(const i64* pair_of, i64 n) {
+  std::vector<std::size_t> v;
+  if (pair_of)
+    for (i64 i = 0; i < n; ++i) v.push_back(static_cast<std::size_t>(pair_of[i]));
+  return v;
+}
+
+// src/Hessian_opt/RiGemmFock.cpp:173 hartreeExchangeFockMatrix(h, RiNonRelSpinMoEri, ...): n_sp spatial
+// orbitals, h/h2/x2/l1/l2 are (2 n_sp)^2; pair_of may be null (no L terms).  use_reference selects the
+// reference's own element-by-element A/B path (RERDMFT_RI_HV_REFERENCE).
+int rrref_hx_fock_nonrel(i64 n_sp, i64 naux, const double* Bmo, const double* h, const double* occ,
+                         const double* h2, const double* x2, const i64* pair_of, const double* l1,
+                         const double* l2, int use_reference, double* F) {
+  return guard([&] {
+    const i64 n = 2 * n_sp;
+    rerdmft::risigma::useReferenceFlag() = use_reference != 0;
+    rerdmft::RiNonRelSpinMoEri eri(static_cast<std::size_t>(n_sp), toMatrix(Bmo, naux, n_sp * n_sp));
+    std::vector<double> o(occ, occ + n);
+    Matrix<double> L1 = pair_of ? toMatrix(l1, n, n) : Matrix<double>();
+    Matrix<double> L2 = pair_of ? toMatrix(l2, n, n) : Matrix<double>();
+    auto f = rerdmft::hartreeExchangeFockMatrix(toMatrix(h, n, n), eri, o, toMatrix(h2, n, n), toMatrix(x2, n, n),
+                                                pairVec(pair_of, n), L1, L2);
+    rerdmft::risigma::useReferenceFlag() = false;
+    fromMatrix(f, F);
+  });
+}
+
+// src/Hessian_opt/RiGemmFock.cpp:161 hartreeExchangeFockMatrix(h, RiMoEri, ...): complex, n x n.
+int rrref_hx_fock_complex(i64 n, i64 naux, const double* Bmo, const double* h, const double* occ, const double* h2,
+                          const double* x2, const i64* pair_of, const double* l1, const double* l2,
+                          int use_reference, double* F) {
+  return guard([&] {
+    rerdmft::risigma::useReferenceFlag() = use_reference != 0;
+    rerdmft::RiMoEri eri(static_cast<std::size_t>(n), toCMatrix(Bmo, naux, n * n));
+    std::vector<double> o(occ, occ + n);
+    Matrix<double> L1 = pair_of ? toMatrix(l1, n, n) : Matrix<double>();
+    Matrix<double> L2 = pair_of ? toMatrix(l2, n, n) : Matrix<double>();
+    auto f = rerdmft::hartreeExchangeFockMatrix(toCMatrix(h, n, n), eri, o, toMatrix(h2, n, n), toMatrix(x2, n, n),
+                                                pairVec(pair_of, n), L1, L2);
+    rerdmft::risigma::useReferenceFlag() = false;
+    fromCMatrix(f, F);
+  });
+}
+
+// src/Utils/DIIS.cpp:53 scfCommutatorError (real and complex)
+int rrref_commutator_error_real(i64 n, const double* F, const double* P, const double* S, double* E) {
+  return guard([&] {
+    fromMatrix(rerdmft::scfCommutatorError(toMatrix(F, n, n), toMatrix(P, n, n), toMatrix(S, n, n)), E);
+  });
+}
+int rrref_commutator_error_complex(i64 n, const double* F, const double* P, const double* S, double* E) {
+  return guard([&] {
+    fromCMatrix(rerdmft::scfCommutatorError(toCMatrix(F, n, n), toCMatrix(P, n, n), toCMatrix(S, n, n)), E);
+  });
+}
+
+// src/Utils/DIIS.cpp:79 Diis<T>::extrapolate, driven over a whole sequence: step t feeds
+// (errors[t], values[t]) into one Diis object and writes its result to out[t]; weights_count[t]
+// receives lastWeights().size().  is_complex selects Diis<complex<double>>.
+int rrref_diis_sequence(int is_complex, i64 max_vectors, i64 steps, i64 size, const double* errors,
+                        const double* values, double* out, i64* weights_count) {
+  return guard([&] {
+    const i64 stride = is_complex ? 2 * size : size;
+    if (is_complex) {
+      rerdmft::Diis<C> d(static_cast<std::size_t>(max_vectors));
+      for (i64 t = 0; t < steps; ++t) {
+        auto r = d.extrapolate(toCMatrix(errors + t * stride, 1, size), toCMatrix(values + t * stride, 1, size));
+        fromCMatrix(r, out + t * stride);
+        weights_count[t] = static_cast<i64>(d.lastWeights().size());
+      }
+    } else {
+      rerdmft::Diis<double> d(static_cast<std::size_t>(max_vectors));
+      for (i64 t = 0; t < steps; ++t) {
+        auto r = d.extrapolate(toMatrix(errors + t * stride, 1, size), toMatrix(values + t * stride, 1, size));
+        fromMatrix(r, out + t * stride);
+        weights_count[t] = static_cast<i64>(d.lastWeights().size());
+      }
+    }
+  });
+}
+
+// src/Linear_Algebra/LinearAlgebra.cpp:267 canonicalOrthogonalize; X_out must hold n*n doubles.
+int rrref_canonical_orth(i64 n, const double* S, double thr, double* X_out, i64* n_eff) {
+  return guard([&] {
+    auto x = rerdmft::canonicalOrthogonalize(toMatrix(S, n, n), thr);
+    *n_eff = static_cast<i64>(x.cols());
+    fromMatrix(x, X_out);
+  });
+}
+// src/Linear_Algebra/LinearAlgebra.cpp:312 canonicalOrthogonalizeHermitian; X_out holds n*n complex.
+int rrref_canonical_orth_hermitian(i64 n, const double* S, double thr, double* X_out, i64* n_eff) {
+  return guard([&] {
+    auto x = rerdmft::canonicalOrthogonalizeHermitian(toCMatrix(S, n, n), thr);
+    *n_eff = static_cast<i64>(x.cols());
+    fromCMatrix(x, X_out);
+  });
+}
+// src/Linear_Algebra/LinearAlgebra.cpp:51 / :122 diagonalizeSymmetric / diagonalizeHermitian
+int rrref_diag_sym(i64 n, const double* A, double* w, double* V) {
+  return guard([&] {
+    auto r = rerdmft::diagonalizeSymmetric(toMatrix(A, n, n));
+    std::memcpy(w, r.eigenvalues.data(), sizeof(double) * static_cast<std::size_t>(n));
+    fromMatrix(r.eigenvectors, V);
+  });
+}
+int rrref_diag_herm(i64 n, const double* A, double* w, double* V) {
+  return guard([&] {
+    auto r = rerdmft::diagonalizeHermitian(toCMatrix(A, n, n));
+    std::memcpy(w, r.eigenvalues.data(), sizeof(double) * static_cast<std::size_t>(n));
+    fromCMatrix(r.eigenvectors, V);
+  });
+}
+
+// SCF result record shared by the three loop wrappers below.
+struct rrref_scf_result {
+  double electronic_energy;
+  i64 iterations;
+  i64 converged;
+};
+
+static void copyHistory(const std::vector<double>& e, double* hist, i64 max_iter) {
+  for (std::size_t i = 0; i < e.size() && static_cast<i64>(i) < max_iter; ++i) hist[i] = e[i];
+}
+
+// src/NON_REL/NonRelHartreeFock.cpp:219 runNonRelativisticHartreeFock(RiNonRelEriSource, ...) with an
+// empty geometry (nuclear repulsion 0).  energy_history gets one electronic energy per iteration.
+int rrref_nonrel_scf(i64 n, i64 naux, const double* B, const double* h, const double* X, i64 n_eff,
+                     const double* S, const double* P0, int n_electrons, int diis_size, int max_iter, double e_tol,
+                     double d_tol, rrref_scf_result* res, double* P_out, double* energy_history) {
+  return guard([&] {
+    rerdmft::RiNonRelEriSource src;
+    src.nl = static_cast<std::size_t>(n);
+    src.eri3_L = toMatrix(B, naux, n * n);
+    src.x_large = toMatrix(X, n, n_eff);
+    src.overlap = toMatrix(S, n, n);
+    auto r = rerdmft::runNonRelativisticHartreeFock(src, toMatrix(h, n, n), src.x_large, toMatrix(P0, n, n),
+                                                     n_electrons, {}, 1.0, src.overlap, diis_size, max_iter, e_tol,
+                                                     d_tol);
+    res->electronic_energy = r.electronic_energy;
+    res->iterations = r.iterations;
+    res->converged = r.converged ? 1 : 0;
+    fromMatrix(r.density_matrix, P_out);
+    std::vector<double> e;
+    for (const auto& rec : r.history) e.push_back(rec.energy);
+    copyHistory(e, energy_history, max_iter);
+  });
+}
+
+// src/X2C_DHF/X2C_HF.cpp:175 runX2CHartreeFockScf(h_x2c, RiX2cEriSource, ...)
+int rrref_x2c_scf(i64 nl, i64 naux, const double* B, const double* h, const double* X, i64 n_eff, const double* S,
+                  const double* P0, int n_electrons, int diis_size, int max_iter, double e_tol, double d_tol,
+                  int kramers, rrref_scf_result* res, double* P_out, double* energy_history) {
+  return guard([&] {
+    rerdmft::RiX2cEriSource src;
+    src.nl = static_cast<std::size_t>(nl);
+    src.eri3_L = toMatrix(B, naux, nl * nl);
+    src.x_large = toCMatrix(X, 2 * nl, n_eff);
+    src.overlap = toCMatrix(S, 2 * nl, 2 * nl);
+    auto r = rerdmft::runX2CHartreeFockScf(toCMatrix(h, 2 * nl, 2 * nl), src, src.x_large,
+                                           toCMatrix(P0, 2 * nl, 2 * nl), n_electrons, {}, 1.0, src.overlap,
+                                           diis_size, max_iter, e_tol, d_tol, kramers != 0);
+    res->electronic_energy = r.electronic_energy;
+    res->iterations = r.iterations;
+    res->converged = r.converged ? 1 : 0;
+    fromCMatrix(r.density_matrix, P_out);
+    std::vector<double> e;
+    for (const auto& rec : r.history) e.push_back(rec.energy);
+    copyHistory(e, energy_history, max_iter);
+  });
+}
+
+// src/C4_DHF/C4_DHF.cpp:178 runDiracHartreeFockScf(h_rkb, RiDirectEriSource, ...)
+int rrref_dhf_scf(i64 nl, i64 ns, i64 naux, const double* B_LL, const double* B_SS, const double* v_total,
+                  i64 n_rkb, const double* s_full, const double* x_full, i64 n_eff, const double* h,
+                  const double* P0, int n_electrons, int diis_size, int max_iter, double e_tol, double d_tol,
+                  int kramers, rrref_scf_result* res, double* P_out, double* energy_history) {
+  return guard([&] {
+    auto src = makeDirect(nl, ns, naux, B_LL, B_SS, v_total, n_rkb, s_full, x_full, n_eff);
+    auto r = rerdmft::runDiracHartreeFockScf(toCMatrix(h, n_rkb, n_rkb), src, src.x_full,
+                                             toCMatrix(P0, n_rkb, n_rkb), n_electrons, {}, 1.0, src.s_full,
+                                             diis_size, max_iter, e_tol, d_tol, kramers != 0);
+    res->electronic_energy = r.electronic_energy;
+    res->iterations = r.iterations;
+    res->converged = r.converged ? 1 : 0;
+    fromCMatrix(r.density_matrix, P_out);
+    std::vector<double> e;
+    for (const auto& rec : r.history) e.push_back(rec.energy);
+    copyHistory(e, energy_history, max_iter);
+  });
+}
+
+}  // extern "C"
