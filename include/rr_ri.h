@@ -1,0 +1,97 @@
+/* librr_ri — B200-native (sm_100a) RI two-electron hot path of ReRDMFT, C ABI.
+ *
+ * Drop-in boundary: the reference's C++ overload set keyed on the ERI-source struct
+ * (src/NON_REL/NonRelFockMatrixRi.h:39, src/X2C_DHF/X2C_FockMatrixRi.h:38,
+ * src/UKB/UkbFockMatrixRi.h:70 and :96, src/UKB/RiMoEri.h:91, src/NON_REL/NonRelSpinRiMoEri.h:101,
+ * src/Hessian_opt/RiGemmFock.h:20-36).  The reference's source structs hold the 3-center tensor
+ * by value; here it is uploaded ONCE into a handle and stays resident in HBM, and every call
+ * passes only the small per-iteration matrices.  include/rr_ri.hpp re-creates the reference's
+ * C++ overloads on top of these functions.
+ *
+ * Conventions
+ *  - Matrices are row-major (the reference's Matrix<T>, src/Matrix.h:13).  Complex matrices are
+ *    interleaved (re, im) doubles, i.e. std::complex<double> / numpy complex128 layout.
+ *  - The RI tensor is (naux, n*n) row-major, B[P*n*n + m*n + k] = (mk|P)
+ *    (src/AO_ints/ThreeCenterIntegrals.h:68 convention).
+ *  - Every function returns RR_OK (0) or an RR_ERR_* code; rr_last_error() gives the message
+ *    (thread-local).  Where the reference throws std::runtime_error on a dimension mismatch,
+ *    the same condition returns RR_ERR_ARG.  No C++ exception crosses this boundary.
+ *  - Pointer arguments live in host memory unless rr_opts.mem == RR_MEM_DEVICE (then they are
+ *    device pointers on the handle's device).  Host outputs are complete on return.
+ */
+#ifndef RR_RI_H
+#define RR_RI_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RR_OK 0
+#define RR_ERR_ARG 1         /* invalid argument or dimension mismatch */
+#define RR_ERR_CUDA 2        /* CUDA runtime error (message in rr_last_error) */
+#define RR_ERR_SOLVER 3      /* eigensolver failure (reference: LAPACKE_* failed to converge) */
+#define RR_ERR_TIMEOUT 4     /* a bounded device-side wait expired (kernel status word) */
+#define RR_ERR_NOMEM 5       /* device allocation failed */
+#define RR_ERR_STATE 6       /* handle in the wrong state for this call */
+#define RR_ERR_UNSUPPORTED 7 /* option not supported by this build */
+
+#define RR_MEM_HOST 0
+#define RR_MEM_DEVICE 1
+
+#define RR_PREC_FP64 0  /* every contraction in FP64 (DMMA tensor cores); matches the reference to ~1e-12 */
+#define RR_PREC_MIXED 1 /* exchange contractions in split-BF16 (3 products, FP32 accumulate) on tcgen05 */
+
+typedef struct rr_ri_store* rr_ri_handle;
+
+typedef struct rr_opts {
+  int32_t mem;       /* RR_MEM_HOST (default) or RR_MEM_DEVICE for every matrix argument of the call */
+  int32_t precision; /* RR_PREC_FP64 (default) or RR_PREC_MIXED */
+  void* stream;      /* cudaStream_t for the call; NULL = the handle's own stream */
+  int32_t sync;      /* device-pointer calls: 1 = block until done (host-pointer calls always block) */
+  int32_t reserved;
+} rr_opts;
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* rr_last_error(void);
+/* Library version, major*10000 + minor*100 + patch. */
+int rr_version(void);
+
+/* Uploads the (naux, n*n) RI tensor once and keeps it resident in HBM.
+ * Replaces constructing RiNonRelEriSource / RiX2cEriSource (src/NON_REL/NonRelFockMatrixRi.h:30,
+ * src/X2C_DHF/X2C_FockMatrixRi.h:29): both hold eri3_L of this shape.  mem: RR_MEM_HOST or
+ * RR_MEM_DEVICE for B.  The handle binds to the current CUDA device. */
+int rr_ri_create(const double* B, int64_t naux, int64_t n, int32_t mem, rr_ri_handle* out);
+
+/* 4-component variant: eri3_LL (naux, nl*nl) and eri3_SS (naux, ns*ns) sharing the aux index
+ * (src/UKB/UkbFockMatrixRi.h:84 RiDirectEriSource). */
+int rr_ri_create_4c(const double* B_LL, const double* B_SS, int64_t naux, int64_t nl, int64_t ns, int32_t mem,
+                    rr_ri_handle* out);
+
+int rr_ri_destroy(rr_ri_handle h);
+
+/* naux, n (nl for 4c) and ns (0 for a single-tensor handle). */
+int rr_ri_info(rr_ri_handle h, int64_t* naux, int64_t* n, int64_t* ns);
+
+/* Blocks until all work queued on the handle's streams is done; reports a device status error
+ * (RR_ERR_TIMEOUT) left by an earlier asynchronous call. */
+int rr_ri_sync(rr_ri_handle h);
+
+/* Restricted nonrelativistic RI Fock matrix, F = h + J - K/2 (n x n, real).
+ * Replaces nonRelFockMatrix(h_core, RiNonRelEriSource, D), src/NON_REL/NonRelFockMatrixRi.cpp:71:
+ * D is the full (factor-2) density; the occupied orbitals are recovered from X^T (S D S / 2) X
+ * (eigenvalues > 0.5) with the caller's X (n x n_eff) and S, exactly as the reference does. */
+int rr_ri_fock_nonrel(rr_ri_handle h, const double* h_core, const double* D, const double* S, const double* X,
+                      int64_t n_eff, double* F, const rr_opts* opts);
+
+/* Coulomb and exchange from given occupied coefficients: J(D = 2 C C^T) and
+ * K' = sum_P (C^T B^P)^T (C^T B^P) (so F = h + J - K'), C is n x n_occ.  The building block of
+ * the device-resident SCF loop; equal to rr_ri_fock_nonrel when D = 2 C C^T. */
+int rr_ri_jk_occupied(rr_ri_handle h, const double* C_occ, int64_t n_occ, double* J, double* K, const rr_opts* opts);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RR_RI_H */

@@ -1,0 +1,28 @@
+/* librr_ri test hooks: direct access to the internal kernel families for unit tests.
+ * All pointers are DEVICE pointers; calls are synchronous.  No reference counterpart: these
+ * exist so the DMMA GEMM and the J streaming passes can be checked in isolation. */
+#ifndef RR_RI_TESTING_H
+#define RR_RI_TESTING_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* C[b] = alpha op(A[b]) op(B[b]) + beta C[b] on the FP64 DMMA GEMM (row-major; op 0 = N, 1 = T;
+ * cplx: interleaved complex; mirror +1/-1 fills the strict lower triangle from the upper one;
+ * allow_split lets the kernel split K with a deterministic reduction). */
+int rr_test_gemm_f64(int64_t M, int64_t N, int64_t K, const double* A, int64_t lda, int64_t strideA, int32_t opA,
+                     const double* B, int64_t ldb, int64_t strideB, int32_t opB, double* C, int64_t ldc,
+                     int64_t strideC, double alpha, double beta, int64_t batch, int32_t cplx, int32_t conjA,
+                     int32_t conjB, int32_t mirror, int32_t allow_split);
+
+/* gamma = B vec(D) and J = B^T gamma through the TMA streaming passes (B: naux x n2, dense). */
+int rr_test_j_passes(const double* B, int64_t naux, int64_t n2, const double* D, double* gamma, double* J);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RR_RI_TESTING_H */

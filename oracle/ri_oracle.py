@@ -243,8 +243,10 @@ def jkl_matrices(Bmo, n, pair_of=None):
     K = np.einsum("Pij,Pji->ij", b3, b3, optimize=True)
     L = None
     if pair_of is not None:
-        pb = b3[:, np.asarray(pair_of), :]  # B(P, ibar, j)
-        L = np.einsum("Pij,Pji->ij", pb, np.transpose(pb, (0, 2, 1)), optimize=True)
+        po = np.asarray(pair_of)
+        pb = b3[:, po, :]  # [P, i, j] = B(P, ibar, j)
+        qb = np.transpose(b3[:, :, po], (0, 2, 1))  # [P, i, j] = B(P, j, ibar)
+        L = np.einsum("Pij,Pij->ij", pb, qb, optimize=True)
     return J, K, L
 
 

@@ -1,0 +1,87 @@
+"""ctypes binding of librr_ri.so (the in-tree CUDA library, C ABI in include/rr_ri.h).
+
+There is no CPU fallback: if the library is missing or cannot be loaded every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "librr_ri.so"
+
+RR_OK, RR_ERR_ARG, RR_ERR_CUDA, RR_ERR_SOLVER, RR_ERR_TIMEOUT, RR_ERR_NOMEM, RR_ERR_STATE, RR_ERR_UNSUPPORTED = range(8)
+RR_MEM_HOST, RR_MEM_DEVICE = 0, 1
+RR_PREC_FP64, RR_PREC_MIXED = 0, 1
+
+_i64 = ctypes.c_int64
+_i32 = ctypes.c_int32
+_vp = ctypes.c_void_p
+_d = ctypes.c_double
+
+
+class RrError(RuntimeError):
+    """Raised when a librr_ri call returns a non-zero status (the reference throws
+    std::runtime_error at the same points)."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[rr error {code}] {msg}")
+        self.code = code
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [("mem", _i32), ("precision", _i32), ("stream", _vp), ("sync", _i32), ("reserved", _i32)]
+
+
+class ScfOpts(ctypes.Structure):
+    _fields_ = [("diis_size", _i32), ("max_iterations", _i32), ("energy_tolerance", _d),
+                ("density_tolerance", _d), ("kramers_restricted", _i32), ("precision", _i32),
+                ("mixed_switch", _d), ("rebuild_every", _i32), ("reserved", _i32)]
+
+
+class ScfResult(ctypes.Structure):
+    _fields_ = [("electronic_energy", _d), ("iterations", _i64), ("converged", _i64),
+                ("mixed_iterations", _i64), ("fp64_iterations", _i64), ("seconds", _d)]
+
+
+_SIGS = {
+    "rr_last_error": (ctypes.c_char_p, []),
+    "rr_version": (ctypes.c_int, []),
+    "rr_ri_create": (ctypes.c_int, [_vp, _i64, _i64, _i32, ctypes.POINTER(_vp)]),
+    "rr_ri_create_4c": (ctypes.c_int, [_vp, _vp, _i64, _i64, _i64, _i32, ctypes.POINTER(_vp)]),
+    "rr_ri_destroy": (ctypes.c_int, [_vp]),
+    "rr_ri_info": (ctypes.c_int, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
+    "rr_ri_sync": (ctypes.c_int, [_vp]),
+    "rr_ri_fock_nonrel": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _i64, _vp, ctypes.POINTER(Opts)]),
+    "rr_ri_jk_occupied": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp, ctypes.POINTER(Opts)]),
+    "rr_test_gemm_f64": (ctypes.c_int, [_i64, _i64, _i64, _vp, _i64, _i64, _i32, _vp, _i64, _i64, _i32, _vp, _i64,
+                                        _i64, _d, _d, _i64, _i32, _i32, _i32, _i32, _i32]),
+    "rr_test_j_passes": (ctypes.c_int, [_vp, _i64, _i64, _vp, _vp, _vp]),
+}
+
+_lib = None
+
+
+def lib():
+    """Loads librr_ri.so (raises if it is absent: there is no fallback path)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is not built; run `python -m rerdmft_b200.build`")
+        L = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name, None)
+            if f is None:
+                continue
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != RR_OK:
+        raise RrError(rc, lib().rr_last_error().decode())
+
+
+def opts(mem: int = RR_MEM_HOST, precision: int = RR_PREC_FP64, stream: int | None = None, sync: int = 1) -> Opts:
+    return Opts(mem, precision, stream, sync, 0)

@@ -1,0 +1,212 @@
+// extern "C" boundary of librr_ri (declared in include/rr_ri.h).  Every entry point converts
+// rr::Error (and any other exception) into a status code plus rr_last_error().
+#include <new>
+
+#include "ri_store.cuh"
+
+namespace rr {
+extern thread_local std::string g_last_error;
+void fock_nonrel(rr_ri_store*, const double*, const double*, const double*, const double*, int64_t, double*,
+                 const rr_opts*);
+void jk_occupied(rr_ri_store*, const double*, int64_t, double*, double*, const rr_opts*);
+}  // namespace rr
+
+namespace {
+
+template <typename F>
+int api(F&& f) {
+  try {
+    rr::g_last_error.clear();
+    f();
+    return RR_OK;
+  } catch (const rr::Error& e) {
+    rr::set_last_error(e.what());
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    rr::set_last_error("host allocation failed");
+    return RR_ERR_NOMEM;
+  } catch (const std::exception& e) {
+    rr::set_last_error(e.what());
+    return RR_ERR_CUDA;
+  }
+}
+
+void upload_tensor(rr::DevBuf<double>& dst, int64_t* pitch_out, const double* src, int64_t naux, int64_t n2, bool host,
+                   cudaStream_t s) {
+  const int64_t pitch = rr::round_up(std::max<int64_t>(n2, 2), 32);
+  *pitch_out = pitch;
+  dst.alloc(static_cast<size_t>(std::max<int64_t>(naux * pitch, 32)));
+  RR_CUDA(cudaMemsetAsync(dst.p, 0, sizeof(double) * dst.n, s));
+  if (naux && n2)
+    RR_CUDA(cudaMemcpy2DAsync(dst.p, sizeof(double) * pitch, src, sizeof(double) * n2, sizeof(double) * n2, naux,
+                              host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
+}
+
+rr_ri_store* checked(rr_ri_handle h) {
+  if (!h) throw rr::Error(RR_ERR_ARG, "null handle");
+  RR_CUDA(cudaSetDevice(h->ctx.device));
+  return h;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* rr_last_error(void) { return rr::g_last_error.c_str(); }
+
+int rr_version(void) { return 100; }
+
+int rr_ri_create(const double* B, int64_t naux, int64_t n, int32_t mem, rr_ri_handle* out) {
+  return api([&] {
+    RR_REQUIRE(out != nullptr, RR_ERR_ARG, "rr_ri_create: out is null");
+    *out = nullptr;
+    RR_REQUIRE(naux >= 0 && n >= 1, RR_ERR_ARG, "rr_ri_create: need naux >= 0 and n >= 1");
+    RR_REQUIRE(B != nullptr || naux == 0, RR_ERR_ARG, "rr_ri_create: B is null");
+    RR_REQUIRE(mem == RR_MEM_HOST || mem == RR_MEM_DEVICE, RR_ERR_ARG, "rr_ri_create: bad mem kind");
+    auto* h = new rr_ri_store();
+    try {
+      h->ctx.init(nullptr);
+      h->naux = naux;
+      h->n = n;
+      h->ntens = 1;
+      h->status.alloc(1);
+      RR_CUDA(cudaMemsetAsync(h->status.p, 0, sizeof(int), h->ctx.main));
+      upload_tensor(h->B[0], &h->pitch[0], B, naux, n * n, mem == RR_MEM_HOST, h->ctx.main);
+      RR_CUDA(cudaStreamSynchronize(h->ctx.main));
+    } catch (...) {
+      h->ctx.destroy();
+      delete h;
+      throw;
+    }
+    *out = h;
+  });
+}
+
+int rr_ri_create_4c(const double* B_LL, const double* B_SS, int64_t naux, int64_t nl, int64_t ns, int32_t mem,
+                    rr_ri_handle* out) {
+  return api([&] {
+    RR_REQUIRE(out != nullptr, RR_ERR_ARG, "rr_ri_create_4c: out is null");
+    *out = nullptr;
+    RR_REQUIRE(naux >= 0 && nl >= 1 && ns >= 0, RR_ERR_ARG, "rr_ri_create_4c: bad dimensions");
+    RR_REQUIRE((B_LL && (B_SS || ns == 0)) || naux == 0, RR_ERR_ARG, "rr_ri_create_4c: null tensor");
+    RR_REQUIRE(mem == RR_MEM_HOST || mem == RR_MEM_DEVICE, RR_ERR_ARG, "rr_ri_create_4c: bad mem kind");
+    auto* h = new rr_ri_store();
+    try {
+      h->ctx.init(nullptr);
+      h->naux = naux;
+      h->n = nl;
+      h->ns = ns;
+      h->ntens = 2;
+      h->status.alloc(1);
+      RR_CUDA(cudaMemsetAsync(h->status.p, 0, sizeof(int), h->ctx.main));
+      upload_tensor(h->B[0], &h->pitch[0], B_LL, naux, nl * nl, mem == RR_MEM_HOST, h->ctx.main);
+      upload_tensor(h->B[1], &h->pitch[1], B_SS, naux, ns * ns, mem == RR_MEM_HOST, h->ctx.main);
+      RR_CUDA(cudaStreamSynchronize(h->ctx.main));
+    } catch (...) {
+      h->ctx.destroy();
+      delete h;
+      throw;
+    }
+    *out = h;
+  });
+}
+
+int rr_ri_destroy(rr_ri_handle h) {
+  return api([&] {
+    if (!h) return;
+    cudaSetDevice(h->ctx.device);
+    cudaDeviceSynchronize();
+    h->ctx.destroy();
+    delete h;
+  });
+}
+
+int rr_ri_info(rr_ri_handle h, int64_t* naux, int64_t* n, int64_t* ns) {
+  return api([&] {
+    if (!h) throw rr::Error(RR_ERR_ARG, "null handle");
+    if (naux) *naux = h->naux;
+    if (n) *n = h->n;
+    if (ns) *ns = h->ns;
+  });
+}
+
+int rr_ri_sync(rr_ri_handle h) {
+  return api([&] {
+    auto* s = checked(h);
+    RR_CUDA(cudaStreamSynchronize(s->ctx.side));
+    rr::check_status(s, s->ctx.main);
+  });
+}
+
+int rr_ri_fock_nonrel(rr_ri_handle h, const double* h_core, const double* D, const double* S, const double* X,
+                      int64_t n_eff, double* F, const rr_opts* opts) {
+  return api([&] {
+    auto* s = checked(h);
+    RR_REQUIRE(h_core && D && S && F && (X || n_eff == 0), RR_ERR_ARG, "rr_ri_fock_nonrel: null matrix");
+    RR_REQUIRE(!opts || opts->precision == RR_PREC_FP64, RR_ERR_UNSUPPORTED,
+               "rr_ri_fock_nonrel: only RR_PREC_FP64 (the mixed path runs through rr_ri_jk_occupied / the SCF driver)");
+    rr::fock_nonrel(s, h_core, D, S, X, n_eff, F, opts);
+  });
+}
+
+int rr_ri_jk_occupied(rr_ri_handle h, const double* C_occ, int64_t n_occ, double* J, double* K, const rr_opts* opts) {
+  return api([&] {
+    auto* s = checked(h);
+    RR_REQUIRE((C_occ || n_occ == 0) && J && K, RR_ERR_ARG, "rr_ri_jk_occupied: null matrix");
+    RR_REQUIRE(!opts || opts->precision == RR_PREC_FP64, RR_ERR_UNSUPPORTED, "rr_ri_jk_occupied: precision");
+    rr::jk_occupied(s, C_occ, n_occ, J, K, opts);
+  });
+}
+
+}  // extern "C"
+
+// ---- test hooks (include/rr_ri_testing.h) ----
+extern "C" int rr_test_gemm_f64(int64_t M, int64_t N, int64_t K, const double* A, int64_t lda, int64_t strideA,
+                                int32_t opA, const double* B, int64_t ldb, int64_t strideB, int32_t opB, double* C,
+                                int64_t ldc, int64_t strideC, double alpha, double beta, int64_t batch, int32_t cplx,
+                                int32_t conjA, int32_t conjB, int32_t mirror, int32_t allow_split) {
+  return api([&] {
+    rr::GemmDesc g;
+    g.M = M; g.N = N; g.K = K;
+    g.A = A; g.lda = lda; g.strideA = strideA; g.opA = opA ? rr::Op::T : rr::Op::N;
+    g.B = B; g.ldb = ldb; g.strideB = strideB; g.opB = opB ? rr::Op::T : rr::Op::N;
+    g.C = C; g.ldc = ldc; g.strideC = strideC;
+    g.alpha = alpha; g.beta = beta; g.batch = batch;
+    g.cplx = cplx != 0; g.conjA = conjA != 0; g.conjB = conjB != 0; g.mirror = mirror;
+    rr::DevBuf<double> work;
+    int64_t cap = 0;
+    if (allow_split) {
+      cap = rr::gemm_work_doubles(g);
+      work.alloc(static_cast<size_t>(std::max<int64_t>(cap, 1)));
+    }
+    rr::gemm(g, nullptr, allow_split ? work.p : nullptr, cap);
+    RR_CUDA(cudaDeviceSynchronize());
+  });
+}
+
+extern "C" int rr_test_j_passes(const double* B, int64_t naux, int64_t n2, const double* D, double* gamma, double* J) {
+  return api([&] {
+    const int64_t pitch = rr::round_up(std::max<int64_t>(n2, 2), 32);
+    rr::DevBuf<double> Bp(static_cast<size_t>(std::max<int64_t>(naux * pitch, 32))), Dp(static_cast<size_t>(pitch));
+    rr::DevBuf<int> err(1);
+    RR_CUDA(cudaMemset(Bp.p, 0, sizeof(double) * Bp.n));
+    RR_CUDA(cudaMemset(Dp.p, 0, sizeof(double) * Dp.n));
+    RR_CUDA(cudaMemset(err.p, 0, sizeof(int)));
+    if (naux) RR_CUDA(cudaMemcpy2D(Bp.p, sizeof(double) * pitch, B, sizeof(double) * n2, sizeof(double) * n2, naux,
+                                   cudaMemcpyDeviceToDevice));
+    RR_CUDA(cudaMemcpy(Dp.p, D, sizeof(double) * n2, cudaMemcpyDeviceToDevice));
+    rr::JTensor t;
+    t.B = Bp.p; t.pitch = pitch; t.len = n2; t.D = Dp.p; t.J = J;
+    rr::JPlan pl = rr::j_plan(1, &t, naux);
+    rr::DevBuf<double> gp(static_cast<size_t>(std::max<int64_t>(pl.gpart_doubles, 1)));
+    rr::DevBuf<double> jp(static_cast<size_t>(std::max<int64_t>(pl.jpart_doubles, 1)));
+    rr::j_pass1(pl, gp.p, err.p, nullptr);
+    rr::j_gamma(pl, gp.p, gamma, nullptr);
+    rr::j_pass2(pl, gp.p, jp.p, err.p, nullptr);
+    rr::j_finish(pl, jp.p, 1.0, nullptr);
+    RR_CUDA(cudaDeviceSynchronize());
+    int e = 0;
+    RR_CUDA(cudaMemcpy(&e, err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    RR_REQUIRE(e == 0, RR_ERR_TIMEOUT, "rr_test_j_passes: device wait bound expired");
+  });
+}

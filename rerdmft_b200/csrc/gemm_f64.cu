@@ -1,0 +1,378 @@
+// FP64 DMMA GEMM: multistage cp.async pipeline (3 stages of 16-deep k tiles), warp tiles of
+// (MT*8) x (NT*8) built from mma.sync.m8n8k4.f64, optional complex (4M) accumulation, split-K
+// with a fixed-order reduction (bit-identical results run to run), and upper-triangle-only
+// scheduling for symmetric / Hermitian outputs.
+#include "gemm_f64.cuh"
+
+namespace rr {
+namespace {
+
+constexpr int KT = 16;
+constexpr int STAGES = 3;
+
+struct Params {
+  int64_t M, N, K;
+  const double* A;
+  int64_t lda, strideA;
+  const double* B;
+  int64_t ldb, strideB;
+  double* C;
+  int64_t ldc, strideC;
+  double alpha, beta;
+  int64_t batch;
+  int splits;
+  int64_t kchunk;
+  double* work;
+  double signA, signB;  // -1 conjugates the imaginary plane of A / B
+  int64_t c_plane_rows, c_plane_stride;
+  int upper_only;
+};
+
+__device__ __forceinline__ void cp_async8(uint32_t saddr, const void* g, int bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(g), "r"(bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+__host__ __device__ constexpr int pad_mn(int x) { return x + ((8 - x % 16) + 16) % 16; }
+
+template <int MT, int NT, int WM, int WN, bool AK, bool BKM, bool CPLX>
+struct Cfg {
+  static constexpr int BM = MT * 8 * WM, BN = NT * 8 * WN, THREADS = 32 * WM * WN, PL = CPLX ? 2 : 1;
+  static constexpr int A_LD = AK ? (KT + 4) : pad_mn(BM);
+  static constexpr int A_SZ = AK ? BM * A_LD : KT * A_LD;
+  static constexpr int B_LD = BKM ? (KT + 4) : pad_mn(BN);
+  static constexpr int B_SZ = BKM ? BN * B_LD : KT * B_LD;
+  static constexpr int STAGE = PL * (A_SZ + B_SZ);
+  static constexpr int SMEM_BYTES = STAGES * STAGE * 8;
+};
+
+// A tile: AK (A stored M x K, k contiguous) -> smem [BM][A_LD]; else (stored K x M) -> [KT][A_LD].
+// B tile: BKM (B stored N x K) -> smem [BN][B_LD]; else (stored K x N) -> [KT][B_LD].
+template <int MT, int NT, int WM, int WN, bool AK, bool BKM, bool CPLX>
+__global__ void __launch_bounds__(32 * WM * WN) dgemm_kernel(const Params p) {
+  using CF = Cfg<MT, NT, WM, WN, AK, BKM, CPLX>;
+  constexpr int BM = CF::BM, BN = CF::BN, THREADS = CF::THREADS, PL = CF::PL;
+  extern __shared__ __align__(16) double smem[];
+
+  const int64_t n0 = static_cast<int64_t>(blockIdx.x) * BN;
+  const int64_t m0 = static_cast<int64_t>(blockIdx.y) * BM;
+  if (p.upper_only && m0 > n0 + BN - 1) return;
+  const int64_t bz = blockIdx.z;
+  const int64_t b = bz / p.splits;
+  const int split = static_cast<int>(bz % p.splits);
+  const int64_t kbeg = split * p.kchunk;
+  const int64_t kend = min(p.K, kbeg + p.kchunk);
+  const int ktiles = kend > kbeg ? static_cast<int>((kend - kbeg + KT - 1) / KT) : 0;
+
+  const double* Ab = p.A + b * p.strideA * PL;
+  const double* Bb = p.B + b * p.strideB * PL;
+  const int tid = threadIdx.x;
+  const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+
+  auto load_stage = [&](int stage, int kt) {
+    const int64_t k0 = kbeg + static_cast<int64_t>(kt) * KT;
+    double* sA = smem + stage * CF::STAGE;
+    double* sB = sA + PL * CF::A_SZ;
+#pragma unroll 4
+    for (int e = tid; e < BM * KT; e += THREADS) {
+      int r, c;
+      int64_t gm, gk;
+      if constexpr (AK) { r = e / KT; c = e % KT; gm = m0 + r; gk = k0 + c; }
+      else { r = e / BM; c = e % BM; gk = k0 + r; gm = m0 + c; }
+      const bool ok = gm < p.M && gk < kend;
+      const int64_t off = ok ? (AK ? gm * p.lda + gk : gk * p.lda + gm) : 0;
+#pragma unroll
+      for (int pl = 0; pl < PL; ++pl) {
+        const uint32_t sa = sbase + static_cast<uint32_t>(((sA - smem) + pl * CF::A_SZ + r * CF::A_LD + c) * 8);
+        cp_async8(sa, Ab + off * PL + pl, ok ? 8 : 0);
+      }
+    }
+#pragma unroll 4
+    for (int e = tid; e < BN * KT; e += THREADS) {
+      int r, c;
+      int64_t gn, gk;
+      if constexpr (BKM) { r = e / KT; c = e % KT; gn = n0 + r; gk = k0 + c; }
+      else { r = e / BN; c = e % BN; gk = k0 + r; gn = n0 + c; }
+      const bool ok = gn < p.N && gk < kend;
+      const int64_t off = ok ? (BKM ? gn * p.ldb + gk : gk * p.ldb + gn) : 0;
+#pragma unroll
+      for (int pl = 0; pl < PL; ++pl) {
+        const uint32_t sa = sbase + static_cast<uint32_t>(((sB - smem) + pl * CF::B_SZ + r * CF::B_LD + c) * 8);
+        cp_async8(sa, Bb + off * PL + pl, ok ? 8 : 0);
+      }
+    }
+  };
+
+  const int lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm = warp / WN, wn = warp % WN;
+  double acc[MT][NT][PL][2];
+#pragma unroll
+  for (int i = 0; i < MT; ++i)
+#pragma unroll
+    for (int j = 0; j < NT; ++j)
+#pragma unroll
+      for (int q = 0; q < PL; ++q) acc[i][j][q][0] = acc[i][j][q][1] = 0.0;
+
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < ktiles) load_stage(s, s);
+    cp_async_commit();
+  }
+
+  for (int kt = 0; kt < ktiles; ++kt) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    const double* sA = smem + (kt % STAGES) * CF::STAGE;
+    const double* sB = sA + PL * CF::A_SZ;
+#pragma unroll
+    for (int ks = 0; ks < KT / 4; ++ks) {
+      const int k = ks * 4 + t;
+      double ar[MT], br[NT], ai[MT], bi[NT];
+#pragma unroll
+      for (int i = 0; i < MT; ++i) {
+        const int m = wm * MT * 8 + i * 8 + g;
+        const int idx = AK ? m * CF::A_LD + k : k * CF::A_LD + m;
+        ar[i] = sA[idx];
+        if constexpr (CPLX) ai[i] = p.signA * sA[CF::A_SZ + idx];
+      }
+#pragma unroll
+      for (int j = 0; j < NT; ++j) {
+        const int n = wn * NT * 8 + j * 8 + g;
+        const int idx = BKM ? n * CF::B_LD + k : k * CF::B_LD + n;
+        br[j] = sB[idx];
+        if constexpr (CPLX) bi[j] = p.signB * sB[CF::B_SZ + idx];
+      }
+#pragma unroll
+      for (int i = 0; i < MT; ++i)
+#pragma unroll
+        for (int j = 0; j < NT; ++j) {
+          dmma(acc[i][j][0][0], acc[i][j][0][1], ar[i], br[j]);
+          if constexpr (CPLX) {
+            dmma(acc[i][j][0][0], acc[i][j][0][1], -ai[i], bi[j]);
+            dmma(acc[i][j][1][0], acc[i][j][1][1], ar[i], bi[j]);
+            dmma(acc[i][j][1][0], acc[i][j][1][1], ai[i], br[j]);
+          }
+        }
+    }
+    const int nk = kt + STAGES - 1;
+    if (nk < ktiles) load_stage(nk % STAGES, nk);
+    cp_async_commit();
+  }
+  cp_async_wait<0>();
+
+#pragma unroll
+  for (int i = 0; i < MT; ++i)
+#pragma unroll
+    for (int j = 0; j < NT; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int64_t row = m0 + wm * MT * 8 + i * 8 + g;
+        const int64_t col = n0 + wn * NT * 8 + j * 8 + 2 * t + e;
+        if (row >= p.M || col >= p.N) continue;
+        if (p.splits > 1) {
+          double* w = p.work + ((bz * p.M + row) * p.N + col) * PL;
+#pragma unroll
+          for (int q = 0; q < PL; ++q) w[q] = acc[i][j][q][e];
+        } else {
+          int64_t rr = row, base = 0;
+          if (p.c_plane_rows > 0) { base = (row / p.c_plane_rows) * p.c_plane_stride; rr = row % p.c_plane_rows; }
+          double* c = p.C + (base + b * p.strideC + rr * p.ldc + col) * PL;
+#pragma unroll
+          for (int q = 0; q < PL; ++q) {
+            const double v = p.alpha * acc[i][j][q][e];
+            c[q] = p.beta != 0.0 ? v + p.beta * c[q] : v;
+          }
+        }
+      }
+}
+
+// Fixed-order split-K reduction: C = alpha * sum_s work[b, s] + beta * C.
+template <int PL>
+__global__ void splitk_reduce_kernel(const Params p) {
+  const int64_t total = p.batch * p.M * p.N;
+  for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < total;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t b = idx / (p.M * p.N);
+    const int64_t rc = idx % (p.M * p.N);
+    const int64_t row = rc / p.N, col = rc % p.N;
+    if (p.upper_only && row > col) continue;  // filled by the mirror pass
+    double s[PL];
+#pragma unroll
+    for (int q = 0; q < PL; ++q) s[q] = 0.0;
+    for (int sp = 0; sp < p.splits; ++sp) {
+      const double* w = p.work + (((b * p.splits + sp) * p.M + row) * p.N + col) * PL;
+#pragma unroll
+      for (int q = 0; q < PL; ++q) s[q] += w[q];
+    }
+    int64_t rr = row, base = 0;
+    if (p.c_plane_rows > 0) { base = (row / p.c_plane_rows) * p.c_plane_stride; rr = row % p.c_plane_rows; }
+    double* c = p.C + (base + b * p.strideC + rr * p.ldc + col) * PL;
+#pragma unroll
+    for (int q = 0; q < PL; ++q) {
+      const double v = p.alpha * s[q];
+      c[q] = p.beta != 0.0 ? v + p.beta * c[q] : v;
+    }
+  }
+}
+
+// Strict lower triangle from the upper one.
+template <int PL>
+__global__ void mirror_kernel(double* C, int64_t n, int64_t ldc, int64_t strideC, int64_t batch, int mode) {
+  const int64_t total = batch * n * n;
+  for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < total;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t b = idx / (n * n), rc = idx % (n * n), i = rc / n, j = rc % n;
+    if (i <= j) continue;
+    const double* src = C + (b * strideC + j * ldc + i) * PL;
+    double* dst = C + (b * strideC + i * ldc + j) * PL;
+    if (PL == 1) {
+      dst[0] = mode > 0 ? src[0] : -src[0];
+    } else {
+      dst[0] = mode > 0 ? src[0] : -src[0];
+      dst[1] = mode > 0 ? -src[1] : src[1];
+    }
+  }
+}
+
+int num_sms() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  return sms;
+}
+
+template <int MT, int NT, int WM, int WN, bool AK, bool BKM, bool CPLX>
+void launch_cfg(const Params& p, dim3 grid, cudaStream_t s) {
+  using CF = Cfg<MT, NT, WM, WN, AK, BKM, CPLX>;
+  auto kern = dgemm_kernel<MT, NT, WM, WN, AK, BKM, CPLX>;
+  static bool attr = false;
+  if (!attr) {
+    RR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, CF::SMEM_BYTES));
+    attr = true;
+  }
+  kern<<<grid, CF::THREADS, CF::SMEM_BYTES, s>>>(p);
+  RR_LAUNCH_CHECK();
+}
+
+struct Shape { int bm, bn; };
+
+template <bool AK, bool BKM>
+Shape shape_real(int64_t M) {
+  if (M <= 48) { int mt = static_cast<int>((M + 7) / 8); return {8 * mt, 128}; }
+  return {64, 64};
+}
+
+template <bool AK, bool BKM>
+void launch_real(const Params& p, dim3 grid, cudaStream_t s) {
+  if (p.M <= 48) {
+    switch ((p.M + 7) / 8) {
+      case 1: return launch_cfg<1, 4, 1, 4, AK, BKM, false>(p, grid, s);
+      case 2: return launch_cfg<2, 4, 1, 4, AK, BKM, false>(p, grid, s);
+      case 3: return launch_cfg<3, 4, 1, 4, AK, BKM, false>(p, grid, s);
+      case 4: return launch_cfg<4, 4, 1, 4, AK, BKM, false>(p, grid, s);
+      case 5: return launch_cfg<5, 4, 1, 4, AK, BKM, false>(p, grid, s);
+      default: return launch_cfg<6, 4, 1, 4, AK, BKM, false>(p, grid, s);
+    }
+  }
+  launch_cfg<4, 4, 2, 2, AK, BKM, false>(p, grid, s);
+}
+
+Shape pick_shape(const GemmDesc& d) {
+  if (d.cplx) return {32, 64};
+  if (d.M <= 48) return {static_cast<int>(8 * ((d.M + 7) / 8)), 128};
+  return {64, 64};
+}
+
+int pick_splits(const GemmDesc& d, Shape sh, int64_t* kchunk) {
+  int64_t tiles = static_cast<int64_t>(ceil_div(d.M, sh.bm)) * ceil_div(d.N, sh.bn) * d.batch;
+  if (d.mirror) tiles = (tiles + ceil_div(d.M, sh.bm) * d.batch) / 2;
+  const int64_t target = 2LL * num_sms();
+  int splits = 1;
+  if (tiles < target && d.K >= 8 * KT) {
+    splits = static_cast<int>(std::min<int64_t>((target + tiles - 1) / tiles, d.K / (4 * KT)));
+    splits = std::max(1, std::min(splits, 64));
+  }
+  int64_t kc = round_up((d.K + splits - 1) / splits, KT);
+  splits = static_cast<int>((d.K + kc - 1) / kc);
+  *kchunk = kc;
+  return std::max(1, splits);
+}
+
+}  // namespace
+
+int64_t gemm_work_doubles(const GemmDesc& d) {
+  int64_t kc;
+  const int s = pick_splits(d, pick_shape(d), &kc);
+  return s > 1 ? d.batch * s * d.M * d.N * (d.cplx ? 2 : 1) : 0;
+}
+
+void gemm(const GemmDesc& d, cudaStream_t stream, double* work, int64_t work_cap) {
+  RR_REQUIRE(d.M >= 0 && d.N >= 0 && d.K >= 0 && d.batch >= 0, RR_ERR_ARG, "gemm: negative size");
+  RR_REQUIRE(!d.mirror || d.M == d.N, RR_ERR_ARG, "gemm: mirror needs a square output");
+  RR_REQUIRE(!d.mirror || d.c_plane_rows == 0, RR_ERR_ARG, "gemm: mirror with planar output");
+  if (d.M == 0 || d.N == 0 || d.batch == 0) return;
+  const Shape sh = pick_shape(d);
+  Params p{};
+  p.M = d.M; p.N = d.N; p.K = d.K;
+  p.A = d.A; p.lda = d.lda; p.strideA = d.strideA;
+  p.B = d.B; p.ldb = d.ldb; p.strideB = d.strideB;
+  p.C = d.C; p.ldc = d.ldc; p.strideC = d.strideC;
+  p.alpha = d.alpha; p.beta = d.beta; p.batch = d.batch;
+  p.signA = d.conjA ? -1.0 : 1.0;
+  p.signB = d.conjB ? -1.0 : 1.0;
+  p.c_plane_rows = d.c_plane_rows; p.c_plane_stride = d.c_plane_stride;
+  p.upper_only = d.mirror != 0;
+  int64_t kc = d.K;
+  int splits = 1;
+  if (work && d.K > 0) {
+    splits = pick_splits(d, sh, &kc);
+    while (splits > 1 && d.batch * splits * d.M * d.N * (d.cplx ? 2 : 1) > work_cap) {
+      splits = (splits + 1) / 2;
+      kc = round_up((d.K + splits - 1) / splits, KT);
+      splits = static_cast<int>((d.K + kc - 1) / kc);
+    }
+  }
+  if (splits <= 1) { splits = 1; kc = std::max<int64_t>(d.K, 1); }
+  p.splits = splits; p.kchunk = kc; p.work = work;
+  RR_REQUIRE(d.batch * splits <= 65535, RR_ERR_ARG, "gemm: batch x splits exceeds the grid z limit");
+  dim3 grid(ceil_div(d.N, sh.bn), ceil_div(d.M, sh.bm), static_cast<unsigned>(d.batch * splits));
+  const bool AK = d.opA == Op::N, BKM = d.opB == Op::T;
+  if (d.cplx) {
+    if (AK && BKM) launch_cfg<2, 4, 2, 2, true, true, true>(p, grid, stream);
+    else if (AK) launch_cfg<2, 4, 2, 2, true, false, true>(p, grid, stream);
+    else if (BKM) launch_cfg<2, 4, 2, 2, false, true, true>(p, grid, stream);
+    else launch_cfg<2, 4, 2, 2, false, false, true>(p, grid, stream);
+  } else {
+    if (AK && BKM) launch_real<true, true>(p, grid, stream);
+    else if (AK) launch_real<true, false>(p, grid, stream);
+    else if (BKM) launch_real<false, true>(p, grid, stream);
+    else launch_real<false, false>(p, grid, stream);
+  }
+  const int blocks = std::min<int64_t>(4LL * num_sms(), std::max<int64_t>(1, (d.batch * d.M * d.N + 255) / 256));
+  if (splits > 1) {
+    if (d.cplx) splitk_reduce_kernel<2><<<blocks, 256, 0, stream>>>(p);
+    else splitk_reduce_kernel<1><<<blocks, 256, 0, stream>>>(p);
+    RR_LAUNCH_CHECK();
+  }
+  if (d.mirror) {
+    if (d.cplx) mirror_kernel<2><<<blocks, 256, 0, stream>>>(d.C, d.M, d.ldc, d.strideC, d.batch, d.mirror);
+    else mirror_kernel<1><<<blocks, 256, 0, stream>>>(d.C, d.M, d.ldc, d.strideC, d.batch, d.mirror);
+    RR_LAUNCH_CHECK();
+  }
+}
+
+}  // namespace rr

@@ -1,0 +1,47 @@
+// FP64 tensor-core GEMM family (DMMA, mma.sync m8n8k4 .f64) used by every FP64 contraction of
+// the RI path: half-transforms, the exchange SYRK, the occupied recovery products, the MO
+// transforms and the generalized-Fock contraction.  tcgen05 has no FP64 kind, so the FP64
+// tensor pipe is reached through DMMA; the BF16 split path lives in mixed_tc.cu.
+//
+// Row-major semantics throughout (the reference's Matrix<T> layout):
+//   C[b] = alpha * op(A[b]) * op(B[b]) + beta * C[b],  op(A): M x K,  op(B): K x N,
+// with op in {N, T} and optional element conjugation for complex (interleaved re,im) operands.
+#pragma once
+
+#include "rr_common.cuh"
+
+namespace rr {
+
+enum class Op : int { N = 0, T = 1 };
+
+struct GemmDesc {
+  int64_t M = 0, N = 0, K = 0;
+  const double* A = nullptr;
+  int64_t lda = 0, strideA = 0;  // in elements (complex elements when cplx)
+  const double* B = nullptr;
+  int64_t ldb = 0, strideB = 0;
+  double* C = nullptr;
+  int64_t ldc = 0, strideC = 0;
+  Op opA = Op::N, opB = Op::N;
+  double alpha = 1.0, beta = 0.0;
+  int64_t batch = 1;
+  bool cplx = false;
+  bool conjA = false, conjB = false;
+  // Output rows r >= c_plane_rows go to C + (r / c_plane_rows) * c_plane_stride, row r % c_plane_rows
+  // (0 disables).  Lets one GEMM write the stacked [re; im] half-transform into two planes.
+  int64_t c_plane_rows = 0, c_plane_stride = 0;
+  // Symmetric outputs: compute only tiles touching the upper triangle, then fill the strict
+  // lower triangle from the upper one: +1 C[i][j] = C[j][i] (Hermitian conj for cplx),
+  // -1 C[i][j] = -C[j][i].  0 = full output.  Requires M == N.
+  int mirror = 0;
+};
+
+// Launches the GEMM on `stream`.  `work` (capacity `work_cap` doubles) is split-K scratch: when
+// the output grid is too small to fill the GPU and work_cap allows, K is split, the partial
+// products go to `work` and a deterministic fixed-order reduction finishes C.  work may be null.
+void gemm(const GemmDesc& d, cudaStream_t stream, double* work = nullptr, int64_t work_cap = 0);
+
+// Doubles of scratch gemm() would like for split-K on this descriptor.
+int64_t gemm_work_doubles(const GemmDesc& d);
+
+}  // namespace rr

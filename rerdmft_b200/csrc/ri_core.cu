@@ -1,0 +1,128 @@
+// Store lifetime, streams, host<->device staging, small elementwise kernels and the FP64
+// eigensolver wrapper shared by the Fock builds.
+#include <algorithm>
+#include <complex>
+
+#include "ri_store.cuh"
+
+namespace rr {
+
+thread_local std::string g_last_error;
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+void Context::init(cudaStream_t user_stream) {
+  RR_CUDA(cudaGetDevice(&device));
+  if (user_stream) {
+    main = user_stream;
+    own_main = false;
+  } else {
+    RR_CUDA(cudaStreamCreateWithFlags(&main, cudaStreamNonBlocking));
+    own_main = true;
+  }
+  RR_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+  RR_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+  RR_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+  RR_SOLVER(cusolverDnCreate(&solver));
+}
+
+void Context::destroy() {
+  if (solver) cusolverDnDestroy(solver);
+  if (fork) cudaEventDestroy(fork);
+  if (join) cudaEventDestroy(join);
+  if (side) cudaStreamDestroy(side);
+  if (own_main && main) cudaStreamDestroy(main);
+  solver = nullptr;
+  fork = join = nullptr;
+  side = main = nullptr;
+}
+
+cudaStream_t call_stream(rr_ri_store* h, const rr_opts* o) {
+  if (o && o->stream) return static_cast<cudaStream_t>(o->stream);
+  return h->ctx.main;
+}
+
+void check_status(rr_ri_store* h, cudaStream_t s) {
+  int word = 0;
+  RR_CUDA(cudaMemcpyAsync(&word, h->status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  RR_CUDA(cudaStreamSynchronize(s));
+  if (word != 0) {
+    RR_CUDA(cudaMemsetAsync(h->status.p, 0, sizeof(int), s));
+    RR_CUDA(cudaStreamSynchronize(s));
+    throw Error(RR_ERR_TIMEOUT, "device wait bound expired (status word 0x" + std::to_string(word) + ")");
+  }
+}
+
+void copy_in(double* dst, const double* src, int64_t count, bool host, cudaStream_t s) {
+  if (count <= 0) return;
+  RR_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * count, host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
+}
+
+void copy_out(double* dst, const double* src, int64_t count, bool host, cudaStream_t s) {
+  if (count <= 0) return;
+  RR_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * count, host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s));
+}
+
+void copy_in_padded(double* dst, int64_t pitch, const double* src, int64_t n2, bool host, cudaStream_t s) {
+  copy_in(dst, src, n2, host, s);
+  if (pitch > n2) RR_CUDA(cudaMemsetAsync(dst + n2, 0, sizeof(double) * (pitch - n2), s));
+}
+
+namespace {
+
+__global__ void axpby_kernel(double* y, const double* x, double a, double b, int64_t n) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    y[i] = a * x[i] + (b != 0.0 ? b * y[i] : 0.0);
+}
+
+__global__ void fock_combine_kernel(double* F, const double* h, const double* J, const double* K, int64_t n) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    F[i] = h[i] + J[i] - K[i];
+}
+
+int blocks_for(int64_t n) { return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 1184))); }
+
+}  // namespace
+
+void axpby(double* y, const double* x, double a, double b, int64_t n, cudaStream_t s) {
+  if (n <= 0) return;
+  axpby_kernel<<<blocks_for(n), 256, 0, s>>>(y, x, a, b, n);
+  RR_LAUNCH_CHECK();
+}
+
+void fock_combine(double* F, const double* h, const double* J, const double* K, int64_t n2, cudaStream_t s) {
+  if (n2 <= 0) return;
+  fock_combine_kernel<<<blocks_for(n2), 256, 0, s>>>(F, h, J, K, n2);
+  RR_LAUNCH_CHECK();
+}
+
+void eigh_sym(rr_ri_store* h, double* a, int64_t n, double* w, cudaStream_t s) {
+  if (n == 0) return;
+  auto& c = h->ctx;
+  RR_SOLVER(cusolverDnSetStream(c.solver, s));
+  int lwork = 0;
+  RR_SOLVER(cusolverDnDsyevd_bufferSize(c.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, static_cast<int>(n),
+                                        a, static_cast<int>(n), w, &lwork));
+  c.solver_work.ensure(static_cast<size_t>(lwork) + 1);
+  c.solver_info.ensure(1);
+  RR_SOLVER(cusolverDnDsyevd(c.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, static_cast<int>(n), a,
+                             static_cast<int>(n), w, c.solver_work.p, lwork, c.solver_info.p));
+}
+
+void eigh_herm(rr_ri_store* h, double* a, int64_t n, double* w, cudaStream_t s) {
+  if (n == 0) return;
+  auto& c = h->ctx;
+  RR_SOLVER(cusolverDnSetStream(c.solver, s));
+  int lwork = 0;
+  auto* az = reinterpret_cast<cuDoubleComplex*>(a);
+  RR_SOLVER(cusolverDnZheevd_bufferSize(c.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, static_cast<int>(n),
+                                        az, static_cast<int>(n), w, &lwork));
+  c.solver_work.ensure(2 * static_cast<size_t>(lwork) + 2);
+  c.solver_info.ensure(1);
+  RR_SOLVER(cusolverDnZheevd(c.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, static_cast<int>(n), az,
+                             static_cast<int>(n), w, reinterpret_cast<cuDoubleComplex*>(c.solver_work.p), lwork,
+                             c.solver_info.p));
+}
+
+}  // namespace rr

@@ -1,0 +1,70 @@
+// The resident RI store behind an rr_ri_handle, and the helpers every entry point shares.
+#pragma once
+
+#include "gemm_f64.cuh"
+#include "j_stream.cuh"
+#include "rr_common.cuh"
+
+struct rr_ri_store {
+  rr::Context ctx;
+  int64_t naux = 0, n = 0, ns = 0;  // n = nl for the 4c store
+  int ntens = 1;
+  rr::DevBuf<double> B[2];  // resident tensors, row pitch `pitch` doubles (256-byte aligned rows)
+  int64_t pitch[2] = {0, 0};
+  rr::DevBuf<int> status;   // device status word written by bounded waits
+  // Scratch, grown on demand and reused across calls.
+  rr::DevBuf<double> mats;  // per-call matrices (inputs, outputs, intermediates)
+  rr::DevBuf<double> T;     // half-transformed exchange intermediate
+  rr::DevBuf<double> work;  // split-K partial products
+  rr::DevBuf<double> jscr;  // J pass-1/pass-2 partial sums
+  rr::DevBuf<double> solver_a;  // eigen-problem matrix / eigenvectors
+  rr::DevBuf<double> solver_w;  // eigenvalues
+  std::vector<double> host_w;
+  // Split-BF16 copies of B for RR_PREC_MIXED (built on first use).
+  rr::DevBuf<uint16_t> Bhi[2], Blo[2];
+  int64_t mixed_pitch[2] = {0, 0};
+  bool mixed_ready = false;
+};
+
+namespace rr {
+
+// Bump allocator over a DevBuf<double>: carve(n) returns 256-byte-aligned sub-buffers.
+struct Arena {
+  DevBuf<double>* buf;
+  int64_t used = 0;
+  std::vector<std::pair<double**, int64_t>> pending;
+  explicit Arena(DevBuf<double>* b) : buf(b) {}
+  // Two-phase: request() records sizes, commit() grows the buffer once and fills pointers.
+  void request(double** p, int64_t count) {
+    pending.emplace_back(p, count);
+    used += round_up(std::max<int64_t>(count, 1), 32);
+  }
+  void commit() {
+    buf->ensure(static_cast<size_t>(used));
+    int64_t off = 0;
+    for (auto& pr : pending) {
+      *pr.first = buf->p + off;
+      off += round_up(std::max<int64_t>(pr.second, 1), 32);
+    }
+    pending.clear();
+  }
+};
+
+cudaStream_t call_stream(rr_ri_store* h, const rr_opts* o);
+void check_status(rr_ri_store* h, cudaStream_t s);  // syncs s, throws RR_ERR_TIMEOUT on a set word
+void copy_in(double* dst, const double* src, int64_t count, bool host, cudaStream_t s);
+void copy_out(double* dst, const double* src, int64_t count, bool host, cudaStream_t s);
+// Pitched copy of a flat n2-vector into a zero-padded buffer of `pitch` doubles.
+void copy_in_padded(double* dst, int64_t pitch, const double* src, int64_t n2, bool host, cudaStream_t s);
+
+// Elementwise helpers (device).
+void axpby(double* y, const double* x, double a, double b, int64_t n, cudaStream_t s);  // y = a x + b y
+// F = h + J - K (real, n2 entries).
+void fock_combine(double* F, const double* h, const double* J, const double* K, int64_t n2, cudaStream_t s);
+// Symmetric eigensolver (cuSOLVER dsyevd) in place on a (n x n) row-major symmetric matrix:
+// on return row j of `a` holds eigenvector j; w ascending.
+void eigh_sym(rr_ri_store* h, double* a, int64_t n, double* w, cudaStream_t s);
+// Hermitian (interleaved complex) version, cuSOLVER zheevd; row j of `a` holds conj(eigenvector j).
+void eigh_herm(rr_ri_store* h, double* a, int64_t n, double* w, cudaStream_t s);
+
+}  // namespace rr

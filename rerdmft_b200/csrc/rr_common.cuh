@@ -1,0 +1,97 @@
+// Shared runtime pieces of librr_ri: status codes, error capture, device buffers and the
+// per-handle execution context (streams, events, cuSOLVER handle, scratch arena).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "rr_ri.h"
+
+namespace rr {
+
+// Error carried across the C ABI: every entry point catches rr::Error and returns its code.
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& msg) : std::runtime_error(msg), code(c) {}
+};
+
+void set_last_error(const std::string& msg);
+
+#define RR_CUDA(expr)                                                                          \
+  do {                                                                                         \
+    cudaError_t _e = (expr);                                                                   \
+    if (_e != cudaSuccess)                                                                     \
+      throw ::rr::Error(RR_ERR_CUDA, std::string(#expr " failed: ") + cudaGetErrorString(_e)); \
+  } while (0)
+
+#define RR_SOLVER(expr)                                                                          \
+  do {                                                                                           \
+    cusolverStatus_t _s = (expr);                                                                \
+    if (_s != CUSOLVER_STATUS_SUCCESS)                                                           \
+      throw ::rr::Error(RR_ERR_SOLVER, std::string(#expr " failed, status ") + std::to_string(_s)); \
+  } while (0)
+
+#define RR_REQUIRE(cond, code, msg)                \
+  do {                                             \
+    if (!(cond)) throw ::rr::Error((code), (msg)); \
+  } while (0)
+
+// Kernel launch check (configuration errors surface here; execution errors at the next sync).
+#define RR_LAUNCH_CHECK() RR_CUDA(cudaGetLastError())
+
+// Owning device allocation (cudaMalloc/cudaFree), move-only.
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  explicit DevBuf(size_t count) { alloc(count); }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+    return *this;
+  }
+  ~DevBuf() { release(); }
+  void alloc(size_t count) {
+    release();
+    if (count) RR_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    n = count;
+  }
+  // Grow-only: keeps the allocation when it is already large enough.
+  void ensure(size_t count) { if (count > n) alloc(count); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+// Execution context owned by a handle: a main stream (the caller's, or a private one), a side
+// stream for the bandwidth-bound J pass that overlaps the exchange GEMMs, and fork/join events.
+struct Context {
+  int device = 0;
+  cudaStream_t main = nullptr;
+  cudaStream_t side = nullptr;
+  bool own_main = false;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  cusolverDnHandle_t solver = nullptr;
+  DevBuf<double> solver_work;
+  DevBuf<int> solver_info;
+  void init(cudaStream_t user_stream);
+  void destroy();
+  void set_stream(cudaStream_t s);
+};
+
+inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+inline int ceil_div(int64_t a, int64_t b) { return static_cast<int>((a + b - 1) / b); }
+
+}  // namespace rr

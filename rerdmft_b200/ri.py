@@ -1,0 +1,150 @@
+"""Host-side mirror of the reference's RI interface, backed by librr_ri (CUDA, sm_100a).
+
+Names, argument meaning and error behaviour follow the reference's C++ overloads:
+
+* ``RiNonRelEriSource`` / ``nonRelFockMatrix``   src/NON_REL/NonRelFockMatrixRi.h:30-40
+* ``RiX2cEriSource`` / ``x2cFockMatrix``         src/X2C_DHF/X2C_FockMatrixRi.h:29-40
+* ``RiDirectEriSource`` / ``rkbFockMatrix`` / ``riFockTwoElectronDirect``
+                                                 src/UKB/UkbFockMatrixRi.h:70-98
+
+The source objects hold the 3-center tensor; here it is uploaded once (lazily, on the first
+call) into a resident ``RiStore`` and only the small per-iteration matrices cross to the GPU.
+Arguments may be numpy arrays (host; results come back as numpy) or CUDA torch tensors
+(device; results stay on the device).  Dimension mismatches raise ``RrError`` (a
+``RuntimeError``) with the reference's message, where the reference throws
+``std::runtime_error``.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import RrError
+
+try:  # torch is only plumbing for device buffers; host (numpy) calls do not need it
+    import torch
+except Exception:  # pragma: no cover
+    torch = None
+
+
+def _is_dev(a) -> bool:
+    return torch is not None and isinstance(a, torch.Tensor) and a.is_cuda
+
+
+def _host(a, dtype) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def _dev(a, dtype):
+    t = a.contiguous()
+    want = torch.float64 if dtype == np.float64 else torch.complex128
+    if t.dtype != want:
+        t = t.to(want)
+    return t
+
+
+def _ptr(a) -> int:
+    if _is_dev(a):
+        return a.data_ptr()
+    return a.ctypes.data
+
+
+class RiStore:
+    """A resident RI tensor on the current CUDA device (rr_ri_create / rr_ri_create_4c)."""
+
+    def __init__(self, B, B_SS=None, nl=None, ns=None):
+        self.handle = ctypes.c_void_p()
+        lib = L.lib()
+        dev = _is_dev(B)
+        conv = _dev if dev else _host
+        B = conv(B, np.float64)
+        naux = B.shape[0]
+        if B_SS is None:
+            n = int(round(np.sqrt(B.shape[1]))) if nl is None else nl
+            if n * n != B.shape[1]:
+                raise RrError(L.RR_ERR_ARG, "RiStore: eri3 column count is not a square")
+            L.check(lib.rr_ri_create(_ptr(B), naux, n, L.RR_MEM_DEVICE if dev else L.RR_MEM_HOST,
+                                     ctypes.byref(self.handle)))
+            self.n, self.ns = n, 0
+        else:
+            B_SS = conv(B_SS, np.float64)
+            if B_SS.shape[0] != naux:
+                raise RrError(L.RR_ERR_ARG,
+                              "riFockTwoElectronDirect: eri3_LL and eri3_SS do not share the same aux dimension")
+            L.check(lib.rr_ri_create_4c(_ptr(B), _ptr(B_SS), naux, nl, ns,
+                                        L.RR_MEM_DEVICE if dev else L.RR_MEM_HOST, ctypes.byref(self.handle)))
+            self.n, self.ns = nl, ns
+        self.naux = naux
+
+    def close(self):
+        if self.handle and self.handle.value:
+            L.lib().rr_ri_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sync(self):
+        L.check(L.lib().rr_ri_sync(self.handle))
+
+
+class RiNonRelEriSource:
+    """src/NON_REL/NonRelFockMatrixRi.h:30: nl, eri3_L (n_aux, nl*nl), x_large, overlap."""
+
+    def __init__(self, nl, eri3_L, x_large, overlap):
+        self.nl = int(nl)
+        self.eri3_L = eri3_L
+        self.x_large = x_large
+        self.overlap = overlap
+        self._store = None
+
+    @property
+    def store(self) -> RiStore:
+        if self._store is None:
+            if self.eri3_L.shape[1] != self.nl * self.nl:
+                raise RrError(L.RR_ERR_ARG, "nonRelFockMatrix (RI): eri3_L column count does not match nl^2")
+            self._store = RiStore(self.eri3_L, nl=self.nl)
+        return self._store
+
+
+def nonRelFockMatrix(h_core, eri: RiNonRelEriSource, density_matrix, stream: int | None = None):
+    """F = h + J - K/2 (src/NON_REL/NonRelFockMatrixRi.cpp:71), computed by rr_ri_fock_nonrel."""
+    nl = eri.nl
+    if tuple(density_matrix.shape) != (nl, nl):
+        raise RrError(L.RR_ERR_ARG, "nonRelFockMatrix (RI): density_matrix dimension does not match nl")
+    if eri.eri3_L.shape[1] != nl * nl:
+        raise RrError(L.RR_ERR_ARG, "nonRelFockMatrix (RI): eri3_L column count does not match nl^2")
+    store = eri.store
+    dev = _is_dev(density_matrix)
+    conv = _dev if dev else _host
+    h = conv(h_core, np.float64)
+    D = conv(density_matrix, np.float64)
+    S = conv(eri.overlap, np.float64)
+    X = conv(eri.x_large, np.float64)
+    if tuple(h.shape) != (nl, nl) or tuple(S.shape) != (nl, nl) or X.shape[0] != nl:
+        raise RrError(L.RR_ERR_ARG, "nonRelFockMatrix (RI): h_core/overlap/x_large dimensions do not match nl")
+    F = torch.empty((nl, nl), dtype=torch.float64, device=D.device) if dev else np.empty((nl, nl))
+    o = L.opts(L.RR_MEM_DEVICE if dev else L.RR_MEM_HOST, stream=stream)
+    L.check(L.lib().rr_ri_fock_nonrel(store.handle, _ptr(h), _ptr(D), _ptr(S), _ptr(X), X.shape[1], _ptr(F),
+                                      ctypes.byref(o)))
+    return F
+
+
+def jk_occupied(store: RiStore, C_occ, stream: int | None = None):
+    """(J, K') for D = 2 C C^T, with F = h + J - K' (rr_ri_jk_occupied)."""
+    dev = _is_dev(C_occ)
+    conv = _dev if dev else _host
+    C = conv(C_occ, np.float64)
+    n = store.n
+    if C.shape[0] != n:
+        raise RrError(L.RR_ERR_ARG, "jk_occupied: C_occ row count does not match n")
+    mk = (lambda: torch.empty((n, n), dtype=torch.float64, device=C.device)) if dev else (lambda: np.empty((n, n)))
+    J, K = mk(), mk()
+    o = L.opts(L.RR_MEM_DEVICE if dev else L.RR_MEM_HOST, stream=stream)
+    L.check(L.lib().rr_ri_jk_occupied(store.handle, _ptr(C), C.shape[1], _ptr(J), _ptr(K), ctypes.byref(o)))
+    return J, K

@@ -1,0 +1,108 @@
+"""Unit tests of the kernel families on the GPU: the FP64 DMMA GEMM (every layout, complex,
+split-K, mirror) and the TMA J streaming passes, against numpy fp64."""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+from rerdmft_b200 import _lib as L  # noqa: E402
+
+
+def _dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _np(t):
+    return t.cpu().numpy()
+
+
+def _op(a, transposed, conj):
+    r = a.T if transposed else a
+    return np.conj(r) if conj else r
+
+
+def _run(M, N, K, opA, opB, batch=1, cplx=False, conjA=False, conjB=False, alpha=1.3, beta=0.0, mirror=0,
+         split=True, seed=0):
+    rng = np.random.default_rng(seed)
+    dt = np.complex128 if cplx else np.float64
+
+    def rnd(*s):
+        x = rng.standard_normal(s)
+        return (x + 1j * rng.standard_normal(s)) if cplx else x
+
+    a_shape = (K, M) if opA else (M, K)
+    b_shape = (N, K) if opB else (K, N)
+    A = rnd(batch, *a_shape).astype(dt)
+    B = rnd(batch, *b_shape).astype(dt)
+    C0 = rnd(batch, M, N).astype(dt)
+    ref = np.stack([alpha * _op(A[i], opA, conjA) @ _op(B[i], opB, conjB) + beta * C0[i] for i in range(batch)])
+    if mirror:
+        for i in range(batch):
+            up = np.triu(ref[i])
+            low = (up.conj().T if mirror > 0 else -up.conj().T) if cplx else (up.T if mirror > 0 else -up.T)
+            ref[i] = up + np.tril(low, -1)
+    dA, dB, dC = _dev(A.view(np.float64)), _dev(B.view(np.float64)), _dev(C0.view(np.float64))
+    lda = a_shape[1]
+    ldb = b_shape[1]
+    L.check(L.lib().rr_test_gemm_f64(M, N, K, dA.data_ptr(), lda, a_shape[0] * a_shape[1], int(opA), dB.data_ptr(), ldb,
+                                     b_shape[0] * b_shape[1], int(opB), dC.data_ptr(), N, M * N, alpha, beta, batch,
+                                     int(cplx), int(conjA), int(conjB), mirror, int(split)))
+    out = _np(dC).view(dt).reshape(batch, M, N)
+    return out, ref
+
+
+@pytest.mark.parametrize("opA", [0, 1])
+@pytest.mark.parametrize("opB", [0, 1])
+@pytest.mark.parametrize("shape", [(1, 1, 1), (7, 13, 5), (40, 400, 400), (64, 64, 64), (65, 33, 129), (3, 250, 17),
+                                   (100, 100, 3000)])
+def test_gemm_real_layouts(opA, opB, shape):
+    M, N, K = shape
+    out, ref = _run(M, N, K, opA, opB, beta=0.7)
+    assert np.abs(out - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max()) * np.sqrt(K)
+
+
+@pytest.mark.parametrize("opA,opB,conjA,conjB", [(0, 0, 0, 0), (1, 0, 1, 0), (0, 1, 0, 1), (1, 1, 1, 1), (0, 1, 1, 0)])
+@pytest.mark.parametrize("shape", [(5, 9, 7), (33, 70, 65), (80, 80, 200)])
+def test_gemm_complex(opA, opB, conjA, conjB, shape):
+    M, N, K = shape
+    out, ref = _run(M, N, K, opA, opB, cplx=True, conjA=bool(conjA), conjB=bool(conjB), beta=0.5)
+    assert np.abs(out - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max()) * np.sqrt(K)
+
+
+@pytest.mark.parametrize("batch", [1, 3, 37])
+def test_gemm_batched_small_m(batch):
+    for M in (1, 8, 13, 40, 47):
+        out, ref = _run(M, 96, 80, 0, 0, batch=batch, seed=M)
+        assert np.abs(out - ref).max() <= 1e-12 * np.abs(ref).max() * 10
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+@pytest.mark.parametrize("mirror", [1, -1])
+def test_gemm_mirror_split(cplx, mirror):
+    # A^T A style product, symmetric part kept by the mirror
+    out, ref = _run(130, 130, 5000, 1, 0, cplx=cplx, mirror=mirror, split=True)
+    assert np.abs(out - ref).max() <= 1e-11 * np.abs(ref).max()
+
+
+def test_gemm_split_is_deterministic():
+    a, _ = _run(96, 96, 20000, 1, 0, split=True, seed=5)
+    b, _ = _run(96, 96, 20000, 1, 0, split=True, seed=5)
+    assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("naux,n2", [(1, 1), (3, 49), (37, 169), (129, 576), (200, 4099), (64, 20000)])
+def test_j_passes(naux, n2):
+    rng = np.random.default_rng(naux + n2)
+    B = rng.standard_normal((naux, n2))
+    D = rng.standard_normal(n2)
+    dB, dD = _dev(B), _dev(D)
+    g = torch.empty(naux, dtype=torch.float64, device="cuda")
+    J = torch.empty(n2, dtype=torch.float64, device="cuda")
+    L.check(L.lib().rr_test_j_passes(dB.data_ptr(), naux, n2, dD.data_ptr(), g.data_ptr(), J.data_ptr()))
+    gref = B @ D
+    Jref = B.T @ gref
+    assert np.abs(_np(g) - gref).max() <= 1e-12 * np.sqrt(n2) * np.abs(gref).max()
+    assert np.abs(_np(J) - Jref).max() <= 1e-12 * np.sqrt(naux * n2) * np.abs(Jref).max()

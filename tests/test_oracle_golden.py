@@ -1,0 +1,124 @@
+"""Pins the numpy restatement (oracle/ri_oracle.py) to golden outputs of the reference itself."""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, golden
+from oracle import ri_oracle as o
+
+TOL = 1e-12
+
+
+@pytest.mark.parametrize("name", sorted(p.stem for p in GOLDEN.glob("nonrel_fock_*.npz")))
+def test_nonrel_fock(name):
+    g = golden(name)
+    F = o.nonrel_fock(g["h"], g["B"], g["D"], g["S"], g["X"])
+    assert np.abs(F - g["F"]).max() < TOL
+    if "D_mix" in g:
+        assert np.abs(o.nonrel_fock(g["h"], g["B"], g["D_mix"], g["S"], g["X"]) - g["F_mix"]).max() < TOL
+
+
+@pytest.mark.parametrize("name", sorted(p.stem for p in GOLDEN.glob("x2c_fock_*.npz")))
+def test_x2c_fock(name):
+    g = golden(name)
+    F = o.x2c_fock(g["h"], g["B"], g["P"], g["S"], g["X"])
+    assert np.abs(F - g["F"]).max() < TOL
+
+
+@pytest.mark.parametrize("name", sorted(p.stem for p in GOLDEN.glob("rkb_fock_*.npz")))
+def test_rkb_and_ukb(name):
+    g = golden(name)
+    nl, ns = g["B_LL"].shape[1] ** 0.5, g["B_SS"].shape[1] ** 0.5
+    nl, ns = int(round(nl)), int(round(ns))
+    F = o.rkb_fock(g["h"], nl, ns, g["B_LL"], g["B_SS"], g["v_total"], g["s_full"], g["x_full"], g["P"])
+    assert np.abs(F - g["F"]).max() < 1e-11
+    G = o.ukb_two_electron(nl, ns, g["B_LL"], g["B_SS"], g["P_ukb"], g["C_occ"], g["occ"])
+    assert np.abs(G - g["G"]).max() < TOL
+
+
+def test_nonrel_mo():
+    g = golden("nonrel_mo")
+    n = g["C"].shape[0]
+    assert np.abs(o.nonrel_mo_build(g["B"], g["C"]) - g["Bmo"]).max() < TOL
+    assert np.abs(o.nonrel_mo_rotated(g["Bmo"], n, g["U"]) - g["Brot"]).max() < TOL
+    assert np.abs(o.nonrel_mo_embedded(g["Bmo"], n) - g["emb"]).max() == 0.0
+    assert np.abs(o.nonrel_mo_eri(g["Bmo"], n, g["quads"]) - g["eri"]).max() < TOL
+    bad = g["U"].copy()
+    bad[0, n] = 0.01
+    with pytest.raises(ValueError):
+        o.nonrel_mo_rotated(g["Bmo"], n, bad)
+
+
+def test_ri_mo():
+    g = golden("ri_mo")
+    nl, ns = int(round(g["B_LL"].shape[1] ** 0.5)), int(round(g["B_SS"].shape[1] ** 0.5))
+    nt = g["c_ukb"].shape[1]
+    assert np.abs(o.ri_mo_build(nl, ns, g["B_LL"], g["B_SS"], g["c_ukb"]) - g["Bmo"]).max() < TOL
+    assert np.abs(o.ri_mo_rotated(g["Bmo"], nt, g["U"]) - g["Brot"]).max() < TOL
+    assert np.abs(o.ri_mo_positive(g["Bmo"], nt, 4) - g["Bpos"]).max() == 0.0
+    assert np.abs(o.ri_mo_eri(g["Bmo"], nt, g["quads"]) - g["eri"]).max() < TOL
+
+
+def test_jkl_matches_element_access():
+    g = golden("ri_mo")
+    nt = g["c_ukb"].shape[1]
+    po = np.arange(nt) ^ 1
+    J, K, Lm = o.jkl_matrices(g["Bmo"], nt, po)
+    for i in range(nt):
+        for j in range(nt):
+            q = np.array([[i, j, i, j], [i, j, j, i], [po[i], j, j, po[i]]])
+            e = o.ri_mo_eri(g["Bmo"], nt, q)
+            assert abs(J[i, j] - e[0]) < TOL and abs(K[i, j] - e[1]) < TOL and abs(Lm[i, j] - e[2]) < TOL
+
+
+def test_hx_fock():
+    g = golden("hx_fock")
+    Fc = o.hx_fock(g["hc"], g["Bc"], g["occ"], g["h2"], g["x2"], g["po"], g["l1"], g["l2"])
+    assert np.abs(Fc - g["Fc"]).max() < TOL
+    assert np.abs(o.hx_fock(g["hc"], g["Bc"], g["occ"], g["h2"], g["x2"]) - g["Fc0"]).max() < TOL
+    nsp = int(round(g["Bmo"].shape[1] ** 0.5))
+    emb = o.nonrel_mo_embedded(g["Bmo"], nsp)
+    Fr = o.hx_fock(g["hr"], emb, g["occr"], g["h2r"], g["x2r"], g["por"], g["l1r"], g["l2r"])
+    assert np.abs(Fr - g["Fr"]).max() < TOL
+
+
+def test_diis():
+    g = golden("diis")
+    d = o.Diis(5)
+    for t in range(g["E"].shape[0]):
+        r = d.extrapolate(g["E"][t], g["V"][t])
+        assert np.abs(r - g["out"][t]).max() < 1e-11
+        assert len(d.last_weights) == g["wc"][t]
+    d = o.Diis(4)
+    for t in range(g["Ec"].shape[0]):
+        r = d.extrapolate(g["Ec"][t], g["Vc"][t])
+        assert np.abs(r - g["outc"][t]).max() < 1e-11
+        assert len(d.last_weights) == g["wcc"][t]
+    assert np.abs(o.commutator_error(g["Fm"], g["Pm"], g["Sm"]) - g["comm"]).max() < TOL
+
+
+def test_scf_loops():
+    g = golden("scf_nonrel")
+    sysd = dict(B=g["B"], h=g["h"], S=g["S"], X=g["X"], D0=g["D0"], n_electrons=int(g["n_electrons"]))
+    r = o.nonrel_scf(sysd)
+    assert r["iterations"] == int(g["iterations"])
+    assert np.abs(r["history"] - g["history"]).max() < 1e-10
+    g = golden("scf_x2c")
+    sysd = dict(B=g["B"], h=g["h"], S=g["S"], X=g["X"], P0=g["P0"], n_electrons=int(g["n_electrons"]))
+    r = o.x2c_scf(sysd)
+    assert r["iterations"] == int(g["iterations"])
+    assert np.abs(r["history"] - g["history"]).max() < 1e-10
+    g = golden("scf_dhf")
+    sysd = {k: g[k] for k in ("B_LL", "B_SS", "v_total", "s_full", "x_full", "h", "P0")}
+    sysd.update(nl=int(g["nl"]), ns=int(g["ns"]), n_electrons=int(g["n_electrons"]))
+    r = o.dhf_scf(sysd)
+    assert r["iterations"] == int(g["iterations"])
+    assert np.abs(r["history"] - g["history"]).max() < 1e-10
+
+
+def test_orthogonalisation():
+    g = golden("orth")
+    X = o.canonical_orthogonalize(g["S"], 1e-6)
+    assert X.shape == g["X"].shape
+    assert np.abs(X @ X.T - g["X"] @ g["X"].T).max() < 1e-9
+    Xh = o.canonical_orthogonalize_hermitian(g["s_full"], 1e-10)
+    assert np.abs(Xh @ Xh.conj().T - g["XXh"]).max() < 1e-10
