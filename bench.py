@@ -1,0 +1,338 @@
+"""RI J+K Fock-build throughput on one B200 (and N replicas under torchrun).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the synthetic nonrelativistic RI J/K kernel configuration): n = 400 AOs, naux = 1600,
+nocc = 40; AO and aux centres uniform in a 20-bohr cube, B^P_mn = c_Pmn exp(-0.3(|r_m-r_P|^2 +
+|r_n-r_P|^2)) with c symmetric N(0,1); D = 2 C_occ C_occ^T with C_occ a QR-orthonormalised
+Gaussian 400 x 40; S = X = I.  One step = one full FP64 RI Fock build F = h + J - K/2 through
+rr_ri_fock_nonrel (occupied recovery, J, K, assembly) -- the reference's nonRelFockMatrix.
+B is 2.05 GB, far larger than the 126 MB L2, so no flush is needed between steps.
+
+Multi-GPU: the path is replicas only (each rank builds its own Fock matrices on its own
+copy of B; no collective), value = total builds/s over all ranks, timed as the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_AO, N_AUX, N_OCC, SEED = 400, 1600, 40, 2024
+METRIC = "RI J+K Fock builds/s"
+UNIT = "builds/s"
+
+
+def make_inputs():
+    from rerdmft_b200 import synth
+
+    rng = np.random.default_rng(SEED + 1)
+    B = synth.ri_tensor(N_AO, N_AUX, SEED, box=20.0, alpha=0.3)
+    C, D = synth.occupied_density(N_AO, N_OCC, rng)
+    a = rng.standard_normal((N_AO, N_AO))
+    h = 0.5 * (a + a.T)
+    return dict(B=B, C=C, D=D, h=h, S=np.eye(N_AO), X=np.eye(N_AO))
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def fp64_gemm_peak(torch) -> float:
+    """Measured FP64 tensor-core peak on this GPU: cuBLAS DGEMM 8192^3 (TFLOP/s, best of 5)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("hbm_gbs", 6650.0), "MEASURED_PEAKS.json"
+    return 6650.0, "fallback"
+
+
+def cpu_reference_rate(inp, seconds: float = 15.0):
+    """The reference's own nonRelFockMatrix (oracle/_ref, compiled from its sources) on the same
+    inputs, all host cores (OMP threads, serial BLAS inside, as the reference expects)."""
+    from oracle import ref
+
+    if not ref.available():
+        return None
+    cores = os.cpu_count() or 1
+    ref.set_threads(cores)
+    t0 = time.perf_counter()
+    ref.nonrel_fock(inp["h"], inp["B"], inp["D"], inp["S"], inp["X"])
+    first = time.perf_counter() - t0
+    reps = max(1, min(20, int(seconds / max(first, 1e-3))))
+    best = first
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        ref.nonrel_fock(inp["h"], inp["B"], inp["D"], inp["S"], inp["X"])
+        best = min(best, time.perf_counter() - t0)
+    return dict(value=1.0 / best, unit=UNIT, cores=cores, kind="reference",
+                sample=f"full workload (n={N_AO}, naux={N_AUX}, nocc={N_OCC}), best of {reps + 1} calls of the "
+                       f"reference nonRelFockMatrix compiled from its sources, OMP_NUM_THREADS={cores}")
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    base = dict(metric=METRIC, unit=UNIT, n_gpus=args.gpus, steps=args.steps, warmup=args.warmup,
+                higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64", data="synthetic",
+                impl="reference",
+                config={"workload": f"nonrel RI J+K Fock build n={N_AO} naux={N_AUX} nocc={N_OCC}",
+                        "precision": "fp64", "l2": "inputs larger than L2"})
+    if rank != 0:
+        return
+    from oracle import ref
+
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/librrref.so not built"}))
+        return
+    inp = make_inputs()
+    cores = os.cpu_count() or 1
+    ref.set_threads(cores)
+    for _ in range(max(0, min(args.warmup, 1))):
+        ref.nonrel_fock(inp["h"], inp["B"], inp["D"], inp["S"], inp["X"])
+    steps = max(1, min(args.steps, 5))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        ref.nonrel_fock(inp["h"], inp["B"], inp["D"], inp["S"], inp["X"])
+    dt = time.perf_counter() - t0
+    v = steps / dt
+    base.update(value=v, ms_per_step=1e3 * dt / steps,
+                cpu_baseline=dict(value=v, unit=UNIT, cores=cores, kind="reference",
+                                  sample=f"{steps} full-size calls (warm-up {min(args.warmup, 1)}) of the reference "
+                                         f"nonRelFockMatrix compiled from its sources, OMP_NUM_THREADS={cores}"),
+                e2e=dict(value=v, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    print(json.dumps(base))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+
+    from rerdmft_b200 import _lib as L
+    from rerdmft_b200 import ri
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    inp = make_inputs()
+    dev = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in inp.items() if k != "C"}
+    src = ri.RiNonRelEriSource(N_AO, dev["B"], dev["X"], dev["S"])
+    store = src.store
+    lib = L.lib()
+    F = torch.empty((N_AO, N_AO), dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    o = L.opts(L.RR_MEM_DEVICE, stream=stream, sync=0)
+    import ctypes
+
+    def step():
+        L.check(lib.rr_ri_fock_nonrel(store.handle, dev["h"].data_ptr(), dev["D"].data_ptr(), dev["S"].data_ptr(),
+                                      dev["X"].data_ptr(), N_AO, F.data_ptr(), ctypes.byref(o)))
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    l0 = lib.rr_kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    launches = lib.rr_kernel_launches() - l0
+    t = e0.elapsed_time(e1) / 1e3
+    if pg:
+        tt = torch.tensor([t], dtype=torch.float64, device="cuda")
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        t = float(tt.item())
+    clk = clocks.stop()
+    store.sync()
+    value = ws * args.steps / t
+
+    # Phase times from profiled calls (events inside the library, same stream).
+    L.check(lib.rr_ri_set_profiling(store.handle, 1))
+    acc = {}
+    nprof = 5
+    for _ in range(nprof):
+        step()
+        tm = L.Timings()
+        L.check(lib.rr_ri_get_timings(store.handle, ctypes.byref(tm)))
+        for k, v in tm.as_dict().items():
+            acc[k] = acc.get(k, 0.0) + v / nprof
+    L.check(lib.rr_ri_set_profiling(store.handle, 0))
+
+    # End to end through the public API with host buffers (pinned): h, D, S, X in, F out.
+    hp = {k: torch.from_numpy(np.ascontiguousarray(inp[k])).pin_memory() for k in ("h", "D", "S", "X")}
+    Fh = torch.empty((N_AO, N_AO), dtype=torch.float64).pin_memory()
+    oh = L.opts(L.RR_MEM_HOST, stream=stream, sync=1)
+
+    def step_host():
+        L.check(lib.rr_ri_fock_nonrel(store.handle, hp["h"].data_ptr(), hp["D"].data_ptr(), hp["S"].data_ptr(),
+                                      hp["X"].data_ptr(), N_AO, Fh.data_ptr(), ctypes.byref(oh)))
+
+    for _ in range(3):
+        step_host()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        step_host()
+    e1.record()
+    torch.cuda.synchronize()
+    te = e0.elapsed_time(e1) / 1e3
+    if pg:
+        tt = torch.tensor([te], dtype=torch.float64, device="cuda")
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        te = float(tt.item())
+    e2e = dict(value=ws * args.steps / te, unit=UNIT, h2d_bytes_per_step=4 * N_AO * N_AO * 8,
+               d2h_bytes_per_step=N_AO * N_AO * 8)
+
+    # Roofline of the dominant kernel group.
+    hbm_peak, hbm_src = measured_peaks()
+    fp64_peak = fp64_gemm_peak(torch) if rank == 0 else None
+    ht_flops = 2.0 * N_AUX * N_OCC * N_AO * N_AO
+    syrk_flops = 2.0 * N_AUX * N_OCC * N_AO * N_AO
+    j_bytes = 2.0 * N_AUX * N_AO * N_AO * 8
+    phases = {k: round(v, 4) for k, v in acc.items()}
+    ht_tf = ht_flops / (acc["half_transform_ms"] / 1e3) / 1e12 if acc.get("half_transform_ms") else None
+    ex_tf = syrk_flops / (acc["exchange_ms"] / 1e3) / 1e12 if acc.get("exchange_ms") else None
+    j_gbs = j_bytes / (acc["coulomb_ms"] / 1e3) / 1e9 if acc.get("coulomb_ms") else None
+    k_ms = acc.get("half_transform_ms", 0.0) + acc.get("exchange_ms", 0.0)
+    k_tf = (ht_flops + syrk_flops) / (k_ms / 1e3) / 1e12 if k_ms else None
+
+    if rank != 0:
+        if pg:
+            pg.destroy_process_group()
+        return
+    cpu = None if args.no_cpu_baseline else cpu_reference_rate(inp)
+    line = dict(
+        metric=METRIC, value=value, unit=UNIT, n_gpus=ws, steps=args.steps, warmup=args.warmup,
+        ms_per_step=1e3 * t / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
+        data="synthetic",
+        config={"workload": f"nonrel RI J+K Fock build n={N_AO} naux={N_AUX} nocc={N_OCC} (FP64, occupied recovery "
+                            f"included)", "parallelism": f"replicas x{ws}", "precision": "fp64",
+                "l2": "inputs larger than L2 (B = 2.05 GB)"},
+        roofline={"bound": "tensor", "kernel": "exchange (FP64 DMMA half-transform + SYRK)",
+                  "achieved": k_tf, "peak": fp64_peak, "unit": "TFLOP/s",
+                  "frac": (k_tf / fp64_peak) if (k_tf and fp64_peak) else None, "traffic": None,
+                  "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 has no entry in MEASURED_PEAKS.json)",
+                  "algorithmic": "4*naux*nocc*n^2 flops per build (half-transform + full-count SYRK)"},
+        coulomb={"bound": "hbm", "achieved": j_gbs, "peak": hbm_peak, "unit": "GB/s",
+                 "frac": (j_gbs / hbm_peak) if j_gbs else None, "peak_source": hbm_src,
+                 "algorithmic": "2*naux*n^2*8 bytes per build"},
+        kernels={"half_transform_tflops": ht_tf, "syrk_tflops_full_count": ex_tf},
+        phases_ms=phases, clocks=clk, e2e=e2e, gpu_launches=int(launches), cpu_baseline=cpu,
+    )
+    print(json.dumps(line))
+    if pg:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

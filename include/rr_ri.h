@@ -45,6 +45,17 @@ extern "C" {
 
 typedef struct rr_ri_store* rr_ri_handle;
 
+/* Per-phase device times of the last profiled call (CUDA events on the streams that ran them). */
+typedef struct rr_timings {
+  double total_ms;          /* first to last event of the call, main stream */
+  double recovery_ms;       /* occupied-orbital recovery: GEMMs + eigensolver (+ host readback) */
+  double half_transform_ms; /* T[P] = C_occ^T B^P (batched FP64 DMMA, or split-BF16 tcgen05) */
+  double exchange_ms;       /* K = sum_P T[P]^T T[P] (SYRK + split-K reduction) */
+  double coulomb_ms;        /* J passes on the side stream (overlaps the exchange) */
+  double epilogue_ms;       /* F assembly and output copies */
+  double reserved[4];
+} rr_timings;
+
 typedef struct rr_opts {
   int32_t mem;       /* RR_MEM_HOST (default) or RR_MEM_DEVICE for every matrix argument of the call */
   int32_t precision; /* RR_PREC_FP64 (default) or RR_PREC_MIXED */
@@ -89,6 +100,15 @@ int rr_ri_fock_nonrel(rr_ri_handle h, const double* h_core, const double* D, con
  * K' = sum_P (C^T B^P)^T (C^T B^P) (so F = h + J - K'), C is n x n_occ.  The building block of
  * the device-resident SCF loop; equal to rr_ri_fock_nonrel when D = 2 C C^T. */
 int rr_ri_jk_occupied(rr_ri_handle h, const double* C_occ, int64_t n_occ, double* J, double* K, const rr_opts* opts);
+
+/* Profiling: when on, each call records CUDA events around its phases; rr_ri_get_timings waits
+ * for the last call's events and returns the phase times.  Off by default (no event overhead). */
+int rr_ri_set_profiling(rr_ri_handle h, int32_t on);
+int rr_ri_get_timings(rr_ri_handle h, rr_timings* out);
+
+/* Number of librr_ri kernel launches issued by this process so far (library kernels such as the
+ * cuSOLVER eigensolver are not counted). */
+int64_t rr_kernel_launches(void);
 
 #ifdef __cplusplus
 }

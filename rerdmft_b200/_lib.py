@@ -32,6 +32,14 @@ class Opts(ctypes.Structure):
     _fields_ = [("mem", _i32), ("precision", _i32), ("stream", _vp), ("sync", _i32), ("reserved", _i32)]
 
 
+class Timings(ctypes.Structure):
+    _fields_ = [("total_ms", _d), ("recovery_ms", _d), ("half_transform_ms", _d), ("exchange_ms", _d),
+                ("coulomb_ms", _d), ("epilogue_ms", _d), ("reserved", _d * 4)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
 class ScfOpts(ctypes.Structure):
     _fields_ = [("diis_size", _i32), ("max_iterations", _i32), ("energy_tolerance", _d),
                 ("density_tolerance", _d), ("kramers_restricted", _i32), ("precision", _i32),
@@ -53,6 +61,9 @@ _SIGS = {
     "rr_ri_sync": (ctypes.c_int, [_vp]),
     "rr_ri_fock_nonrel": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _i64, _vp, ctypes.POINTER(Opts)]),
     "rr_ri_jk_occupied": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp, ctypes.POINTER(Opts)]),
+    "rr_ri_set_profiling": (ctypes.c_int, [_vp, _i32]),
+    "rr_ri_get_timings": (ctypes.c_int, [_vp, ctypes.c_void_p]),
+    "rr_kernel_launches": (ctypes.c_int64, []),
     "rr_test_gemm_f64": (ctypes.c_int, [_i64, _i64, _i64, _vp, _i64, _i64, _i32, _vp, _i64, _i64, _i32, _vp, _i64,
                                         _i64, _d, _d, _i64, _i32, _i32, _i32, _i32, _i32]),
     "rr_test_j_passes": (ctypes.c_int, [_vp, _i64, _i64, _vp, _vp, _vp]),

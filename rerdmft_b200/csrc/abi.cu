@@ -116,6 +116,8 @@ int rr_ri_destroy(rr_ri_handle h) {
     if (!h) return;
     cudaSetDevice(h->ctx.device);
     cudaDeviceSynchronize();
+    for (auto& e : h->ev)
+      if (e) cudaEventDestroy(e);
     h->ctx.destroy();
     delete h;
   });
@@ -157,6 +159,39 @@ int rr_ri_jk_occupied(rr_ri_handle h, const double* C_occ, int64_t n_occ, double
     rr::jk_occupied(s, C_occ, n_occ, J, K, opts);
   });
 }
+
+int rr_ri_set_profiling(rr_ri_handle h, int32_t on) {
+  return api([&] {
+    auto* s = checked(h);
+    s->profiling = on != 0;
+    for (bool& u : s->ev_used) u = false;
+  });
+}
+
+int rr_ri_get_timings(rr_ri_handle h, rr_timings* out) {
+  return api([&] {
+    auto* s = checked(h);
+    RR_REQUIRE(out != nullptr, RR_ERR_ARG, "rr_ri_get_timings: out is null");
+    *out = rr_timings{};
+    RR_REQUIRE(s->ev_used[0] && s->ev_used[4], RR_ERR_STATE, "rr_ri_get_timings: no profiled call recorded");
+    RR_CUDA(cudaEventSynchronize(s->ev[4]));
+    auto el = [&](int a, int b) -> double {
+      if (!s->ev_used[a] || !s->ev_used[b]) return 0.0;
+      float ms = 0.f;
+      RR_CUDA(cudaEventSynchronize(s->ev[b]));
+      RR_CUDA(cudaEventElapsedTime(&ms, s->ev[a], s->ev[b]));
+      return static_cast<double>(ms);
+    };
+    out->total_ms = el(0, 4);
+    out->recovery_ms = el(0, 1);
+    out->half_transform_ms = el(1, 2);
+    out->exchange_ms = s->ev_used[2] ? el(2, 3) : el(1, 3);
+    out->coulomb_ms = el(5, 6);
+    out->epilogue_ms = el(3, 4);
+  });
+}
+
+int64_t rr_kernel_launches(void) { return rr::launches(); }
 
 }  // extern "C"
 

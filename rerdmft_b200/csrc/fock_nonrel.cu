@@ -45,6 +45,7 @@ void exchange_nonrel(rr_ri_store* h, const double* Ct, int64_t ldct, bool ct_tra
   ht.C = h->T.p; ht.ldc = n; ht.strideC = nocc * n;
   ht.batch = naux;
   gemm(ht, s);
+  prof_mark(h, 2, s);
 
   GemmDesc sk;
   sk.M = n; sk.N = n; sk.K = naux * nocc;
@@ -72,9 +73,11 @@ void coulomb_async(rr_ri_store* h, const double* Dp, double* J, double scale, cu
   auto& c = h->ctx;
   RR_CUDA(cudaEventRecord(c.fork, s));
   RR_CUDA(cudaStreamWaitEvent(c.side, c.fork, 0));
+  prof_mark(h, 5, c.side);
   j_pass1(pl, gpart, h->status.p, c.side);
   j_pass2(pl, gpart, jpart, h->status.p, c.side);
   j_finish(pl, jpart, scale, c.side);
+  prof_mark(h, 6, c.side);
   RR_CUDA(cudaEventRecord(c.join, c.side));
 }
 
@@ -109,6 +112,7 @@ void fock_nonrel(rr_ri_store* h, const double* hc, const double* D, const double
   ar.commit();
   if (!host) { hd = const_cast<double*>(hc); Sd = const_cast<double*>(S); Xd = const_cast<double*>(X); Fd = F; }
 
+  prof_mark(h, 0, s);
   copy_in_padded(Dp, pitch, D, n2, host, s);
   if (host) {
     copy_in(hd, hc, n2, true, s);
@@ -151,10 +155,13 @@ void fock_nonrel(rr_ri_store* h, const double* hc, const double* D, const double
     ct.C = Ct; ct.ldc = n;
     gemm(ct, s);
   }
+  prof_mark(h, 1, s);
   exchange_nonrel(h, Ct, n, false, nocc, K, s);
+  prof_mark(h, 3, s);
   coulomb_join(h, s);
   fock_combine(Fd, hd, J, K, n2, s);
   if (host) copy_out(F, Fd, n2, true, s);
+  prof_mark(h, 4, s);
   if (host || (o && o->sync)) check_status(h, s);
 }
 
@@ -174,6 +181,7 @@ void jk_occupied(rr_ri_store* h, const double* C, int64_t nocc, double* Jout, do
     ar.request(&K, n2);
   }
   ar.commit();
+  prof_mark(h, 0, s);
   if (host) copy_in(Cd, C, n * nocc, true, s);
   else { Cd = const_cast<double*>(C); J = Jout; K = Kout; }
   RR_CUDA(cudaMemsetAsync(Dp + n2, 0, sizeof(double) * (pitch - n2), s));
@@ -183,12 +191,15 @@ void jk_occupied(rr_ri_store* h, const double* C, int64_t nocc, double* Jout, do
     RR_CUDA(cudaMemsetAsync(Dp, 0, sizeof(double) * n2, s));
   }
   coulomb_async(h, Dp, J, 1.0, s);
+  prof_mark(h, 1, s);
   exchange_nonrel(h, Cd, nocc, true, nocc, K, s);
+  prof_mark(h, 3, s);
   coulomb_join(h, s);
   if (host) {
     copy_out(Jout, J, n2, true, s);
     copy_out(Kout, K, n2, true, s);
   }
+  prof_mark(h, 4, s);
   if (host || (o && o->sync)) check_status(h, s);
 }
 

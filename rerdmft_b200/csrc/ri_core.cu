@@ -1,6 +1,7 @@
 // Store lifetime, streams, host<->device staging, small elementwise kernels and the FP64
 // eigensolver wrapper shared by the Fock builds.
 #include <algorithm>
+#include <atomic>
 #include <complex>
 
 #include "ri_store.cuh"
@@ -9,6 +10,10 @@ namespace rr {
 
 thread_local std::string g_last_error;
 void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+static std::atomic<int64_t> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+int64_t launches() { return g_launches.load(std::memory_order_relaxed); }
 
 void Context::init(cudaStream_t user_stream) {
   RR_CUDA(cudaGetDevice(&device));
@@ -39,6 +44,13 @@ void Context::destroy() {
 cudaStream_t call_stream(rr_ri_store* h, const rr_opts* o) {
   if (o && o->stream) return static_cast<cudaStream_t>(o->stream);
   return h->ctx.main;
+}
+
+void prof_mark(rr_ri_store* h, int i, cudaStream_t s) {
+  if (!h->profiling) return;
+  if (!h->ev[i]) RR_CUDA(cudaEventCreate(&h->ev[i]));
+  RR_CUDA(cudaEventRecord(h->ev[i], s));
+  h->ev_used[i] = true;
 }
 
 void check_status(rr_ri_store* h, cudaStream_t s) {

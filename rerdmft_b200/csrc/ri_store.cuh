@@ -24,6 +24,11 @@ struct rr_ri_store {
   rr::DevBuf<uint16_t> Bhi[2], Blo[2];
   int64_t mixed_pitch[2] = {0, 0};
   bool mixed_ready = false;
+  // Profiling events: 0 start, 1 recovery done, 2 half-transform done, 3 exchange done, 4 end
+  // (main stream); 5 J start, 6 J end (side stream).
+  bool profiling = false;
+  cudaEvent_t ev[8] = {};
+  bool ev_used[8] = {};
 };
 
 namespace rr {
@@ -51,6 +56,9 @@ struct Arena {
 };
 
 cudaStream_t call_stream(rr_ri_store* h, const rr_opts* o);
+// Records profiling event i on stream s when profiling is on.
+void prof_mark(rr_ri_store* h, int i, cudaStream_t s);
+int64_t launches();
 void check_status(rr_ri_store* h, cudaStream_t s);  // syncs s, throws RR_ERR_TIMEOUT on a set word
 void copy_in(double* dst, const double* src, int64_t count, bool host, cudaStream_t s);
 void copy_out(double* dst, const double* src, int64_t count, bool host, cudaStream_t s);

@@ -43,8 +43,14 @@ void set_last_error(const std::string& msg);
     if (!(cond)) throw ::rr::Error((code), (msg)); \
   } while (0)
 
-// Kernel launch check (configuration errors surface here; execution errors at the next sync).
-#define RR_LAUNCH_CHECK() RR_CUDA(cudaGetLastError())
+// Kernel launch check (configuration errors surface here; execution errors at the next sync);
+// also counts the launch for rr_kernel_launches().
+void count_launch();
+#define RR_LAUNCH_CHECK()             \
+  do {                                \
+    RR_CUDA(cudaGetLastError());      \
+    ::rr::count_launch();             \
+  } while (0)
 
 // Owning device allocation (cudaMalloc/cudaFree), move-only.
 template <typename T>
