@@ -96,6 +96,26 @@ int rr_ri_sync(rr_ri_handle h);
 int rr_ri_fock_nonrel(rr_ri_handle h, const double* h_core, const double* D, const double* S, const double* X,
                       int64_t n_eff, double* F, const rr_opts* opts);
 
+/* X2C RI Fock matrix in the [alpha; beta] spin-orbital AO basis (2nl x 2nl, complex).
+ * Replaces x2cFockMatrix(h_x2c, RiX2cEriSource, P), src/X2C_DHF/X2C_FockMatrixRi.cpp:79: J from
+ * Re(P_aa + P_bb) on both diagonal blocks, K over the two spin flavours from the occupied spinors
+ * recovered from X^dagger (S P S) X (eigenvalues > 0.5, sqrt(eigenvalue)-weighted).  X: 2nl x n_eff. */
+int rr_ri_fock_x2c(rr_ri_handle h, const double* h_x2c, const double* P, const double* S, const double* X,
+                   int64_t n_eff, double* F, const rr_opts* opts);
+
+/* Two-electron part in the UKB basis [L-alpha, L-beta, S-alpha, S-beta] (n_ukb = 2nl + 2ns,
+ * complex) from P_ukb (J) and the caller's occupied coefficients C_occ (n_ukb x n_occ, complex) and
+ * occupations (K).  Replaces riFockTwoElectronDirect, src/UKB/UkbFockMatrixRi.cpp:35. */
+int rr_ri_two_electron_ukb(rr_ri_handle h, const double* P_ukb, const double* C_occ, int64_t n_occ,
+                           const double* occupations, double* G, const rr_opts* opts);
+
+/* 4-component RKB Fock matrix F = h + v^dagger G(v P v^dagger, v C_occ) v (n_rkb x n_rkb, complex).
+ * Replaces rkbFockMatrix(h_rkb, RiDirectEriSource, P), src/UKB/UkbFockMatrixRi.cpp:185: the occupied
+ * RKB spinors are recovered from x_full^dagger (s_full P s_full) x_full (eigenvalues > 0.5).
+ * v_total: n_ukb x n_rkb; s_full: n_rkb x n_rkb; x_full: n_rkb x n_eff. */
+int rr_ri_fock_rkb(rr_ri_handle h, const double* h_rkb, const double* v_total, int64_t n_rkb, const double* s_full,
+                   const double* x_full, int64_t n_eff, const double* P, double* F, const rr_opts* opts);
+
 /* Coulomb and exchange from given occupied coefficients: J(D = 2 C C^T) and
  * K' = sum_P (C^T B^P)^T (C^T B^P) (so F = h + J - K'), C is n x n_occ.  The building block of
  * the device-resident SCF loop; equal to rr_ri_fock_nonrel when D = 2 C C^T. */

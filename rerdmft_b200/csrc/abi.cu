@@ -9,6 +9,11 @@ extern thread_local std::string g_last_error;
 void fock_nonrel(rr_ri_store*, const double*, const double*, const double*, const double*, int64_t, double*,
                  const rr_opts*);
 void jk_occupied(rr_ri_store*, const double*, int64_t, double*, double*, const rr_opts*);
+void fock_x2c(rr_ri_store*, const double*, const double*, const double*, const double*, int64_t, double*,
+              const rr_opts*);
+void ukb_two_electron(rr_ri_store*, const double*, const double*, int64_t, const double*, double*, const rr_opts*);
+void fock_rkb(rr_ri_store*, const double*, const double*, int64_t, const double*, const double*, int64_t,
+              const double*, double*, const rr_opts*);
 }  // namespace rr
 
 namespace {
@@ -157,6 +162,36 @@ int rr_ri_jk_occupied(rr_ri_handle h, const double* C_occ, int64_t n_occ, double
     RR_REQUIRE((C_occ || n_occ == 0) && J && K, RR_ERR_ARG, "rr_ri_jk_occupied: null matrix");
     RR_REQUIRE(!opts || opts->precision == RR_PREC_FP64, RR_ERR_UNSUPPORTED, "rr_ri_jk_occupied: precision");
     rr::jk_occupied(s, C_occ, n_occ, J, K, opts);
+  });
+}
+
+int rr_ri_fock_x2c(rr_ri_handle h, const double* h_x2c, const double* P, const double* S, const double* X,
+                   int64_t n_eff, double* F, const rr_opts* opts) {
+  return api([&] {
+    auto* s = checked(h);
+    RR_REQUIRE(h_x2c && P && S && F && (X || n_eff == 0), RR_ERR_ARG, "rr_ri_fock_x2c: null matrix");
+    RR_REQUIRE(!opts || opts->precision == RR_PREC_FP64, RR_ERR_UNSUPPORTED, "rr_ri_fock_x2c: precision");
+    rr::fock_x2c(s, h_x2c, P, S, X, n_eff, F, opts);
+  });
+}
+
+int rr_ri_two_electron_ukb(rr_ri_handle h, const double* P_ukb, const double* C_occ, int64_t n_occ,
+                           const double* occupations, double* G, const rr_opts* opts) {
+  return api([&] {
+    auto* s = checked(h);
+    RR_REQUIRE(P_ukb && G && ((C_occ && occupations) || n_occ == 0), RR_ERR_ARG, "rr_ri_two_electron_ukb: null matrix");
+    RR_REQUIRE(!opts || opts->precision == RR_PREC_FP64, RR_ERR_UNSUPPORTED, "rr_ri_two_electron_ukb: precision");
+    rr::ukb_two_electron(s, P_ukb, C_occ, n_occ, occupations, G, opts);
+  });
+}
+
+int rr_ri_fock_rkb(rr_ri_handle h, const double* h_rkb, const double* v_total, int64_t n_rkb, const double* s_full,
+                   const double* x_full, int64_t n_eff, const double* P, double* F, const rr_opts* opts) {
+  return api([&] {
+    auto* s = checked(h);
+    RR_REQUIRE(h_rkb && v_total && s_full && P && F && (x_full || n_eff == 0), RR_ERR_ARG, "rr_ri_fock_rkb: null matrix");
+    RR_REQUIRE(!opts || opts->precision == RR_PREC_FP64, RR_ERR_UNSUPPORTED, "rr_ri_fock_rkb: precision");
+    rr::fock_rkb(s, h_rkb, v_total, n_rkb, s_full, x_full, n_eff, P, F, opts);
   });
 }
 

@@ -67,7 +67,7 @@ void coulomb_async(rr_ri_store* h, const double* Dp, double* J, double scale, cu
   t.D = Dp;
   t.J = J;
   JPlan pl = j_plan(1, &t, h->naux);
-  h->jscr.ensure(static_cast<size_t>(pl.gpart_doubles + pl.jpart_doubles + 32));
+  h->jscr.ensure(static_cast<size_t>(round_up(pl.gpart_doubles, 32) + pl.jpart_doubles + 32));
   double* gpart = h->jscr.p;
   double* jpart = h->jscr.p + round_up(pl.gpart_doubles, 32);
   auto& c = h->ctx;
@@ -81,7 +81,36 @@ void coulomb_async(rr_ri_store* h, const double* Dp, double* J, double scale, cu
   RR_CUDA(cudaEventRecord(c.join, c.side));
 }
 
+// Same for one or two tensors sharing gamma (4c: LL and SS); Dp[t] pitched, J[t] dense outputs.
+void coulomb_async_multi(rr_ri_store* h, int ntens, const double* const* Dp, double* const* J, cudaStream_t s) {
+  JTensor t[2];
+  const int64_t nn[2] = {h->n, h->ns};
+  for (int i = 0; i < ntens; ++i) {
+    t[i].B = h->B[i].p;
+    t[i].pitch = h->pitch[i];
+    t[i].len = nn[i] * nn[i];
+    t[i].D = Dp[i];
+    t[i].J = J[i];
+  }
+  JPlan pl = j_plan(ntens, t, h->naux);
+  h->jscr.ensure(static_cast<size_t>(round_up(pl.gpart_doubles, 32) + pl.jpart_doubles + 32));
+  double* gpart = h->jscr.p;
+  double* jpart = h->jscr.p + round_up(pl.gpart_doubles, 32);
+  auto& c = h->ctx;
+  RR_CUDA(cudaEventRecord(c.fork, s));
+  RR_CUDA(cudaStreamWaitEvent(c.side, c.fork, 0));
+  prof_mark(h, 5, c.side);
+  j_pass1(pl, gpart, h->status.p, c.side);
+  j_pass2(pl, gpart, jpart, h->status.p, c.side);
+  j_finish(pl, jpart, 1.0, c.side);
+  prof_mark(h, 6, c.side);
+  RR_CUDA(cudaEventRecord(c.join, c.side));
+}
+
 void coulomb_join(rr_ri_store* h, cudaStream_t s) { RR_CUDA(cudaStreamWaitEvent(s, h->ctx.join, 0)); }
+
+int64_t occupied_ct(rr_ri_store* h, const double* X, const double* S, const double* Dp, int64_t n, int64_t n_eff,
+                    double scale, bool cplx, bool weighted, double* Ct, cudaStream_t s);
 
 void fock_nonrel(rr_ri_store* h, const double* hc, const double* D, const double* S, const double* X, int64_t n_eff,
                  double* F, const rr_opts* o) {
@@ -92,17 +121,12 @@ void fock_nonrel(rr_ri_store* h, const double* hc, const double* D, const double
   cudaStream_t s = call_stream(h, o);
   const int64_t pitch = round_up(std::max<int64_t>(n2, 2), 32);
 
-  double *Dp, *hd, *Sd, *Xd, *Fd, *J, *K, *SD, *SDS, *Y, *Pe, *W, *Ct;
+  double *Dp, *hd, *Sd, *Xd, *Fd, *J, *K, *Ct;
   Arena ar(&h->mats);
   ar.request(&Dp, pitch);
   ar.request(&J, n2);
   ar.request(&K, n2);
-  ar.request(&SD, n2);
-  ar.request(&SDS, n2);
-  ar.request(&Y, n * n_eff);
-  ar.request(&Pe, n_eff * n_eff);
-  ar.request(&W, n_eff);
-  ar.request(&Ct, n * n_eff);
+  ar.request(&Ct, n * std::max<int64_t>(n_eff, 1));
   if (host) {
     ar.request(&hd, n2);
     ar.request(&Sd, n2);
@@ -120,41 +144,8 @@ void fock_nonrel(rr_ri_store* h, const double* hc, const double* D, const double
     copy_in(Xd, X, n * n_eff, true, s);
   }
   coulomb_async(h, Dp, J, 1.0, s);
-
-  // Occupied recovery: P_eff = X^T (S D S / 2) X, keep eigenvalues > 0.5.
-  GemmDesc g;
-  g.M = n; g.N = n; g.K = n;
-  g.A = Sd; g.lda = n; g.B = Dp; g.ldb = n; g.C = SD; g.ldc = n;
-  gemm(g, s);
-  g.A = SD; g.B = Sd; g.C = SDS;
-  gemm(g, s);
-  g.N = n_eff; g.A = SDS; g.B = Xd; g.ldb = n_eff; g.C = Y; g.ldc = n_eff;
-  gemm(g, s);
-  GemmDesc pe;
-  pe.M = n_eff; pe.N = n_eff; pe.K = n;
-  pe.A = Xd; pe.lda = n_eff; pe.opA = Op::T;
-  pe.B = Y; pe.ldb = n_eff; pe.C = Pe; pe.ldc = n_eff; pe.alpha = 0.5;
-  gemm(pe, s);
-  eigh_sym(h, Pe, n_eff, W, s);
-  h->host_w.resize(static_cast<size_t>(std::max<int64_t>(n_eff, 1)));
-  if (n_eff) RR_CUDA(cudaMemcpyAsync(h->host_w.data(), W, sizeof(double) * n_eff, cudaMemcpyDeviceToHost, s));
-  RR_CUDA(cudaStreamSynchronize(s));
-  int info = 0;
-  if (n_eff) {
-    RR_CUDA(cudaMemcpy(&info, h->ctx.solver_info.p, sizeof(int), cudaMemcpyDeviceToHost));
-    RR_REQUIRE(info == 0, RR_ERR_SOLVER, "rr_ri_fock_nonrel: dsyevd failed to converge");
-  }
-  int64_t nocc = 0;
-  for (int64_t i = 0; i < n_eff; ++i) nocc += h->host_w[static_cast<size_t>(i)] > 0.5 ? 1 : 0;
-  // Eigenvalues ascend, so the kept eigenvectors are the last nocc rows of Pe (row j = vector j).
-  if (nocc) {
-    GemmDesc ct;
-    ct.M = nocc; ct.N = n; ct.K = n_eff;
-    ct.A = Pe + (n_eff - nocc) * n_eff; ct.lda = n_eff;
-    ct.B = Xd; ct.ldb = n_eff; ct.opB = Op::T;
-    ct.C = Ct; ct.ldc = n;
-    gemm(ct, s);
-  }
+  // Occupied recovery (X^T (S D S / 2) X, eigenvalues > 0.5) as c_t = F^T X^T.
+  const int64_t nocc = occupied_ct(h, Xd, Sd, Dp, n, n_eff, 0.5, false, false, Ct, s);
   prof_mark(h, 1, s);
   exchange_nonrel(h, Ct, n, false, nocc, K, s);
   prof_mark(h, 3, s);

@@ -1,0 +1,362 @@
+// Relativistic RI Fock builds: X2C (2 spin blocks) and the 4-component UKB/RKB build (4 blocks).
+//
+// References: src/X2C_DHF/X2C_FockMatrixRi.cpp:79-205 (x2cFockMatrix),
+// src/UKB/UkbFockMatrixRi.cpp:35-183 (riFockTwoElectronDirect), :185-216 (rkbFockMatrix).
+//
+// The 3-center tensors are real and the coefficients complex.  As in the reference, the complex
+// half-transform is carried out as real GEMMs on split real/imaginary rows; the exchange blocks
+// K_fu = V_f^dagger V_u (V_f = tmp_f over all P, flattened to (naux*r) x fs_f) then map onto
+// real FP64 DMMA GEMMs:  Re K = [Re V_f; Im V_f]^T [Re V_u; Im V_u]  (one GEMM: the two planes are
+// stored back to back) and  Im K = Re V_f^T Im V_u - Im V_f^T Re V_u  (two GEMMs).  Diagonal
+// blocks f = u compute only upper tiles (Re symmetric, Im antisymmetric) and mirror.
+#include <algorithm>
+#include <array>
+
+#include "ri_store.cuh"
+
+namespace rr {
+
+int64_t occupied_ct(rr_ri_store* h, const double* X, const double* S, const double* Dp, int64_t n, int64_t n_eff,
+                    double scale, bool cplx, bool weighted, double* Ct, cudaStream_t s);
+void prof_mark(rr_ri_store* h, int i, cudaStream_t s);
+
+namespace {
+
+int blocks_for(int64_t n) { return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 1184))); }
+
+// Real part of the spin-summed density of two same-size flavour blocks into a pitched buffer:
+// out[a*fs + b] = Re(P(o0+a, o0+b) + P(o1+a, o1+b)), P complex n x n.
+__global__ void spin_sum_kernel(double* out, const double* P, int64_t n, int64_t o0, int64_t o1, int64_t fs) {
+  for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < fs * fs;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t a = idx / fs, b = idx % fs;
+    out[idx] = P[((o0 + a) * n + o0 + b) * 2] + P[((o1 + a) * n + o1 + b) * 2];
+  }
+}
+
+// Planar split of one flavour's columns of Ct (r x ntot complex): out (2r x fs) real,
+// rows [0, r) real parts, rows [r, 2r) imaginary parts.
+__global__ void split_rows_kernel(double* out, const double* Ct, int64_t r, int64_t ntot, int64_t off, int64_t fs) {
+  for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < 2 * r * fs;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t i = idx / fs, a = idx % fs;
+    const int64_t ii = i < r ? i : i - r;
+    out[idx] = Ct[(ii * ntot + off + a) * 2 + (i < r ? 0 : 1)];
+  }
+}
+
+// G (complex ntot x ntot) block (f,u): G(of+a, ou+b) = -(Kre + i Kim)(a,b), and for f != u also
+// G(ou+b, of+a) = -conj(K(a,b)).  diag_j (real fs x fs) is added on a diagonal block.
+__global__ void place_block_kernel(double* G, int64_t ntot, int64_t of, int64_t ou, int64_t fsf, int64_t fsu,
+                                   const double* Kre, const double* Kim, const double* diag_j, int both) {
+  for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < fsf * fsu;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t a = idx / fsu, b = idx % fsu;
+    const double re = -Kre[idx], im = -Kim[idx];
+    double* g = G + ((of + a) * ntot + ou + b) * 2;
+    g[0] = re + (diag_j ? diag_j[idx] : 0.0);
+    g[1] = im;
+    if (both) {
+      double* gt = G + ((ou + b) * ntot + of + a) * 2;
+      gt[0] = re;
+      gt[1] = -im;
+    }
+  }
+}
+
+// Ct (r x ntot complex) = diag(sqrt(occ)) C^dagger for C (ntot x r complex).
+__global__ void ct_from_occupied_kernel(double* Ct, const double* C, const double* occ, int64_t ntot, int64_t r) {
+  for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < r * ntot;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t i = idx / ntot, a = idx % ntot;
+    const double w = sqrt(occ[i]);
+    Ct[idx * 2] = w * C[(a * r + i) * 2];
+    Ct[idx * 2 + 1] = -w * C[(a * r + i) * 2 + 1];
+  }
+}
+
+// out = h + G  (complex, interleaved; count complex entries)
+__global__ void add_kernel(double* out, const double* h, const double* G, int64_t count2) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < count2;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    out[i] = h[i] + G[i];
+}
+
+struct Flavours {
+  int nf = 0;
+  std::array<int64_t, 4> off{}, fs{};
+  std::array<int, 4> tens{};
+};
+
+}  // namespace
+
+void coulomb_async_multi(rr_ri_store* h, int ntens, const double* const* Dp, double* const* J, cudaStream_t s);
+
+// Two-electron matrix G (complex ntot x ntot) = J - K for the given flavours from Ct (r x ntot,
+// complex), the reference's c_t of all flavours side by side.  Pdens: pitched real spin-summed
+// densities per tensor (J input).  Writes G.
+void two_electron_rel(rr_ri_store* h, const Flavours& fl, int64_t ntot, const double* Ct, int64_t r,
+                      const double* const* Dp, double* G, cudaStream_t s) {
+  const int64_t naux = h->naux;
+  const int ntens = h->ntens;
+  std::array<int64_t, 2> nt = {h->n, h->ns};
+  // J (side stream) into per-tensor J buffers
+  double *J[2] = {nullptr, nullptr}, *Cs[4], *Kre, *Kim;
+  int64_t fsmax = 0;
+  for (int f = 0; f < fl.nf; ++f) fsmax = std::max(fsmax, fl.fs[f]);
+  Arena ar(&h->mats);
+  for (int t = 0; t < ntens; ++t) ar.request(&J[t], nt[t] * nt[t]);
+  for (int f = 0; f < fl.nf; ++f) ar.request(&Cs[f], 2 * std::max<int64_t>(r, 1) * fl.fs[f]);
+  ar.request(&Kre, fsmax * fsmax);
+  ar.request(&Kim, fsmax * fsmax);
+  ar.commit();
+  coulomb_async_multi(h, ntens, Dp, J, s);
+  RR_CUDA(cudaMemsetAsync(G, 0, sizeof(double) * 2 * ntot * ntot, s));
+  // T planes: flavour f occupies [Re (naux*r*fs) | Im (naux*r*fs)]
+  std::array<double*, 4> T{};
+  int64_t tsize = 0;
+  for (int f = 0; f < fl.nf; ++f) tsize += 2 * naux * r * fl.fs[f];
+  if (r > 0 && naux > 0) {
+    h->T.ensure(static_cast<size_t>(tsize));
+    int64_t o = 0;
+    for (int f = 0; f < fl.nf; ++f) { T[f] = h->T.p + o; o += 2 * naux * r * fl.fs[f]; }
+    for (int f = 0; f < fl.nf; ++f) {
+      split_rows_kernel<<<blocks_for(2 * r * fl.fs[f]), 256, 0, s>>>(Cs[f], Ct, r, ntot, fl.off[f], fl.fs[f]);
+      RR_LAUNCH_CHECK();
+      const int t = fl.tens[f];
+      GemmDesc ht;
+      ht.M = 2 * r; ht.N = fl.fs[f]; ht.K = fl.fs[f];
+      ht.A = Cs[f]; ht.lda = fl.fs[f];
+      ht.B = h->B[t].p; ht.ldb = fl.fs[f]; ht.strideB = h->pitch[t];
+      ht.C = T[f]; ht.ldc = fl.fs[f]; ht.strideC = r * fl.fs[f];
+      ht.c_plane_rows = r; ht.c_plane_stride = naux * r * fl.fs[f];
+      ht.batch = naux;
+      gemm(ht, s);
+    }
+  }
+  prof_mark(h, 2, s);
+  for (int f = 0; f < fl.nf; ++f)
+    for (int u = f; u < fl.nf; ++u) {
+      const int64_t ff = fl.fs[f], fu = fl.fs[u];
+      if (r > 0 && naux > 0) {
+        const int64_t kk = naux * r;
+        GemmDesc g;
+        g.M = ff; g.N = fu;
+        g.opA = Op::T; g.lda = ff; g.ldb = fu; g.ldc = fu;
+        // Re K = [Re; Im]_f^T [Re; Im]_u
+        g.K = 2 * kk; g.A = T[f]; g.B = T[u]; g.C = Kre; g.mirror = f == u ? 1 : 0;
+        int64_t want = gemm_work_doubles(g);
+        h->work.ensure(static_cast<size_t>(std::max<int64_t>(want, 1)));
+        gemm(g, s, h->work.p, static_cast<int64_t>(h->work.n));
+        // Im K = Re_f^T Im_u - Im_f^T Re_u
+        g.K = kk; g.A = T[f]; g.B = T[u] + kk * fu; g.C = Kim; g.alpha = 1.0; g.beta = 0.0;
+        g.mirror = f == u ? -1 : 0;
+        gemm(g, s, h->work.p, static_cast<int64_t>(h->work.n));
+        g.A = T[f] + kk * ff; g.B = T[u]; g.alpha = -1.0; g.beta = 1.0;
+        gemm(g, s, h->work.p, static_cast<int64_t>(h->work.n));
+      } else {
+        RR_CUDA(cudaMemsetAsync(Kre, 0, sizeof(double) * ff * fu, s));
+        RR_CUDA(cudaMemsetAsync(Kim, 0, sizeof(double) * ff * fu, s));
+      }
+      if (f == u) RR_CUDA(cudaStreamWaitEvent(s, h->ctx.join, 0));  // J needed on the diagonal blocks
+      place_block_kernel<<<blocks_for(ff * fu), 256, 0, s>>>(G, ntot, fl.off[f], fl.off[u], ff, fu, Kre, Kim,
+                                                              f == u ? J[fl.tens[f]] : nullptr, f != u);
+      RR_LAUNCH_CHECK();
+    }
+  prof_mark(h, 3, s);
+}
+
+void fock_x2c(rr_ri_store* h, const double* hc, const double* P, const double* S, const double* X, int64_t n_eff,
+              double* F, const rr_opts* o) {
+  RR_REQUIRE(h->ntens == 1, RR_ERR_STATE, "rr_ri_fock_x2c: handle holds a 4-component store");
+  const int64_t nl = h->n, n = 2 * nl, nn2 = n * n * 2;
+  RR_REQUIRE(n_eff >= 0 && n_eff <= n, RR_ERR_ARG, "rr_ri_fock_x2c: n_eff out of range");
+  const bool host = !o || o->mem == RR_MEM_HOST;
+  cudaStream_t s = call_stream(h, o);
+  const int64_t pitch = round_up(std::max<int64_t>(nl * nl, 2), 32);
+  double *Pd = nullptr, *hd = nullptr, *Sd = nullptr, *Xd = nullptr, *Fd = nullptr, *Dp, *Ct, *G;
+  // This call's matrices live in `solver_w`: two_electron_rel and occupied_ct re-carve `mats` and
+  // `solver_a` for their own intermediates.
+  Arena ar(&h->solver_w);
+  ar.request(&Dp, pitch);
+  ar.request(&Ct, 2 * n * std::max<int64_t>(n_eff, 1));
+  ar.request(&G, nn2);
+  if (host) {
+    ar.request(&hd, nn2);
+    ar.request(&Pd, nn2);
+    ar.request(&Sd, nn2);
+    ar.request(&Xd, 2 * n * n_eff);
+    ar.request(&Fd, nn2);
+  }
+  ar.commit();
+  if (!host) {
+    hd = const_cast<double*>(hc); Pd = const_cast<double*>(P); Sd = const_cast<double*>(S); Xd = const_cast<double*>(X);
+    Fd = F;
+  }
+  prof_mark(h, 0, s);
+  if (host) {
+    copy_in(hd, hc, nn2, true, s);
+    copy_in(Pd, P, nn2, true, s);
+    copy_in(Sd, S, nn2, true, s);
+    copy_in(Xd, X, 2 * n * n_eff, true, s);
+  }
+  RR_CUDA(cudaMemsetAsync(Dp, 0, sizeof(double) * pitch, s));
+  spin_sum_kernel<<<blocks_for(nl * nl), 256, 0, s>>>(Dp, Pd, n, 0, nl, nl);
+  RR_LAUNCH_CHECK();
+  const int64_t r = occupied_ct(h, Xd, Sd, Pd, n, n_eff, 1.0, true, true, Ct, s);
+  prof_mark(h, 1, s);
+  Flavours fl;
+  fl.nf = 2;
+  fl.off = {0, nl, 0, 0};
+  fl.fs = {nl, nl, 0, 0};
+  fl.tens = {0, 0, 0, 0};
+  const double* dps[1] = {Dp};
+  two_electron_rel(h, fl, n, Ct, r, dps, G, s);
+  add_kernel<<<blocks_for(nn2), 256, 0, s>>>(Fd, hd, G, nn2);
+  RR_LAUNCH_CHECK();
+  if (host) copy_out(F, Fd, nn2, true, s);
+  prof_mark(h, 4, s);
+  if (host || (o && o->sync)) check_status(h, s);
+}
+
+// riFockTwoElectronDirect: G from P_ukb (J) and caller-supplied C_occ_ukb / occupations (K).
+void ukb_two_electron(rr_ri_store* h, const double* P, const double* C, int64_t nocc, const double* occ, double* Gout,
+                      const rr_opts* o) {
+  RR_REQUIRE(h->ntens == 2, RR_ERR_STATE, "rr_ri_two_electron_ukb: needs a 4-component store (rr_ri_create_4c)");
+  const int64_t nl = h->n, ns = h->ns, nu = 2 * nl + 2 * ns, nn2 = nu * nu * 2;
+  RR_REQUIRE(nocc >= 0 && nocc <= nu, RR_ERR_ARG, "riFockTwoElectronDirect: c_occ_ukb dimension does not match n_ukb x occupations.size()");
+  const bool host = !o || o->mem == RR_MEM_HOST;
+  cudaStream_t s = call_stream(h, o);
+  const int64_t pl = round_up(std::max<int64_t>(nl * nl, 2), 32), ps = round_up(std::max<int64_t>(ns * ns, 2), 32);
+  double *DL, *DS, *Ct, *Pd = const_cast<double*>(P), *Cd = const_cast<double*>(C), *od = const_cast<double*>(occ),
+         *G = Gout;
+  Arena ar(&h->solver_w);
+  ar.request(&DL, pl);
+  ar.request(&DS, ps);
+  ar.request(&Ct, 2 * nu * std::max<int64_t>(nocc, 1));
+  if (host) {
+    ar.request(&Cd, 2 * nu * std::max<int64_t>(nocc, 1));
+    ar.request(&od, nocc);
+    ar.request(&Pd, nn2);
+    ar.request(&G, nn2);
+  }
+  ar.commit();
+  if (host) {
+    copy_in(Pd, P, nn2, true, s);
+    copy_in(Cd, C, 2 * nu * nocc, true, s);
+    copy_in(od, occ, nocc, true, s);
+  }
+  prof_mark(h, 0, s);
+  RR_CUDA(cudaMemsetAsync(DL, 0, sizeof(double) * pl, s));
+  RR_CUDA(cudaMemsetAsync(DS, 0, sizeof(double) * ps, s));
+  spin_sum_kernel<<<blocks_for(nl * nl), 256, 0, s>>>(DL, Pd, nu, 0, nl, nl);
+  RR_LAUNCH_CHECK();
+  if (ns) {
+    spin_sum_kernel<<<blocks_for(ns * ns), 256, 0, s>>>(DS, Pd, nu, 2 * nl, 2 * nl + ns, ns);
+    RR_LAUNCH_CHECK();
+  }
+  if (nocc) {
+    ct_from_occupied_kernel<<<blocks_for(nocc * nu), 256, 0, s>>>(Ct, Cd, od, nu, nocc);
+    RR_LAUNCH_CHECK();
+  }
+  prof_mark(h, 1, s);
+  Flavours fl;
+  fl.nf = 4;
+  fl.off = {0, nl, 2 * nl, 2 * nl + ns};
+  fl.fs = {nl, nl, ns, ns};
+  fl.tens = {0, 0, 1, 1};
+  const double* dps[2] = {DL, DS};
+  two_electron_rel(h, fl, nu, Ct, nocc, dps, G, s);
+  if (host) copy_out(Gout, G, nn2, true, s);
+  prof_mark(h, 4, s);
+  if (host || (o && o->sync)) check_status(h, s);
+}
+
+// rkbFockMatrix: recovery in the RKB basis with x_full / s_full, embedding with v_total.
+void fock_rkb(rr_ri_store* h, const double* hc, const double* v, int64_t n_rkb, const double* s_full,
+              const double* x_full, int64_t n_eff, const double* P, double* F, const rr_opts* o) {
+  RR_REQUIRE(h->ntens == 2, RR_ERR_STATE, "rr_ri_fock_rkb: needs a 4-component store (rr_ri_create_4c)");
+  const int64_t nl = h->n, ns = h->ns, nu = 2 * nl + 2 * ns;
+  RR_REQUIRE(n_rkb >= 1 && n_eff >= 0 && n_eff <= n_rkb, RR_ERR_ARG, "rr_ri_fock_rkb: bad n_rkb / n_eff");
+  const bool host = !o || o->mem == RR_MEM_HOST;
+  cudaStream_t s = call_stream(h, o);
+  const int64_t rr2 = n_rkb * n_rkb * 2, uu2 = nu * nu * 2, ur2 = nu * n_rkb * 2;
+  const int64_t pl = round_up(std::max<int64_t>(nl * nl, 2), 32), ps = round_up(std::max<int64_t>(ns * ns, 2), 32);
+  double *DL, *DS, *Ct_rkb, *Ct_ukb, *Pu, *G, *VP, *GV;
+  double *hd = const_cast<double*>(hc), *vd = const_cast<double*>(v), *sd = const_cast<double*>(s_full),
+         *xd = const_cast<double*>(x_full), *Pd = const_cast<double*>(P), *Fd = F;
+  Arena ar(&h->solver_w);
+  ar.request(&DL, pl);
+  ar.request(&DS, ps);
+  ar.request(&Ct_rkb, 2 * n_rkb * std::max<int64_t>(n_eff, 1));
+  ar.request(&Ct_ukb, 2 * nu * std::max<int64_t>(n_eff, 1));
+  ar.request(&Pu, uu2);
+  ar.request(&G, uu2);
+  ar.request(&VP, ur2);
+  ar.request(&GV, ur2);
+  if (host) {
+    ar.request(&hd, rr2);
+    ar.request(&vd, ur2);
+    ar.request(&sd, rr2);
+    ar.request(&xd, 2 * n_rkb * n_eff);
+    ar.request(&Pd, rr2);
+    ar.request(&Fd, rr2);
+  }
+  ar.commit();
+  if (host) {
+    copy_in(hd, hc, rr2, true, s);
+    copy_in(vd, v, ur2, true, s);
+    copy_in(sd, s_full, rr2, true, s);
+    copy_in(xd, x_full, 2 * n_rkb * n_eff, true, s);
+    copy_in(Pd, P, rr2, true, s);
+  }
+  prof_mark(h, 0, s);
+  const int64_t r = occupied_ct(h, xd, sd, Pd, n_rkb, n_eff, 1.0, true, true, Ct_rkb, s);
+  // c_t (UKB) = c_t (RKB) v_total^dagger  (C_occ_ukb = v_total C_occ_rkb)
+  GemmDesc g;
+  g.cplx = true;
+  if (r > 0) {
+    g.M = r; g.N = nu; g.K = n_rkb;
+    g.A = Ct_rkb; g.lda = n_rkb; g.B = vd; g.ldb = n_rkb; g.opB = Op::T; g.conjB = true;
+    g.C = Ct_ukb; g.ldc = nu;
+    gemm(g, s);
+  }
+  // P_ukb = v P v^dagger
+  GemmDesc a;
+  a.cplx = true;
+  a.M = nu; a.N = n_rkb; a.K = n_rkb; a.A = vd; a.lda = n_rkb; a.B = Pd; a.ldb = n_rkb; a.C = VP; a.ldc = n_rkb;
+  gemm(a, s);
+  a.M = nu; a.N = nu; a.K = n_rkb; a.A = VP; a.lda = n_rkb; a.B = vd; a.ldb = n_rkb; a.opB = Op::T; a.conjB = true;
+  a.C = Pu; a.ldc = nu;
+  gemm(a, s);
+  RR_CUDA(cudaMemsetAsync(DL, 0, sizeof(double) * pl, s));
+  RR_CUDA(cudaMemsetAsync(DS, 0, sizeof(double) * ps, s));
+  spin_sum_kernel<<<blocks_for(nl * nl), 256, 0, s>>>(DL, Pu, nu, 0, nl, nl);
+  RR_LAUNCH_CHECK();
+  if (ns) {
+    spin_sum_kernel<<<blocks_for(ns * ns), 256, 0, s>>>(DS, Pu, nu, 2 * nl, 2 * nl + ns, ns);
+    RR_LAUNCH_CHECK();
+  }
+  prof_mark(h, 1, s);
+  Flavours fl;
+  fl.nf = 4;
+  fl.off = {0, nl, 2 * nl, 2 * nl + ns};
+  fl.fs = {nl, nl, ns, ns};
+  fl.tens = {0, 0, 1, 1};
+  const double* dps[2] = {DL, DS};
+  two_electron_rel(h, fl, nu, Ct_ukb, r, dps, G, s);
+  // F = h + v^dagger G v
+  GemmDesc b;
+  b.cplx = true;
+  b.M = nu; b.N = n_rkb; b.K = nu; b.A = G; b.lda = nu; b.B = vd; b.ldb = n_rkb; b.C = GV; b.ldc = n_rkb;
+  gemm(b, s);
+  if (Fd != hd) copy_out(Fd, hd, rr2, false, s);
+  b.M = n_rkb; b.N = n_rkb; b.K = nu; b.A = vd; b.lda = n_rkb; b.opA = Op::T; b.conjA = true; b.B = GV; b.ldb = n_rkb;
+  b.C = Fd; b.ldc = n_rkb; b.beta = 1.0;
+  gemm(b, s);
+  if (host) copy_out(F, Fd, rr2, true, s);
+  prof_mark(h, 4, s);
+  if (host || (o && o->sync)) check_status(h, s);
+}
+
+}  // namespace rr

@@ -148,3 +148,110 @@ def jk_occupied(store: RiStore, C_occ, stream: int | None = None):
     o = L.opts(L.RR_MEM_DEVICE if dev else L.RR_MEM_HOST, stream=stream)
     L.check(L.lib().rr_ri_jk_occupied(store.handle, _ptr(C), C.shape[1], _ptr(J), _ptr(K), ctypes.byref(o)))
     return J, K
+
+
+def _cplx_out(shape, like_dev, device=None):
+    if like_dev:
+        return torch.empty(shape, dtype=torch.complex128, device=device)
+    return np.empty(shape, dtype=np.complex128)
+
+
+class RiX2cEriSource:
+    """src/X2C_DHF/X2C_FockMatrixRi.h:29: nl, eri3_L (n_aux, nl*nl) real, x_large / overlap complex."""
+
+    def __init__(self, nl, eri3_L, x_large, overlap):
+        self.nl = int(nl)
+        self.eri3_L = eri3_L
+        self.x_large = x_large
+        self.overlap = overlap
+        self._store = None
+
+    @property
+    def store(self) -> RiStore:
+        if self._store is None:
+            if self.eri3_L.shape[1] != self.nl * self.nl:
+                raise RrError(L.RR_ERR_ARG, "x2cFockMatrix (RI): eri3_L column count does not match nl^2")
+            self._store = RiStore(self.eri3_L, nl=self.nl)
+        return self._store
+
+
+def x2cFockMatrix(h_x2c, eri: RiX2cEriSource, density_matrix, stream: int | None = None):
+    """src/X2C_DHF/X2C_FockMatrixRi.cpp:79 via rr_ri_fock_x2c (complex 2nl x 2nl)."""
+    n = 2 * eri.nl
+    if tuple(density_matrix.shape) != (n, n):
+        raise RrError(L.RR_ERR_ARG, "x2cFockMatrix (RI): density_matrix dimension does not match 2*nLarge")
+    if eri.eri3_L.shape[1] != eri.nl * eri.nl:
+        raise RrError(L.RR_ERR_ARG, "x2cFockMatrix (RI): eri3_L column count does not match nl^2")
+    store = eri.store
+    dev = _is_dev(density_matrix)
+    conv = _dev if dev else _host
+    h = conv(h_x2c, np.complex128)
+    P = conv(density_matrix, np.complex128)
+    S = conv(eri.overlap, np.complex128)
+    X = conv(eri.x_large, np.complex128)
+    F = _cplx_out((n, n), dev, P.device if dev else None)
+    o = L.opts(L.RR_MEM_DEVICE if dev else L.RR_MEM_HOST, stream=stream)
+    L.check(L.lib().rr_ri_fock_x2c(store.handle, _ptr(h), _ptr(P), _ptr(S), _ptr(X), X.shape[1], _ptr(F),
+                                   ctypes.byref(o)))
+    return F
+
+
+class RiDirectEriSource:
+    """src/UKB/UkbFockMatrixRi.h:84: nl, ns, eri3_LL, eri3_SS (real), v_total, s_full, x_full (complex)."""
+
+    def __init__(self, nl, ns, eri3_LL, eri3_SS, v_total=None, s_full=None, x_full=None):
+        self.nl, self.ns = int(nl), int(ns)
+        self.eri3_LL, self.eri3_SS = eri3_LL, eri3_SS
+        self.v_total, self.s_full, self.x_full = v_total, s_full, x_full
+        self._store = None
+
+    @property
+    def store(self) -> RiStore:
+        if self._store is None:
+            if self.eri3_LL.shape[1] != self.nl ** 2 or self.eri3_SS.shape[1] != self.ns ** 2:
+                raise RrError(L.RR_ERR_ARG,
+                              "riFockTwoElectronDirect: eri3_LL/eri3_SS column count does not match nl^2/ns^2")
+            self._store = RiStore(self.eri3_LL, self.eri3_SS, nl=self.nl, ns=self.ns)
+        return self._store
+
+
+def riFockTwoElectronDirect(eri: RiDirectEriSource, density_ukb, c_occ_ukb, occupations, stream: int | None = None):
+    """src/UKB/UkbFockMatrixRi.cpp:35 via rr_ri_two_electron_ukb (the tensors come from `eri`)."""
+    nu = 2 * eri.nl + 2 * eri.ns
+    if tuple(density_ukb.shape) != (nu, nu):
+        raise RrError(L.RR_ERR_ARG, "riFockTwoElectronDirect: density_ukb dimension does not match 2*nLarge+2*nSmall")
+    if c_occ_ukb.shape[0] != nu or c_occ_ukb.shape[1] != len(occupations):
+        raise RrError(L.RR_ERR_ARG, "riFockTwoElectronDirect: c_occ_ukb dimension does not match n_ukb x occupations.size()")
+    store = eri.store
+    dev = _is_dev(density_ukb)
+    conv = _dev if dev else _host
+    P = conv(density_ukb, np.complex128)
+    C = conv(c_occ_ukb, np.complex128)
+    occ = conv(occupations, np.float64)
+    G = _cplx_out((nu, nu), dev, P.device if dev else None)
+    o = L.opts(L.RR_MEM_DEVICE if dev else L.RR_MEM_HOST, stream=stream)
+    L.check(L.lib().rr_ri_two_electron_ukb(store.handle, _ptr(P), _ptr(C), C.shape[1], _ptr(occ), _ptr(G),
+                                           ctypes.byref(o)))
+    return G
+
+
+def rkbFockMatrix(h_rkb, eri: RiDirectEriSource, density_matrix, stream: int | None = None):
+    """src/UKB/UkbFockMatrixRi.cpp:185 via rr_ri_fock_rkb."""
+    n_rkb = h_rkb.shape[0]
+    if tuple(density_matrix.shape) != (n_rkb, n_rkb):
+        raise RrError(L.RR_ERR_ARG, "rkbFockMatrix (RI): density_matrix dimension does not match h_rkb")
+    store = eri.store
+    dev = _is_dev(density_matrix)
+    conv = _dev if dev else _host
+    h = conv(h_rkb, np.complex128)
+    P = conv(density_matrix, np.complex128)
+    v = conv(eri.v_total, np.complex128)
+    s = conv(eri.s_full, np.complex128)
+    x = conv(eri.x_full, np.complex128)
+    if v.shape != (2 * eri.nl + 2 * eri.ns, n_rkb) or x.shape[0] != n_rkb:
+        raise RrError(L.RR_ERR_ARG, "rkbFockMatrix (RI): v_total/x_full dimensions are inconsistent")
+    F = _cplx_out((n_rkb, n_rkb), dev, P.device if dev else None)
+    o = L.opts(L.RR_MEM_DEVICE if dev else L.RR_MEM_HOST, stream=stream)
+    L.check(L.lib().rr_ri_fock_rkb(store.handle, _ptr(h), _ptr(v), n_rkb, _ptr(s), _ptr(x), x.shape[1], _ptr(P),
+                                   _ptr(F), ctypes.byref(o)))
+    return F
