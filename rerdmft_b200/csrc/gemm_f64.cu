@@ -31,6 +31,9 @@ struct Params {
 __device__ __forceinline__ void cp_async8(uint32_t saddr, const void* g, int bytes) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(g), "r"(bytes));
 }
+__device__ __forceinline__ void cp_async16(uint32_t saddr, const void* g, int bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(saddr), "l"(g), "r"(bytes));
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -57,7 +60,7 @@ struct Cfg {
 
 // A tile: AK (A stored M x K, k contiguous) -> smem [BM][A_LD]; else (stored K x M) -> [KT][A_LD].
 // B tile: BKM (B stored N x K) -> smem [BN][B_LD]; else (stored K x N) -> [KT][B_LD].
-template <int MT, int NT, int WM, int WN, bool AK, bool BKM, bool CPLX>
+template <int MT, int NT, int WM, int WN, bool AK, bool BKM, bool CPLX, int V>
 __global__ void __launch_bounds__(32 * WM * WN) dgemm_kernel(const Params p) {
   using CF = Cfg<MT, NT, WM, WN, AK, BKM, CPLX>;
   constexpr int BM = CF::BM, BN = CF::BN, THREADS = CF::THREADS, PL = CF::PL;
@@ -78,36 +81,58 @@ __global__ void __launch_bounds__(32 * WM * WN) dgemm_kernel(const Params p) {
   const int tid = threadIdx.x;
   const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
 
+  // V = 2: 16-byte copies of two consecutive elements along the contiguous dimension (the host
+  // only selects it when every row start and the bases are 16-byte aligned and the contiguous
+  // extents are even); V = 1: 8-byte copies.  Out-of-range elements are zero-filled.
   auto load_stage = [&](int stage, int kt) {
     const int64_t k0 = kbeg + static_cast<int64_t>(kt) * KT;
     double* sA = smem + stage * CF::STAGE;
     double* sB = sA + PL * CF::A_SZ;
+    constexpr int AW = AK ? KT : BM;  // contiguous width of the A tile
+    constexpr int BW = BKM ? KT : BN;
 #pragma unroll 4
-    for (int e = tid; e < BM * KT; e += THREADS) {
-      int r, c;
+    for (int e = tid * V; e < BM * KT; e += THREADS * V) {
+      const int r = e / AW, c = e % AW;
       int64_t gm, gk;
-      if constexpr (AK) { r = e / KT; c = e % KT; gm = m0 + r; gk = k0 + c; }
-      else { r = e / BM; c = e % BM; gk = k0 + r; gm = m0 + c; }
-      const bool ok = gm < p.M && gk < kend;
-      const int64_t off = ok ? (AK ? gm * p.lda + gk : gk * p.lda + gm) : 0;
+      if constexpr (AK) { gm = m0 + r; gk = k0 + c; }
+      else { gk = k0 + r; gm = m0 + c; }
+      const int64_t goff = AK ? gm * p.lda + gk : gk * p.lda + gm;
 #pragma unroll
       for (int pl = 0; pl < PL; ++pl) {
         const uint32_t sa = sbase + static_cast<uint32_t>(((sA - smem) + pl * CF::A_SZ + r * CF::A_LD + c) * 8);
-        cp_async8(sa, Ab + off * PL + pl, ok ? 8 : 0);
+        if constexpr (V == 2 && !CPLX) {
+          // both elements valid, only the first, or none (contiguous extent even => pairs never straddle)
+          const bool row_ok = AK ? gm < p.M : gk < kend;
+          const int64_t cpos = AK ? gk : gm;
+          const int64_t cend = AK ? kend : p.M;
+          const int nvalid = row_ok ? static_cast<int>(max(int64_t(0), min(int64_t(2), cend - cpos))) : 0;
+          cp_async16(sa, nvalid ? Ab + goff : Ab, nvalid * 8);
+        } else {
+          const bool ok = gm < p.M && gk < kend;
+          cp_async8(sa, Ab + (ok ? goff : 0) * PL + pl, ok ? 8 : 0);
+        }
       }
     }
 #pragma unroll 4
-    for (int e = tid; e < BN * KT; e += THREADS) {
-      int r, c;
+    for (int e = tid * V; e < BN * KT; e += THREADS * V) {
+      const int r = e / BW, c = e % BW;
       int64_t gn, gk;
-      if constexpr (BKM) { r = e / KT; c = e % KT; gn = n0 + r; gk = k0 + c; }
-      else { r = e / BN; c = e % BN; gk = k0 + r; gn = n0 + c; }
-      const bool ok = gn < p.N && gk < kend;
-      const int64_t off = ok ? (BKM ? gn * p.ldb + gk : gk * p.ldb + gn) : 0;
+      if constexpr (BKM) { gn = n0 + r; gk = k0 + c; }
+      else { gk = k0 + r; gn = n0 + c; }
+      const int64_t goff = BKM ? gn * p.ldb + gk : gk * p.ldb + gn;
 #pragma unroll
       for (int pl = 0; pl < PL; ++pl) {
         const uint32_t sa = sbase + static_cast<uint32_t>(((sB - smem) + pl * CF::B_SZ + r * CF::B_LD + c) * 8);
-        cp_async8(sa, Bb + off * PL + pl, ok ? 8 : 0);
+        if constexpr (V == 2 && !CPLX) {
+          const bool row_ok = BKM ? gn < p.N : gk < kend;
+          const int64_t cpos = BKM ? gk : gn;
+          const int64_t cend = BKM ? kend : p.N;
+          const int nvalid = row_ok ? static_cast<int>(max(int64_t(0), min(int64_t(2), cend - cpos))) : 0;
+          cp_async16(sa, nvalid ? Bb + goff : Bb, nvalid * 8);
+        } else {
+          const bool ok = gn < p.N && gk < kend;
+          cp_async8(sa, Bb + (ok ? goff : 0) * PL + pl, ok ? 8 : 0);
+        }
       }
     }
   };
@@ -255,10 +280,10 @@ int num_sms() {
   return sms;
 }
 
-template <int MT, int NT, int WM, int WN, bool AK, bool BKM, bool CPLX>
-void launch_cfg(const Params& p, dim3 grid, cudaStream_t s) {
+template <int MT, int NT, int WM, int WN, bool AK, bool BKM, bool CPLX, int V>
+void launch_cfg_v(const Params& p, dim3 grid, cudaStream_t s) {
   using CF = Cfg<MT, NT, WM, WN, AK, BKM, CPLX>;
-  auto kern = dgemm_kernel<MT, NT, WM, WN, AK, BKM, CPLX>;
+  auto kern = dgemm_kernel<MT, NT, WM, WN, AK, BKM, CPLX, V>;
   static bool attr = false;
   if (!attr) {
     RR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, CF::SMEM_BYTES));
@@ -266,6 +291,23 @@ void launch_cfg(const Params& p, dim3 grid, cudaStream_t s) {
   }
   kern<<<grid, CF::THREADS, CF::SMEM_BYTES, s>>>(p);
   RR_LAUNCH_CHECK();
+}
+
+// 16-byte loads need: real data, 16-byte aligned bases and batch strides, even leading dims and
+// even contiguous extents (so a pair never straddles the end of a row).
+bool vec2_ok(const Params& p, bool AK, bool BKM) {
+  auto al = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15) == 0; };
+  const bool a = al(p.A) && p.lda % 2 == 0 && p.strideA % 2 == 0 && (AK ? p.K % 2 == 0 : p.M % 2 == 0);
+  const bool b = al(p.B) && p.ldb % 2 == 0 && p.strideB % 2 == 0 && (BKM ? p.K % 2 == 0 : p.N % 2 == 0);
+  return a && b && p.kchunk % 2 == 0;
+}
+
+template <int MT, int NT, int WM, int WN, bool AK, bool BKM, bool CPLX>
+void launch_cfg(const Params& p, dim3 grid, cudaStream_t s) {
+  if constexpr (!CPLX) {
+    if (vec2_ok(p, AK, BKM)) return launch_cfg_v<MT, NT, WM, WN, AK, BKM, CPLX, 2>(p, grid, s);
+  }
+  launch_cfg_v<MT, NT, WM, WN, AK, BKM, CPLX, 1>(p, grid, s);
 }
 
 struct Shape { int bm, bn; };

@@ -88,27 +88,29 @@ __global__ void projector_kernel(double* A, int64_t n) {
 constexpr int PC_THREADS = 1024;
 
 // Left-looking pivoted Cholesky of a Hermitian PSD W (n x n, row-major, interleaved when PL = 2):
-// W = L L^dagger, L (n x rmax, leading dim ldl).  The target rank is round(trace(Pi)); the loop
-// also stops when the largest remaining diagonal drops below tol * its initial maximum.
-// rank_out[0] = rank reached.  smem: d[n], used[n] (as double), lp[2 * rmax].
+// W = L L^dagger with L stored TRANSPOSED, Lt (rmax x n, row k = column k of L), so column writes
+// and the per-row dot products read coalesced.  The target rank is round(trace(Pi)); the loop also
+// stops when the largest remaining diagonal drops below tol * its initial maximum.
+// rank_out[0] = rank reached; rows >= rank of Lt are zeroed.  smem: d[n], used[n].
 template <int PL>
-__global__ void __launch_bounds__(PC_THREADS) pivchol_kernel(const double* W, const double* Pi, int64_t n, double* L,
-                                                             int64_t ldl, int64_t rmax, double tol, int* rank_out) {
+__global__ void __launch_bounds__(PC_THREADS) pivchol_kernel(const double* W, const double* Pi, int64_t n, double* Lt,
+                                                             int64_t rmax, double tol, int* rank_out) {
   extern __shared__ double sm[];
   double* d = sm;
   double* used = sm + n;
-  double* lp = used + n;
   __shared__ double rv[32];
   __shared__ int ri[32];
-  __shared__ double s_dmax0;
+  __shared__ double s_dmax0, s_dp;
   __shared__ int s_target, s_p;
-  __shared__ double s_dp;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   double tr = 0.0;
+  double bv = -DBL_MAX;
+  int bi = -1;
   for (int64_t i = tid; i < n; i += PC_THREADS) {
     d[i] = W[(i * n + i) * PL];
     used[i] = 0.0;
     tr += Pi[(i * n + i) * PL];
+    if (d[i] > bv) { bv = d[i]; bi = static_cast<int>(i); }
   }
   for (int o = 16; o > 0; o >>= 1) tr += __shfl_xor_sync(0xffffffffu, tr, o);
   if (lane == 0) rv[warp] = tr;
@@ -116,18 +118,13 @@ __global__ void __launch_bounds__(PC_THREADS) pivchol_kernel(const double* W, co
   if (tid == 0) {
     double t = 0.0;
     for (int w = 0; w < PC_THREADS / 32; ++w) t += rv[w];
-    int target = static_cast<int>(llrint(t));
-    s_target = max(0, min(target, static_cast<int>(rmax)));
+    s_target = max(0, min(static_cast<int>(llrint(t)), static_cast<int>(rmax)));
   }
   __syncthreads();
   const int target = s_target;
   int k = 0;
   for (; k < target; ++k) {
-    // argmax of the remaining diagonal over unused rows
-    double bv = -DBL_MAX;
-    int bi = -1;
-    for (int64_t i = tid; i < n; i += PC_THREADS)
-      if (used[i] == 0.0 && d[i] > bv) { bv = d[i]; bi = static_cast<int>(i); }
+    // block argmax of the thread-local candidates (smallest index on ties)
     for (int o = 16; o > 0; o >>= 1) {
       const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
       const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
@@ -143,43 +140,40 @@ __global__ void __launch_bounds__(PC_THREADS) pivchol_kernel(const double* W, co
       if (k == 0) s_dmax0 = v;
       s_p = ix;
       s_dp = v;
+      if (ix >= 0) used[ix] = 1.0;
     }
     __syncthreads();
     const int p = s_p;
     const double dp = s_dp;
     if (p < 0 || !(dp > tol * s_dmax0) || !(dp > 0.0)) break;
-    for (int j = tid; j < k * PL; j += PC_THREADS) lp[j] = L[p * ldl * PL + j];
-    __syncthreads();
     const double inv = rsqrt(dp);
+    bv = -DBL_MAX;
+    bi = -1;
     for (int64_t i = tid; i < n; i += PC_THREADS) {
       // column p of W = conj(row p) for a Hermitian W (row p is contiguous)
       double cr = W[(p * n + i) * PL];
       double ci = PL == 2 ? -W[(p * n + i) * PL + 1] : 0.0;
-      const double* li = L + i * ldl * PL;
       for (int j = 0; j < k; ++j) {
+        const double* lj = Lt + j * n * PL;
         if (PL == 2) {  // c -= L[i][j] * conj(L[p][j])
-          const double ar = li[2 * j], ai = li[2 * j + 1], br = lp[2 * j], bi2 = lp[2 * j + 1];
+          const double ar = lj[2 * i], ai = lj[2 * i + 1], br = lj[2 * p], bi2 = lj[2 * p + 1];
           cr -= ar * br + ai * bi2;
           ci -= ai * br - ar * bi2;
         } else {
-          cr -= li[j] * lp[j];
+          cr -= lj[i] * lj[p];
         }
       }
-      double* out = L + (i * ldl + k) * PL;
+      double* out = Lt + (k * n + i) * PL;
       out[0] = cr * inv;
       if (PL == 2) out[1] = ci * inv;
-      d[i] -= (cr * cr + ci * ci) / dp;
+      const double di = d[i] - (cr * cr + ci * ci) / dp;
+      d[i] = di;
+      if (used[i] == 0.0 && di > bv) { bv = di; bi = static_cast<int>(i); }
     }
-    __syncthreads();
-    if (tid == 0) used[p] = 1.0;
+    // Lt row k is read by every thread in the next step: make the writes visible block-wide.
     __syncthreads();
   }
-  // zero the unused columns so a caller may read rmax columns
-  for (int64_t idx = tid; idx < n * (rmax - k); idx += PC_THREADS) {
-    const int64_t i = idx / (rmax - k), j = k + idx % (rmax - k);
-    L[(i * ldl + j) * PL] = 0.0;
-    if (PL == 2) L[(i * ldl + j) * PL + 1] = 0.0;
-  }
+  for (int64_t idx = tid; idx < (rmax - k) * n * PL; idx += PC_THREADS) Lt[k * n * PL + idx] = 0.0;
   if (tid == 0) rank_out[0] = k;
 }
 
@@ -209,22 +203,26 @@ int64_t occupied_ct(rr_ri_store* h, const double* X, const double* S, const doub
   ar.commit();
   rank = reinterpret_cast<int*>(res + 2);
 
+  // Small GEMMs split K across the GPU: give them the handle's scratch.
+  h->work.ensure(static_cast<size_t>(std::max<int64_t>(static_cast<int64_t>(h->work.n), 8 * n * n * PL)));
+  double* wk = h->work.p;
+  const int64_t wcap = static_cast<int64_t>(h->work.n);
   // P_eff = X^dagger (S D S * scale) X
   GemmDesc g;
   g.cplx = cplx;
   g.M = n; g.N = n; g.K = n;
   g.A = S; g.lda = n; g.B = Dp; g.ldb = n; g.C = SD; g.ldc = n;
-  gemm(g, s);
+  gemm(g, s, wk, wcap);
   g.A = SD; g.B = S; g.C = SDS;
-  gemm(g, s);
+  gemm(g, s, wk, wcap);
   g.N = n_eff; g.A = SDS; g.B = X; g.ldb = n_eff; g.C = Y; g.ldc = n_eff;
-  gemm(g, s);
+  gemm(g, s, wk, wcap);
   GemmDesc pe;
   pe.cplx = cplx;
   pe.M = n_eff; pe.N = n_eff; pe.K = n;
   pe.A = X; pe.lda = n_eff; pe.opA = Op::T; pe.conjA = cplx;
   pe.B = Y; pe.ldb = n_eff; pe.C = Pe; pe.ldc = n_eff; pe.alpha = scale;
-  gemm(pe, s);
+  gemm(pe, s, wk, wcap);
 
   // Newton-Schulz sign iteration on A = 2 Pe - I.
   if (cplx) ns_init_kernel<2><<<blocks_for(n_eff * n_eff), 256, 0, s>>>(A, Pe, n_eff);
@@ -239,7 +237,7 @@ int64_t occupied_ct(rr_ri_store* h, const double* X, const double* S, const doub
   const int max_iter = 100;
   for (int it = 0; it < max_iter; ++it) {
     sq.A = A; sq.B = A; sq.C = T; sq.alpha = 1.0;
-    gemm(sq, s);
+    gemm(sq, s, wk, wcap);
     RR_CUDA(cudaMemsetAsync(res, 0, 2 * sizeof(double), s));
     if (cplx) ns_residual_kernel<2><<<static_cast<int>(std::min<int64_t>(n_eff, 592)), 256, 0, s>>>(T, n_eff, res);
     else ns_residual_kernel<1><<<static_cast<int>(std::min<int64_t>(n_eff, 592)), 256, 0, s>>>(T, n_eff, res);
@@ -253,7 +251,7 @@ int64_t occupied_ct(rr_ri_store* h, const double* X, const double* S, const doub
     }
     // A <- 1.5 A - 0.5 A T (always at least one refinement step)
     sq.A = A; sq.B = T; sq.C = A2; sq.alpha = 1.0;
-    gemm(sq, s);
+    gemm(sq, s, wk, wcap);
     axpby(A, A2, -0.5, 1.5, n_eff * n_eff * PL, s);
     if (hres[0] < 1e-10) { converged = true; break; }
   }
@@ -265,34 +263,35 @@ int64_t occupied_ct(rr_ri_store* h, const double* X, const double* S, const doub
   const double* W = A;
   if (weighted) {  // W = Pi Pe Pi
     sq.A = A; sq.B = Pe; sq.C = T;
-    gemm(sq, s);
+    gemm(sq, s, wk, wcap);
     sq.A = T; sq.B = A; sq.C = A2;
-    gemm(sq, s);
+    gemm(sq, s, wk, wcap);
     W = A2;
   }
-  const size_t smem = sizeof(double) * (2 * n_eff + 2 * n_eff);
+  const size_t smem = sizeof(double) * 2 * n_eff;
+  RR_REQUIRE(smem <= 200 * 1024, RR_ERR_ARG, "occupied recovery: n_eff too large for the pivoted Cholesky kernel");
   if (cplx) {
     auto k = pivchol_kernel<2>;
     RR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    k<<<1, PC_THREADS, smem, s>>>(W, A, n_eff, F, n_eff, n_eff, 1e-12, rank);
+    k<<<1, PC_THREADS, smem, s>>>(W, A, n_eff, F, n_eff, 1e-12, rank);
   } else {
     auto k = pivchol_kernel<1>;
     RR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    k<<<1, PC_THREADS, smem, s>>>(W, A, n_eff, F, n_eff, n_eff, 1e-12, rank);
+    k<<<1, PC_THREADS, smem, s>>>(W, A, n_eff, F, n_eff, 1e-12, rank);
   }
   RR_LAUNCH_CHECK();
   int r = 0;
   RR_CUDA(cudaMemcpyAsync(&r, rank, sizeof(int), cudaMemcpyDeviceToHost, s));
   RR_CUDA(cudaStreamSynchronize(s));
   if (r == 0) return 0;
-  // c_t = F^dagger X^dagger  (r x n)
+  // c_t = F^dagger X^dagger = conj(Lt) X^dagger  (r x n)
   GemmDesc ct;
   ct.cplx = cplx;
   ct.M = r; ct.N = n; ct.K = n_eff;
-  ct.A = F; ct.lda = n_eff; ct.opA = Op::T; ct.conjA = cplx;
+  ct.A = F; ct.lda = n_eff; ct.opA = Op::N; ct.conjA = cplx;
   ct.B = X; ct.ldb = n_eff; ct.opB = Op::T; ct.conjB = cplx;
   ct.C = Ct; ct.ldc = n;
-  gemm(ct, s);
+  gemm(ct, s, wk, wcap);
   return r;
 }
 
