@@ -74,8 +74,8 @@ int rr_ri_create(const double* B, int64_t naux, int64_t n, int32_t mem, rr_ri_ha
       h->naux = naux;
       h->n = n;
       h->ntens = 1;
-      h->status.alloc(1);
-      RR_CUDA(cudaMemsetAsync(h->status.p, 0, sizeof(int), h->ctx.main));
+      h->status.alloc(2);
+      RR_CUDA(cudaMemsetAsync(h->status.p, 0, 2 * sizeof(int), h->ctx.main));
       upload_tensor(h->B[0], &h->pitch[0], B, naux, n * n, mem == RR_MEM_HOST, h->ctx.main);
       RR_CUDA(cudaStreamSynchronize(h->ctx.main));
     } catch (...) {
@@ -102,8 +102,8 @@ int rr_ri_create_4c(const double* B_LL, const double* B_SS, int64_t naux, int64_
       h->n = nl;
       h->ns = ns;
       h->ntens = 2;
-      h->status.alloc(1);
-      RR_CUDA(cudaMemsetAsync(h->status.p, 0, sizeof(int), h->ctx.main));
+      h->status.alloc(2);
+      RR_CUDA(cudaMemsetAsync(h->status.p, 0, 2 * sizeof(int), h->ctx.main));
       upload_tensor(h->B[0], &h->pitch[0], B_LL, naux, nl * nl, mem == RR_MEM_HOST, h->ctx.main);
       upload_tensor(h->B[1], &h->pitch[1], B_SS, naux, ns * ns, mem == RR_MEM_HOST, h->ctx.main);
       RR_CUDA(cudaStreamSynchronize(h->ctx.main));

@@ -66,7 +66,7 @@ void coulomb_async(rr_ri_store* h, const double* Dp, double* J, double scale, cu
   t.len = h->n * h->n;
   t.D = Dp;
   t.J = J;
-  JPlan pl = j_plan(1, &t, h->naux);
+  JPlan pl = j_plan(1, &t, h->naux, 1);
   h->jscr.ensure(static_cast<size_t>(round_up(pl.gpart_doubles, 32) + pl.jpart_doubles + 32));
   double* gpart = h->jscr.p;
   double* jpart = h->jscr.p + round_up(pl.gpart_doubles, 32);
@@ -92,7 +92,7 @@ void coulomb_async_multi(rr_ri_store* h, int ntens, const double* const* Dp, dou
     t[i].D = Dp[i];
     t[i].J = J[i];
   }
-  JPlan pl = j_plan(ntens, t, h->naux);
+  JPlan pl = j_plan(ntens, t, h->naux, 1);
   h->jscr.ensure(static_cast<size_t>(round_up(pl.gpart_doubles, 32) + pl.jpart_doubles + 32));
   double* gpart = h->jscr.p;
   double* jpart = h->jscr.p + round_up(pl.gpart_doubles, 32);
@@ -143,10 +143,11 @@ void fock_nonrel(rr_ri_store* h, const double* hc, const double* D, const double
     copy_in(Sd, S, n2, true, s);
     copy_in(Xd, X, n * n_eff, true, s);
   }
-  coulomb_async(h, Dp, J, 1.0, s);
-  // Occupied recovery (X^T (S D S / 2) X, eigenvalues > 0.5) as c_t = F^T X^T.
+  // Occupied recovery (X^T (S D S / 2) X, eigenvalues > 0.5) as c_t = F^T X^T, then the J passes
+  // on the side stream, overlapping the compute-bound exchange GEMMs.
   const int64_t nocc = occupied_ct(h, Xd, Sd, Dp, n, n_eff, 0.5, false, false, Ct, s);
   prof_mark(h, 1, s);
+  coulomb_async(h, Dp, J, 1.0, s);
   exchange_nonrel(h, Ct, n, false, nocc, K, s);
   prof_mark(h, 3, s);
   coulomb_join(h, s);

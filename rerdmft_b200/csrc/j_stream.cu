@@ -244,8 +244,8 @@ int sm_count() {
   return sms;
 }
 
-int grid_size(int64_t items) {
-  return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(items, 3LL * sm_count())));
+int grid_size(int64_t items, int ctas_per_sm) {
+  return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(items, static_cast<int64_t>(ctas_per_sm) * sm_count())));
 }
 
 void set_smem_attr() {
@@ -259,18 +259,19 @@ void set_smem_attr() {
 
 }  // namespace
 
-JPlan j_plan(int ntens, const JTensor* t, int64_t naux) {
+JPlan j_plan(int ntens, const JTensor* t, int64_t naux, int ctas_per_sm) {
   RR_REQUIRE(ntens >= 1 && ntens <= 2, RR_ERR_ARG, "j_plan: 1 or 2 tensors");
   JPlan pl;
   pl.ntens = ntens;
   pl.naux = naux;
+  pl.ctas_per_sm = std::max(1, ctas_per_sm);
   for (int i = 0; i < ntens; ++i) {
     pl.t[i] = t[i];
     RR_REQUIRE(t[i].pitch % 32 == 0 && t[i].pitch >= round_up(t[i].len, 2), RR_ERR_ARG, "j_plan: bad pitch");
     RR_REQUIRE(reinterpret_cast<uintptr_t>(t[i].B) % 256 == 0 && reinterpret_cast<uintptr_t>(t[i].D) % 16 == 0,
                RR_ERR_ARG, "j_plan: misaligned tensor or density");
   }
-  const int64_t grid = 3LL * sm_count();
+  const int64_t grid = static_cast<int64_t>(pl.ctas_per_sm) * sm_count();
   // Pass 1: about 16 items per CTA, whole 16 KB chunks per segment.
   for (int i = 0; i < ntens; ++i) {
     const int64_t chunks = std::max<int64_t>(1, (t[i].len + CW - 1) / CW);
@@ -300,7 +301,7 @@ void j_pass1(const JPlan& pl, double* gpart, int* err, cudaStream_t s) {
   p.items = pl.naux * p.segtot;
   p.gpart = gpart;
   p.err = err;
-  j_pass1_kernel<<<grid_size(p.items), THREADS, SMEM, s>>>(p);
+  j_pass1_kernel<<<grid_size(p.items, pl.ctas_per_sm), THREADS, SMEM, s>>>(p);
   RR_LAUNCH_CHECK();
 }
 
@@ -322,7 +323,7 @@ void j_pass2(const JPlan& pl, const double* gpart, double* jpart, int* err, cuda
   p.gpart = gpart;
   p.jpart = jpart;
   p.err = err;
-  j_pass2_kernel<<<grid_size(p.items), THREADS, SMEM, s>>>(p);
+  j_pass2_kernel<<<grid_size(p.items, pl.ctas_per_sm), THREADS, SMEM, s>>>(p);
   RR_LAUNCH_CHECK();
 }
 

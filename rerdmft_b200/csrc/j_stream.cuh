@@ -26,9 +26,10 @@ struct JPlan {
   int nrange = 0;            // pass-2 aux ranges
   int64_t gpart_doubles = 0; // naux * (nseg[0] + nseg[1])
   int64_t jpart_doubles = 0; // nrange * (len[0] + len[1])
+  int ctas_per_sm = 3;       // 1 when the passes share the GPU with concurrent GEMMs
 };
 
-JPlan j_plan(int ntens, const JTensor* t, int64_t naux);
+JPlan j_plan(int ntens, const JTensor* t, int64_t naux, int ctas_per_sm = 3);
 
 // gpart: plan.gpart_doubles scratch; jpart: plan.jpart_doubles scratch; err: device status word.
 void j_pass1(const JPlan& plan, double* gpart, int* err, cudaStream_t s);

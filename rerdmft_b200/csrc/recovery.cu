@@ -9,11 +9,12 @@
 //      sign iteration A <- A (3 - A^2)/2 on A = 2 P_eff - 1 (FP64 DMMA GEMMs only; for an
 //      idempotent density A^2 = 1 already and one refinement step is all that runs);
 //   2. W = Pi (NON_REL) or Pi P_eff Pi (weighted);
-//   3. F = pivoted Cholesky of W (rank r = round(trace Pi) = number of eigenvalues > 1/2), one
-//      CTA, left-looking, deterministic;
+//   3. an orthonormal basis Q of range(Pi) (rank r = trace Pi = number of eigenvalues > 1/2) by
+//      CholeskyQR2 of Pi G for a fixed pseudo-random G (deterministic), and F = Q for NON_REL or
+//      F = Q chol(Q^dagger P_eff Q) for the weighted case, so F F^dagger = W;
 //   4. c_t = F^dagger X^dagger (r x n), the reference's c_t up to a unitary mixing of the occupied
 //      rows, which K is invariant to.
-// One host read of r is the only synchronisation.
+// The Newton-Schulz residual read-back (which also yields trace Pi) is the only synchronisation.
 #include <cfloat>
 
 #include "ri_store.cuh"
@@ -38,11 +39,16 @@ __device__ __forceinline__ void atomic_max_pos(double* addr, double v) {
   atomicMax(reinterpret_cast<unsigned long long*>(addr), static_cast<unsigned long long>(__double_as_longlong(v)));
 }
 
-// out[0] = max |T - I|, out[1] = max_i sum_j |T_ij|  (out zeroed by the caller).
+// out[0] = max |T - I|, out[1] = max_i sum_j |T_ij|, out[2] += Re trace(A)  (out zeroed by the caller).
 template <int PL>
-__global__ void ns_residual_kernel(const double* T, int64_t n, double* out) {
+__global__ void ns_residual_kernel(const double* T, const double* A, int64_t n, double* out) {
   __shared__ double red0[32], red1[32];
   double m0 = 0.0, m1 = 0.0;
+  if (threadIdx.x == 0) {
+    double tr = 0.0;
+    for (int64_t i = blockIdx.x; i < n; i += gridDim.x) tr += A[(i * n + i) * PL];
+    atomicAdd(out + 2, tr);
+  }
   for (int64_t i = blockIdx.x; i < n; i += gridDim.x) {
     double rs = 0.0;
     for (int64_t j = threadIdx.x; j < n; j += blockDim.x) {
@@ -85,96 +91,103 @@ __global__ void projector_kernel(double* A, int64_t n) {
   }
 }
 
-constexpr int PC_THREADS = 1024;
-
-// Left-looking pivoted Cholesky of a Hermitian PSD W (n x n, row-major, interleaved when PL = 2):
-// W = L L^dagger with L stored TRANSPOSED, Lt (rmax x n, row k = column k of L), so column writes
-// and the per-row dot products read coalesced.  The target rank is round(trace(Pi)); the loop also
-// stops when the largest remaining diagonal drops below tol * its initial maximum.
-// rank_out[0] = rank reached; rows >= rank of Lt are zeroed.  smem: d[n], used[n].
+// Deterministic pseudo-random test matrix G (rows x cols, interleaved when PL = 2), entries in
+// [-1, 1) from a 64-bit integer hash of the index (splitmix64).
 template <int PL>
-__global__ void __launch_bounds__(PC_THREADS) pivchol_kernel(const double* W, const double* Pi, int64_t n, double* Lt,
-                                                             int64_t rmax, double tol, int* rank_out) {
-  extern __shared__ double sm[];
-  double* d = sm;
-  double* used = sm + n;
-  __shared__ double rv[32];
-  __shared__ int ri[32];
-  __shared__ double s_dmax0, s_dp;
-  __shared__ int s_target, s_p;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  double tr = 0.0;
-  double bv = -DBL_MAX;
-  int bi = -1;
-  for (int64_t i = tid; i < n; i += PC_THREADS) {
-    d[i] = W[(i * n + i) * PL];
-    used[i] = 0.0;
-    tr += Pi[(i * n + i) * PL];
-    if (d[i] > bv) { bv = d[i]; bi = static_cast<int>(i); }
+__global__ void fill_test_matrix_kernel(double* G, int64_t count) {
+  for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < count * PL;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    uint64_t z = static_cast<uint64_t>(idx) + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    G[idx] = static_cast<double>(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
   }
-  for (int o = 16; o > 0; o >>= 1) tr += __shfl_xor_sync(0xffffffffu, tr, o);
-  if (lane == 0) rv[warp] = tr;
-  __syncthreads();
-  if (tid == 0) {
-    double t = 0.0;
-    for (int w = 0; w < PC_THREADS / 32; ++w) t += rv[w];
-    s_target = max(0, min(static_cast<int>(llrint(t)), static_cast<int>(rmax)));
-  }
-  __syncthreads();
-  const int target = s_target;
-  int k = 0;
-  for (; k < target; ++k) {
-    // block argmax of the thread-local candidates (smallest index on ties)
-    for (int o = 16; o > 0; o >>= 1) {
-      const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
-      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-      if (ov > bv || (ov == bv && oi >= 0 && (bi < 0 || oi < bi))) { bv = ov; bi = oi; }
-    }
-    if (lane == 0) { rv[warp] = bv; ri[warp] = bi; }
+}
+
+constexpr int SC_THREADS = 256;
+
+// In-place Cholesky M = L L^dagger of a small Hermitian positive-definite r x r matrix (row-major,
+// interleaved when PL = 2); on return the lower triangle holds L and the strict upper triangle is
+// zero.  One CTA, column by column.  status[0] |= 1 on a non-positive pivot.
+template <int PL>
+__global__ void __launch_bounds__(SC_THREADS) small_chol_kernel(double* M, int64_t r, int* status) {
+  for (int64_t j = 0; j < r; ++j) {
     __syncthreads();
-    if (tid == 0) {
-      double v = -DBL_MAX;
-      int ix = -1;
-      for (int w = 0; w < PC_THREADS / 32; ++w)
-        if (rv[w] > v || (rv[w] == v && ri[w] >= 0 && (ix < 0 || ri[w] < ix))) { v = rv[w]; ix = ri[w]; }
-      if (k == 0) s_dmax0 = v;
-      s_p = ix;
-      s_dp = v;
-      if (ix >= 0) used[ix] = 1.0;
+    double djj = M[(j * r + j) * PL];
+    for (int64_t k = 0; k < j; ++k) {
+      const double lr = M[(j * r + k) * PL], li = PL == 2 ? M[(j * r + k) * PL + 1] : 0.0;
+      djj -= lr * lr + li * li;
     }
-    __syncthreads();
-    const int p = s_p;
-    const double dp = s_dp;
-    if (p < 0 || !(dp > tol * s_dmax0) || !(dp > 0.0)) break;
-    const double inv = rsqrt(dp);
-    bv = -DBL_MAX;
-    bi = -1;
-    for (int64_t i = tid; i < n; i += PC_THREADS) {
-      // column p of W = conj(row p) for a Hermitian W (row p is contiguous)
-      double cr = W[(p * n + i) * PL];
-      double ci = PL == 2 ? -W[(p * n + i) * PL + 1] : 0.0;
-      for (int j = 0; j < k; ++j) {
-        const double* lj = Lt + j * n * PL;
-        if (PL == 2) {  // c -= L[i][j] * conj(L[p][j])
-          const double ar = lj[2 * i], ai = lj[2 * i + 1], br = lj[2 * p], bi2 = lj[2 * p + 1];
-          cr -= ar * br + ai * bi2;
-          ci -= ai * br - ar * bi2;
-        } else {
-          cr -= lj[i] * lj[p];
-        }
+    if (!(djj > 0.0)) {
+      if (threadIdx.x == 0) atomicOr(status, 1);
+      djj = 1e-300;
+    }
+    const double ljj = sqrt(djj);
+    for (int64_t i = j + 1 + threadIdx.x; i < r; i += SC_THREADS) {
+      // L[i][j] = (M[i][j] - sum_k L[i][k] conj(L[j][k])) / L[j][j]
+      double cr = M[(i * r + j) * PL], ci = PL == 2 ? M[(i * r + j) * PL + 1] : 0.0;
+      for (int64_t k = 0; k < j; ++k) {
+        const double ar = M[(i * r + k) * PL], ai = PL == 2 ? M[(i * r + k) * PL + 1] : 0.0;
+        const double br = M[(j * r + k) * PL], bi = PL == 2 ? M[(j * r + k) * PL + 1] : 0.0;
+        cr -= ar * br + ai * bi;
+        if (PL == 2) ci -= ai * br - ar * bi;
       }
-      double* out = Lt + (k * n + i) * PL;
-      out[0] = cr * inv;
-      if (PL == 2) out[1] = ci * inv;
-      const double di = d[i] - (cr * cr + ci * ci) / dp;
-      d[i] = di;
-      if (used[i] == 0.0 && di > bv) { bv = di; bi = static_cast<int>(i); }
+      M[(i * r + j) * PL] = cr / ljj;
+      if (PL == 2) M[(i * r + j) * PL + 1] = ci / ljj;
     }
-    // Lt row k is read by every thread in the next step: make the writes visible block-wide.
     __syncthreads();
+    if (threadIdx.x == 0) {
+      M[(j * r + j) * PL] = ljj;
+      if (PL == 2) M[(j * r + j) * PL + 1] = 0.0;
+    }
+    for (int64_t i = threadIdx.x; i < j; i += SC_THREADS) {  // zero the strict upper part of column j
+      M[(i * r + j) * PL] = 0.0;
+      if (PL == 2) M[(i * r + j) * PL + 1] = 0.0;
+    }
   }
-  for (int64_t idx = tid; idx < (rmax - k) * n * PL; idx += PC_THREADS) Lt[k * n * PL + idx] = 0.0;
-  if (tid == 0) rank_out[0] = k;
+}
+
+// Y (rows x r) <- Y L^{-dagger} (solve X L^dagger = Y row by row), L lower triangular r x r.
+template <int PL>
+__global__ void trsm_right_kernel(double* Y, const double* L, int64_t rows, int64_t r) {
+  for (int64_t row = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; row < rows;
+       row += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double* y = Y + row * r * PL;
+    for (int64_t j = 0; j < r; ++j) {
+      // x_j = (y_j - sum_{k<j} x_k conj(L[j][k])) / L[j][j]
+      double cr = y[j * PL], ci = PL == 2 ? y[j * PL + 1] : 0.0;
+      for (int64_t k = 0; k < j; ++k) {
+        const double xr = y[k * PL], xi = PL == 2 ? y[k * PL + 1] : 0.0;
+        const double lr = L[(j * r + k) * PL], li = PL == 2 ? L[(j * r + k) * PL + 1] : 0.0;
+        cr -= xr * lr + xi * li;
+        if (PL == 2) ci -= xi * lr - xr * li;
+      }
+      const double d = L[(j * r + j) * PL];
+      y[j * PL] = cr / d;
+      if (PL == 2) y[j * PL + 1] = ci / d;
+    }
+  }
+}
+
+// Y (rows x r) <- Y L, L lower triangular r x r.
+template <int PL>
+__global__ void trmm_right_kernel(double* Y, const double* L, int64_t rows, int64_t r) {
+  for (int64_t row = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; row < rows;
+       row += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double* y = Y + row * r * PL;
+    for (int64_t j = 0; j < r; ++j) {  // x_j = sum_{k>=j} y_k L[k][j]; increasing j reads only k >= j
+      double cr = 0.0, ci = 0.0;
+      for (int64_t k = j; k < r; ++k) {
+        const double yr = y[k * PL], yi = PL == 2 ? y[k * PL + 1] : 0.0;
+        const double lr = L[(k * r + j) * PL], li = PL == 2 ? L[(k * r + j) * PL + 1] : 0.0;
+        cr += yr * lr - yi * li;
+        if (PL == 2) ci += yr * li + yi * lr;
+      }
+      y[j * PL] = cr;
+      if (PL == 2) y[j * PL + 1] = ci;
+    }
+  }
 }
 
 int blocks_for(int64_t n) { return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 1184))); }
@@ -199,9 +212,10 @@ int64_t occupied_ct(rr_ri_store* h, const double* X, const double* S, const doub
   ar.request(&T, n_eff * n_eff * PL);
   ar.request(&A2, n_eff * n_eff * PL);
   ar.request(&F, n_eff * n_eff * PL);
-  ar.request(&res, 4);
+  ar.request(&res, 8);
   ar.commit();
-  rank = reinterpret_cast<int*>(res + 2);
+  rank = reinterpret_cast<int*>(res + 4);
+  (void)rank;
 
   // Small GEMMs split K across the GPU: give them the handle's scratch.
   h->work.ensure(static_cast<size_t>(std::max<int64_t>(static_cast<int64_t>(h->work.n), 8 * n * n * PL)));
@@ -232,17 +246,17 @@ int64_t occupied_ct(rr_ri_store* h, const double* X, const double* S, const doub
   sq.cplx = cplx;
   sq.M = n_eff; sq.N = n_eff; sq.K = n_eff;
   sq.lda = n_eff; sq.ldb = n_eff; sq.ldc = n_eff;
-  double hres[2] = {0.0, 0.0};
+  double hres[3] = {0.0, 0.0, 0.0};
   bool converged = false;
   const int max_iter = 100;
   for (int it = 0; it < max_iter; ++it) {
     sq.A = A; sq.B = A; sq.C = T; sq.alpha = 1.0;
     gemm(sq, s, wk, wcap);
-    RR_CUDA(cudaMemsetAsync(res, 0, 2 * sizeof(double), s));
-    if (cplx) ns_residual_kernel<2><<<static_cast<int>(std::min<int64_t>(n_eff, 592)), 256, 0, s>>>(T, n_eff, res);
-    else ns_residual_kernel<1><<<static_cast<int>(std::min<int64_t>(n_eff, 592)), 256, 0, s>>>(T, n_eff, res);
+    RR_CUDA(cudaMemsetAsync(res, 0, 3 * sizeof(double), s));
+    if (cplx) ns_residual_kernel<2><<<static_cast<int>(std::min<int64_t>(n_eff, 592)), 256, 0, s>>>(T, A, n_eff, res);
+    else ns_residual_kernel<1><<<static_cast<int>(std::min<int64_t>(n_eff, 592)), 256, 0, s>>>(T, A, n_eff, res);
     RR_LAUNCH_CHECK();
-    RR_CUDA(cudaMemcpyAsync(hres, res, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    RR_CUDA(cudaMemcpyAsync(hres, res, 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
     RR_CUDA(cudaStreamSynchronize(s));
     if (it == 0 && hres[1] > 2.5) {
       // ||A||_2 <= sqrt(||A^2||_inf): scale into the convergence region of the iteration
@@ -260,35 +274,61 @@ int64_t occupied_ct(rr_ri_store* h, const double* X, const double* S, const doub
   if (cplx) projector_kernel<2><<<blocks_for(n_eff * n_eff), 256, 0, s>>>(A, n_eff);
   else projector_kernel<1><<<blocks_for(n_eff * n_eff), 256, 0, s>>>(A, n_eff);
   RR_LAUNCH_CHECK();
-  const double* W = A;
-  if (weighted) {  // W = Pi Pe Pi
-    sq.A = A; sq.B = Pe; sq.C = T;
-    gemm(sq, s, wk, wcap);
-    sq.A = T; sq.B = A; sq.C = A2;
-    gemm(sq, s, wk, wcap);
-    W = A2;
-  }
-  const size_t smem = sizeof(double) * 2 * n_eff;
-  RR_REQUIRE(smem <= 200 * 1024, RR_ERR_ARG, "occupied recovery: n_eff too large for the pivoted Cholesky kernel");
-  if (cplx) {
-    auto k = pivchol_kernel<2>;
-    RR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    k<<<1, PC_THREADS, smem, s>>>(W, A, n_eff, F, n_eff, 1e-12, rank);
-  } else {
-    auto k = pivchol_kernel<1>;
-    RR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    k<<<1, PC_THREADS, smem, s>>>(W, A, n_eff, F, n_eff, 1e-12, rank);
-  }
-  RR_LAUNCH_CHECK();
-  int r = 0;
-  RR_CUDA(cudaMemcpyAsync(&r, rank, sizeof(int), cudaMemcpyDeviceToHost, s));
-  RR_CUDA(cudaStreamSynchronize(s));
+  // Rank = number of eigenvalues above 1/2 = trace(Pi) = (n_eff + trace(sign))/2.
+  const int64_t r = std::max<int64_t>(0, std::min<int64_t>(n_eff, std::llround(0.5 * (n_eff + hres[2]))));
   if (r == 0) return 0;
-  // c_t = F^dagger X^dagger = conj(Lt) X^dagger  (r x n)
+  // Orthonormal basis of range(Pi): Y = Pi G (fixed pseudo-random G), CholeskyQR2.
+  double *G, *Y2, *M, *PQ;
+  Arena ar2(&h->T);  // the exchange intermediate is not live yet
+  ar2.request(&G, n_eff * r * PL);
+  ar2.request(&Y2, n_eff * r * PL);
+  ar2.request(&M, r * r * PL);
+  ar2.request(&PQ, n_eff * r * PL);
+  ar2.commit();
+  if (cplx) fill_test_matrix_kernel<2><<<blocks_for(n_eff * r * 2), 256, 0, s>>>(G, n_eff * r);
+  else fill_test_matrix_kernel<1><<<blocks_for(n_eff * r), 256, 0, s>>>(G, n_eff * r);
+  RR_LAUNCH_CHECK();
+  GemmDesc y;
+  y.cplx = cplx;
+  y.M = n_eff; y.N = r; y.K = n_eff;
+  y.A = A; y.lda = n_eff; y.B = G; y.ldb = r; y.C = Y2; y.ldc = r;
+  gemm(y, s, wk, wcap);
+  GemmDesc gm;  // M = Y^dagger Y
+  gm.cplx = cplx;
+  gm.M = r; gm.N = r; gm.K = n_eff;
+  gm.A = Y2; gm.lda = r; gm.opA = Op::T; gm.conjA = cplx;
+  gm.B = Y2; gm.ldb = r; gm.C = M; gm.ldc = r;
+  auto chol = [&](double* mat) {
+    if (cplx) small_chol_kernel<2><<<1, SC_THREADS, 0, s>>>(mat, r, h->status.p + 1);
+    else small_chol_kernel<1><<<1, SC_THREADS, 0, s>>>(mat, r, h->status.p + 1);
+    RR_LAUNCH_CHECK();
+  };
+  for (int pass = 0; pass < 2; ++pass) {
+    gemm(gm, s, wk, wcap);
+    chol(M);
+    if (cplx) trsm_right_kernel<2><<<blocks_for(n_eff), 256, 0, s>>>(Y2, M, n_eff, r);
+    else trsm_right_kernel<1><<<blocks_for(n_eff), 256, 0, s>>>(Y2, M, n_eff, r);
+    RR_LAUNCH_CHECK();
+  }
+  if (weighted) {  // F = Q chol(Q^dagger Pe Q): F F^dagger = Pi Pe Pi
+    GemmDesc pq;
+    pq.cplx = cplx;
+    pq.M = n_eff; pq.N = r; pq.K = n_eff;
+    pq.A = Pe; pq.lda = n_eff; pq.B = Y2; pq.ldb = r; pq.C = PQ; pq.ldc = r;
+    gemm(pq, s, wk, wcap);
+    GemmDesc qp = gm;
+    qp.B = PQ;
+    gemm(qp, s, wk, wcap);
+    chol(M);
+    if (cplx) trmm_right_kernel<2><<<blocks_for(n_eff), 256, 0, s>>>(Y2, M, n_eff, r);
+    else trmm_right_kernel<1><<<blocks_for(n_eff), 256, 0, s>>>(Y2, M, n_eff, r);
+    RR_LAUNCH_CHECK();
+  }
+  // c_t = F^dagger X^dagger  (r x n)
   GemmDesc ct;
   ct.cplx = cplx;
   ct.M = r; ct.N = n; ct.K = n_eff;
-  ct.A = F; ct.lda = n_eff; ct.opA = Op::N; ct.conjA = cplx;
+  ct.A = Y2; ct.lda = r; ct.opA = Op::T; ct.conjA = cplx;
   ct.B = X; ct.ldb = n_eff; ct.opB = Op::T; ct.conjB = cplx;
   ct.C = Ct; ct.ldc = n;
   gemm(ct, s, wk, wcap);

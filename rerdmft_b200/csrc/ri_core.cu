@@ -54,13 +54,16 @@ void prof_mark(rr_ri_store* h, int i, cudaStream_t s) {
 }
 
 void check_status(rr_ri_store* h, cudaStream_t s) {
-  int word = 0;
-  RR_CUDA(cudaMemcpyAsync(&word, h->status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  // word 0: bounded-wait expiries (TMA pipelines); word 1: numerical failures (recovery Cholesky)
+  int word[2] = {0, 0};
+  RR_CUDA(cudaMemcpyAsync(word, h->status.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
   RR_CUDA(cudaStreamSynchronize(s));
-  if (word != 0) {
-    RR_CUDA(cudaMemsetAsync(h->status.p, 0, sizeof(int), s));
+  if (word[0] != 0 || word[1] != 0) {
+    RR_CUDA(cudaMemsetAsync(h->status.p, 0, 2 * sizeof(int), s));
     RR_CUDA(cudaStreamSynchronize(s));
-    throw Error(RR_ERR_TIMEOUT, "device wait bound expired (status word 0x" + std::to_string(word) + ")");
+    if (word[0] != 0)
+      throw Error(RR_ERR_TIMEOUT, "device wait bound expired (status word 0x" + std::to_string(word[0]) + ")");
+    throw Error(RR_ERR_SOLVER, "occupied recovery: the occupied-space Gram matrix is not positive definite");
   }
 }
 
