@@ -342,11 +342,12 @@ Shape pick_shape(const GemmDesc& d) {
 int pick_splits(const GemmDesc& d, Shape sh, int64_t* kchunk) {
   int64_t tiles = static_cast<int64_t>(ceil_div(d.M, sh.bm)) * ceil_div(d.N, sh.bn) * d.batch;
   if (d.mirror) tiles = (tiles + ceil_div(d.M, sh.bm) * d.batch) / 2;
-  const int64_t target = 2LL * num_sms();
+  // Enough CTAs for several waves (load balance across SMs), K chunks of at least 128.
+  const int64_t target = 8LL * num_sms();
   int splits = 1;
-  if (tiles < target && d.K >= 8 * KT) {
-    splits = static_cast<int>(std::min<int64_t>((target + tiles - 1) / tiles, d.K / (4 * KT)));
-    splits = std::max(1, std::min(splits, 64));
+  if (tiles < 2LL * num_sms() && d.K >= 8 * KT) {
+    splits = static_cast<int>(std::min<int64_t>((target + tiles - 1) / tiles, d.K / (8 * KT)));
+    splits = std::max(1, std::min(splits, 128));
   }
   int64_t kc = round_up((d.K + splits - 1) / splits, KT);
   splits = static_cast<int>((d.K + kc - 1) / kc);

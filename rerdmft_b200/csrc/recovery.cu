@@ -105,87 +105,78 @@ __global__ void fill_test_matrix_kernel(double* G, int64_t count) {
   }
 }
 
-constexpr int SC_THREADS = 256;
+constexpr int SC_THREADS = 512;
 
-// In-place Cholesky M = L L^dagger of a small Hermitian positive-definite r x r matrix (row-major,
-// interleaved when PL = 2); on return the lower triangle holds L and the strict upper triangle is
-// zero.  One CTA, column by column.  status[0] |= 1 on a non-positive pivot.
+// Cholesky M = L L^dagger of a small Hermitian positive-definite r x r matrix (row-major,
+// interleaved when PL = 2), one CTA, right-looking with the whole block on each trailing update.
+// `work` holds the r x r factor (shared memory when it fits, else global scratch).  Output:
+// out = L^{-dagger} (want_inverse) or L (upper triangle zero), r x r row-major, so that
+// Y <- Y out is a plain GEMM.  status[0] |= 1 on a non-positive pivot.
 template <int PL>
-__global__ void __launch_bounds__(SC_THREADS) small_chol_kernel(double* M, int64_t r, int* status) {
+__global__ void __launch_bounds__(SC_THREADS) chol_small_kernel(const double* M, int64_t r, double* out,
+                                                                double* gwork, int want_inverse, int* status) {
+  extern __shared__ double sm[];
+  double* L = gwork ? gwork : sm;
+  const int tid = threadIdx.x;
+  for (int64_t i = tid; i < r * r * PL; i += SC_THREADS) L[i] = M[i];
+  __syncthreads();
   for (int64_t j = 0; j < r; ++j) {
+    double d = L[(j * r + j) * PL];
+    if (!(d > 0.0)) {
+      if (tid == 0) atomicOr(status, 1);
+      d = 1e-300;
+    }
+    const double ljj = sqrt(d);
     __syncthreads();
-    double djj = M[(j * r + j) * PL];
-    for (int64_t k = 0; k < j; ++k) {
-      const double lr = M[(j * r + k) * PL], li = PL == 2 ? M[(j * r + k) * PL + 1] : 0.0;
-      djj -= lr * lr + li * li;
+    for (int64_t i = j + 1 + tid; i < r; i += SC_THREADS) {
+      L[(i * r + j) * PL] /= ljj;
+      if (PL == 2) L[(i * r + j) * PL + 1] /= ljj;
     }
-    if (!(djj > 0.0)) {
-      if (threadIdx.x == 0) atomicOr(status, 1);
-      djj = 1e-300;
-    }
-    const double ljj = sqrt(djj);
-    for (int64_t i = j + 1 + threadIdx.x; i < r; i += SC_THREADS) {
-      // L[i][j] = (M[i][j] - sum_k L[i][k] conj(L[j][k])) / L[j][j]
-      double cr = M[(i * r + j) * PL], ci = PL == 2 ? M[(i * r + j) * PL + 1] : 0.0;
-      for (int64_t k = 0; k < j; ++k) {
-        const double ar = M[(i * r + k) * PL], ai = PL == 2 ? M[(i * r + k) * PL + 1] : 0.0;
-        const double br = M[(j * r + k) * PL], bi = PL == 2 ? M[(j * r + k) * PL + 1] : 0.0;
-        cr -= ar * br + ai * bi;
-        if (PL == 2) ci -= ai * br - ar * bi;
-      }
-      M[(i * r + j) * PL] = cr / ljj;
-      if (PL == 2) M[(i * r + j) * PL + 1] = ci / ljj;
+    if (tid == 0) {
+      L[(j * r + j) * PL] = ljj;
+      if (PL == 2) L[(j * r + j) * PL + 1] = 0.0;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-      M[(j * r + j) * PL] = ljj;
-      if (PL == 2) M[(j * r + j) * PL + 1] = 0.0;
+    // trailing update of the lower triangle: A[i][k] -= L[i][j] conj(L[k][j]), j < k <= i
+    const int64_t m = r - j - 1;
+    for (int64_t e = tid; e < m * m; e += SC_THREADS) {
+      const int64_t i = j + 1 + e / m, k = j + 1 + e % m;
+      if (k > i) continue;
+      const double ar = L[(i * r + j) * PL], ai = PL == 2 ? L[(i * r + j) * PL + 1] : 0.0;
+      const double br = L[(k * r + j) * PL], bi = PL == 2 ? L[(k * r + j) * PL + 1] : 0.0;
+      L[(i * r + k) * PL] -= ar * br + ai * bi;
+      if (PL == 2) L[(i * r + k) * PL + 1] -= ai * br - ar * bi;
     }
-    for (int64_t i = threadIdx.x; i < j; i += SC_THREADS) {  // zero the strict upper part of column j
-      M[(i * r + j) * PL] = 0.0;
-      if (PL == 2) M[(i * r + j) * PL + 1] = 0.0;
-    }
+    __syncthreads();
   }
-}
-
-// Y (rows x r) <- Y L^{-dagger} (solve X L^dagger = Y row by row), L lower triangular r x r.
-template <int PL>
-__global__ void trsm_right_kernel(double* Y, const double* L, int64_t rows, int64_t r) {
-  for (int64_t row = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; row < rows;
-       row += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    double* y = Y + row * r * PL;
-    for (int64_t j = 0; j < r; ++j) {
-      // x_j = (y_j - sum_{k<j} x_k conj(L[j][k])) / L[j][j]
-      double cr = y[j * PL], ci = PL == 2 ? y[j * PL + 1] : 0.0;
-      for (int64_t k = 0; k < j; ++k) {
-        const double xr = y[k * PL], xi = PL == 2 ? y[k * PL + 1] : 0.0;
-        const double lr = L[(j * r + k) * PL], li = PL == 2 ? L[(j * r + k) * PL + 1] : 0.0;
-        cr -= xr * lr + xi * li;
-        if (PL == 2) ci -= xi * lr - xr * li;
-      }
-      const double d = L[(j * r + j) * PL];
-      y[j * PL] = cr / d;
-      if (PL == 2) y[j * PL + 1] = ci / d;
+  if (!want_inverse) {
+    for (int64_t e = tid; e < r * r; e += SC_THREADS) {
+      const int64_t i = e / r, k = e % r;
+      out[e * PL] = k <= i ? L[e * PL] : 0.0;
+      if (PL == 2) out[e * PL + 1] = k <= i ? L[e * PL + 1] : 0.0;
     }
+    return;
   }
-}
-
-// Y (rows x r) <- Y L, L lower triangular r x r.
-template <int PL>
-__global__ void trmm_right_kernel(double* Y, const double* L, int64_t rows, int64_t r) {
-  for (int64_t row = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; row < rows;
-       row += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    double* y = Y + row * r * PL;
-    for (int64_t j = 0; j < r; ++j) {  // x_j = sum_{k>=j} y_k L[k][j]; increasing j reads only k >= j
-      double cr = 0.0, ci = 0.0;
-      for (int64_t k = j; k < r; ++k) {
-        const double yr = y[k * PL], yi = PL == 2 ? y[k * PL + 1] : 0.0;
-        const double lr = L[(k * r + j) * PL], li = PL == 2 ? L[(k * r + j) * PL + 1] : 0.0;
-        cr += yr * lr - yi * li;
-        if (PL == 2) ci += yr * li + yi * lr;
+  // Column c of L^{-1}: forward substitution on e_c, one thread per column; written as row c of
+  // out = (L^{-1})^dagger, i.e. out[c][i] = conj(Linv[i][c]).
+  for (int64_t c = tid; c < r; c += SC_THREADS) {
+    double* o = out + c * r * PL;
+    for (int64_t i = 0; i < c; ++i) {
+      o[i * PL] = 0.0;
+      if (PL == 2) o[i * PL + 1] = 0.0;
+    }
+    for (int64_t i = c; i < r; ++i) {
+      // x_i = (delta_ic - sum_{c<=k<i} L[i][k] x_k) / L[i][i]; o holds conj(x)
+      double xr = i == c ? 1.0 : 0.0, xi = 0.0;
+      for (int64_t k = c; k < i; ++k) {
+        const double lr = L[(i * r + k) * PL], li = PL == 2 ? L[(i * r + k) * PL + 1] : 0.0;
+        const double yr = o[k * PL], yi = PL == 2 ? -o[k * PL + 1] : 0.0;  // x_k
+        xr -= lr * yr - li * yi;
+        if (PL == 2) xi -= lr * yi + li * yr;
       }
-      y[j * PL] = cr;
-      if (PL == 2) y[j * PL + 1] = ci;
+      const double dii = L[(i * r + i) * PL];
+      o[i * PL] = xr / dii;
+      if (PL == 2) o[i * PL + 1] = -xi / dii;
     }
   }
 }
@@ -277,14 +268,20 @@ int64_t occupied_ct(rr_ri_store* h, const double* X, const double* S, const doub
   // Rank = number of eigenvalues above 1/2 = trace(Pi) = (n_eff + trace(sign))/2.
   const int64_t r = std::max<int64_t>(0, std::min<int64_t>(n_eff, std::llround(0.5 * (n_eff + hres[2]))));
   if (r == 0) return 0;
-  // Orthonormal basis of range(Pi): Y = Pi G (fixed pseudo-random G), CholeskyQR2.
-  double *G, *Y2, *M, *PQ;
+  // Orthonormal basis of range(Pi): Y = Pi G (fixed pseudo-random G), CholeskyQR2 with the small
+  // triangular factors applied as GEMMs.
+  double *G, *Y2, *Y3, *M, *Wt, *PQ, *gw;
   Arena ar2(&h->T);  // the exchange intermediate is not live yet
   ar2.request(&G, n_eff * r * PL);
   ar2.request(&Y2, n_eff * r * PL);
+  ar2.request(&Y3, n_eff * r * PL);
   ar2.request(&M, r * r * PL);
+  ar2.request(&Wt, r * r * PL);
   ar2.request(&PQ, n_eff * r * PL);
+  ar2.request(&gw, r * r * PL);
   ar2.commit();
+  const size_t chol_smem = sizeof(double) * r * r * PL;
+  const bool chol_in_smem = chol_smem <= 160 * 1024;
   if (cplx) fill_test_matrix_kernel<2><<<blocks_for(n_eff * r * 2), 256, 0, s>>>(G, n_eff * r);
   else fill_test_matrix_kernel<1><<<blocks_for(n_eff * r), 256, 0, s>>>(G, n_eff * r);
   RR_LAUNCH_CHECK();
@@ -293,37 +290,51 @@ int64_t occupied_ct(rr_ri_store* h, const double* X, const double* S, const doub
   y.M = n_eff; y.N = r; y.K = n_eff;
   y.A = A; y.lda = n_eff; y.B = G; y.ldb = r; y.C = Y2; y.ldc = r;
   gemm(y, s, wk, wcap);
+  auto chol = [&](const double* mat, int inverse) {
+    const size_t sm = chol_in_smem ? chol_smem : 0;
+    if (cplx) {
+      auto k = chol_small_kernel<2>;
+      if (sm > 48 * 1024) RR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
+      k<<<1, SC_THREADS, sm, s>>>(mat, r, Wt, chol_in_smem ? nullptr : gw, inverse, h->status.p + 1);
+    } else {
+      auto k = chol_small_kernel<1>;
+      if (sm > 48 * 1024) RR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
+      k<<<1, SC_THREADS, sm, s>>>(mat, r, Wt, chol_in_smem ? nullptr : gw, inverse, h->status.p + 1);
+    }
+    RR_LAUNCH_CHECK();
+  };
   GemmDesc gm;  // M = Y^dagger Y
   gm.cplx = cplx;
   gm.M = r; gm.N = r; gm.K = n_eff;
-  gm.A = Y2; gm.lda = r; gm.opA = Op::T; gm.conjA = cplx;
-  gm.B = Y2; gm.ldb = r; gm.C = M; gm.ldc = r;
-  auto chol = [&](double* mat) {
-    if (cplx) small_chol_kernel<2><<<1, SC_THREADS, 0, s>>>(mat, r, h->status.p + 1);
-    else small_chol_kernel<1><<<1, SC_THREADS, 0, s>>>(mat, r, h->status.p + 1);
-    RR_LAUNCH_CHECK();
-  };
+  gm.opA = Op::T; gm.conjA = cplx; gm.lda = r; gm.ldb = r; gm.C = M; gm.ldc = r;
+  GemmDesc yw;  // Y_out = Y_in Wt
+  yw.cplx = cplx;
+  yw.M = n_eff; yw.N = r; yw.K = r;
+  yw.lda = r; yw.B = Wt; yw.ldb = r; yw.ldc = r;
+  double* cur = Y2;
+  double* nxt = Y3;
   for (int pass = 0; pass < 2; ++pass) {
+    gm.A = cur; gm.B = cur;
     gemm(gm, s, wk, wcap);
-    chol(M);
-    if (cplx) trsm_right_kernel<2><<<blocks_for(n_eff), 256, 0, s>>>(Y2, M, n_eff, r);
-    else trsm_right_kernel<1><<<blocks_for(n_eff), 256, 0, s>>>(Y2, M, n_eff, r);
-    RR_LAUNCH_CHECK();
+    chol(M, 1);
+    yw.A = cur; yw.C = nxt;
+    gemm(yw, s, wk, wcap);
+    std::swap(cur, nxt);
   }
   if (weighted) {  // F = Q chol(Q^dagger Pe Q): F F^dagger = Pi Pe Pi
     GemmDesc pq;
     pq.cplx = cplx;
     pq.M = n_eff; pq.N = r; pq.K = n_eff;
-    pq.A = Pe; pq.lda = n_eff; pq.B = Y2; pq.ldb = r; pq.C = PQ; pq.ldc = r;
+    pq.A = Pe; pq.lda = n_eff; pq.B = cur; pq.ldb = r; pq.C = PQ; pq.ldc = r;
     gemm(pq, s, wk, wcap);
-    GemmDesc qp = gm;
-    qp.B = PQ;
-    gemm(qp, s, wk, wcap);
-    chol(M);
-    if (cplx) trmm_right_kernel<2><<<blocks_for(n_eff), 256, 0, s>>>(Y2, M, n_eff, r);
-    else trmm_right_kernel<1><<<blocks_for(n_eff), 256, 0, s>>>(Y2, M, n_eff, r);
-    RR_LAUNCH_CHECK();
+    gm.A = cur; gm.B = PQ;
+    gemm(gm, s, wk, wcap);
+    chol(M, 0);
+    yw.A = cur; yw.C = nxt;
+    gemm(yw, s, wk, wcap);
+    std::swap(cur, nxt);
   }
+  Y2 = cur;
   // c_t = F^dagger X^dagger  (r x n)
   GemmDesc ct;
   ct.cplx = cplx;
