@@ -30,8 +30,13 @@ void density_from_occupied(double* Dp, const double* C, int64_t n, int64_t nocc,
 
 // Exchange K' = sum_P (Ct B^P)^T (Ct B^P) for a given Ct (nocc x n, row-major with leading
 // dimension ldct, or its transpose when ct_transposed: Ct = C^T with C stored n x nocc).
+// When Dp is given, the half-transform GEMM also accumulates the Coulomb gamma partials (J pass 1
+// fused into the B stream it already reads) and J pass 2 is launched on the side stream right
+// after it, overlapping the SYRK; J then lands in Jout (join with coulomb_join).
+void coulomb_pass2_async(rr_ri_store* h, const double* Dp, double* J, const double* gpart, int nseg, cudaStream_t s);
+
 void exchange_nonrel(rr_ri_store* h, const double* Ct, int64_t ldct, bool ct_transposed, int64_t nocc, double* K,
-                     cudaStream_t s) {
+                     cudaStream_t s, const double* Dp = nullptr, double* Jout = nullptr) {
   const int64_t n = h->n, naux = h->naux;
   if (nocc == 0 || naux == 0) {
     RR_CUDA(cudaMemsetAsync(K, 0, sizeof(double) * n * n, s));
@@ -44,8 +49,21 @@ void exchange_nonrel(rr_ri_store* h, const double* Ct, int64_t ldct, bool ct_tra
   ht.B = h->B[0].p; ht.ldb = n; ht.opB = Op::N; ht.strideB = h->pitch[0];
   ht.C = h->T.p; ht.ldc = n; ht.strideC = nocc * n;
   ht.batch = naux;
+  int nseg = 0;
+  if (Dp) {
+    nseg = ceil_div(n, gemm_tile_n(ht));
+    // Size the scratch for pass 2 as well now: growing it later would drop the partials.
+    JTensor t;
+    t.B = h->B[0].p; t.pitch = h->pitch[0]; t.len = n * n; t.D = Dp; t.J = Jout;
+    const JPlan pl = j_plan(1, &t, naux, 1);
+    h->jscr.ensure(static_cast<size_t>(round_up(naux * nseg, 32) + pl.jpart_doubles + 32));
+    ht.gamma_D = Dp;
+    ht.gamma_ld = n;
+    ht.gamma_out = h->jscr.p;
+  }
   gemm(ht, s);
   prof_mark(h, 2, s);
+  if (Dp) coulomb_pass2_async(h, Dp, Jout, h->jscr.p, nseg, s);
 
   GemmDesc sk;
   sk.M = n; sk.N = n; sk.K = naux * nocc;
@@ -107,6 +125,31 @@ void coulomb_async_multi(rr_ri_store* h, int ntens, const double* const* Dp, dou
   RR_CUDA(cudaEventRecord(c.join, c.side));
 }
 
+// J pass 2 (+ finish) on the side stream from gamma partials produced by the fused half-transform
+// (nseg partials per aux row at gpart); forks from s.
+void coulomb_pass2_async(rr_ri_store* h, const double* Dp, double* J, const double* gpart, int nseg, cudaStream_t s) {
+  JTensor t;
+  t.B = h->B[0].p;
+  t.pitch = h->pitch[0];
+  t.len = h->n * h->n;
+  t.D = Dp;
+  t.J = J;
+  JPlan pl = j_plan(1, &t, h->naux, 1);
+  pl.nseg[0] = nseg;
+  pl.gpart_doubles = h->naux * nseg;
+  const int64_t goff = round_up(pl.gpart_doubles, 32);
+  h->jscr.ensure(static_cast<size_t>(goff + pl.jpart_doubles + 32));  // gpart stays at offset 0
+  double* jpart = h->jscr.p + goff;
+  auto& c = h->ctx;
+  RR_CUDA(cudaEventRecord(c.fork, s));
+  RR_CUDA(cudaStreamWaitEvent(c.side, c.fork, 0));
+  prof_mark(h, 5, c.side);
+  j_pass2(pl, gpart, jpart, h->status.p, c.side);
+  j_finish(pl, jpart, 1.0, c.side);
+  prof_mark(h, 6, c.side);
+  RR_CUDA(cudaEventRecord(c.join, c.side));
+}
+
 void coulomb_join(rr_ri_store* h, cudaStream_t s) { RR_CUDA(cudaStreamWaitEvent(s, h->ctx.join, 0)); }
 
 int64_t occupied_ct(rr_ri_store* h, const double* X, const double* S, const double* Dp, int64_t n, int64_t n_eff,
@@ -147,8 +190,8 @@ void fock_nonrel(rr_ri_store* h, const double* hc, const double* D, const double
   // on the side stream, overlapping the compute-bound exchange GEMMs.
   const int64_t nocc = occupied_ct(h, Xd, Sd, Dp, n, n_eff, 0.5, false, false, Ct, s);
   prof_mark(h, 1, s);
-  coulomb_async(h, Dp, J, 1.0, s);
-  exchange_nonrel(h, Ct, n, false, nocc, K, s);
+  if (nocc == 0 || h->naux == 0) coulomb_async(h, Dp, J, 1.0, s);
+  exchange_nonrel(h, Ct, n, false, nocc, K, s, Dp, J);
   prof_mark(h, 3, s);
   coulomb_join(h, s);
   fock_combine(Fd, hd, J, K, n2, s);
@@ -182,9 +225,9 @@ void jk_occupied(rr_ri_store* h, const double* C, int64_t nocc, double* Jout, do
   } else {
     RR_CUDA(cudaMemsetAsync(Dp, 0, sizeof(double) * n2, s));
   }
-  coulomb_async(h, Dp, J, 1.0, s);
   prof_mark(h, 1, s);
-  exchange_nonrel(h, Cd, nocc, true, nocc, K, s);
+  if (nocc == 0 || h->naux == 0) coulomb_async(h, Dp, J, 1.0, s);
+  exchange_nonrel(h, Cd, nocc, true, nocc, K, s, Dp, J);
   prof_mark(h, 3, s);
   coulomb_join(h, s);
   if (host) {
