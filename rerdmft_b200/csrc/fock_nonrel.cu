@@ -30,13 +30,12 @@ void density_from_occupied(double* Dp, const double* C, int64_t n, int64_t nocc,
 
 // Exchange K' = sum_P (Ct B^P)^T (Ct B^P) for a given Ct (nocc x n, row-major with leading
 // dimension ldct, or its transpose when ct_transposed: Ct = C^T with C stored n x nocc).
-// When Dp is given, the half-transform GEMM also accumulates the Coulomb gamma partials (J pass 1
-// fused into the B stream it already reads) and J pass 2 is launched on the side stream right
-// after it, overlapping the SYRK; J then lands in Jout (join with coulomb_join).
-void coulomb_pass2_async(rr_ri_store* h, const double* Dp, double* J, const double* gpart, int nseg, cudaStream_t s);
+void coulomb_pass2_release(rr_ri_store* h, cudaStream_t s);
 
+// release_pass2: right after the half-transform, release the pending J pass 2 onto the side stream
+// so that it overlaps the compute-bound SYRK.
 void exchange_nonrel(rr_ri_store* h, const double* Ct, int64_t ldct, bool ct_transposed, int64_t nocc, double* K,
-                     cudaStream_t s, const double* Dp = nullptr, double* Jout = nullptr) {
+                     cudaStream_t s, bool release_pass2 = false) {
   const int64_t n = h->n, naux = h->naux;
   if (nocc == 0 || naux == 0) {
     RR_CUDA(cudaMemsetAsync(K, 0, sizeof(double) * n * n, s));
@@ -49,21 +48,9 @@ void exchange_nonrel(rr_ri_store* h, const double* Ct, int64_t ldct, bool ct_tra
   ht.B = h->B[0].p; ht.ldb = n; ht.opB = Op::N; ht.strideB = h->pitch[0];
   ht.C = h->T.p; ht.ldc = n; ht.strideC = nocc * n;
   ht.batch = naux;
-  int nseg = 0;
-  if (Dp) {
-    nseg = ceil_div(n, gemm_tile_n(ht));
-    // Size the scratch for pass 2 as well now: growing it later would drop the partials.
-    JTensor t;
-    t.B = h->B[0].p; t.pitch = h->pitch[0]; t.len = n * n; t.D = Dp; t.J = Jout;
-    const JPlan pl = j_plan(1, &t, naux, 1);
-    h->jscr.ensure(static_cast<size_t>(round_up(naux * nseg, 32) + pl.jpart_doubles + 32));
-    ht.gamma_D = Dp;
-    ht.gamma_ld = n;
-    ht.gamma_out = h->jscr.p;
-  }
   gemm(ht, s);
   prof_mark(h, 2, s);
-  if (Dp) coulomb_pass2_async(h, Dp, Jout, h->jscr.p, nseg, s);
+  if (release_pass2) coulomb_pass2_release(h, s);
 
   GemmDesc sk;
   sk.M = n; sk.N = n; sk.K = naux * nocc;
@@ -125,9 +112,11 @@ void coulomb_async_multi(rr_ri_store* h, int ntens, const double* const* Dp, dou
   RR_CUDA(cudaEventRecord(c.join, c.side));
 }
 
-// J pass 2 (+ finish) on the side stream from gamma partials produced by the fused half-transform
-// (nseg partials per aux row at gpart); forks from s.
-void coulomb_pass2_async(rr_ri_store* h, const double* Dp, double* J, const double* gpart, int nseg, cudaStream_t s) {
+// Two-phase J for the nonrelativistic build: pass 1 starts on the side stream at once (it only
+// needs D and overlaps the occupied recovery); pass 2 waits for the `mid` event, recorded on the
+// main stream after the half-transform, so it overlaps the compute-bound SYRK instead of competing
+// with the half-transform for HBM.
+void coulomb_split_async(rr_ri_store* h, const double* Dp, double* J, cudaStream_t s) {
   JTensor t;
   t.B = h->B[0].p;
   t.pitch = h->pitch[0];
@@ -135,19 +124,31 @@ void coulomb_pass2_async(rr_ri_store* h, const double* Dp, double* J, const doub
   t.D = Dp;
   t.J = J;
   JPlan pl = j_plan(1, &t, h->naux, 1);
-  pl.nseg[0] = nseg;
-  pl.gpart_doubles = h->naux * nseg;
-  const int64_t goff = round_up(pl.gpart_doubles, 32);
-  h->jscr.ensure(static_cast<size_t>(goff + pl.jpart_doubles + 32));  // gpart stays at offset 0
-  double* jpart = h->jscr.p + goff;
+  h->jscr.ensure(static_cast<size_t>(round_up(pl.gpart_doubles, 32) + pl.jpart_doubles + 32));
+  double* gpart = h->jscr.p;
+  double* jpart = h->jscr.p + round_up(pl.gpart_doubles, 32);
   auto& c = h->ctx;
+  if (!c.mid) RR_CUDA(cudaEventCreateWithFlags(&c.mid, cudaEventDisableTiming));
   RR_CUDA(cudaEventRecord(c.fork, s));
   RR_CUDA(cudaStreamWaitEvent(c.side, c.fork, 0));
   prof_mark(h, 5, c.side);
-  j_pass2(pl, gpart, jpart, h->status.p, c.side);
-  j_finish(pl, jpart, 1.0, c.side);
+  j_pass1(pl, gpart, h->status.p, c.side);
+  h->pending_pass2 = pl;
+  h->pending_gpart = gpart;
+  h->pending_jpart = jpart;
+  h->has_pending_pass2 = true;
+}
+
+void coulomb_pass2_release(rr_ri_store* h, cudaStream_t s) {
+  if (!h->has_pending_pass2) return;
+  auto& c = h->ctx;
+  RR_CUDA(cudaEventRecord(c.mid, s));
+  RR_CUDA(cudaStreamWaitEvent(c.side, c.mid, 0));
+  j_pass2(h->pending_pass2, h->pending_gpart, h->pending_jpart, h->status.p, c.side);
+  j_finish(h->pending_pass2, h->pending_jpart, 1.0, c.side);
   prof_mark(h, 6, c.side);
   RR_CUDA(cudaEventRecord(c.join, c.side));
+  h->has_pending_pass2 = false;
 }
 
 void coulomb_join(rr_ri_store* h, cudaStream_t s) { RR_CUDA(cudaStreamWaitEvent(s, h->ctx.join, 0)); }
@@ -186,12 +187,13 @@ void fock_nonrel(rr_ri_store* h, const double* hc, const double* D, const double
     copy_in(Sd, S, n2, true, s);
     copy_in(Xd, X, n * n_eff, true, s);
   }
-  // Occupied recovery (X^T (S D S / 2) X, eigenvalues > 0.5) as c_t = F^T X^T, then the J passes
-  // on the side stream, overlapping the compute-bound exchange GEMMs.
+  // J pass 1 on the side stream alongside the occupied recovery (X^T (S D S / 2) X, eigenvalues
+  // > 0.5, as c_t = F^T X^T); J pass 2 alongside the SYRK.
+  coulomb_split_async(h, Dp, J, s);
   const int64_t nocc = occupied_ct(h, Xd, Sd, Dp, n, n_eff, 0.5, false, false, Ct, s);
   prof_mark(h, 1, s);
-  if (nocc == 0 || h->naux == 0) coulomb_async(h, Dp, J, 1.0, s);
-  exchange_nonrel(h, Ct, n, false, nocc, K, s, Dp, J);
+  exchange_nonrel(h, Ct, n, false, nocc, K, s, true);
+  coulomb_pass2_release(h, s);  // no-op unless the exchange had nothing to transform
   prof_mark(h, 3, s);
   coulomb_join(h, s);
   fock_combine(Fd, hd, J, K, n2, s);
@@ -225,9 +227,10 @@ void jk_occupied(rr_ri_store* h, const double* C, int64_t nocc, double* Jout, do
   } else {
     RR_CUDA(cudaMemsetAsync(Dp, 0, sizeof(double) * n2, s));
   }
+  coulomb_split_async(h, Dp, J, s);
   prof_mark(h, 1, s);
-  if (nocc == 0 || h->naux == 0) coulomb_async(h, Dp, J, 1.0, s);
-  exchange_nonrel(h, Cd, nocc, true, nocc, K, s, Dp, J);
+  exchange_nonrel(h, Cd, nocc, true, nocc, K, s, true);
+  coulomb_pass2_release(h, s);
   prof_mark(h, 3, s);
   coulomb_join(h, s);
   if (host) {

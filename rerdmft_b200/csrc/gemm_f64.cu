@@ -26,9 +26,6 @@ struct Params {
   double signA, signB;  // -1 conjugates the imaginary plane of A / B
   int64_t c_plane_rows, c_plane_stride;
   int upper_only;
-  const double* gD;
-  int64_t ldD;
-  double* gpart;
 };
 
 __device__ __forceinline__ void cp_async8(uint32_t saddr, const void* g, int bytes) {
@@ -63,7 +60,7 @@ struct Cfg {
 
 // A tile: AK (A stored M x K, k contiguous) -> smem [BM][A_LD]; else (stored K x M) -> [KT][A_LD].
 // B tile: BKM (B stored N x K) -> smem [BN][B_LD]; else (stored K x N) -> [KT][B_LD].
-template <int MT, int NT, int WM, int WN, bool AK, bool BKM, bool CPLX, int V, bool GAM = false>
+template <int MT, int NT, int WM, int WN, bool AK, bool BKM, bool CPLX, int V>
 __global__ void __launch_bounds__(32 * WM * WN) dgemm_kernel(const Params p) {
   using CF = Cfg<MT, NT, WM, WN, AK, BKM, CPLX>;
   constexpr int BM = CF::BM, BN = CF::BN, THREADS = CF::THREADS, PL = CF::PL;
@@ -157,22 +154,11 @@ __global__ void __launch_bounds__(32 * WM * WN) dgemm_kernel(const Params p) {
     cp_async_commit();
   }
 
-  double gacc = 0.0;
   for (int kt = 0; kt < ktiles; ++kt) {
     cp_async_wait<STAGES - 2>();
     __syncthreads();
     const double* sA = smem + (kt % STAGES) * CF::STAGE;
     const double* sB = sA + PL * CF::A_SZ;
-    if constexpr (GAM) {
-      // gamma partial over this B tile (stored [KT][B_LD], k rows, n columns)
-      const int64_t k0 = kbeg + static_cast<int64_t>(kt) * KT;
-#pragma unroll 4
-      for (int e = tid; e < KT * BN; e += THREADS) {
-        const int r = e / BN, c = e % BN;
-        const int64_t gk = k0 + r, gn = n0 + c;
-        if (gk < kend && gn < p.N) gacc = fma(sB[r * CF::B_LD + c], __ldg(p.gD + gk * p.ldD + gn), gacc);
-      }
-    }
 #pragma unroll
     for (int ks = 0; ks < KT / 4; ++ks) {
       const int k = ks * 4 + t;
@@ -208,19 +194,6 @@ __global__ void __launch_bounds__(32 * WM * WN) dgemm_kernel(const Params p) {
     cp_async_commit();
   }
   cp_async_wait<0>();
-  if constexpr (GAM) {
-    // block reduction of the gamma partial (fixed order: deterministic)
-    __syncthreads();
-    for (int o = 16; o > 0; o >>= 1) gacc += __shfl_xor_sync(0xffffffffu, gacc, o);
-    double* red = smem;
-    if ((tid & 31) == 0) red[tid >> 5] = gacc;
-    __syncthreads();
-    if (tid == 0 && blockIdx.y == 0) {
-      double t = 0.0;
-      for (int w = 0; w < THREADS / 32; ++w) t += red[w];
-      p.gpart[b * gridDim.x + blockIdx.x] = t;
-    }
-  }
 
 #pragma unroll
   for (int i = 0; i < MT; ++i)
@@ -307,10 +280,10 @@ int num_sms() {
   return sms;
 }
 
-template <int MT, int NT, int WM, int WN, bool AK, bool BKM, bool CPLX, int V, bool GAM = false>
+template <int MT, int NT, int WM, int WN, bool AK, bool BKM, bool CPLX, int V>
 void launch_cfg_v(const Params& p, dim3 grid, cudaStream_t s) {
   using CF = Cfg<MT, NT, WM, WN, AK, BKM, CPLX>;
-  auto kern = dgemm_kernel<MT, NT, WM, WN, AK, BKM, CPLX, V, GAM>;
+  auto kern = dgemm_kernel<MT, NT, WM, WN, AK, BKM, CPLX, V>;
   static bool attr = false;
   if (!attr) {
     RR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, CF::SMEM_BYTES));
@@ -331,12 +304,6 @@ bool vec2_ok(const Params& p, bool AK, bool BKM) {
 
 template <int MT, int NT, int WM, int WN, bool AK, bool BKM, bool CPLX>
 void launch_cfg(const Params& p, dim3 grid, cudaStream_t s) {
-  if constexpr (!CPLX && !BKM) {
-    if (p.gpart) {
-      if (vec2_ok(p, AK, BKM)) return launch_cfg_v<MT, NT, WM, WN, AK, BKM, CPLX, 2, true>(p, grid, s);
-      return launch_cfg_v<MT, NT, WM, WN, AK, BKM, CPLX, 1, true>(p, grid, s);
-    }
-  }
   if constexpr (!CPLX) {
     if (vec2_ok(p, AK, BKM)) return launch_cfg_v<MT, NT, WM, WN, AK, BKM, CPLX, 2>(p, grid, s);
   }
@@ -390,8 +357,6 @@ int pick_splits(const GemmDesc& d, Shape sh, int64_t* kchunk) {
 
 }  // namespace
 
-int gemm_tile_n(const GemmDesc& d) { return pick_shape(d).bn; }
-
 int64_t gemm_work_doubles(const GemmDesc& d) {
   int64_t kc;
   const int s = pick_splits(d, pick_shape(d), &kc);
@@ -414,13 +379,6 @@ void gemm(const GemmDesc& d, cudaStream_t stream, double* work, int64_t work_cap
   p.signB = d.conjB ? -1.0 : 1.0;
   p.c_plane_rows = d.c_plane_rows; p.c_plane_stride = d.c_plane_stride;
   p.upper_only = d.mirror != 0;
-  p.gD = d.gamma_D;
-  p.ldD = d.gamma_ld;
-  p.gpart = d.gamma_out;
-  if (d.gamma_out) {
-    RR_REQUIRE(!d.cplx && d.opB == Op::N && d.M <= sh.bm, RR_ERR_ARG, "gemm: fused gamma needs real B (op N), one row of tiles");
-    work = nullptr;  // the fused partials assume one K range per CTA
-  }
   int64_t kc = d.K;
   int splits = 1;
   if (work && d.K > 0) {

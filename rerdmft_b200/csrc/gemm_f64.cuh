@@ -34,17 +34,7 @@ struct GemmDesc {
   // lower triangle from the upper one: +1 C[i][j] = C[j][i] (Hermitian conj for cplx),
   // -1 C[i][j] = -C[j][i].  0 = full output.  Requires M == N.
   int mirror = 0;
-  // Fused Coulomb pass 1 (real, op(B) = N, single row of output tiles, no split-K): while the
-  // B tiles stream through shared memory, also accumulate gamma partials
-  //   gamma_out[b * ceil(N / BN) + tile] = sum_{k, n in tile} B[b](k, n) * gamma_D[k * gamma_ld + n].
-  const double* gamma_D = nullptr;
-  int64_t gamma_ld = 0;
-  double* gamma_out = nullptr;
 };
-
-// Output-column tile width gemm() uses for this descriptor (gamma partials per batch entry =
-// ceil(N / width)).
-int gemm_tile_n(const GemmDesc& d);
 
 // Launches the GEMM on `stream`.  `work` (capacity `work_cap` doubles) is split-K scratch: when
 // the output grid is too small to fill the GPU and work_cap allows, K is split, the partial

@@ -34,10 +34,11 @@ void Context::destroy() {
   if (solver) cusolverDnDestroy(solver);
   if (fork) cudaEventDestroy(fork);
   if (join) cudaEventDestroy(join);
+  if (mid) cudaEventDestroy(mid);
   if (side) cudaStreamDestroy(side);
   if (own_main && main) cudaStreamDestroy(main);
   solver = nullptr;
-  fork = join = nullptr;
+  fork = join = mid = nullptr;
   side = main = nullptr;
 }
 

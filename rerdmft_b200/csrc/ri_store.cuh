@@ -26,6 +26,11 @@ struct rr_ri_store {
   bool mixed_ready = false;
   // Profiling events: 0 start, 1 recovery done, 2 half-transform done, 3 exchange done, 4 end
   // (main stream); 5 J start, 6 J end (side stream).
+  // Coulomb pass 2 waiting for the half-transform (see coulomb_split_async).
+  rr::JPlan pending_pass2;
+  double* pending_gpart = nullptr;
+  double* pending_jpart = nullptr;
+  bool has_pending_pass2 = false;
   bool profiling = false;
   cudaEvent_t ev[8] = {};
   bool ev_used[8] = {};

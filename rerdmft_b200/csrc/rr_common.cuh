@@ -88,7 +88,7 @@ struct Context {
   cudaStream_t main = nullptr;
   cudaStream_t side = nullptr;
   bool own_main = false;
-  cudaEvent_t fork = nullptr, join = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr, mid = nullptr;
   cusolverDnHandle_t solver = nullptr;
   DevBuf<double> solver_work;
   DevBuf<int> solver_info;
