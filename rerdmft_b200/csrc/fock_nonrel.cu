@@ -30,15 +30,17 @@ void density_from_occupied(double* Dp, const double* C, int64_t n, int64_t nocc,
 
 // Exchange K' = sum_P (Ct B^P)^T (Ct B^P) for a given Ct (nocc x n, row-major with leading
 // dimension ldct, or its transpose when ct_transposed: Ct = C^T with C stored n x nocc).
-void coulomb_pass2_release(rr_ri_store* h, cudaStream_t s);
+void coulomb_after_ht(rr_ri_store* h, const double* Dp, const double* Ct, int64_t nocc, double* J, cudaStream_t s);
 
-// release_pass2: right after the half-transform, release the pending J pass 2 onto the side stream
-// so that it overlaps the compute-bound SYRK.
+// With Dp given, the Coulomb matrix J (from the pitched density Dp) is queued on the side stream
+// right after the half-transform (coulomb_after_ht) and lands in Jout; join with coulomb_join.
+// The exchange reads c_t as Ct (nocc x n, ld ldct) or, when ct_transposed, as C^T of C (n x ldct).
 void exchange_nonrel(rr_ri_store* h, const double* Ct, int64_t ldct, bool ct_transposed, int64_t nocc, double* K,
-                     cudaStream_t s, bool release_pass2 = false) {
+                     cudaStream_t s, const double* Dp = nullptr, double* Jout = nullptr) {
   const int64_t n = h->n, naux = h->naux;
   if (nocc == 0 || naux == 0) {
     RR_CUDA(cudaMemsetAsync(K, 0, sizeof(double) * n * n, s));
+    if (Dp) coulomb_after_ht(h, Dp, Ct, 0, Jout, s);
     return;
   }
   h->T.ensure(static_cast<size_t>(naux * nocc * n));
@@ -50,7 +52,10 @@ void exchange_nonrel(rr_ri_store* h, const double* Ct, int64_t ldct, bool ct_tra
   ht.batch = naux;
   gemm(ht, s);
   prof_mark(h, 2, s);
-  if (release_pass2) coulomb_pass2_release(h, s);
+  if (Dp) {
+    RR_REQUIRE(!ct_transposed && ldct == n, RR_ERR_STATE, "exchange_nonrel: Coulomb from T needs row-major c_t");
+    coulomb_after_ht(h, Dp, Ct, nocc, Jout, s);
+  }
 
   GemmDesc sk;
   sk.M = n; sk.N = n; sk.K = naux * nocc;
@@ -112,43 +117,103 @@ void coulomb_async_multi(rr_ri_store* h, int ntens, const double* const* Dp, dou
   RR_CUDA(cudaEventRecord(c.join, c.side));
 }
 
-// Two-phase J for the nonrelativistic build: pass 1 starts on the side stream at once (it only
-// needs D and overlaps the occupied recovery); pass 2 waits for the `mid` event, recorded on the
-// main stream after the half-transform, so it overlaps the compute-bound SYRK instead of competing
-// with the half-transform for HBM.
-void coulomb_split_async(rr_ri_store* h, const double* Dp, double* J, cudaStream_t s) {
+namespace {
+
+// flag[0] = 1 when max |D - Drec| <= 1e-13 * max(1, max |D|), i.e. the density equals 2 C C^T of
+// the recovered occupied orbitals (an idempotent density inside span(X)).  One CTA.
+__global__ void density_match_kernel(const double* D, const double* Drec, int64_t n2, int* flag) {
+  __shared__ double r0[32], r1[32];
+  double md = 0.0, mx = 0.0;
+  for (int64_t i = threadIdx.x; i < n2; i += blockDim.x) {
+    md = fmax(md, fabs(D[i] - Drec[i]));
+    mx = fmax(mx, fabs(D[i]));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    md = fmax(md, __shfl_xor_sync(0xffffffffu, md, o));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  }
+  if ((threadIdx.x & 31) == 0) { r0[threadIdx.x >> 5] = md; r1[threadIdx.x >> 5] = mx; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) { a = fmax(a, r0[w]); b = fmax(b, r1[w]); }
+    flag[0] = a <= 1e-13 * fmax(1.0, b) ? 1 : 0;
+  }
+}
+
+// gamma_P = sum_mn B^P_mn D_mn = 2 sum_{i,a} T[P](i, a) Ct(i, a) when D = 2 Ct^T Ct (T[P] = Ct B^P):
+// the Coulomb pass 1 from the 40x smaller half-transformed tensor.  One CTA per P; runs only when
+// flag[0] is set, writing segment 0 of gpart (the other segments zero).
+__global__ void gamma_from_t_kernel(const double* T, const double* Ct, int64_t nocc, int64_t n, int64_t naux,
+                                    int segtot, double* gpart, const int* flag) {
+  if (!flag[0]) return;
+  __shared__ double red[32];
+  for (int64_t P = blockIdx.x; P < naux; P += gridDim.x) {
+    const double* tp = T + P * nocc * n;
+    double acc = 0.0;
+    for (int64_t e = threadIdx.x; e < nocc * n; e += blockDim.x) acc = fma(tp[e], Ct[e], acc);
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) t += red[w];
+      gpart[P * segtot] = 2.0 * t;
+      for (int sgi = 1; sgi < segtot; ++sgi) gpart[P * segtot + sgi] = 0.0;
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+// Coulomb for the nonrelativistic build, queued on the side stream once the half-transform is
+// done (event `mid` on s), overlapping the compute-bound SYRK:
+//   - if D = 2 C C^T for the recovered orbitals C (checked on the device), gamma comes from the
+//     half-transformed tensor T (205 MB at n=400/naux=1600/nocc=40) instead of B (2 GB);
+//   - otherwise pass 1 streams B (the kernel is launched either way and exits when not needed);
+//   - pass 2 (J = B^T gamma) streams B once.
+// Ct: nocc x n (leading dim n) c_t rows the half-transform used; T: its output.
+void coulomb_after_ht(rr_ri_store* h, const double* Dp, const double* Ct, int64_t nocc, double* J, cudaStream_t s) {
+  const int64_t n = h->n, naux = h->naux, n2 = n * n;
   JTensor t;
   t.B = h->B[0].p;
   t.pitch = h->pitch[0];
-  t.len = h->n * h->n;
+  t.len = n2;
   t.D = Dp;
   t.J = J;
-  JPlan pl = j_plan(1, &t, h->naux, 1);
-  h->jscr.ensure(static_cast<size_t>(round_up(pl.gpart_doubles, 32) + pl.jpart_doubles + 32));
+  JPlan pl = j_plan(1, &t, naux, 1);
+  const int segtot = pl.nseg[0];
+  const int64_t goff = round_up(pl.gpart_doubles, 32), joff = goff + round_up(pl.jpart_doubles, 32);
+  h->jscr.ensure(static_cast<size_t>(joff + round_up(n2, 32) + 64));
   double* gpart = h->jscr.p;
-  double* jpart = h->jscr.p + round_up(pl.gpart_doubles, 32);
+  double* jpart = h->jscr.p + goff;
+  double* Drec = h->jscr.p + joff;
+  int* flag = reinterpret_cast<int*>(h->jscr.p + joff + round_up(n2, 32));
   auto& c = h->ctx;
   if (!c.mid) RR_CUDA(cudaEventCreateWithFlags(&c.mid, cudaEventDisableTiming));
-  RR_CUDA(cudaEventRecord(c.fork, s));
-  RR_CUDA(cudaStreamWaitEvent(c.side, c.fork, 0));
-  prof_mark(h, 5, c.side);
-  j_pass1(pl, gpart, h->status.p, c.side);
-  h->pending_pass2 = pl;
-  h->pending_gpart = gpart;
-  h->pending_jpart = jpart;
-  h->has_pending_pass2 = true;
-}
-
-void coulomb_pass2_release(rr_ri_store* h, cudaStream_t s) {
-  if (!h->has_pending_pass2) return;
-  auto& c = h->ctx;
   RR_CUDA(cudaEventRecord(c.mid, s));
   RR_CUDA(cudaStreamWaitEvent(c.side, c.mid, 0));
-  j_pass2(h->pending_pass2, h->pending_gpart, h->pending_jpart, h->status.p, c.side);
-  j_finish(h->pending_pass2, h->pending_jpart, 1.0, c.side);
+  prof_mark(h, 5, c.side);
+  if (nocc > 0 && naux > 0) {
+    GemmDesc g;  // Drec = 2 Ct^T Ct
+    g.M = n; g.N = n; g.K = nocc;
+    g.A = Ct; g.lda = n; g.opA = Op::T;
+    g.B = Ct; g.ldb = n; g.C = Drec; g.ldc = n; g.alpha = 2.0;
+    gemm(g, c.side);
+    density_match_kernel<<<1, 1024, 0, c.side>>>(Dp, Drec, n2, flag);
+    RR_LAUNCH_CHECK();
+    gamma_from_t_kernel<<<static_cast<int>(std::min<int64_t>(naux, 1184)), 256, 0, c.side>>>(h->T.p, Ct, nocc, n, naux,
+                                                                                           segtot, gpart, flag);
+    RR_LAUNCH_CHECK();
+  } else {
+    RR_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), c.side));
+  }
+  j_pass1(pl, gpart, h->status.p, c.side, flag);
+  j_pass2(pl, gpart, jpart, h->status.p, c.side);
+  j_finish(pl, jpart, 1.0, c.side);
   prof_mark(h, 6, c.side);
   RR_CUDA(cudaEventRecord(c.join, c.side));
-  h->has_pending_pass2 = false;
 }
 
 void coulomb_join(rr_ri_store* h, cudaStream_t s) { RR_CUDA(cudaStreamWaitEvent(s, h->ctx.join, 0)); }
@@ -187,13 +252,11 @@ void fock_nonrel(rr_ri_store* h, const double* hc, const double* D, const double
     copy_in(Sd, S, n2, true, s);
     copy_in(Xd, X, n * n_eff, true, s);
   }
-  // J pass 1 on the side stream alongside the occupied recovery (X^T (S D S / 2) X, eigenvalues
-  // > 0.5, as c_t = F^T X^T); J pass 2 alongside the SYRK.
-  coulomb_split_async(h, Dp, J, s);
+  // Occupied recovery (X^T (S D S / 2) X, eigenvalues > 0.5) as c_t = F^T X^T; the exchange queues
+  // the Coulomb passes on the side stream after its half-transform.
   const int64_t nocc = occupied_ct(h, Xd, Sd, Dp, n, n_eff, 0.5, false, false, Ct, s);
   prof_mark(h, 1, s);
-  exchange_nonrel(h, Ct, n, false, nocc, K, s, true);
-  coulomb_pass2_release(h, s);  // no-op unless the exchange had nothing to transform
+  exchange_nonrel(h, Ct, n, false, nocc, K, s, Dp, J);
   prof_mark(h, 3, s);
   coulomb_join(h, s);
   fock_combine(Fd, hd, J, K, n2, s);
@@ -209,9 +272,10 @@ void jk_occupied(rr_ri_store* h, const double* C, int64_t nocc, double* Jout, do
   const bool host = !o || o->mem == RR_MEM_HOST;
   cudaStream_t s = call_stream(h, o);
   const int64_t pitch = round_up(std::max<int64_t>(n2, 2), 32);
-  double *Dp, *Cd, *J, *K;
+  double *Dp, *Cd, *J, *K, *Ctj;
   Arena ar(&h->mats);
   ar.request(&Dp, pitch);
+  ar.request(&Ctj, std::max<int64_t>(nocc, 1) * n);
   if (host) {
     ar.request(&Cd, n * nocc);
     ar.request(&J, n2);
@@ -227,10 +291,9 @@ void jk_occupied(rr_ri_store* h, const double* C, int64_t nocc, double* Jout, do
   } else {
     RR_CUDA(cudaMemsetAsync(Dp, 0, sizeof(double) * n2, s));
   }
-  coulomb_split_async(h, Dp, J, s);
   prof_mark(h, 1, s);
-  exchange_nonrel(h, Cd, nocc, true, nocc, K, s, true);
-  coulomb_pass2_release(h, s);
+  transpose(Ctj, Cd, n, nocc, s);  // c_t = C^T, row-major nocc x n
+  exchange_nonrel(h, Ctj, n, false, nocc, K, s, Dp, J);
   prof_mark(h, 3, s);
   coulomb_join(h, s);
   if (host) {

@@ -24,6 +24,7 @@ struct P1 {
   int64_t items;
   double* gpart;
   int* err;
+  const int* skip;
 };
 
 struct P2 {
@@ -60,6 +61,7 @@ __device__ __forceinline__ void decode1(const P1& p, int64_t it, int& tau, int64
 }
 
 __global__ void __launch_bounds__(THREADS) j_pass1_kernel(const P1 p) {
+  if (p.skip && *p.skip) return;
   extern __shared__ __align__(128) unsigned char sm[];
   double* ring = reinterpret_cast<double*>(sm);
   uint64_t* full = reinterpret_cast<uint64_t*>(sm + NST * CW * 8);
@@ -285,7 +287,7 @@ JPlan j_plan(int ntens, const JTensor* t, int64_t naux, int ctas_per_sm) {
   return pl;
 }
 
-void j_pass1(const JPlan& pl, double* gpart, int* err, cudaStream_t s) {
+void j_pass1(const JPlan& pl, double* gpart, int* err, cudaStream_t s, const int* skip) {
   if (pl.naux == 0) return;
   set_smem_attr();
   P1 p{};
@@ -301,6 +303,7 @@ void j_pass1(const JPlan& pl, double* gpart, int* err, cudaStream_t s) {
   p.items = pl.naux * p.segtot;
   p.gpart = gpart;
   p.err = err;
+  p.skip = skip;
   j_pass1_kernel<<<grid_size(p.items, pl.ctas_per_sm), THREADS, SMEM, s>>>(p);
   RR_LAUNCH_CHECK();
 }

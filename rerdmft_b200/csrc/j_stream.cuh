@@ -32,7 +32,9 @@ struct JPlan {
 JPlan j_plan(int ntens, const JTensor* t, int64_t naux, int ctas_per_sm = 3);
 
 // gpart: plan.gpart_doubles scratch; jpart: plan.jpart_doubles scratch; err: device status word.
-void j_pass1(const JPlan& plan, double* gpart, int* err, cudaStream_t s);
+// skip (device int, may be null): when *skip != 0 at launch time the pass does nothing (the
+// gamma partials were produced another way, decided on the device).
+void j_pass1(const JPlan& plan, double* gpart, int* err, cudaStream_t s, const int* skip = nullptr);
 void j_pass2(const JPlan& plan, const double* gpart, double* jpart, int* err, cudaStream_t s);
 // J[t][k] = scale * sum_r jpart[r][t][k]   (fixed order over r)
 void j_finish(const JPlan& plan, const double* jpart, double scale, cudaStream_t s);

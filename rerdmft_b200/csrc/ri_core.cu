@@ -97,6 +97,14 @@ __global__ void fock_combine_kernel(double* F, const double* h, const double* J,
     F[i] = h[i] + J[i] - K[i];
 }
 
+__global__ void transpose_kernel(double* out, const double* in, int64_t rows, int64_t cols) {
+  for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < rows * cols;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t i = idx / cols, j = idx % cols;
+    out[j * rows + i] = in[idx];
+  }
+}
+
 int blocks_for(int64_t n) { return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 1184))); }
 
 }  // namespace
@@ -104,6 +112,12 @@ int blocks_for(int64_t n) { return static_cast<int>(std::max<int64_t>(1, std::mi
 void axpby(double* y, const double* x, double a, double b, int64_t n, cudaStream_t s) {
   if (n <= 0) return;
   axpby_kernel<<<blocks_for(n), 256, 0, s>>>(y, x, a, b, n);
+  RR_LAUNCH_CHECK();
+}
+
+void transpose(double* out, const double* in, int64_t rows, int64_t cols, cudaStream_t s) {
+  if (rows * cols <= 0) return;
+  transpose_kernel<<<blocks_for(rows * cols), 256, 0, s>>>(out, in, rows, cols);
   RR_LAUNCH_CHECK();
 }
 

@@ -26,11 +26,6 @@ struct rr_ri_store {
   bool mixed_ready = false;
   // Profiling events: 0 start, 1 recovery done, 2 half-transform done, 3 exchange done, 4 end
   // (main stream); 5 J start, 6 J end (side stream).
-  // Coulomb pass 2 waiting for the half-transform (see coulomb_split_async).
-  rr::JPlan pending_pass2;
-  double* pending_gpart = nullptr;
-  double* pending_jpart = nullptr;
-  bool has_pending_pass2 = false;
   bool profiling = false;
   cudaEvent_t ev[8] = {};
   bool ev_used[8] = {};
@@ -72,6 +67,8 @@ void copy_in_padded(double* dst, int64_t pitch, const double* src, int64_t n2, b
 
 // Elementwise helpers (device).
 void axpby(double* y, const double* x, double a, double b, int64_t n, cudaStream_t s);  // y = a x + b y
+// out (cols x rows) = in^T for a real row-major rows x cols matrix.
+void transpose(double* out, const double* in, int64_t rows, int64_t cols, cudaStream_t s);
 // F = h + J - K (real, n2 entries).
 void fock_combine(double* F, const double* h, const double* J, const double* K, int64_t n2, cudaStream_t s);
 // Symmetric eigensolver (cuSOLVER dsyevd) in place on a (n x n) row-major symmetric matrix:
