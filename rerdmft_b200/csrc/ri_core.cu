@@ -24,7 +24,11 @@ void Context::init(cudaStream_t user_stream) {
     RR_CUDA(cudaStreamCreateWithFlags(&main, cudaStreamNonBlocking));
     own_main = true;
   }
-  RR_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+  // The side stream carries the bandwidth-bound Coulomb passes that run alongside compute-bound
+  // GEMMs on the main stream; its higher priority lets their CTAs be dispatched as GEMM CTAs retire.
+  int lo = 0, hi = 0;
+  RR_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+  RR_CUDA(cudaStreamCreateWithPriority(&side, cudaStreamNonBlocking, hi));
   RR_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
   RR_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
   RR_SOLVER(cusolverDnCreate(&solver));
