@@ -30,7 +30,8 @@ void density_from_occupied(double* Dp, const double* C, int64_t n, int64_t nocc,
 
 // Exchange K' = sum_P (Ct B^P)^T (Ct B^P) for a given Ct (nocc x n, row-major with leading
 // dimension ldct, or its transpose when ct_transposed: Ct = C^T with C stored n x nocc).
-void coulomb_after_ht(rr_ri_store* h, const double* Dp, const double* Ct, int64_t nocc, double* J, cudaStream_t s);
+void coulomb_after_ht(rr_ri_store* h, const double* Dp, const double* Ct, int64_t nocc, double* J,
+                      const double* tgam, int tseg, cudaStream_t s);
 
 // With Dp given, the Coulomb matrix J (from the pitched density Dp) is queued on the side stream
 // right after the half-transform (coulomb_after_ht) and lands in Jout; join with coulomb_join.
@@ -40,7 +41,7 @@ void exchange_nonrel(rr_ri_store* h, const double* Ct, int64_t ldct, bool ct_tra
   const int64_t n = h->n, naux = h->naux;
   if (nocc == 0 || naux == 0) {
     RR_CUDA(cudaMemsetAsync(K, 0, sizeof(double) * n * n, s));
-    if (Dp) coulomb_after_ht(h, Dp, Ct, 0, Jout, s);
+    if (Dp) coulomb_after_ht(h, Dp, Ct, 0, Jout, nullptr, 0, s);
     return;
   }
   h->T.ensure(static_cast<size_t>(naux * nocc * n));
@@ -50,12 +51,22 @@ void exchange_nonrel(rr_ri_store* h, const double* Ct, int64_t ldct, bool ct_tra
   ht.B = h->B[0].p; ht.ldb = n; ht.opB = Op::N; ht.strideB = h->pitch[0];
   ht.C = h->T.p; ht.ldc = n; ht.strideC = nocc * n;
   ht.batch = naux;
+  double* tgam = nullptr;
+  int tseg = 0;
+  if (Dp) {
+    // gamma partials from the half-transform epilogue: 2 * sum T[P] . Ct per output tile
+    RR_REQUIRE(!ct_transposed && ldct == n, RR_ERR_STATE, "exchange_nonrel: Coulomb from T needs row-major c_t");
+    tseg = static_cast<int>(gemm_tiles_per_batch(ht));
+    h->tgam.ensure(static_cast<size_t>(std::max<int64_t>(naux * tseg, 1)));
+    tgam = h->tgam.p;
+    ht.edot_E = Ct;
+    ht.edot_ld = n;
+    ht.edot_scale = 2.0;
+    ht.edot_out = tgam;
+  }
   gemm(ht, s);
   prof_mark(h, 2, s);
-  if (Dp) {
-    RR_REQUIRE(!ct_transposed && ldct == n, RR_ERR_STATE, "exchange_nonrel: Coulomb from T needs row-major c_t");
-    coulomb_after_ht(h, Dp, Ct, nocc, Jout, s);
-  }
+  if (Dp) coulomb_after_ht(h, Dp, Ct, nocc, Jout, tgam, tseg, s);
 
   GemmDesc sk;
   sk.M = n; sk.N = n; sk.K = naux * nocc;
@@ -119,12 +130,16 @@ void coulomb_async_multi(rr_ri_store* h, int ntens, const double* const* Dp, dou
 
 namespace {
 
-// flag[0] = 1 when max |D - Drec| <= 1e-13 * max(1, max |D|), i.e. the density equals 2 C C^T of
-// the recovered occupied orbitals (an idempotent density inside span(X)).  One CTA.
-__global__ void density_match_kernel(const double* D, const double* Drec, int64_t n2, int* flag) {
+__device__ __forceinline__ void atomic_max_pos(double* addr, double v) {
+  atomicMax(reinterpret_cast<unsigned long long*>(addr), static_cast<unsigned long long>(__double_as_longlong(v)));
+}
+
+// m[0] = max |D - Drec|, m[1] = max |D| (m zeroed by the caller).
+__global__ void density_diff_kernel(const double* D, const double* Drec, int64_t n2, double* m) {
   __shared__ double r0[32], r1[32];
   double md = 0.0, mx = 0.0;
-  for (int64_t i = threadIdx.x; i < n2; i += blockDim.x) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n2;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     md = fmax(md, fabs(D[i] - Drec[i]));
     mx = fmax(mx, fabs(D[i]));
   }
@@ -137,44 +152,24 @@ __global__ void density_match_kernel(const double* D, const double* Drec, int64_
   if (threadIdx.x == 0) {
     double a = 0.0, b = 0.0;
     for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) { a = fmax(a, r0[w]); b = fmax(b, r1[w]); }
-    flag[0] = a <= 1e-13 * fmax(1.0, b) ? 1 : 0;
+    atomic_max_pos(m, a);
+    atomic_max_pos(m + 1, b);
   }
 }
 
-// gamma_P = sum_mn B^P_mn D_mn = 2 sum_{i,a} T[P](i, a) Ct(i, a) when D = 2 Ct^T Ct (T[P] = Ct B^P):
-// the Coulomb pass 1 from the 40x smaller half-transformed tensor.  One CTA per P; runs only when
-// flag[0] is set, writing segment 0 of gpart (the other segments zero).
-__global__ void gamma_from_t_kernel(const double* T, const double* Ct, int64_t nocc, int64_t n, int64_t naux,
-                                    int segtot, double* gpart, const int* flag) {
-  if (!flag[0]) return;
-  __shared__ double red[32];
-  for (int64_t P = blockIdx.x; P < naux; P += gridDim.x) {
-    const double* tp = T + P * nocc * n;
-    double acc = 0.0;
-    for (int64_t e = threadIdx.x; e < nocc * n; e += blockDim.x) acc = fma(tp[e], Ct[e], acc);
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double t = 0.0;
-      for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) t += red[w];
-      gpart[P * segtot] = 2.0 * t;
-      for (int sgi = 1; sgi < segtot; ++sgi) gpart[P * segtot + sgi] = 0.0;
-    }
-    __syncthreads();
-  }
-}
+// flag = 1 when the density equals 2 C C^T of the recovered orbitals to 1e-13 relative.
+__global__ void density_flag_kernel(const double* m, int* flag) { flag[0] = m[0] <= 1e-13 * fmax(1.0, m[1]) ? 1 : 0; }
 
 }  // namespace
 
-// Coulomb for the nonrelativistic build, queued on the side stream once the half-transform is
-// done (event `mid` on s), overlapping the compute-bound SYRK:
-//   - if D = 2 C C^T for the recovered orbitals C (checked on the device), gamma comes from the
-//     half-transformed tensor T (205 MB at n=400/naux=1600/nocc=40) instead of B (2 GB);
-//   - otherwise pass 1 streams B (the kernel is launched either way and exits when not needed);
-//   - pass 2 (J = B^T gamma) streams B once.
-// Ct: nocc x n (leading dim n) c_t rows the half-transform used; T: its output.
-void coulomb_after_ht(rr_ri_store* h, const double* Dp, const double* Ct, int64_t nocc, double* J, cudaStream_t s) {
+// Coulomb for the nonrelativistic build.  The half-transform GEMM already produced, in its
+// epilogue, gamma partials from T:  gamma_P = sum_mn B^P_mn D_mn = 2 sum_{i,a} T[P](i,a) Ct(i,a)
+// whenever D = 2 Ct^T Ct.  Here, on the side stream after the half-transform (event `mid`), that
+// identity is checked on the device (Drec = 2 Ct^T Ct vs D); pass 1 streams B only when it fails
+// (the kernel is launched either way and exits at once when not needed); pass 2 streams B once,
+// overlapping the compute-bound SYRK.  tgam: naux * tseg partials from the half-transform.
+void coulomb_after_ht(rr_ri_store* h, const double* Dp, const double* Ct, int64_t nocc, double* J,
+                      const double* tgam, int tseg, cudaStream_t s) {
   const int64_t n = h->n, naux = h->naux, n2 = n * n;
   JTensor t;
   t.B = h->B[0].p;
@@ -183,34 +178,35 @@ void coulomb_after_ht(rr_ri_store* h, const double* Dp, const double* Ct, int64_
   t.D = Dp;
   t.J = J;
   JPlan pl = j_plan(1, &t, naux, 1);
-  const int segtot = pl.nseg[0];
   const int64_t goff = round_up(pl.gpart_doubles, 32), joff = goff + round_up(pl.jpart_doubles, 32);
-  h->jscr.ensure(static_cast<size_t>(joff + round_up(n2, 32) + 64));
+  const int64_t toff = joff + round_up(n2, 32);
+  h->jscr.ensure(static_cast<size_t>(toff + 64));
   double* gpart = h->jscr.p;
   double* jpart = h->jscr.p + goff;
   double* Drec = h->jscr.p + joff;
-  int* flag = reinterpret_cast<int*>(h->jscr.p + joff + round_up(n2, 32));
+  double* mm = h->jscr.p + toff;
+  int* flag = reinterpret_cast<int*>(mm + 4);
   auto& c = h->ctx;
   if (!c.mid) RR_CUDA(cudaEventCreateWithFlags(&c.mid, cudaEventDisableTiming));
   RR_CUDA(cudaEventRecord(c.mid, s));
   RR_CUDA(cudaStreamWaitEvent(c.side, c.mid, 0));
   prof_mark(h, 5, c.side);
-  if (nocc > 0 && naux > 0) {
+  if (nocc > 0 && naux > 0 && tgam) {
     GemmDesc g;  // Drec = 2 Ct^T Ct
     g.M = n; g.N = n; g.K = nocc;
     g.A = Ct; g.lda = n; g.opA = Op::T;
     g.B = Ct; g.ldb = n; g.C = Drec; g.ldc = n; g.alpha = 2.0;
     gemm(g, c.side);
-    density_match_kernel<<<1, 1024, 0, c.side>>>(Dp, Drec, n2, flag);
+    RR_CUDA(cudaMemsetAsync(mm, 0, 2 * sizeof(double), c.side));
+    density_diff_kernel<<<static_cast<int>(std::min<int64_t>((n2 + 255) / 256, 296)), 256, 0, c.side>>>(Dp, Drec, n2, mm);
     RR_LAUNCH_CHECK();
-    gamma_from_t_kernel<<<static_cast<int>(std::min<int64_t>(naux, 1184)), 256, 0, c.side>>>(h->T.p, Ct, nocc, n, naux,
-                                                                                           segtot, gpart, flag);
+    density_flag_kernel<<<1, 1, 0, c.side>>>(mm, flag);
     RR_LAUNCH_CHECK();
   } else {
     RR_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), c.side));
   }
   j_pass1(pl, gpart, h->status.p, c.side, flag);
-  j_pass2(pl, gpart, jpart, h->status.p, c.side);
+  j_pass2(pl, gpart, jpart, h->status.p, c.side, tgam, tseg, flag);
   j_finish(pl, jpart, 1.0, c.side);
   prof_mark(h, 6, c.side);
   RR_CUDA(cudaEventRecord(c.join, c.side));

@@ -26,6 +26,10 @@ struct Params {
   double signA, signB;  // -1 conjugates the imaginary plane of A / B
   int64_t c_plane_rows, c_plane_stride;
   int upper_only;
+  const double* eE;
+  int64_t eld;
+  double escale;
+  double* eout;
 };
 
 __device__ __forceinline__ void cp_async8(uint32_t saddr, const void* g, int bytes) {
@@ -60,7 +64,7 @@ struct Cfg {
 
 // A tile: AK (A stored M x K, k contiguous) -> smem [BM][A_LD]; else (stored K x M) -> [KT][A_LD].
 // B tile: BKM (B stored N x K) -> smem [BN][B_LD]; else (stored K x N) -> [KT][B_LD].
-template <int MT, int NT, int WM, int WN, bool AK, bool BKM, bool CPLX, int V>
+template <int MT, int NT, int WM, int WN, bool AK, bool BKM, bool CPLX, int V, bool EDOT = false>
 __global__ void __launch_bounds__(32 * WM * WN) dgemm_kernel(const Params p) {
   using CF = Cfg<MT, NT, WM, WN, AK, BKM, CPLX>;
   constexpr int BM = CF::BM, BN = CF::BN, THREADS = CF::THREADS, PL = CF::PL;
@@ -195,6 +199,7 @@ __global__ void __launch_bounds__(32 * WM * WN) dgemm_kernel(const Params p) {
   }
   cp_async_wait<0>();
 
+  double edot = 0.0;
 #pragma unroll
   for (int i = 0; i < MT; ++i)
 #pragma unroll
@@ -204,6 +209,7 @@ __global__ void __launch_bounds__(32 * WM * WN) dgemm_kernel(const Params p) {
         const int64_t row = m0 + wm * MT * 8 + i * 8 + g;
         const int64_t col = n0 + wn * NT * 8 + j * 8 + 2 * t + e;
         if (row >= p.M || col >= p.N) continue;
+        if constexpr (EDOT) edot = fma(p.alpha * acc[i][j][0][e], __ldg(p.eE + row * p.eld + col), edot);
         if (p.splits > 1) {
           double* w = p.work + ((bz * p.M + row) * p.N + col) * PL;
 #pragma unroll
@@ -219,6 +225,17 @@ __global__ void __launch_bounds__(32 * WM * WN) dgemm_kernel(const Params p) {
           }
         }
       }
+  if constexpr (EDOT) {
+    __syncthreads();  // main loop done with the shared ring: reuse it for the reduction
+    for (int o = 16; o > 0; o >>= 1) edot += __shfl_xor_sync(0xffffffffu, edot, o);
+    if (lane == 0) smem[warp] = edot;
+    __syncthreads();
+    if (tid == 0) {
+      double tsum = 0.0;
+      for (int w = 0; w < THREADS / 32; ++w) tsum += smem[w];
+      p.eout[b * (gridDim.x * gridDim.y) + blockIdx.y * gridDim.x + blockIdx.x] = p.escale * tsum;
+    }
+  }
 }
 
 // Fixed-order split-K reduction: C = alpha * sum_s work[b, s] + beta * C.
@@ -280,10 +297,10 @@ int num_sms() {
   return sms;
 }
 
-template <int MT, int NT, int WM, int WN, bool AK, bool BKM, bool CPLX, int V>
+template <int MT, int NT, int WM, int WN, bool AK, bool BKM, bool CPLX, int V, bool EDOT = false>
 void launch_cfg_v(const Params& p, dim3 grid, cudaStream_t s) {
   using CF = Cfg<MT, NT, WM, WN, AK, BKM, CPLX>;
-  auto kern = dgemm_kernel<MT, NT, WM, WN, AK, BKM, CPLX, V>;
+  auto kern = dgemm_kernel<MT, NT, WM, WN, AK, BKM, CPLX, V, EDOT>;
   static bool attr = false;
   if (!attr) {
     RR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, CF::SMEM_BYTES));
@@ -304,6 +321,12 @@ bool vec2_ok(const Params& p, bool AK, bool BKM) {
 
 template <int MT, int NT, int WM, int WN, bool AK, bool BKM, bool CPLX>
 void launch_cfg(const Params& p, dim3 grid, cudaStream_t s) {
+  if constexpr (!CPLX && AK && !BKM) {  // the half-transform layout is the only one with an epilogue dot
+    if (p.eout) {
+      if (vec2_ok(p, AK, BKM)) return launch_cfg_v<MT, NT, WM, WN, AK, BKM, CPLX, 2, true>(p, grid, s);
+      return launch_cfg_v<MT, NT, WM, WN, AK, BKM, CPLX, 1, true>(p, grid, s);
+    }
+  }
   if constexpr (!CPLX) {
     if (vec2_ok(p, AK, BKM)) return launch_cfg_v<MT, NT, WM, WN, AK, BKM, CPLX, 2>(p, grid, s);
   }
@@ -357,6 +380,11 @@ int pick_splits(const GemmDesc& d, Shape sh, int64_t* kchunk) {
 
 }  // namespace
 
+int64_t gemm_tiles_per_batch(const GemmDesc& d) {
+  const Shape sh = pick_shape(d);
+  return static_cast<int64_t>(ceil_div(d.N, sh.bn)) * ceil_div(d.M, sh.bm);
+}
+
 int64_t gemm_work_doubles(const GemmDesc& d) {
   int64_t kc;
   const int s = pick_splits(d, pick_shape(d), &kc);
@@ -379,6 +407,15 @@ void gemm(const GemmDesc& d, cudaStream_t stream, double* work, int64_t work_cap
   p.signB = d.conjB ? -1.0 : 1.0;
   p.c_plane_rows = d.c_plane_rows; p.c_plane_stride = d.c_plane_stride;
   p.upper_only = d.mirror != 0;
+  p.eE = d.edot_E;
+  p.eld = d.edot_ld;
+  p.escale = d.edot_scale;
+  p.eout = d.edot_out;
+  if (d.edot_out) {
+    RR_REQUIRE(!d.cplx && d.opA == Op::N && d.opB == Op::N && d.c_plane_rows == 0 && !d.mirror, RR_ERR_ARG,
+               "gemm: epilogue dot supports the real N,N layout only");
+    work = nullptr;  // one K range per CTA
+  }
   int64_t kc = d.K;
   int splits = 1;
   if (work && d.K > 0) {

@@ -34,7 +34,17 @@ struct GemmDesc {
   // lower triangle from the upper one: +1 C[i][j] = C[j][i] (Hermitian conj for cplx),
   // -1 C[i][j] = -C[j][i].  0 = full output.  Requires M == N.
   int mirror = 0;
+  // Epilogue dot (real, no split-K): per output tile also
+  //   edot_out[b * tiles + tile] = edot_scale * sum_{(m,n) in tile} C[b](m, n) * edot_E[m * edot_ld + n]
+  // with tiles = (output tile columns) x (output tile rows), tile = ty * tiles_x + tx.
+  const double* edot_E = nullptr;
+  int64_t edot_ld = 0;
+  double edot_scale = 1.0;
+  double* edot_out = nullptr;
 };
+
+// Output tiles per batch entry gemm() uses for this descriptor (size of an edot segment).
+int64_t gemm_tiles_per_batch(const GemmDesc& d);
 
 // Launches the GEMM on `stream`.  `work` (capacity `work_cap` doubles) is split-K scratch: when
 // the output grid is too small to fill the GPU and work_cap allows, K is split, the partial

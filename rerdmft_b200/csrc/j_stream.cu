@@ -40,6 +40,9 @@ struct P2 {
   const double* gpart;
   double* jpart;
   int* err;
+  const double* alt;
+  int alt_seg;
+  const int* alt_flag;
 };
 
 __device__ __forceinline__ int64_t min64(int64_t a, int64_t b) { return a < b ? a : b; }
@@ -175,6 +178,9 @@ __global__ void __launch_bounds__(THREADS) j_pass2_kernel(const P2 p) {
     return;
   }
   const int ct = threadIdx.x;
+  const bool use_alt = p.alt_flag && *p.alt_flag;
+  const double* gsrc = use_alt ? p.alt : p.gpart;
+  const int gseg = use_alt ? p.alt_seg : p.segtot;
   uint32_t q = 0;
   for (int64_t it = blockIdx.x; it < p.items; it += gridDim.x) {
     int tau;
@@ -189,8 +195,8 @@ __global__ void __launch_bounds__(THREADS) j_pass2_kernel(const P2 p) {
       const int st = q % NST;
       const bool ok = mbar_wait(&full[st], (q / NST) & 1, p.err, ERR_P2_CONS, dead);
       double gam = 0.0;
-      const double* gp = p.gpart + P * p.segtot;
-      for (int s = 0; s < p.segtot; ++s) gam += __ldg(gp + s);
+      const double* gp = gsrc + P * gseg;
+      for (int s = 0; s < gseg; ++s) gam += __ldg(gp + s);
       const double2* sb = reinterpret_cast<const double2*>(ring + st * CW);
       if (ok) {
 #pragma unroll
@@ -308,7 +314,8 @@ void j_pass1(const JPlan& pl, double* gpart, int* err, cudaStream_t s, const int
   RR_LAUNCH_CHECK();
 }
 
-void j_pass2(const JPlan& pl, const double* gpart, double* jpart, int* err, cudaStream_t s) {
+void j_pass2(const JPlan& pl, const double* gpart, double* jpart, int* err, cudaStream_t s, const double* alt,
+             int alt_seg, const int* alt_flag) {
   if (pl.naux == 0) return;
   set_smem_attr();
   P2 p{};
@@ -326,6 +333,9 @@ void j_pass2(const JPlan& pl, const double* gpart, double* jpart, int* err, cuda
   p.gpart = gpart;
   p.jpart = jpart;
   p.err = err;
+  p.alt = alt;
+  p.alt_seg = alt_seg;
+  p.alt_flag = alt_flag;
   j_pass2_kernel<<<grid_size(p.items, pl.ctas_per_sm), THREADS, SMEM, s>>>(p);
   RR_LAUNCH_CHECK();
 }

@@ -35,7 +35,10 @@ JPlan j_plan(int ntens, const JTensor* t, int64_t naux, int ctas_per_sm = 3);
 // skip (device int, may be null): when *skip != 0 at launch time the pass does nothing (the
 // gamma partials were produced another way, decided on the device).
 void j_pass1(const JPlan& plan, double* gpart, int* err, cudaStream_t s, const int* skip = nullptr);
-void j_pass2(const JPlan& plan, const double* gpart, double* jpart, int* err, cudaStream_t s);
+// alt / alt_seg / alt_flag (optional): when *alt_flag != 0 at run time, gamma_P is summed from
+// alt[P * alt_seg ...] instead of gpart.
+void j_pass2(const JPlan& plan, const double* gpart, double* jpart, int* err, cudaStream_t s,
+             const double* alt = nullptr, int alt_seg = 0, const int* alt_flag = nullptr);
 // J[t][k] = scale * sum_r jpart[r][t][k]   (fixed order over r)
 void j_finish(const JPlan& plan, const double* jpart, double scale, cudaStream_t s);
 

@@ -105,61 +105,58 @@ __global__ void fill_test_matrix_kernel(double* G, int64_t count) {
   }
 }
 
-constexpr int SC_THREADS = 512;
-
 // Cholesky M = L L^dagger of a small Hermitian positive-definite r x r matrix (row-major,
-// interleaved when PL = 2), one CTA, right-looking with the whole block on each trailing update.
-// `work` holds the r x r factor (shared memory when it fits, else global scratch).  Output:
-// out = L^{-dagger} (want_inverse) or L (upper triangle zero), r x r row-major, so that
+// interleaved when PL = 2) by ONE warp: right-looking, lanes split each trailing update, only warp
+// barriers.  `work` holds the r x r factor (shared memory when it fits, else global scratch).
+// Output: out = L^{-dagger} (want_inverse) or L (upper triangle zero), r x r row-major, so that
 // Y <- Y out is a plain GEMM.  status[0] |= 1 on a non-positive pivot.
 template <int PL>
-__global__ void __launch_bounds__(SC_THREADS) chol_small_kernel(const double* M, int64_t r, double* out,
-                                                                double* gwork, int want_inverse, int* status) {
+__global__ void __launch_bounds__(32) chol_small_kernel(const double* M, int64_t r, double* out, double* gwork,
+                                                        int want_inverse, int* status) {
   extern __shared__ double sm[];
   double* L = gwork ? gwork : sm;
-  const int tid = threadIdx.x;
-  for (int64_t i = tid; i < r * r * PL; i += SC_THREADS) L[i] = M[i];
-  __syncthreads();
+  const int lane = threadIdx.x;
+  for (int64_t i = lane; i < r * r * PL; i += 32) L[i] = M[i];
+  __syncwarp();
   for (int64_t j = 0; j < r; ++j) {
     double d = L[(j * r + j) * PL];
     if (!(d > 0.0)) {
-      if (tid == 0) atomicOr(status, 1);
+      if (lane == 0) atomicOr(status, 1);
       d = 1e-300;
     }
-    const double ljj = sqrt(d);
-    __syncthreads();
-    for (int64_t i = j + 1 + tid; i < r; i += SC_THREADS) {
-      L[(i * r + j) * PL] /= ljj;
-      if (PL == 2) L[(i * r + j) * PL + 1] /= ljj;
+    const double inv = 1.0 / sqrt(d);
+    __syncwarp();
+    for (int64_t i = j + 1 + lane; i < r; i += 32) {
+      L[(i * r + j) * PL] *= inv;
+      if (PL == 2) L[(i * r + j) * PL + 1] *= inv;
     }
-    if (tid == 0) {
-      L[(j * r + j) * PL] = ljj;
+    if (lane == 0) {
+      L[(j * r + j) * PL] = sqrt(d);
       if (PL == 2) L[(j * r + j) * PL + 1] = 0.0;
     }
-    __syncthreads();
-    // trailing update of the lower triangle: A[i][k] -= L[i][j] conj(L[k][j]), j < k <= i
-    const int64_t m = r - j - 1;
-    for (int64_t e = tid; e < m * m; e += SC_THREADS) {
-      const int64_t i = j + 1 + e / m, k = j + 1 + e % m;
-      if (k > i) continue;
+    __syncwarp();
+    // trailing lower triangle: A[i][k] -= L[i][j] conj(L[k][j]), j < k <= i; lane owns rows i
+    for (int64_t i = j + 1 + lane; i < r; i += 32) {
       const double ar = L[(i * r + j) * PL], ai = PL == 2 ? L[(i * r + j) * PL + 1] : 0.0;
-      const double br = L[(k * r + j) * PL], bi = PL == 2 ? L[(k * r + j) * PL + 1] : 0.0;
-      L[(i * r + k) * PL] -= ar * br + ai * bi;
-      if (PL == 2) L[(i * r + k) * PL + 1] -= ai * br - ar * bi;
+      for (int64_t k = j + 1; k <= i; ++k) {
+        const double br = L[(k * r + j) * PL], bi = PL == 2 ? L[(k * r + j) * PL + 1] : 0.0;
+        L[(i * r + k) * PL] -= ar * br + ai * bi;
+        if (PL == 2) L[(i * r + k) * PL + 1] -= ai * br - ar * bi;
+      }
     }
-    __syncthreads();
+    __syncwarp();
   }
   if (!want_inverse) {
-    for (int64_t e = tid; e < r * r; e += SC_THREADS) {
+    for (int64_t e = lane; e < r * r; e += 32) {
       const int64_t i = e / r, k = e % r;
       out[e * PL] = k <= i ? L[e * PL] : 0.0;
       if (PL == 2) out[e * PL + 1] = k <= i ? L[e * PL + 1] : 0.0;
     }
     return;
   }
-  // Column c of L^{-1}: forward substitution on e_c, one thread per column; written as row c of
+  // Column c of L^{-1}: forward substitution on e_c, one lane per column; written as row c of
   // out = (L^{-1})^dagger, i.e. out[c][i] = conj(Linv[i][c]).
-  for (int64_t c = tid; c < r; c += SC_THREADS) {
+  for (int64_t c = lane; c < r; c += 32) {
     double* o = out + c * r * PL;
     for (int64_t i = 0; i < c; ++i) {
       o[i * PL] = 0.0;
@@ -295,11 +292,11 @@ int64_t occupied_ct(rr_ri_store* h, const double* X, const double* S, const doub
     if (cplx) {
       auto k = chol_small_kernel<2>;
       if (sm > 48 * 1024) RR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
-      k<<<1, SC_THREADS, sm, s>>>(mat, r, Wt, chol_in_smem ? nullptr : gw, inverse, h->status.p + 1);
+      k<<<1, 32, sm, s>>>(mat, r, Wt, chol_in_smem ? nullptr : gw, inverse, h->status.p + 1);
     } else {
       auto k = chol_small_kernel<1>;
       if (sm > 48 * 1024) RR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
-      k<<<1, SC_THREADS, sm, s>>>(mat, r, Wt, chol_in_smem ? nullptr : gw, inverse, h->status.p + 1);
+      k<<<1, 32, sm, s>>>(mat, r, Wt, chol_in_smem ? nullptr : gw, inverse, h->status.p + 1);
     }
     RR_LAUNCH_CHECK();
   };

@@ -17,6 +17,7 @@ struct rr_ri_store {
   rr::DevBuf<double> T;     // half-transformed exchange intermediate
   rr::DevBuf<double> work;  // split-K partial products
   rr::DevBuf<double> jscr;  // J pass-1/pass-2 partial sums
+  rr::DevBuf<double> tgam;  // gamma partials from the half-transform epilogue
   rr::DevBuf<double> solver_a;  // eigen-problem matrix / eigenvectors
   rr::DevBuf<double> solver_w;  // eigenvalues
   std::vector<double> host_w;
