@@ -166,8 +166,9 @@ __global__ void density_flag_kernel(const double* m, int* flag) { flag[0] = m[0]
 // epilogue, gamma partials from T:  gamma_P = sum_mn B^P_mn D_mn = 2 sum_{i,a} T[P](i,a) Ct(i,a)
 // whenever D = 2 Ct^T Ct.  Here, on the side stream after the half-transform (event `mid`), that
 // identity is checked on the device (Drec = 2 Ct^T Ct vs D); pass 1 streams B only when it fails
-// (the kernel is launched either way and exits at once when not needed); pass 2 streams B once,
-// overlapping the compute-bound SYRK.  tgam: naux * tseg partials from the half-transform.
+// (the kernel is launched either way and exits at once when not needed); pass 2 streams B once.
+// The passes run on `s` itself with the whole GPU (3 CTAs per SM): measured on B200, sharing the SMs
+// with the SYRK halved both.  tgam: naux * tseg partials from the half-transform.
 void coulomb_after_ht(rr_ri_store* h, const double* Dp, const double* Ct, int64_t nocc, double* J,
                       const double* tgam, int tseg, cudaStream_t s) {
   const int64_t n = h->n, naux = h->naux, n2 = n * n;
@@ -177,7 +178,7 @@ void coulomb_after_ht(rr_ri_store* h, const double* Dp, const double* Ct, int64_
   t.len = n2;
   t.D = Dp;
   t.J = J;
-  JPlan pl = j_plan(1, &t, naux, 1);
+  JPlan pl = j_plan(1, &t, naux, 3);
   const int64_t goff = round_up(pl.gpart_doubles, 32), joff = goff + round_up(pl.jpart_doubles, 32);
   const int64_t toff = joff + round_up(n2, 32);
   h->jscr.ensure(static_cast<size_t>(toff + 64));
@@ -187,29 +188,26 @@ void coulomb_after_ht(rr_ri_store* h, const double* Dp, const double* Ct, int64_
   double* mm = h->jscr.p + toff;
   int* flag = reinterpret_cast<int*>(mm + 4);
   auto& c = h->ctx;
-  if (!c.mid) RR_CUDA(cudaEventCreateWithFlags(&c.mid, cudaEventDisableTiming));
-  RR_CUDA(cudaEventRecord(c.mid, s));
-  RR_CUDA(cudaStreamWaitEvent(c.side, c.mid, 0));
-  prof_mark(h, 5, c.side);
+  prof_mark(h, 5, s);
   if (nocc > 0 && naux > 0 && tgam) {
     GemmDesc g;  // Drec = 2 Ct^T Ct
     g.M = n; g.N = n; g.K = nocc;
     g.A = Ct; g.lda = n; g.opA = Op::T;
     g.B = Ct; g.ldb = n; g.C = Drec; g.ldc = n; g.alpha = 2.0;
-    gemm(g, c.side);
-    RR_CUDA(cudaMemsetAsync(mm, 0, 2 * sizeof(double), c.side));
-    density_diff_kernel<<<static_cast<int>(std::min<int64_t>((n2 + 255) / 256, 296)), 256, 0, c.side>>>(Dp, Drec, n2, mm);
+    gemm(g, s);
+    RR_CUDA(cudaMemsetAsync(mm, 0, 2 * sizeof(double), s));
+    density_diff_kernel<<<static_cast<int>(std::min<int64_t>((n2 + 255) / 256, 296)), 256, 0, s>>>(Dp, Drec, n2, mm);
     RR_LAUNCH_CHECK();
-    density_flag_kernel<<<1, 1, 0, c.side>>>(mm, flag);
+    density_flag_kernel<<<1, 1, 0, s>>>(mm, flag);
     RR_LAUNCH_CHECK();
   } else {
-    RR_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), c.side));
+    RR_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s));
   }
-  j_pass1(pl, gpart, h->status.p, c.side, flag);
-  j_pass2(pl, gpart, jpart, h->status.p, c.side, tgam, tseg, flag);
-  j_finish(pl, jpart, 1.0, c.side);
-  prof_mark(h, 6, c.side);
-  RR_CUDA(cudaEventRecord(c.join, c.side));
+  j_pass1(pl, gpart, h->status.p, s, flag);
+  j_pass2(pl, gpart, jpart, h->status.p, s, tgam, tseg, flag);
+  j_finish(pl, jpart, 1.0, s);
+  prof_mark(h, 6, s);
+  RR_CUDA(cudaEventRecord(c.join, s));  // coulomb_join is then a no-op wait on the same stream
 }
 
 void coulomb_join(rr_ri_store* h, cudaStream_t s) { RR_CUDA(cudaStreamWaitEvent(s, h->ctx.join, 0)); }
