@@ -121,6 +121,59 @@ int rr_ri_fock_rkb(rr_ri_handle h, const double* h_rkb, const double* v_total, i
  * the device-resident SCF loop; equal to rr_ri_fock_nonrel when D = 2 C C^T. */
 int rr_ri_jk_occupied(rr_ri_handle h, const double* C_occ, int64_t n_occ, double* J, double* K, const rr_opts* opts);
 
+/* ---------------- MO-basis RI tensors (functional stage) ---------------- */
+
+typedef struct rr_mo_store* rr_mo_handle;
+
+#define RR_MO_NONREL_SPIN 0 /* RiNonRelSpinMoEri: real spatial tensor (naux, n*n); accessors span 2n spin orbitals */
+#define RR_MO_COMPLEX 1     /* RiMoEri: complex tensor (naux, n*n) over n spinors */
+
+/* buildRiNonRelSpinMoEri(eri3_L, n, C), src/NON_REL/NonRelSpinRiMoEri.cpp:13: B_mo^P = C^T B^P C
+ * with the handle's resident eri3_L; C is n x n (the spatial alpha half of the coefficients). */
+int rr_mo_build_nonrel(rr_ri_handle ri, const double* C, rr_mo_handle* out, const rr_opts* opts);
+
+/* buildRiMoEri(RiDirectEriSource, c_ukb), src/UKB/RiMoEri.cpp:64: B(P,p,q) = sum over the four UKB
+ * blocks of sum conj(c(mu,p)) c(nu,q) (mu nu|P); c_ukb is n_ukb x n_total complex (n_ukb = 2nl+2ns
+ * of a 4-component handle; an X2C handle is the ns = 0 case). */
+int rr_mo_build_ukb(rr_ri_handle ri4c, const double* c_ukb, int64_t n_total, rr_mo_handle* out, const rr_opts* opts);
+
+/* Wraps an existing MO tensor (naux, n*n; kind RR_MO_NONREL_SPIN real or RR_MO_COMPLEX complex). */
+int rr_mo_from_tensor(const double* Bmo, int64_t naux, int64_t n, int32_t kind, int32_t mem, rr_mo_handle* out);
+int rr_mo_destroy(rr_mo_handle m);
+/* naux, n (spatial orbitals for RR_MO_NONREL_SPIN, spinors for RR_MO_COMPLEX) and the kind. */
+int rr_mo_info(rr_mo_handle m, int64_t* naux, int64_t* n, int32_t* kind);
+/* Copies the tensor out (the reference's b()). */
+int rr_mo_copy_tensor(rr_mo_handle m, double* out, const rr_opts* opts);
+
+/* rotated(U): RiNonRelSpinMoEri::rotated (U 2n x 2n real, must be blockdiag(u,u) to 1e-3, the two
+ * blocks are averaged; src/NON_REL/NonRelSpinRiMoEri.cpp:45) or RiMoEri::rotated (U n x n complex,
+ * B' = U^dagger B U; src/UKB/RiMoEri.cpp:88).  A new handle is returned; m is unchanged. */
+int rr_mo_rotated(rr_mo_handle m, const double* U, rr_mo_handle* out, const rr_opts* opts);
+
+/* RiMoEri::positiveBlock(off), src/UKB/RiMoEri.cpp:112: both MO legs restricted to [off, n). */
+int rr_mo_positive_block(rr_mo_handle m, int64_t off, rr_mo_handle* out, const rr_opts* opts);
+
+/* RiNonRelSpinMoEri::embeddedB(), src/NON_REL/NonRelSpinRiMoEri.h:77: (naux, (2n)^2) block-diagonal. */
+int rr_mo_embedded(rr_mo_handle m, double* out, const rr_opts* opts);
+
+/* operator()(a,b,c,d) for `count` index quadruples (abcd: 4*count int64):
+ * sum_P B(P,a,c) B(P,b,d) with the nonrelativistic spin selection rule where it applies
+ * (src/NON_REL/NonRelSpinRiMoEri.h:40, src/UKB/RiMoEri.h:50).  out: count doubles or complex. */
+int rr_mo_eri(rr_mo_handle m, int64_t count, const int64_t* abcd, double* out, const rr_opts* opts);
+
+/* The functional stage's integral reads as whole matrices over the accessor dimension d
+ * (2n or n): J_ij = eri(i,j,i,j), K_ij = eri(i,j,j,i) and, when pair_of (d int64) and L are given,
+ * L_ij = eri(pair_of[i], j, j, pair_of[i]) (src/Occ_opt/PNOFs.cpp:306-321). */
+int rr_mo_jkl(rr_mo_handle m, const int64_t* pair_of, double* J, double* K, double* L, const rr_opts* opts);
+
+/* hartreeExchangeFockMatrix(h, eri, occupations, two_rdm_h, two_rdm_x, pair_of, l1, l2) GEMM form,
+ * src/Hessian_opt/RiGemmFock.cpp:52-184 (riHxFockGemm; the nonrelativistic overload works on
+ * embeddedB).  d = accessor dimension; h and F are d x d (complex for RR_MO_COMPLEX), occupations d,
+ * two_rdm_* real d x d; pair_of may be NULL (no L terms; l1/l2 ignored). */
+int rr_mo_hx_fock(rr_mo_handle m, const double* h, const double* occupations, const double* two_rdm_h,
+                  const double* two_rdm_x, const int64_t* pair_of, const double* two_rdm_l1, const double* two_rdm_l2,
+                  double* F, const rr_opts* opts);
+
 /* Profiling: when on, each call records CUDA events around its phases; rr_ri_get_timings waits
  * for the last call's events and returns the phase times.  Off by default (no event overhead). */
 int rr_ri_set_profiling(rr_ri_handle h, int32_t on);

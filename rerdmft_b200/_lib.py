@@ -12,6 +12,7 @@ LIB_PATH = Path(__file__).resolve().parent / "librr_ri.so"
 RR_OK, RR_ERR_ARG, RR_ERR_CUDA, RR_ERR_SOLVER, RR_ERR_TIMEOUT, RR_ERR_NOMEM, RR_ERR_STATE, RR_ERR_UNSUPPORTED = range(8)
 RR_MEM_HOST, RR_MEM_DEVICE = 0, 1
 RR_PREC_FP64, RR_PREC_MIXED = 0, 1
+RR_MO_NONREL_SPIN, RR_MO_COMPLEX = 0, 1
 
 _i64 = ctypes.c_int64
 _i32 = ctypes.c_int32
@@ -64,6 +65,18 @@ _SIGS = {
     "rr_ri_fock_x2c": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _i64, _vp, ctypes.POINTER(Opts)]),
     "rr_ri_two_electron_ukb": (ctypes.c_int, [_vp, _vp, _vp, _i64, _vp, _vp, ctypes.POINTER(Opts)]),
     "rr_ri_fock_rkb": (ctypes.c_int, [_vp, _vp, _vp, _i64, _vp, _vp, _i64, _vp, _vp, ctypes.POINTER(Opts)]),
+    "rr_mo_build_nonrel": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(_vp), ctypes.POINTER(Opts)]),
+    "rr_mo_build_ukb": (ctypes.c_int, [_vp, _vp, _i64, ctypes.POINTER(_vp), ctypes.POINTER(Opts)]),
+    "rr_mo_from_tensor": (ctypes.c_int, [_vp, _i64, _i64, _i32, _i32, ctypes.POINTER(_vp)]),
+    "rr_mo_destroy": (ctypes.c_int, [_vp]),
+    "rr_mo_info": (ctypes.c_int, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i32)]),
+    "rr_mo_copy_tensor": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(Opts)]),
+    "rr_mo_rotated": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(_vp), ctypes.POINTER(Opts)]),
+    "rr_mo_positive_block": (ctypes.c_int, [_vp, _i64, ctypes.POINTER(_vp), ctypes.POINTER(Opts)]),
+    "rr_mo_embedded": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(Opts)]),
+    "rr_mo_eri": (ctypes.c_int, [_vp, _i64, _vp, _vp, ctypes.POINTER(Opts)]),
+    "rr_mo_jkl": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, ctypes.POINTER(Opts)]),
+    "rr_mo_hx_fock": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(Opts)]),
     "rr_ri_set_profiling": (ctypes.c_int, [_vp, _i32]),
     "rr_ri_get_timings": (ctypes.c_int, [_vp, ctypes.c_void_p]),
     "rr_kernel_launches": (ctypes.c_int64, []),

@@ -2,7 +2,7 @@
 // rr::Error (and any other exception) into a status code plus rr_last_error().
 #include <new>
 
-#include "ri_store.cuh"
+#include "mo_store.cuh"
 
 namespace rr {
 extern thread_local std::string g_last_error;
@@ -46,6 +46,46 @@ void upload_tensor(rr::DevBuf<double>& dst, int64_t* pitch_out, const double* sr
     RR_CUDA(cudaMemcpy2DAsync(dst.p, sizeof(double) * pitch, src, sizeof(double) * n2, sizeof(double) * n2, naux,
                               host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
 }
+
+rr_mo_store* new_mo(int cplx, int64_t naux, int64_t n) {
+  auto* m = new rr_mo_store();
+  try {
+    m->ctx.init(nullptr);
+  } catch (...) {
+    delete m;
+    throw;
+  }
+  m->cplx = cplx;
+  m->naux = naux;
+  m->n = n;
+  return m;
+}
+
+void free_mo(rr_mo_store* m) {
+  if (!m) return;
+  m->ctx.destroy();
+  delete m;
+}
+
+rr_mo_store* checked_mo(rr_mo_handle m) {
+  if (!m) throw rr::Error(RR_ERR_ARG, "null MO handle");
+  RR_CUDA(cudaSetDevice(m->ctx.device));
+  return m;
+}
+
+bool host_mem(const rr_opts* o) { return !o || o->mem == RR_MEM_HOST; }
+
+template <typename F>
+void with_new_mo(rr_mo_handle* out, rr_mo_store* m, F&& f) {
+  try {
+    f();
+  } catch (...) {
+    free_mo(m);
+    throw;
+  }
+  *out = m;
+}
+
 
 rr_ri_store* checked(rr_ri_handle h) {
   if (!h) throw rr::Error(RR_ERR_ARG, "null handle");
@@ -227,6 +267,170 @@ int rr_ri_get_timings(rr_ri_handle h, rr_timings* out) {
 }
 
 int64_t rr_kernel_launches(void) { return rr::launches(); }
+
+// ---------------- MO tensors ----------------
+
+int rr_mo_build_nonrel(rr_ri_handle ri, const double* C, rr_mo_handle* out, const rr_opts* opts) {
+  return api([&] {
+    auto* s = checked(ri);
+    RR_REQUIRE(out && C, RR_ERR_ARG, "rr_mo_build_nonrel: null argument");
+    *out = nullptr;
+    RR_REQUIRE(s->ntens == 1, RR_ERR_STATE, "rr_mo_build_nonrel: needs a single-tensor handle");
+    auto* m = new_mo(0, s->naux, s->n);
+    with_new_mo(out, m, [&] {
+      cudaStream_t st = rr::call_stream(s, opts);
+      rr::mo_build_nonrel(s, C, m, host_mem(opts), st);
+      RR_CUDA(cudaStreamSynchronize(st));
+    });
+  });
+}
+
+int rr_mo_build_ukb(rr_ri_handle ri4c, const double* c_ukb, int64_t n_total, rr_mo_handle* out, const rr_opts* opts) {
+  return api([&] {
+    auto* s = checked(ri4c);
+    RR_REQUIRE(out && (c_ukb || n_total == 0) && n_total >= 0, RR_ERR_ARG, "rr_mo_build_ukb: bad argument");
+    *out = nullptr;
+    RR_REQUIRE(s->ntens == 2, RR_ERR_STATE, "rr_mo_build_ukb: needs a 4-component handle (rr_ri_create_4c)");
+    auto* m = new_mo(1, s->naux, n_total);
+    with_new_mo(out, m, [&] {
+      cudaStream_t st = rr::call_stream(s, opts);
+      rr::mo_build_ukb(s, c_ukb, n_total, m, host_mem(opts), st);
+      RR_CUDA(cudaStreamSynchronize(st));
+    });
+  });
+}
+
+int rr_mo_from_tensor(const double* Bmo, int64_t naux, int64_t n, int32_t kind, int32_t mem, rr_mo_handle* out) {
+  return api([&] {
+    RR_REQUIRE(out && naux >= 0 && n >= 0 && (Bmo || naux * n == 0), RR_ERR_ARG, "rr_mo_from_tensor: bad argument");
+    RR_REQUIRE(kind == RR_MO_NONREL_SPIN || kind == RR_MO_COMPLEX, RR_ERR_ARG, "rr_mo_from_tensor: bad kind");
+    *out = nullptr;
+    auto* m = new_mo(kind == RR_MO_COMPLEX, naux, n);
+    with_new_mo(out, m, [&] {
+      const int64_t cnt = naux * n * n * (kind == RR_MO_COMPLEX ? 2 : 1);
+      m->B.alloc(static_cast<size_t>(std::max<int64_t>(cnt, 1)));
+      rr::copy_in(m->B.p, Bmo, cnt, mem == RR_MEM_HOST, m->ctx.main);
+      RR_CUDA(cudaStreamSynchronize(m->ctx.main));
+    });
+  });
+}
+
+int rr_mo_destroy(rr_mo_handle m) {
+  return api([&] {
+    if (!m) return;
+    cudaSetDevice(m->ctx.device);
+    cudaDeviceSynchronize();
+    free_mo(m);
+  });
+}
+
+int rr_mo_info(rr_mo_handle m, int64_t* naux, int64_t* n, int32_t* kind) {
+  return api([&] {
+    if (!m) throw rr::Error(RR_ERR_ARG, "null MO handle");
+    if (naux) *naux = m->naux;
+    if (n) *n = m->n;
+    if (kind) *kind = m->cplx ? RR_MO_COMPLEX : RR_MO_NONREL_SPIN;
+  });
+}
+
+int rr_mo_copy_tensor(rr_mo_handle m, double* out, const rr_opts* opts) {
+  return api([&] {
+    auto* s = checked_mo(m);
+    RR_REQUIRE(out || s->naux * s->n == 0, RR_ERR_ARG, "rr_mo_copy_tensor: null output");
+    cudaStream_t st = rr::mo_stream(s, opts);
+    rr::copy_out(out, s->B.p, s->naux * s->n * s->n * (s->cplx ? 2 : 1), host_mem(opts), st);
+    RR_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int rr_mo_rotated(rr_mo_handle m, const double* U, rr_mo_handle* out, const rr_opts* opts) {
+  return api([&] {
+    auto* s = checked_mo(m);
+    RR_REQUIRE(out && U, RR_ERR_ARG, "rr_mo_rotated: null argument");
+    *out = nullptr;
+    auto* d = new_mo(s->cplx, s->naux, s->n);
+    with_new_mo(out, d, [&] {
+      cudaStream_t st = rr::mo_stream(s, opts);
+      rr::mo_rotate(s, U, d, host_mem(opts), st);
+      RR_CUDA(cudaStreamSynchronize(st));
+    });
+  });
+}
+
+int rr_mo_positive_block(rr_mo_handle m, int64_t off, rr_mo_handle* out, const rr_opts* opts) {
+  return api([&] {
+    auto* s = checked_mo(m);
+    RR_REQUIRE(out && off >= 0 && off <= s->n, RR_ERR_ARG, "rr_mo_positive_block: bad offset");
+    *out = nullptr;
+    auto* d = new_mo(s->cplx, s->naux, s->n - off);
+    with_new_mo(out, d, [&] {
+      cudaStream_t st = rr::mo_stream(s, opts);
+      rr::mo_positive_block(s, off, d, st);
+      RR_CUDA(cudaStreamSynchronize(st));
+    });
+  });
+}
+
+int rr_mo_embedded(rr_mo_handle m, double* out, const rr_opts* opts) {
+  return api([&] {
+    auto* s = checked_mo(m);
+    RR_REQUIRE(!s->cplx, RR_ERR_STATE, "rr_mo_embedded: only for the nonrelativistic spin-orbital kind");
+    RR_REQUIRE(out || s->naux * s->n == 0, RR_ERR_ARG, "rr_mo_embedded: null output");
+    cudaStream_t st = rr::mo_stream(s, opts);
+    rr::mo_embedded(s, out, host_mem(opts), st);
+    RR_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int rr_mo_eri(rr_mo_handle m, int64_t count, const int64_t* abcd, double* out, const rr_opts* opts) {
+  return api([&] {
+    auto* s = checked_mo(m);
+    RR_REQUIRE(count >= 0 && (count == 0 || (abcd && out)), RR_ERR_ARG, "rr_mo_eri: bad argument");
+    if (host_mem(opts)) {
+      const int64_t dim = s->cplx ? s->n : 2 * s->n;
+      for (int64_t i = 0; i < 4 * count; ++i)
+        RR_REQUIRE(abcd[i] >= 0 && abcd[i] < dim, RR_ERR_ARG, "rr_mo_eri: index out of range");
+    }
+    cudaStream_t st = rr::mo_stream(s, opts);
+    rr::mo_eri(s, count, abcd, out, host_mem(opts), st);
+    RR_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int rr_mo_jkl(rr_mo_handle m, const int64_t* pair_of, double* J, double* K, double* L, const rr_opts* opts) {
+  return api([&] {
+    auto* s = checked_mo(m);
+    RR_REQUIRE(J && K, RR_ERR_ARG, "rr_mo_jkl: null output");
+    RR_REQUIRE(!L || pair_of, RR_ERR_ARG, "rr_mo_jkl: L needs pair_of");
+    if (pair_of && host_mem(opts)) {
+      const int64_t dim = s->cplx ? s->n : 2 * s->n;
+      for (int64_t i = 0; i < dim; ++i)
+        RR_REQUIRE(pair_of[i] >= 0 && pair_of[i] < dim, RR_ERR_ARG, "rr_mo_jkl: pair_of out of range");
+    }
+    cudaStream_t st = rr::mo_stream(s, opts);
+    rr::mo_jkl(s, pair_of, J, K, L, host_mem(opts), st);
+    RR_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int rr_mo_hx_fock(rr_mo_handle m, const double* h, const double* occupations, const double* two_rdm_h,
+                  const double* two_rdm_x, const int64_t* pair_of, const double* two_rdm_l1, const double* two_rdm_l2,
+                  double* F, const rr_opts* opts) {
+  return api([&] {
+    auto* s = checked_mo(m);
+    RR_REQUIRE(h && occupations && two_rdm_h && two_rdm_x && F, RR_ERR_ARG, "rr_mo_hx_fock: null matrix");
+    RR_REQUIRE(!pair_of || (two_rdm_l1 && two_rdm_l2), RR_ERR_ARG,
+               "hartreeExchangeFockMatrix: pair_of/two_rdm_l1/two_rdm_l2 dimensions inconsistent with h");
+    if (pair_of && host_mem(opts)) {
+      const int64_t dim = s->cplx ? s->n : 2 * s->n;
+      for (int64_t i = 0; i < dim; ++i)
+        RR_REQUIRE(pair_of[i] >= 0 && pair_of[i] < dim, RR_ERR_ARG, "rr_mo_hx_fock: pair_of out of range");
+    }
+    cudaStream_t st = rr::mo_stream(s, opts);
+    rr::mo_hx_fock(s, h, occupations, two_rdm_h, two_rdm_x, pair_of, two_rdm_l1, two_rdm_l2, F, host_mem(opts), st);
+    RR_CUDA(cudaStreamSynchronize(st));
+  });
+}
 
 }  // extern "C"
 

@@ -25,6 +25,7 @@ struct Params {
   double* work;
   double signA, signB;  // -1 conjugates the imaginary plane of A / B
   int64_t c_plane_rows, c_plane_stride;
+  int64_t ccs;  // output column stride
   int upper_only;
   const double* eE;
   int64_t eld;
@@ -217,7 +218,7 @@ __global__ void __launch_bounds__(32 * WM * WN) dgemm_kernel(const Params p) {
         } else {
           int64_t rr = row, base = 0;
           if (p.c_plane_rows > 0) { base = (row / p.c_plane_rows) * p.c_plane_stride; rr = row % p.c_plane_rows; }
-          double* c = p.C + (base + b * p.strideC + rr * p.ldc + col) * PL;
+          double* c = p.C + (base + b * p.strideC + rr * p.ldc + col * p.ccs) * PL;
 #pragma unroll
           for (int q = 0; q < PL; ++q) {
             const double v = p.alpha * acc[i][j][q][e];
@@ -258,7 +259,7 @@ __global__ void splitk_reduce_kernel(const Params p) {
     }
     int64_t rr = row, base = 0;
     if (p.c_plane_rows > 0) { base = (row / p.c_plane_rows) * p.c_plane_stride; rr = row % p.c_plane_rows; }
-    double* c = p.C + (base + b * p.strideC + rr * p.ldc + col) * PL;
+    double* c = p.C + (base + b * p.strideC + rr * p.ldc + col * p.ccs) * PL;
 #pragma unroll
     for (int q = 0; q < PL; ++q) {
       const double v = p.alpha * s[q];
@@ -406,6 +407,9 @@ void gemm(const GemmDesc& d, cudaStream_t stream, double* work, int64_t work_cap
   p.signA = d.conjA ? -1.0 : 1.0;
   p.signB = d.conjB ? -1.0 : 1.0;
   p.c_plane_rows = d.c_plane_rows; p.c_plane_stride = d.c_plane_stride;
+  p.ccs = d.c_col_stride;
+  RR_REQUIRE(d.c_col_stride >= 1 && (d.c_col_stride == 1 || !d.cplx), RR_ERR_ARG, "gemm: bad output column stride");
+  RR_REQUIRE(d.c_col_stride == 1 || !d.mirror, RR_ERR_ARG, "gemm: mirror with strided output");
   p.upper_only = d.mirror != 0;
   p.eE = d.edot_E;
   p.eld = d.edot_ld;

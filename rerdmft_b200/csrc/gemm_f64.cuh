@@ -30,6 +30,9 @@ struct GemmDesc {
   // Output rows r >= c_plane_rows go to C + (r / c_plane_rows) * c_plane_stride, row r % c_plane_rows
   // (0 disables).  Lets one GEMM write the stacked [re; im] half-transform into two planes.
   int64_t c_plane_rows = 0, c_plane_stride = 0;
+  // Element stride between consecutive output columns (real outputs only; 2 with c_plane_stride = 1
+  // and c_plane_rows = M/2 writes a stacked [re; im] product as interleaved complex).
+  int64_t c_col_stride = 1;
   // Symmetric outputs: compute only tiles touching the upper triangle, then fill the strict
   // lower triangle from the upper one: +1 C[i][j] = C[j][i] (Hermitian conj for cplx),
   // -1 C[i][j] = -C[j][i].  0 = full output.  Requires M == N.
