@@ -21,6 +21,10 @@ int rr_test_gemm_f64(int64_t M, int64_t N, int64_t K, const double* A, int64_t l
 /* gamma = B vec(D) and J = B^T gamma through the TMA streaming passes (B: naux x n2, dense). */
 int rr_test_j_passes(const double* B, int64_t naux, int64_t n2, const double* D, double* gamma, double* J);
 
+/* K = sum_P (Ct B^P)^T (Ct B^P) through the split-BF16 tcgen05 exchange (B: naux x n*n dense,
+ * Ct: nocc x n, K: n x n; all FP64 device pointers). */
+int rr_test_mixed_exchange(const double* B, int64_t naux, int64_t n, const double* Ct, int64_t nocc, double* K);
+
 #ifdef __cplusplus
 }
 #endif

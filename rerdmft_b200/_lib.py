@@ -82,6 +82,7 @@ _SIGS = {
     "rr_kernel_launches": (ctypes.c_int64, []),
     "rr_test_gemm_f64": (ctypes.c_int, [_i64, _i64, _i64, _vp, _i64, _i64, _i32, _vp, _i64, _i64, _i32, _vp, _i64,
                                         _i64, _d, _d, _i64, _i32, _i32, _i32, _i32, _i32]),
+    "rr_test_mixed_exchange": (ctypes.c_int, [_vp, _i64, _i64, _vp, _i64, _vp]),
     "rr_test_j_passes": (ctypes.c_int, [_vp, _i64, _i64, _vp, _vp, _vp]),
 }
 

@@ -200,7 +200,8 @@ int rr_ri_jk_occupied(rr_ri_handle h, const double* C_occ, int64_t n_occ, double
   return api([&] {
     auto* s = checked(h);
     RR_REQUIRE((C_occ || n_occ == 0) && J && K, RR_ERR_ARG, "rr_ri_jk_occupied: null matrix");
-    RR_REQUIRE(!opts || opts->precision == RR_PREC_FP64, RR_ERR_UNSUPPORTED, "rr_ri_jk_occupied: precision");
+    RR_REQUIRE(!opts || opts->precision == RR_PREC_FP64 || opts->precision == RR_PREC_MIXED, RR_ERR_UNSUPPORTED,
+               "rr_ri_jk_occupied: unknown precision");
     rr::jk_occupied(s, C_occ, n_occ, J, K, opts);
   });
 }
@@ -455,6 +456,21 @@ extern "C" int rr_test_gemm_f64(int64_t M, int64_t N, int64_t K, const double* A
     }
     rr::gemm(g, nullptr, allow_split ? work.p : nullptr, cap);
     RR_CUDA(cudaDeviceSynchronize());
+  });
+}
+
+extern "C" int rr_test_mixed_exchange(const double* B, int64_t naux, int64_t n, const double* Ct, int64_t nocc,
+                                      double* K) {
+  return api([&] {
+    rr::MixedOperands mo;
+    rr::DevBuf<int> err(2);
+    RR_CUDA(cudaMemset(err.p, 0, 2 * sizeof(int)));
+    rr::mixed_prepare(mo, B, n * n, n, naux, nullptr);
+    rr::mixed_exchange(mo, Ct, n, nocc, K, err.p, nullptr);
+    RR_CUDA(cudaDeviceSynchronize());
+    int e = 0;
+    RR_CUDA(cudaMemcpy(&e, err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    RR_REQUIRE(e == 0, RR_ERR_TIMEOUT, "rr_test_mixed_exchange: device wait bound expired (0x" + std::to_string(e) + ")");
   });
 }
 

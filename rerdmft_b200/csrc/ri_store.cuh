@@ -3,6 +3,7 @@
 
 #include "gemm_f64.cuh"
 #include "j_stream.cuh"
+#include "mixed.cuh"
 #include "rr_common.cuh"
 
 struct rr_ri_store {
@@ -21,10 +22,8 @@ struct rr_ri_store {
   rr::DevBuf<double> solver_a;  // eigen-problem matrix / eigenvectors
   rr::DevBuf<double> solver_w;  // eigenvalues
   std::vector<double> host_w;
-  // Split-BF16 copies of B for RR_PREC_MIXED (built on first use).
-  rr::DevBuf<uint16_t> Bhi[2], Blo[2];
-  int64_t mixed_pitch[2] = {0, 0};
-  bool mixed_ready = false;
+  // Split-BF16 copy of B for RR_PREC_MIXED (built on first use).
+  rr::MixedOperands mixed;
   // Profiling events: 0 start, 1 recovery done, 2 half-transform done, 3 exchange done, 4 end
   // (main stream); 5 J start, 6 J end (side stream).
   bool profiling = false;
