@@ -121,6 +121,39 @@ int rr_ri_fock_rkb(rr_ri_handle h, const double* h_rkb, const double* v_total, i
  * the device-resident SCF loop; equal to rr_ri_fock_nonrel when D = 2 C C^T. */
 int rr_ri_jk_occupied(rr_ri_handle h, const double* C_occ, int64_t n_occ, double* J, double* K, const rr_opts* opts);
 
+/* ---------------- device-resident SCF loops ---------------- */
+
+typedef struct rr_scf_opts {
+  int32_t diis_size;          /* DIIS_SIZE (reference default 5; < 2 disables DIIS) */
+  int32_t max_iterations;     /* reference default 100 */
+  double energy_tolerance;    /* ENERGY_TOLERANCE (1e-8) */
+  double density_tolerance;   /* DENSITY_TOLERANCE (1e-6) */
+  int32_t kramers_restricted; /* X2C / 4c: project densities onto their time-reversal-even part */
+  int32_t precision;          /* RR_PREC_FP64 or RR_PREC_MIXED (split-BF16 exchange, FP64 for the last iterations) */
+  double mixed_switch;        /* RR_PREC_MIXED: switch to FP64 builds once |dE| < mixed_switch */
+  int32_t reserved0;
+  int32_t reserved1;
+} rr_scf_opts;
+
+typedef struct rr_scf_result {
+  double electronic_energy; /* 1/2 Tr[P (h + F)] of the last iteration (no nuclear repulsion) */
+  int64_t iterations;
+  int64_t converged;
+  int64_t mixed_iterations; /* Fock builds with the split-BF16 exchange */
+  int64_t fp64_iterations;  /* Fock builds in FP64 */
+  double seconds;           /* wall time of the loop, inputs on the device to density out */
+} rr_scf_result;
+
+/* Restricted nonrelativistic SCF with the RI Fock build, DIIS on e = FPS - SPF and the aufbau
+ * density from the lowest n_electrons/2 eigenvectors of X^T F X (obtained by SP2 purification on
+ * the GPU).  Replaces runNonRelativisticHartreeFock(RiNonRelEriSource, ...),
+ * src/NON_REL/NonRelHartreeFock.cpp:117-198/219 (nuclear repulsion is the caller's; no mixing:
+ * DIIS replaces it as in the reference).  energy_history (optional) receives one electronic energy
+ * per iteration (max_iterations doubles); P_out the density of the last iteration. */
+int rr_scf_run_nonrel(rr_ri_handle h, const double* h_core, const double* X, int64_t n_eff, const double* S,
+                      const double* P0, int32_t n_electrons, const rr_scf_opts* scf, rr_scf_result* result,
+                      double* P_out, double* energy_history, const rr_opts* opts);
+
 /* ---------------- MO-basis RI tensors (functional stage) ---------------- */
 
 typedef struct rr_mo_store* rr_mo_handle;

@@ -14,6 +14,8 @@ void fock_x2c(rr_ri_store*, const double*, const double*, const double*, const d
 void ukb_two_electron(rr_ri_store*, const double*, const double*, int64_t, const double*, double*, const rr_opts*);
 void fock_rkb(rr_ri_store*, const double*, const double*, int64_t, const double*, const double*, int64_t,
               const double*, double*, const rr_opts*);
+void scf_nonrel(rr_ri_store*, const double*, const double*, int64_t, const double*, const double*, int,
+                const rr_scf_opts*, rr_scf_result*, double*, double*, const rr_opts*);
 }  // namespace rr
 
 namespace {
@@ -233,6 +235,21 @@ int rr_ri_fock_rkb(rr_ri_handle h, const double* h_rkb, const double* v_total, i
     RR_REQUIRE(h_rkb && v_total && s_full && P && F && (x_full || n_eff == 0), RR_ERR_ARG, "rr_ri_fock_rkb: null matrix");
     RR_REQUIRE(!opts || opts->precision == RR_PREC_FP64, RR_ERR_UNSUPPORTED, "rr_ri_fock_rkb: precision");
     rr::fock_rkb(s, h_rkb, v_total, n_rkb, s_full, x_full, n_eff, P, F, opts);
+  });
+}
+
+int rr_scf_run_nonrel(rr_ri_handle h, const double* h_core, const double* X, int64_t n_eff, const double* S,
+                      const double* P0, int32_t n_electrons, const rr_scf_opts* scf, rr_scf_result* result,
+                      double* P_out, double* energy_history, const rr_opts* opts) {
+  return api([&] {
+    auto* s = checked(h);
+    RR_REQUIRE(h_core && X && S && P0 && scf && result && P_out, RR_ERR_ARG, "rr_scf_run_nonrel: null argument");
+    RR_REQUIRE(n_eff >= 1 && n_eff <= s->n, RR_ERR_ARG, "rr_scf_run_nonrel: n_eff out of range");
+    RR_REQUIRE(scf->max_iterations >= 1, RR_ERR_ARG, "rr_scf_run_nonrel: max_iterations < 1");
+    RR_REQUIRE(scf->precision == RR_PREC_FP64 || scf->precision == RR_PREC_MIXED, RR_ERR_UNSUPPORTED,
+               "rr_scf_run_nonrel: unknown precision");
+    *result = rr_scf_result{};
+    rr::scf_nonrel(s, h_core, X, n_eff, S, P0, n_electrons, scf, result, P_out, energy_history, opts);
   });
 }
 

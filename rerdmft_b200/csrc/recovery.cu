@@ -182,6 +182,94 @@ int blocks_for(int64_t n) { return static_cast<int>(std::max<int64_t>(1, std::mi
 
 }  // namespace
 
+// From a rank-r orthogonal projector Pi (n_eff x n_eff, in the orthonormal basis of X) build
+// c_t = F^dagger X^dagger (r x n, leading dim n) with F F^dagger = Pi (Pe == nullptr) or
+// Pi Pe Pi (weighted): Y = Pi G for a fixed pseudo-random G, CholeskyQR2, optional weighting.
+void projector_ct(rr_ri_store* h, const double* A, const double* Pe, const double* X, int64_t n, int64_t n_eff,
+                  int64_t r, bool cplx, double* Ct, cudaStream_t s) {
+  const int PL = cplx ? 2 : 1;
+  const bool weighted = Pe != nullptr;
+  if (r == 0) return;
+  h->work.ensure(static_cast<size_t>(std::max<int64_t>(static_cast<int64_t>(h->work.n), 8 * n * n * PL)));
+  double* wk = h->work.p;
+  const int64_t wcap = static_cast<int64_t>(h->work.n);
+  // Orthonormal basis of range(Pi): Y = Pi G (fixed pseudo-random G), CholeskyQR2 with the small
+  // triangular factors applied as GEMMs.
+  double *G, *Y2, *Y3, *M, *Wt, *PQ, *gw;
+  Arena ar2(&h->T);  // the exchange intermediate is not live yet
+  ar2.request(&G, n_eff * r * PL);
+  ar2.request(&Y2, n_eff * r * PL);
+  ar2.request(&Y3, n_eff * r * PL);
+  ar2.request(&M, r * r * PL);
+  ar2.request(&Wt, r * r * PL);
+  ar2.request(&PQ, n_eff * r * PL);
+  ar2.request(&gw, r * r * PL);
+  ar2.commit();
+  const size_t chol_smem = sizeof(double) * r * r * PL;
+  const bool chol_in_smem = chol_smem <= 160 * 1024;
+  if (cplx) fill_test_matrix_kernel<2><<<blocks_for(n_eff * r * 2), 256, 0, s>>>(G, n_eff * r);
+  else fill_test_matrix_kernel<1><<<blocks_for(n_eff * r), 256, 0, s>>>(G, n_eff * r);
+  RR_LAUNCH_CHECK();
+  GemmDesc y;
+  y.cplx = cplx;
+  y.M = n_eff; y.N = r; y.K = n_eff;
+  y.A = A; y.lda = n_eff; y.B = G; y.ldb = r; y.C = Y2; y.ldc = r;
+  gemm(y, s, wk, wcap);
+  auto chol = [&](const double* mat, int inverse) {
+    const size_t sm = chol_in_smem ? chol_smem : 0;
+    if (cplx) {
+      auto k = chol_small_kernel<2>;
+      if (sm > 48 * 1024) RR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
+      k<<<1, 32, sm, s>>>(mat, r, Wt, chol_in_smem ? nullptr : gw, inverse, h->status.p + 1);
+    } else {
+      auto k = chol_small_kernel<1>;
+      if (sm > 48 * 1024) RR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
+      k<<<1, 32, sm, s>>>(mat, r, Wt, chol_in_smem ? nullptr : gw, inverse, h->status.p + 1);
+    }
+    RR_LAUNCH_CHECK();
+  };
+  GemmDesc gm;  // M = Y^dagger Y
+  gm.cplx = cplx;
+  gm.M = r; gm.N = r; gm.K = n_eff;
+  gm.opA = Op::T; gm.conjA = cplx; gm.lda = r; gm.ldb = r; gm.C = M; gm.ldc = r;
+  GemmDesc yw;  // Y_out = Y_in Wt
+  yw.cplx = cplx;
+  yw.M = n_eff; yw.N = r; yw.K = r;
+  yw.lda = r; yw.B = Wt; yw.ldb = r; yw.ldc = r;
+  double* cur = Y2;
+  double* nxt = Y3;
+  for (int pass = 0; pass < 2; ++pass) {
+    gm.A = cur; gm.B = cur;
+    gemm(gm, s, wk, wcap);
+    chol(M, 1);
+    yw.A = cur; yw.C = nxt;
+    gemm(yw, s, wk, wcap);
+    std::swap(cur, nxt);
+  }
+  if (weighted) {  // F = Q chol(Q^dagger Pe Q): F F^dagger = Pi Pe Pi
+    GemmDesc pq;
+    pq.cplx = cplx;
+    pq.M = n_eff; pq.N = r; pq.K = n_eff;
+    pq.A = Pe; pq.lda = n_eff; pq.B = cur; pq.ldb = r; pq.C = PQ; pq.ldc = r;
+    gemm(pq, s, wk, wcap);
+    gm.A = cur; gm.B = PQ;
+    gemm(gm, s, wk, wcap);
+    chol(M, 0);
+    yw.A = cur; yw.C = nxt;
+    gemm(yw, s, wk, wcap);
+    std::swap(cur, nxt);
+  }
+  Y2 = cur;
+  // c_t = F^dagger X^dagger  (r x n)
+  GemmDesc ct;
+  ct.cplx = cplx;
+  ct.M = r; ct.N = n; ct.K = n_eff;
+  ct.A = Y2; ct.lda = r; ct.opA = Op::T; ct.conjA = cplx;
+  ct.B = X; ct.ldb = n_eff; ct.opB = Op::T; ct.conjB = cplx;
+  ct.C = Ct; ct.ldc = n;
+  gemm(ct, s, wk, wcap);
+}
+
 // Recovers c_t (r x n, row-major) from the density.  cplx selects interleaved complex matrices;
 // weighted multiplies the projector by P_eff (sqrt(occupation) weighting of X2C / 4c).
 // Dp: density (n x n, ld n); S (n x n); X (n x n_eff).  Returns r.
@@ -265,81 +353,7 @@ int64_t occupied_ct(rr_ri_store* h, const double* X, const double* S, const doub
   // Rank = number of eigenvalues above 1/2 = trace(Pi) = (n_eff + trace(sign))/2.
   const int64_t r = std::max<int64_t>(0, std::min<int64_t>(n_eff, std::llround(0.5 * (n_eff + hres[2]))));
   if (r == 0) return 0;
-  // Orthonormal basis of range(Pi): Y = Pi G (fixed pseudo-random G), CholeskyQR2 with the small
-  // triangular factors applied as GEMMs.
-  double *G, *Y2, *Y3, *M, *Wt, *PQ, *gw;
-  Arena ar2(&h->T);  // the exchange intermediate is not live yet
-  ar2.request(&G, n_eff * r * PL);
-  ar2.request(&Y2, n_eff * r * PL);
-  ar2.request(&Y3, n_eff * r * PL);
-  ar2.request(&M, r * r * PL);
-  ar2.request(&Wt, r * r * PL);
-  ar2.request(&PQ, n_eff * r * PL);
-  ar2.request(&gw, r * r * PL);
-  ar2.commit();
-  const size_t chol_smem = sizeof(double) * r * r * PL;
-  const bool chol_in_smem = chol_smem <= 160 * 1024;
-  if (cplx) fill_test_matrix_kernel<2><<<blocks_for(n_eff * r * 2), 256, 0, s>>>(G, n_eff * r);
-  else fill_test_matrix_kernel<1><<<blocks_for(n_eff * r), 256, 0, s>>>(G, n_eff * r);
-  RR_LAUNCH_CHECK();
-  GemmDesc y;
-  y.cplx = cplx;
-  y.M = n_eff; y.N = r; y.K = n_eff;
-  y.A = A; y.lda = n_eff; y.B = G; y.ldb = r; y.C = Y2; y.ldc = r;
-  gemm(y, s, wk, wcap);
-  auto chol = [&](const double* mat, int inverse) {
-    const size_t sm = chol_in_smem ? chol_smem : 0;
-    if (cplx) {
-      auto k = chol_small_kernel<2>;
-      if (sm > 48 * 1024) RR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
-      k<<<1, 32, sm, s>>>(mat, r, Wt, chol_in_smem ? nullptr : gw, inverse, h->status.p + 1);
-    } else {
-      auto k = chol_small_kernel<1>;
-      if (sm > 48 * 1024) RR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
-      k<<<1, 32, sm, s>>>(mat, r, Wt, chol_in_smem ? nullptr : gw, inverse, h->status.p + 1);
-    }
-    RR_LAUNCH_CHECK();
-  };
-  GemmDesc gm;  // M = Y^dagger Y
-  gm.cplx = cplx;
-  gm.M = r; gm.N = r; gm.K = n_eff;
-  gm.opA = Op::T; gm.conjA = cplx; gm.lda = r; gm.ldb = r; gm.C = M; gm.ldc = r;
-  GemmDesc yw;  // Y_out = Y_in Wt
-  yw.cplx = cplx;
-  yw.M = n_eff; yw.N = r; yw.K = r;
-  yw.lda = r; yw.B = Wt; yw.ldb = r; yw.ldc = r;
-  double* cur = Y2;
-  double* nxt = Y3;
-  for (int pass = 0; pass < 2; ++pass) {
-    gm.A = cur; gm.B = cur;
-    gemm(gm, s, wk, wcap);
-    chol(M, 1);
-    yw.A = cur; yw.C = nxt;
-    gemm(yw, s, wk, wcap);
-    std::swap(cur, nxt);
-  }
-  if (weighted) {  // F = Q chol(Q^dagger Pe Q): F F^dagger = Pi Pe Pi
-    GemmDesc pq;
-    pq.cplx = cplx;
-    pq.M = n_eff; pq.N = r; pq.K = n_eff;
-    pq.A = Pe; pq.lda = n_eff; pq.B = cur; pq.ldb = r; pq.C = PQ; pq.ldc = r;
-    gemm(pq, s, wk, wcap);
-    gm.A = cur; gm.B = PQ;
-    gemm(gm, s, wk, wcap);
-    chol(M, 0);
-    yw.A = cur; yw.C = nxt;
-    gemm(yw, s, wk, wcap);
-    std::swap(cur, nxt);
-  }
-  Y2 = cur;
-  // c_t = F^dagger X^dagger  (r x n)
-  GemmDesc ct;
-  ct.cplx = cplx;
-  ct.M = r; ct.N = n; ct.K = n_eff;
-  ct.A = Y2; ct.lda = r; ct.opA = Op::T; ct.conjA = cplx;
-  ct.B = X; ct.ldb = n_eff; ct.opB = Op::T; ct.conjB = cplx;
-  ct.C = Ct; ct.ldc = n;
-  gemm(ct, s, wk, wcap);
+  projector_ct(h, A, weighted ? Pe : nullptr, X, n, n_eff, r, cplx, Ct, s);
   return r;
 }
 

@@ -1,0 +1,427 @@
+// Device-resident RHF SCF loop over the RI Fock build (reference: nonRelScfImpl,
+// src/NON_REL/NonRelHartreeFock.cpp:117-198, and Diis<T>, src/Utils/DIIS.cpp:53-131).
+//
+// Per iteration, everything but a 6x6 DIIS solve stays on the GPU:
+//   F = h + J(P) - K(C_occ)         (J FP64; K FP64 DMMA or split-BF16 tcgen05 by phase)
+//   E = 1/2 Tr[P (h + F)]           (the un-extrapolated F, as the reference)
+//   e = F P S - S P F, DIIS extrapolation (newest-first history, scaled B, bordered solve,
+//   drop-oldest on a singular system: the reference's algorithm, solved on the host)
+//   F_ortho = X^T F_scf X, then the aufbau projector onto its lowest nocc eigenvectors by SP2
+//   trace-correcting purification (GEMMs only; no eigensolver), C_occ from the projector
+//   P_new = 2 C_occ C_occ^T; converged when dP < tolP OR dE < tolE (from the second iteration).
+// The first iteration builds F from the caller's start density through the drop-in Fock build
+// (occupied recovery included); later iterations reuse the loop's own C_occ.
+//
+// Mixed precision (RR_PREC_MIXED): iterations run with the split-BF16 exchange until |dE| falls
+// below `mixed_switch`, then the loop switches to FP64 builds for the remaining iterations, so the
+// converged energy is that of the FP64 Fock matrix.
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "ri_store.cuh"
+
+namespace rr {
+
+void exchange_nonrel(rr_ri_store* h, const double* Ct, int64_t ldct, bool ct_transposed, int64_t nocc, double* K,
+                     cudaStream_t s, const double* Dp, double* Jout);
+void coulomb_after_ht(rr_ri_store* h, const double* Dp, const double* Ct, int64_t nocc, double* J, const double* tgam,
+                      int tseg, cudaStream_t s);
+void coulomb_join(rr_ri_store* h, cudaStream_t s);
+void fock_nonrel(rr_ri_store* h, const double* hc, const double* D, const double* S, const double* X, int64_t n_eff,
+                 double* F, const rr_opts* o);
+void projector_ct(rr_ri_store* h, const double* A, const double* Pe, const double* X, int64_t n, int64_t n_eff,
+                  int64_t r, bool cplx, double* Ct, cudaStream_t s);
+
+namespace {
+
+int blocks_for(int64_t n) { return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 1184))); }
+
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) t += red[w];
+  __syncthreads();
+  return t;
+}
+
+// Gershgorin bounds of a symmetric n x n matrix: out[0] = min_i (a_ii - r_i), out[1] = max (a_ii + r_i).
+__global__ void gershgorin_kernel(const double* A, int64_t n, double* out) {
+  __shared__ double lo_s[32], hi_s[32];
+  double lo = 1e300, hi = -1e300;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+    double r = 0.0;
+    for (int64_t j = 0; j < n; ++j)
+      if (j != i) r += fabs(A[i * n + j]);
+    lo = fmin(lo, A[i * n + i] - r);
+    hi = fmax(hi, A[i * n + i] + r);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  if ((threadIdx.x & 31) == 0) { lo_s[threadIdx.x >> 5] = lo; hi_s[threadIdx.x >> 5] = hi; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) { lo = fmin(lo, lo_s[w]); hi = fmax(hi, hi_s[w]); }
+    out[0] = lo;
+    out[1] = hi;
+  }
+}
+
+// X = (emax I - F) / (emax - emin): spectrum mapped into [0, 1], lowest states near 1.
+__global__ void sp2_init_kernel(double* X, const double* F, int64_t n, const double* b) {
+  const double emin = b[0], emax = b[1], inv = 1.0 / fmax(emax - emin, 1e-300);
+  for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < n * n;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t i = idx / n, j = idx % n;
+    X[idx] = ((i == j ? emax : 0.0) - F[idx]) * inv;
+  }
+}
+
+// tr[0] = trace X, tr[1] = trace T (one CTA).
+__global__ void two_traces_kernel(const double* X, const double* T, int64_t n, double* tr) {
+  __shared__ double red[32];
+  double a = 0.0, b = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+    a += X[i * n + i];
+    b += T[i * n + i];
+  }
+  a = block_sum(a, red);
+  b = block_sum(b, red);
+  if (threadIdx.x == 0) { tr[0] = a; tr[1] = b; }
+}
+
+// SP2 step (trace correcting): X <- X^2 if that brings the trace closer to N, else 2X - X^2.
+__global__ void sp2_update_kernel(double* X, const double* T, int64_t n, const double* tr, double N) {
+  const double trx = tr[0], trt = tr[1];
+  const bool square = fabs(trt - N) < fabs(2.0 * trx - trt - N);
+  for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < n * n;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    X[idx] = square ? T[idx] : 2.0 * X[idx] - T[idx];
+}
+
+// out[0] = Tr[P A^T-free]: sum_ij P_ij (h + F)_ji  (energy trace), one CTA
+__global__ void energy_kernel(const double* P, const double* h, const double* F, int64_t n, double* out) {
+  __shared__ double red[32];
+  double acc = 0.0;
+  for (int64_t idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+    const int64_t i = idx / n, j = idx % n;
+    acc += P[idx] * (h[j * n + i] + F[j * n + i]);
+  }
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) out[0] = 0.5 * acc;
+}
+
+// out[0] = max |A - B| (one CTA)
+__global__ void maxdiff_kernel(const double* A, const double* B, int64_t cnt, double* out) {
+  __shared__ double red[32];
+  double m = 0.0;
+  for (int64_t i = threadIdx.x; i < cnt; i += blockDim.x) m = fmax(m, fabs(A[i] - B[i]));
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
+    out[0] = m;
+  }
+}
+
+constexpr int DIIS_MAX = 16;
+struct DotArgs {
+  const double* v[DIIS_MAX];
+  int count;
+};
+
+// out[k] = <e, v_k> for k < count (one CTA, fixed order)
+__global__ void diis_dots_kernel(const double* e, DotArgs a, int64_t cnt, double* out) {
+  __shared__ double red[32];
+  for (int k = 0; k < a.count; ++k) {
+    double acc = 0.0;
+    for (int64_t i = threadIdx.x; i < cnt; i += blockDim.x) acc += e[i] * a.v[k][i];
+    acc = block_sum(acc, red);
+    if (threadIdx.x == 0) out[k] = acc;
+  }
+}
+
+struct CombArgs {
+  const double* v[DIIS_MAX];
+  double w[DIIS_MAX];
+  int count;
+};
+
+__global__ void diis_combine_kernel(double* out, CombArgs a, int64_t cnt) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < cnt;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double s = 0.0;
+    for (int k = 0; k < a.count; ++k) s += a.w[k] * a.v[k][i];
+    out[i] = s;
+  }
+}
+
+// The reference's dense solve (DIIS.cpp:18-48): Gaussian elimination with partial pivoting, false
+// when min |pivot| / max |pivot| is not above tol.
+bool solve_dense(std::vector<double> m, std::vector<double> rhs, size_t n, double tol, std::vector<double>& x) {
+  std::vector<double> piv(n);
+  for (size_t k = 0; k < n; ++k) {
+    size_t best = k;
+    for (size_t i = k + 1; i < n; ++i)
+      if (std::fabs(m[i * n + k]) > std::fabs(m[best * n + k])) best = i;
+    if (best != k) {
+      for (size_t j = 0; j < n; ++j) std::swap(m[k * n + j], m[best * n + j]);
+      std::swap(rhs[k], rhs[best]);
+    }
+    piv[k] = std::fabs(m[k * n + k]);
+    if (piv[k] == 0.0) return false;
+    for (size_t i = k + 1; i < n; ++i) {
+      const double f = m[i * n + k] / m[k * n + k];
+      for (size_t j = k; j < n; ++j) m[i * n + j] -= f * m[k * n + j];
+      rhs[i] -= f * rhs[k];
+    }
+  }
+  double pmax = piv[0], pmin = piv[0];
+  for (double v : piv) { pmax = std::max(pmax, v); pmin = std::min(pmin, v); }
+  if (!(pmin > tol * pmax)) return false;
+  x.assign(n, 0.0);
+  for (size_t ii = n; ii-- > 0;) {
+    double sum = rhs[ii];
+    for (size_t j = ii + 1; j < n; ++j) sum -= m[ii * n + j] * x[j];
+    x[ii] = sum / m[ii * n + ii];
+  }
+  return true;
+}
+
+// Device-resident DIIS history (src/Utils/DIIS.cpp:79-131): slots hold (error, value) pairs; the
+// newest-first order and the B matrix are kept on the host.
+struct DeviceDiis {
+  int max_vectors = 0;
+  int64_t len = 0;
+  DevBuf<double> err, val, dots;
+  std::vector<int> order;  // slot indices, newest first
+  std::vector<std::vector<double>> bmat;  // bmat[slot][slot]
+  void init(int maxv, int64_t length) {
+    max_vectors = maxv;
+    len = length;
+    const int slots = std::max(maxv, 1);
+    err.alloc(static_cast<size_t>(slots * length));
+    val.alloc(static_cast<size_t>(slots * length));
+    dots.alloc(DIIS_MAX);
+    order.clear();
+    bmat.assign(slots, std::vector<double>(slots, 0.0));
+  }
+  // Stores (e, F) and writes the extrapolated F into out (or copies F when nothing extrapolates).
+  void extrapolate(const double* e, const double* F, double* out, cudaStream_t s) {
+    if (max_vectors < 2) {
+      copy_out(out, F, len, false, s);
+      return;
+    }
+    int slot;
+    if (static_cast<int>(order.size()) < max_vectors) {
+      slot = static_cast<int>(order.size());
+    } else {
+      slot = order.back();
+      order.pop_back();
+    }
+    copy_out(err.p + slot * len, e, len, false, s);
+    copy_out(val.p + slot * len, F, len, false, s);
+    order.insert(order.begin(), slot);
+    DotArgs a{};
+    a.count = static_cast<int>(order.size());
+    for (int k = 0; k < a.count; ++k) a.v[k] = err.p + order[k] * len;
+    diis_dots_kernel<<<1, 1024, 0, s>>>(err.p + slot * len, a, len, dots.p);
+    RR_LAUNCH_CHECK();
+    std::vector<double> d(a.count);
+    RR_CUDA(cudaMemcpyAsync(d.data(), dots.p, sizeof(double) * a.count, cudaMemcpyDeviceToHost, s));
+    RR_CUDA(cudaStreamSynchronize(s));
+    for (int k = 0; k < a.count; ++k) bmat[slot][order[k]] = bmat[order[k]][slot] = d[k];
+    const size_t total = order.size();
+    for (size_t m = total; m >= 2; --m) {
+      double scale = 0.0;
+      for (size_t i = 0; i < m; ++i) scale = std::max(scale, bmat[order[i]][order[i]]);
+      if (!(scale > 0.0)) break;
+      const size_t nn = m + 1;
+      std::vector<double> A(nn * nn, 0.0), rhs(nn, 0.0), x;
+      for (size_t i = 0; i < m; ++i)
+        for (size_t j = 0; j < m; ++j) A[i * nn + j] = bmat[order[i]][order[j]] / scale;
+      for (size_t i = 0; i < m; ++i) A[i * nn + m] = A[m * nn + i] = -1.0;
+      rhs[m] = -1.0;
+      if (!solve_dense(A, rhs, nn, 1e-14, x)) continue;
+      CombArgs c{};
+      c.count = static_cast<int>(m);
+      for (size_t i = 0; i < m; ++i) { c.v[i] = val.p + order[i] * len; c.w[i] = x[i]; }
+      diis_combine_kernel<<<blocks_for(len), 256, 0, s>>>(out, c, len);
+      RR_LAUNCH_CHECK();
+      return;
+    }
+    copy_out(out, F, len, false, s);
+  }
+};
+
+}  // namespace
+
+// SP2 purification: projector (n x n, into Pi) onto the lowest `nocc` eigenvectors of the symmetric
+// F (n x n).  T is scratch (n x n).  Host checks every 4 steps; at most 120 steps.
+void sp2_projector(rr_ri_store* h, const double* F, int64_t n, int64_t nocc, double* Pi, double* T, double* scal,
+                   cudaStream_t s) {
+  gershgorin_kernel<<<1, 512, 0, s>>>(F, n, scal);
+  RR_LAUNCH_CHECK();
+  sp2_init_kernel<<<blocks_for(n * n), 256, 0, s>>>(Pi, F, n, scal);
+  RR_LAUNCH_CHECK();
+  GemmDesc g;
+  g.M = n; g.N = n; g.K = n;
+  g.A = Pi; g.lda = n; g.B = Pi; g.ldb = n; g.C = T; g.ldc = n;
+  h->work.ensure(static_cast<size_t>(std::max<int64_t>(static_cast<int64_t>(h->work.n), 8 * n * n)));
+  const double N = static_cast<double>(nocc);
+  for (int it = 0; it < 120; ++it) {
+    gemm(g, s, h->work.p, static_cast<int64_t>(h->work.n));
+    two_traces_kernel<<<1, 512, 0, s>>>(Pi, T, n, scal + 2);
+    RR_LAUNCH_CHECK();
+    sp2_update_kernel<<<blocks_for(n * n), 256, 0, s>>>(Pi, T, n, scal + 2, N);
+    RR_LAUNCH_CHECK();
+    if (it % 4 == 3) {
+      double tr[2];
+      RR_CUDA(cudaMemcpyAsync(tr, scal + 2, sizeof(tr), cudaMemcpyDeviceToHost, s));
+      RR_CUDA(cudaStreamSynchronize(s));
+      // idempotency measure of the pre-update X: |tr X - tr X^2| (sum of lambda (1 - lambda))
+      if (std::fabs(tr[0] - tr[1]) < 1e-11 * std::max<double>(1.0, N) && std::fabs(tr[0] - N) < 1e-6) return;
+    }
+  }
+  throw Error(RR_ERR_SOLVER, "SCF: density purification did not converge (no gap at the Fermi level?)");
+}
+
+void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff, const double* S, const double* P0,
+                int n_electrons, const rr_scf_opts* so, rr_scf_result* res, double* P_out, double* hist,
+                const rr_opts* o) {
+  RR_REQUIRE(h->ntens == 1, RR_ERR_STATE, "rr_scf_run_nonrel: handle holds a 4-component store");
+  RR_REQUIRE(n_electrons > 0 && n_electrons % 2 == 0, RR_ERR_ARG,
+             "nonRelDensityMatrix: n_electrons must be a positive even number (closed-shell restricted Hartree-Fock)");
+  const int64_t n = h->n, n2 = n * n, nocc = n_electrons / 2;
+  RR_REQUIRE(nocc <= n_eff, RR_ERR_ARG, "nonRelDensityMatrix: n_electrons/2 exceeds the number of available spatial orbitals");
+  const bool host = !o || o->mem == RR_MEM_HOST;
+  cudaStream_t s = call_stream(h, o);
+  const auto t_start = std::chrono::steady_clock::now();
+  const int64_t pitch = round_up(std::max<int64_t>(n2, 2), 32);
+  DevBuf<double> buf;
+  Arena ar(&buf);
+  double *hd, *Xd, *Sd, *P, *Pn, *F, *J, *K, *Fs, *e, *PS, *SP, *tmp, *Fo, *Pi, *T2, *Ct, *scal;
+  ar.request(&hd, n2);
+  ar.request(&Xd, n * n_eff);
+  ar.request(&Sd, n2);
+  ar.request(&P, pitch);
+  ar.request(&Pn, pitch);
+  ar.request(&F, n2);
+  ar.request(&J, n2);
+  ar.request(&K, n2);
+  ar.request(&Fs, n2);
+  ar.request(&e, n2);
+  ar.request(&PS, n2);
+  ar.request(&SP, n2);
+  ar.request(&tmp, std::max(n2, n * n_eff));
+  ar.request(&Fo, n_eff * n_eff);
+  ar.request(&Pi, n_eff * n_eff);
+  ar.request(&T2, n_eff * n_eff);
+  ar.request(&Ct, nocc * n);
+  ar.request(&scal, 64);
+  ar.commit();
+  copy_in(hd, hc, n2, host, s);
+  copy_in(Xd, X, n * n_eff, host, s);
+  copy_in(Sd, S, n2, host, s);
+  copy_in_padded(P, pitch, P0, n2, host, s);
+  RR_CUDA(cudaMemsetAsync(Pn + n2, 0, sizeof(double) * (pitch - n2), s));
+  const bool mixed_requested = so->precision == RR_PREC_MIXED;
+  bool mixed = mixed_requested;
+  DeviceDiis diis;
+  const bool use_diis = so->diis_size >= 2;
+  diis.init(use_diis ? so->diis_size : 0, n2);
+  RR_REQUIRE(so->diis_size <= DIIS_MAX, RR_ERR_ARG, "rr_scf_run_nonrel: diis_size too large");
+  h->work.ensure(static_cast<size_t>(std::max<int64_t>(static_cast<int64_t>(h->work.n), 8 * n2)));
+  GemmDesc g;
+  g.M = n; g.N = n; g.K = n; g.lda = n; g.ldb = n; g.ldc = n;
+  double prev = 0.0;
+  int64_t it = 0, n_mixed = 0, n_fp64 = 0;
+  bool converged = false;
+  for (it = 1; it <= so->max_iterations; ++it) {
+    // ---- Fock matrix of the current density ----
+    if (it == 1) {
+      rr_opts od{};
+      od.mem = RR_MEM_DEVICE;
+      od.stream = s;
+      od.sync = 0;
+      fock_nonrel(h, hd, P, Sd, Xd, n_eff, F, &od);
+      ++n_fp64;
+    } else if (mixed) {
+      mixed_prepare(h->mixed, h->B[0].p, h->pitch[0], n, h->naux, s);
+      mixed_exchange(h->mixed, Ct, n, nocc, K, h->status.p, s);
+      coulomb_after_ht(h, P, Ct, 0, J, nullptr, 0, s);
+      coulomb_join(h, s);
+      fock_combine(F, hd, J, K, n2, s);
+      ++n_mixed;
+    } else {
+      exchange_nonrel(h, Ct, n, false, nocc, K, s, P, J);
+      coulomb_join(h, s);
+      fock_combine(F, hd, J, K, n2, s);
+      ++n_fp64;
+    }
+    // ---- energy with the un-extrapolated F ----
+    energy_kernel<<<1, 1024, 0, s>>>(P, hd, F, n, scal);
+    RR_LAUNCH_CHECK();
+    // ---- DIIS on e = F P S - S P F ----
+    if (use_diis) {
+      g.A = P; g.B = Sd; g.C = PS; g.alpha = 1.0; g.beta = 0.0;
+      gemm(g, s, h->work.p, static_cast<int64_t>(h->work.n));
+      g.A = Sd; g.B = P; g.C = SP;
+      gemm(g, s, h->work.p, static_cast<int64_t>(h->work.n));
+      g.A = F; g.B = PS; g.C = e;
+      gemm(g, s, h->work.p, static_cast<int64_t>(h->work.n));
+      g.A = SP; g.B = F; g.C = e; g.alpha = -1.0; g.beta = 1.0;
+      gemm(g, s, h->work.p, static_cast<int64_t>(h->work.n));
+      diis.extrapolate(e, F, Fs, s);
+    } else {
+      copy_out(Fs, F, n2, false, s);
+    }
+    // ---- F_ortho = X^T F_scf X, aufbau projector, new orbitals and density ----
+    GemmDesc a;
+    a.M = n; a.N = n_eff; a.K = n; a.A = Fs; a.lda = n; a.B = Xd; a.ldb = n_eff; a.C = tmp; a.ldc = n_eff;
+    gemm(a, s, h->work.p, static_cast<int64_t>(h->work.n));
+    a.M = n_eff; a.N = n_eff; a.K = n; a.A = Xd; a.lda = n_eff; a.opA = Op::T; a.B = tmp; a.ldb = n_eff; a.C = Fo;
+    a.ldc = n_eff;
+    gemm(a, s, h->work.p, static_cast<int64_t>(h->work.n));
+    sp2_projector(h, Fo, n_eff, nocc, Pi, T2, scal + 8, s);
+    projector_ct(h, Pi, nullptr, Xd, n, n_eff, nocc, false, Ct, s);
+    GemmDesc dp;
+    dp.M = n; dp.N = n; dp.K = nocc; dp.A = Ct; dp.lda = n; dp.opA = Op::T; dp.B = Ct; dp.ldb = n; dp.C = Pn; dp.ldc = n;
+    dp.alpha = 2.0;
+    gemm(dp, s, h->work.p, static_cast<int64_t>(h->work.n));
+    maxdiff_kernel<<<1, 1024, 0, s>>>(Pn, P, n2, scal + 1);
+    RR_LAUNCH_CHECK();
+    double hv[2];
+    RR_CUDA(cudaMemcpyAsync(hv, scal, sizeof(hv), cudaMemcpyDeviceToHost, s));
+    RR_CUDA(cudaStreamSynchronize(s));
+    const double energy = hv[0], dP = hv[1], dE = std::fabs(energy - prev);
+    if (hist) hist[it - 1] = energy;
+    res->electronic_energy = energy;
+    const bool conv = it > 1 && (dP < so->density_tolerance || dE < so->energy_tolerance);
+    prev = energy;
+    if (conv && !mixed) {
+      converged = true;
+      break;
+    }
+    if (mixed && it > 1 && (dE < so->mixed_switch || conv)) mixed = false;  // finish in FP64
+    std::swap(P, Pn);
+  }
+  if (it > so->max_iterations) it = so->max_iterations;
+  check_status(h, s);
+  copy_out(P_out, P, n2, host, s);
+  RR_CUDA(cudaStreamSynchronize(s));
+  res->iterations = it;
+  res->converged = converged ? 1 : 0;
+  res->mixed_iterations = n_mixed;
+  res->fp64_iterations = n_fp64;
+  res->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+}
+
+}  // namespace rr
