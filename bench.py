@@ -44,6 +44,69 @@ def make_inputs():
     return dict(B=B, C=C, D=D, h=h, S=np.eye(N_AO), X=np.eye(N_AO))
 
 
+def make_scf_system():
+    """SCF inputs of the same shape (n=400, naux=1600, nocc=40): rerdmft_b200.synth.nonrel_system with a
+    0.5 Ha core gap and the two-electron part scaled by 8 (B by sqrt 8) so that the orbitals change
+    over the iterations (the reference's loop needs 9 of them), an overlap near identity, its
+    canonical X and the core-guess density."""
+    from rerdmft_b200 import synth
+
+    s = synth.nonrel_system(N_AO, N_AUX, N_OCC, seed=SEED + 7, box=20.0, gap=0.5)
+    s["B"] *= np.sqrt(8.0)
+    return s
+
+
+def scf_times(torch, want_cpu: bool):
+    """Time to an energy change below 1e-8 Ha on one GPU: FP64 loop vs mixed loop (split-BF16
+    exchange until |dE| < 1e-5, then FP64), plus the reference's own SCF loop on the host cores."""
+    from rerdmft_b200 import ri, scf
+
+    s = make_scf_system()
+    src = ri.RiNonRelEriSource(N_AO, s["B"], s["X"], s["S"])
+    kw = dict(energy_tolerance=1e-8, density_tolerance=1e-6)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        scf.runNonRelativisticHartreeFock(src, s["h"], s["X"], s["D0"], s["n_electrons"], precision=prec, **kw)  # warm
+        best = None
+        for _ in range(3):
+            r = scf.runNonRelativisticHartreeFock(src, s["h"], s["X"], s["D0"], s["n_electrons"], precision=prec, **kw)
+            if best is None or r["seconds"] < best["seconds"]:
+                best = r
+        out[prec] = dict(seconds=best["seconds"], energy=best["energy"], iterations=best["iterations"],
+                         converged=best["converged"], mixed_iterations=best["mixed_iterations"],
+                         fp64_iterations=best["fp64_iterations"])
+    out["mixed_over_fp64_time"] = out["mixed"]["seconds"] / out["fp64"]["seconds"]
+    out["mixed_minus_fp64_energy"] = out["mixed"]["energy"] - out["fp64"]["energy"]
+    if want_cpu:
+        from oracle import ref
+
+        if ref.available():
+            ref.set_threads(os.cpu_count() or 1)
+            t0 = time.perf_counter()
+            rr = ref.nonrel_scf(s, e_tol=1e-8, d_tol=1e-6)
+            out["reference_cpu"] = dict(seconds=time.perf_counter() - t0, energy=rr["energy"],
+                                        iterations=rr["iterations"], cores=os.cpu_count() or 1)
+            out["gpu_fp64_minus_reference_energy"] = out["fp64"]["energy"] - rr["energy"]
+    src.store.close()
+    return out
+
+
+def max_over_ranks(pg, seconds: float, device: str) -> float:
+    """The job's time: the slowest rank's (all-reduce MAX of one float; unchanged with one rank)."""
+    if pg is None:
+        return seconds
+    import torch
+
+    tt = torch.tensor([seconds], dtype=torch.float64, device=device)
+    pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+    return float(tt.item())
+
+
+def replica_throughput(world_size: int, steps: int, seconds: float) -> float:
+    """Whole-job builds/s: every replica runs `steps` builds within the slowest rank's time."""
+    return world_size * steps / seconds
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -246,13 +309,10 @@ def main():
     torch.cuda.synchronize()
     launches = lib.rr_kernel_launches() - l0
     t = e0.elapsed_time(e1) / 1e3
-    if pg:
-        tt = torch.tensor([t], dtype=torch.float64, device="cuda")
-        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-        t = float(tt.item())
+    t = max_over_ranks(pg, t, "cuda")
     clk = clocks.stop()
     store.sync()
-    value = ws * args.steps / t
+    value = replica_throughput(ws, args.steps, t)
 
     # Phase times from profiled calls (events inside the library, same stream).
     L.check(lib.rr_ri_set_profiling(store.handle, 1))
@@ -286,11 +346,8 @@ def main():
     e1.record()
     torch.cuda.synchronize()
     te = e0.elapsed_time(e1) / 1e3
-    if pg:
-        tt = torch.tensor([te], dtype=torch.float64, device="cuda")
-        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-        te = float(tt.item())
-    e2e = dict(value=ws * args.steps / te, unit=UNIT, h2d_bytes_per_step=4 * N_AO * N_AO * 8,
+    te = max_over_ranks(pg, te, "cuda")
+    e2e = dict(value=replica_throughput(ws, args.steps, te), unit=UNIT, h2d_bytes_per_step=4 * N_AO * N_AO * 8,
                d2h_bytes_per_step=N_AO * N_AO * 8)
 
     # Roofline of the dominant kernel group.
@@ -312,6 +369,9 @@ def main():
             pg.destroy_process_group()
         return
     cpu = None if args.no_cpu_baseline else cpu_reference_rate(inp)
+    del dev, src, store
+    torch.cuda.empty_cache()
+    scf_block = scf_times(torch, want_cpu=not args.no_cpu_baseline)
     line = dict(
         metric=METRIC, value=value, unit=UNIT, n_gpus=ws, steps=args.steps, warmup=args.warmup,
         ms_per_step=1e3 * t / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
@@ -332,6 +392,7 @@ def main():
                  "algorithmic_rate_gbs": (j_bytes / (acc["coulomb_ms"] / 1e3) / 1e9) if acc.get("coulomb_ms") else None},
         kernels={"half_transform_tflops": ht_tf, "syrk_tflops_full_count": ex_tf},
         phases_ms=phases, clocks=clk, e2e=e2e, gpu_launches=int(launches), cpu_baseline=cpu,
+        time_to_1e8_ha=scf_block,
     )
     print(json.dumps(line))
     if pg:

@@ -1,0 +1,383 @@
+/* C++17 drop-in for the reference's RI overload set, written over the C ABI of librr_ri (rr_ri.h).
+ *
+ * Build: compile ONE translation unit of the reference's project as
+ *     #define RR_RI_DROPIN_DEFINE
+ *     #include "rr_ri.hpp"
+ * in place of src/NON_REL/NonRelFockMatrixRi.cpp, src/X2C_DHF/X2C_FockMatrixRi.cpp,
+ * src/UKB/UkbFockMatrixRi.cpp, src/NON_REL/NonRelSpinRiMoEri.cpp, src/UKB/RiMoEri.cpp and
+ * src/Hessian_opt/RiGemmFock.cpp, and link with -lrr_ri.  The declarations stay the reference's own
+ * headers (included below), so the SCF loops (NonRelHartreeFock.cpp:132, X2C_HF.cpp:77,
+ * C4_DHF.cpp:81), main.cpp and the functional stage compile unchanged.
+ *
+ * Behaviour kept from the reference: value semantics (results return by value in host
+ * Matrix<T>), std::runtime_error on a dimension mismatch or any library failure (the message is
+ * rr_last_error()), single-threaded callers.
+ *
+ * Residency: the reference passes the same source object (which holds B by value) on every SCF
+ * iteration.  The tensor is uploaded on first sight and reused while the source's buffer address,
+ * shape and a 64-sample fingerprint of its values stay the same; up to kCacheEntries tensors stay
+ * resident (the least recently used one is released first).
+ */
+#ifndef RR_RI_HPP
+#define RR_RI_HPP
+
+#include <complex>
+#include <cstdint>
+#include <cstring>
+#include <list>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "rr_ri.h"
+
+#include "NonRelFockMatrixRi.h"
+#include "NonRelSpinRiMoEri.h"
+#include "RiGemmFock.h"
+#include "RiMoEri.h"
+#include "UkbFockMatrixRi.h"
+#include "X2C_FockMatrixRi.h"
+
+namespace rr_dropin {
+
+inline void check(int rc) {
+  if (rc != RR_OK) throw std::runtime_error(rr_last_error());
+}
+
+inline void require(bool ok, const char* msg) {
+  if (!ok) throw std::runtime_error(msg);
+}
+
+template <typename T>
+const double* dptr(const rerdmft::Matrix<T>& m) {
+  return reinterpret_cast<const double*>(m.data());
+}
+template <typename T>
+double* dptr(rerdmft::Matrix<T>& m) {
+  return reinterpret_cast<double*>(m.data());
+}
+
+// FNV-1a over 64 evenly spaced entries (their bit patterns) and the shape.
+inline uint64_t fingerprint(const rerdmft::Matrix<double>& m) {
+  uint64_t h = 1469598103934665603ull;
+  auto mix = [&](uint64_t v) {
+    for (int b = 0; b < 8; ++b) {
+      h ^= (v >> (8 * b)) & 0xffu;
+      h *= 1099511628211ull;
+    }
+  };
+  mix(m.rows());
+  mix(m.cols());
+  const std::size_t total = m.rows() * m.cols();
+  for (std::size_t k = 0; k < 64 && total; ++k) {
+    uint64_t bits;
+    std::memcpy(&bits, m.data() + (k * (total - 1)) / 63, sizeof bits);
+    mix(bits);
+  }
+  return h;
+}
+
+struct Entry {
+  const void* a;
+  const void* b;
+  uint64_t fa, fb;
+  std::size_t nl, ns;
+  rr_ri_handle h;
+};
+
+constexpr std::size_t kCacheEntries = 4;
+
+class Cache {
+ public:
+  ~Cache() {
+    for (auto& e : entries_) rr_ri_destroy(e.h);
+  }
+  // Resident handle for one tensor (ns == 0, b == nullptr) or an LL/SS pair.
+  rr_ri_handle get(const rerdmft::Matrix<double>& A, const rerdmft::Matrix<double>* B, std::size_t nl,
+                   std::size_t ns) {
+    std::lock_guard<std::mutex> lock(mu_);
+    const uint64_t fa = fingerprint(A), fb = B ? fingerprint(*B) : 0;
+    const void* pb = B ? static_cast<const void*>(B->data()) : nullptr;
+    for (auto it = entries_.begin(); it != entries_.end(); ++it) {
+      if (it->a == A.data() && it->b == pb && it->fa == fa && it->fb == fb && it->nl == nl && it->ns == ns) {
+        entries_.splice(entries_.begin(), entries_, it);
+        return entries_.front().h;
+      }
+    }
+    rr_ri_handle h = nullptr;
+    if (B)
+      check(rr_ri_create_4c(A.data(), B->data(), static_cast<int64_t>(A.rows()), static_cast<int64_t>(nl),
+                            static_cast<int64_t>(ns), RR_MEM_HOST, &h));
+    else
+      check(rr_ri_create(A.data(), static_cast<int64_t>(A.rows()), static_cast<int64_t>(nl), RR_MEM_HOST, &h));
+    entries_.push_front(Entry{A.data(), pb, fa, fb, nl, ns, h});
+    if (entries_.size() > kCacheEntries) {
+      rr_ri_destroy(entries_.back().h);
+      entries_.pop_back();
+    }
+    return h;
+  }
+
+ private:
+  std::mutex mu_;
+  std::list<Entry> entries_;
+};
+
+inline Cache& cache() {
+  static Cache c;
+  return c;
+}
+
+// Owning wrapper of an MO handle.
+struct Mo {
+  rr_mo_handle h = nullptr;
+  Mo() = default;
+  explicit Mo(rr_mo_handle x) : h(x) {}
+  Mo(const Mo&) = delete;
+  Mo& operator=(const Mo&) = delete;
+  ~Mo() {
+    if (h) rr_mo_destroy(h);
+  }
+};
+
+inline std::vector<int64_t> to_i64(const std::vector<std::size_t>& v) {
+  return std::vector<int64_t>(v.begin(), v.end());
+}
+
+}  // namespace rr_dropin
+
+#ifdef RR_RI_DROPIN_DEFINE
+
+namespace rerdmft {
+
+// src/NON_REL/NonRelFockMatrixRi.h:39
+Matrix<double> nonRelFockMatrix(const Matrix<double>& h_core, const RiNonRelEriSource& eri,
+                                const Matrix<double>& density_matrix) {
+  const std::size_t nl = eri.nl;
+  rr_dropin::require(density_matrix.rows() == nl && density_matrix.cols() == nl,
+                     "nonRelFockMatrix (RI): density_matrix dimension does not match nl");
+  rr_dropin::require(eri.eri3_L.cols() == nl * nl, "nonRelFockMatrix (RI): eri3_L column count does not match nl^2");
+  rr_dropin::require(h_core.rows() == nl && h_core.cols() == nl && eri.overlap.rows() == nl &&
+                         eri.overlap.cols() == nl && eri.x_large.rows() == nl,
+                     "nonRelFockMatrix (RI): h_core/overlap/x_large dimensions do not match nl");
+  rr_ri_handle h = rr_dropin::cache().get(eri.eri3_L, nullptr, nl, 0);
+  Matrix<double> F(nl, nl);
+  rr_dropin::check(rr_ri_fock_nonrel(h, h_core.data(), density_matrix.data(), eri.overlap.data(),
+                                     eri.x_large.data(), static_cast<int64_t>(eri.x_large.cols()), F.data(), nullptr));
+  return F;
+}
+
+// src/X2C_DHF/X2C_FockMatrixRi.h:38
+Matrix<std::complex<double>> x2cFockMatrix(const Matrix<std::complex<double>>& h_x2c, const RiX2cEriSource& eri,
+                                           const Matrix<std::complex<double>>& density_matrix) {
+  const std::size_t n = 2 * eri.nl;
+  rr_dropin::require(density_matrix.rows() == n && density_matrix.cols() == n,
+                     "x2cFockMatrix (RI): density_matrix dimension does not match 2*nLarge");
+  rr_dropin::require(eri.eri3_L.cols() == eri.nl * eri.nl,
+                     "x2cFockMatrix (RI): eri3_L column count does not match nl^2");
+  rr_ri_handle h = rr_dropin::cache().get(eri.eri3_L, nullptr, eri.nl, 0);
+  Matrix<std::complex<double>> F(n, n);
+  rr_dropin::check(rr_ri_fock_x2c(h, rr_dropin::dptr(h_x2c), rr_dropin::dptr(density_matrix),
+                                  rr_dropin::dptr(eri.overlap), rr_dropin::dptr(eri.x_large),
+                                  static_cast<int64_t>(eri.x_large.cols()), rr_dropin::dptr(F), nullptr));
+  return F;
+}
+
+// src/UKB/UkbFockMatrixRi.h:70
+Matrix<std::complex<double>> riFockTwoElectronDirect(std::size_t nl, std::size_t ns, const Matrix<double>& eri3_LL,
+                                                      const Matrix<double>& eri3_SS,
+                                                      const Matrix<std::complex<double>>& density_ukb,
+                                                      const Matrix<std::complex<double>>& c_occ_ukb,
+                                                      const std::vector<double>& occupations) {
+  const std::size_t nu = 2 * nl + 2 * ns;
+  rr_dropin::require(density_ukb.rows() == nu && density_ukb.cols() == nu,
+                     "riFockTwoElectronDirect: density_ukb dimension does not match 2*nLarge+2*nSmall");
+  rr_dropin::require(c_occ_ukb.rows() == nu && c_occ_ukb.cols() == occupations.size(),
+                     "riFockTwoElectronDirect: c_occ_ukb dimension does not match n_ukb x occupations.size()");
+  rr_dropin::require(eri3_LL.rows() == eri3_SS.rows(),
+                     "riFockTwoElectronDirect: eri3_LL and eri3_SS do not share the same aux dimension");
+  rr_dropin::require(eri3_LL.cols() == nl * nl && eri3_SS.cols() == ns * ns,
+                     "riFockTwoElectronDirect: eri3_LL/eri3_SS column count does not match nl^2/ns^2");
+  rr_ri_handle h = rr_dropin::cache().get(eri3_LL, &eri3_SS, nl, ns);
+  Matrix<std::complex<double>> G(nu, nu);
+  rr_dropin::check(rr_ri_two_electron_ukb(h, rr_dropin::dptr(density_ukb), rr_dropin::dptr(c_occ_ukb),
+                                          static_cast<int64_t>(occupations.size()), occupations.data(),
+                                          rr_dropin::dptr(G), nullptr));
+  return G;
+}
+
+// src/UKB/UkbFockMatrixRi.h:96
+Matrix<std::complex<double>> rkbFockMatrix(const Matrix<std::complex<double>>& h_rkb, const RiDirectEriSource& eri,
+                                           const Matrix<std::complex<double>>& density_matrix) {
+  const std::size_t n_rkb = h_rkb.rows();
+  rr_dropin::require(density_matrix.rows() == n_rkb && density_matrix.cols() == n_rkb,
+                     "rkbFockMatrix (RI): density_matrix dimension does not match h_rkb");
+  rr_dropin::require(eri.v_total.rows() == 2 * eri.nl + 2 * eri.ns && eri.v_total.cols() == n_rkb &&
+                         eri.x_full.rows() == n_rkb,
+                     "rkbFockMatrix (RI): v_total/x_full dimensions are inconsistent");
+  rr_ri_handle h = rr_dropin::cache().get(eri.eri3_LL, &eri.eri3_SS, eri.nl, eri.ns);
+  Matrix<std::complex<double>> F(n_rkb, n_rkb);
+  rr_dropin::check(rr_ri_fock_rkb(h, rr_dropin::dptr(h_rkb), rr_dropin::dptr(eri.v_total),
+                                  static_cast<int64_t>(n_rkb), rr_dropin::dptr(eri.s_full),
+                                  rr_dropin::dptr(eri.x_full), static_cast<int64_t>(eri.x_full.cols()),
+                                  rr_dropin::dptr(density_matrix), rr_dropin::dptr(F), nullptr));
+  return F;
+}
+
+// src/NON_REL/NonRelSpinRiMoEri.h:101
+RiNonRelSpinMoEri buildRiNonRelSpinMoEri(const Matrix<double>& eri3_L, std::size_t n_spatial,
+                                         const Matrix<double>& c_spatial) {
+  rr_dropin::require(c_spatial.rows() == n_spatial && c_spatial.cols() == n_spatial,
+                     "buildRiNonRelSpinMoEri: c_spatial dimensions do not match n_spatial");
+  rr_dropin::require(eri3_L.cols() == n_spatial * n_spatial,
+                     "buildRiNonRelSpinMoEri: eri3_L column count does not match n_spatial*n_spatial");
+  rr_ri_handle h = rr_dropin::cache().get(eri3_L, nullptr, n_spatial, 0);
+  rr_mo_handle m = nullptr;
+  rr_dropin::check(rr_mo_build_nonrel(h, c_spatial.data(), &m, nullptr));
+  rr_dropin::Mo mo(m);
+  Matrix<double> b(eri3_L.rows(), n_spatial * n_spatial);
+  rr_dropin::check(rr_mo_copy_tensor(mo.h, b.data(), nullptr));
+  return RiNonRelSpinMoEri(n_spatial, std::move(b));
+}
+
+// src/NON_REL/NonRelSpinRiMoEri.h:57
+RiNonRelSpinMoEri RiNonRelSpinMoEri::rotated(const Matrix<double>& u) const {
+  const std::size_t n = n_spatial_;
+  rr_dropin::require(u.rows() == 2 * n && u.cols() == 2 * n,
+                     "RiNonRelSpinMoEri::rotated: u dimensions do not match 2*n_spatial");
+  rr_mo_handle src = nullptr, out = nullptr;
+  rr_dropin::check(rr_mo_from_tensor(b_.data(), static_cast<int64_t>(b_.rows()), static_cast<int64_t>(n),
+                                     RR_MO_NONREL_SPIN, RR_MEM_HOST, &src));
+  rr_dropin::Mo s(src);
+  rr_dropin::check(rr_mo_rotated(s.h, u.data(), &out, nullptr));
+  rr_dropin::Mo o(out);
+  Matrix<double> b(b_.rows(), n * n);
+  rr_dropin::check(rr_mo_copy_tensor(o.h, b.data(), nullptr));
+  return RiNonRelSpinMoEri(n, std::move(b));
+}
+
+// src/UKB/RiMoEri.h:91
+RiMoEri buildRiMoEri(const RiDirectEriSource& eri, const Matrix<std::complex<double>>& c_ukb) {
+  rr_dropin::require(c_ukb.rows() == 2 * eri.nl + 2 * eri.ns,
+                     "buildRiMoEri: c_ukb row count does not match 2*nLarge+2*nSmall");
+  rr_ri_handle h = rr_dropin::cache().get(eri.eri3_LL, &eri.eri3_SS, eri.nl, eri.ns);
+  const std::size_t nt = c_ukb.cols();
+  rr_mo_handle m = nullptr;
+  rr_dropin::check(rr_mo_build_ukb(h, rr_dropin::dptr(c_ukb), static_cast<int64_t>(nt), &m, nullptr));
+  rr_dropin::Mo mo(m);
+  Matrix<std::complex<double>> b(eri.eri3_LL.rows(), nt * nt);
+  rr_dropin::check(rr_mo_copy_tensor(mo.h, rr_dropin::dptr(b), nullptr));
+  return RiMoEri(nt, std::move(b));
+}
+
+// src/UKB/RiMoEri.h:76
+RiMoEri RiMoEri::rotated(const Matrix<std::complex<double>>& u) const {
+  const std::size_t n = n_total_;
+  rr_dropin::require(u.rows() == n && u.cols() == n, "RiMoEri::rotated: u dimensions do not match n_total");
+  rr_mo_handle src = nullptr, out = nullptr;
+  rr_dropin::check(rr_mo_from_tensor(rr_dropin::dptr(b_), static_cast<int64_t>(b_.rows()), static_cast<int64_t>(n),
+                                     RR_MO_COMPLEX, RR_MEM_HOST, &src));
+  rr_dropin::Mo s(src);
+  rr_dropin::check(rr_mo_rotated(s.h, rr_dropin::dptr(u), &out, nullptr));
+  rr_dropin::Mo o(out);
+  Matrix<std::complex<double>> b(b_.rows(), n * n);
+  rr_dropin::check(rr_mo_copy_tensor(o.h, rr_dropin::dptr(b), nullptr));
+  return RiMoEri(n, std::move(b));
+}
+
+// src/UKB/RiMoEri.h:82
+RiMoEri RiMoEri::positiveBlock(std::size_t off) const {
+  const std::size_t n = n_total_;
+  rr_dropin::require(off <= n, "RiMoEri::positiveBlock: offset exceeds n_total");
+  rr_mo_handle src = nullptr, out = nullptr;
+  rr_dropin::check(rr_mo_from_tensor(rr_dropin::dptr(b_), static_cast<int64_t>(b_.rows()), static_cast<int64_t>(n),
+                                     RR_MO_COMPLEX, RR_MEM_HOST, &src));
+  rr_dropin::Mo s(src);
+  rr_dropin::check(rr_mo_positive_block(s.h, static_cast<int64_t>(off), &out, nullptr));
+  rr_dropin::Mo o(out);
+  const std::size_t m = n - off;
+  Matrix<std::complex<double>> b(b_.rows(), m * m);
+  rr_dropin::check(rr_mo_copy_tensor(o.h, rr_dropin::dptr(b), nullptr));
+  return RiMoEri(m, std::move(b));
+}
+
+namespace rr_dropin_detail {
+
+// riHxFockGemm's checks (src/Hessian_opt/RiGemmFock.cpp:57-63, :125) with `who` naming the caller.
+template <typename T>
+Matrix<T> hx_fock(const char* who, const Matrix<T>& h, const double* bmo, std::size_t naux, std::size_t n,
+                  int32_t kind, std::size_t d, const std::vector<double>& occupations,
+                  const Matrix<double>& two_rdm_h, const Matrix<double>& two_rdm_x,
+                  const std::vector<std::size_t>& pair_of, const Matrix<double>& two_rdm_l1,
+                  const Matrix<double>& two_rdm_l2) {
+  const std::string w(who);
+  rr_dropin::require(d == h.rows(), (w + ": eri dimensions inconsistent with h").c_str());
+  rr_dropin::require(h.cols() == d, (w + ": h is not square").c_str());
+  rr_dropin::require(occupations.size() == d, (w + ": occupations size inconsistent with h").c_str());
+  rr_dropin::require(two_rdm_h.rows() == d && two_rdm_h.cols() == d && two_rdm_x.rows() == d && two_rdm_x.cols() == d,
+                     (w + ": two_rdm_h/two_rdm_x dimensions inconsistent with h").c_str());
+  const bool have_l = !pair_of.empty();
+  rr_dropin::require(!have_l || (pair_of.size() == d && two_rdm_l1.rows() == d && two_rdm_l1.cols() == d &&
+                                 two_rdm_l2.rows() == d && two_rdm_l2.cols() == d),
+                     (w + ": pair_of/two_rdm_l1/two_rdm_l2 dimensions inconsistent with h").c_str());
+  rr_mo_handle src = nullptr;
+  rr_dropin::check(rr_mo_from_tensor(bmo, static_cast<int64_t>(naux), static_cast<int64_t>(n), kind, RR_MEM_HOST,
+                                     &src));
+  rr_dropin::Mo s(src);
+  const std::vector<int64_t> po = rr_dropin::to_i64(pair_of);
+  Matrix<T> F(d, d);
+  rr_dropin::check(rr_mo_hx_fock(s.h, rr_dropin::dptr(h), occupations.data(), two_rdm_h.data(), two_rdm_x.data(),
+                                 have_l ? po.data() : nullptr, have_l ? two_rdm_l1.data() : nullptr,
+                                 have_l ? two_rdm_l2.data() : nullptr, rr_dropin::dptr(F), nullptr));
+  return F;
+}
+
+}  // namespace rr_dropin_detail
+
+// src/Hessian_opt/RiGemmFock.h:20
+Matrix<std::complex<double>> hartreeExchangeFockMatrix(const Matrix<std::complex<double>>& h, const RiMoEri& eri,
+                                                       const std::vector<double>& occupations,
+                                                       const Matrix<double>& two_rdm_h,
+                                                       const Matrix<double>& two_rdm_x,
+                                                       const std::vector<std::size_t>& pair_of,
+                                                       const Matrix<double>& two_rdm_l1,
+                                                       const Matrix<double>& two_rdm_l2) {
+  return rr_dropin_detail::hx_fock("hartreeExchangeFockMatrix", h, rr_dropin::dptr(eri.b()), eri.b().rows(),
+                                   eri.dim(), RR_MO_COMPLEX, eri.dim(), occupations, two_rdm_h, two_rdm_x, pair_of,
+                                   two_rdm_l1, two_rdm_l2);
+}
+
+// src/Hessian_opt/RiGemmFock.h:25
+Matrix<double> hartreeExchangeFockMatrix(const Matrix<double>& h, const RiNonRelSpinMoEri& eri,
+                                         const std::vector<double>& occupations, const Matrix<double>& two_rdm_h,
+                                         const Matrix<double>& two_rdm_x, const std::vector<std::size_t>& pair_of,
+                                         const Matrix<double>& two_rdm_l1, const Matrix<double>& two_rdm_l2) {
+  return rr_dropin_detail::hx_fock("hartreeExchangeFockMatrix", h, eri.b().data(), eri.b().rows(), eri.nSpatial(),
+                                   RR_MO_NONREL_SPIN, eri.dim(), occupations, two_rdm_h, two_rdm_x, pair_of,
+                                   two_rdm_l1, two_rdm_l2);
+}
+
+// src/Hessian_opt/RiGemmFock.h:30
+Matrix<std::complex<double>> jkOnlyFockMatrix(const Matrix<std::complex<double>>& h, const RiMoEri& eri,
+                                              const std::vector<double>& occupations,
+                                              const Matrix<double>& two_rdm_h, const Matrix<double>& two_rdm_x) {
+  return rr_dropin_detail::hx_fock("jkOnlyFockMatrix", h, rr_dropin::dptr(eri.b()), eri.b().rows(), eri.dim(),
+                                   RR_MO_COMPLEX, eri.dim(), occupations, two_rdm_h, two_rdm_x, {}, Matrix<double>(),
+                                   Matrix<double>());
+}
+
+// src/Hessian_opt/RiGemmFock.h:34
+Matrix<double> jkOnlyFockMatrix(const Matrix<double>& h, const RiNonRelSpinMoEri& eri,
+                                const std::vector<double>& occupations, const Matrix<double>& two_rdm_h,
+                                const Matrix<double>& two_rdm_x) {
+  return rr_dropin_detail::hx_fock("jkOnlyFockMatrix", h, eri.b().data(), eri.b().rows(), eri.nSpatial(),
+                                   RR_MO_NONREL_SPIN, eri.dim(), occupations, two_rdm_h, two_rdm_x, {},
+                                   Matrix<double>(), Matrix<double>());
+}
+
+}  // namespace rerdmft
+
+#endif  // RR_RI_DROPIN_DEFINE
+
+#endif  // RR_RI_HPP

@@ -17,7 +17,11 @@ from pathlib import Path
 import numpy as np
 
 _HERE = Path(__file__).resolve().parent
-LIB_PATH = _HERE / "_ref" / "librrref.so"
+REF_PATH = _HERE / "_ref" / "librrref.so"
+# The same reference objects with the six RI .cpp files replaced by include/rr_ri.hpp over
+# librr_ri (`make -C oracle dropin`): the reference's own loops and bridge on the GPU path.
+DROPIN_PATH = _HERE / "_ref" / "librrref_dropin.so"
+LIB_PATH = DROPIN_PATH if os.environ.get("RRREF_LIB") == "dropin" else REF_PATH
 _lib = None
 
 _i64 = ctypes.c_int64

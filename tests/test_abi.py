@@ -1,7 +1,9 @@
 """CPU checks of the C boundary: the library loads and exports every symbol declared in
-include/*.h, and argument validation that happens before any device work."""
+include/*.h, argument validation that happens before any device work, and the C++ drop-in
+(include/rr_ri.hpp) linked into the reference's own objects exports the reference's overloads."""
 import ctypes
 import re
+import subprocess
 from pathlib import Path
 
 import pytest
@@ -13,7 +15,7 @@ def _declared():
     names = set()
     for h in (ROOT / "include").glob("*.h"):
         txt = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
-        for m in re.finditer(r"\b(?:int|const char\*|void)\s+(rr_[a-z0-9_]+)\s*\(", txt):
+        for m in re.finditer(r"\b(?:int|int64_t|const char\*|void)\s+(rr_[a-z0-9_]+)\s*\(", txt):
             names.add(m.group(1))
     return names
 
@@ -42,3 +44,20 @@ def test_argument_errors_before_device_work():
     assert lib.rr_ri_create(None, 4, 3, 0, ctypes.byref(h)) == _lib.RR_ERR_ARG
     assert lib.rr_ri_info(None, None, None, None) == _lib.RR_ERR_ARG
     assert lib.rr_ri_destroy(None) == _lib.RR_OK
+
+
+def test_cpp_dropin_defines_the_reference_overloads():
+    so = ROOT / "oracle" / "_ref" / "librrref_dropin.so"
+    if not so.exists():
+        pytest.skip("oracle/_ref/librrref_dropin.so not built (make -C oracle dropin needs the reference tree)")
+    syms = subprocess.run(["nm", "-DC", "--defined-only", str(so)], capture_output=True, text=True, check=True).stdout
+    for sig in ("rerdmft::nonRelFockMatrix(rerdmft::Matrix<double> const&, rerdmft::RiNonRelEriSource const&",
+                "rerdmft::x2cFockMatrix(rerdmft::Matrix<std::complex<double> > const&, rerdmft::RiX2cEriSource const&",
+                "rerdmft::rkbFockMatrix(rerdmft::Matrix<std::complex<double> > const&, rerdmft::RiDirectEriSource const&",
+                "rerdmft::riFockTwoElectronDirect(", "rerdmft::buildRiNonRelSpinMoEri(", "rerdmft::buildRiMoEri(",
+                "rerdmft::RiNonRelSpinMoEri::rotated(", "rerdmft::RiMoEri::rotated(", "rerdmft::RiMoEri::positiveBlock(",
+                "rerdmft::hartreeExchangeFockMatrix(", "rerdmft::jkOnlyFockMatrix("):
+        assert sig in syms, sig
+    needed = subprocess.run(["readelf", "-d", str(so)], capture_output=True, text=True, check=True).stdout
+    assert "librr_ri.so" in needed
+    ctypes.CDLL(str(so))  # loads without a GPU
