@@ -121,6 +121,23 @@ int rr_ri_fock_rkb(rr_ri_handle h, const double* h_rkb, const double* v_total, i
  * the device-resident SCF loop; equal to rr_ri_fock_nonrel when D = 2 C C^T. */
 int rr_ri_jk_occupied(rr_ri_handle h, const double* C_occ, int64_t n_occ, double* J, double* K, const rr_opts* opts);
 
+/* Coulomb matrix J = B^T (B vec D) (n x n, FP64) of a 2-component handle, computed with NO device
+ * allocation: all scratch lives in one fixed 32 MiB device array inside the library (no
+ * cudaMalloc, cudaFree or allocating library call on any path).  No counterpart in the reference:
+ * it serves callers that cannot let the library allocate (a resident tensor that fills the device,
+ * streams that a cudaFree would stall, a host that owns device memory through its own pool).
+ *  - Sizes: round_up(n^2, 32) (copy of D) + round_up(n^2, 32) (J staging, host pointers only)
+ *    + round_up(naux * s, 32) (pass-1 partials, s <= 64 segments per aux row) + n^2 (one pass-2
+ *    range) doubles must fit in 4,194,304: n up to about 1150 with host pointers, 1400 with device
+ *    pointers.  Larger sizes return RR_ERR_ARG with the required count, before any device work.
+ *  - The first call on each device looks up the array's address (cudaGetSymbolAddress, which may
+ *    load the module); make that first call before any stream capture on that device.
+ *  - Nothing needs to be zeroed by the caller; the call clears the padding it reads.
+ *  - There is one array per device: calls that overlap on one device (different streams or
+ *    threads, any handles) race on it.  Order such calls on one stream or serialise them.
+ *  - opts: mem, stream and sync as for the other calls; precision must be RR_PREC_FP64. */
+int rr_ri_coulomb_noalloc(rr_ri_handle h, const double* D, double* J, const rr_opts* opts);
+
 /* ---------------- device-resident SCF loops ---------------- */
 
 typedef struct rr_scf_opts {

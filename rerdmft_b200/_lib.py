@@ -62,6 +62,7 @@ _SIGS = {
     "rr_ri_sync": (ctypes.c_int, [_vp]),
     "rr_ri_fock_nonrel": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _i64, _vp, ctypes.POINTER(Opts)]),
     "rr_ri_jk_occupied": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp, ctypes.POINTER(Opts)]),
+    "rr_ri_coulomb_noalloc": (ctypes.c_int, [_vp, _vp, _vp, ctypes.POINTER(Opts)]),
     "rr_ri_fock_x2c": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _i64, _vp, ctypes.POINTER(Opts)]),
     "rr_ri_two_electron_ukb": (ctypes.c_int, [_vp, _vp, _vp, _i64, _vp, _vp, ctypes.POINTER(Opts)]),
     "rr_ri_fock_rkb": (ctypes.c_int, [_vp, _vp, _vp, _i64, _vp, _vp, _i64, _vp, _vp, ctypes.POINTER(Opts)]),
