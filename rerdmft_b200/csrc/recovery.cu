@@ -178,6 +178,107 @@ __global__ void __launch_bounds__(32) chol_small_kernel(const double* M, int64_t
   }
 }
 
+// Same contract as chol_small_kernel for r x r matrices whose factor and inverse both fit in shared
+// memory, by one CTA of CHOL_THREADS threads with one __syncthreads per elimination step:
+//  * step j of the factorisation updates the trailing triangle with the UNSCALED column j
+//    (A[i][k] -= A[i][j] conj(A[k][j]) / d_j, spread over all threads) and, in the same phase,
+//    finishes column j-1 (scale by 1/sqrt(d), set the diagonal), which nothing reads any more;
+//  * the inverse is forward elimination on X = I with the same one-phase-per-row scheme.
+constexpr int CHOL_THREADS = 256;
+
+template <int PL>
+__global__ void __launch_bounds__(CHOL_THREADS) chol_block_kernel(const double* M, int r, double* out,
+                                                                  int want_inverse, int* status) {
+  extern __shared__ double sm[];
+  double* A = sm;                 // r x r, factor in the lower triangle
+  double* X = sm + r * r * PL;    // r x r, L^{-1}
+  double* piv = X + r * r * PL;   // r pivots d_j before the square root
+  const int t = threadIdx.x;
+  for (int e = t; e < r * r * PL; e += CHOL_THREADS) A[e] = M[e];
+  __syncthreads();
+  for (int j = 0; j <= r; ++j) {
+    if (j > 0) {  // finish column j-1 (its pivot was saved in step j-1; nothing reads the column now)
+      const int c = j - 1;
+      double d = piv[c];
+      if (!(d > 0.0)) d = 1e-300;
+      const double inv = 1.0 / sqrt(d);
+      for (int i = c + 1 + t; i < r; i += CHOL_THREADS) {
+        A[(i * r + c) * PL] *= inv;
+        if (PL == 2) A[(i * r + c) * PL + 1] *= inv;
+      }
+      if (t == 0) {
+        if (!(piv[c] > 0.0)) atomicOr(status, 1);
+        A[(c * r + c) * PL] = sqrt(d);
+        if (PL == 2) A[(c * r + c) * PL + 1] = 0.0;
+      }
+    }
+    if (j < r) {
+      double d = A[(j * r + j) * PL];  // final: step j writes only columns k > j
+      if (t == 0) piv[j] = d;
+      if (!(d > 0.0)) d = 1e-300;
+      const double inv_d = 1.0 / d;
+      const int m = r - j - 1;  // trailing triangle rows j+1..r-1, element (i, k) with k <= i
+      const int tri = m * (m + 1) / 2;
+      for (int e = t; e < tri; e += CHOL_THREADS) {
+        // e -> (a, b) with 0 <= b <= a < m, row-major over the triangle
+        int a = static_cast<int>((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
+        while (a * (a + 1) / 2 > e) --a;
+        while ((a + 1) * (a + 2) / 2 <= e) ++a;
+        const int b = e - a * (a + 1) / 2;
+        const int i = j + 1 + a, k = j + 1 + b;
+        const double ar = A[(i * r + j) * PL], ai = PL == 2 ? A[(i * r + j) * PL + 1] : 0.0;
+        const double br = A[(k * r + j) * PL], bi = PL == 2 ? A[(k * r + j) * PL + 1] : 0.0;
+        A[(i * r + k) * PL] -= (ar * br + ai * bi) * inv_d;
+        if (PL == 2) A[(i * r + k) * PL + 1] -= (ai * br - ar * bi) * inv_d;
+      }
+    }
+    __syncthreads();
+  }
+  if (!want_inverse) {
+    for (int e = t; e < r * r; e += CHOL_THREADS) {
+      const int i = e / r, k = e % r;
+      out[e * PL] = k <= i ? A[e * PL] : 0.0;
+      if (PL == 2) out[e * PL + 1] = k <= i ? A[e * PL + 1] : 0.0;
+    }
+    return;
+  }
+  for (int e = t; e < r * r; e += CHOL_THREADS) {
+    X[e * PL] = (e / r == e % r) ? 1.0 : 0.0;
+    if (PL == 2) X[e * PL + 1] = 0.0;
+  }
+  __syncthreads();
+  // Row j of X is final once divided by L[j][j]; rows i > j subtract L[i][j] / L[j][j] times the
+  // undivided row j (columns c <= j), and row j-1 is divided in the same phase.
+  for (int j = 0; j <= r; ++j) {
+    if (j > 0) {
+      const int q = j - 1;
+      const double inv = 1.0 / A[(q * r + q) * PL];
+      for (int c = t; c <= q; c += CHOL_THREADS) {
+        X[(q * r + c) * PL] *= inv;
+        if (PL == 2) X[(q * r + c) * PL + 1] *= inv;
+      }
+    }
+    if (j < r) {
+      const double inv = 1.0 / A[(j * r + j) * PL];
+      const int rows = r - j - 1, cols = j + 1;
+      for (int e = t; e < rows * cols; e += CHOL_THREADS) {
+        const int i = j + 1 + e / cols, c = e % cols;
+        const double lr = A[(i * r + j) * PL] * inv, li = PL == 2 ? A[(i * r + j) * PL + 1] * inv : 0.0;
+        const double xr = X[(j * r + c) * PL], xi = PL == 2 ? X[(j * r + c) * PL + 1] : 0.0;
+        X[(i * r + c) * PL] -= lr * xr - li * xi;
+        if (PL == 2) X[(i * r + c) * PL + 1] -= lr * xi + li * xr;
+      }
+    }
+    __syncthreads();
+  }
+  // out = (L^{-1})^dagger: out[c][i] = conj(X[i][c])
+  for (int e = t; e < r * r; e += CHOL_THREADS) {
+    const int c = e / r, i = e % r;
+    out[e * PL] = i >= c ? X[(i * r + c) * PL] : 0.0;
+    if (PL == 2) out[e * PL + 1] = i >= c ? -X[(i * r + c) * PL + 1] : 0.0;
+  }
+}
+
 int blocks_for(int64_t n) { return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 1184))); }
 
 }  // namespace
@@ -207,6 +308,9 @@ void projector_ct(rr_ri_store* h, const double* A, const double* Pe, const doubl
   ar2.commit();
   const size_t chol_smem = sizeof(double) * r * r * PL;
   const bool chol_in_smem = chol_smem <= 160 * 1024;
+  // factor + inverse + pivots in shared memory: the one-CTA kernel; else the one-warp kernel
+  const size_t block_smem = sizeof(double) * (2 * r * r * PL + r);
+  const bool chol_block = block_smem <= 160 * 1024;
   if (cplx) fill_test_matrix_kernel<2><<<blocks_for(n_eff * r * 2), 256, 0, s>>>(G, n_eff * r);
   else fill_test_matrix_kernel<1><<<blocks_for(n_eff * r), 256, 0, s>>>(G, n_eff * r);
   RR_LAUNCH_CHECK();
@@ -216,6 +320,20 @@ void projector_ct(rr_ri_store* h, const double* A, const double* Pe, const doubl
   y.A = A; y.lda = n_eff; y.B = G; y.ldb = r; y.C = Y2; y.ldc = r;
   gemm(y, s, wk, wcap);
   auto chol = [&](const double* mat, int inverse) {
+    if (chol_block) {
+      const int sm = static_cast<int>(block_smem);
+      if (cplx) {
+        auto k = chol_block_kernel<2>;
+        if (sm > 48 * 1024) RR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        k<<<1, CHOL_THREADS, sm, s>>>(mat, static_cast<int>(r), Wt, inverse, h->status.p + 1);
+      } else {
+        auto k = chol_block_kernel<1>;
+        if (sm > 48 * 1024) RR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        k<<<1, CHOL_THREADS, sm, s>>>(mat, static_cast<int>(r), Wt, inverse, h->status.p + 1);
+      }
+      RR_LAUNCH_CHECK();
+      return;
+    }
     const size_t sm = chol_in_smem ? chol_smem : 0;
     if (cplx) {
       auto k = chol_small_kernel<2>;
