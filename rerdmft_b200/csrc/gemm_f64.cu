@@ -50,7 +50,10 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-__host__ __device__ constexpr int pad_mn(int x) { return x + ((8 - x % 16) + 16) % 16; }
+// Row pitch (doubles) of the [k][m] / [k][n] tiles: a fragment load reads element (k = t, m = g)
+// for lane 4g + t, so with pitch = 4 (mod 16) every half-warp touches 16 distinct 8-byte bank pairs
+// (t * pitch + g covers 0..15); an even pitch keeps the 16-byte cp.async destinations aligned.
+__host__ __device__ constexpr int pad_mn(int x) { return x + ((4 - x % 16) + 16) % 16; }
 
 template <int MT, int NT, int WM, int WN, bool AK, bool BKM, bool CPLX>
 struct Cfg {
@@ -336,10 +339,13 @@ void launch_cfg(const Params& p, dim3 grid, cudaStream_t s) {
 
 struct Shape { int bm, bn; };
 
-template <bool AK, bool BKM>
-Shape shape_real(int64_t M) {
-  if (M <= 48) { int mt = static_cast<int>((M + 7) / 8); return {8 * mt, 128}; }
-  return {64, 64};
+// Square tiles for M > 48: 80 x 80 (5 x 5 fragments per warp) for long-K products (the exchange
+// SYRK) when it covers M x N with less padding than 64 x 64 (n = 400: 400^2 instead of 448^2
+// computed); short-K products keep 64 x 64, whose larger CTA count hides their latency better.
+bool use_tile80(int64_t M, int64_t N, int64_t K) {
+  const int64_t p64 = static_cast<int64_t>(ceil_div(M, 64)) * 64 * ceil_div(N, 64) * 64;
+  const int64_t p80 = static_cast<int64_t>(ceil_div(M, 80)) * 80 * ceil_div(N, 80) * 80;
+  return K >= 8192 && p80 < p64;
 }
 
 template <bool AK, bool BKM>
@@ -354,12 +360,14 @@ void launch_real(const Params& p, dim3 grid, cudaStream_t s) {
       default: return launch_cfg<6, 4, 1, 4, AK, BKM, false>(p, grid, s);
     }
   }
+  if (use_tile80(p.M, p.N, p.K)) return launch_cfg<5, 5, 2, 2, AK, BKM, false>(p, grid, s);
   launch_cfg<4, 4, 2, 2, AK, BKM, false>(p, grid, s);
 }
 
 Shape pick_shape(const GemmDesc& d) {
   if (d.cplx) return {32, 64};
   if (d.M <= 48) return {static_cast<int>(8 * ((d.M + 7) / 8)), 128};
+  if (use_tile80(d.M, d.N, d.K)) return {80, 80};
   return {64, 64};
 }
 
