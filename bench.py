@@ -29,6 +29,9 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 N_AO, N_AUX, N_OCC, SEED = 400, 1600, 40, 2024
+# DRAM bytes (read + write) of one half-transform launch at this workload, from the ncu capture in
+# profiles/dgemm_half_transform_n400_naux1600_nocc40.md (B read once, T written once).
+HT_TRAFFIC_BYTES = 2.048573e9 + 0.198356e9
 METRIC = "RI J+K Fock builds/s"
 UNIT = "builds/s"
 
@@ -379,10 +382,16 @@ def main():
         config={"workload": f"nonrel RI J+K Fock build n={N_AO} naux={N_AUX} nocc={N_OCC} (FP64, occupied recovery "
                             f"included)", "parallelism": f"replicas x{ws}", "precision": "fp64",
                 "l2": "inputs larger than L2 (B = 2.05 GB)"},
-        roofline={"bound": "tensor", "kernel": "exchange (FP64 DMMA half-transform + SYRK)",
-                  "achieved": k_tf, "peak": fp64_peak, "unit": "TFLOP/s",
-                  "frac": (k_tf / fp64_peak) if (k_tf and fp64_peak) else None, "traffic": None,
+        roofline={"bound": "tensor", "kernel": "dgemm_kernel half-transform T^P = Ct B^P (FP64 DMMA, 45% of a build)",
+                  "achieved": ht_tf, "peak": fp64_peak, "unit": "TFLOP/s",
+                  "frac": (ht_tf / fp64_peak) if (ht_tf and fp64_peak) else None, "traffic": HT_TRAFFIC_BYTES,
+                  "traffic_source": "dram read+write of one launch, ncu capture in "
+                                    "profiles/dgemm_half_transform_n400_naux1600_nocc40.md",
+                  "algorithmic_bytes": 8.0 * N_AUX * (N_AO * N_AO + N_OCC * N_AO),
                   "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 has no entry in MEASURED_PEAKS.json)",
+                  "algorithmic": "2*naux*nocc*n^2 flops per launch (one launch per build)"},
+        exchange={"bound": "tensor", "kernel": "half-transform + SYRK (FP64 DMMA)", "achieved": k_tf,
+                  "peak": fp64_peak, "unit": "TFLOP/s", "frac": (k_tf / fp64_peak) if (k_tf and fp64_peak) else None,
                   "algorithmic": "4*naux*nocc*n^2 flops per build (half-transform + full-count SYRK)"},
         coulomb={"bound": "hbm", "achieved": j_gbs, "peak": hbm_peak, "unit": "GB/s",
                  "frac": (j_gbs / hbm_peak) if j_gbs else None, "peak_source": hbm_src,
