@@ -59,6 +59,69 @@ def make_scf_system():
     return s
 
 
+NL4, NS4, NAUX4, NOCC4 = 200, 600, 1000, 40
+
+
+def rkb_fock_times(torch, fp64_peak, want_cpu: bool, steps: int = 10):
+    """4-component Kramers-restricted RKB Fock build (rkbFockMatrix) at nl=200, ns=600, naux=1000,
+    20 Kramers pairs: LL and SS tensors by the cube/Gaussian recipe (20-bohr cube), device-resident,
+    timed with CUDA events; the reference's own rkbFockMatrix timed once on the host cores."""
+    import ctypes
+
+    from rerdmft_b200 import _lib as L
+    from rerdmft_b200 import ri, synth
+
+    s = synth.rkb_system(NL4, NS4, NAUX4, 2 * (NOCC4 // 2), seed=SEED + 11, box=20.0)
+    dev = {k: torch.from_numpy(np.ascontiguousarray(s[k])).cuda()
+           for k in ("B_LL", "B_SS", "v_total", "s_full", "x_full", "h", "P0")}
+    src = ri.RiDirectEriSource(NL4, NS4, dev["B_LL"], dev["B_SS"], dev["v_total"], dev["s_full"], dev["x_full"])
+    store = src.store
+    lib = L.lib()
+    n_rkb = s["n_rkb"]
+    F = torch.empty((n_rkb, n_rkb), dtype=torch.complex128, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    o = L.opts(L.RR_MEM_DEVICE, stream=stream, sync=0)
+    x = dev["x_full"]
+
+    def step():
+        L.check(lib.rr_ri_fock_rkb(store.handle, dev["h"].data_ptr(), dev["v_total"].data_ptr(), n_rkb,
+                                   dev["s_full"].data_ptr(), x.data_ptr(), x.shape[1], dev["P0"].data_ptr(),
+                                   F.data_ptr(), ctypes.byref(o)))
+
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    store.sync()
+    ms = e0.elapsed_time(e1) / steps
+    fl = [NL4, NL4, NS4, NS4]
+    pair = sum(fl[f] * fl[u] for f in range(4) for u in range(f, 4))
+    flops = 4.0 * NOCC4 * (2 * NL4 ** 2 + 2 * NS4 ** 2) * NAUX4 + 8.0 * NOCC4 * pair * NAUX4
+    tf = flops / (ms / 1e3) / 1e12
+    out = dict(workload=f"rkbFockMatrix nl={NL4} ns={NS4} naux={NAUX4} nocc={NOCC4} spinors (FP64 complex)",
+               ms_per_build=ms, builds_per_s=1e3 / ms, algorithmic_gflop=flops / 1e9, achieved_tflops=tf,
+               frac_of_dgemm=(tf / fp64_peak) if fp64_peak else None,
+               j_bytes=2.0 * NAUX4 * (NL4 ** 2 + NS4 ** 2) * 8)
+    if want_cpu:
+        from oracle import ref
+
+        if ref.available():
+            ref.set_threads(os.cpu_count() or 1)
+            t0 = time.perf_counter()
+            ref.rkb_fock(s["h"], NL4, NS4, s["B_LL"], s["B_SS"], s["v_total"], s["s_full"], s["x_full"], s["P0"])
+            dt = time.perf_counter() - t0
+            out["reference_cpu"] = dict(seconds_per_build=dt, cores=os.cpu_count() or 1,
+                                        sample="one full-size call of the reference rkbFockMatrix")
+    del dev, src, store, F
+    torch.cuda.empty_cache()
+    return out
+
+
 def scf_times(torch, want_cpu: bool):
     """Time to an energy change below 1e-8 Ha on one GPU: FP64 loop vs mixed loop (split-BF16
     exchange until |dE| < 1e-5, then FP64), plus the reference's own SCF loop on the host cores."""
@@ -375,6 +438,7 @@ def main():
     del dev, src, store
     torch.cuda.empty_cache()
     scf_block = scf_times(torch, want_cpu=not args.no_cpu_baseline)
+    rkb_block = rkb_fock_times(torch, fp64_peak, want_cpu=not args.no_cpu_baseline)
     line = dict(
         metric=METRIC, value=value, unit=UNIT, n_gpus=ws, steps=args.steps, warmup=args.warmup,
         ms_per_step=1e3 * t / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
@@ -402,6 +466,7 @@ def main():
         kernels={"half_transform_tflops": ht_tf, "syrk_tflops_full_count": ex_tf},
         phases_ms=phases, clocks=clk, e2e=e2e, gpu_launches=int(launches), cpu_baseline=cpu,
         time_to_1e8_ha=scf_block,
+        rkb_fock_4c=rkb_block,
     )
     print(json.dumps(line))
     if pg:

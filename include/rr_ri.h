@@ -148,8 +148,8 @@ typedef struct rr_scf_opts {
   int32_t kramers_restricted; /* X2C / 4c: project densities onto their time-reversal-even part */
   int32_t precision;          /* RR_PREC_FP64 or RR_PREC_MIXED (split-BF16 exchange, FP64 for the last iterations) */
   double mixed_switch;        /* RR_PREC_MIXED: switch to FP64 builds once |dE| < mixed_switch */
-  int32_t reserved0;
-  int32_t reserved1;
+  double mixing;              /* without DIIS (diis_size < 2): next density = mixing P_new + (1 - mixing) P,
+                                 the reference's linear mixing; 0 is taken as 1 */
 } rr_scf_opts;
 
 typedef struct rr_scf_result {
@@ -164,12 +164,34 @@ typedef struct rr_scf_result {
 /* Restricted nonrelativistic SCF with the RI Fock build, DIIS on e = FPS - SPF and the aufbau
  * density from the lowest n_electrons/2 eigenvectors of X^T F X (obtained by SP2 purification on
  * the GPU).  Replaces runNonRelativisticHartreeFock(RiNonRelEriSource, ...),
- * src/NON_REL/NonRelHartreeFock.cpp:117-198/219 (nuclear repulsion is the caller's; no mixing:
- * DIIS replaces it as in the reference).  energy_history (optional) receives one electronic energy
- * per iteration (max_iterations doubles); P_out the density of the last iteration. */
+ * src/NON_REL/NonRelHartreeFock.cpp:117-198/219 (nuclear repulsion is the caller's; DIIS replaces
+ * the linear mixing as in the reference).  energy_history (optional) receives one electronic
+ * energy per iteration (max_iterations doubles); P_out the density of the last iteration. */
 int rr_scf_run_nonrel(rr_ri_handle h, const double* h_core, const double* X, int64_t n_eff, const double* S,
                       const double* P0, int32_t n_electrons, const rr_scf_opts* scf, rr_scf_result* result,
                       double* P_out, double* energy_history, const rr_opts* opts);
+
+/* X2C-HF SCF on a 2-component handle: runX2CHartreeFockScf(h_x2c, RiX2cEriSource, x_large, P0,
+ * n_electrons, ..., overlap, diis, ...), src/X2C_DHF/X2C_HF.cpp:43-138.  Complex interleaved
+ * matrices: h_x2c, S, P0 (2nl x 2nl), X (2nl x n_eff).  Per iteration: F = x2cFockMatrix(P) on the
+ * GPU, E = 1/2 Re Tr[P (h + F)], DIIS on e = FPS - SPF, P_new = X Pi X^dagger with Pi the SP2
+ * projector onto the lowest n_electrons eigenvectors of X^dagger F X (one electron per spinor),
+ * Kramers projection of every density ([alpha; beta] layout) when kramers_restricted and
+ * n_electrons is even. */
+int rr_scf_run_x2c(rr_ri_handle h, const double* h_x2c, const double* X, int64_t n_eff, const double* S,
+                   const double* P0, int32_t n_electrons, const rr_scf_opts* scf, rr_scf_result* result,
+                   double* P_out, double* energy_history, const rr_opts* opts);
+
+/* 4-component DHF SCF on a 4c handle: runDiracHartreeFockScf(h_rkb, RiDirectEriSource, x_full, P0,
+ * n_electrons, ..., s_full, diis, ...), src/C4_DHF/C4_DHF.cpp:45-142.  Complex interleaved: h_rkb,
+ * s_full, P0 (n_rkb x n_rkb), v_total (n_ukb x n_rkb), x_full (n_rkb x n_rkb: rkbDensityMatrix
+ * needs the full basis).  F = rkbFockMatrix(P) on the GPU; the density fills the n_electrons
+ * positive-energy spinors above the n_rkb/2 negative-energy ones (RkbDensityMatrix.cpp:16-43):
+ * P_new = X (Pi_{n_rkb/2 + n_e} - Pi_{n_rkb/2}) X^dagger from two SP2 projectors; Kramers
+ * projection in the [L-alpha; L-beta; S-alpha; S-beta] layout. */
+int rr_scf_run_dhf(rr_ri_handle h, const double* h_rkb, const double* v_total, int64_t n_rkb, const double* s_full,
+                   const double* x_full, const double* P0, int32_t n_electrons, const rr_scf_opts* scf,
+                   rr_scf_result* result, double* P_out, double* energy_history, const rr_opts* opts);
 
 /* ---------------- MO-basis RI tensors (functional stage) ---------------- */
 

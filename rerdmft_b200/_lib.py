@@ -44,7 +44,7 @@ class Timings(ctypes.Structure):
 class ScfOpts(ctypes.Structure):
     _fields_ = [("diis_size", _i32), ("max_iterations", _i32), ("energy_tolerance", _d),
                 ("density_tolerance", _d), ("kramers_restricted", _i32), ("precision", _i32),
-                ("mixed_switch", _d), ("reserved0", _i32), ("reserved1", _i32)]
+                ("mixed_switch", _d), ("mixing", _d)]
 
 
 class ScfResult(ctypes.Structure):
@@ -80,6 +80,10 @@ _SIGS = {
     "rr_mo_hx_fock": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(Opts)]),
     "rr_scf_run_nonrel": (ctypes.c_int, [_vp, _vp, _vp, _i64, _vp, _vp, _i32, ctypes.POINTER(ScfOpts),
                                          ctypes.POINTER(ScfResult), _vp, _vp, ctypes.POINTER(Opts)]),
+    "rr_scf_run_x2c": (ctypes.c_int, [_vp, _vp, _vp, _i64, _vp, _vp, _i32, ctypes.POINTER(ScfOpts),
+                                      ctypes.POINTER(ScfResult), _vp, _vp, ctypes.POINTER(Opts)]),
+    "rr_scf_run_dhf": (ctypes.c_int, [_vp, _vp, _vp, _i64, _vp, _vp, _vp, _i32, ctypes.POINTER(ScfOpts),
+                                      ctypes.POINTER(ScfResult), _vp, _vp, ctypes.POINTER(Opts)]),
     "rr_ri_set_profiling": (ctypes.c_int, [_vp, _i32]),
     "rr_ri_get_timings": (ctypes.c_int, [_vp, ctypes.c_void_p]),
     "rr_kernel_launches": (ctypes.c_int64, []),

@@ -16,6 +16,8 @@ void fock_rkb(rr_ri_store*, const double*, const double*, int64_t, const double*
               const double*, double*, const rr_opts*);
 void scf_nonrel(rr_ri_store*, const double*, const double*, int64_t, const double*, const double*, int,
                 const rr_scf_opts*, rr_scf_result*, double*, double*, const rr_opts*);
+void scf_rel(rr_ri_store*, int, const double*, const double*, int64_t, const double*, int64_t, const double*,
+             const double*, int, const rr_scf_opts*, rr_scf_result*, double*, double*, const rr_opts*);
 }  // namespace rr
 
 namespace {
@@ -250,6 +252,40 @@ int rr_scf_run_nonrel(rr_ri_handle h, const double* h_core, const double* X, int
                "rr_scf_run_nonrel: unknown precision");
     *result = rr_scf_result{};
     rr::scf_nonrel(s, h_core, X, n_eff, S, P0, n_electrons, scf, result, P_out, energy_history, opts);
+  });
+}
+
+int rr_scf_run_x2c(rr_ri_handle h, const double* h_x2c, const double* X, int64_t n_eff, const double* S,
+                   const double* P0, int32_t n_electrons, const rr_scf_opts* scf, rr_scf_result* result,
+                   double* P_out, double* energy_history, const rr_opts* opts) {
+  return api([&] {
+    auto* s = checked(h);
+    RR_REQUIRE(s->ntens == 1, RR_ERR_STATE, "rr_scf_run_x2c: handle holds a 4-component store");
+    RR_REQUIRE(h_x2c && X && S && P0 && scf && result && P_out, RR_ERR_ARG, "rr_scf_run_x2c: null argument");
+    RR_REQUIRE(n_eff >= 1 && n_eff <= 2 * s->n, RR_ERR_ARG, "rr_scf_run_x2c: n_eff out of range");
+    RR_REQUIRE(scf->max_iterations >= 1, RR_ERR_ARG, "rr_scf_run_x2c: max_iterations < 1");
+    RR_REQUIRE(scf->precision == RR_PREC_FP64, RR_ERR_UNSUPPORTED, "rr_scf_run_x2c: precision");
+    *result = rr_scf_result{};
+    rr::scf_rel(s, 0, h_x2c, nullptr, 2 * s->n, X, n_eff, S, P0, n_electrons, scf, result, P_out, energy_history,
+                opts);
+  });
+}
+
+int rr_scf_run_dhf(rr_ri_handle h, const double* h_rkb, const double* v_total, int64_t n_rkb, const double* s_full,
+                   const double* x_full, const double* P0, int32_t n_electrons, const rr_scf_opts* scf,
+                   rr_scf_result* result, double* P_out, double* energy_history, const rr_opts* opts) {
+  return api([&] {
+    auto* s = checked(h);
+    RR_REQUIRE(s->ntens == 2, RR_ERR_STATE, "rr_scf_run_dhf: needs a 4-component store (rr_ri_create_4c)");
+    RR_REQUIRE(h_rkb && v_total && s_full && x_full && P0 && scf && result && P_out, RR_ERR_ARG,
+               "rr_scf_run_dhf: null argument");
+    RR_REQUIRE(n_rkb >= 4 && n_rkb % 4 == 0, RR_ERR_ARG,
+               "rkbDensityMatrix: RKB basis dimension must be even (4*nLarge)");
+    RR_REQUIRE(scf->max_iterations >= 1, RR_ERR_ARG, "rr_scf_run_dhf: max_iterations < 1");
+    RR_REQUIRE(scf->precision == RR_PREC_FP64, RR_ERR_UNSUPPORTED, "rr_scf_run_dhf: precision");
+    *result = rr_scf_result{};
+    rr::scf_rel(s, 1, h_rkb, v_total, n_rkb, x_full, n_rkb, s_full, P0, n_electrons, scf, result, P_out,
+                energy_history, opts);
   });
 }
 

@@ -60,7 +60,7 @@ cudaStream_t call_stream(rr_ri_store* h, const rr_opts* o);
 void prof_mark(rr_ri_store* h, int i, cudaStream_t s);
 int64_t launches();
 void sp2_projector(rr_ri_store* h, const double* F, int64_t n, int64_t nocc, double* Pi, double* T, double* scal,
-                   cudaStream_t s);
+                   cudaStream_t s, bool cplx = false);
 void check_status(rr_ri_store* h, cudaStream_t s);  // syncs s, throws RR_ERR_TIMEOUT on a set word
 void copy_in(double* dst, const double* src, int64_t count, bool host, cudaStream_t s);
 void copy_out(double* dst, const double* src, int64_t count, bool host, cudaStream_t s);

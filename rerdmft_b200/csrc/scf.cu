@@ -33,6 +33,10 @@ void fock_nonrel(rr_ri_store* h, const double* hc, const double* D, const double
                  double* F, const rr_opts* o);
 void projector_ct(rr_ri_store* h, const double* A, const double* Pe, const double* X, int64_t n, int64_t n_eff,
                   int64_t r, bool cplx, double* Ct, cudaStream_t s);
+void fock_x2c(rr_ri_store* h, const double* hc, const double* P, const double* S, const double* X, int64_t n_eff,
+              double* F, const rr_opts* o);
+void fock_rkb(rr_ri_store* h, const double* hc, const double* v, int64_t n_rkb, const double* s_full,
+              const double* x_full, int64_t n_eff, const double* P, double* F, const rr_opts* o);
 
 namespace {
 
@@ -49,16 +53,18 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
   return t;
 }
 
-// Gershgorin bounds of a symmetric n x n matrix: out[0] = min_i (a_ii - r_i), out[1] = max (a_ii + r_i).
+// Gershgorin bounds of a symmetric / Hermitian n x n matrix (PL = 2: interleaved complex):
+// out[0] = min_i (a_ii - r_i), out[1] = max (a_ii + r_i), r_i = sum_{j != i} |a_ij|.
+template <int PL>
 __global__ void gershgorin_kernel(const double* A, int64_t n, double* out) {
   __shared__ double lo_s[32], hi_s[32];
   double lo = 1e300, hi = -1e300;
   for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
     double r = 0.0;
     for (int64_t j = 0; j < n; ++j)
-      if (j != i) r += fabs(A[i * n + j]);
-    lo = fmin(lo, A[i * n + i] - r);
-    hi = fmax(hi, A[i * n + i] + r);
+      if (j != i) r += PL == 2 ? hypot(A[(i * n + j) * PL], A[(i * n + j) * PL + 1]) : fabs(A[i * n + j]);
+    lo = fmin(lo, A[(i * n + i) * PL] - r);
+    hi = fmax(hi, A[(i * n + i) * PL] + r);
   }
   for (int o = 16; o > 0; o >>= 1) {
     lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
@@ -74,60 +80,85 @@ __global__ void gershgorin_kernel(const double* A, int64_t n, double* out) {
 }
 
 // X = (emax I - F) / (emax - emin): spectrum mapped into [0, 1], lowest states near 1.
+template <int PL>
 __global__ void sp2_init_kernel(double* X, const double* F, int64_t n, const double* b) {
   const double emin = b[0], emax = b[1], inv = 1.0 / fmax(emax - emin, 1e-300);
   for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < n * n;
        idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int64_t i = idx / n, j = idx % n;
-    X[idx] = ((i == j ? emax : 0.0) - F[idx]) * inv;
+    X[idx * PL] = ((i == j ? emax : 0.0) - F[idx * PL]) * inv;
+    if (PL == 2) X[idx * PL + 1] = -F[idx * PL + 1] * inv;
   }
 }
 
-// tr[0] = trace X, tr[1] = trace T (one CTA).
+// tr[0] = Re trace X, tr[1] = Re trace T (one CTA).
+template <int PL>
 __global__ void two_traces_kernel(const double* X, const double* T, int64_t n, double* tr) {
   __shared__ double red[32];
   double a = 0.0, b = 0.0;
   for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
-    a += X[i * n + i];
-    b += T[i * n + i];
+    a += X[(i * n + i) * PL];
+    b += T[(i * n + i) * PL];
   }
   a = block_sum(a, red);
   b = block_sum(b, red);
   if (threadIdx.x == 0) { tr[0] = a; tr[1] = b; }
 }
 
-// SP2 step (trace correcting): X <- X^2 if that brings the trace closer to N, else 2X - X^2.
-__global__ void sp2_update_kernel(double* X, const double* T, int64_t n, const double* tr, double N) {
+// SP2 step (trace correcting): X <- X^2 if that brings the trace closer to N, else 2X - X^2
+// (elementwise over `cnt` doubles, so it serves interleaved complex matrices as well).
+__global__ void sp2_update_kernel(double* X, const double* T, int64_t cnt, const double* tr, double N) {
   const double trx = tr[0], trt = tr[1];
   const bool square = fabs(trt - N) < fabs(2.0 * trx - trt - N);
-  for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < n * n;
+  for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < cnt;
        idx += static_cast<int64_t>(gridDim.x) * blockDim.x)
     X[idx] = square ? T[idx] : 2.0 * X[idx] - T[idx];
 }
 
-// out[0] = Tr[P A^T-free]: sum_ij P_ij (h + F)_ji  (energy trace), one CTA
+// out[0] = 1/2 Re Tr[P (h + F)] = 1/2 Re sum_ij P_ij (h + F)_ji  (one CTA)
+template <int PL>
 __global__ void energy_kernel(const double* P, const double* h, const double* F, int64_t n, double* out) {
   __shared__ double red[32];
   double acc = 0.0;
   for (int64_t idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
-    const int64_t i = idx / n, j = idx % n;
-    acc += P[idx] * (h[j * n + i] + F[j * n + i]);
+    const int64_t i = idx / n, j = idx % n, t = j * n + i;
+    acc += P[idx * PL] * (h[t * PL] + F[t * PL]);
+    if (PL == 2) acc -= P[idx * PL + 1] * (h[t * PL + 1] + F[t * PL + 1]);
   }
   acc = block_sum(acc, red);
   if (threadIdx.x == 0) out[0] = 0.5 * acc;
 }
 
-// out[0] = max |A - B| (one CTA)
+// out[0] = max |A - B| over cnt (complex) elements (one CTA)
+template <int PL>
 __global__ void maxdiff_kernel(const double* A, const double* B, int64_t cnt, double* out) {
   __shared__ double red[32];
   double m = 0.0;
-  for (int64_t i = threadIdx.x; i < cnt; i += blockDim.x) m = fmax(m, fabs(A[i] - B[i]));
+  for (int64_t i = threadIdx.x; i < cnt; i += blockDim.x)
+    m = fmax(m, PL == 2 ? hypot(A[2 * i] - B[2 * i], A[2 * i + 1] - B[2 * i + 1]) : fabs(A[i] - B[i]));
   for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
   __syncthreads();
   if (threadIdx.x == 0) {
     for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
     out[0] = m;
+  }
+}
+
+// Time-reversal-even part of a complex n x n matrix in a layout of equal spin blocks of length nb
+// alternating alpha / beta ([alpha; beta] X2C AO layout: nb = n/2, src/Utils/KramersPairing.cpp:320;
+// [L-alpha; L-beta; S-alpha; S-beta] RKB layout: nb = n/4, :351):
+//   out(a, b) = 1/2 (P(a, b) + s_a s_b conj(P(partner a, partner b))),
+// partner = the other block of the alpha/beta pair, s = +1 on alpha blocks, -1 on beta blocks.
+__global__ void kramers_even_kernel(double* out, const double* P, int64_t n, int64_t nb) {
+  for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < n * n;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t a = idx / n, b = idx % n;
+    const int64_t pa = ((a / nb) ^ 1) * nb + a % nb, pb = ((b / nb) ^ 1) * nb + b % nb;
+    const double sg = (((a / nb) % 2 == 0) ? 1.0 : -1.0) * (((b / nb) % 2 == 0) ? 1.0 : -1.0);
+    const int64_t q = pa * n + pb;
+    out[2 * idx] = 0.5 * (P[2 * idx] + sg * P[2 * q]);
+    out[2 * idx + 1] = 0.5 * (P[2 * idx + 1] - sg * P[2 * q + 1]);
   }
 }
 
@@ -264,23 +295,33 @@ struct DeviceDiis {
 }  // namespace
 
 // SP2 purification: projector (n x n, into Pi) onto the lowest `nocc` eigenvectors of the symmetric
-// F (n x n).  T is scratch (n x n).  Host checks every 4 steps; at most 120 steps.
+// (Hermitian when cplx, interleaved) F (n x n).  T is scratch (n x n).  Host checks every 4 steps;
+// at most 120 steps.
 void sp2_projector(rr_ri_store* h, const double* F, int64_t n, int64_t nocc, double* Pi, double* T, double* scal,
-                   cudaStream_t s) {
-  gershgorin_kernel<<<1, 512, 0, s>>>(F, n, scal);
-  RR_LAUNCH_CHECK();
-  sp2_init_kernel<<<blocks_for(n * n), 256, 0, s>>>(Pi, F, n, scal);
+                   cudaStream_t s, bool cplx) {
+  const int PL = cplx ? 2 : 1;
+  if (cplx) {
+    gershgorin_kernel<2><<<1, 512, 0, s>>>(F, n, scal);
+    RR_LAUNCH_CHECK();
+    sp2_init_kernel<2><<<blocks_for(n * n), 256, 0, s>>>(Pi, F, n, scal);
+  } else {
+    gershgorin_kernel<1><<<1, 512, 0, s>>>(F, n, scal);
+    RR_LAUNCH_CHECK();
+    sp2_init_kernel<1><<<blocks_for(n * n), 256, 0, s>>>(Pi, F, n, scal);
+  }
   RR_LAUNCH_CHECK();
   GemmDesc g;
+  g.cplx = cplx;
   g.M = n; g.N = n; g.K = n;
   g.A = Pi; g.lda = n; g.B = Pi; g.ldb = n; g.C = T; g.ldc = n;
-  h->work.ensure(static_cast<size_t>(std::max<int64_t>(static_cast<int64_t>(h->work.n), 8 * n * n)));
+  h->work.ensure(static_cast<size_t>(std::max<int64_t>(static_cast<int64_t>(h->work.n), 8 * n * n * PL)));
   const double N = static_cast<double>(nocc);
   for (int it = 0; it < 120; ++it) {
     gemm(g, s, h->work.p, static_cast<int64_t>(h->work.n));
-    two_traces_kernel<<<1, 512, 0, s>>>(Pi, T, n, scal + 2);
+    if (cplx) two_traces_kernel<2><<<1, 512, 0, s>>>(Pi, T, n, scal + 2);
+    else two_traces_kernel<1><<<1, 512, 0, s>>>(Pi, T, n, scal + 2);
     RR_LAUNCH_CHECK();
-    sp2_update_kernel<<<blocks_for(n * n), 256, 0, s>>>(Pi, T, n, scal + 2, N);
+    sp2_update_kernel<<<blocks_for(n * n * PL), 256, 0, s>>>(Pi, T, n * n * PL, scal + 2, N);
     RR_LAUNCH_CHECK();
     if (it % 4 == 3) {
       double tr[2];
@@ -367,7 +408,7 @@ void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff
       ++n_fp64;
     }
     // ---- energy with the un-extrapolated F ----
-    energy_kernel<<<1, 1024, 0, s>>>(P, hd, F, n, scal);
+    energy_kernel<1><<<1, 1024, 0, s>>>(P, hd, F, n, scal);
     RR_LAUNCH_CHECK();
     // ---- DIIS on e = F P S - S P F ----
     if (use_diis) {
@@ -390,13 +431,13 @@ void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff
     a.M = n_eff; a.N = n_eff; a.K = n; a.A = Xd; a.lda = n_eff; a.opA = Op::T; a.B = tmp; a.ldb = n_eff; a.C = Fo;
     a.ldc = n_eff;
     gemm(a, s, h->work.p, static_cast<int64_t>(h->work.n));
-    sp2_projector(h, Fo, n_eff, nocc, Pi, T2, scal + 8, s);
+    sp2_projector(h, Fo, n_eff, nocc, Pi, T2, scal + 8, s, false);
     projector_ct(h, Pi, nullptr, Xd, n, n_eff, nocc, false, Ct, s);
     GemmDesc dp;
     dp.M = n; dp.N = n; dp.K = nocc; dp.A = Ct; dp.lda = n; dp.opA = Op::T; dp.B = Ct; dp.ldb = n; dp.C = Pn; dp.ldc = n;
     dp.alpha = 2.0;
     gemm(dp, s, h->work.p, static_cast<int64_t>(h->work.n));
-    maxdiff_kernel<<<1, 1024, 0, s>>>(Pn, P, n2, scal + 1);
+    maxdiff_kernel<1><<<1, 1024, 0, s>>>(Pn, P, n2, scal + 1);
     RR_LAUNCH_CHECK();
     double hv[2];
     RR_CUDA(cudaMemcpyAsync(hv, scal, sizeof(hv), cudaMemcpyDeviceToHost, s));
@@ -411,6 +452,10 @@ void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff
       break;
     }
     if (mixed && it > 1 && (dE < so->mixed_switch || conv)) mixed = false;  // finish in FP64
+    if (!use_diis && so->mixing > 0.0 && so->mixing != 1.0) {
+      // linear mixing: only the density of the next build changes (NonRelHartreeFock.cpp:185-195)
+      axpby(Pn, P, 1.0 - so->mixing, so->mixing, n2, s);
+    }
     std::swap(P, Pn);
   }
   if (it > so->max_iterations) it = so->max_iterations;
@@ -421,6 +466,148 @@ void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff
   res->converged = converged ? 1 : 0;
   res->mixed_iterations = n_mixed;
   res->fp64_iterations = n_fp64;
+  res->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+}
+
+// X2C-HF (kind 0) and 4c-DHF (kind 1) SCF loops on the device (X2C_HF.cpp:43-138,
+// C4_DHF.cpp:45-142).  Matrices are complex interleaved.  The Fock build is the drop-in one
+// (x2cFockMatrix / rkbFockMatrix, occupied recovery from the density included); the new density is
+// X Pi X^dagger with Pi from SP2 (X2C: lowest n_e states; DHF: the n_e states above the n/2
+// negative-energy ones, as the difference of two projectors).
+void scf_rel(rr_ri_store* h, int kind, const double* hc, const double* v_total, int64_t n, const double* X,
+             int64_t n_eff, const double* S, const double* P0, int n_electrons, const rr_scf_opts* so,
+             rr_scf_result* res, double* P_out, double* hist, const rr_opts* o) {
+  const bool dhf = kind == 1;
+  const int64_t n2 = n * n, c2 = 2 * n2, ce = 2 * n * n_eff, ee = 2 * n_eff * n_eff;
+  const int64_t nlo = dhf ? n / 2 : 0;  // states below the occupied window
+  RR_REQUIRE(n_electrons > 0 && nlo + n_electrons <= n_eff, RR_ERR_ARG,
+             dhf ? "rkbDensityMatrix: n_electrons must be a positive number of spinors that fits within the "
+                   "positive-energy half of the RKB basis"
+                 : "x2cDensityMatrix: n_electrons must be a positive number of spinors that fits within the basis");
+  const bool host = !o || o->mem == RR_MEM_HOST;
+  cudaStream_t s = call_stream(h, o);
+  const auto t_start = std::chrono::steady_clock::now();
+  const int64_t nu = dhf ? 2 * h->n + 2 * h->ns : 0;
+  DevBuf<double> buf;
+  Arena ar(&buf);
+  double *hd, *Xd, *Sd, *vd = nullptr, *P, *Pn, *F, *Fs, *e, *PS, *SP, *tmp, *Fo, *Pi, *Pi2, *T2, *scal;
+  ar.request(&hd, c2);
+  ar.request(&Xd, ce);
+  ar.request(&Sd, c2);
+  if (dhf) ar.request(&vd, 2 * nu * n);
+  ar.request(&P, c2);
+  ar.request(&Pn, c2);
+  ar.request(&F, c2);
+  ar.request(&Fs, c2);
+  ar.request(&e, c2);
+  ar.request(&PS, c2);
+  ar.request(&SP, c2);
+  ar.request(&tmp, std::max(c2, ce));
+  ar.request(&Fo, ee);
+  ar.request(&Pi, ee);
+  ar.request(&Pi2, dhf ? ee : 1);
+  ar.request(&T2, ee);
+  ar.request(&scal, 64);
+  ar.commit();
+  copy_in(hd, hc, c2, host, s);
+  copy_in(Xd, X, ce, host, s);
+  copy_in(Sd, S, c2, host, s);
+  if (dhf) copy_in(vd, v_total, 2 * nu * n, host, s);
+  const bool restrict_active = so->kramers_restricted && n_electrons % 2 == 0;
+  const int64_t nb = dhf ? n / 4 : n / 2;
+  if (restrict_active) {
+    copy_in(Pn, P0, c2, host, s);
+    kramers_even_kernel<<<blocks_for(n2), 256, 0, s>>>(P, Pn, n, nb);
+    RR_LAUNCH_CHECK();
+  } else {
+    copy_in(P, P0, c2, host, s);
+  }
+  DeviceDiis diis;
+  const bool use_diis = so->diis_size >= 2;
+  RR_REQUIRE(so->diis_size <= DIIS_MAX, RR_ERR_ARG, "SCF: diis_size too large");
+  diis.init(use_diis ? so->diis_size : 0, c2);
+  h->work.ensure(static_cast<size_t>(std::max<int64_t>(static_cast<int64_t>(h->work.n), 8 * c2)));
+  double* wk = h->work.p;
+  const int64_t wcap = static_cast<int64_t>(h->work.n);
+  GemmDesc g;  // n x n complex products
+  g.cplx = true;
+  g.M = n; g.N = n; g.K = n; g.lda = n; g.ldb = n; g.ldc = n;
+  rr_opts od{};
+  od.mem = RR_MEM_DEVICE;
+  od.stream = s;
+  double prev = 0.0;
+  int64_t it = 0;
+  bool converged = false;
+  for (it = 1; it <= so->max_iterations; ++it) {
+    if (dhf) fock_rkb(h, hd, vd, n, Sd, Xd, n_eff, P, F, &od);
+    else fock_x2c(h, hd, P, Sd, Xd, n_eff, F, &od);
+    energy_kernel<2><<<1, 1024, 0, s>>>(P, hd, F, n, scal);
+    RR_LAUNCH_CHECK();
+    if (use_diis) {
+      g.A = P; g.B = Sd; g.C = PS; g.alpha = 1.0; g.beta = 0.0;
+      gemm(g, s, wk, wcap);
+      g.A = Sd; g.B = P; g.C = SP;
+      gemm(g, s, wk, wcap);
+      g.A = F; g.B = PS; g.C = e;
+      gemm(g, s, wk, wcap);
+      g.A = SP; g.B = F; g.C = e; g.alpha = -1.0; g.beta = 1.0;
+      gemm(g, s, wk, wcap);
+      g.alpha = 1.0; g.beta = 0.0;
+      diis.extrapolate(e, F, Fs, s);
+    } else {
+      copy_out(Fs, F, c2, false, s);
+    }
+    // F_ortho = X^dagger F_scf X
+    GemmDesc a;
+    a.cplx = true;
+    a.M = n; a.N = n_eff; a.K = n; a.A = Fs; a.lda = n; a.B = Xd; a.ldb = n_eff; a.C = tmp; a.ldc = n_eff;
+    gemm(a, s, wk, wcap);
+    a.M = n_eff; a.N = n_eff; a.K = n; a.A = Xd; a.lda = n_eff; a.opA = Op::T; a.conjA = true; a.B = tmp;
+    a.ldb = n_eff; a.C = Fo; a.ldc = n_eff;
+    gemm(a, s, wk, wcap);
+    // window projector in the orthonormal basis
+    sp2_projector(h, Fo, n_eff, nlo + n_electrons, Pi, T2, scal + 8, s, true);
+    if (nlo > 0) {
+      sp2_projector(h, Fo, n_eff, nlo, Pi2, T2, scal + 8, s, true);
+      axpby(Pi, Pi2, -1.0, 1.0, ee, s);
+    }
+    // P_new = X Pi X^dagger (Kramers-projected)
+    GemmDesc b;
+    b.cplx = true;
+    b.M = n; b.N = n_eff; b.K = n_eff; b.A = Xd; b.lda = n_eff; b.B = Pi; b.ldb = n_eff; b.C = tmp; b.ldc = n_eff;
+    gemm(b, s, wk, wcap);
+    b.M = n; b.N = n; b.K = n_eff; b.A = tmp; b.lda = n_eff; b.B = Xd; b.ldb = n_eff; b.opB = Op::T; b.conjB = true;
+    b.C = restrict_active ? e : Pn; b.ldc = n;
+    gemm(b, s, wk, wcap);
+    if (restrict_active) {
+      kramers_even_kernel<<<blocks_for(n2), 256, 0, s>>>(Pn, e, n, nb);
+      RR_LAUNCH_CHECK();
+    }
+    maxdiff_kernel<2><<<1, 1024, 0, s>>>(Pn, P, n2, scal + 1);
+    RR_LAUNCH_CHECK();
+    double hv[2];
+    RR_CUDA(cudaMemcpyAsync(hv, scal, sizeof(hv), cudaMemcpyDeviceToHost, s));
+    RR_CUDA(cudaStreamSynchronize(s));
+    const double energy = hv[0], dP = hv[1], dE = std::fabs(energy - prev);
+    if (hist) hist[it - 1] = energy;
+    res->electronic_energy = energy;
+    const bool conv = it > 1 && (dP < so->density_tolerance || dE < so->energy_tolerance);
+    prev = energy;
+    if (conv) {
+      converged = true;
+      break;
+    }
+    if (!use_diis && so->mixing > 0.0 && so->mixing != 1.0) axpby(Pn, P, 1.0 - so->mixing, so->mixing, c2, s);
+    std::swap(P, Pn);
+  }
+  if (it > so->max_iterations) it = so->max_iterations;
+  check_status(h, s);
+  copy_out(P_out, P, c2, host, s);
+  RR_CUDA(cudaStreamSynchronize(s));
+  res->iterations = it;
+  res->converged = converged ? 1 : 0;
+  res->mixed_iterations = 0;
+  res->fp64_iterations = it;
   res->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
 }
 

@@ -1,6 +1,11 @@
 """Device-resident SCF drivers (rr_scf_run_*), mirroring the reference's SCF entry points.
 
 * ``runNonRelativisticHartreeFock``  src/NON_REL/NonRelHartreeFock.cpp:219 (RiNonRelEriSource overload)
+* ``runX2CHartreeFockScf``           src/X2C_DHF/X2C_HF.h:131 (RiX2cEriSource overload)
+* ``runDiracHartreeFockScf``         src/C4_DHF/C4_DHF.h:116 (RiDirectEriSource overload)
+
+Nuclear repulsion is the caller's (the reference adds it from the geometry); the returned energy
+is electronic.
 """
 from __future__ import annotations
 
@@ -9,13 +14,22 @@ import ctypes
 import numpy as np
 
 from . import _lib as L
-from .ri import RiNonRelEriSource, _host, _ptr
+from ._lib import RrError
+from .ri import RiDirectEriSource, RiNonRelEriSource, RiX2cEriSource, _host, _ptr
 
 
-def _opts(diis_size, max_iterations, energy_tolerance, density_tolerance, precision, mixed_switch, kramers=True):
+def _opts(diis_size, max_iterations, energy_tolerance, density_tolerance, precision, mixed_switch, kramers=True,
+          mixing=1.0):
     prec = {"fp64": L.RR_PREC_FP64, "mixed": L.RR_PREC_MIXED}[precision]
     return L.ScfOpts(diis_size, max_iterations, energy_tolerance, density_tolerance, 1 if kramers else 0, prec,
-                     mixed_switch, 0, 0)
+                     mixed_switch, mixing)
+
+
+def _result(res, P, hist):
+    it = int(res.iterations)
+    return dict(energy=res.electronic_energy, iterations=it, converged=bool(res.converged), P=P,
+                history=hist[:it].copy(), seconds=res.seconds, mixed_iterations=int(res.mixed_iterations),
+                fp64_iterations=int(res.fp64_iterations))
 
 
 def runNonRelativisticHartreeFock(eri: RiNonRelEriSource, h_core, x_large, initial_density, n_electrons: int,
@@ -39,3 +53,45 @@ def runNonRelativisticHartreeFock(eri: RiNonRelEriSource, h_core, x_large, initi
     return dict(energy=res.electronic_energy, iterations=it, converged=bool(res.converged), P=P,
                 history=hist[:it].copy(), seconds=res.seconds, mixed_iterations=int(res.mixed_iterations),
                 fp64_iterations=int(res.fp64_iterations))
+
+
+def runX2CHartreeFockScf(h_x2c, eri: RiX2cEriSource, x_large, initial_density, n_electrons: int, overlap=None,
+                         diis_size: int = 5, max_iterations: int = 100, energy_tolerance: float = 1e-8,
+                         density_tolerance: float = 1e-6, kramers_restricted: bool = True, mixing: float = 1.0) -> dict:
+    """X2C-HF on the GPU (rr_scf_run_x2c).  `overlap` defaults to the source's overlap."""
+    n = 2 * eri.nl
+    S = _host(eri.overlap if overlap is None else overlap, np.complex128)
+    h = _host(h_x2c, np.complex128)
+    X = _host(x_large, np.complex128)
+    P0 = _host(initial_density, np.complex128)
+    if h.shape != (n, n) or P0.shape != (n, n) or S.shape != (n, n) or X.shape[0] != n:
+        raise RrError(L.RR_ERR_ARG, "runX2CHartreeFockScf: matrix dimensions do not match 2*nLarge")
+    so = _opts(diis_size, max_iterations, energy_tolerance, density_tolerance, "fp64", 0.0, kramers_restricted, mixing)
+    res = L.ScfResult()
+    P = np.empty((n, n), dtype=np.complex128)
+    hist = np.full(max_iterations, np.nan)
+    L.check(L.lib().rr_scf_run_x2c(eri.store.handle, _ptr(h), _ptr(X), X.shape[1], _ptr(S), _ptr(P0), n_electrons,
+                                   ctypes.byref(so), ctypes.byref(res), _ptr(P), _ptr(hist), ctypes.byref(L.opts())))
+    return _result(res, P, hist)
+
+
+def runDiracHartreeFockScf(h_rkb, eri: RiDirectEriSource, x_full, initial_density, n_electrons: int, overlap=None,
+                           diis_size: int = 5, max_iterations: int = 100, energy_tolerance: float = 1e-8,
+                           density_tolerance: float = 1e-6, kramers_restricted: bool = True,
+                           mixing: float = 1.0) -> dict:
+    """4c-DHF on the GPU (rr_scf_run_dhf).  `overlap` defaults to the source's s_full."""
+    h = _host(h_rkb, np.complex128)
+    n = h.shape[0]
+    S = _host(eri.s_full if overlap is None else overlap, np.complex128)
+    X = _host(x_full, np.complex128)
+    v = _host(eri.v_total, np.complex128)
+    P0 = _host(initial_density, np.complex128)
+    if X.shape != (n, n):
+        raise RrError(L.RR_ERR_ARG, "rkbDensityMatrix: C_DHF is not square")
+    so = _opts(diis_size, max_iterations, energy_tolerance, density_tolerance, "fp64", 0.0, kramers_restricted, mixing)
+    res = L.ScfResult()
+    P = np.empty((n, n), dtype=np.complex128)
+    hist = np.full(max_iterations, np.nan)
+    L.check(L.lib().rr_scf_run_dhf(eri.store.handle, _ptr(h), _ptr(v), n, _ptr(S), _ptr(X), _ptr(P0), n_electrons,
+                                   ctypes.byref(so), ctypes.byref(res), _ptr(P), _ptr(hist), ctypes.byref(L.opts())))
+    return _result(res, P, hist)

@@ -45,3 +45,64 @@ def test_nonrel_mixed_reaches_fp64_energy(n, naux, nocc, seed):
     assert r64["converged"] and rm["converged"]
     assert rm["mixed_iterations"] >= 1 and rm["fp64_iterations"] >= 1
     assert abs(rm["energy"] - r64["energy"]) <= 1e-8
+
+
+def _run_x2c(sysd, **kw):
+    src = ri.RiX2cEriSource(int(sysd["h"].shape[0]) // 2, sysd["B"], sysd["X"], sysd["S"])
+    return scf.runX2CHartreeFockScf(sysd["h"], src, sysd["X"], sysd["P0"], int(sysd["n_electrons"]), **kw)
+
+
+def _run_dhf(sysd, **kw):
+    src = ri.RiDirectEriSource(int(sysd["nl"]), int(sysd["ns"]), sysd["B_LL"], sysd["B_SS"], sysd["v_total"],
+                               sysd["s_full"], sysd["x_full"])
+    return scf.runDiracHartreeFockScf(sysd["h"], src, sysd["x_full"], sysd["P0"], int(sysd["n_electrons"]), **kw)
+
+
+def test_x2c_golden_history():
+    g = golden("scf_x2c")
+    r = _run_x2c(g)
+    assert r["converged"]
+    assert r["iterations"] == int(g["iterations"])
+    assert np.abs(r["history"] - g["history"]).max() <= 1e-8
+    assert np.abs(r["P"] - g["P"]).max() <= 1e-6
+
+
+def test_dhf_golden_history():
+    g = golden("scf_dhf")
+    r = _run_dhf(g)
+    assert r["converged"]
+    assert r["iterations"] == int(g["iterations"])
+    assert np.abs(r["history"] - g["history"]).max() <= 1e-8
+    assert np.abs(r["P"] - g["P"]).max() <= 1e-6
+
+
+@pytest.mark.parametrize("nl,naux,ne,seed", [(12, 60, 6, 21), (40, 160, 10, 22)])
+def test_x2c_vs_reference(ref_lib, nl, naux, ne, seed):
+    s = synth.x2c_system(nl, naux, ne, seed=seed)
+    r = _run_x2c(s)
+    rr = ref_lib.x2c_scf(s)
+    assert r["converged"] and rr["converged"]
+    assert r["iterations"] == rr["iterations"]
+    assert np.abs(r["history"] - rr["history"]).max() <= 1e-8
+
+
+@pytest.mark.parametrize("nl,ns,naux,ne,seed", [(6, 11, 40, 4, 23), (12, 25, 80, 8, 24)])
+def test_dhf_vs_reference(ref_lib, nl, ns, naux, ne, seed):
+    s = synth.rkb_system(nl, ns, naux, ne, seed=seed)
+    r = _run_dhf(s)
+    rr = ref_lib.dhf_scf(s)
+    assert r["converged"] and rr["converged"]
+    assert r["iterations"] == rr["iterations"]
+    assert np.abs(r["history"] - rr["history"]).max() <= 1e-8
+
+
+def test_x2c_without_kramers_projection_and_with_mixing(ref_lib):
+    s = synth.x2c_system(10, 50, 6, seed=25)
+    r = _run_x2c(s, kramers_restricted=False)
+    rr = ref_lib.x2c_scf(s, kramers=False)
+    assert r["iterations"] == rr["iterations"]
+    assert np.abs(r["history"] - rr["history"]).max() <= 1e-8
+    # plain linear mixing (no DIIS) reaches the same state; tight tolerances because the reference's
+    # OR rule stops a slowly mixed iteration as soon as one step changes E by less than tolE
+    rm = _run_x2c(s, diis_size=0, mixing=0.5, max_iterations=400, energy_tolerance=1e-13, density_tolerance=1e-10)
+    assert rm["converged"] and abs(rm["energy"] - r["energy"]) <= 1e-7
