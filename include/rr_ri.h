@@ -246,6 +246,91 @@ int rr_mo_hx_fock(rr_mo_handle m, const double* h, const double* occupations, co
                   const double* two_rdm_x, const int64_t* pair_of, const double* two_rdm_l1, const double* two_rdm_l2,
                   double* F, const rr_opts* opts);
 
+/* ---------------- orbital-rotation optimisation (functional stage) ---------------- */
+
+/* AdamOptions, src/Utils/ADAM.h:41-60 (rr_adam_default_options fills the reference's defaults). */
+typedef struct rr_adam_options {
+  double learning_rate;         /* 0.01 */
+  double rate_factor;           /* 0.2: learning_rate *= rate_factor after a run that did not improve */
+  double beta1, beta2, epsilon; /* 0.7, 0.9, 1e-15 */
+  int32_t base_iterations;      /* 10 */
+  int32_t iterations_increment; /* 20 */
+  int32_t max_iterations_limit; /* 200 */
+  int32_t reserved;
+  double gradient_tolerance; /* 1e-5 */
+  double energy_tolerance;   /* 1e-9 */
+} rr_adam_options;
+
+/* AdamResult, src/Utils/ADAM.h:182-197. */
+typedef struct rr_adam_result {
+  int32_t improved, gradient_converged, energy_converged, restart_requested;
+  int32_t iterations, reserved;
+  double energy_start, energy_best, energy_difference, max_gradient, learning_rate;
+} rr_adam_result;
+
+typedef struct rr_orbopt_store* rr_orbopt_handle;
+
+int rr_adam_default_options(rr_adam_options* out);
+
+/* The ADAM orbital-rotation problem of FULL_OPTIMIZATION (RotationProblem,
+ * src/Full_opt/FullOptimization.cpp:1330-1548, with AdamOptimizer, src/Utils/ADAM.cpp:133-213) for a
+ * nonrelativistic RI MO tensor m (rr_mo_build_nonrel / RR_MO_NONREL_SPIN) and a fixed-occupation
+ * hartree-exchange functional, all on the GPU.  The handle takes a copy of m's tensor.  Host
+ * arguments: h (n x n spatial one-electron matrix in m's MO basis), occupations (2n spin
+ * orbitals), two_rdm_h / two_rdm_x (2n x 2n), optional pair_of (2n) with two_rdm_l1 / two_rdm_l2
+ * (2n x 2n); options NULL = the reference defaults.  Pairs are adamPairIndices(2n) (p > q); the
+ * spin-twin pairs get the averaged gradient, so every rotation is spin restricted. */
+int rr_orbopt_create(rr_mo_handle m, const double* h, const double* occupations, const double* two_rdm_h,
+                     const double* two_rdm_x, const int64_t* pair_of, const double* two_rdm_l1,
+                     const double* two_rdm_l2, const rr_adam_options* options, rr_orbopt_handle* out);
+int rr_orbopt_destroy(rr_orbopt_handle h);
+int rr_orbopt_info(rr_orbopt_handle h, int64_t* n_pairs, int64_t* n_spatial, int64_t* naux);
+/* One AdamOptimizer::run: ADAM steps from the current orbitals until the gradient or energy
+ * converges or the run's step budget ends; the best orbitals found become current.  The learning
+ * rate, the extra-iteration allowance and the restart flag persist between runs, as in the
+ * reference. */
+int rr_orbopt_run(rr_orbopt_handle h, rr_adam_result* result);
+/* Energy 1/2 sum_q [n_q h_qq + F_qq] and the pair gradient (n_pairs) at the current orbitals. */
+int rr_orbopt_energy(rr_orbopt_handle h, double* energy);
+int rr_orbopt_gradient(rr_orbopt_handle h, double* gradient);
+/* Per-pair preconditioning scales s (n_pairs, positive; NULL = plain ADAM): ADAM sees g / sqrt(s)
+ * and the rotation uses step / sqrt(s), the variable change the reference's min-max stage applies
+ * (FullOptimization.cpp:1362-1369).  No counterpart for the learned use in the reference. */
+int rr_orbopt_set_scales(rr_orbopt_handle h, const double* scales);
+/* hartreeExchangeHessianElement(p,q,p,q) per pair at the current orbitals
+ * (src/Hessian_opt/HartreeExchangeHessian.cpp:221), the labels of the learned preconditioner. */
+int rr_orbopt_hessian_diagonal(rr_orbopt_handle h, double* out);
+/* Preconditioner inputs per pair (i = q, a = p): F_ii, F_aa, n_i, n_a, J_ia, K_ia, J_ii, J_aa
+ * (n_pairs x 8 floats; F the generalized Fock matrix, J/K the MO Coulomb and exchange integrals). */
+int rr_orbopt_features(rr_orbopt_handle h, float* out);
+/* Current accumulated spatial rotation (n x n), rotated h (n x n) and MO tensor (naux x n^2);
+ * any pointer may be NULL. */
+int rr_orbopt_state(rr_orbopt_handle h, double* rotation, double* h_out, double* Bmo_out);
+
+/* ---------------- learned preconditioner (no counterpart in the reference) ----------------
+ * An 8 -> 64 -> 64 -> 64 -> 1 tanh MLP predicting log |hartreeExchangeHessianElement(p,q,p,q)| from the
+ * rr_orbopt_features inputs; trained in FP32 by the library's own kernels, BF16 inference.  Its
+ * predictions become rr_orbopt_set_scales scales; without it the optimiser is plain ADAM. */
+typedef struct rr_mlp_store* rr_mlp_handle;
+#define RR_MLP_PARAMS 8961 /* W1 64x8, b1, W2 64x64, b2, W3 64x64, b3, W4 1x64, b4 (row-major, in that order) */
+#define RR_MLP_NORM 18     /* input mean[8], input spread[8], label mean, label spread */
+
+int rr_mlp_create(uint64_t seed, rr_mlp_handle* out); /* Xavier-uniform weights from the seed */
+int rr_mlp_destroy(rr_mlp_handle h);
+/* Mini-batch Adam (beta 0.9 / 0.999) on the mean squared error of the standardised labels; the
+ * first call fixes the input / label standardisation from its data.  X: count x 8, y: count (host).
+ * loss_per_epoch (optional): mean squared error per epoch, in standardised units. */
+int rr_mlp_train(rr_mlp_handle h, const float* X, const float* y, int64_t count, int32_t epochs, int32_t batch,
+                 float learning_rate, uint64_t shuffle_seed, float* loss_per_epoch);
+/* y = prediction in label units; bf16 != 0 runs the BF16 inference kernel, else FP32. */
+int rr_mlp_predict(rr_mlp_handle h, const float* X, int64_t count, int32_t bf16, float* y);
+/* Loss (mean squared error, standardised units) and its gradient (RR_MLP_PARAMS floats) over all
+ * `count` samples: the training kernels' forward and backward passes, for gradient checks. */
+int rr_mlp_loss_and_grad(rr_mlp_handle h, const float* X, const float* y, int64_t count, float* loss, float* grad);
+/* RR_MLP_PARAMS weights followed by the RR_MLP_NORM standardisation constants. */
+int rr_mlp_get_params(rr_mlp_handle h, float* params);
+int rr_mlp_set_params(rr_mlp_handle h, const float* params);
+
 /* Profiling: when on, each call records CUDA events around its phases; rr_ri_get_timings waits
  * for the last call's events and returns the phase times.  Off by default (no event overhead). */
 int rr_ri_set_profiling(rr_ri_handle h, int32_t on);

@@ -25,6 +25,21 @@ int rr_test_j_passes(const double* B, int64_t naux, int64_t n2, const double* D,
  * Ct: nocc x n, K: n x n; all FP64 device pointers). */
 int rr_test_mixed_exchange(const double* B, int64_t naux, int64_t n, const double* Ct, int64_t nocc, double* K);
 
+/* Adam<T>::step (src/Utils/ADAM.cpp:33-51) on the device over `nsteps` host gradients (rows of
+ * grads, n entries, interleaved complex when cplx); steps receives the nsteps x n updates. */
+int rr_test_adam_steps(int64_t n, int32_t cplx, int64_t nsteps, double lr, double b1, double b2, double eps,
+                       const double* grads, double* steps);
+
+/* exp(-kappa) of a real antisymmetric n x n host matrix by the device scaling-and-squaring route the
+ * orbital optimiser uses (src/Hessian_opt/SpinorRotation.cpp:17 computes the same matrix). */
+int rr_test_rotation_matrix(int64_t n, const double* kappa, double* U);
+
+/* AdamOptimizer<double>::run `runs` times (ADAM.cpp:140-213) on E(x) = sum (a x^2 / 2 + b x) +
+ * c (sum x^2)^2 with x += step, driven by the device ADAM and the library's run logic. */
+int rr_test_adam_run_quadratic(int64_t n, const double* a, const double* b, double c, const double* x0, int32_t runs,
+                               double* energy_best, int32_t* iterations, int32_t* restart, double* rate,
+                               double* x_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -280,3 +280,81 @@ def dhf_scf(sysd, diis_size=5, max_iter=100, e_tol=1e-8, d_tol=1e-6, kramers=Tru
                                ctypes.byref(res), _p(P), _p(hist)))
     return dict(energy=res.electronic_energy, iterations=res.iterations, converged=bool(res.converged), P=P,
                 history=hist[: res.iterations].copy())
+
+
+# ---------------------------------------------------------------- orbital-rotation optimisation
+
+
+def adam_steps(grads, lr=0.01, b1=0.7, b2=0.9, eps=1e-15):
+    """Adam<T>::step (src/Utils/ADAM.cpp:33-51) over the rows of `grads` (real or complex)."""
+    g = np.ascontiguousarray(grads)
+    cplx = np.iscomplexobj(g)
+    g = g.astype(np.complex128 if cplx else np.float64)
+    out = np.empty_like(g)
+    _check(lib().rrref_adam_steps(_i64(g.shape[1]), ctypes.c_int(int(cplx)), _i64(g.shape[0]), ctypes.c_double(lr),
+                                  ctypes.c_double(b1), ctypes.c_double(b2), ctypes.c_double(eps),
+                                  g.ctypes.data_as(_dp), out.ctypes.data_as(_dp)))
+    return out
+
+
+def adam_run_quadratic(a, b, c, x0, runs):
+    """AdamOptimizer<double>::run (ADAM.cpp:140-213) `runs` times on
+    E(x) = sum (a x^2/2 + b x) + c (sum x^2)^2 with x += step."""
+    a, b, x0 = _d(a), _d(b), _d(x0)
+    n = a.size
+    eb = np.empty(runs)
+    it = np.empty(runs, dtype=np.int32)
+    rs = np.empty(runs, dtype=np.int32)
+    lr = np.empty(runs)
+    x = np.empty(n)
+    _check(lib().rrref_adam_run_quadratic(_i64(n), _p(a), _p(b), ctypes.c_double(c), _p(x0), ctypes.c_int(runs),
+                                          _p(eb), it.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                          rs.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _p(lr), _p(x)))
+    return dict(energy_best=eb, iterations=it, restart=rs.astype(bool), rate=lr, x=x)
+
+
+def rotation_matrix(kappa):
+    """spinorRotationMatrix(kappa) = exp(-kappa) (src/Hessian_opt/SpinorRotation.cpp:17)."""
+    k = np.ascontiguousarray(kappa)
+    cplx = np.iscomplexobj(k)
+    k = k.astype(np.complex128 if cplx else np.float64)
+    U = np.empty_like(k)
+    _check(lib().rrref_rotation_matrix(_i64(k.shape[0]), ctypes.c_int(int(cplx)), k.ctypes.data_as(_dp),
+                                       U.ctypes.data_as(_dp)))
+    return U
+
+
+def orbital_gradient(F):
+    """orbitalGradient(F): g_pq = 2 (F_qp - conj F_pq) for p >= q (src/Hessian_opt/OrbitalGradient.h)."""
+    f = np.ascontiguousarray(F)
+    cplx = np.iscomplexobj(f)
+    f = f.astype(np.complex128 if cplx else np.float64)
+    g = np.empty_like(f)
+    _check(lib().rrref_orbital_gradient(_i64(f.shape[0]), ctypes.c_int(int(cplx)), f.ctypes.data_as(_dp),
+                                        g.ctypes.data_as(_dp)))
+    return np.tril(g)
+
+
+def hx_hessian_diag_nonrel(Bmo_spatial, n_sp, h, occ, h2, x2, F, pairs, pair_of=None, l1=None, l2=None):
+    """hartreeExchangeHessianElement(p,q,p,q) per pair (src/Hessian_opt/HartreeExchangeHessian.cpp:221)."""
+    pr = np.ascontiguousarray(pairs, dtype=np.int64).reshape(-1, 2)
+    out = np.empty(pr.shape[0])
+    po = None if pair_of is None else np.ascontiguousarray(pair_of, dtype=np.int64)
+    _check(lib().rrref_hx_hessian_diag_nonrel(_i64(n_sp), _i64(Bmo_spatial.shape[0]), _p(_d(Bmo_spatial)), _p(_d(h)),
+                                              _p(_d(occ)), _p(_d(h2)), _p(_d(x2)), _p(_d(F)),
+                                              None if po is None else _p(po),
+                                              None if po is None else _p(_d(l1)),
+                                              None if po is None else _p(_d(l2)), _i64(pr.shape[0]), _p(pr),
+                                              _p(out)))
+    return out
+
+
+def hx_energy_nonrel(Bmo_spatial, n_sp, h, occ, h2, x2, pair_of=None, l1=None, l2=None):
+    """hartreeExchangeEnergy (src/Hessian_opt/HartreeExchangeGradient.cpp:233)."""
+    E = ctypes.c_double()
+    po = None if pair_of is None else np.ascontiguousarray(pair_of, dtype=np.int64)
+    _check(lib().rrref_hx_energy_nonrel(_i64(n_sp), _i64(Bmo_spatial.shape[0]), _p(_d(Bmo_spatial)), _p(_d(h)),
+                                        _p(_d(occ)), _p(_d(h2)), _p(_d(x2)), None if po is None else _p(po),
+                                        None if po is None else _p(_d(l1)), None if po is None else _p(_d(l2)),
+                                        ctypes.byref(E)))
+    return E.value

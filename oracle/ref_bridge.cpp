@@ -30,6 +30,10 @@
 #include "X2C_HF.h"
 #include "JkOnlyFock.h"
 #include "HartreeExchangeGradient.h"
+#include "ADAM.h"
+#include "HartreeExchangeHessian.h"
+#include "OrbitalGradient.h"
+#include "SpinorRotation.h"
 
 extern "C" void scipy_openblas_set_num_threads(int n);
 
@@ -430,6 +434,154 @@ int rrref_dhf_scf(i64 nl, i64 ns, i64 naux, const double* B_LL, const double* B_
     std::vector<double> e;
     for (const auto& rec : r.history) e.push_back(rec.energy);
     copyHistory(e, energy_history, max_iter);
+  });
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Orbital-rotation optimisation (functional stage): ADAM, rotations, gradient, Hessian diagonal.
+
+namespace {
+
+rerdmft::AdamOptions adamOptions(double lr, double b1, double b2, double eps) {
+  rerdmft::AdamOptions o;
+  o.learning_rate = lr;
+  o.beta1 = b1;
+  o.beta2 = b2;
+  o.epsilon = eps;
+  return o;
+}
+
+// E(x) = sum_i (a_i x_i^2 / 2 + b_i x_i) + c (sum_i x_i^2)^2, x += step: a deterministic
+// AdamProblem for checking the run / restart logic.
+class QuadraticProblem : public rerdmft::AdamProblem<double> {
+ public:
+  QuadraticProblem(std::vector<double> a, std::vector<double> b, double c, std::vector<double> x)
+      : a_(std::move(a)), b_(std::move(b)), c_(c), x_(std::move(x)), best_(x_) {}
+  std::size_t dimension() const override { return x_.size(); }
+  double energy() override {
+    double e = 0.0, r = 0.0;
+    for (std::size_t i = 0; i < x_.size(); ++i) {
+      e += 0.5 * a_[i] * x_[i] * x_[i] + b_[i] * x_[i];
+      r += x_[i] * x_[i];
+    }
+    return e + c_ * r * r;
+  }
+  std::vector<double> gradient() override {
+    double r = 0.0;
+    for (double v : x_) r += v * v;
+    std::vector<double> g(x_.size());
+    for (std::size_t i = 0; i < x_.size(); ++i) g[i] = a_[i] * x_[i] + b_[i] + 4.0 * c_ * r * x_[i];
+    return g;
+  }
+  void rotate(const std::vector<double>& step) override {
+    for (std::size_t i = 0; i < x_.size(); ++i) x_[i] += step[i];
+  }
+  void saveBest() override { best_ = x_; }
+  void restoreBest() override { x_ = best_; }
+  const std::vector<double>& x() const { return x_; }
+
+ private:
+  std::vector<double> a_, b_;
+  double c_;
+  std::vector<double> x_, best_;
+};
+
+}  // namespace
+
+extern "C" {
+
+// src/Utils/ADAM.cpp:33-51 Adam<T>::step over `nsteps` gradients (row t of grads / steps).
+int rrref_adam_steps(i64 n, int cplx, i64 nsteps, double lr, double b1, double b2, double eps, const double* grads,
+                     double* steps) {
+  return guard([&] {
+    const auto o = adamOptions(lr, b1, b2, eps);
+    if (cplx) {
+      rerdmft::Adam<C> adam(static_cast<std::size_t>(n), o);
+      const C* g = reinterpret_cast<const C*>(grads);
+      C* out = reinterpret_cast<C*>(steps);
+      for (i64 t = 0; t < nsteps; ++t) {
+        auto st = adam.step(std::vector<C>(g + t * n, g + (t + 1) * n));
+        std::memcpy(out + t * n, st.data(), sizeof(C) * static_cast<std::size_t>(n));
+      }
+    } else {
+      rerdmft::Adam<double> adam(static_cast<std::size_t>(n), o);
+      for (i64 t = 0; t < nsteps; ++t) {
+        auto st = adam.step(std::vector<double>(grads + t * n, grads + (t + 1) * n));
+        std::memcpy(steps + t * n, st.data(), sizeof(double) * static_cast<std::size_t>(n));
+      }
+    }
+  });
+}
+
+// src/Utils/ADAM.cpp:140-213 AdamOptimizer<double>::run, `runs` times in a row on QuadraticProblem.
+// Per run: energy_best, iterations, restart flag, learning rate used; x_out: final point.
+int rrref_adam_run_quadratic(i64 n, const double* a, const double* b, double c, const double* x0, int runs,
+                             double* energy_best, int* iterations, int* restart, double* rate, double* x_out) {
+  return guard([&] {
+    QuadraticProblem prob(std::vector<double>(a, a + n), std::vector<double>(b, b + n), c,
+                          std::vector<double>(x0, x0 + n));
+    rerdmft::AdamOptimizer<double> opt;
+    for (int r = 0; r < runs; ++r) {
+      const auto res = opt.run(prob);
+      energy_best[r] = res.energy_best;
+      iterations[r] = res.iterations;
+      restart[r] = res.restart_requested ? 1 : 0;
+      rate[r] = res.learning_rate;
+    }
+    std::memcpy(x_out, prob.x().data(), sizeof(double) * static_cast<std::size_t>(n));
+  });
+}
+
+// src/Hessian_opt/SpinorRotation.cpp:17 spinorRotationMatrix(kappa) = exp(-kappa).
+int rrref_rotation_matrix(i64 n, int cplx, const double* kappa, double* U) {
+  return guard([&] {
+    if (cplx) fromCMatrix(rerdmft::spinorRotationMatrix(toCMatrix(kappa, n, n)), U);
+    else fromMatrix(rerdmft::spinorRotationMatrix(toMatrix(kappa, n, n)), U);
+  });
+}
+
+// src/Hessian_opt/OrbitalGradient.h orbitalGradient(F): g_pq = 2 (F_qp - conj F_pq), p >= q.
+int rrref_orbital_gradient(i64 n, int cplx, const double* F, double* g) {
+  return guard([&] {
+    if (cplx) fromCMatrix(rerdmft::orbitalGradient(toCMatrix(F, n, n)), g);
+    else fromMatrix(rerdmft::orbitalGradient(toMatrix(F, n, n)), g);
+  });
+}
+
+// src/Hessian_opt/HartreeExchangeHessian.cpp:221 hartreeExchangeHessianElement(p,q,p,q) for each
+// pair (p,q) of `pairs`, NON_REL spin-orbital RI tensor (RiNonRelSpinMoEri over n_sp spatial).
+int rrref_hx_hessian_diag_nonrel(i64 n_sp, i64 naux, const double* Bmo, const double* h, const double* occ,
+                                 const double* h2, const double* x2, const double* F, const i64* pair_of,
+                                 const double* l1, const double* l2, i64 npairs, const i64* pairs, double* out) {
+  return guard([&] {
+    const i64 n = 2 * n_sp;
+    rerdmft::RiNonRelSpinMoEri eri(static_cast<std::size_t>(n_sp), toMatrix(Bmo, naux, n_sp * n_sp));
+    std::vector<double> o(occ, occ + n);
+    Matrix<double> L1 = pair_of ? toMatrix(l1, n, n) : Matrix<double>();
+    Matrix<double> L2 = pair_of ? toMatrix(l2, n, n) : Matrix<double>();
+    const auto H = toMatrix(h, n, n), H2 = toMatrix(h2, n, n), X2 = toMatrix(x2, n, n), FF = toMatrix(F, n, n);
+    const auto po = pairVec(pair_of, n);
+    for (i64 i = 0; i < npairs; ++i) {
+      const auto p = static_cast<std::size_t>(pairs[2 * i]), q = static_cast<std::size_t>(pairs[2 * i + 1]);
+      out[i] = rerdmft::hartreeExchangeHessianElement(H, eri, o, H2, X2, FF, p, q, p, q, po, L1, L2);
+    }
+  });
+}
+
+// src/Hessian_opt/HartreeExchangeGradient.cpp:233 hartreeExchangeEnergy, NON_REL spin-orbital RI tensor.
+int rrref_hx_energy_nonrel(i64 n_sp, i64 naux, const double* Bmo, const double* h, const double* occ,
+                           const double* h2, const double* x2, const i64* pair_of, const double* l1, const double* l2,
+                           double* E) {
+  return guard([&] {
+    const i64 n = 2 * n_sp;
+    rerdmft::RiNonRelSpinMoEri eri(static_cast<std::size_t>(n_sp), toMatrix(Bmo, naux, n_sp * n_sp));
+    std::vector<double> o(occ, occ + n);
+    Matrix<double> L1 = pair_of ? toMatrix(l1, n, n) : Matrix<double>();
+    Matrix<double> L2 = pair_of ? toMatrix(l2, n, n) : Matrix<double>();
+    *E = rerdmft::hartreeExchangeEnergy(toMatrix(h, n, n), eri, o, toMatrix(h2, n, n), toMatrix(x2, n, n),
+                                        pairVec(pair_of, n), L1, L2);
   });
 }
 

@@ -442,3 +442,208 @@ def dhf_scf(sysd, diis_size=5, max_iter=100, e_tol=1e-8, d_tol=1e-6, kramers=Tru
 
     return _scf(lambda p: rkb_fock(h, *args, p), h, sysd["x_full"], sysd["s_full"], sysd["P0"], dens, diis_size,
                 max_iter, e_tol, d_tol, restrict)
+
+
+# --------------------------------------------------------------------------- orbital rotations
+
+
+def adam_step_sequence(grads, lr=0.01, b1=0.7, b2=0.9, eps=1e-15):
+    """Adam<T>::step (src/Utils/ADAM.cpp:33-51): AMSGrad-style moments; complex entries share one
+    real second moment |g|^2 (the step keeps the direction of the complex gradient)."""
+    grads = np.asarray(grads)
+    m1 = np.zeros(grads.shape[1], dtype=grads.dtype)
+    m2 = np.zeros(grads.shape[1])
+    mx = np.zeros(grads.shape[1])
+    out = np.empty_like(grads)
+    for t, g in enumerate(grads, start=1):
+        c1, c2 = 1.0 - b1 ** t, 1.0 - b2 ** t
+        m1 = b1 * m1 + (1.0 - b1) * g
+        m2 = b2 * m2 + (1.0 - b2) * np.abs(g) ** 2
+        mx = np.maximum(mx, m2 / c2)
+        out[t - 1] = -lr * (m1 / c1) / (np.sqrt(mx) + eps)
+    return out
+
+
+def pair_indices(n):
+    """adamPairIndices(n) (src/Utils/ADAM.cpp:57): (1,0), (2,0), (2,1), (3,0), ..."""
+    return [(p, q) for p in range(n) for q in range(p)]
+
+
+def kappa_matrix(n, pairs, step):
+    """adamKappaMatrix (ADAM.cpp:92-128): kappa_pq = step, kappa_qp = -conj(step)."""
+    k = np.zeros((n, n), dtype=np.result_type(step, float))
+    for (p, q), s in zip(pairs, step):
+        k[p, q] = s
+        k[q, p] = -np.conj(s)
+    return k
+
+
+def rotation_matrix(kappa):
+    """exp(-kappa) for anti-Hermitian kappa via the Hermitian i*kappa = V w V^dagger
+    (src/Hessian_opt/SpinorRotation.cpp:17-90)."""
+    w, v = np.linalg.eigh(1j * kappa)
+    u = (v * np.exp(1j * w)) @ v.conj().T
+    return u.real if np.isrealobj(kappa) else u
+
+
+def orbital_gradient(F):
+    """g_pq = 2 (F_qp - conj F_pq), lower triangle p >= q (src/Hessian_opt/OrbitalGradient.h)."""
+    return np.tril(2.0 * (F.T - np.conj(F)))
+
+
+def hx_energy_from_fock(h, occ, F):
+    """E = 1/2 sum_q [n_q Re h_qq + Re F_qq]: the double-counting identity the reference's rotation
+    problem uses with the generalized Fock of hx_fock (src/Full_opt/FullOptimization.cpp:1383)."""
+    return 0.5 * float(np.sum(np.asarray(occ) * np.real(np.diag(h))) + np.real(np.trace(F)))
+
+
+def _eri(b3, a, b, c, d):
+    return float(b3[:, a, c] @ b3[:, b, d])
+
+
+def hx_hessian_diag(h, Bmo, occ, h2, x2, F, pairs, pair_of=None, l1=None, l2=None):
+    """hartreeExchangeHessianElement(p,q,p,q) (src/Hessian_opt/HartreeExchangeHessian.cpp:221) for
+    real orbitals: the antisymmetrised combination of the bare G_pq,rs terms (:57-118 H/X part,
+    :124-161 L1/L2 part) with eri(a,b,c,d) = sum_P B(P,a,c) B(P,b,d).  Pure Python loops: small n."""
+    n = h.shape[0]
+    b3 = Bmo.reshape(-1, n, n)
+    occ = np.asarray(occ, dtype=float)
+
+    def raw(p, q, r, s):
+        t = 0.0
+        if q == r:
+            t += F[p, s]
+            t -= h[s, p] * occ[r]
+            t += sum(h2[r, u] * (_eri(b3, u, s, p, u) - _eri(b3, s, u, p, u)) for u in range(n))
+        if s == p:
+            t += F[q, r]
+            t -= h[q, r] * occ[p]
+            t += sum(h2[p, u] * (_eri(b3, u, q, r, u) - _eri(b3, u, q, u, r)) for u in range(n))
+        i1, i2 = _eri(b3, s, q, p, r), _eri(b3, s, q, r, p)
+        t += i1 * (x2[r, q] - h2[s, q] + x2[p, s] - x2[r, p])
+        t += i2 * (h2[r, p] + x2[q, s] - x2[p, s] - x2[r, q])
+        return t
+
+    def raw_l(p, q, r, s):
+        po = pair_of
+        t = 0.0
+        if q == po[s]:
+            t -= 2.0 * sum(_eri(b3, u, po[u], p, r) * (l1[u, s] + l2[u, q]) for u in range(n))
+        c = l1[r, q] + l2[r, po[q]]
+        t += 2.0 * c * (_eri(b3, po[r], s, p, po[q]) - _eri(b3, s, po[r], p, po[q]))
+        c = l1[p, s] + l2[p, po[s]]
+        t += 2.0 * c * (_eri(b3, po[p], q, r, po[s]) - _eri(b3, po[p], q, po[s], r))
+        if p == po[r]:
+            t += 2.0 * sum(_eri(b3, s, q, w, po[w]) * (l1[r, w] + l2[r, po[w]]) for w in range(n))
+        return t
+
+    out = []
+    for p, q in pairs:
+        v = raw(p, q, p, q) - raw(p, q, q, p) - raw(q, p, p, q) + raw(q, p, q, p)
+        if pair_of is not None:
+            v += raw_l(p, q, p, q) - raw_l(p, q, q, p) - raw_l(q, p, p, q) + raw_l(q, p, q, p)
+        out.append(v)
+    return np.array(out)
+
+
+class RotationProblemNumpy:
+    """RotationProblem (src/Full_opt/FullOptimization.cpp:1330-1548) for RiNonRelSpinMoEri and a
+    fixed-occupation hartree-exchange functional: spin-orbital pairs p > q, twin-averaged gradient,
+    rotations exp(-kappa) of the spatial block, energy from the generalized-Fock identity."""
+
+    def __init__(self, Bmo, h, occ, h2, x2, pair_of=None, l1=None, l2=None):
+        self.n = h.shape[0]
+        self.d = 2 * self.n
+        self.B, self.h = Bmo.copy(), h.copy()
+        self.occ, self.h2, self.x2 = occ, h2, x2
+        self.po, self.l1, self.l2 = pair_of, l1, l2
+        self.pairs = pair_indices(self.d)
+        idx = {pq: i for i, pq in enumerate(self.pairs)}
+        self.twin = []
+        for p, q in self.pairs:
+            pp, qq = (p + self.n) % self.d, (q + self.n) % self.d
+            self.twin.append(idx[(pp, qq)] if pp > qq else -1)
+        self.best = None
+
+    def spin_h(self):
+        H = np.zeros((self.d, self.d))
+        H[: self.n, : self.n] = self.h
+        H[self.n:, self.n:] = self.h
+        return H
+
+    def fock(self):
+        return hx_fock(self.spin_h(), nonrel_mo_embedded(self.B, self.n), self.occ, self.h2, self.x2, self.po, self.l1,
+                       self.l2)
+
+    def energy(self):
+        return hx_energy_from_fock(self.spin_h(), self.occ, self.fock())
+
+    def gradient(self):
+        g = orbital_gradient(self.fock())
+        raw = np.array([g[p, q] for p, q in self.pairs])
+        out = raw.copy()
+        for i, t in enumerate(self.twin):
+            if t >= 0:
+                out[i] = 0.5 * (raw[i] + raw[t])
+        return out
+
+    def rotate(self, step):
+        k = kappa_matrix(self.d, self.pairs, step)
+        u = rotation_matrix(k)[: self.n, : self.n]
+        b3 = self.B.reshape(-1, self.n, self.n)
+        self.B = np.einsum("ai,Pab,bj->Pij", u, b3, u, optimize=True).reshape(b3.shape[0], -1)
+        self.h = u.T @ self.h @ u
+
+    def save_best(self):
+        self.best = (self.B.copy(), self.h.copy())
+
+    def restore_best(self):
+        self.B, self.h = self.best[0].copy(), self.best[1].copy()
+
+
+class AdamOptimizerNumpy:
+    """AdamOptimizer<double>::run (src/Utils/ADAM.cpp:140-213) with the AdamOptions defaults."""
+
+    def __init__(self, lr=0.01, rate_factor=0.2, base=10, inc=20, limit=200, gtol=1e-5, etol=1e-9):
+        self.opt = dict(lr=lr, rate_factor=rate_factor, base=base, inc=inc, limit=limit, gtol=gtol, etol=etol)
+        self.lr, self.extra, self.restart = lr, 0, False
+
+    def run(self, prob):
+        o = self.opt
+        self.restart = False
+        max_calls = o["base"] + self.extra
+        if max_calls > o["limit"]:
+            max_calls = o["base"]
+        n = len(prob.pairs) if hasattr(prob, "pairs") else prob.dim
+        m1, m2, mx, t = np.zeros(n), np.zeros(n), np.zeros(n), 0
+        e_old = prob.energy()
+        e_best = e_old
+        prob.save_best()
+        improved, ediff = False, 0.0
+        while True:
+            g = prob.gradient()
+            if np.abs(g).max() < o["gtol"]:
+                self.lr, self.extra = o["lr"], 0
+                break
+            t += 1
+            c1, c2 = 1 - 0.7 ** t, 1 - 0.9 ** t
+            m1 = 0.7 * m1 + 0.3 * g
+            m2 = 0.9 * m2 + 0.1 * g * g
+            mx = np.maximum(mx, m2 / c2)
+            prob.rotate(-self.lr * (m1 / c1) / (np.sqrt(mx) + 1e-15))
+            e = prob.energy()
+            if e < e_best:
+                improved, e_best = True, e
+                prob.save_best()
+            ediff = e - e_old
+            if t > 1 and abs(ediff) < o["etol"]:
+                break
+            e_old = e
+            if t == max_calls:
+                break
+        if not improved and abs(ediff) > o["etol"]:
+            self.restart = True
+            self.lr *= o["rate_factor"]
+            self.extra += o["inc"]
+        prob.restore_best()
+        return dict(iterations=t, energy_best=e_best, restart_requested=self.restart)

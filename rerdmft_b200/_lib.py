@@ -47,12 +47,49 @@ class ScfOpts(ctypes.Structure):
                 ("mixed_switch", _d), ("mixing", _d)]
 
 
+class AdamOptions(ctypes.Structure):
+    _fields_ = [("learning_rate", _d), ("rate_factor", _d), ("beta1", _d), ("beta2", _d), ("epsilon", _d),
+                ("base_iterations", _i32), ("iterations_increment", _i32), ("max_iterations_limit", _i32),
+                ("reserved", _i32), ("gradient_tolerance", _d), ("energy_tolerance", _d)]
+
+
+class AdamResult(ctypes.Structure):
+    _fields_ = [("improved", _i32), ("gradient_converged", _i32), ("energy_converged", _i32),
+                ("restart_requested", _i32), ("iterations", _i32), ("reserved", _i32), ("energy_start", _d),
+                ("energy_best", _d), ("energy_difference", _d), ("max_gradient", _d), ("learning_rate", _d)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
 class ScfResult(ctypes.Structure):
     _fields_ = [("electronic_energy", _d), ("iterations", _i64), ("converged", _i64),
                 ("mixed_iterations", _i64), ("fp64_iterations", _i64), ("seconds", _d)]
 
 
 _SIGS = {
+    "rr_adam_default_options": (ctypes.c_int, [ctypes.POINTER(AdamOptions)]),
+    "rr_orbopt_create": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(AdamOptions),
+                                        ctypes.POINTER(_vp)]),
+    "rr_orbopt_destroy": (ctypes.c_int, [_vp]),
+    "rr_orbopt_info": (ctypes.c_int, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
+    "rr_orbopt_run": (ctypes.c_int, [_vp, ctypes.POINTER(AdamResult)]),
+    "rr_orbopt_energy": (ctypes.c_int, [_vp, ctypes.POINTER(_d)]),
+    "rr_orbopt_gradient": (ctypes.c_int, [_vp, _vp]),
+    "rr_orbopt_set_scales": (ctypes.c_int, [_vp, _vp]),
+    "rr_orbopt_hessian_diagonal": (ctypes.c_int, [_vp, _vp]),
+    "rr_orbopt_features": (ctypes.c_int, [_vp, _vp]),
+    "rr_orbopt_state": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    "rr_mlp_create": (ctypes.c_int, [ctypes.c_uint64, ctypes.POINTER(_vp)]),
+    "rr_mlp_destroy": (ctypes.c_int, [_vp]),
+    "rr_mlp_train": (ctypes.c_int, [_vp, _vp, _vp, _i64, _i32, _i32, ctypes.c_float, ctypes.c_uint64, _vp]),
+    "rr_mlp_predict": (ctypes.c_int, [_vp, _vp, _i64, _i32, _vp]),
+    "rr_mlp_loss_and_grad": (ctypes.c_int, [_vp, _vp, _vp, _i64, ctypes.POINTER(ctypes.c_float), _vp]),
+    "rr_mlp_get_params": (ctypes.c_int, [_vp, _vp]),
+    "rr_mlp_set_params": (ctypes.c_int, [_vp, _vp]),
+    "rr_test_adam_steps": (ctypes.c_int, [_i64, _i32, _i64, _d, _d, _d, _d, _vp, _vp]),
+    "rr_test_rotation_matrix": (ctypes.c_int, [_i64, _vp, _vp]),
+    "rr_test_adam_run_quadratic": (ctypes.c_int, [_i64, _vp, _vp, _d, _vp, _i32, _vp, _vp, _vp, _vp, _vp]),
     "rr_last_error": (ctypes.c_char_p, []),
     "rr_version": (ctypes.c_int, []),
     "rr_ri_create": (ctypes.c_int, [_vp, _i64, _i64, _i32, ctypes.POINTER(_vp)]),

@@ -1,0 +1,255 @@
+"""Orbital-rotation optimisation of the functional stage on the GPU, and its learned preconditioner.
+
+* ``RotationProblem``        src/Full_opt/FullOptimization.cpp:1330-1548 (RotationProblem) with
+                             ``run`` = AdamOptimizer::run, src/Utils/ADAM.cpp:140-213
+* ``adam_default_options``   AdamOptions, src/Utils/ADAM.h:41-60
+* ``run_full_optimization``  the orbital half of the FULL_OPTIMIZATION macro loop: repeated ADAM runs at
+                             fixed occupations until the best energy changes by less than ``tol`` without
+                             a restart request (m_noft_driver's rule, ADAM.h:205-209)
+* ``LearnedPreconditioner``  no counterpart in the reference: an MLP predicting the diagonal orbital
+                             Hessian (hartreeExchangeHessianElement(p,q,p,q)) from eight per-pair inputs;
+                             its predictions rescale the ADAM pairs (rr_orbopt_set_scales)
+
+The functional is a fixed-occupation hartree-exchange form (two_rdm_h, two_rdm_x and optionally the
+pair terms pair_of / two_rdm_l1 / two_rdm_l2) over the nonrelativistic spin-orbital RI tensor
+(``mo.RiNonRelSpinMoEri``), as in the reference's RI FULL_OPTIMIZATION.
+"""
+from __future__ import annotations
+
+import ctypes
+import time
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import RrError
+
+
+def _d(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def adam_default_options() -> L.AdamOptions:
+    o = L.AdamOptions()
+    L.check(L.lib().rr_adam_default_options(ctypes.byref(o)))
+    return o
+
+
+class RotationProblem:
+    """ADAM orbital-rotation problem on the GPU for `eri` (RiNonRelSpinMoEri, n spatial orbitals).
+
+    h: n x n spatial one-electron matrix in eri's MO basis; occupations: 2n; two_rdm_h / two_rdm_x:
+    2n x 2n; optional pair_of (2n) with two_rdm_l1 / two_rdm_l2 (2n x 2n)."""
+
+    def __init__(self, eri, h, occupations, two_rdm_h, two_rdm_x, pair_of=None, two_rdm_l1=None, two_rdm_l2=None,
+                 options: L.AdamOptions | None = None):
+        n = eri.n
+        d = 2 * n
+        h = _d(h)
+        if h.shape != (n, n):
+            raise RrError(L.RR_ERR_ARG, "RotationProblem: h must be the n x n spatial matrix")
+        occ = _d(occupations)
+        h2, x2 = _d(two_rdm_h), _d(two_rdm_x)
+        if occ.shape != (d,) or h2.shape != (d, d) or x2.shape != (d, d):
+            raise RrError(L.RR_ERR_ARG, "RotationProblem: occupations / two-RDMs must span the 2n spin orbitals")
+        po = None if pair_of is None else np.ascontiguousarray(pair_of, dtype=np.int64)
+        l1 = None if po is None else _d(two_rdm_l1)
+        l2 = None if po is None else _d(two_rdm_l2)
+        self.handle = ctypes.c_void_p()
+        L.check(L.lib().rr_orbopt_create(eri.handle, h.ctypes.data, occ.ctypes.data, h2.ctypes.data, x2.ctypes.data,
+                                         None if po is None else po.ctypes.data,
+                                         None if po is None else l1.ctypes.data,
+                                         None if po is None else l2.ctypes.data,
+                                         None if options is None else ctypes.byref(options), ctypes.byref(self.handle)))
+        self.n, self.d = n, d
+        self.n_pairs = d * (d - 1) // 2
+        p = np.array([pp for pp in range(d) for _ in range(pp)])
+        q = np.array([qq for pp in range(d) for qq in range(pp)])
+        self.pairs = np.stack([p, q], axis=1) if self.n_pairs else np.zeros((0, 2), dtype=int)
+        self.cross_spin = (p >= n) != (q >= n) if self.n_pairs else np.zeros(0, dtype=bool)
+
+    def close(self):
+        if self.handle and self.handle.value:
+            L.lib().rr_orbopt_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self) -> dict:
+        r = L.AdamResult()
+        L.check(L.lib().rr_orbopt_run(self.handle, ctypes.byref(r)))
+        return r.as_dict()
+
+    def energy(self) -> float:
+        e = ctypes.c_double()
+        L.check(L.lib().rr_orbopt_energy(self.handle, ctypes.byref(e)))
+        return e.value
+
+    def gradient(self) -> np.ndarray:
+        g = np.empty(self.n_pairs)
+        L.check(L.lib().rr_orbopt_gradient(self.handle, g.ctypes.data))
+        return g
+
+    def hessian_diagonal(self) -> np.ndarray:
+        h = np.empty(self.n_pairs)
+        L.check(L.lib().rr_orbopt_hessian_diagonal(self.handle, h.ctypes.data))
+        return h
+
+    def features(self) -> np.ndarray:
+        f = np.empty((self.n_pairs, 8), dtype=np.float32)
+        L.check(L.lib().rr_orbopt_features(self.handle, f.ctypes.data))
+        return f
+
+    def set_scales(self, scales=None):
+        if scales is None:
+            L.check(L.lib().rr_orbopt_set_scales(self.handle, None))
+            return
+        s = _d(scales)
+        if s.shape != (self.n_pairs,):
+            raise RrError(L.RR_ERR_ARG, "RotationProblem.set_scales: one scale per pair")
+        L.check(L.lib().rr_orbopt_set_scales(self.handle, s.ctypes.data))
+
+    def state(self, with_tensor: bool = False):
+        """(accumulated spatial rotation, rotated h, rotated MO tensor or None)."""
+        u = np.empty((self.n, self.n))
+        h = np.empty((self.n, self.n))
+        naux = ctypes.c_int64()
+        L.check(L.lib().rr_orbopt_info(self.handle, None, None, ctypes.byref(naux)))
+        b = np.empty((naux.value, self.n * self.n)) if with_tensor else None
+        L.check(L.lib().rr_orbopt_state(self.handle, u.ctypes.data, h.ctypes.data, None if b is None else b.ctypes.data))
+        return u, h, b
+
+
+def hessian_scales(problem: RotationProblem, hdiag, clip: float = 16.0) -> np.ndarray:
+    """Scales from a (predicted or exact) diagonal Hessian: |H| / median over the same-spin pairs,
+    clipped to [1/clip, 1], so pairs softer than the median take up to sqrt(clip) times larger
+    rotations and none is slowed down (shrinking the stiff pairs as well cost more iterations than it
+    saved on the synthetic functional-stage problems); cross-spin pairs (zero gradient) keep 1."""
+    h = np.abs(np.asarray(hdiag, dtype=float))
+    same = ~problem.cross_spin
+    med = np.median(h[same]) if same.any() else 1.0
+    if not med > 0:
+        med = 1.0
+    s = np.clip(h / med, 1.0 / clip, 1.0)
+    s[problem.cross_spin] = 1.0
+    return s
+
+
+class LearnedPreconditioner:
+    """The 8 -> 64 -> 64 -> 64 -> 1 MLP (librr_ri rr_mlp_*) mapping rr_orbopt_features to
+    log |H_diag|; trained in FP32, BF16 inference."""
+
+    N_PARAMS = 8961
+    N_NORM = 18
+
+    def __init__(self, seed: int = 0):
+        self.handle = ctypes.c_void_p()
+        L.check(L.lib().rr_mlp_create(ctypes.c_uint64(seed), ctypes.byref(self.handle)))
+
+    def close(self):
+        if self.handle and self.handle.value:
+            L.lib().rr_mlp_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def labels(hdiag) -> np.ndarray:
+        return np.log(np.maximum(np.abs(np.asarray(hdiag, dtype=float)), 1e-8)).astype(np.float32)
+
+    def train(self, X, y, epochs: int = 60, batch: int = 256, learning_rate: float = 2e-3, seed: int = 1):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        hist = np.empty(epochs, dtype=np.float32)
+        L.check(L.lib().rr_mlp_train(self.handle, X.ctypes.data, y.ctypes.data, X.shape[0], epochs, batch,
+                                     ctypes.c_float(learning_rate), ctypes.c_uint64(seed), hist.ctypes.data))
+        return hist
+
+    def predict(self, X, bf16: bool = True) -> np.ndarray:
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        y = np.empty(X.shape[0], dtype=np.float32)
+        L.check(L.lib().rr_mlp_predict(self.handle, X.ctypes.data, X.shape[0], int(bf16), y.ctypes.data))
+        return y
+
+    def loss_and_grad(self, X, y):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        g = np.empty(self.N_PARAMS, dtype=np.float32)
+        loss = ctypes.c_float()
+        L.check(L.lib().rr_mlp_loss_and_grad(self.handle, X.ctypes.data, y.ctypes.data, X.shape[0], ctypes.byref(loss),
+                                             g.ctypes.data))
+        return float(loss.value), g
+
+    def get_params(self) -> np.ndarray:
+        p = np.empty(self.N_PARAMS + self.N_NORM, dtype=np.float32)
+        L.check(L.lib().rr_mlp_get_params(self.handle, p.ctypes.data))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        if p.shape != (self.N_PARAMS + self.N_NORM,):
+            raise RrError(L.RR_ERR_ARG, "LearnedPreconditioner.set_params: wrong parameter count")
+        L.check(L.lib().rr_mlp_set_params(self.handle, p.ctypes.data))
+
+    def scales(self, problem: RotationProblem, clip: float = 16.0, bf16: bool = True) -> np.ndarray:
+        return hessian_scales(problem, np.exp(self.predict(problem.features(), bf16=bf16)), clip)
+
+
+def run_full_optimization(problem: RotationProblem, tol: float = 1e-8, max_macro: int = 400,
+                          preconditioner: LearnedPreconditioner | None = None, exact_hessian: bool = False,
+                          clip: float = 16.0) -> dict:
+    """Macro loop of ADAM runs at fixed occupations (the orbital half of FULL_OPTIMIZATION): stop when
+    two successive runs' best energies differ by less than `tol` and the optimiser asked for no
+    restart.  With a preconditioner (or exact_hessian) the pair scales are refreshed before every
+    run from the current orbitals."""
+    t0 = time.perf_counter()
+    e_prev = None
+    steps = 0
+    history = []
+    for m in range(1, max_macro + 1):
+        if preconditioner is not None:
+            problem.set_scales(preconditioner.scales(problem, clip))
+        elif exact_hessian:
+            problem.set_scales(hessian_scales(problem, problem.hessian_diagonal(), clip))
+        r = problem.run()
+        steps += r["iterations"]
+        history.append(r["energy_best"])
+        if e_prev is not None and abs(r["energy_best"] - e_prev) < tol and not r["restart_requested"]:
+            return dict(macro_iterations=m, adam_steps=steps, energy=r["energy_best"], converged=True,
+                        seconds=time.perf_counter() - t0, history=np.array(history))
+        e_prev = r["energy_best"]
+    return dict(macro_iterations=max_macro, adam_steps=steps, energy=history[-1], converged=False,
+                seconds=time.perf_counter() - t0, history=np.array(history))
+
+
+def muller_functional(occ_spatial):
+    """Spin-orbital occupations and the Mueller-type two-RDM factors two_rdm_h = n_p n_q,
+    two_rdm_x = sqrt(n_p n_q) of a fixed set of spatial occupations (a JK-only functional)."""
+    n = np.concatenate([occ_spatial, occ_spatial]).astype(float)
+    return n, np.outer(n, n), np.sqrt(np.outer(n, n))
+
+
+def training_data(problems, samples_per_problem: int = 4, runs_between: int = 2, rng=None):
+    """(features, labels) from each problem at several points of its plain-ADAM path: features from
+    rr_orbopt_features, labels log |hartreeExchangeHessianElement(p,q,p,q)|, same-spin pairs only."""
+    rng = rng if rng is not None else np.random.default_rng(0)
+    Xs, ys = [], []
+    for prob in problems:
+        prob.set_scales(None)
+        for k in range(samples_per_problem):
+            f = prob.features()
+            hd = prob.hessian_diagonal()
+            keep = ~prob.cross_spin
+            Xs.append(f[keep])
+            ys.append(LearnedPreconditioner.labels(hd[keep]))
+            for _ in range(runs_between):
+                prob.run()
+    return np.concatenate(Xs), np.concatenate(ys)
