@@ -253,3 +253,24 @@ def training_data(problems, samples_per_problem: int = 4, runs_between: int = 2,
             for _ in range(runs_between):
                 prob.run()
     return np.concatenate(Xs), np.concatenate(ys)
+
+
+PARAMS_FILE = __import__("pathlib").Path(__file__).resolve().parent / "data" / "precond_mlp.npy"
+
+
+def problem_from_system(sysd: dict, options: L.AdamOptions | None = None):
+    """(RotationProblem, MO tensor) for a dict of rerdmft_b200.synth.functional_system's form."""
+    from .mo import RiNonRelSpinMoEri
+
+    eri = RiNonRelSpinMoEri.from_tensor(sysd["Bmo"], sysd["ns"])
+    extra = {k: sysd[k] for k in ("pair_of", "two_rdm_l1", "two_rdm_l2") if k in sysd}
+    prob = RotationProblem(eri, sysd["h"], sysd["occupations"], sysd["two_rdm_h"], sysd["two_rdm_x"],
+                           options=options, **extra)
+    return prob, eri
+
+
+def load_default_preconditioner() -> LearnedPreconditioner:
+    """The preconditioner trained by ``python -m rerdmft_b200.precond_train`` (shipped parameters)."""
+    net = LearnedPreconditioner(seed=0)
+    net.set_params(np.load(PARAMS_FILE))
+    return net

@@ -205,3 +205,32 @@ def rkb_system(nl: int, ns: int, naux: int, n_electrons: int, seed: int, b_scale
     P0 = kramers_even(occ_cols @ occ_cols.conj().T, 4)
     return dict(nl=nl, ns=ns, naux=naux, B_LL=B_LL, B_SS=B_SS, v_total=v, s_full=s_full, x_full=x_full,
                 h=h_rkb, P0=P0, n_electrons=n_electrons, n_rkb=n_rkb, n_ukb=n_ukb)
+
+
+def functional_system(ns: int, naux: int, seed: int, nocc: int | None = None, with_pairs: bool = False,
+                      box: float = 8.0) -> dict:
+    """Fixed-occupation functional-stage inputs for the nonrelativistic spin-orbital RI tensor: an
+    MO-basis tensor (naux, ns^2) of the cube/Gaussian recipe in a random orthonormal basis, a
+    one-electron matrix h with nocc low levels (not diagonal in that basis), natural occupations
+    (nocc near 1, the rest decaying from 0.05) with the Mueller-type two-RDM factors
+    two_rdm_h = n_p n_q, two_rdm_x = sqrt(n_p n_q) over the 2 ns spin orbitals, and optionally
+    small random pair terms (pair_of, two_rdm_l1, two_rdm_l2)."""
+    rng = np.random.default_rng(seed)
+    B = ri_tensor(ns, naux, seed, box=box)
+    B *= 2.4 / max(1e-30, np.sqrt(np.abs(B).max() * np.sqrt(naux)))
+    q = random_orthogonal(ns, rng)
+    Bmo = np.einsum("ai,Pab,bj->Pij", q, B.reshape(naux, ns, ns), q, optimize=True).reshape(naux, ns * ns)
+    nocc = max(1, ns // 4) if nocc is None else nocc
+    e = np.sort(np.concatenate([-3.0 + rng.random(nocc), 0.5 + 3 * rng.random(ns - nocc)]))
+    qq = random_orthogonal(ns, rng)
+    h = (qq * e) @ qq.T
+    occ_sp = np.concatenate([0.97 - 0.05 * rng.random(nocc), 0.05 * np.exp(-np.arange(ns - nocc) / 2.0)])
+    occ = np.concatenate([occ_sp, occ_sp])
+    out = dict(ns=ns, naux=naux, Bmo=Bmo, h=h, occupations=occ, two_rdm_h=np.outer(occ, occ),
+               two_rdm_x=np.sqrt(np.outer(occ, occ)))
+    if with_pairs:
+        d = 2 * ns
+        out["pair_of"] = np.array([(i + 1) % d if i % 2 == 0 else i - 1 for i in range(d)])
+        out["two_rdm_l1"] = 0.01 * rng.standard_normal((d, d))
+        out["two_rdm_l2"] = 0.01 * rng.standard_normal((d, d))
+    return out
