@@ -205,29 +205,44 @@ class LearnedPreconditioner:
 
 def run_full_optimization(problem: RotationProblem, tol: float = 1e-8, max_macro: int = 400,
                           preconditioner: LearnedPreconditioner | None = None, exact_hessian: bool = False,
-                          clip: float = 16.0) -> dict:
+                          clip: float = 16.0, polish: bool = True) -> dict:
     """Macro loop of ADAM runs at fixed occupations (the orbital half of FULL_OPTIMIZATION): stop when
     two successive runs' best energies differ by less than `tol` and the optimiser asked for no
     restart.  With a preconditioner (or exact_hessian) the pair scales are refreshed before every
-    run from the current orbitals."""
+    run from the current orbitals; with `polish` the plain method then continues from the
+    preconditioned result until it meets the same rule, so plain ADAM judges the converged energy
+    (the rescaled runs only move the start).  Iterations of both phases are counted."""
     t0 = time.perf_counter()
-    e_prev = None
     steps = 0
     history = []
-    for m in range(1, max_macro + 1):
-        if preconditioner is not None:
-            problem.set_scales(preconditioner.scales(problem, clip))
-        elif exact_hessian:
-            problem.set_scales(hessian_scales(problem, problem.hessian_diagonal(), clip))
-        r = problem.run()
-        steps += r["iterations"]
-        history.append(r["energy_best"])
-        if e_prev is not None and abs(r["energy_best"] - e_prev) < tol and not r["restart_requested"]:
-            return dict(macro_iterations=m, adam_steps=steps, energy=r["energy_best"], converged=True,
-                        seconds=time.perf_counter() - t0, history=np.array(history))
-        e_prev = r["energy_best"]
-    return dict(macro_iterations=max_macro, adam_steps=steps, energy=history[-1], converged=False,
-                seconds=time.perf_counter() - t0, history=np.array(history))
+    scaled = preconditioner is not None or exact_hessian
+    phases = ["scaled", "plain"] if scaled and polish else (["scaled"] if scaled else ["plain"])
+    m = 0
+    converged = False
+    scaled_macro = 0
+    e_prev = None
+    for phase in phases:
+        if phase == "plain":
+            problem.set_scales(None)
+        # the plain rule compares with the previous run's best energy, whichever phase ran it
+        converged = False
+        while m < max_macro:
+            m += 1
+            if phase == "scaled":
+                scaled_macro += 1
+                if preconditioner is not None:
+                    problem.set_scales(preconditioner.scales(problem, clip))
+                else:
+                    problem.set_scales(hessian_scales(problem, problem.hessian_diagonal(), clip))
+            r = problem.run()
+            steps += r["iterations"]
+            history.append(r["energy_best"])
+            if e_prev is not None and abs(r["energy_best"] - e_prev) < tol and not r["restart_requested"]:
+                converged = True
+                break
+            e_prev = r["energy_best"]
+    return dict(macro_iterations=m, adam_steps=steps, energy=history[-1], converged=converged,
+                scaled_macro_iterations=scaled_macro, seconds=time.perf_counter() - t0, history=np.array(history))
 
 
 def muller_functional(occ_spatial):
