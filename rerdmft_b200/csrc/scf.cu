@@ -53,29 +53,59 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
   return t;
 }
 
-// Gershgorin bounds of a symmetric / Hermitian n x n matrix (PL = 2: interleaved complex):
-// out[0] = min_i (a_ii - r_i), out[1] = max (a_ii + r_i), r_i = sum_{j != i} |a_ij|.
+// Two-stage reductions: RED_CTAS CTAs write one partial each (CTA b owns a fixed chunk), then one
+// CTA per row combines the partials in a fixed order, so sums are identical run to run.
+constexpr int RED_CTAS = 256;
+
+template <int OP>  // 0 sum, 1 min, 2 max
+__global__ void reduce_partials_kernel(const double* part, int cols, double scale, double* out) {
+  __shared__ double red[32];
+  const double* row = part + static_cast<int64_t>(blockIdx.x) * cols;
+  double v = OP == 0 ? 0.0 : (OP == 1 ? 1e300 : -1e300);
+  for (int i = threadIdx.x; i < cols; i += blockDim.x) v = OP == 0 ? v + row[i] : (OP == 1 ? fmin(v, row[i]) : fmax(v, row[i]));
+  for (int o = 16; o > 0; o >>= 1) {
+    const double w = __shfl_xor_sync(0xffffffffu, v, o);
+    v = OP == 0 ? v + w : (OP == 1 ? fmin(v, w) : fmax(v, w));
+  }
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = red[0];
+    for (int w = 1; w < static_cast<int>(blockDim.x >> 5); ++w)
+      t = OP == 0 ? t + red[w] : (OP == 1 ? fmin(t, red[w]) : fmax(t, red[w]));
+    out[blockIdx.x] = scale * t;
+  }
+}
+
+__device__ __forceinline__ void chunk_of(int64_t cnt, int64_t& beg, int64_t& end) {
+  const int64_t per = (cnt + gridDim.x - 1) / gridDim.x;
+  beg = blockIdx.x * per;
+  end = beg + per < cnt ? beg + per : cnt;
+}
+
+// Gershgorin bounds, stage 1: a warp per row; part[0][b] = min (a_ii - r_i), part[1][b] = max (a_ii + r_i)
+// over this CTA's rows.
 template <int PL>
-__global__ void gershgorin_kernel(const double* A, int64_t n, double* out) {
+__global__ void gershgorin_partial_kernel(const double* A, int64_t n, double* part) {
   __shared__ double lo_s[32], hi_s[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   double lo = 1e300, hi = -1e300;
-  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * nw + warp; i < n; i += static_cast<int64_t>(gridDim.x) * nw) {
     double r = 0.0;
-    for (int64_t j = 0; j < n; ++j)
+    for (int64_t j = lane; j < n; j += 32)
       if (j != i) r += PL == 2 ? hypot(A[(i * n + j) * PL], A[(i * n + j) * PL + 1]) : fabs(A[i * n + j]);
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
     lo = fmin(lo, A[(i * n + i) * PL] - r);
     hi = fmax(hi, A[(i * n + i) * PL] + r);
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-    hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-  }
-  if ((threadIdx.x & 31) == 0) { lo_s[threadIdx.x >> 5] = lo; hi_s[threadIdx.x >> 5] = hi; }
+  if (lane == 0) { lo_s[warp] = lo; hi_s[warp] = hi; }
   __syncthreads();
   if (threadIdx.x == 0) {
-    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) { lo = fmin(lo, lo_s[w]); hi = fmax(hi, hi_s[w]); }
-    out[0] = lo;
-    out[1] = hi;
+    for (int w = 1; w < nw; ++w) { lo = fmin(lo, lo_s[w]); hi = fmax(hi, hi_s[w]); }
+    lo = fmin(lo, lo_s[0]);
+    hi = fmax(hi, hi_s[0]);
+    part[blockIdx.x] = lo;
+    part[gridDim.x + blockIdx.x] = hi;
   }
 }
 
@@ -115,33 +145,37 @@ __global__ void sp2_update_kernel(double* X, const double* T, int64_t cnt, const
     X[idx] = square ? T[idx] : 2.0 * X[idx] - T[idx];
 }
 
-// out[0] = 1/2 Re Tr[P (h + F)] = 1/2 Re sum_ij P_ij (h + F)_ji  (one CTA)
+// Stage 1 of 1/2 Re Tr[P (h + F)]: part[b] = this CTA's share of sum_ij P_ij (h + F)_ji.
 template <int PL>
-__global__ void energy_kernel(const double* P, const double* h, const double* F, int64_t n, double* out) {
+__global__ void energy_partial_kernel(const double* P, const double* h, const double* F, int64_t n, double* part) {
   __shared__ double red[32];
+  int64_t beg, end;
+  chunk_of(n * n, beg, end);
   double acc = 0.0;
-  for (int64_t idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+  for (int64_t idx = beg + threadIdx.x; idx < end; idx += blockDim.x) {
     const int64_t i = idx / n, j = idx % n, t = j * n + i;
     acc += P[idx * PL] * (h[t * PL] + F[t * PL]);
     if (PL == 2) acc -= P[idx * PL + 1] * (h[t * PL + 1] + F[t * PL + 1]);
   }
   acc = block_sum(acc, red);
-  if (threadIdx.x == 0) out[0] = 0.5 * acc;
+  if (threadIdx.x == 0) part[blockIdx.x] = acc;
 }
 
-// out[0] = max |A - B| over cnt (complex) elements (one CTA)
+// Stage 1 of max |A - B|.
 template <int PL>
-__global__ void maxdiff_kernel(const double* A, const double* B, int64_t cnt, double* out) {
+__global__ void maxdiff_partial_kernel(const double* A, const double* B, int64_t cnt, double* part) {
   __shared__ double red[32];
+  int64_t beg, end;
+  chunk_of(cnt, beg, end);
   double m = 0.0;
-  for (int64_t i = threadIdx.x; i < cnt; i += blockDim.x)
+  for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x)
     m = fmax(m, PL == 2 ? hypot(A[2 * i] - B[2 * i], A[2 * i + 1] - B[2 * i + 1]) : fabs(A[i] - B[i]));
   for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
   __syncthreads();
   if (threadIdx.x == 0) {
-    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
-    out[0] = m;
+    for (int w = 1; w < static_cast<int>(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
+    part[blockIdx.x] = m;
   }
 }
 
@@ -168,14 +202,16 @@ struct DotArgs {
   int count;
 };
 
-// out[k] = <e, v_k> for k < count (one CTA, fixed order)
-__global__ void diis_dots_kernel(const double* e, DotArgs a, int64_t cnt, double* out) {
+// Stage 1 of <e, v_k>: part[k][b] = this CTA's share.
+__global__ void diis_dots_partial_kernel(const double* e, DotArgs a, int64_t cnt, double* part) {
   __shared__ double red[32];
+  int64_t beg, end;
+  chunk_of(cnt, beg, end);
   for (int k = 0; k < a.count; ++k) {
     double acc = 0.0;
-    for (int64_t i = threadIdx.x; i < cnt; i += blockDim.x) acc += e[i] * a.v[k][i];
+    for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) acc += e[i] * a.v[k][i];
     acc = block_sum(acc, red);
-    if (threadIdx.x == 0) out[k] = acc;
+    if (threadIdx.x == 0) part[k * gridDim.x + blockIdx.x] = acc;
   }
 }
 
@@ -240,7 +276,7 @@ struct DeviceDiis {
     const int slots = std::max(maxv, 1);
     err.alloc(static_cast<size_t>(slots * length));
     val.alloc(static_cast<size_t>(slots * length));
-    dots.alloc(DIIS_MAX);
+    dots.alloc(DIIS_MAX * (RED_CTAS + 1));
     order.clear();
     bmat.assign(slots, std::vector<double>(slots, 0.0));
   }
@@ -263,7 +299,10 @@ struct DeviceDiis {
     DotArgs a{};
     a.count = static_cast<int>(order.size());
     for (int k = 0; k < a.count; ++k) a.v[k] = err.p + order[k] * len;
-    diis_dots_kernel<<<1, 1024, 0, s>>>(err.p + slot * len, a, len, dots.p);
+    double* part = dots.p + DIIS_MAX;
+    diis_dots_partial_kernel<<<RED_CTAS, 256, 0, s>>>(err.p + slot * len, a, len, part);
+    RR_LAUNCH_CHECK();
+    reduce_partials_kernel<0><<<a.count, 256, 0, s>>>(part, RED_CTAS, 1.0, dots.p);
     RR_LAUNCH_CHECK();
     std::vector<double> d(a.count);
     RR_CUDA(cudaMemcpyAsync(d.data(), dots.p, sizeof(double) * a.count, cudaMemcpyDeviceToHost, s));
@@ -300,21 +339,23 @@ struct DeviceDiis {
 void sp2_projector(rr_ri_store* h, const double* F, int64_t n, int64_t nocc, double* Pi, double* T, double* scal,
                    cudaStream_t s, bool cplx) {
   const int PL = cplx ? 2 : 1;
-  if (cplx) {
-    gershgorin_kernel<2><<<1, 512, 0, s>>>(F, n, scal);
-    RR_LAUNCH_CHECK();
-    sp2_init_kernel<2><<<blocks_for(n * n), 256, 0, s>>>(Pi, F, n, scal);
-  } else {
-    gershgorin_kernel<1><<<1, 512, 0, s>>>(F, n, scal);
-    RR_LAUNCH_CHECK();
-    sp2_init_kernel<1><<<blocks_for(n * n), 256, 0, s>>>(Pi, F, n, scal);
-  }
+  h->work.ensure(static_cast<size_t>(std::max<int64_t>(static_cast<int64_t>(h->work.n), 8 * n * n * PL)));
+  double* part = h->work.p;  // free until the first GEMM below (same stream)
+  const int gcta = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(RED_CTAS, (n + 7) / 8)));
+  if (cplx) gershgorin_partial_kernel<2><<<gcta, 256, 0, s>>>(F, n, part);
+  else gershgorin_partial_kernel<1><<<gcta, 256, 0, s>>>(F, n, part);
+  RR_LAUNCH_CHECK();
+  reduce_partials_kernel<1><<<1, 256, 0, s>>>(part, gcta, 1.0, scal);
+  RR_LAUNCH_CHECK();
+  reduce_partials_kernel<2><<<1, 256, 0, s>>>(part + gcta, gcta, 1.0, scal + 1);
+  RR_LAUNCH_CHECK();
+  if (cplx) sp2_init_kernel<2><<<blocks_for(n * n), 256, 0, s>>>(Pi, F, n, scal);
+  else sp2_init_kernel<1><<<blocks_for(n * n), 256, 0, s>>>(Pi, F, n, scal);
   RR_LAUNCH_CHECK();
   GemmDesc g;
   g.cplx = cplx;
   g.M = n; g.N = n; g.K = n;
   g.A = Pi; g.lda = n; g.B = Pi; g.ldb = n; g.C = T; g.ldc = n;
-  h->work.ensure(static_cast<size_t>(std::max<int64_t>(static_cast<int64_t>(h->work.n), 8 * n * n * PL)));
   const double N = static_cast<double>(nocc);
   for (int it = 0; it < 120; ++it) {
     gemm(g, s, h->work.p, static_cast<int64_t>(h->work.n));
@@ -348,7 +389,7 @@ void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff
   const int64_t pitch = round_up(std::max<int64_t>(n2, 2), 32);
   DevBuf<double> buf;
   Arena ar(&buf);
-  double *hd, *Xd, *Sd, *P, *Pn, *F, *J, *K, *Fs, *e, *PS, *SP, *tmp, *Fo, *Pi, *T2, *Ct, *scal;
+  double *hd, *Xd, *Sd, *P, *Pn, *F, *J, *K, *Fs, *e, *PS, *SP, *tmp, *Fo, *Pi, *T2, *Ct, *scal, *red;
   ar.request(&hd, n2);
   ar.request(&Xd, n * n_eff);
   ar.request(&Sd, n2);
@@ -367,6 +408,7 @@ void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff
   ar.request(&T2, n_eff * n_eff);
   ar.request(&Ct, nocc * n);
   ar.request(&scal, 64);
+  ar.request(&red, RED_CTAS);
   ar.commit();
   copy_in(hd, hc, n2, host, s);
   copy_in(Xd, X, n * n_eff, host, s);
@@ -408,7 +450,9 @@ void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff
       ++n_fp64;
     }
     // ---- energy with the un-extrapolated F ----
-    energy_kernel<1><<<1, 1024, 0, s>>>(P, hd, F, n, scal);
+    energy_partial_kernel<1><<<RED_CTAS, 256, 0, s>>>(P, hd, F, n, red);
+    RR_LAUNCH_CHECK();
+    reduce_partials_kernel<0><<<1, 256, 0, s>>>(red, RED_CTAS, 0.5, scal);
     RR_LAUNCH_CHECK();
     // ---- DIIS on e = F P S - S P F ----
     if (use_diis) {
@@ -437,7 +481,9 @@ void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff
     dp.M = n; dp.N = n; dp.K = nocc; dp.A = Ct; dp.lda = n; dp.opA = Op::T; dp.B = Ct; dp.ldb = n; dp.C = Pn; dp.ldc = n;
     dp.alpha = 2.0;
     gemm(dp, s, h->work.p, static_cast<int64_t>(h->work.n));
-    maxdiff_kernel<1><<<1, 1024, 0, s>>>(Pn, P, n2, scal + 1);
+    maxdiff_partial_kernel<1><<<RED_CTAS, 256, 0, s>>>(Pn, P, n2, red);
+    RR_LAUNCH_CHECK();
+    reduce_partials_kernel<2><<<1, 256, 0, s>>>(red, RED_CTAS, 1.0, scal + 1);
     RR_LAUNCH_CHECK();
     double hv[2];
     RR_CUDA(cudaMemcpyAsync(hv, scal, sizeof(hv), cudaMemcpyDeviceToHost, s));
@@ -490,7 +536,7 @@ void scf_rel(rr_ri_store* h, int kind, const double* hc, const double* v_total, 
   const int64_t nu = dhf ? 2 * h->n + 2 * h->ns : 0;
   DevBuf<double> buf;
   Arena ar(&buf);
-  double *hd, *Xd, *Sd, *vd = nullptr, *P, *Pn, *F, *Fs, *e, *PS, *SP, *tmp, *Fo, *Pi, *Pi2, *T2, *scal;
+  double *hd, *Xd, *Sd, *vd = nullptr, *P, *Pn, *F, *Fs, *e, *PS, *SP, *tmp, *Fo, *Pi, *Pi2, *T2, *scal, *red;
   ar.request(&hd, c2);
   ar.request(&Xd, ce);
   ar.request(&Sd, c2);
@@ -508,6 +554,7 @@ void scf_rel(rr_ri_store* h, int kind, const double* hc, const double* v_total, 
   ar.request(&Pi2, dhf ? ee : 1);
   ar.request(&T2, ee);
   ar.request(&scal, 64);
+  ar.request(&red, RED_CTAS);
   ar.commit();
   copy_in(hd, hc, c2, host, s);
   copy_in(Xd, X, ce, host, s);
@@ -541,7 +588,9 @@ void scf_rel(rr_ri_store* h, int kind, const double* hc, const double* v_total, 
   for (it = 1; it <= so->max_iterations; ++it) {
     if (dhf) fock_rkb(h, hd, vd, n, Sd, Xd, n_eff, P, F, &od);
     else fock_x2c(h, hd, P, Sd, Xd, n_eff, F, &od);
-    energy_kernel<2><<<1, 1024, 0, s>>>(P, hd, F, n, scal);
+    energy_partial_kernel<2><<<RED_CTAS, 256, 0, s>>>(P, hd, F, n, red);
+    RR_LAUNCH_CHECK();
+    reduce_partials_kernel<0><<<1, 256, 0, s>>>(red, RED_CTAS, 0.5, scal);
     RR_LAUNCH_CHECK();
     if (use_diis) {
       g.A = P; g.B = Sd; g.C = PS; g.alpha = 1.0; g.beta = 0.0;
@@ -583,7 +632,9 @@ void scf_rel(rr_ri_store* h, int kind, const double* hc, const double* v_total, 
       kramers_even_kernel<<<blocks_for(n2), 256, 0, s>>>(Pn, e, n, nb);
       RR_LAUNCH_CHECK();
     }
-    maxdiff_kernel<2><<<1, 1024, 0, s>>>(Pn, P, n2, scal + 1);
+    maxdiff_partial_kernel<2><<<RED_CTAS, 256, 0, s>>>(Pn, P, n2, red);
+    RR_LAUNCH_CHECK();
+    reduce_partials_kernel<2><<<1, 256, 0, s>>>(red, RED_CTAS, 1.0, scal + 1);
     RR_LAUNCH_CHECK();
     double hv[2];
     RR_CUDA(cudaMemcpyAsync(hv, scal, sizeof(hv), cudaMemcpyDeviceToHost, s));
