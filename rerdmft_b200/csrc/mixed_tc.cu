@@ -193,6 +193,175 @@ __global__ void __launch_bounds__(128, 1)
   if (warp == 0) tmem_dealloc(tmem, CF::TMEM_COLS);
 }
 
+// Persistent half-transform: one CTA per SM walks the (P, 128-row tile) items round robin with one
+// continuous TMA ring across items and two TMEM accumulators, so the epilogue of item j (TMEM ->
+// split BF16 rows of T2D) overlaps the MMAs of item j + 1.  Roles: warps 0-3 drain TMEM (lanes
+// 32 w .. 32 w + 31) and write T2D, warp 4 lane 0 issues the TMA ring, warp 5 lane 0 the MMAs.
+// Barriers: full / empty per ring stage, tfull / tempty per accumulator (MMA commit -> epilogue,
+// four epilogue warps -> MMA), mdone (all MMAs retired) before TMEM is released.  All waits bounded.
+constexpr int HT_THREADS = 192;
+constexpr int ERR_HT_FULL = 1 << 7, ERR_HT_EMPTY = 1 << 8, ERR_HT_TFULL = 1 << 9, ERR_HT_TEMPTY = 1 << 10,
+              ERR_HT_DONE = 1 << 11;
+
+template <int BN, int STAGES>
+struct HCfg {
+  static constexpr int B_TILE = BN * BK * 2;
+  static constexpr int STAGE = 2 * A_TILE + 2 * B_TILE;
+  static constexpr int BNP = BN <= 32 ? 32 : (BN <= 64 ? 64 : 128);  // TMEM columns per accumulator
+  static constexpr int TMEM_COLS = 2 * BNP <= 64 ? 64 : (2 * BNP <= 128 ? 128 : 256);
+  static constexpr int SMEM = STAGES * STAGE + 1024 + 256;
+  static_assert(B_TILE % 1024 == 0, "B tile must keep 1024-byte alignment");
+  static_assert(BN % 16 == 0 && BN >= 16 && BN <= 128, "UMMA N for M = 128");
+};
+
+template <int BN, int STAGES>
+__global__ void __launch_bounds__(HT_THREADS, 1)
+    umma_ht_persistent_kernel(const __grid_constant__ CUtensorMap mapA_hi, const __grid_constant__ CUtensorMap mapA_lo,
+                              const __grid_constant__ CUtensorMap mapB_hi, const __grid_constant__ CUtensorMap mapB_lo,
+                              const UParams p, int mtiles, int naux) {
+  using CF = HCfg<BN, STAGES>;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * CF::STAGE);
+  uint64_t* empty = full + STAGES;
+  uint64_t* tfull = empty + STAGES;
+  uint64_t* tempty = tfull + 2;
+  uint64_t* mdone = tempty + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mdone + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t total = static_cast<int64_t>(mtiles) * naux;
+  const int nkb = p.kblocks;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+    for (int b = 0; b < 2; ++b) { mbar_init(&tfull[b], 1); mbar_init(&tempty[b], 4); }
+    mbar_init(mdone, 1);
+    fence_barrier_init();
+    prefetch_tmap(&mapA_hi);
+    prefetch_tmap(&mapA_lo);
+    prefetch_tmap(&mapB_hi);
+    prefetch_tmap(&mapB_lo);
+  }
+  if (warp == 0) {
+    tmem_alloc(tmem_slot, CF::TMEM_COLS);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  bool dead = false;
+
+  if (warp == 4) {
+    if (lane == 0) {  // TMA producer
+      uint32_t q = 0;
+      for (int64_t item = blockIdx.x; item < total && !dead; item += gridDim.x) {
+        const int P = static_cast<int>(item / mtiles), m0 = static_cast<int>(item % mtiles) * BM;
+        for (int k = 0; k < nkb; ++k, ++q) {
+          const int s = q % STAGES;
+          if (q >= STAGES && !mbar_wait(&empty[s], ((q / STAGES) & 1) ^ 1, p.err, ERR_HT_EMPTY, dead)) break;
+          unsigned char* st = smem + s * CF::STAGE;
+          const int kc = k * BK;
+          mbar_arrive_expect_tx(&full[s], CF::STAGE);
+          tma_load_3d(st, &mapA_hi, kc, m0, P, &full[s]);
+          tma_load_3d(st + A_TILE, &mapA_lo, kc, m0, P, &full[s]);
+          tma_load_2d(st + 2 * A_TILE, &mapB_hi, kc, 0, &full[s]);
+          tma_load_2d(st + 2 * A_TILE + CF::B_TILE, &mapB_lo, kc, 0, &full[s]);
+        }
+      }
+    }
+  } else if (warp == 5) {
+    if (lane == 0) {  // MMA issuer
+      constexpr uint32_t idesc = idesc_bf16_f32(BM, BN);
+      uint32_t q = 0, j = 0;
+      for (int64_t item = blockIdx.x; item < total; item += gridDim.x, ++j) {
+        const uint32_t b = j & 1;
+        if (j >= 2) mbar_wait(&tempty[b], ((j >> 1) - 1) & 1, p.err, ERR_HT_TEMPTY, dead);
+        tc_fence_after();
+        const uint32_t d = tmem + b * CF::BNP;
+        for (int k = 0; k < nkb; ++k, ++q) {
+          const int s = q % STAGES;
+          mbar_wait(&full[s], (q / STAGES) & 1, p.err, ERR_HT_FULL, dead);
+          tc_fence_after();
+          if (!dead) {
+            const uint32_t base = smem_u32(smem + s * CF::STAGE);
+            const uint64_t ahi = sdesc_k_sw128(base), alo = sdesc_k_sw128(base + A_TILE);
+            const uint64_t bhi = sdesc_k_sw128(base + 2 * A_TILE), blo = sdesc_k_sw128(base + 2 * A_TILE + CF::B_TILE);
+#pragma unroll
+            for (int kk = 0; kk < BK / 16; ++kk) {
+              const uint64_t dk = static_cast<uint64_t>(kk * 32) >> 4;
+              umma_bf16(d, ahi + dk, bhi + dk, idesc, (k > 0 || kk > 0) ? 1u : 0u);
+              umma_bf16(d, ahi + dk, blo + dk, idesc, 1u);
+              umma_bf16(d, alo + dk, bhi + dk, idesc, 1u);
+            }
+          }
+          umma_commit(&empty[s]);
+        }
+        umma_commit(&tfull[b]);
+        if (dead) break;
+      }
+      umma_commit(mdone);
+    }
+  } else {  // epilogue warps 0-3
+    uint32_t j = 0;
+    const uint32_t lane_base = static_cast<uint32_t>(warp * 32) << 16;
+    for (int64_t item = blockIdx.x; item < total; item += gridDim.x, ++j) {
+      const uint32_t b = j & 1;
+      const bool ok = mbar_wait(&tfull[b], (j >> 1) & 1, p.err, ERR_HT_TFULL, dead);
+      tc_fence_after();
+      float v[BN];
+      if (ok) {
+#pragma unroll
+        for (int c0 = 0; c0 < BN; c0 += 16) tmem_ld16(tmem + lane_base + b * CF::BNP + c0, v + c0);
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty[b]);
+      if (!ok) break;
+      const int P = static_cast<int>(item / mtiles), m0 = static_cast<int>(item % mtiles) * BM;
+      const int row = m0 + warp * 32 + lane;
+      if (row < p.M) {
+        const int64_t rbase = static_cast<int64_t>(row) * p.t_ld + static_cast<int64_t>(P) * p.nocc;
+        if ((p.nocc & 7) == 0 && (p.t_ld & 7) == 0) {
+          // 16-byte stores: rbase is a multiple of 8 elements when nocc and the row pitch are
+#pragma unroll
+          for (int c = 0; c < BN; c += 8) {
+            if (c < p.nocc) {
+              uint32_t h[4], l[4];
+#pragma unroll
+              for (int e = 0; e < 4; ++e) {
+                const __nv_bfloat16 h0 = __float2bfloat16_rn(v[c + 2 * e]), h1 = __float2bfloat16_rn(v[c + 2 * e + 1]);
+                const __nv_bfloat16 l0 = __float2bfloat16_rn(v[c + 2 * e] - __bfloat162float(h0));
+                const __nv_bfloat16 l1 = __float2bfloat16_rn(v[c + 2 * e + 1] - __bfloat162float(h1));
+                h[e] = static_cast<uint32_t>(__bfloat16_as_ushort(h0)) | (static_cast<uint32_t>(__bfloat16_as_ushort(h1)) << 16);
+                l[e] = static_cast<uint32_t>(__bfloat16_as_ushort(l0)) | (static_cast<uint32_t>(__bfloat16_as_ushort(l1)) << 16);
+              }
+              *reinterpret_cast<uint4*>(p.t_hi + rbase + c) = make_uint4(h[0], h[1], h[2], h[3]);
+              *reinterpret_cast<uint4*>(p.t_lo + rbase + c) = make_uint4(l[0], l[1], l[2], l[3]);
+            }
+          }
+        } else {
+#pragma unroll
+          for (int c = 0; c < BN; ++c) {
+            if (c < p.nocc) {
+              const __nv_bfloat16 hi = __float2bfloat16_rn(v[c]);
+              p.t_hi[rbase + c] = hi;
+              p.t_lo[rbase + c] = __float2bfloat16_rn(v[c] - __bfloat162float(hi));
+            }
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (warp == 0) {
+    bool ddead = false;
+    mbar_wait(mdone, 0, p.err, ERR_HT_DONE, ddead);  // every MMA retired before TMEM is released
+    tc_fence_after();
+    tmem_dealloc(tmem, CF::TMEM_COLS);
+  }
+}
+
 // Fixed-order reduction of the split-K partial tiles into K (FP64), mirrored to the lower
 // triangle: K[a][b] = sum_s work[s][pair(a,b)][a % BM][b % BN].
 template <int BN>
@@ -387,8 +556,18 @@ void mixed_exchange(MixedOperands& mo, const double* Ct, int64_t ldct, int64_t n
       p.err = err;
       // Columns [kt, ldt) of T2D are row padding for TMA alignment; the maps' extents stop at kt,
       // so they are never read.
-      launch_umma<HT_BN, 4, 0>(a_hi, a_lo, b_hi, b_lo, p, dim3(static_cast<unsigned>((n + BM - 1) / BM),
-                                                              static_cast<unsigned>(naux)), s);
+      const int mtiles = static_cast<int>((n + BM - 1) / BM);
+      using HC = HCfg<HT_BN, 4>;
+      auto kern = umma_ht_persistent_kernel<HT_BN, 4>;
+      static bool attr = false;
+      if (!attr) {
+        RR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, HC::SMEM));
+        attr = true;
+      }
+      const int64_t items = static_cast<int64_t>(mtiles) * naux;
+      const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(items, sm_count())));
+      kern<<<grid, HT_THREADS, HC::SMEM, s>>>(a_hi, a_lo, b_hi, b_lo, p, mtiles, static_cast<int>(naux));
+      RR_LAUNCH_CHECK();
     }
     {
       uint64_t dims[2] = {static_cast<uint64_t>(kt), static_cast<uint64_t>(n)};
