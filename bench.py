@@ -151,6 +151,54 @@ def orbital_optimization_block():
     return out
 
 
+def x2c_batch_block(want_cpu: bool, count: int = 64, workers: int = 16):
+    """Batched X2C-HF geometry scan: `count` instances with uneven nl in [20, 120] (seeded), naux = 4 nl,
+    4 or 14 electrons (LiH- / CO-like) alternating, each converged to 1e-8 Ha; one handle per
+    instance, run one after another (workers = 1) and concurrently (rr_scf_run_x2c_batch)."""
+    from rerdmft_b200 import ri, scf, synth
+
+    rng = np.random.default_rng(SEED + 44)
+    sizes = rng.integers(20, 121, size=count)
+    probs, systems = [], []
+    for k, nl in enumerate(sizes):
+        sysd = synth.x2c_system(int(nl), 4 * int(nl), 4 if k % 2 == 0 else 14, seed=SEED + 100 + k)
+        src = ri.RiX2cEriSource(int(nl), sysd["B"], sysd["X"], sysd["S"])
+        src.store  # upload outside the timed region
+        systems.append(sysd)
+        probs.append(dict(eri=src, h_x2c=sysd["h"], x_large=sysd["X"], initial_density=sysd["P0"],
+                          n_electrons=sysd["n_electrons"]))
+    scf.runX2CHartreeFockScfBatch(probs[:4], workers=4)  # warm-up
+    t0 = time.perf_counter()
+    seq = scf.runX2CHartreeFockScfBatch(probs, workers=1)
+    t_seq = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    par = scf.runX2CHartreeFockScfBatch(probs, workers=workers)
+    t_par = time.perf_counter() - t0
+    out = dict(workload=f"{count} X2C-HF instances, nl in [20, 120] (uneven), naux = 4 nl, 4 / 14 electrons, FP64",
+               seconds_one_after_another=t_seq, seconds_concurrent=t_par, workers=workers,
+               instances_per_s=count / t_par, converged=int(sum(r["converged"] for r in par)),
+               iterations_total=int(sum(r["iterations"] for r in par)),
+               max_energy_difference_sequential_vs_concurrent=float(max(abs(a["energy"] - b["energy"])
+                                                                      for a, b in zip(seq, par))))
+    if want_cpu:
+        from oracle import ref
+
+        if ref.available():
+            ref.set_threads(os.cpu_count() or 1)
+            sample = list(range(0, count, 8))
+            t0 = time.perf_counter()
+            for k in sample:
+                ref.x2c_scf(systems[k])
+            dt = time.perf_counter() - t0
+            share = sum(int(sizes[k]) ** 3 for k in sample) / sum(int(x) ** 3 for x in sizes)
+            out["reference_cpu"] = dict(seconds_sample=dt, sample=f"instances {sample} (every 8th)",
+                                        cores=os.cpu_count() or 1,
+                                        seconds_all_estimated_by_nl3=dt / share)
+    for p in probs:
+        p["eri"].store.close()
+    return out
+
+
 def scf_times(torch, want_cpu: bool):
     """Time to an energy change below 1e-8 Ha on one GPU: FP64 loop vs mixed loop (split-BF16
     exchange until |dE| < 1e-5, then FP64), plus the reference's own SCF loop on the host cores."""
@@ -469,6 +517,7 @@ def main():
     scf_block = scf_times(torch, want_cpu=not args.no_cpu_baseline)
     rkb_block = rkb_fock_times(torch, fp64_peak, want_cpu=not args.no_cpu_baseline)
     orb_block = orbital_optimization_block()
+    x2c_block = x2c_batch_block(want_cpu=not args.no_cpu_baseline)
     line = dict(
         metric=METRIC, value=value, unit=UNIT, n_gpus=ws, steps=args.steps, warmup=args.warmup,
         ms_per_step=1e3 * t / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
@@ -498,6 +547,7 @@ def main():
         time_to_1e8_ha=scf_block,
         rkb_fock_4c=rkb_block,
         orbital_optimization=orb_block,
+        x2c_batch=x2c_block,
     )
     print(json.dumps(line))
     if pg:

@@ -246,6 +246,29 @@ int rr_mo_hx_fock(rr_mo_handle m, const double* h, const double* occupations, co
                   const double* two_rdm_x, const int64_t* pair_of, const double* two_rdm_l1, const double* two_rdm_l2,
                   double* F, const rr_opts* opts);
 
+/* One X2C-HF problem of a batch (its own 2-component handle and inputs, as for rr_scf_run_x2c);
+ * result and status are outputs (status: RR_OK or the error code of this instance). */
+typedef struct rr_x2c_instance {
+  rr_ri_handle h;
+  const double* h_x2c;
+  const double* X;
+  int64_t n_eff;
+  const double* S;
+  const double* P0;
+  int32_t n_electrons;
+  int32_t status;
+  double* P_out;
+  double* energy_history; /* optional */
+  rr_scf_result result;
+} rr_x2c_instance;
+
+/* A batch of independent X2C-HF SCF problems of uneven size (a geometry scan) run concurrently:
+ * `workers` host threads take the instances in order, each instance running rr_scf_run_x2c on its
+ * handle's own stream, so the small per-instance kernels of different instances overlap on the
+ * GPU.  Host pointers.  Returns RR_OK when every instance succeeded, else the first failing
+ * instance's code (all instances run; each reports its own status). */
+int rr_scf_run_x2c_batch(rr_x2c_instance* instances, int64_t count, const rr_scf_opts* scf, int32_t workers);
+
 /* ---------------- orbital-rotation optimisation (functional stage) ---------------- */
 
 /* AdamOptions, src/Utils/ADAM.h:41-60 (rr_adam_default_options fills the reference's defaults). */

@@ -67,7 +67,14 @@ class ScfResult(ctypes.Structure):
                 ("mixed_iterations", _i64), ("fp64_iterations", _i64), ("seconds", _d)]
 
 
+class X2cInstance(ctypes.Structure):
+    _fields_ = [("h", _vp), ("h_x2c", _vp), ("X", _vp), ("n_eff", _i64), ("S", _vp), ("P0", _vp),
+                ("n_electrons", _i32), ("status", _i32), ("P_out", _vp), ("energy_history", _vp),
+                ("result", ScfResult)]
+
+
 _SIGS = {
+    "rr_scf_run_x2c_batch": (ctypes.c_int, [ctypes.POINTER(X2cInstance), _i64, ctypes.POINTER(ScfOpts), _i32]),
     "rr_adam_default_options": (ctypes.c_int, [ctypes.POINTER(AdamOptions)]),
     "rr_orbopt_create": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(AdamOptions),
                                         ctypes.POINTER(_vp)]),

@@ -1,6 +1,9 @@
 // extern "C" boundary of librr_ri (declared in include/rr_ri.h).  Every entry point converts
 // rr::Error (and any other exception) into a status code plus rr_last_error().
+#include <atomic>
 #include <new>
+#include <thread>
+#include <vector>
 
 #include "mo_store.cuh"
 
@@ -268,6 +271,31 @@ int rr_scf_run_x2c(rr_ri_handle h, const double* h_x2c, const double* X, int64_t
     *result = rr_scf_result{};
     rr::scf_rel(s, 0, h_x2c, nullptr, 2 * s->n, X, n_eff, S, P0, n_electrons, scf, result, P_out, energy_history,
                 opts);
+  });
+}
+
+int rr_scf_run_x2c_batch(rr_x2c_instance* instances, int64_t count, const rr_scf_opts* scf, int32_t workers) {
+  return api([&] {
+    RR_REQUIRE(count >= 0 && (instances || count == 0) && scf, RR_ERR_ARG, "rr_scf_run_x2c_batch: null argument");
+    RR_REQUIRE(workers >= 1, RR_ERR_ARG, "rr_scf_run_x2c_batch: workers < 1");
+    std::atomic<int64_t> next{0};
+    auto work = [&] {
+      for (;;) {
+        const int64_t i = next.fetch_add(1);
+        if (i >= count) return;
+        rr_x2c_instance& in = instances[i];
+        in.status = rr_scf_run_x2c(in.h, in.h_x2c, in.X, in.n_eff, in.S, in.P0, in.n_electrons, scf, &in.result,
+                                   in.P_out, in.energy_history, nullptr);
+      }
+    };
+    const int nw = static_cast<int>(std::min<int64_t>(workers, std::max<int64_t>(count, 1)));
+    std::vector<std::thread> pool;
+    for (int w = 1; w < nw; ++w) pool.emplace_back(work);
+    work();
+    for (auto& t : pool) t.join();
+    for (int64_t i = 0; i < count; ++i)
+      if (instances[i].status != RR_OK)
+        throw rr::Error(instances[i].status, "rr_scf_run_x2c_batch: instance " + std::to_string(i) + " failed");
   });
 }
 

@@ -2,6 +2,7 @@
 // (MT*8) x (NT*8) built from mma.sync.m8n8k4.f64, optional complex (4M) accumulation, split-K
 // with a fixed-order reduction (bit-identical results run to run), and upper-triangle-only
 // scheduling for symmetric / Hermitian outputs.
+#include <atomic>
 #include "gemm_f64.cuh"
 
 namespace rr {
@@ -305,7 +306,7 @@ template <int MT, int NT, int WM, int WN, bool AK, bool BKM, bool CPLX, int V, b
 void launch_cfg_v(const Params& p, dim3 grid, cudaStream_t s) {
   using CF = Cfg<MT, NT, WM, WN, AK, BKM, CPLX>;
   auto kern = dgemm_kernel<MT, NT, WM, WN, AK, BKM, CPLX, V, EDOT>;
-  static bool attr = false;
+  static std::atomic<bool> attr{false};  // host threads may race here: the attribute is idempotent
   if (!attr) {
     RR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, CF::SMEM_BYTES));
     attr = true;

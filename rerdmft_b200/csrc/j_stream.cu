@@ -1,5 +1,6 @@
 // Coulomb streaming passes (see j_stream.cuh).  One producer warp issues 16 KB TMA bulk copies
 // into a 4-stage shared-memory ring; 8 consumer warps read them with 128-bit shared loads.
+#include <atomic>
 #include "j_stream.cuh"
 #include "tma_util.cuh"
 
@@ -257,7 +258,7 @@ int grid_size(int64_t items, int ctas_per_sm) {
 }
 
 void set_smem_attr() {
-  static bool done = false;
+  static std::atomic<bool> done{false};  // host threads may race here: the attribute is idempotent
   if (!done) {
     RR_CUDA(cudaFuncSetAttribute(j_pass1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
     RR_CUDA(cudaFuncSetAttribute(j_pass2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));

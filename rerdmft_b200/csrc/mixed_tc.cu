@@ -11,6 +11,7 @@
 //                   FP32, reduced in FP64 in a fixed order.
 // Roles: warp 0 lane 0 issues the TMA ring (SWIZZLE_128B tiles of 64 BF16 along K), warp 1 lane 0
 // issues the MMAs, all four warps drain TMEM in the epilogue.  Every wait is bounded.
+#include <atomic>
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
 
@@ -469,7 +470,7 @@ void launch_umma(const CUtensorMap& a_hi, const CUtensorMap& a_lo, const CUtenso
                  const UParams& p, dim3 grid, cudaStream_t s) {
   using CF = UCfg<BN, STAGES, MODE>;
   auto k = umma_split_kernel<BN, STAGES, MODE>;
-  static bool attr = false;
+  static std::atomic<bool> attr{false};  // host threads may race here: the attribute is idempotent
   if (!attr) {
     RR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, CF::SMEM));
     attr = true;
@@ -559,7 +560,7 @@ void mixed_exchange(MixedOperands& mo, const double* Ct, int64_t ldct, int64_t n
       const int mtiles = static_cast<int>((n + BM - 1) / BM);
       using HC = HCfg<HT_BN, 4>;
       auto kern = umma_ht_persistent_kernel<HT_BN, 4>;
-      static bool attr = false;
+      static std::atomic<bool> attr{false};  // host threads may race here: the attribute is idempotent
       if (!attr) {
         RR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, HC::SMEM));
         attr = true;

@@ -95,3 +95,32 @@ def runDiracHartreeFockScf(h_rkb, eri: RiDirectEriSource, x_full, initial_densit
     L.check(L.lib().rr_scf_run_dhf(eri.store.handle, _ptr(h), _ptr(v), n, _ptr(S), _ptr(X), _ptr(P0), n_electrons,
                                    ctypes.byref(so), ctypes.byref(res), _ptr(P), _ptr(hist), ctypes.byref(L.opts())))
     return _result(res, P, hist)
+
+
+def runX2CHartreeFockScfBatch(problems, workers: int = 16, diis_size: int = 5, max_iterations: int = 100,
+                              energy_tolerance: float = 1e-8, density_tolerance: float = 1e-6,
+                              kramers_restricted: bool = True) -> list:
+    """A batch of independent X2C-HF problems (a geometry scan of uneven sizes) run concurrently
+    (rr_scf_run_x2c_batch: `workers` host threads, one stream per problem's handle).  Each problem is
+    a dict with eri (RiX2cEriSource), h_x2c, x_large, initial_density, n_electrons and optionally
+    overlap.  Returns one result dict per problem, as runX2CHartreeFockScf."""
+    keep, insts = [], (L.X2cInstance * len(problems))()
+    outs = []
+    for i, pr in enumerate(problems):
+        eri = pr["eri"]
+        n = 2 * eri.nl
+        S = _host(eri.overlap if pr.get("overlap") is None else pr["overlap"], np.complex128)
+        h = _host(pr["h_x2c"], np.complex128)
+        X = _host(pr["x_large"], np.complex128)
+        P0 = _host(pr["initial_density"], np.complex128)
+        if h.shape != (n, n) or P0.shape != (n, n) or S.shape != (n, n) or X.shape[0] != n:
+            raise RrError(L.RR_ERR_ARG, "runX2CHartreeFockScfBatch: matrix dimensions do not match 2*nLarge")
+        P = np.empty((n, n), dtype=np.complex128)
+        hist = np.full(max_iterations, np.nan)
+        keep += [S, h, X, P0]
+        outs.append((P, hist))
+        insts[i] = L.X2cInstance(eri.store.handle, _ptr(h), _ptr(X), X.shape[1], _ptr(S), _ptr(P0),
+                                 int(pr["n_electrons"]), 0, _ptr(P), _ptr(hist), L.ScfResult())
+    so = _opts(diis_size, max_iterations, energy_tolerance, density_tolerance, "fp64", 0.0, kramers_restricted, 1.0)
+    L.check(L.lib().rr_scf_run_x2c_batch(insts, len(problems), ctypes.byref(so), workers))
+    return [_result(insts[i].result, P, hist) for i, (P, hist) in enumerate(outs)]

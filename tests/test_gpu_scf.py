@@ -106,3 +106,19 @@ def test_x2c_without_kramers_projection_and_with_mixing(ref_lib):
     # OR rule stops a slowly mixed iteration as soon as one step changes E by less than tolE
     rm = _run_x2c(s, diis_size=0, mixing=0.5, max_iterations=400, energy_tolerance=1e-13, density_tolerance=1e-10)
     assert rm["converged"] and abs(rm["energy"] - r["energy"]) <= 1e-7
+
+
+def test_x2c_batch_matches_single_runs(ref_lib):
+    systems = [synth.x2c_system(nl, 4 * nl, ne, seed=30 + k) for k, (nl, ne) in
+               enumerate([(8, 4), (14, 6), (20, 4), (11, 2), (17, 8), (9, 4)])]
+    probs = []
+    for s in systems:
+        src = ri.RiX2cEriSource(s["nl"], s["B"], s["X"], s["S"])
+        probs.append(dict(eri=src, h_x2c=s["h"], x_large=s["X"], initial_density=s["P0"], n_electrons=s["n_electrons"]))
+    batch = scf.runX2CHartreeFockScfBatch(probs, workers=3)
+    for s, b in zip(systems, batch):
+        single = _run_x2c(s)
+        assert b["converged"] and b["iterations"] == single["iterations"]
+        assert np.array_equal(b["history"], single["history"])
+    rr = ref_lib.x2c_scf(systems[2])
+    assert np.abs(batch[2]["history"] - rr["history"]).max() <= 1e-8
