@@ -61,7 +61,9 @@ typedef struct rr_opts {
   int32_t precision; /* RR_PREC_FP64 (default) or RR_PREC_MIXED */
   void* stream;      /* cudaStream_t for the call; NULL = the handle's own stream */
   int32_t sync;      /* device-pointer calls: 1 = block until done (host-pointer calls always block) */
-  int32_t reserved;
+  int32_t incremental; /* RR_PREC_MIXED relativistic builds: 1 = add the split-BF16 exchange of the change of
+                          the occupied spinors since the handle's previous mixed build (same rank), so the
+                          rounding error scales with the density change; 0 = full split-BF16 exchange */
 } rr_opts;
 
 /* Message of the last failing call on this thread ("" if none). */
@@ -99,7 +101,9 @@ int rr_ri_fock_nonrel(rr_ri_handle h, const double* h_core, const double* D, con
 /* X2C RI Fock matrix in the [alpha; beta] spin-orbital AO basis (2nl x 2nl, complex).
  * Replaces x2cFockMatrix(h_x2c, RiX2cEriSource, P), src/X2C_DHF/X2C_FockMatrixRi.cpp:79: J from
  * Re(P_aa + P_bb) on both diagonal blocks, K over the two spin flavours from the occupied spinors
- * recovered from X^dagger (S P S) X (eigenvalues > 0.5, sqrt(eigenvalue)-weighted).  X: 2nl x n_eff. */
+ * recovered from X^dagger (S P S) X (eigenvalues > 0.5, sqrt(eigenvalue)-weighted).  X: 2nl x n_eff.
+ * opts->precision = RR_PREC_MIXED: K from the split-BF16 tcgen05 exchange (J stays FP64), full or
+ * incremental (opts->incremental); the handle keeps the accumulated K between such calls. */
 int rr_ri_fock_x2c(rr_ri_handle h, const double* h_x2c, const double* P, const double* S, const double* X,
                    int64_t n_eff, double* F, const rr_opts* opts);
 
@@ -112,7 +116,8 @@ int rr_ri_two_electron_ukb(rr_ri_handle h, const double* P_ukb, const double* C_
 /* 4-component RKB Fock matrix F = h + v^dagger G(v P v^dagger, v C_occ) v (n_rkb x n_rkb, complex).
  * Replaces rkbFockMatrix(h_rkb, RiDirectEriSource, P), src/UKB/UkbFockMatrixRi.cpp:185: the occupied
  * RKB spinors are recovered from x_full^dagger (s_full P s_full) x_full (eigenvalues > 0.5).
- * v_total: n_ukb x n_rkb; s_full: n_rkb x n_rkb; x_full: n_rkb x n_eff. */
+ * v_total: n_ukb x n_rkb; s_full: n_rkb x n_rkb; x_full: n_rkb x n_eff.  RR_PREC_MIXED as for
+ * rr_ri_fock_x2c (the LL and SS exchange blocks on tcgen05). */
 int rr_ri_fock_rkb(rr_ri_handle h, const double* h_rkb, const double* v_total, int64_t n_rkb, const double* s_full,
                    const double* x_full, int64_t n_eff, const double* P, double* F, const rr_opts* opts);
 
@@ -159,6 +164,10 @@ typedef struct rr_scf_result {
   int64_t mixed_iterations; /* Fock builds with the split-BF16 exchange */
   int64_t fp64_iterations;  /* Fock builds in FP64 */
   double seconds;           /* wall time of the loop, inputs on the device to density out */
+  /* Device time per phase, summed over the iterations (only when rr_ri_set_profiling is on, else 0):
+   * Fock builds (the final FP64 build of a mixed loop not included), energy + DIIS, density step
+   * (orthogonal transform, SP2 projector(s), back-transform, density change). */
+  double build_ms, diis_ms, density_ms;
 } rr_scf_result;
 
 /* Restricted nonrelativistic SCF with the RI Fock build, DIIS on e = FPS - SPF and the aufbau
@@ -177,7 +186,11 @@ int rr_scf_run_nonrel(rr_ri_handle h, const double* h_core, const double* X, int
  * GPU, E = 1/2 Re Tr[P (h + F)], DIIS on e = FPS - SPF, P_new = X Pi X^dagger with Pi the SP2
  * projector onto the lowest n_electrons eigenvectors of X^dagger F X (one electron per spinor),
  * Kramers projection of every density ([alpha; beta] layout) when kramers_restricted and
- * n_electrons is even. */
+ * n_electrons is even.
+ * RR_PREC_MIXED: the first build uses the full split-BF16 exchange, later builds add the split-BF16
+ * exchange of the density change (incremental); mixed_switch > 0 re-seeds the accumulated exchange
+ * once with an FP64 build when |dE| < mixed_switch.  After convergence one FP64 build of the final
+ * density gives the reported energy (counted in iterations and fp64_iterations). */
 int rr_scf_run_x2c(rr_ri_handle h, const double* h_x2c, const double* X, int64_t n_eff, const double* S,
                    const double* P0, int32_t n_electrons, const rr_scf_opts* scf, rr_scf_result* result,
                    double* P_out, double* energy_history, const rr_opts* opts);
@@ -188,7 +201,8 @@ int rr_scf_run_x2c(rr_ri_handle h, const double* h_x2c, const double* X, int64_t
  * needs the full basis).  F = rkbFockMatrix(P) on the GPU; the density fills the n_electrons
  * positive-energy spinors above the n_rkb/2 negative-energy ones (RkbDensityMatrix.cpp:16-43):
  * P_new = X (Pi_{n_rkb/2 + n_e} - Pi_{n_rkb/2}) X^dagger from two SP2 projectors; Kramers
- * projection in the [L-alpha; L-beta; S-alpha; S-beta] layout. */
+ * projection in the [L-alpha; L-beta; S-alpha; S-beta] layout.  RR_PREC_MIXED as for
+ * rr_scf_run_x2c. */
 int rr_scf_run_dhf(rr_ri_handle h, const double* h_rkb, const double* v_total, int64_t n_rkb, const double* s_full,
                    const double* x_full, const double* P0, int32_t n_electrons, const rr_scf_opts* scf,
                    rr_scf_result* result, double* P_out, double* energy_history, const rr_opts* opts);

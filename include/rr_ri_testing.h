@@ -25,6 +25,11 @@ int rr_test_j_passes(const double* B, int64_t naux, int64_t n2, const double* D,
  * Ct: nocc x n, K: n x n; all FP64 device pointers). */
 int rr_test_mixed_exchange(const double* B, int64_t naux, int64_t n, const double* Ct, int64_t nocc, double* K);
 
+/* dK = K(Ct) - K(Ct_prev) through the incremental split-BF16 exchange:
+ * sum_P (W B^P)^T (U B^P) + (U B^P)^T (W B^P), W = (Ct + Ct_prev)/2, U = Ct - Ct_prev (device pointers). */
+int rr_test_mixed_exchange_delta(const double* B, int64_t naux, int64_t n, const double* Ct, const double* Ct_prev,
+                                 int64_t nocc, double* dK);
+
 /* Adam<T>::step (src/Utils/ADAM.cpp:33-51) on the device over `nsteps` host gradients (rows of
  * grads, n entries, interleaved complex when cplx); steps receives the nsteps x n updates. */
 int rr_test_adam_steps(int64_t n, int32_t cplx, int64_t nsteps, double lr, double b1, double b2, double eps,

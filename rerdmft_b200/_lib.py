@@ -30,7 +30,7 @@ class RrError(RuntimeError):
 
 
 class Opts(ctypes.Structure):
-    _fields_ = [("mem", _i32), ("precision", _i32), ("stream", _vp), ("sync", _i32), ("reserved", _i32)]
+    _fields_ = [("mem", _i32), ("precision", _i32), ("stream", _vp), ("sync", _i32), ("incremental", _i32)]
 
 
 class Timings(ctypes.Structure):
@@ -64,7 +64,8 @@ class AdamResult(ctypes.Structure):
 
 class ScfResult(ctypes.Structure):
     _fields_ = [("electronic_energy", _d), ("iterations", _i64), ("converged", _i64),
-                ("mixed_iterations", _i64), ("fp64_iterations", _i64), ("seconds", _d)]
+                ("mixed_iterations", _i64), ("fp64_iterations", _i64), ("seconds", _d),
+                ("build_ms", _d), ("diis_ms", _d), ("density_ms", _d)]
 
 
 class X2cInstance(ctypes.Structure):
@@ -134,6 +135,7 @@ _SIGS = {
     "rr_test_gemm_f64": (ctypes.c_int, [_i64, _i64, _i64, _vp, _i64, _i64, _i32, _vp, _i64, _i64, _i32, _vp, _i64,
                                         _i64, _d, _d, _i64, _i32, _i32, _i32, _i32, _i32]),
     "rr_test_mixed_exchange": (ctypes.c_int, [_vp, _i64, _i64, _vp, _i64, _vp]),
+    "rr_test_mixed_exchange_delta": (ctypes.c_int, [_vp, _i64, _i64, _vp, _vp, _i64, _vp]),
     "rr_test_j_passes": (ctypes.c_int, [_vp, _i64, _i64, _vp, _vp, _vp]),
 }
 
@@ -162,5 +164,6 @@ def check(rc: int) -> None:
         raise RrError(rc, lib().rr_last_error().decode())
 
 
-def opts(mem: int = RR_MEM_HOST, precision: int = RR_PREC_FP64, stream: int | None = None, sync: int = 1) -> Opts:
-    return Opts(mem, precision, stream, sync, 0)
+def opts(mem: int = RR_MEM_HOST, precision: int = RR_PREC_FP64, stream: int | None = None, sync: int = 1,
+         incremental: int = 0) -> Opts:
+    return Opts(mem, precision, stream, sync, incremental)

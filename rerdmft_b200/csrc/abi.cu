@@ -13,10 +13,10 @@ void fock_nonrel(rr_ri_store*, const double*, const double*, const double*, cons
                  const rr_opts*);
 void jk_occupied(rr_ri_store*, const double*, int64_t, double*, double*, const rr_opts*);
 void fock_x2c(rr_ri_store*, const double*, const double*, const double*, const double*, int64_t, double*,
-              const rr_opts*);
+              const rr_opts*, const RelBuild* = nullptr);
 void ukb_two_electron(rr_ri_store*, const double*, const double*, int64_t, const double*, double*, const rr_opts*);
 void fock_rkb(rr_ri_store*, const double*, const double*, int64_t, const double*, const double*, int64_t,
-              const double*, double*, const rr_opts*);
+              const double*, double*, const rr_opts*, const RelBuild* = nullptr);
 void scf_nonrel(rr_ri_store*, const double*, const double*, int64_t, const double*, const double*, int,
                 const rr_scf_opts*, rr_scf_result*, double*, double*, const rr_opts*);
 void scf_rel(rr_ri_store*, int, const double*, const double*, int64_t, const double*, int64_t, const double*,
@@ -218,8 +218,12 @@ int rr_ri_fock_x2c(rr_ri_handle h, const double* h_x2c, const double* P, const d
   return api([&] {
     auto* s = checked(h);
     RR_REQUIRE(h_x2c && P && S && F && (X || n_eff == 0), RR_ERR_ARG, "rr_ri_fock_x2c: null matrix");
-    RR_REQUIRE(!opts || opts->precision == RR_PREC_FP64, RR_ERR_UNSUPPORTED, "rr_ri_fock_x2c: precision");
-    rr::fock_x2c(s, h_x2c, P, S, X, n_eff, F, opts);
+    RR_REQUIRE(!opts || opts->precision == RR_PREC_FP64 || opts->precision == RR_PREC_MIXED, RR_ERR_UNSUPPORTED,
+               "rr_ri_fock_x2c: precision");
+    rr::RelBuild rb;
+    rb.mixed = true;
+    rb.incremental = opts && opts->incremental != 0;
+    rr::fock_x2c(s, h_x2c, P, S, X, n_eff, F, opts, opts && opts->precision == RR_PREC_MIXED ? &rb : nullptr);
   });
 }
 
@@ -238,8 +242,13 @@ int rr_ri_fock_rkb(rr_ri_handle h, const double* h_rkb, const double* v_total, i
   return api([&] {
     auto* s = checked(h);
     RR_REQUIRE(h_rkb && v_total && s_full && P && F && (x_full || n_eff == 0), RR_ERR_ARG, "rr_ri_fock_rkb: null matrix");
-    RR_REQUIRE(!opts || opts->precision == RR_PREC_FP64, RR_ERR_UNSUPPORTED, "rr_ri_fock_rkb: precision");
-    rr::fock_rkb(s, h_rkb, v_total, n_rkb, s_full, x_full, n_eff, P, F, opts);
+    RR_REQUIRE(!opts || opts->precision == RR_PREC_FP64 || opts->precision == RR_PREC_MIXED, RR_ERR_UNSUPPORTED,
+               "rr_ri_fock_rkb: precision");
+    rr::RelBuild rb;
+    rb.mixed = true;
+    rb.incremental = opts && opts->incremental != 0;
+    rr::fock_rkb(s, h_rkb, v_total, n_rkb, s_full, x_full, n_eff, P, F, opts,
+                 opts && opts->precision == RR_PREC_MIXED ? &rb : nullptr);
   });
 }
 
@@ -267,7 +276,8 @@ int rr_scf_run_x2c(rr_ri_handle h, const double* h_x2c, const double* X, int64_t
     RR_REQUIRE(h_x2c && X && S && P0 && scf && result && P_out, RR_ERR_ARG, "rr_scf_run_x2c: null argument");
     RR_REQUIRE(n_eff >= 1 && n_eff <= 2 * s->n, RR_ERR_ARG, "rr_scf_run_x2c: n_eff out of range");
     RR_REQUIRE(scf->max_iterations >= 1, RR_ERR_ARG, "rr_scf_run_x2c: max_iterations < 1");
-    RR_REQUIRE(scf->precision == RR_PREC_FP64, RR_ERR_UNSUPPORTED, "rr_scf_run_x2c: precision");
+    RR_REQUIRE(scf->precision == RR_PREC_FP64 || scf->precision == RR_PREC_MIXED, RR_ERR_UNSUPPORTED,
+               "rr_scf_run_x2c: precision");
     *result = rr_scf_result{};
     rr::scf_rel(s, 0, h_x2c, nullptr, 2 * s->n, X, n_eff, S, P0, n_electrons, scf, result, P_out, energy_history,
                 opts);
@@ -310,7 +320,8 @@ int rr_scf_run_dhf(rr_ri_handle h, const double* h_rkb, const double* v_total, i
     RR_REQUIRE(n_rkb >= 4 && n_rkb % 4 == 0, RR_ERR_ARG,
                "rkbDensityMatrix: RKB basis dimension must be even (4*nLarge)");
     RR_REQUIRE(scf->max_iterations >= 1, RR_ERR_ARG, "rr_scf_run_dhf: max_iterations < 1");
-    RR_REQUIRE(scf->precision == RR_PREC_FP64, RR_ERR_UNSUPPORTED, "rr_scf_run_dhf: precision");
+    RR_REQUIRE(scf->precision == RR_PREC_FP64 || scf->precision == RR_PREC_MIXED, RR_ERR_UNSUPPORTED,
+               "rr_scf_run_dhf: precision");
     *result = rr_scf_result{};
     rr::scf_rel(s, 1, h_rkb, v_total, n_rkb, x_full, n_rkb, s_full, P0, n_electrons, scf, result, P_out,
                 energy_history, opts);
@@ -544,14 +555,35 @@ extern "C" int rr_test_mixed_exchange(const double* B, int64_t naux, int64_t n, 
                                       double* K) {
   return api([&] {
     rr::MixedOperands mo;
+    rr::MixedScratch scr;
     rr::DevBuf<int> err(2);
     RR_CUDA(cudaMemset(err.p, 0, 2 * sizeof(int)));
     rr::mixed_prepare(mo, B, n * n, n, naux, nullptr);
-    rr::mixed_exchange(mo, Ct, n, nocc, K, err.p, nullptr);
+    rr::mixed_exchange(mo, scr, Ct, n, nocc, K, err.p, nullptr);
     RR_CUDA(cudaDeviceSynchronize());
     int e = 0;
     RR_CUDA(cudaMemcpy(&e, err.p, sizeof(int), cudaMemcpyDeviceToHost));
     RR_REQUIRE(e == 0, RR_ERR_TIMEOUT, "rr_test_mixed_exchange: device wait bound expired (0x" + std::to_string(e) + ")");
+  });
+}
+
+extern "C" int rr_test_mixed_exchange_delta(const double* B, int64_t naux, int64_t n, const double* Ct,
+                                            const double* Ct_prev, int64_t nocc, double* dK) {
+  return api([&] {
+    rr::MixedOperands mo;
+    rr::MixedScratch scr;
+    rr::DevBuf<int> err(2);
+    RR_CUDA(cudaMemset(err.p, 0, 2 * sizeof(int)));
+    rr::mixed_prepare(mo, B, n * n, n, naux, nullptr);
+    rr::ExFlavours fl;
+    fl.nf = 1;
+    fl.fs[0] = n;
+    rr::mixed_exchange_general(&mo, scr, fl, naux, Ct, Ct_prev, n, nocc, false, dK, n, false, err.p, nullptr);
+    RR_CUDA(cudaDeviceSynchronize());
+    int e = 0;
+    RR_CUDA(cudaMemcpy(&e, err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    RR_REQUIRE(e == 0, RR_ERR_TIMEOUT,
+               "rr_test_mixed_exchange_delta: device wait bound expired (0x" + std::to_string(e) + ")");
   });
 }
 

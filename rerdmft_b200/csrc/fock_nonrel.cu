@@ -289,9 +289,9 @@ void jk_occupied(rr_ri_store* h, const double* C, int64_t nocc, double* Jout, do
   transpose(Ctj, Cd, n, nocc, s);  // c_t = C^T, row-major nocc x n
   if (o && o->precision == RR_PREC_MIXED) {
     // Split-BF16 exchange on tcgen05; Coulomb in FP64 (two streaming passes over B).
-    mixed_prepare(h->mixed, h->B[0].p, h->pitch[0], n, h->naux, s);
+    mixed_prepare(h->mixed[0], h->B[0].p, h->pitch[0], n, h->naux, s);
     prof_mark(h, 2, s);
-    mixed_exchange(h->mixed, Ctj, n, nocc, K, h->status.p, s);
+    mixed_exchange(h->mixed[0], h->mscr, Ctj, n, nocc, K, h->status.p, s);
     coulomb_after_ht(h, Dp, Ctj, 0, J, nullptr, 0, s);
   } else {
     exchange_nonrel(h, Ctj, n, false, nocc, K, s, Dp, J);

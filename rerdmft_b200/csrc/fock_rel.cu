@@ -45,14 +45,14 @@ __global__ void split_rows_kernel(double* out, const double* Ct, int64_t r, int6
   }
 }
 
-// G (complex ntot x ntot) block (f,u): G(of+a, ou+b) = -(Kre + i Kim)(a,b), and for f != u also
-// G(ou+b, of+a) = -conj(K(a,b)).  diag_j (real fs x fs) is added on a diagonal block.
+// G (complex ntot x ntot) block (f,u): G(of+a, ou+b) = sgn (Kre + i Kim)(a,b), and for f != u also
+// G(ou+b, of+a) = sgn conj(K(a,b)).  diag_j (real fs x fs) is added on a diagonal block.
 __global__ void place_block_kernel(double* G, int64_t ntot, int64_t of, int64_t ou, int64_t fsf, int64_t fsu,
-                                   const double* Kre, const double* Kim, const double* diag_j, int both) {
+                                   const double* Kre, const double* Kim, const double* diag_j, int both, double sgn) {
   for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < fsf * fsu;
        idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int64_t a = idx / fsu, b = idx % fsu;
-    const double re = -Kre[idx], im = -Kim[idx];
+    const double re = sgn * Kre[idx], im = sgn * Kim[idx];
     double* g = G + ((of + a) * ntot + ou + b) * 2;
     g[0] = re + (diag_j ? diag_j[idx] : 0.0);
     g[1] = im;
@@ -61,6 +61,22 @@ __global__ void place_block_kernel(double* G, int64_t ntot, int64_t of, int64_t 
       gt[0] = re;
       gt[1] = -im;
     }
+  }
+}
+
+// G = -K (count doubles).
+__global__ void neg_copy_kernel(double* G, const double* K, int64_t count) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < count;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    G[i] = -K[i];
+}
+
+// Real part of the diagonal block (off, off) of G (complex ntot x ntot) += J (real fs x fs).
+__global__ void add_j_block_kernel(double* G, int64_t ntot, int64_t off, int64_t fs, const double* J) {
+  for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < fs * fs;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t a = idx / fs, b = idx % fs;
+    G[((off + a) * ntot + off + b) * 2] += J[idx];
   }
 }
 
@@ -94,9 +110,10 @@ void coulomb_async_multi(rr_ri_store* h, int ntens, const double* const* Dp, dou
 
 // Two-electron matrix G (complex ntot x ntot) = J - K for the given flavours from Ct (r x ntot,
 // complex), the reference's c_t of all flavours side by side.  Pdens: pitched real spin-summed
-// densities per tensor (J input).  Writes G.
+// densities per tensor (J input).  Writes G.  With rb the exchange goes through the handle's
+// accumulator (RelBuild).
 void two_electron_rel(rr_ri_store* h, const Flavours& fl, int64_t ntot, const double* Ct, int64_t r,
-                      const double* const* Dp, double* G, cudaStream_t s) {
+                      const double* const* Dp, double* G, cudaStream_t s, const RelBuild* rb) {
   const int64_t naux = h->naux;
   const int ntens = h->ntens;
   std::array<int64_t, 2> nt = {h->n, h->ns};
@@ -111,12 +128,32 @@ void two_electron_rel(rr_ri_store* h, const Flavours& fl, int64_t ntot, const do
   ar.request(&Kim, fsmax * fsmax);
   ar.commit();
   coulomb_async_multi(h, ntens, Dp, J, s);
-  RR_CUDA(cudaMemsetAsync(G, 0, sizeof(double) * 2 * ntot * ntot, s));
+  if (rb) {
+    h->rel_k.ensure(static_cast<size_t>(2 * ntot * ntot));
+    if (rb->mixed) {
+      const bool incr = rb->incremental && h->rel_r == r && h->rel_ntot == ntot && r > 0;
+      ExFlavours ef;
+      ef.nf = fl.nf;
+      for (int f = 0; f < fl.nf; ++f) {
+        ef.off[f] = fl.off[f];
+        ef.fs[f] = fl.fs[f];
+        ef.tens[f] = fl.tens[f];
+      }
+      for (int t = 0; t < ntens; ++t) mixed_prepare(h->mixed[t], h->B[t].p, h->pitch[t], nt[t], naux, s);
+      prof_mark(h, 2, s);
+      mixed_exchange_general(h->mixed, h->mscr, ef, naux, Ct, incr ? h->rel_ct.p : nullptr, ntot, r, true, h->rel_k.p,
+                             ntot, incr, h->status.p, s);
+      prof_mark(h, 3, s);
+    }
+  }
+  const bool fp64_k = !rb || !rb->mixed;
+  double* Gk = rb ? h->rel_k.p : G;  // where the FP64 blocks land
+  if (fp64_k) RR_CUDA(cudaMemsetAsync(Gk, 0, sizeof(double) * 2 * ntot * ntot, s));
   // T planes: flavour f occupies [Re (naux*r*fs) | Im (naux*r*fs)]
   std::array<double*, 4> T{};
   int64_t tsize = 0;
   for (int f = 0; f < fl.nf; ++f) tsize += 2 * naux * r * fl.fs[f];
-  if (r > 0 && naux > 0) {
+  if (fp64_k && r > 0 && naux > 0) {
     h->T.ensure(static_cast<size_t>(tsize));
     int64_t o = 0;
     for (int f = 0; f < fl.nf; ++f) { T[f] = h->T.p + o; o += 2 * naux * r * fl.fs[f]; }
@@ -134,8 +171,8 @@ void two_electron_rel(rr_ri_store* h, const Flavours& fl, int64_t ntot, const do
       gemm(ht, s);
     }
   }
-  prof_mark(h, 2, s);
-  for (int f = 0; f < fl.nf; ++f)
+  if (fp64_k) prof_mark(h, 2, s);
+  for (int f = 0; f < fl.nf && fp64_k; ++f)
     for (int u = f; u < fl.nf; ++u) {
       const int64_t ff = fl.fs[f], fu = fl.fs[u];
       if (r > 0 && naux > 0) {
@@ -158,16 +195,31 @@ void two_electron_rel(rr_ri_store* h, const Flavours& fl, int64_t ntot, const do
         RR_CUDA(cudaMemsetAsync(Kre, 0, sizeof(double) * ff * fu, s));
         RR_CUDA(cudaMemsetAsync(Kim, 0, sizeof(double) * ff * fu, s));
       }
-      if (f == u) RR_CUDA(cudaStreamWaitEvent(s, h->ctx.join, 0));  // J needed on the diagonal blocks
-      place_block_kernel<<<blocks_for(ff * fu), 256, 0, s>>>(G, ntot, fl.off[f], fl.off[u], ff, fu, Kre, Kim,
-                                                              f == u ? J[fl.tens[f]] : nullptr, f != u);
+      const bool add_j = f == u && !rb;
+      if (add_j) RR_CUDA(cudaStreamWaitEvent(s, h->ctx.join, 0));  // J needed on the diagonal blocks
+      place_block_kernel<<<blocks_for(ff * fu), 256, 0, s>>>(Gk, ntot, fl.off[f], fl.off[u], ff, fu, Kre, Kim,
+                                                              add_j ? J[fl.tens[f]] : nullptr, f != u, rb ? 1.0 : -1.0);
       RR_LAUNCH_CHECK();
     }
-  prof_mark(h, 3, s);
+  if (fp64_k) prof_mark(h, 3, s);
+  if (rb) {
+    // G = J - K from the accumulator; remember c_t for the next incremental build
+    neg_copy_kernel<<<blocks_for(2 * ntot * ntot), 256, 0, s>>>(G, h->rel_k.p, 2 * ntot * ntot);
+    RR_LAUNCH_CHECK();
+    RR_CUDA(cudaStreamWaitEvent(s, h->ctx.join, 0));
+    for (int f = 0; f < fl.nf; ++f) {
+      add_j_block_kernel<<<blocks_for(fl.fs[f] * fl.fs[f]), 256, 0, s>>>(G, ntot, fl.off[f], fl.fs[f], J[fl.tens[f]]);
+      RR_LAUNCH_CHECK();
+    }
+    h->rel_ct.ensure(static_cast<size_t>(std::max<int64_t>(2 * r * ntot, 1)));
+    if (r > 0) RR_CUDA(cudaMemcpyAsync(h->rel_ct.p, Ct, sizeof(double) * 2 * r * ntot, cudaMemcpyDeviceToDevice, s));
+    h->rel_r = r;
+    h->rel_ntot = ntot;
+  }
 }
 
 void fock_x2c(rr_ri_store* h, const double* hc, const double* P, const double* S, const double* X, int64_t n_eff,
-              double* F, const rr_opts* o) {
+              double* F, const rr_opts* o, const RelBuild* rb) {
   RR_REQUIRE(h->ntens == 1, RR_ERR_STATE, "rr_ri_fock_x2c: handle holds a 4-component store");
   const int64_t nl = h->n, n = 2 * nl, nn2 = n * n * 2;
   RR_REQUIRE(n_eff >= 0 && n_eff <= n, RR_ERR_ARG, "rr_ri_fock_x2c: n_eff out of range");
@@ -211,7 +263,7 @@ void fock_x2c(rr_ri_store* h, const double* hc, const double* P, const double* S
   fl.fs = {nl, nl, 0, 0};
   fl.tens = {0, 0, 0, 0};
   const double* dps[1] = {Dp};
-  two_electron_rel(h, fl, n, Ct, r, dps, G, s);
+  two_electron_rel(h, fl, n, Ct, r, dps, G, s, rb);
   add_kernel<<<blocks_for(nn2), 256, 0, s>>>(Fd, hd, G, nn2);
   RR_LAUNCH_CHECK();
   if (host) copy_out(F, Fd, nn2, true, s);
@@ -266,7 +318,7 @@ void ukb_two_electron(rr_ri_store* h, const double* P, const double* C, int64_t 
   fl.fs = {nl, nl, ns, ns};
   fl.tens = {0, 0, 1, 1};
   const double* dps[2] = {DL, DS};
-  two_electron_rel(h, fl, nu, Ct, nocc, dps, G, s);
+  two_electron_rel(h, fl, nu, Ct, nocc, dps, G, s, nullptr);
   if (host) copy_out(Gout, G, nn2, true, s);
   prof_mark(h, 4, s);
   if (host || (o && o->sync)) check_status(h, s);
@@ -274,7 +326,7 @@ void ukb_two_electron(rr_ri_store* h, const double* P, const double* C, int64_t 
 
 // rkbFockMatrix: recovery in the RKB basis with x_full / s_full, embedding with v_total.
 void fock_rkb(rr_ri_store* h, const double* hc, const double* v, int64_t n_rkb, const double* s_full,
-              const double* x_full, int64_t n_eff, const double* P, double* F, const rr_opts* o) {
+              const double* x_full, int64_t n_eff, const double* P, double* F, const rr_opts* o, const RelBuild* rb) {
   RR_REQUIRE(h->ntens == 2, RR_ERR_STATE, "rr_ri_fock_rkb: needs a 4-component store (rr_ri_create_4c)");
   const int64_t nl = h->n, ns = h->ns, nu = 2 * nl + 2 * ns;
   RR_REQUIRE(n_rkb >= 1 && n_eff >= 0 && n_eff <= n_rkb, RR_ERR_ARG, "rr_ri_fock_rkb: bad n_rkb / n_eff");
@@ -344,7 +396,7 @@ void fock_rkb(rr_ri_store* h, const double* hc, const double* v, int64_t n_rkb, 
   fl.fs = {nl, nl, ns, ns};
   fl.tens = {0, 0, 1, 1};
   const double* dps[2] = {DL, DS};
-  two_electron_rel(h, fl, nu, Ct_ukb, r, dps, G, s);
+  two_electron_rel(h, fl, nu, Ct_ukb, r, dps, G, s, rb);
   // F = h + v^dagger G v
   GemmDesc b;
   b.cplx = true;

@@ -3,6 +3,8 @@
 // with a fixed-order reduction (bit-identical results run to run), and upper-triangle-only
 // scheduling for symmetric / Hermitian outputs.
 #include <atomic>
+#include <cstdlib>
+
 #include "gemm_f64.cuh"
 
 namespace rr {
@@ -471,6 +473,21 @@ void gemm(const GemmDesc& d, cudaStream_t stream, double* work, int64_t work_cap
     if (d.cplx) mirror_kernel<2><<<blocks, 256, 0, stream>>>(d.C, d.M, d.ldc, d.strideC, d.batch, d.mirror);
     else mirror_kernel<1><<<blocks, 256, 0, stream>>>(d.C, d.M, d.ldc, d.strideC, d.batch, d.mirror);
     RR_LAUNCH_CHECK();
+  }
+  // RR_DEBUG_SYNC=1: finish every product before returning and name the one that failed.
+  static const bool debug_sync = std::getenv("RR_DEBUG_SYNC") != nullptr;
+  if (debug_sync) {
+    const cudaError_t e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess)
+      throw Error(RR_ERR_CUDA, "gemm M=" + std::to_string(d.M) + " N=" + std::to_string(d.N) + " K=" +
+                                   std::to_string(d.K) + " batch=" + std::to_string(d.batch) + " cplx=" +
+                                   std::to_string(d.cplx) + " mirror=" + std::to_string(d.mirror) + " opA=" +
+                                   std::to_string(static_cast<int>(d.opA)) + " opB=" +
+                                   std::to_string(static_cast<int>(d.opB)) + " lda=" + std::to_string(d.lda) +
+                                   " ldb=" + std::to_string(d.ldb) + " ldc=" + std::to_string(d.ldc) + " splits=" +
+                                   std::to_string(splits) + " kchunk=" + std::to_string(kc) + " tile=" +
+                                   std::to_string(sh.bm) + "x" + std::to_string(sh.bn) + " work_cap=" +
+                                   std::to_string(work_cap) + ": " + cudaGetErrorString(e));
   }
 }
 

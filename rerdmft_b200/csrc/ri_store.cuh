@@ -22,8 +22,13 @@ struct rr_ri_store {
   rr::DevBuf<double> solver_a;  // eigen-problem matrix / eigenvectors
   rr::DevBuf<double> solver_w;  // eigenvalues
   std::vector<double> host_w;
-  // Split-BF16 copy of B for RR_PREC_MIXED (built on first use).
-  rr::MixedOperands mixed;
+  // Split-BF16 copies of B[t] for RR_PREC_MIXED (built on first use) and their call scratch.
+  rr::MixedOperands mixed[2];
+  rr::MixedScratch mscr;
+  // Incremental relativistic builds: the exchange accumulated so far (interleaved complex
+  // ntot x ntot) and the c_t it belongs to (r x ntot).
+  rr::DevBuf<double> rel_k, rel_ct;
+  int64_t rel_r = -1, rel_ntot = 0;
   // Profiling events: 0 start, 1 recovery done, 2 half-transform done, 3 exchange done, 4 end
   // (main stream); 5 J start, 6 J end (side stream).
   bool profiling = false;
@@ -53,6 +58,17 @@ struct Arena {
     }
     pending.clear();
   }
+};
+
+// How a relativistic Fock build forms its exchange.  nullptr: FP64, straight into G.  Otherwise the
+// exchange goes through the handle's accumulator (rel_k), G = J - rel_k:
+//   mixed:           split-BF16 exchange on tcgen05; with `incremental` (and a previous build of the
+//                    same rank) only the exchange of c_t - c_t(previous) is added to rel_k, so the
+//                    rounding error scales with the density change;
+//   otherwise:       FP64 exchange that (re)seeds rel_k.
+struct RelBuild {
+  bool mixed = false;
+  bool incremental = false;
 };
 
 cudaStream_t call_stream(rr_ri_store* h, const rr_opts* o);

@@ -46,10 +46,13 @@ void set_last_error(const std::string& msg);
 // Kernel launch check (configuration errors surface here; execution errors at the next sync);
 // also counts the launch for rr_kernel_launches().
 void count_launch();
-#define RR_LAUNCH_CHECK()             \
-  do {                                \
-    RR_CUDA(cudaGetLastError());      \
-    ::rr::count_launch();             \
+#define RR_LAUNCH_CHECK()                                                                           \
+  do {                                                                                              \
+    cudaError_t _le = cudaGetLastError();                                                           \
+    if (_le != cudaSuccess)                                                                         \
+      throw ::rr::Error(RR_ERR_CUDA, std::string("kernel launch at " __FILE__ ":") +               \
+                                         std::to_string(__LINE__) + ": " + cudaGetErrorString(_le)); \
+    ::rr::count_launch();                                                                           \
   } while (0)
 
 // Owning device allocation (cudaMalloc/cudaFree), move-only.

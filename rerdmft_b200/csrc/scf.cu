@@ -34,9 +34,10 @@ void fock_nonrel(rr_ri_store* h, const double* hc, const double* D, const double
 void projector_ct(rr_ri_store* h, const double* A, const double* Pe, const double* X, int64_t n, int64_t n_eff,
                   int64_t r, bool cplx, double* Ct, cudaStream_t s);
 void fock_x2c(rr_ri_store* h, const double* hc, const double* P, const double* S, const double* X, int64_t n_eff,
-              double* F, const rr_opts* o);
+              double* F, const rr_opts* o, const RelBuild* rb = nullptr);
 void fock_rkb(rr_ri_store* h, const double* hc, const double* v, int64_t n_rkb, const double* s_full,
-              const double* x_full, int64_t n_eff, const double* P, double* F, const rr_opts* o);
+              const double* x_full, int64_t n_eff, const double* P, double* F, const rr_opts* o,
+              const RelBuild* rb = nullptr);
 
 namespace {
 
@@ -331,6 +332,39 @@ struct DeviceDiis {
   }
 };
 
+// Per-phase device times of an SCF loop (only with profiling on): 0 Fock build, 1 energy + DIIS,
+// 2 density step (orthogonal transform, SP2 projector, back-transform, density change).
+struct PhaseTimer {
+  bool on = false;
+  cudaEvent_t ev[4] = {};
+  double ms[3] = {0.0, 0.0, 0.0};
+  explicit PhaseTimer(bool enable) : on(enable) {
+    if (on)
+      for (auto& e : ev) RR_CUDA(cudaEventCreate(&e));
+  }
+  ~PhaseTimer() {
+    if (on)
+      for (auto& e : ev) cudaEventDestroy(e);
+  }
+  void mark(int i, cudaStream_t s) {
+    if (on) RR_CUDA(cudaEventRecord(ev[i], s));
+  }
+  // after the stream has passed mark 3
+  void accumulate() {
+    if (!on) return;
+    for (int i = 0; i < 3; ++i) {
+      float t = 0.f;
+      RR_CUDA(cudaEventElapsedTime(&t, ev[i], ev[i + 1]));
+      ms[i] += t;
+    }
+  }
+  void store(rr_scf_result* r) const {
+    r->build_ms = ms[0];
+    r->diis_ms = ms[1];
+    r->density_ms = ms[2];
+  }
+};
+
 }  // namespace
 
 // SP2 purification: projector (n x n, into Pi) onto the lowest `nocc` eigenvectors of the symmetric
@@ -356,6 +390,7 @@ void sp2_projector(rr_ri_store* h, const double* F, int64_t n, int64_t nocc, dou
   g.cplx = cplx;
   g.M = n; g.N = n; g.K = n;
   g.A = Pi; g.lda = n; g.B = Pi; g.ldb = n; g.C = T; g.ldc = n;
+  g.mirror = 1;  // X is Hermitian, so is X^2: upper tiles, the rest mirrored
   const double N = static_cast<double>(nocc);
   for (int it = 0; it < 120; ++it) {
     gemm(g, s, h->work.p, static_cast<int64_t>(h->work.n));
@@ -427,7 +462,9 @@ void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff
   double prev = 0.0;
   int64_t it = 0, n_mixed = 0, n_fp64 = 0;
   bool converged = false;
+  PhaseTimer pt(h->profiling);
   for (it = 1; it <= so->max_iterations; ++it) {
+    pt.mark(0, s);
     // ---- Fock matrix of the current density ----
     if (it == 1) {
       rr_opts od{};
@@ -437,8 +474,8 @@ void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff
       fock_nonrel(h, hd, P, Sd, Xd, n_eff, F, &od);
       ++n_fp64;
     } else if (mixed) {
-      mixed_prepare(h->mixed, h->B[0].p, h->pitch[0], n, h->naux, s);
-      mixed_exchange(h->mixed, Ct, n, nocc, K, h->status.p, s);
+      mixed_prepare(h->mixed[0], h->B[0].p, h->pitch[0], n, h->naux, s);
+      mixed_exchange(h->mixed[0], h->mscr, Ct, n, nocc, K, h->status.p, s);
       coulomb_after_ht(h, P, Ct, 0, J, nullptr, 0, s);
       coulomb_join(h, s);
       fock_combine(F, hd, J, K, n2, s);
@@ -449,6 +486,7 @@ void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff
       fock_combine(F, hd, J, K, n2, s);
       ++n_fp64;
     }
+    pt.mark(1, s);
     // ---- energy with the un-extrapolated F ----
     energy_partial_kernel<1><<<RED_CTAS, 256, 0, s>>>(P, hd, F, n, red);
     RR_LAUNCH_CHECK();
@@ -468,6 +506,7 @@ void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff
     } else {
       copy_out(Fs, F, n2, false, s);
     }
+    pt.mark(2, s);
     // ---- F_ortho = X^T F_scf X, aufbau projector, new orbitals and density ----
     GemmDesc a;
     a.M = n; a.N = n_eff; a.K = n; a.A = Fs; a.lda = n; a.B = Xd; a.ldb = n_eff; a.C = tmp; a.ldc = n_eff;
@@ -485,9 +524,11 @@ void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff
     RR_LAUNCH_CHECK();
     reduce_partials_kernel<2><<<1, 256, 0, s>>>(red, RED_CTAS, 1.0, scal + 1);
     RR_LAUNCH_CHECK();
+    pt.mark(3, s);
     double hv[2];
     RR_CUDA(cudaMemcpyAsync(hv, scal, sizeof(hv), cudaMemcpyDeviceToHost, s));
     RR_CUDA(cudaStreamSynchronize(s));
+    pt.accumulate();
     const double energy = hv[0], dP = hv[1], dE = std::fabs(energy - prev);
     if (hist) hist[it - 1] = energy;
     res->electronic_energy = energy;
@@ -513,6 +554,7 @@ void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff
   res->mixed_iterations = n_mixed;
   res->fp64_iterations = n_fp64;
   res->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+  pt.store(res);
 }
 
 // X2C-HF (kind 0) and 4c-DHF (kind 1) SCF loops on the device (X2C_HF.cpp:43-138,
@@ -574,8 +616,10 @@ void scf_rel(rr_ri_store* h, int kind, const double* hc, const double* v_total, 
   RR_REQUIRE(so->diis_size <= DIIS_MAX, RR_ERR_ARG, "SCF: diis_size too large");
   diis.init(use_diis ? so->diis_size : 0, c2);
   h->work.ensure(static_cast<size_t>(std::max<int64_t>(static_cast<int64_t>(h->work.n), 8 * c2)));
-  double* wk = h->work.p;
-  const int64_t wcap = static_cast<int64_t>(h->work.n);
+  // The Fock build may grow h->work (split-K partials of the exchange), so every product below
+  // takes the buffer as it is at its own call.
+  auto wk = [h] { return h->work.p; };
+  auto wcap = [h] { return static_cast<int64_t>(h->work.n); };
   GemmDesc g;  // n x n complex products
   g.cplx = true;
   g.M = n; g.N = n; g.K = n; g.lda = n; g.ldb = n; g.ldc = n;
@@ -583,37 +627,64 @@ void scf_rel(rr_ri_store* h, int kind, const double* hc, const double* v_total, 
   od.mem = RR_MEM_DEVICE;
   od.stream = s;
   double prev = 0.0;
-  int64_t it = 0;
+  int64_t it = 0, n_mixed = 0, n_fp64 = 0;
   bool converged = false;
-  for (it = 1; it <= so->max_iterations; ++it) {
-    if (dhf) fock_rkb(h, hd, vd, n, Sd, Xd, n_eff, P, F, &od);
-    else fock_x2c(h, hd, P, Sd, Xd, n_eff, F, &od);
+  // Mixed precision: the first build is a full split-BF16 one, every later build adds the split-BF16
+  // exchange of the change of c_t (its error shrinks with the density change), optionally re-seeded
+  // once by an FP64 build when |dE| < mixed_switch; once converged, the last iteration is an FP64
+  // build of the final density whose energy is reported.
+  bool mixed = so->precision == RR_PREC_MIXED, reseed = false, reseeded = false;
+  h->rel_r = -1;
+  auto build = [&](const RelBuild* rb) {
+    if (dhf) fock_rkb(h, hd, vd, n, Sd, Xd, n_eff, P, F, &od, rb);
+    else fock_x2c(h, hd, P, Sd, Xd, n_eff, F, &od, rb);
+  };
+  auto energy_of_f = [&] {
     energy_partial_kernel<2><<<RED_CTAS, 256, 0, s>>>(P, hd, F, n, red);
     RR_LAUNCH_CHECK();
     reduce_partials_kernel<0><<<1, 256, 0, s>>>(red, RED_CTAS, 0.5, scal);
     RR_LAUNCH_CHECK();
+  };
+  PhaseTimer pt(h->profiling);
+  for (it = 1; it <= so->max_iterations; ++it) {
+    pt.mark(0, s);
+    if (mixed) {
+      RelBuild rb;
+      rb.mixed = !reseed;
+      rb.incremental = it > 1;
+      build(&rb);
+      if (reseed) ++n_fp64;
+      else ++n_mixed;
+      reseed = false;
+    } else {
+      build(nullptr);
+      ++n_fp64;
+    }
+    pt.mark(1, s);
+    energy_of_f();
     if (use_diis) {
       g.A = P; g.B = Sd; g.C = PS; g.alpha = 1.0; g.beta = 0.0;
-      gemm(g, s, wk, wcap);
+      gemm(g, s, wk(), wcap());
       g.A = Sd; g.B = P; g.C = SP;
-      gemm(g, s, wk, wcap);
+      gemm(g, s, wk(), wcap());
       g.A = F; g.B = PS; g.C = e;
-      gemm(g, s, wk, wcap);
+      gemm(g, s, wk(), wcap());
       g.A = SP; g.B = F; g.C = e; g.alpha = -1.0; g.beta = 1.0;
-      gemm(g, s, wk, wcap);
+      gemm(g, s, wk(), wcap());
       g.alpha = 1.0; g.beta = 0.0;
       diis.extrapolate(e, F, Fs, s);
     } else {
       copy_out(Fs, F, c2, false, s);
     }
+    pt.mark(2, s);
     // F_ortho = X^dagger F_scf X
     GemmDesc a;
     a.cplx = true;
     a.M = n; a.N = n_eff; a.K = n; a.A = Fs; a.lda = n; a.B = Xd; a.ldb = n_eff; a.C = tmp; a.ldc = n_eff;
-    gemm(a, s, wk, wcap);
+    gemm(a, s, wk(), wcap());
     a.M = n_eff; a.N = n_eff; a.K = n; a.A = Xd; a.lda = n_eff; a.opA = Op::T; a.conjA = true; a.B = tmp;
     a.ldb = n_eff; a.C = Fo; a.ldc = n_eff;
-    gemm(a, s, wk, wcap);
+    gemm(a, s, wk(), wcap());
     // window projector in the orthonormal basis
     sp2_projector(h, Fo, n_eff, nlo + n_electrons, Pi, T2, scal + 8, s, true);
     if (nlo > 0) {
@@ -624,10 +695,10 @@ void scf_rel(rr_ri_store* h, int kind, const double* hc, const double* v_total, 
     GemmDesc b;
     b.cplx = true;
     b.M = n; b.N = n_eff; b.K = n_eff; b.A = Xd; b.lda = n_eff; b.B = Pi; b.ldb = n_eff; b.C = tmp; b.ldc = n_eff;
-    gemm(b, s, wk, wcap);
+    gemm(b, s, wk(), wcap());
     b.M = n; b.N = n; b.K = n_eff; b.A = tmp; b.lda = n_eff; b.B = Xd; b.ldb = n_eff; b.opB = Op::T; b.conjB = true;
     b.C = restrict_active ? e : Pn; b.ldc = n;
-    gemm(b, s, wk, wcap);
+    gemm(b, s, wk(), wcap());
     if (restrict_active) {
       kramers_even_kernel<<<blocks_for(n2), 256, 0, s>>>(Pn, e, n, nb);
       RR_LAUNCH_CHECK();
@@ -636,18 +707,35 @@ void scf_rel(rr_ri_store* h, int kind, const double* hc, const double* v_total, 
     RR_LAUNCH_CHECK();
     reduce_partials_kernel<2><<<1, 256, 0, s>>>(red, RED_CTAS, 1.0, scal + 1);
     RR_LAUNCH_CHECK();
+    pt.mark(3, s);
     double hv[2];
     RR_CUDA(cudaMemcpyAsync(hv, scal, sizeof(hv), cudaMemcpyDeviceToHost, s));
     RR_CUDA(cudaStreamSynchronize(s));
+    pt.accumulate();
     const double energy = hv[0], dP = hv[1], dE = std::fabs(energy - prev);
     if (hist) hist[it - 1] = energy;
     res->electronic_energy = energy;
     const bool conv = it > 1 && (dP < so->density_tolerance || dE < so->energy_tolerance);
     prev = energy;
     if (conv) {
+      if (mixed) {
+        // last iteration in FP64: the FP64 Fock matrix of the converged density and its energy
+        build(nullptr);
+        ++n_fp64;
+        energy_of_f();
+        double ev = 0.0;
+        RR_CUDA(cudaMemcpyAsync(&ev, scal, sizeof(double), cudaMemcpyDeviceToHost, s));
+        RR_CUDA(cudaStreamSynchronize(s));
+        res->electronic_energy = ev;
+        if (it < so->max_iterations) {
+          ++it;
+          if (hist) hist[it - 1] = ev;
+        }
+      }
       converged = true;
       break;
     }
+    if (mixed && !reseeded && so->mixed_switch > 0.0 && it > 1 && dE < so->mixed_switch) reseed = reseeded = true;
     if (!use_diis && so->mixing > 0.0 && so->mixing != 1.0) axpby(Pn, P, 1.0 - so->mixing, so->mixing, c2, s);
     std::swap(P, Pn);
   }
@@ -657,9 +745,10 @@ void scf_rel(rr_ri_store* h, int kind, const double* hc, const double* v_total, 
   RR_CUDA(cudaStreamSynchronize(s));
   res->iterations = it;
   res->converged = converged ? 1 : 0;
-  res->mixed_iterations = 0;
-  res->fp64_iterations = it;
+  res->mixed_iterations = n_mixed;
+  res->fp64_iterations = n_fp64;
   res->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+  pt.store(res);
 }
 
 }  // namespace rr

@@ -175,8 +175,16 @@ class RiX2cEriSource:
         return self._store
 
 
-def x2cFockMatrix(h_x2c, eri: RiX2cEriSource, density_matrix, stream: int | None = None):
-    """src/X2C_DHF/X2C_FockMatrixRi.cpp:79 via rr_ri_fock_x2c (complex 2nl x 2nl)."""
+def _prec_opts(dev, stream, precision, incremental):
+    prec = {"fp64": L.RR_PREC_FP64, "mixed": L.RR_PREC_MIXED}[precision]
+    return L.opts(L.RR_MEM_DEVICE if dev else L.RR_MEM_HOST, prec, stream=stream, incremental=1 if incremental else 0)
+
+
+def x2cFockMatrix(h_x2c, eri: RiX2cEriSource, density_matrix, stream: int | None = None, precision: str = "fp64",
+                  incremental: bool = False):
+    """src/X2C_DHF/X2C_FockMatrixRi.cpp:79 via rr_ri_fock_x2c (complex 2nl x 2nl).  precision="mixed":
+    split-BF16 exchange; incremental=True adds the exchange of the change since the source's previous
+    mixed build (a full one when there is none)."""
     n = 2 * eri.nl
     if tuple(density_matrix.shape) != (n, n):
         raise RrError(L.RR_ERR_ARG, "x2cFockMatrix (RI): density_matrix dimension does not match 2*nLarge")
@@ -190,7 +198,7 @@ def x2cFockMatrix(h_x2c, eri: RiX2cEriSource, density_matrix, stream: int | None
     S = conv(eri.overlap, np.complex128)
     X = conv(eri.x_large, np.complex128)
     F = _cplx_out((n, n), dev, P.device if dev else None)
-    o = L.opts(L.RR_MEM_DEVICE if dev else L.RR_MEM_HOST, stream=stream)
+    o = _prec_opts(dev, stream, precision, incremental)
     L.check(L.lib().rr_ri_fock_x2c(store.handle, _ptr(h), _ptr(P), _ptr(S), _ptr(X), X.shape[1], _ptr(F),
                                    ctypes.byref(o)))
     return F
@@ -235,8 +243,9 @@ def riFockTwoElectronDirect(eri: RiDirectEriSource, density_ukb, c_occ_ukb, occu
     return G
 
 
-def rkbFockMatrix(h_rkb, eri: RiDirectEriSource, density_matrix, stream: int | None = None):
-    """src/UKB/UkbFockMatrixRi.cpp:185 via rr_ri_fock_rkb."""
+def rkbFockMatrix(h_rkb, eri: RiDirectEriSource, density_matrix, stream: int | None = None, precision: str = "fp64",
+                  incremental: bool = False):
+    """src/UKB/UkbFockMatrixRi.cpp:185 via rr_ri_fock_rkb.  precision / incremental as for x2cFockMatrix."""
     n_rkb = h_rkb.shape[0]
     if tuple(density_matrix.shape) != (n_rkb, n_rkb):
         raise RrError(L.RR_ERR_ARG, "rkbFockMatrix (RI): density_matrix dimension does not match h_rkb")
@@ -251,7 +260,7 @@ def rkbFockMatrix(h_rkb, eri: RiDirectEriSource, density_matrix, stream: int | N
     if v.shape != (2 * eri.nl + 2 * eri.ns, n_rkb) or x.shape[0] != n_rkb:
         raise RrError(L.RR_ERR_ARG, "rkbFockMatrix (RI): v_total/x_full dimensions are inconsistent")
     F = _cplx_out((n_rkb, n_rkb), dev, P.device if dev else None)
-    o = L.opts(L.RR_MEM_DEVICE if dev else L.RR_MEM_HOST, stream=stream)
+    o = _prec_opts(dev, stream, precision, incremental)
     L.check(L.lib().rr_ri_fock_rkb(store.handle, _ptr(h), _ptr(v), n_rkb, _ptr(s), _ptr(x), x.shape[1], _ptr(P),
                                    _ptr(F), ctypes.byref(o)))
     return F

@@ -29,7 +29,8 @@ def _result(res, P, hist):
     it = int(res.iterations)
     return dict(energy=res.electronic_energy, iterations=it, converged=bool(res.converged), P=P,
                 history=hist[:it].copy(), seconds=res.seconds, mixed_iterations=int(res.mixed_iterations),
-                fp64_iterations=int(res.fp64_iterations))
+                fp64_iterations=int(res.fp64_iterations),
+                phase_ms=dict(build=res.build_ms, diis=res.diis_ms, density=res.density_ms))
 
 
 def runNonRelativisticHartreeFock(eri: RiNonRelEriSource, h_core, x_large, initial_density, n_electrons: int,
@@ -49,16 +50,17 @@ def runNonRelativisticHartreeFock(eri: RiNonRelEriSource, h_core, x_large, initi
     hist = np.full(max_iterations, np.nan)
     L.check(L.lib().rr_scf_run_nonrel(eri.store.handle, _ptr(h), _ptr(X), X.shape[1], _ptr(S), _ptr(P0), n_electrons,
                                       ctypes.byref(so), ctypes.byref(res), _ptr(P), _ptr(hist), ctypes.byref(L.opts())))
-    it = int(res.iterations)
-    return dict(energy=res.electronic_energy, iterations=it, converged=bool(res.converged), P=P,
-                history=hist[:it].copy(), seconds=res.seconds, mixed_iterations=int(res.mixed_iterations),
-                fp64_iterations=int(res.fp64_iterations))
+    return _result(res, P, hist)
 
 
 def runX2CHartreeFockScf(h_x2c, eri: RiX2cEriSource, x_large, initial_density, n_electrons: int, overlap=None,
                          diis_size: int = 5, max_iterations: int = 100, energy_tolerance: float = 1e-8,
-                         density_tolerance: float = 1e-6, kramers_restricted: bool = True, mixing: float = 1.0) -> dict:
-    """X2C-HF on the GPU (rr_scf_run_x2c).  `overlap` defaults to the source's overlap."""
+                         density_tolerance: float = 1e-6, kramers_restricted: bool = True, mixing: float = 1.0,
+                         precision: str = "fp64", mixed_switch: float = 0.0) -> dict:
+    """X2C-HF on the GPU (rr_scf_run_x2c).  `overlap` defaults to the source's overlap.
+    precision="mixed": incremental split-BF16 exchange, the last iteration an FP64 build of the
+    converged density; mixed_switch > 0 re-seeds the accumulated exchange once in FP64 when
+    |dE| < mixed_switch."""
     n = 2 * eri.nl
     S = _host(eri.overlap if overlap is None else overlap, np.complex128)
     h = _host(h_x2c, np.complex128)
@@ -66,7 +68,8 @@ def runX2CHartreeFockScf(h_x2c, eri: RiX2cEriSource, x_large, initial_density, n
     P0 = _host(initial_density, np.complex128)
     if h.shape != (n, n) or P0.shape != (n, n) or S.shape != (n, n) or X.shape[0] != n:
         raise RrError(L.RR_ERR_ARG, "runX2CHartreeFockScf: matrix dimensions do not match 2*nLarge")
-    so = _opts(diis_size, max_iterations, energy_tolerance, density_tolerance, "fp64", 0.0, kramers_restricted, mixing)
+    so = _opts(diis_size, max_iterations, energy_tolerance, density_tolerance, precision, mixed_switch,
+               kramers_restricted, mixing)
     res = L.ScfResult()
     P = np.empty((n, n), dtype=np.complex128)
     hist = np.full(max_iterations, np.nan)
@@ -78,8 +81,9 @@ def runX2CHartreeFockScf(h_x2c, eri: RiX2cEriSource, x_large, initial_density, n
 def runDiracHartreeFockScf(h_rkb, eri: RiDirectEriSource, x_full, initial_density, n_electrons: int, overlap=None,
                            diis_size: int = 5, max_iterations: int = 100, energy_tolerance: float = 1e-8,
                            density_tolerance: float = 1e-6, kramers_restricted: bool = True,
-                           mixing: float = 1.0) -> dict:
-    """4c-DHF on the GPU (rr_scf_run_dhf).  `overlap` defaults to the source's s_full."""
+                           mixing: float = 1.0, precision: str = "fp64", mixed_switch: float = 0.0) -> dict:
+    """4c-DHF on the GPU (rr_scf_run_dhf).  `overlap` defaults to the source's s_full.  precision and
+    mixed_switch as for runX2CHartreeFockScf."""
     h = _host(h_rkb, np.complex128)
     n = h.shape[0]
     S = _host(eri.s_full if overlap is None else overlap, np.complex128)
@@ -88,7 +92,8 @@ def runDiracHartreeFockScf(h_rkb, eri: RiDirectEriSource, x_full, initial_densit
     P0 = _host(initial_density, np.complex128)
     if X.shape != (n, n):
         raise RrError(L.RR_ERR_ARG, "rkbDensityMatrix: C_DHF is not square")
-    so = _opts(diis_size, max_iterations, energy_tolerance, density_tolerance, "fp64", 0.0, kramers_restricted, mixing)
+    so = _opts(diis_size, max_iterations, energy_tolerance, density_tolerance, precision, mixed_switch,
+               kramers_restricted, mixing)
     res = L.ScfResult()
     P = np.empty((n, n), dtype=np.complex128)
     hist = np.full(max_iterations, np.nan)
@@ -99,7 +104,8 @@ def runDiracHartreeFockScf(h_rkb, eri: RiDirectEriSource, x_full, initial_densit
 
 def runX2CHartreeFockScfBatch(problems, workers: int = 16, diis_size: int = 5, max_iterations: int = 100,
                               energy_tolerance: float = 1e-8, density_tolerance: float = 1e-6,
-                              kramers_restricted: bool = True) -> list:
+                              kramers_restricted: bool = True, precision: str = "fp64",
+                              mixed_switch: float = 0.0) -> list:
     """A batch of independent X2C-HF problems (a geometry scan of uneven sizes) run concurrently
     (rr_scf_run_x2c_batch: `workers` host threads, one stream per problem's handle).  Each problem is
     a dict with eri (RiX2cEriSource), h_x2c, x_large, initial_density, n_electrons and optionally
@@ -121,6 +127,7 @@ def runX2CHartreeFockScfBatch(problems, workers: int = 16, diis_size: int = 5, m
         outs.append((P, hist))
         insts[i] = L.X2cInstance(eri.store.handle, _ptr(h), _ptr(X), X.shape[1], _ptr(S), _ptr(P0),
                                  int(pr["n_electrons"]), 0, _ptr(P), _ptr(hist), L.ScfResult())
-    so = _opts(diis_size, max_iterations, energy_tolerance, density_tolerance, "fp64", 0.0, kramers_restricted, 1.0)
+    so = _opts(diis_size, max_iterations, energy_tolerance, density_tolerance, precision, mixed_switch,
+               kramers_restricted, 1.0)
     L.check(L.lib().rr_scf_run_x2c_batch(insts, len(problems), ctypes.byref(so), workers))
     return [_result(insts[i].result, P, hist) for i, (P, hist) in enumerate(outs)]
