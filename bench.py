@@ -234,6 +234,77 @@ def scf_times(torch, want_cpu: bool):
     return out
 
 
+# Relativistic time-to-convergence systems (the 4-component shapes of the Kramers-restricted DHF
+# configuration, and an X2C-HF system of 400 spinors): the synthetic generator's two-electron part
+# is scaled (B by the factor, so J and K by its square) so that the FP64 loops need several
+# iterations, as molecular SCFs do.
+X2C_NL, X2C_NAUX, X2C_NE, X2C_GAP, X2C_B = 200, 1000, 80, 1.5, 6.0
+DHF_GAP, DHF_B = 0.4, 3.0
+
+
+def rel_scf_times(want_cpu: bool, rkb_ref_build_s=None):
+    """Time to an energy change below 1e-8 Ha on one GPU for X2C-HF and 4c-DHF: the FP64 loop against
+    the mixed loop (incremental split-BF16 exchange, one FP64 build of the final density), best of two
+    runs each, with per-phase device times; the reference's CPU time is one of its own Fock builds of the
+    same system times the FP64 iteration count (its loop spends nearly all its time in those builds)."""
+    from rerdmft_b200 import _lib as L
+    from rerdmft_b200 import ri, scf, synth
+
+    def compare(run, src):
+        L.check(L.lib().rr_ri_set_profiling(src.store.handle, 1))
+        out = {}
+        for prec in ("fp64", "mixed"):
+            run(prec)  # warm-up (builds the split-BF16 operands once)
+            best = None
+            for _ in range(2):
+                r = run(prec)
+                if best is None or r["seconds"] < best["seconds"]:
+                    best = r
+            out[prec] = dict(seconds=best["seconds"], energy=best["energy"], iterations=best["iterations"],
+                             converged=best["converged"], mixed_iterations=best["mixed_iterations"],
+                             fp64_iterations=best["fp64_iterations"],
+                             phase_ms={k: round(v, 3) for k, v in best["phase_ms"].items()})
+        out["mixed_over_fp64_time"] = out["mixed"]["seconds"] / out["fp64"]["seconds"]
+        out["mixed_minus_fp64_energy"] = out["mixed"]["energy"] - out["fp64"]["energy"]
+        return out
+
+    res = {}
+    s = synth.x2c_system(X2C_NL, X2C_NAUX, X2C_NE, seed=SEED + 21, box=20.0, gap=X2C_GAP)
+    B = s["B"] * X2C_B
+    src = ri.RiX2cEriSource(X2C_NL, B, s["X"], s["S"])
+    res["x2c_hf"] = compare(lambda prec: scf.runX2CHartreeFockScf(s["h"], src, s["X"], s["P0"], X2C_NE, precision=prec),
+                            src)
+    res["x2c_hf"]["workload"] = (f"X2C-HF nl={X2C_NL} ({2 * X2C_NL} spinors) naux={X2C_NAUX} {X2C_NE} electrons, "
+                                 f"core gap {X2C_GAP} Ha, B x {X2C_B}")
+    if want_cpu:
+        from oracle import ref
+
+        if ref.available():
+            ref.set_threads(os.cpu_count() or 1)
+            t0 = time.perf_counter()
+            ref.x2c_fock(s["h"], B, s["P0"], s["S"], s["X"])
+            dt = time.perf_counter() - t0
+            res["x2c_hf"]["reference_cpu"] = dict(
+                seconds_estimate=dt * res["x2c_hf"]["fp64"]["iterations"], seconds_per_build=dt,
+                cores=os.cpu_count() or 1, sample="one reference x2cFockMatrix of this system x the FP64 iteration count")
+    src.store.close()
+    del B, s
+    s = synth.rkb_system(NL4, NS4, NAUX4, 2 * (NOCC4 // 2), seed=SEED + 11, box=20.0, gap=DHF_GAP)
+    src = ri.RiDirectEriSource(NL4, NS4, s["B_LL"] * DHF_B, s["B_SS"] * DHF_B, s["v_total"], s["s_full"], s["x_full"])
+    ne = 2 * (NOCC4 // 2)
+    res["dhf_4c"] = compare(lambda prec: scf.runDiracHartreeFockScf(s["h"], src, s["x_full"], s["P0"], ne,
+                                                                      precision=prec), src)
+    res["dhf_4c"]["workload"] = (f"4c-DHF nl={NL4} ns={NS4} naux={NAUX4} {ne} electrons (RKB basis {4 * NL4}), "
+                                 f"core gap {DHF_GAP} Ha, B x {DHF_B}")
+    if want_cpu and rkb_ref_build_s:
+        res["dhf_4c"]["reference_cpu"] = dict(
+            seconds_estimate=rkb_ref_build_s * res["dhf_4c"]["fp64"]["iterations"], seconds_per_build=rkb_ref_build_s,
+            cores=os.cpu_count() or 1,
+            sample="the reference rkbFockMatrix time of the 4c Fock-build block (same shapes) x the FP64 iteration count")
+    src.store.close()
+    return res
+
+
 def max_over_ranks(pg, seconds: float, device: str) -> float:
     """The job's time: the slowest rank's (all-reduce MAX of one float; unchanged with one rank)."""
     if pg is None:
@@ -518,6 +589,8 @@ def main():
     rkb_block = rkb_fock_times(torch, fp64_peak, want_cpu=not args.no_cpu_baseline)
     orb_block = orbital_optimization_block()
     x2c_block = x2c_batch_block(want_cpu=not args.no_cpu_baseline)
+    rel_block = rel_scf_times(not args.no_cpu_baseline,
+                              (rkb_block.get("reference_cpu") or {}).get("seconds_per_build"))
     line = dict(
         metric=METRIC, value=value, unit=UNIT, n_gpus=ws, steps=args.steps, warmup=args.warmup,
         ms_per_step=1e3 * t / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
@@ -545,6 +618,7 @@ def main():
         kernels={"half_transform_tflops": ht_tf, "syrk_tflops_full_count": ex_tf},
         phases_ms=phases, clocks=clk, e2e=e2e, gpu_launches=int(launches), cpu_baseline=cpu,
         time_to_1e8_ha=scf_block,
+        time_to_1e8_ha_relativistic=rel_block,
         rkb_fock_4c=rkb_block,
         orbital_optimization=orb_block,
         x2c_batch=x2c_block,

@@ -13,10 +13,11 @@ void fock_nonrel(rr_ri_store*, const double*, const double*, const double*, cons
                  const rr_opts*);
 void jk_occupied(rr_ri_store*, const double*, int64_t, double*, double*, const rr_opts*);
 void fock_x2c(rr_ri_store*, const double*, const double*, const double*, const double*, int64_t, double*,
-              const rr_opts*, const RelBuild* = nullptr);
+              const rr_opts*, const RelBuild* = nullptr, const double* = nullptr, int64_t = 0);
 void ukb_two_electron(rr_ri_store*, const double*, const double*, int64_t, const double*, double*, const rr_opts*);
 void fock_rkb(rr_ri_store*, const double*, const double*, int64_t, const double*, const double*, int64_t,
-              const double*, double*, const rr_opts*, const RelBuild* = nullptr);
+              const double*, double*, const rr_opts*, const RelBuild* = nullptr, const double* = nullptr,
+              int64_t = 0);
 void scf_nonrel(rr_ri_store*, const double*, const double*, int64_t, const double*, const double*, int,
                 const rr_scf_opts*, rr_scf_result*, double*, double*, const rr_opts*);
 void scf_rel(rr_ri_store*, int, const double*, const double*, int64_t, const double*, int64_t, const double*,

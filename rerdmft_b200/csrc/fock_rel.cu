@@ -18,6 +18,8 @@ namespace rr {
 
 int64_t occupied_ct(rr_ri_store* h, const double* X, const double* S, const double* Dp, int64_t n, int64_t n_eff,
                     double scale, bool cplx, bool weighted, double* Ct, cudaStream_t s);
+void projector_ct(rr_ri_store* h, const double* A, const double* Pe, const double* X, int64_t n, int64_t n_eff,
+                  int64_t r, bool cplx, double* Ct, cudaStream_t s);
 void prof_mark(rr_ri_store* h, int i, cudaStream_t s);
 
 namespace {
@@ -218,8 +220,11 @@ void two_electron_rel(rr_ri_store* h, const Flavours& fl, int64_t ntot, const do
   }
 }
 
+// With `proj` (device, n_eff x n_eff, a rank-proj_rank orthogonal projector in the orthonormal basis
+// of X whose X proj X^dagger is P, as the SCF loop has it from SP2) the occupied spinors come from
+// that projector directly instead of being recovered from P.
 void fock_x2c(rr_ri_store* h, const double* hc, const double* P, const double* S, const double* X, int64_t n_eff,
-              double* F, const rr_opts* o, const RelBuild* rb) {
+              double* F, const rr_opts* o, const RelBuild* rb, const double* proj, int64_t proj_rank) {
   RR_REQUIRE(h->ntens == 1, RR_ERR_STATE, "rr_ri_fock_x2c: handle holds a 4-component store");
   const int64_t nl = h->n, n = 2 * nl, nn2 = n * n * 2;
   RR_REQUIRE(n_eff >= 0 && n_eff <= n, RR_ERR_ARG, "rr_ri_fock_x2c: n_eff out of range");
@@ -255,7 +260,9 @@ void fock_x2c(rr_ri_store* h, const double* hc, const double* P, const double* S
   RR_CUDA(cudaMemsetAsync(Dp, 0, sizeof(double) * pitch, s));
   spin_sum_kernel<<<blocks_for(nl * nl), 256, 0, s>>>(Dp, Pd, n, 0, nl, nl);
   RR_LAUNCH_CHECK();
-  const int64_t r = occupied_ct(h, Xd, Sd, Pd, n, n_eff, 1.0, true, true, Ct, s);
+  int64_t r = proj_rank;
+  if (proj) projector_ct(h, proj, nullptr, Xd, n, n_eff, r, true, Ct, s);
+  else r = occupied_ct(h, Xd, Sd, Pd, n, n_eff, 1.0, true, true, Ct, s);
   prof_mark(h, 1, s);
   Flavours fl;
   fl.nf = 2;
@@ -325,8 +332,10 @@ void ukb_two_electron(rr_ri_store* h, const double* P, const double* C, int64_t 
 }
 
 // rkbFockMatrix: recovery in the RKB basis with x_full / s_full, embedding with v_total.
+// `proj` / `proj_rank` as for fock_x2c (in the orthonormal basis of x_full).
 void fock_rkb(rr_ri_store* h, const double* hc, const double* v, int64_t n_rkb, const double* s_full,
-              const double* x_full, int64_t n_eff, const double* P, double* F, const rr_opts* o, const RelBuild* rb) {
+              const double* x_full, int64_t n_eff, const double* P, double* F, const rr_opts* o, const RelBuild* rb,
+              const double* proj, int64_t proj_rank) {
   RR_REQUIRE(h->ntens == 2, RR_ERR_STATE, "rr_ri_fock_rkb: needs a 4-component store (rr_ri_create_4c)");
   const int64_t nl = h->n, ns = h->ns, nu = 2 * nl + 2 * ns;
   RR_REQUIRE(n_rkb >= 1 && n_eff >= 0 && n_eff <= n_rkb, RR_ERR_ARG, "rr_ri_fock_rkb: bad n_rkb / n_eff");
@@ -363,7 +372,9 @@ void fock_rkb(rr_ri_store* h, const double* hc, const double* v, int64_t n_rkb, 
     copy_in(Pd, P, rr2, true, s);
   }
   prof_mark(h, 0, s);
-  const int64_t r = occupied_ct(h, xd, sd, Pd, n_rkb, n_eff, 1.0, true, true, Ct_rkb, s);
+  int64_t r = proj_rank;
+  if (proj) projector_ct(h, proj, nullptr, xd, n_rkb, n_eff, r, true, Ct_rkb, s);
+  else r = occupied_ct(h, xd, sd, Pd, n_rkb, n_eff, 1.0, true, true, Ct_rkb, s);
   // c_t (UKB) = c_t (RKB) v_total^dagger  (C_occ_ukb = v_total C_occ_rkb)
   GemmDesc g;
   g.cplx = true;
@@ -373,14 +384,26 @@ void fock_rkb(rr_ri_store* h, const double* hc, const double* v, int64_t n_rkb, 
     g.C = Ct_ukb; g.ldc = nu;
     gemm(g, s);
   }
-  // P_ukb = v P v^dagger
+  // P_ukb = v P v^dagger, only its four diagonal flavour blocks (all that J reads): each block
+  // v_f P v_f^dagger is Hermitian, so upper tiles and a mirror
   GemmDesc a;
   a.cplx = true;
   a.M = nu; a.N = n_rkb; a.K = n_rkb; a.A = vd; a.lda = n_rkb; a.B = Pd; a.ldb = n_rkb; a.C = VP; a.ldc = n_rkb;
-  gemm(a, s);
-  a.M = nu; a.N = nu; a.K = n_rkb; a.A = VP; a.lda = n_rkb; a.B = vd; a.ldb = n_rkb; a.opB = Op::T; a.conjB = true;
-  a.C = Pu; a.ldc = nu;
-  gemm(a, s);
+  gemm(a, s, h->work.p, static_cast<int64_t>(h->work.n));
+  {
+    const int64_t boff[4] = {0, nl, 2 * nl, 2 * nl + ns}, bfs[4] = {nl, nl, ns, ns};
+    for (int f = 0; f < 4; ++f) {
+      if (bfs[f] == 0) continue;
+      GemmDesc d;
+      d.cplx = true;
+      d.M = bfs[f]; d.N = bfs[f]; d.K = n_rkb;
+      d.A = VP + 2 * boff[f] * n_rkb; d.lda = n_rkb;
+      d.B = vd + 2 * boff[f] * n_rkb; d.ldb = n_rkb; d.opB = Op::T; d.conjB = true;
+      d.C = Pu + 2 * (boff[f] * nu + boff[f]); d.ldc = nu;
+      d.mirror = 1;
+      gemm(d, s, h->work.p, static_cast<int64_t>(h->work.n));
+    }
+  }
   RR_CUDA(cudaMemsetAsync(DL, 0, sizeof(double) * pl, s));
   RR_CUDA(cudaMemsetAsync(DS, 0, sizeof(double) * ps, s));
   spin_sum_kernel<<<blocks_for(nl * nl), 256, 0, s>>>(DL, Pu, nu, 0, nl, nl);
@@ -405,7 +428,8 @@ void fock_rkb(rr_ri_store* h, const double* hc, const double* v, int64_t n_rkb, 
   if (Fd != hd) copy_out(Fd, hd, rr2, false, s);
   b.M = n_rkb; b.N = n_rkb; b.K = nu; b.A = vd; b.lda = n_rkb; b.opA = Op::T; b.conjA = true; b.B = GV; b.ldb = n_rkb;
   b.C = Fd; b.ldc = n_rkb; b.beta = 1.0;
-  gemm(b, s);
+  b.mirror = 1;  // F = h + v^dagger G v is Hermitian
+  gemm(b, s, h->work.p, static_cast<int64_t>(h->work.n));
   if (host) copy_out(F, Fd, rr2, true, s);
   prof_mark(h, 4, s);
   if (host || (o && o->sync)) check_status(h, s);

@@ -19,6 +19,7 @@ struct MixedScratch {
   DevBuf<uint16_t> coef_hi, coef_lo;
   DevBuf<uint16_t> pl_hi, pl_lo;
   DevBuf<float> work;
+  DevBuf<double> xacc;  // incremental builds: X = sum_P (W B^P)^dagger (U B^P) before K += X + X^dagger
 };
 
 // Flavour blocks of the exchange: columns [off, off + fs) of c_t contract with tensor `tens`.
@@ -33,9 +34,9 @@ struct ExFlavours {
 // Builds the resident split copy of B (rows of `pitch` doubles per aux index) once per store.
 void mixed_prepare(MixedOperands& mo, const double* B, int64_t pitch, int64_t n, int64_t naux, cudaStream_t s);
 
-// Split-BF16 exchange on tcgen05 for every flavour block f <= u:
+// Split-BF16 exchange on tcgen05 for every flavour block (f, u):
 //   K_fu = sum_P (Ct_f B^P)^dagger (Ct_u B^P)                         (Ct_prev == nullptr)
-//   K_fu = sum_P (W_f B^P)^dagger (U_u B^P) + (U_f B^P)^dagger (W_u B^P),
+//   K_fu = X_fu + X_uf^dagger,  X_fu = sum_P (W_f B^P)^dagger (U_u B^P),
 //          W = (Ct + Ct_prev) / 2, U = Ct - Ct_prev                    (Ct_prev given)
 // The second form is exactly K(Ct) - K(Ct_prev), with a rounding error proportional to |U|
 // instead of |Ct|.  Ct / Ct_prev: r x ld row-major, real or interleaved complex (cplx).  K: real or

@@ -203,6 +203,22 @@ __global__ void umma_place_kernel(const float* wre, const float* wim, int splits
   }
 }
 
+// K (+)= X + X^dagger over the whole ldk x ldk matrix (real: X + X^T; complex interleaved).
+__global__ void herm_add_kernel(double* K, const double* X, int64_t ldk, int accumulate, int cplx) {
+  for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < ldk * ldk;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t i = idx / ldk, j = idx % ldk, t = j * ldk + i;
+    if (cplx) {
+      const double re = X[2 * idx] + X[2 * t], im = X[2 * idx + 1] - X[2 * t + 1];
+      K[2 * idx] = accumulate ? K[2 * idx] + re : re;
+      K[2 * idx + 1] = accumulate ? K[2 * idx + 1] + im : im;
+    } else {
+      const double v = X[idx] + X[t];
+      K[idx] = accumulate ? K[idx] + v : v;
+    }
+  }
+}
+
 // ---- persistent half-transform ----
 // One CTA per SM walks the (P, 128-row tile) items round robin with one continuous TMA ring across
 // items and two TMEM accumulators, so the epilogue of item j (TMEM -> split BF16 planes) overlaps the
@@ -216,12 +232,13 @@ constexpr int ERR_HT_FULL = 1 << 7, ERR_HT_EMPTY = 1 << 8, ERR_HT_TFULL = 1 << 9
 
 // Epilogue layout.  The pass's columns form `groups` groups of `period` columns (one flavour each);
 // a group is made of blocks of `blk` columns.  Column c of group g, in block q = c / blk, goes to
-// plane o of that group at column P * period + dst[o][q] * blk + c % blk, multiplied by sgn[o][q].
+// plane o of that group at column P * operiod + dst[o][q] * blk + c % blk, multiplied by
+// sgn[o][q]; dst[o][q] < 0 leaves block q out of plane o.
 struct HtEpi {
   __nv_bfloat16* hi[2][3];
   __nv_bfloat16* lo[2][3];
   int64_t ld;  // row pitch of every plane (elements)
-  int ncols, groups, planes, period, blk;
+  int ncols, groups, planes, period, operiod, blk;
   signed char dst[3][4], sgn[3][4];
 };
 
@@ -244,7 +261,7 @@ __device__ __forceinline__ uint32_t pack_bf16(float x, float y) {
 
 // Writes 16 accumulator columns c0 .. c0 + 15 of row `row` (aux index P) into the planes.
 __device__ __forceinline__ void ht_store16(const HtEpi& e, int64_t row, int P, int c0, const float* v, bool vec) {
-  const int64_t rbase = row * e.ld + static_cast<int64_t>(P) * e.period;
+  const int64_t rbase = row * e.ld + static_cast<int64_t>(P) * e.operiod;
   if (vec) {
 #pragma unroll
     for (int h8 = 0; h8 < 16; h8 += 8) {
@@ -252,6 +269,7 @@ __device__ __forceinline__ void ht_store16(const HtEpi& e, int64_t row, int P, i
       if (gc < e.ncols) {
         const int g = gc / e.period, c = gc - g * e.period, q = c / e.blk, cin = c - q * e.blk;
         for (int o = 0; o < e.planes; ++o) {
+          if (e.dst[o][q] < 0) continue;
           const float sg = static_cast<float>(e.sgn[o][q]);
           const int64_t off = rbase + e.dst[o][q] * e.blk + cin;
           uint32_t h[4], l[4];
@@ -274,6 +292,7 @@ __device__ __forceinline__ void ht_store16(const HtEpi& e, int64_t row, int P, i
       if (gc >= e.ncols) continue;
       const int g = gc / e.period, c = gc - g * e.period, q = c / e.blk, cin = c - q * e.blk;
       for (int o = 0; o < e.planes; ++o) {
+        if (e.dst[o][q] < 0) continue;
         const float x = static_cast<float>(e.sgn[o][q]) * v[t];
         const __nv_bfloat16 hi = __float2bfloat16_rn(x);
         const int64_t off = rbase + e.dst[o][q] * e.blk + cin;
@@ -375,7 +394,8 @@ __global__ void __launch_bounds__(HT_THREADS, 1)
     uint32_t j = 0;
     const uint32_t lane_base = static_cast<uint32_t>(warp * 32) << 16;
     // 16-byte stores need 8-column runs that stay inside one block and aligned plane columns.
-    const bool vec = (e.blk & 7) == 0 && (e.period & 7) == 0 && (e.ncols & 7) == 0 && (e.ld & 7) == 0;
+    const bool vec = (e.blk & 7) == 0 && (e.period & 7) == 0 && (e.operiod & 7) == 0 && (e.ncols & 7) == 0 &&
+                     (e.ld & 7) == 0;
     for (int64_t item = blockIdx.x; item < total; item += gridDim.x, ++j) {
       const uint32_t b = j & 1;
       const bool ok = mbar_wait(&tfull[b], (j >> 1) & 1, err, ERR_HT_TFULL, dead);
@@ -647,11 +667,19 @@ void mixed_exchange_general(const MixedOperands* ops, MixedScratch& scr, const E
     RR_REQUIRE(mo.ready && mo.n == fl.fs[f] && mo.naux == naux, RR_ERR_STATE, "mixed exchange: operands not prepared");
     RR_REQUIRE(fl.fs[f] <= 65535, RR_ERR_ARG, "mixed exchange: dimensions exceed the grid limits");
   }
-  if (!accumulate) RR_CUDA(cudaMemsetAsync(K, 0, sizeof(double) * ldk * ldk * (cplx ? 2 : 1), s));
+  const int pl = cplx ? 2 : 1;
+  if (!accumulate) RR_CUDA(cudaMemsetAsync(K, 0, sizeof(double) * ldk * ldk * pl, s));
   if (r == 0 || naux == 0) return;
+  // Full build:        coefficient rows [Ct] (real) or [Re Ct, Im Ct]; planes A = T, (complex) B_im =
+  //                    [Im, -Re]; blocks f <= u: Re K = A_f A_u^T (Hermitian diagonal blocks: upper
+  //                    tiles), Im K = A_f B_im,u^T.
+  // Incremental build: rows [W, U] or [Re W, Im W, Re U, Im U]; planes A = W part, B_re = U part,
+  //                    (complex) B_im = [Im U, -Re U]; X_fu = A_f B_u^T for every ordered pair (f, u),
+  //                    then K += X + X^dagger (= K(Ct) - K(Ct_prev)).
   const bool incr = Ct_prev != nullptr;
   const int mode = cplx ? (incr ? 3 : 2) : (incr ? 1 : 0);
-  const int nblk = mode == 0 ? 1 : (mode == 3 ? 4 : 2);
+  const int nblk = mode == 0 ? 1 : (mode == 3 ? 4 : 2);      // coefficient blocks per flavour group
+  const int oblk = incr ? nblk / 2 : nblk;                     // blocks per aux index in a plane
   const int planes = mode == 0 ? 1 : (mode == 3 ? 3 : 2);
   const int pre = incr ? 1 : 0;  // plane holding the B operand of the real part (imaginary: the last plane)
   // Occupied rows per slice: one flavour's group must fit a 256-column accumulator.
@@ -659,8 +687,8 @@ void mixed_exchange_general(const MixedOperands* ops, MixedScratch& scr, const E
   const int64_t nslices = (r + rs_max - 1) / rs_max;
   const int64_t rs_full = (r + nslices - 1) / nslices;
   const int r8 = static_cast<int>(round8(rs_full));
-  const int period = nblk * r8;
-  const int64_t kt = naux * period, ldt = round8(kt);
+  const int period = nblk * r8, operiod = oblk * r8;
+  const int64_t kt = naux * operiod, ldt = round8(kt);
   // Passes: flavours of one tensor, two per pass when both groups fit 256 columns.
   int ntens = 1;
   for (int f = 0; f < fl.nf; ++f) ntens = std::max(ntens, fl.tens[f] + 1);
@@ -681,6 +709,14 @@ void mixed_exchange_general(const MixedOperands* ops, MixedScratch& scr, const E
       }
     }
   }
+  // Exchange products of one slice: (f, u, upper tiles).
+  struct Blk { int f, u; bool upper; };
+  std::vector<Blk> blocks;
+  for (int f = 0; f < fl.nf; ++f)
+    for (int u = 0; u < fl.nf; ++u) {
+      if (!incr && u < f) continue;
+      blocks.push_back({f, u, !incr && f == u});
+    }
   // Scratch sizes for the whole call, before the first launch.
   int64_t coef_sz = 0, pl_sz = 0, work_sz = 0;
   int64_t pl_off[4];
@@ -689,30 +725,34 @@ void mixed_exchange_general(const MixedOperands* ops, MixedScratch& scr, const E
     pl_off[f] = pl_sz;
     pl_sz += round_up(planes * fl.fs[f] * ldt, 128);
   }
-  for (int f = 0; f < fl.nf; ++f)
-    for (int u = cplx ? f : 0; u < (cplx ? fl.nf : 1); ++u) {
-      const BlockPlan bp = plan_block(fl.fs[f], fl.fs[u], kt, f == u);
-      work_sz = std::max<int64_t>(work_sz, (cplx ? 2 : 1) * static_cast<int64_t>(bp.splits) * bp.tiles * BM * GBN);
-    }
+  for (const Blk& b : blocks) {
+    const BlockPlan bp = plan_block(fl.fs[b.f], fl.fs[b.u], kt, b.upper);
+    work_sz = std::max<int64_t>(work_sz, pl * static_cast<int64_t>(bp.splits) * bp.tiles * BM * GBN);
+  }
   scr.coef_hi.ensure(static_cast<size_t>(coef_sz));
   scr.coef_lo.ensure(static_cast<size_t>(coef_sz));
   scr.pl_hi.ensure(static_cast<size_t>(pl_sz));
   scr.pl_lo.ensure(static_cast<size_t>(pl_sz));
   scr.work.ensure(static_cast<size_t>(work_sz));
+  if (incr) scr.xacc.ensure(static_cast<size_t>(ldk * ldk * pl));
+  double* target = incr ? scr.xacc.p : K;  // X (incremental) or K itself
+  if (incr) RR_CUDA(cudaMemsetAsync(target, 0, sizeof(double) * ldk * ldk * pl, s));
   auto plane = [&](uint16_t* base, int f, int o) { return base + pl_off[f] + static_cast<int64_t>(o) * fl.fs[f] * ldt; };
 
-  // Plane layouts per mode: dst block and sign of each source block.
-  signed char dst[3][4] = {{0, 1, 2, 3}, {0, 0, 0, 0}, {0, 0, 0, 0}};
+  // Plane layouts per mode: destination block (-1: not in this plane) and sign of each source block.
+  signed char dst[3][4] = {{0, 1, 2, 3}, {-1, -1, -1, -1}, {-1, -1, -1, -1}};
   signed char sgn[3][4] = {{1, 1, 1, 1}, {1, 1, 1, 1}, {1, 1, 1, 1}};
-  if (mode == 1) {  // [W, U] -> [U, W]
-    dst[1][0] = 1; dst[1][1] = 0;
-  } else if (mode == 2) {  // [Re, Im] -> [Im, -Re]
+  if (mode == 1) {  // [W, U]: A = W, B = U
+    dst[0][1] = -1;
+    dst[1][1] = 0;
+  } else if (mode == 2) {  // [Re, Im]: A = [Re, Im], B_im = [Im, -Re]
     dst[1][0] = 1; dst[1][1] = 0;
     sgn[1][0] = -1;
-  } else if (mode == 3) {  // [Wr, Wi, Ur, Ui] -> [Ur, Ui, Wr, Wi] and [Ui, -Ur, Wi, -Wr]
-    dst[1][0] = 2; dst[1][1] = 3; dst[1][2] = 0; dst[1][3] = 1;
-    dst[2][0] = 3; dst[2][1] = 2; dst[2][2] = 1; dst[2][3] = 0;
-    sgn[2][0] = -1; sgn[2][2] = -1;
+  } else if (mode == 3) {  // [Wr, Wi, Ur, Ui]: A = [Wr, Wi], B_re = [Ur, Ui], B_im = [Ui, -Ur]
+    dst[0][2] = -1; dst[0][3] = -1;
+    dst[1][2] = 0; dst[1][3] = 1;
+    dst[2][2] = 1; dst[2][3] = 0;
+    sgn[2][2] = -1;
   }
 
   for (int64_t sl = 0; sl < nslices; ++sl) {
@@ -739,29 +779,33 @@ void mixed_exchange_general(const MixedOperands* ops, MixedScratch& scr, const E
       e.groups = p.g;
       e.planes = planes;
       e.period = period;
+      e.operiod = operiod;
       e.blk = r8;
       std::memcpy(e.dst, dst, sizeof(dst));
       std::memcpy(e.sgn, sgn, sizeof(sgn));
       launch_ht(mo, scr.coef_hi.p, scr.coef_lo.p, rows, e, err, s);
     }
-    // Exchange blocks: Re (and Im) of A = plane 0 of f against the B planes of u.
-    for (int f = 0; f < fl.nf; ++f)
-      for (int u = cplx ? f : 0; u < (cplx ? fl.nf : 1); ++u) {
-        const BlockPlan bp = plan_block(fl.fs[f], fl.fs[u], kt, f == u);
-        const int64_t part = static_cast<int64_t>(bp.splits) * bp.tiles * BM * GBN;
-        float* wre = scr.work.p;
-        float* wim = cplx ? scr.work.p + part : nullptr;
-        launch_gemm(bp, plane(scr.pl_hi.p, f, 0), plane(scr.pl_lo.p, f, 0), fl.fs[f], plane(scr.pl_hi.p, u, pre),
-                    plane(scr.pl_lo.p, u, pre), fl.fs[u], kt, ldt, wre, err, s);
-        if (cplx)
-          launch_gemm(bp, plane(scr.pl_hi.p, f, 0), plane(scr.pl_lo.p, f, 0), fl.fs[f],
-                      plane(scr.pl_hi.p, u, planes - 1), plane(scr.pl_lo.p, u, planes - 1), fl.fs[u], kt, ldt, wim, err,
-                      s);
-        umma_place_kernel<<<grid_for(fl.fs[f] * fl.fs[u]), 256, 0, s>>>(
-            wre, wim, bp.splits, bp.tiles, bp.ntn, bp.upper ? 1 : 0, static_cast<int>(fl.fs[f]),
-            static_cast<int>(fl.fs[u]), K, ldk, fl.off[f], fl.off[u], f != u ? 1 : 0, 1, cplx ? 1 : 0);
-        RR_LAUNCH_CHECK();
-      }
+    for (const Blk& b : blocks) {
+      const BlockPlan bp = plan_block(fl.fs[b.f], fl.fs[b.u], kt, b.upper);
+      const int64_t part = static_cast<int64_t>(bp.splits) * bp.tiles * BM * GBN;
+      float* wre = scr.work.p;
+      float* wim = cplx ? scr.work.p + part : nullptr;
+      launch_gemm(bp, plane(scr.pl_hi.p, b.f, 0), plane(scr.pl_lo.p, b.f, 0), fl.fs[b.f], plane(scr.pl_hi.p, b.u, pre),
+                  plane(scr.pl_lo.p, b.u, pre), fl.fs[b.u], kt, ldt, wre, err, s);
+      if (cplx)
+        launch_gemm(bp, plane(scr.pl_hi.p, b.f, 0), plane(scr.pl_lo.p, b.f, 0), fl.fs[b.f],
+                    plane(scr.pl_hi.p, b.u, planes - 1), plane(scr.pl_lo.p, b.u, planes - 1), fl.fs[b.u], kt, ldt,
+                    wim, err, s);
+      const int both = !incr && b.f != b.u ? 1 : 0;
+      umma_place_kernel<<<grid_for(fl.fs[b.f] * fl.fs[b.u]), 256, 0, s>>>(
+          wre, wim, bp.splits, bp.tiles, bp.ntn, bp.upper ? 1 : 0, static_cast<int>(fl.fs[b.f]),
+          static_cast<int>(fl.fs[b.u]), target, ldk, fl.off[b.f], fl.off[b.u], both, 1, cplx ? 1 : 0);
+      RR_LAUNCH_CHECK();
+    }
+  }
+  if (incr) {
+    herm_add_kernel<<<grid_for(ldk * ldk), 256, 0, s>>>(K, scr.xacc.p, ldk, 1, cplx ? 1 : 0);
+    RR_LAUNCH_CHECK();
   }
 }
 

@@ -106,80 +106,11 @@ __global__ void fill_test_matrix_kernel(double* G, int64_t count) {
 }
 
 // Cholesky M = L L^dagger of a small Hermitian positive-definite r x r matrix (row-major,
-// interleaved when PL = 2) by ONE warp: right-looking, lanes split each trailing update, only warp
-// barriers.  `work` holds the r x r factor (shared memory when it fits, else global scratch).
-// Output: out = L^{-dagger} (want_inverse) or L (upper triangle zero), r x r row-major, so that
-// Y <- Y out is a plain GEMM.  status[0] |= 1 on a non-positive pivot.
-template <int PL>
-__global__ void __launch_bounds__(32) chol_small_kernel(const double* M, int64_t r, double* out, double* gwork,
-                                                        int want_inverse, int* status) {
-  extern __shared__ double sm[];
-  double* L = gwork ? gwork : sm;
-  const int lane = threadIdx.x;
-  for (int64_t i = lane; i < r * r * PL; i += 32) L[i] = M[i];
-  __syncwarp();
-  for (int64_t j = 0; j < r; ++j) {
-    double d = L[(j * r + j) * PL];
-    if (!(d > 0.0)) {
-      if (lane == 0) atomicOr(status, 1);
-      d = 1e-300;
-    }
-    const double inv = 1.0 / sqrt(d);
-    __syncwarp();
-    for (int64_t i = j + 1 + lane; i < r; i += 32) {
-      L[(i * r + j) * PL] *= inv;
-      if (PL == 2) L[(i * r + j) * PL + 1] *= inv;
-    }
-    if (lane == 0) {
-      L[(j * r + j) * PL] = sqrt(d);
-      if (PL == 2) L[(j * r + j) * PL + 1] = 0.0;
-    }
-    __syncwarp();
-    // trailing lower triangle: A[i][k] -= L[i][j] conj(L[k][j]), j < k <= i; lane owns rows i
-    for (int64_t i = j + 1 + lane; i < r; i += 32) {
-      const double ar = L[(i * r + j) * PL], ai = PL == 2 ? L[(i * r + j) * PL + 1] : 0.0;
-      for (int64_t k = j + 1; k <= i; ++k) {
-        const double br = L[(k * r + j) * PL], bi = PL == 2 ? L[(k * r + j) * PL + 1] : 0.0;
-        L[(i * r + k) * PL] -= ar * br + ai * bi;
-        if (PL == 2) L[(i * r + k) * PL + 1] -= ai * br - ar * bi;
-      }
-    }
-    __syncwarp();
-  }
-  if (!want_inverse) {
-    for (int64_t e = lane; e < r * r; e += 32) {
-      const int64_t i = e / r, k = e % r;
-      out[e * PL] = k <= i ? L[e * PL] : 0.0;
-      if (PL == 2) out[e * PL + 1] = k <= i ? L[e * PL + 1] : 0.0;
-    }
-    return;
-  }
-  // Column c of L^{-1}: forward substitution on e_c, one lane per column; written as row c of
-  // out = (L^{-1})^dagger, i.e. out[c][i] = conj(Linv[i][c]).
-  for (int64_t c = lane; c < r; c += 32) {
-    double* o = out + c * r * PL;
-    for (int64_t i = 0; i < c; ++i) {
-      o[i * PL] = 0.0;
-      if (PL == 2) o[i * PL + 1] = 0.0;
-    }
-    for (int64_t i = c; i < r; ++i) {
-      // x_i = (delta_ic - sum_{c<=k<i} L[i][k] x_k) / L[i][i]; o holds conj(x)
-      double xr = i == c ? 1.0 : 0.0, xi = 0.0;
-      for (int64_t k = c; k < i; ++k) {
-        const double lr = L[(i * r + k) * PL], li = PL == 2 ? L[(i * r + k) * PL + 1] : 0.0;
-        const double yr = o[k * PL], yi = PL == 2 ? -o[k * PL + 1] : 0.0;  // x_k
-        xr -= lr * yr - li * yi;
-        if (PL == 2) xi -= lr * yi + li * yr;
-      }
-      const double dii = L[(i * r + i) * PL];
-      o[i * PL] = xr / dii;
-      if (PL == 2) o[i * PL + 1] = -xi / dii;
-    }
-  }
-}
-
-// Same contract as chol_small_kernel for r x r matrices whose factor and inverse both fit in shared
-// memory, by one CTA of CHOL_THREADS threads with one __syncthreads per elimination step:
+// interleaved when PL = 2).  Output: out = L^{-dagger} (want_inverse) or L (upper triangle zero),
+// r x r row-major, so that Y <- Y out is a plain GEMM.  status[0] |= 1 on a non-positive pivot.
+// One CTA of CHOL_THREADS threads; the factor, the inverse and the pivots live in shared memory, or
+// in `gbuf` (global, 2 r^2 PL + r doubles, L2-resident at these sizes) when they do not fit.  One
+// __syncthreads per elimination step:
 //  * step j of the factorisation updates the trailing triangle with the UNSCALED column j
 //    (A[i][k] -= A[i][j] conj(A[k][j]) / d_j, spread over all threads) and, in the same phase,
 //    finishes column j-1 (scale by 1/sqrt(d), set the diagonal), which nothing reads any more;
@@ -188,10 +119,10 @@ constexpr int CHOL_THREADS = 256;
 
 template <int PL>
 __global__ void __launch_bounds__(CHOL_THREADS) chol_block_kernel(const double* M, int r, double* out,
-                                                                  int want_inverse, int* status) {
+                                                                  int want_inverse, int* status, double* gbuf) {
   extern __shared__ double sm[];
-  double* A = sm;                 // r x r, factor in the lower triangle
-  double* X = sm + r * r * PL;    // r x r, L^{-1}
+  double* A = gbuf ? gbuf : sm;   // r x r, factor in the lower triangle
+  double* X = A + r * r * PL;     // r x r, L^{-1}
   double* piv = X + r * r * PL;   // r pivots d_j before the square root
   const int t = threadIdx.x;
   for (int e = t; e < r * r * PL; e += CHOL_THREADS) A[e] = M[e];
@@ -218,13 +149,10 @@ __global__ void __launch_bounds__(CHOL_THREADS) chol_block_kernel(const double* 
       if (!(d > 0.0)) d = 1e-300;
       const double inv_d = 1.0 / d;
       const int m = r - j - 1;  // trailing triangle rows j+1..r-1, element (i, k) with k <= i
-      const int tri = m * (m + 1) / 2;
-      for (int e = t; e < tri; e += CHOL_THREADS) {
-        // e -> (a, b) with 0 <= b <= a < m, row-major over the triangle
-        int a = static_cast<int>((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
-        while (a * (a + 1) / 2 > e) --a;
-        while ((a + 1) * (a + 2) / 2 <= e) ++a;
-        const int b = e - a * (a + 1) / 2;
+      // square sweep of the m x m trailing block (upper half skipped): integer index math only
+      for (int e = t; e < m * m; e += CHOL_THREADS) {
+        const int a = e / m, b = e - a * m;
+        if (b > a) continue;
         const int i = j + 1 + a, k = j + 1 + b;
         const double ar = A[(i * r + j) * PL], ai = PL == 2 ? A[(i * r + j) * PL + 1] : 0.0;
         const double br = A[(k * r + j) * PL], bi = PL == 2 ? A[(k * r + j) * PL + 1] : 0.0;
@@ -304,13 +232,11 @@ void projector_ct(rr_ri_store* h, const double* A, const double* Pe, const doubl
   ar2.request(&M, r * r * PL);
   ar2.request(&Wt, r * r * PL);
   ar2.request(&PQ, n_eff * r * PL);
-  ar2.request(&gw, r * r * PL);
+  ar2.request(&gw, 2 * r * r * PL + r);
   ar2.commit();
-  const size_t chol_smem = sizeof(double) * r * r * PL;
-  const bool chol_in_smem = chol_smem <= 160 * 1024;
-  // factor + inverse + pivots in shared memory: the one-CTA kernel; else the one-warp kernel
+  // factor + inverse + pivots in shared memory when they fit, else in the global scratch gw
   const size_t block_smem = sizeof(double) * (2 * r * r * PL + r);
-  const bool chol_block = block_smem <= 160 * 1024;
+  const bool chol_in_smem = block_smem <= 227 * 1024;
   if (cplx) fill_test_matrix_kernel<2><<<blocks_for(n_eff * r * 2), 256, 0, s>>>(G, n_eff * r);
   else fill_test_matrix_kernel<1><<<blocks_for(n_eff * r), 256, 0, s>>>(G, n_eff * r);
   RR_LAUNCH_CHECK();
@@ -320,29 +246,16 @@ void projector_ct(rr_ri_store* h, const double* A, const double* Pe, const doubl
   y.A = A; y.lda = n_eff; y.B = G; y.ldb = r; y.C = Y2; y.ldc = r;
   gemm(y, s, wk, wcap);
   auto chol = [&](const double* mat, int inverse) {
-    if (chol_block) {
-      const int sm = static_cast<int>(block_smem);
-      if (cplx) {
-        auto k = chol_block_kernel<2>;
-        if (sm > 48 * 1024) RR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-        k<<<1, CHOL_THREADS, sm, s>>>(mat, static_cast<int>(r), Wt, inverse, h->status.p + 1);
-      } else {
-        auto k = chol_block_kernel<1>;
-        if (sm > 48 * 1024) RR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-        k<<<1, CHOL_THREADS, sm, s>>>(mat, static_cast<int>(r), Wt, inverse, h->status.p + 1);
-      }
-      RR_LAUNCH_CHECK();
-      return;
-    }
-    const size_t sm = chol_in_smem ? chol_smem : 0;
+    const int sm = chol_in_smem ? static_cast<int>(block_smem) : 0;
+    double* gb = chol_in_smem ? nullptr : gw;
     if (cplx) {
-      auto k = chol_small_kernel<2>;
-      if (sm > 48 * 1024) RR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
-      k<<<1, 32, sm, s>>>(mat, r, Wt, chol_in_smem ? nullptr : gw, inverse, h->status.p + 1);
+      auto k = chol_block_kernel<2>;
+      if (sm > 48 * 1024) RR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+      k<<<1, CHOL_THREADS, sm, s>>>(mat, static_cast<int>(r), Wt, inverse, h->status.p + 1, gb);
     } else {
-      auto k = chol_small_kernel<1>;
-      if (sm > 48 * 1024) RR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)));
-      k<<<1, 32, sm, s>>>(mat, r, Wt, chol_in_smem ? nullptr : gw, inverse, h->status.p + 1);
+      auto k = chol_block_kernel<1>;
+      if (sm > 48 * 1024) RR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+      k<<<1, CHOL_THREADS, sm, s>>>(mat, static_cast<int>(r), Wt, inverse, h->status.p + 1, gb);
     }
     RR_LAUNCH_CHECK();
   };

@@ -34,10 +34,11 @@ void fock_nonrel(rr_ri_store* h, const double* hc, const double* D, const double
 void projector_ct(rr_ri_store* h, const double* A, const double* Pe, const double* X, int64_t n, int64_t n_eff,
                   int64_t r, bool cplx, double* Ct, cudaStream_t s);
 void fock_x2c(rr_ri_store* h, const double* hc, const double* P, const double* S, const double* X, int64_t n_eff,
-              double* F, const rr_opts* o, const RelBuild* rb = nullptr);
+              double* F, const rr_opts* o, const RelBuild* rb = nullptr, const double* proj = nullptr,
+              int64_t proj_rank = 0);
 void fock_rkb(rr_ri_store* h, const double* hc, const double* v, int64_t n_rkb, const double* s_full,
               const double* x_full, int64_t n_eff, const double* P, double* F, const rr_opts* o,
-              const RelBuild* rb = nullptr);
+              const RelBuild* rb = nullptr, const double* proj = nullptr, int64_t proj_rank = 0);
 
 namespace {
 
@@ -110,40 +111,78 @@ __global__ void gershgorin_partial_kernel(const double* A, int64_t n, double* pa
   }
 }
 
-// X = (emax I - F) / (emax - emin): spectrum mapped into [0, 1], lowest states near 1.
+// SP2 kernels run on RED_CTAS CTAs, each on its chunk of the n x n matrix, and leave per-CTA
+// partials (Re tr X, ||X||_F^2) of the matrix they wrote; for Hermitian X, ||X||_F^2 = tr X^2, so
+// the next step has both traces without a separate pass over X^2.
 template <int PL>
-__global__ void sp2_init_kernel(double* X, const double* F, int64_t n, const double* b) {
-  const double emin = b[0], emax = b[1], inv = 1.0 / fmax(emax - emin, 1e-300);
-  for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < n * n;
-       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int64_t i = idx / n, j = idx % n;
-    X[idx * PL] = ((i == j ? emax : 0.0) - F[idx * PL]) * inv;
-    if (PL == 2) X[idx * PL + 1] = -F[idx * PL + 1] * inv;
+__device__ __forceinline__ void sp2_partials(double tr, double fro, double* red, double* part) {
+  tr = block_sum(tr, red);
+  fro = block_sum(fro, red);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = tr;
+    part[gridDim.x + blockIdx.x] = fro;
   }
 }
 
-// tr[0] = Re trace X, tr[1] = Re trace T (one CTA).
+// X = (emax I - F) / (emax - emin): spectrum mapped into [0, 1], lowest states near 1.
 template <int PL>
-__global__ void two_traces_kernel(const double* X, const double* T, int64_t n, double* tr) {
+__global__ void sp2_init_kernel(double* X, const double* F, int64_t n, const double* b, double* part) {
   __shared__ double red[32];
+  const double emin = b[0], emax = b[1], inv = 1.0 / fmax(emax - emin, 1e-300);
+  int64_t beg, end;
+  chunk_of(n * n, beg, end);
+  double tr = 0.0, fro = 0.0;
+  for (int64_t idx = beg + threadIdx.x; idx < end; idx += blockDim.x) {
+    const int64_t i = idx / n, j = idx % n;
+    const double re = ((i == j ? emax : 0.0) - F[idx * PL]) * inv;
+    X[idx * PL] = re;
+    fro += re * re;
+    if (i == j) tr += re;
+    if (PL == 2) {
+      const double im = -F[idx * PL + 1] * inv;
+      X[idx * PL + 1] = im;
+      fro += im * im;
+    }
+  }
+  sp2_partials<PL>(tr, fro, red, part);
+}
+
+// SP2 step (trace correcting): with t1 = tr X and t2 = tr X^2 from the partials `pin` of X,
+// X <- X^2 (= T) if that brings the trace closer to N, else 2X - X^2.  tr_out (written by CTA 0)
+// receives (t1, t2) for the host's convergence check; `pout` the partials of the new X.
+template <int PL>
+__global__ void sp2_step_kernel(double* X, const double* T, int64_t n, const double* pin, double* pout,
+                                double* tr_out, double N) {
+  __shared__ double red[32];
+  __shared__ int sq;
+  const int np = gridDim.x;  // the partials come from a launch of the same size
   double a = 0.0, b = 0.0;
-  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
-    a += X[(i * n + i) * PL];
-    b += T[(i * n + i) * PL];
+  for (int i = threadIdx.x; i < np; i += blockDim.x) {
+    a += pin[i];
+    b += pin[np + i];
   }
   a = block_sum(a, red);
   b = block_sum(b, red);
-  if (threadIdx.x == 0) { tr[0] = a; tr[1] = b; }
-}
-
-// SP2 step (trace correcting): X <- X^2 if that brings the trace closer to N, else 2X - X^2
-// (elementwise over `cnt` doubles, so it serves interleaved complex matrices as well).
-__global__ void sp2_update_kernel(double* X, const double* T, int64_t cnt, const double* tr, double N) {
-  const double trx = tr[0], trt = tr[1];
-  const bool square = fabs(trt - N) < fabs(2.0 * trx - trt - N);
-  for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < cnt;
-       idx += static_cast<int64_t>(gridDim.x) * blockDim.x)
-    X[idx] = square ? T[idx] : 2.0 * X[idx] - T[idx];
+  if (threadIdx.x == 0) {
+    sq = fabs(b - N) < fabs(2.0 * a - b - N) ? 1 : 0;
+    if (blockIdx.x == 0) { tr_out[0] = a; tr_out[1] = b; }
+  }
+  __syncthreads();
+  const bool square = sq != 0;
+  int64_t beg, end;
+  chunk_of(n * n, beg, end);
+  double tr = 0.0, fro = 0.0;
+  for (int64_t idx = beg + threadIdx.x; idx < end; idx += blockDim.x) {
+    const int64_t i = idx / n, j = idx % n;
+#pragma unroll
+    for (int q = 0; q < PL; ++q) {
+      const double x = square ? T[idx * PL + q] : 2.0 * X[idx * PL + q] - T[idx * PL + q];
+      X[idx * PL + q] = x;
+      fro += x * x;
+      if (q == 0 && i == j) tr += x;
+    }
+  }
+  sp2_partials<PL>(tr, fro, red, pout);
 }
 
 // Stage 1 of 1/2 Re Tr[P (h + F)]: part[b] = this CTA's share of sum_ij P_ij (h + F)_ji.
@@ -365,7 +404,121 @@ struct PhaseTimer {
   }
 };
 
+// ---- tight spectral bounds for SP2 (block Krylov Ritz values) ----
+
+// K[:, 0:m] (n rows, row pitch ldk) = deterministic pseudo-random numbers in [-1, 1) (splitmix64).
+template <int PL>
+__global__ void krylov_start_kernel(double* K, int64_t n, int ldk, int m) {
+  for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < n * m * PL;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t row = idx / (m * PL), c = idx % (m * PL);
+    uint64_t z = static_cast<uint64_t>(idx) * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    K[row * ldk * PL + c] = static_cast<double>(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+  }
+}
+
+// Columns c0 .. c0 + gridDim.x - 1 of K scaled to unit 2-norm (one CTA per column).
+template <int PL>
+__global__ void normalize_cols_kernel(double* K, int64_t n, int ldk, int c0) {
+  __shared__ double red[32];
+  __shared__ double scale;
+  const int c = c0 + blockIdx.x;
+  double s2 = 0.0;
+  for (int64_t r = threadIdx.x; r < n; r += blockDim.x)
+#pragma unroll
+    for (int q = 0; q < PL; ++q) {
+      const double v = K[(r * ldk + c) * PL + q];
+      s2 += v * v;
+    }
+  s2 = block_sum(s2, red);
+  if (threadIdx.x == 0) scale = s2 > 0.0 ? 1.0 / sqrt(s2) : 0.0;
+  __syncthreads();
+  for (int64_t r = threadIdx.x; r < n; r += blockDim.x)
+#pragma unroll
+    for (int q = 0; q < PL; ++q) K[(r * ldk + c) * PL + q] *= scale;
+}
+
+// b = [lo, hi] (the Gershgorin interval on entry) narrowed to the Ritz interval widened by 10% of
+// its spread on both sides, when the small eigenproblem succeeded.
+__global__ void ritz_bounds_kernel(const double* w, int k, const int* info, double* b) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double lo = w[0], hi = w[k - 1], spread = hi - lo;
+  if (*info != 0 || !(spread >= 0.0) || !isfinite(lo) || !isfinite(hi)) return;
+  const double m = 0.1 * spread + 1e-12 * fmax(fabs(lo), fabs(hi));
+  const double nlo = fmax(b[0], lo - m), nhi = fmin(b[1], hi + m);
+  if (nhi > nlo) { b[0] = nlo; b[1] = nhi; }
+}
+
 }  // namespace
+
+// Narrows the SP2 spectral interval b (device, [lo, hi], Gershgorin on entry) of the Hermitian n x n
+// F with the Ritz values of F on the block Krylov space [V, F V, F^2 V, F^3 V] (V: 8 fixed
+// pseudo-random vectors), widened by 10% of their spread: a generalized 32 x 32 eigenproblem
+// (K^dagger F K) y = theta (K^dagger K) y on the device (cuSOLVER).  Small matrices keep b.
+void ritz_bounds(rr_ri_store* h, const double* F, int64_t n, bool cplx, double* b, cudaStream_t s) {
+  constexpr int m = 8, q = 4, k = m * q;
+  if (n < 4 * k) return;
+  const int PL = cplx ? 2 : 1;
+  double *K, *FK, *T, *M, *w;
+  Arena ar(&h->solver_a);
+  ar.request(&K, n * k * PL);
+  ar.request(&FK, n * k * PL);
+  ar.request(&T, k * k * PL);
+  ar.request(&M, k * k * PL);
+  ar.request(&w, k);
+  ar.commit();
+  if (cplx) krylov_start_kernel<2><<<blocks_for(n * m * 2), 256, 0, s>>>(K, n, k, m);
+  else krylov_start_kernel<1><<<blocks_for(n * m), 256, 0, s>>>(K, n, k, m);
+  RR_LAUNCH_CHECK();
+  for (int j = 0; j < q; ++j) {
+    if (j > 0) {
+      GemmDesc g;
+      g.cplx = cplx;
+      g.M = n; g.N = m; g.K = n;
+      g.A = F; g.lda = n; g.B = K + (j - 1) * m * PL; g.ldb = k; g.C = K + j * m * PL; g.ldc = k;
+      gemm(g, s, h->work.p, static_cast<int64_t>(h->work.n));
+    }
+    if (cplx) normalize_cols_kernel<2><<<m, 256, 0, s>>>(K, n, k, j * m);
+    else normalize_cols_kernel<1><<<m, 256, 0, s>>>(K, n, k, j * m);
+    RR_LAUNCH_CHECK();
+  }
+  GemmDesc f;
+  f.cplx = cplx;
+  f.M = n; f.N = k; f.K = n; f.A = F; f.lda = n; f.B = K; f.ldb = k; f.C = FK; f.ldc = k;
+  gemm(f, s, h->work.p, static_cast<int64_t>(h->work.n));
+  GemmDesc t;
+  t.cplx = cplx;
+  t.M = k; t.N = k; t.K = n; t.A = K; t.lda = k; t.opA = Op::T; t.conjA = cplx; t.B = FK; t.ldb = k; t.C = T; t.ldc = k;
+  gemm(t, s, h->work.p, static_cast<int64_t>(h->work.n));
+  t.B = K; t.C = M;
+  t.mirror = 1;
+  gemm(t, s, h->work.p, static_cast<int64_t>(h->work.n));
+  auto& c = h->ctx;
+  RR_SOLVER(cusolverDnSetStream(c.solver, s));
+  c.solver_info.ensure(1);
+  int lwork = 0;
+  if (cplx) {
+    auto* tz = reinterpret_cast<cuDoubleComplex*>(T);
+    auto* mz = reinterpret_cast<cuDoubleComplex*>(M);
+    RR_SOLVER(cusolverDnZhegvd_bufferSize(c.solver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_NOVECTOR,
+                                          CUBLAS_FILL_MODE_UPPER, k, tz, k, mz, k, w, &lwork));
+    c.solver_work.ensure(2 * static_cast<size_t>(lwork) + 2);
+    RR_SOLVER(cusolverDnZhegvd(c.solver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_NOVECTOR, CUBLAS_FILL_MODE_UPPER, k,
+                               tz, k, mz, k, w, reinterpret_cast<cuDoubleComplex*>(c.solver_work.p), lwork,
+                               c.solver_info.p));
+  } else {
+    RR_SOLVER(cusolverDnDsygvd_bufferSize(c.solver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_NOVECTOR,
+                                          CUBLAS_FILL_MODE_UPPER, k, T, k, M, k, w, &lwork));
+    c.solver_work.ensure(static_cast<size_t>(lwork) + 1);
+    RR_SOLVER(cusolverDnDsygvd(c.solver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_NOVECTOR, CUBLAS_FILL_MODE_UPPER, k, T,
+                               k, M, k, w, c.solver_work.p, lwork, c.solver_info.p));
+  }
+  ritz_bounds_kernel<<<1, 32, 0, s>>>(w, k, c.solver_info.p, b);
+  RR_LAUNCH_CHECK();
+}
 
 // SP2 purification: projector (n x n, into Pi) onto the lowest `nocc` eigenvectors of the symmetric
 // (Hermitian when cplx, interleaved) F (n x n).  T is scratch (n x n).  Host checks every 4 steps;
@@ -373,8 +526,8 @@ struct PhaseTimer {
 void sp2_projector(rr_ri_store* h, const double* F, int64_t n, int64_t nocc, double* Pi, double* T, double* scal,
                    cudaStream_t s, bool cplx) {
   const int PL = cplx ? 2 : 1;
-  h->work.ensure(static_cast<size_t>(std::max<int64_t>(static_cast<int64_t>(h->work.n), 8 * n * n * PL)));
-  double* part = h->work.p;  // free until the first GEMM below (same stream)
+  h->work.ensure(static_cast<size_t>(std::max<int64_t>(static_cast<int64_t>(h->work.n), 8 * n * n * PL + 6 * RED_CTAS)));
+  double* part = h->work.p;  // Gershgorin partials, then the SP2 trace partials
   const int gcta = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(RED_CTAS, (n + 7) / 8)));
   if (cplx) gershgorin_partial_kernel<2><<<gcta, 256, 0, s>>>(F, n, part);
   else gershgorin_partial_kernel<1><<<gcta, 256, 0, s>>>(F, n, part);
@@ -383,21 +536,32 @@ void sp2_projector(rr_ri_store* h, const double* F, int64_t n, int64_t nocc, dou
   RR_LAUNCH_CHECK();
   reduce_partials_kernel<2><<<1, 256, 0, s>>>(part + gcta, gcta, 1.0, scal + 1);
   RR_LAUNCH_CHECK();
-  if (cplx) sp2_init_kernel<2><<<blocks_for(n * n), 256, 0, s>>>(Pi, F, n, scal);
-  else sp2_init_kernel<1><<<blocks_for(n * n), 256, 0, s>>>(Pi, F, n, scal);
-  RR_LAUNCH_CHECK();
+  // Gershgorin interval kept in scal[4..5]; the Ritz interval (tighter: fewer SP2 steps) is tried first
+  RR_CUDA(cudaMemcpyAsync(scal + 4, scal, 2 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  ritz_bounds(h, F, n, cplx, scal, s);
+  // ping-pong partials of X after the Gershgorin partials (the GEMM's split-K scratch follows them)
+  double* sp_part[2] = {part + 2 * RED_CTAS, part + 4 * RED_CTAS};
+  auto init = [&] {
+    if (cplx) sp2_init_kernel<2><<<RED_CTAS, 256, 0, s>>>(Pi, F, n, scal, sp_part[0]);
+    else sp2_init_kernel<1><<<RED_CTAS, 256, 0, s>>>(Pi, F, n, scal, sp_part[0]);
+    RR_LAUNCH_CHECK();
+  };
+  init();
   GemmDesc g;
   g.cplx = cplx;
   g.M = n; g.N = n; g.K = n;
   g.A = Pi; g.lda = n; g.B = Pi; g.ldb = n; g.C = T; g.ldc = n;
   g.mirror = 1;  // X is Hermitian, so is X^2: upper tiles, the rest mirrored
   const double N = static_cast<double>(nocc);
-  for (int it = 0; it < 120; ++it) {
-    gemm(g, s, h->work.p, static_cast<int64_t>(h->work.n));
-    if (cplx) two_traces_kernel<2><<<1, 512, 0, s>>>(Pi, T, n, scal + 2);
-    else two_traces_kernel<1><<<1, 512, 0, s>>>(Pi, T, n, scal + 2);
-    RR_LAUNCH_CHECK();
-    sp2_update_kernel<<<blocks_for(n * n * PL), 256, 0, s>>>(Pi, T, n * n * PL, scal + 2, N);
+  double* gw = part + 6 * RED_CTAS;  // split-K scratch of the X^2 products
+  const int64_t gcap = static_cast<int64_t>(h->work.n) - 6 * RED_CTAS;
+  bool gershgorin = false;
+  for (int it = 0, step = 0; step < 120; ++it, ++step) {
+    gemm(g, s, gw, gcap);
+    if (cplx)
+      sp2_step_kernel<2><<<RED_CTAS, 256, 0, s>>>(Pi, T, n, sp_part[it & 1], sp_part[(it + 1) & 1], scal + 2, N);
+    else
+      sp2_step_kernel<1><<<RED_CTAS, 256, 0, s>>>(Pi, T, n, sp_part[it & 1], sp_part[(it + 1) & 1], scal + 2, N);
     RR_LAUNCH_CHECK();
     if (it % 4 == 3) {
       double tr[2];
@@ -405,6 +569,15 @@ void sp2_projector(rr_ri_store* h, const double* F, int64_t n, int64_t nocc, dou
       RR_CUDA(cudaStreamSynchronize(s));
       // idempotency measure of the pre-update X: |tr X - tr X^2| (sum of lambda (1 - lambda))
       if (std::fabs(tr[0] - tr[1]) < 1e-11 * std::max<double>(1.0, N) && std::fabs(tr[0] - N) < 1e-6) return;
+      // With every eigenvalue of X in [0, 1], tr X^2 <= tr X; otherwise the Ritz interval missed part
+      // of the spectrum: start again from the Gershgorin interval.
+      if (!gershgorin && (tr[1] > tr[0] + 1e-9 * std::max<double>(1.0, N) || step + 1 >= 60)) {
+        gershgorin = true;
+        RR_CUDA(cudaMemcpyAsync(scal, scal + 4, 2 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        init();
+        it = -1;
+        step = -1;
+      }
     }
   }
   throw Error(RR_ERR_SOLVER, "SCF: density purification did not converge (no gap at the Fermi level?)");
@@ -513,12 +686,14 @@ void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff
     gemm(a, s, h->work.p, static_cast<int64_t>(h->work.n));
     a.M = n_eff; a.N = n_eff; a.K = n; a.A = Xd; a.lda = n_eff; a.opA = Op::T; a.B = tmp; a.ldb = n_eff; a.C = Fo;
     a.ldc = n_eff;
+    a.mirror = 1;  // X^T F X is symmetric
     gemm(a, s, h->work.p, static_cast<int64_t>(h->work.n));
     sp2_projector(h, Fo, n_eff, nocc, Pi, T2, scal + 8, s, false);
     projector_ct(h, Pi, nullptr, Xd, n, n_eff, nocc, false, Ct, s);
     GemmDesc dp;
     dp.M = n; dp.N = n; dp.K = nocc; dp.A = Ct; dp.lda = n; dp.opA = Op::T; dp.B = Ct; dp.ldb = n; dp.C = Pn; dp.ldc = n;
     dp.alpha = 2.0;
+    dp.mirror = 1;  // 2 C C^T is symmetric
     gemm(dp, s, h->work.p, static_cast<int64_t>(h->work.n));
     maxdiff_partial_kernel<1><<<RED_CTAS, 256, 0, s>>>(Pn, P, n2, red);
     RR_LAUNCH_CHECK();
@@ -635,9 +810,16 @@ void scf_rel(rr_ri_store* h, int kind, const double* hc, const double* v_total, 
   // build of the final density whose energy is reported.
   bool mixed = so->precision == RR_PREC_MIXED, reseed = false, reseeded = false;
   h->rel_r = -1;
+  // After the first iteration the density is X Pi X^dagger (Kramers-projected) with Pi the SP2
+  // (window) projector, so the builds take the occupied spinors from Pi; linear mixing makes the
+  // density non-idempotent and keeps the recovery from P.
+  const bool mixing_on = !use_diis && so->mixing > 0.0 && so->mixing != 1.0;
+  bool have_proj = false;
   auto build = [&](const RelBuild* rb) {
-    if (dhf) fock_rkb(h, hd, vd, n, Sd, Xd, n_eff, P, F, &od, rb);
-    else fock_x2c(h, hd, P, Sd, Xd, n_eff, F, &od, rb);
+    const double* pj = have_proj ? Pi : nullptr;
+    const int64_t pr = have_proj ? n_electrons : 0;
+    if (dhf) fock_rkb(h, hd, vd, n, Sd, Xd, n_eff, P, F, &od, rb, pj, pr);
+    else fock_x2c(h, hd, P, Sd, Xd, n_eff, F, &od, rb, pj, pr);
   };
   auto energy_of_f = [&] {
     energy_partial_kernel<2><<<RED_CTAS, 256, 0, s>>>(P, hd, F, n, red);
@@ -684,6 +866,7 @@ void scf_rel(rr_ri_store* h, int kind, const double* hc, const double* v_total, 
     gemm(a, s, wk(), wcap());
     a.M = n_eff; a.N = n_eff; a.K = n; a.A = Xd; a.lda = n_eff; a.opA = Op::T; a.conjA = true; a.B = tmp;
     a.ldb = n_eff; a.C = Fo; a.ldc = n_eff;
+    a.mirror = 1;  // X^dagger F X is Hermitian
     gemm(a, s, wk(), wcap());
     // window projector in the orthonormal basis
     sp2_projector(h, Fo, n_eff, nlo + n_electrons, Pi, T2, scal + 8, s, true);
@@ -698,6 +881,7 @@ void scf_rel(rr_ri_store* h, int kind, const double* hc, const double* v_total, 
     gemm(b, s, wk(), wcap());
     b.M = n; b.N = n; b.K = n_eff; b.A = tmp; b.lda = n_eff; b.B = Xd; b.ldb = n_eff; b.opB = Op::T; b.conjB = true;
     b.C = restrict_active ? e : Pn; b.ldc = n;
+    b.mirror = 1;  // X Pi X^dagger is Hermitian
     gemm(b, s, wk(), wcap());
     if (restrict_active) {
       kramers_even_kernel<<<blocks_for(n2), 256, 0, s>>>(Pn, e, n, nb);
@@ -719,7 +903,10 @@ void scf_rel(rr_ri_store* h, int kind, const double* hc, const double* v_total, 
     prev = energy;
     if (conv) {
       if (mixed) {
-        // last iteration in FP64: the FP64 Fock matrix of the converged density and its energy
+        // last iteration in FP64: the FP64 Fock matrix of the newest density and its energy
+        if (mixing_on) axpby(Pn, P, 1.0 - so->mixing, so->mixing, c2, s);
+        have_proj = !mixing_on;
+        std::swap(P, Pn);
         build(nullptr);
         ++n_fp64;
         energy_of_f();
@@ -736,7 +923,8 @@ void scf_rel(rr_ri_store* h, int kind, const double* hc, const double* v_total, 
       break;
     }
     if (mixed && !reseeded && so->mixed_switch > 0.0 && it > 1 && dE < so->mixed_switch) reseed = reseeded = true;
-    if (!use_diis && so->mixing > 0.0 && so->mixing != 1.0) axpby(Pn, P, 1.0 - so->mixing, so->mixing, c2, s);
+    if (mixing_on) axpby(Pn, P, 1.0 - so->mixing, so->mixing, c2, s);
+    have_proj = !mixing_on;
     std::swap(P, Pn);
   }
   if (it > so->max_iterations) it = so->max_iterations;

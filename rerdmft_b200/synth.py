@@ -161,7 +161,7 @@ def x2c_system(nl: int, naux: int, n_electrons: int, seed: int, b_scale: float |
 
 
 def rkb_system(nl: int, ns: int, naux: int, n_electrons: int, seed: int, b_scale: float | None = None,
-               box: float = 8.0, small_scale: float = 0.05) -> dict:
+               box: float = 8.0, small_scale: float = 0.05, gap: float = 1.5) -> dict:
     """4-component RKB inputs.  RKB basis [L-alpha, L-beta, S-alpha, S-beta] of dimension
     n_rkb = 4 nl; UKB basis of dimension n_ukb = 2 nl + 2 ns; v_total (n_ukb x n_rkb) embeds
     the large block as the identity and each RKB small function as a combination of UKB small
@@ -194,7 +194,7 @@ def rkb_system(nl: int, ns: int, naux: int, n_electrons: int, seed: int, b_scale
     npair_neg = npair // 2
     npair_occ = n_electrons // 2
     e = np.concatenate([-60.0 - 5.0 * rng.random(npair_neg), -2.0 + 0.8 * rng.random(npair_occ),
-                        0.3 + 2.5 * rng.random(npair - npair_neg - npair_occ)])
+                        gap - 1.2 + 2.5 * rng.random(npair - npair_neg - npair_occ)])
     h_ortho = _kramers_spectrum(n_eff, 4, e, rng)
     sx = s_full @ x_full
     h_rkb = sx @ h_ortho @ sx.conj().T
