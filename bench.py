@@ -463,6 +463,81 @@ def run_reference(args):
     print(json.dumps(base))
 
 
+def run_case(args):
+    """Single workloads for profiling and kernel timing (one GPU, device-resident inputs, CUDA events):
+    headline      the FP64 nonrel Fock build of the headline workload only (no extra blocks);
+    mixed_exchange  the split-BF16 tcgen05 exchange K = sum_P (Ct B^P)^T (Ct B^P) at n=400, naux=1600,
+                  nocc=40 (rr_ri_jk_occupied, RR_PREC_MIXED; J stays FP64);
+    rkb_mixed     the 4c RKB Fock build of the Kramers-restricted DHF shapes with the split-BF16 exchange,
+                  full then incremental (nl=200, ns=600, naux=1000, 40 spinors)."""
+    import ctypes
+
+    import torch
+
+    from rerdmft_b200 import _lib as L
+    from rerdmft_b200 import ri, synth
+
+    torch.cuda.set_stream(torch.cuda.Stream())  # events and library calls on one real stream
+    lib = L.lib()
+    stream = torch.cuda.current_stream().cuda_stream
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(step, steps, warmup):
+        for _ in range(warmup):
+            step()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    out = dict(case=args.case, steps=args.steps, warmup=args.warmup)
+    if args.case in ("headline", "mixed_exchange"):
+        inp = make_inputs()
+        dev = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in inp.items()}
+        store = ri.RiNonRelEriSource(N_AO, dev["B"], dev["X"], dev["S"]).store
+        if args.case == "headline":
+            F = torch.empty((N_AO, N_AO), dtype=torch.float64, device="cuda")
+            o = L.opts(L.RR_MEM_DEVICE, stream=stream, sync=0)
+            ms = timed(lambda: L.check(lib.rr_ri_fock_nonrel(store.handle, dev["h"].data_ptr(), dev["D"].data_ptr(),
+                                                             dev["S"].data_ptr(), dev["X"].data_ptr(), N_AO,
+                                                             F.data_ptr(), ctypes.byref(o))), args.steps, args.warmup)
+            out.update(workload=f"FP64 nonrel Fock build n={N_AO} naux={N_AUX} nocc={N_OCC}", ms_per_build=ms)
+        else:
+            J = torch.empty((N_AO, N_AO), dtype=torch.float64, device="cuda")
+            K = torch.empty_like(J)
+            C = dev["C"].contiguous()
+            o = L.opts(L.RR_MEM_DEVICE, precision=L.RR_PREC_MIXED, stream=stream, sync=0)
+            ms = timed(lambda: L.check(lib.rr_ri_jk_occupied(store.handle, C.data_ptr(), N_OCC, J.data_ptr(),
+                                                             K.data_ptr(), ctypes.byref(o))), args.steps, args.warmup)
+            out.update(workload=f"split-BF16 J/K n={N_AO} naux={N_AUX} nocc={N_OCC}", ms_per_call=ms)
+        store.sync()
+    elif args.case == "rkb_mixed":
+        s = synth.rkb_system(NL4, NS4, NAUX4, 2 * (NOCC4 // 2), seed=SEED + 11, box=20.0)
+        dev = {k: torch.from_numpy(np.ascontiguousarray(s[k])).cuda()
+               for k in ("B_LL", "B_SS", "v_total", "s_full", "x_full", "h", "P0")}
+        store = ri.RiDirectEriSource(NL4, NS4, dev["B_LL"], dev["B_SS"], dev["v_total"], dev["s_full"],
+                                     dev["x_full"]).store
+        n_rkb = s["n_rkb"]
+        F = torch.empty((n_rkb, n_rkb), dtype=torch.complex128, device="cuda")
+        x = dev["x_full"]
+
+        def step(incremental):
+            o = L.opts(L.RR_MEM_DEVICE, precision=L.RR_PREC_MIXED, stream=stream, sync=0, incremental=incremental)
+            L.check(lib.rr_ri_fock_rkb(store.handle, dev["h"].data_ptr(), dev["v_total"].data_ptr(), n_rkb,
+                                       dev["s_full"].data_ptr(), x.data_ptr(), x.shape[1], dev["P0"].data_ptr(),
+                                       F.data_ptr(), ctypes.byref(o)))
+
+        full = timed(lambda: step(0), args.steps, args.warmup)
+        incr = timed(lambda: step(1), args.steps, args.warmup)
+        out.update(workload=f"mixed rkbFockMatrix nl={NL4} ns={NS4} naux={NAUX4} nocc={NOCC4}", ms_full=full,
+                   ms_incremental=incr)
+        store.sync()
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -470,10 +545,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--case", default=None, choices=["headline", "mixed_exchange", "rkb_mixed"],
+                    help="run one workload for profiling instead of the bench line")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         return run_reference(args)
+    if args.case:
+        return run_case(args)
 
     import torch
 
@@ -482,6 +561,9 @@ def main():
 
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
+    # A real stream: the library runs on the stream it is given, and the CUDA events below are recorded
+    # on the same one (torch's legacy default stream has handle 0, which the library reads as "its own").
+    torch.cuda.set_stream(torch.cuda.Stream())
     pg = None
     if ws > 1:
         import datetime
