@@ -244,7 +244,7 @@ DHF_GAP, DHF_B = 0.4, 3.0
 
 def rel_scf_times(want_cpu: bool, rkb_ref_build_s=None):
     """Time to an energy change below 1e-8 Ha on one GPU for X2C-HF and 4c-DHF: the FP64 loop against
-    the mixed loop (incremental split-BF16 exchange, one FP64 build of the final density), best of two
+    the mixed loop (incremental split-BF16 exchange, one FP64 build of the final density), best of three
     runs each, with per-phase device times; the reference's CPU time is one of its own Fock builds of the
     same system times the FP64 iteration count (its loop spends nearly all its time in those builds)."""
     from rerdmft_b200 import _lib as L
@@ -256,7 +256,7 @@ def rel_scf_times(want_cpu: bool, rkb_ref_build_s=None):
         for prec in ("fp64", "mixed"):
             run(prec)  # warm-up (builds the split-BF16 operands once)
             best = None
-            for _ in range(2):
+            for _ in range(3):
                 r = run(prec)
                 if best is None or r["seconds"] < best["seconds"]:
                     best = r
