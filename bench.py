@@ -200,8 +200,9 @@ def x2c_batch_block(want_cpu: bool, count: int = 64, workers: int = 16):
 
 
 def scf_times(torch, want_cpu: bool):
-    """Time to an energy change below 1e-8 Ha on one GPU: FP64 loop vs mixed loop (split-BF16
-    exchange until |dE| < 1e-5, then FP64), plus the reference's own SCF loop on the host cores."""
+    """Time to an energy change below 1e-8 Ha on one GPU: FP64 loop vs mixed loop (incremental
+    split-BF16 exchange, one FP64 build of the final density), plus the reference's own SCF loop on the
+    host cores."""
     from rerdmft_b200 import ri, scf
 
     s = make_scf_system()

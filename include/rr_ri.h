@@ -152,7 +152,8 @@ typedef struct rr_scf_opts {
   double density_tolerance;   /* DENSITY_TOLERANCE (1e-6) */
   int32_t kramers_restricted; /* X2C / 4c: project densities onto their time-reversal-even part */
   int32_t precision;          /* RR_PREC_FP64 or RR_PREC_MIXED (split-BF16 exchange, FP64 for the last iterations) */
-  double mixed_switch;        /* RR_PREC_MIXED: switch to FP64 builds once |dE| < mixed_switch */
+  double mixed_switch;        /* RR_PREC_MIXED: > 0 re-seeds the accumulated exchange once with an FP64
+                                 build when |dE| < mixed_switch (0: never) */
   double mixing;              /* without DIIS (diis_size < 2): next density = mixing P_new + (1 - mixing) P,
                                  the reference's linear mixing; 0 is taken as 1 */
 } rr_scf_opts;
@@ -175,7 +176,10 @@ typedef struct rr_scf_result {
  * the GPU).  Replaces runNonRelativisticHartreeFock(RiNonRelEriSource, ...),
  * src/NON_REL/NonRelHartreeFock.cpp:117-198/219 (nuclear repulsion is the caller's; DIIS replaces
  * the linear mixing as in the reference).  energy_history (optional) receives one electronic
- * energy per iteration (max_iterations doubles); P_out the density of the last iteration. */
+ * energy per iteration (max_iterations doubles); P_out the density of the last iteration.
+ * RR_PREC_MIXED: after the first (FP64) build, a full split-BF16 exchange, then builds adding the
+ * split-BF16 exchange of the density change (J stays FP64); mixed_switch as for rr_scf_run_x2c; after
+ * convergence one FP64 build of the final density gives the reported energy. */
 int rr_scf_run_nonrel(rr_ri_handle h, const double* h_core, const double* X, int64_t n_eff, const double* S,
                       const double* P0, int32_t n_electrons, const rr_scf_opts* scf, rr_scf_result* result,
                       double* P_out, double* energy_history, const rr_opts* opts);

@@ -131,9 +131,9 @@ void two_electron_rel(rr_ri_store* h, const Flavours& fl, int64_t ntot, const do
   ar.commit();
   coulomb_async_multi(h, ntens, Dp, J, s);
   if (rb) {
-    h->rel_k.ensure(static_cast<size_t>(2 * ntot * ntot));
+    h->inc_k.ensure(static_cast<size_t>(2 * ntot * ntot));
     if (rb->mixed) {
-      const bool incr = rb->incremental && h->rel_r == r && h->rel_ntot == ntot && r > 0;
+      const bool incr = rb->incremental && h->inc_r == r && h->inc_ld == ntot && r > 0;
       ExFlavours ef;
       ef.nf = fl.nf;
       for (int f = 0; f < fl.nf; ++f) {
@@ -143,13 +143,13 @@ void two_electron_rel(rr_ri_store* h, const Flavours& fl, int64_t ntot, const do
       }
       for (int t = 0; t < ntens; ++t) mixed_prepare(h->mixed[t], h->B[t].p, h->pitch[t], nt[t], naux, s);
       prof_mark(h, 2, s);
-      mixed_exchange_general(h->mixed, h->mscr, ef, naux, Ct, incr ? h->rel_ct.p : nullptr, ntot, r, true, h->rel_k.p,
+      mixed_exchange_general(h->mixed, h->mscr, ef, naux, Ct, incr ? h->inc_ct.p : nullptr, ntot, r, true, h->inc_k.p,
                              ntot, incr, h->status.p, s);
       prof_mark(h, 3, s);
     }
   }
   const bool fp64_k = !rb || !rb->mixed;
-  double* Gk = rb ? h->rel_k.p : G;  // where the FP64 blocks land
+  double* Gk = rb ? h->inc_k.p : G;  // where the FP64 blocks land
   if (fp64_k) RR_CUDA(cudaMemsetAsync(Gk, 0, sizeof(double) * 2 * ntot * ntot, s));
   // T planes: flavour f occupies [Re (naux*r*fs) | Im (naux*r*fs)]
   std::array<double*, 4> T{};
@@ -206,17 +206,17 @@ void two_electron_rel(rr_ri_store* h, const Flavours& fl, int64_t ntot, const do
   if (fp64_k) prof_mark(h, 3, s);
   if (rb) {
     // G = J - K from the accumulator; remember c_t for the next incremental build
-    neg_copy_kernel<<<blocks_for(2 * ntot * ntot), 256, 0, s>>>(G, h->rel_k.p, 2 * ntot * ntot);
+    neg_copy_kernel<<<blocks_for(2 * ntot * ntot), 256, 0, s>>>(G, h->inc_k.p, 2 * ntot * ntot);
     RR_LAUNCH_CHECK();
     RR_CUDA(cudaStreamWaitEvent(s, h->ctx.join, 0));
     for (int f = 0; f < fl.nf; ++f) {
       add_j_block_kernel<<<blocks_for(fl.fs[f] * fl.fs[f]), 256, 0, s>>>(G, ntot, fl.off[f], fl.fs[f], J[fl.tens[f]]);
       RR_LAUNCH_CHECK();
     }
-    h->rel_ct.ensure(static_cast<size_t>(std::max<int64_t>(2 * r * ntot, 1)));
-    if (r > 0) RR_CUDA(cudaMemcpyAsync(h->rel_ct.p, Ct, sizeof(double) * 2 * r * ntot, cudaMemcpyDeviceToDevice, s));
-    h->rel_r = r;
-    h->rel_ntot = ntot;
+    h->inc_ct.ensure(static_cast<size_t>(std::max<int64_t>(2 * r * ntot, 1)));
+    if (r > 0) RR_CUDA(cudaMemcpyAsync(h->inc_ct.p, Ct, sizeof(double) * 2 * r * ntot, cudaMemcpyDeviceToDevice, s));
+    h->inc_r = r;
+    h->inc_ld = ntot;
   }
 }
 

@@ -25,10 +25,11 @@ struct rr_ri_store {
   // Split-BF16 copies of B[t] for RR_PREC_MIXED (built on first use) and their call scratch.
   rr::MixedOperands mixed[2];
   rr::MixedScratch mscr;
-  // Incremental relativistic builds: the exchange accumulated so far (interleaved complex
-  // ntot x ntot) and the c_t it belongs to (r x ntot).
-  rr::DevBuf<double> rel_k, rel_ct;
-  int64_t rel_r = -1, rel_ntot = 0;
+  // Incremental (density-change) builds of the mixed SCF loops: the exchange accumulated so far
+  // (n x n real, or ntot x ntot interleaved complex) and the c_t it belongs to (inc_r rows of
+  // inc_ld entries).
+  rr::DevBuf<double> inc_k, inc_ct;
+  int64_t inc_r = -1, inc_ld = 0;
   // Profiling events: 0 start, 1 recovery done, 2 half-transform done, 3 exchange done, 4 end
   // (main stream); 5 J start, 6 J end (side stream).
   bool profiling = false;
@@ -61,11 +62,11 @@ struct Arena {
 };
 
 // How a relativistic Fock build forms its exchange.  nullptr: FP64, straight into G.  Otherwise the
-// exchange goes through the handle's accumulator (rel_k), G = J - rel_k:
+// exchange goes through the handle's accumulator (inc_k), G = J - inc_k:
 //   mixed:           split-BF16 exchange on tcgen05; with `incremental` (and a previous build of the
-//                    same rank) only the exchange of c_t - c_t(previous) is added to rel_k, so the
+//                    same rank) only the exchange of c_t - c_t(previous) is added to inc_k, so the
 //                    rounding error scales with the density change;
-//   otherwise:       FP64 exchange that (re)seeds rel_k.
+//   otherwise:       FP64 exchange that (re)seeds inc_k.
 struct RelBuild {
   bool mixed = false;
   bool incremental = false;

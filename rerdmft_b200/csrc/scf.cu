@@ -12,9 +12,9 @@
 // The first iteration builds F from the caller's start density through the drop-in Fock build
 // (occupied recovery included); later iterations reuse the loop's own C_occ.
 //
-// Mixed precision (RR_PREC_MIXED): iterations run with the split-BF16 exchange until |dE| falls
-// below `mixed_switch`, then the loop switches to FP64 builds for the remaining iterations, so the
-// converged energy is that of the FP64 Fock matrix.
+// Mixed precision (RR_PREC_MIXED): an incremental split-BF16 exchange (the exchange of the change
+// of the occupied orbitals is added to the previous one, so the rounding error follows the density
+// change), J in FP64, and one FP64 build of the converged density for the reported energy.
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -623,8 +623,13 @@ void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff
   copy_in(Sd, S, n2, host, s);
   copy_in_padded(P, pitch, P0, n2, host, s);
   RR_CUDA(cudaMemsetAsync(Pn + n2, 0, sizeof(double) * (pitch - n2), s));
-  const bool mixed_requested = so->precision == RR_PREC_MIXED;
-  bool mixed = mixed_requested;
+  // Mixed precision: after the first (FP64, drop-in) build, a full split-BF16 exchange, then builds
+  // that add the split-BF16 exchange of the change of c_t (its error shrinks with the density
+  // change), re-seeded once by an FP64 exchange when |dE| < mixed_switch; once converged, one FP64
+  // build of the newest density gives the reported energy.
+  const bool mixed = so->precision == RR_PREC_MIXED;
+  bool reseed = false, reseeded = false;
+  h->inc_r = -1;
   DeviceDiis diis;
   const bool use_diis = so->diis_size >= 2;
   diis.init(use_diis ? so->diis_size : 0, n2);
@@ -647,12 +652,30 @@ void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff
       fock_nonrel(h, hd, P, Sd, Xd, n_eff, F, &od);
       ++n_fp64;
     } else if (mixed) {
-      mixed_prepare(h->mixed[0], h->B[0].p, h->pitch[0], n, h->naux, s);
-      mixed_exchange(h->mixed[0], h->mscr, Ct, n, nocc, K, h->status.p, s);
-      coulomb_after_ht(h, P, Ct, 0, J, nullptr, 0, s);
+      // the exchange accumulates in h->inc_k: a full split-BF16 exchange first, then the split-BF16
+      // exchange of the change of c_t (or, once, an FP64 re-seed); J stays FP64
+      h->inc_k.ensure(static_cast<size_t>(n2));
+      if (reseed) {
+        exchange_nonrel(h, Ct, n, false, nocc, h->inc_k.p, s, P, J);
+        ++n_fp64;
+      } else {
+        mixed_prepare(h->mixed[0], h->B[0].p, h->pitch[0], n, h->naux, s);
+        const bool incr = h->inc_r == nocc && h->inc_ld == n;
+        ExFlavours fl;
+        fl.nf = 1;
+        fl.fs[0] = n;
+        mixed_exchange_general(h->mixed, h->mscr, fl, h->naux, Ct, incr ? h->inc_ct.p : nullptr, n, nocc, false,
+                               h->inc_k.p, n, incr, h->status.p, s);
+        coulomb_after_ht(h, P, Ct, 0, J, nullptr, 0, s);
+        ++n_mixed;
+      }
+      reseed = false;
+      h->inc_ct.ensure(static_cast<size_t>(std::max<int64_t>(nocc * n, 1)));
+      RR_CUDA(cudaMemcpyAsync(h->inc_ct.p, Ct, sizeof(double) * nocc * n, cudaMemcpyDeviceToDevice, s));
+      h->inc_r = nocc;
+      h->inc_ld = n;
       coulomb_join(h, s);
-      fock_combine(F, hd, J, K, n2, s);
-      ++n_mixed;
+      fock_combine(F, hd, J, h->inc_k.p, n2, s);
     } else {
       exchange_nonrel(h, Ct, n, false, nocc, K, s, P, J);
       coulomb_join(h, s);
@@ -709,12 +732,34 @@ void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff
     res->electronic_energy = energy;
     const bool conv = it > 1 && (dP < so->density_tolerance || dE < so->energy_tolerance);
     prev = energy;
-    if (conv && !mixed) {
+    const bool mixing_on = !use_diis && so->mixing > 0.0 && so->mixing != 1.0;
+    if (conv) {
+      if (mixed) {
+        // last iteration in FP64: the FP64 Fock matrix of the newest density and its energy
+        if (mixing_on) axpby(Pn, P, 1.0 - so->mixing, so->mixing, n2, s);
+        std::swap(P, Pn);
+        exchange_nonrel(h, Ct, n, false, nocc, K, s, P, J);
+        coulomb_join(h, s);
+        fock_combine(F, hd, J, K, n2, s);
+        ++n_fp64;
+        energy_partial_kernel<1><<<RED_CTAS, 256, 0, s>>>(P, hd, F, n, red);
+        RR_LAUNCH_CHECK();
+        reduce_partials_kernel<0><<<1, 256, 0, s>>>(red, RED_CTAS, 0.5, scal);
+        RR_LAUNCH_CHECK();
+        double ev = 0.0;
+        RR_CUDA(cudaMemcpyAsync(&ev, scal, sizeof(double), cudaMemcpyDeviceToHost, s));
+        RR_CUDA(cudaStreamSynchronize(s));
+        res->electronic_energy = ev;
+        if (it < so->max_iterations) {
+          ++it;
+          if (hist) hist[it - 1] = ev;
+        }
+      }
       converged = true;
       break;
     }
-    if (mixed && it > 1 && (dE < so->mixed_switch || conv)) mixed = false;  // finish in FP64
-    if (!use_diis && so->mixing > 0.0 && so->mixing != 1.0) {
+    if (mixed && !reseeded && so->mixed_switch > 0.0 && it > 1 && dE < so->mixed_switch) reseed = reseeded = true;
+    if (mixing_on) {
       // linear mixing: only the density of the next build changes (NonRelHartreeFock.cpp:185-195)
       axpby(Pn, P, 1.0 - so->mixing, so->mixing, n2, s);
     }
@@ -809,7 +854,7 @@ void scf_rel(rr_ri_store* h, int kind, const double* hc, const double* v_total, 
   // once by an FP64 build when |dE| < mixed_switch; once converged, the last iteration is an FP64
   // build of the final density whose energy is reported.
   bool mixed = so->precision == RR_PREC_MIXED, reseed = false, reseeded = false;
-  h->rel_r = -1;
+  h->inc_r = -1;
   // After the first iteration the density is X Pi X^dagger (Kramers-projected) with Pi the SP2
   // (window) projector, so the builds take the occupied spinors from Pi; linear mixing makes the
   // density non-idempotent and keeps the recovery from P.

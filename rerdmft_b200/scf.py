@@ -36,9 +36,11 @@ def _result(res, P, hist):
 def runNonRelativisticHartreeFock(eri: RiNonRelEriSource, h_core, x_large, initial_density, n_electrons: int,
                                   diis_size: int = 5, max_iterations: int = 100, energy_tolerance: float = 1e-8,
                                   density_tolerance: float = 1e-6, precision: str = "fp64",
-                                  mixed_switch: float = 1e-5) -> dict:
+                                  mixed_switch: float = 0.0) -> dict:
     """RHF SCF on the GPU; returns energy (electronic), iterations, converged, density P, the
-    per-iteration energy history, wall seconds and the mixed / FP64 build counts."""
+    per-iteration energy history, wall seconds and the mixed / FP64 build counts.  precision="mixed":
+    FP64 first build, then incremental split-BF16 exchange, one FP64 build of the final density;
+    mixed_switch > 0 re-seeds the accumulated exchange once in FP64 when |dE| < mixed_switch."""
     n = eri.nl
     h = _host(h_core, np.float64)
     X = _host(x_large, np.float64)

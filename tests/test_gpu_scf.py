@@ -41,10 +41,14 @@ def test_nonrel_vs_oracle(n, naux, nocc, seed):
 def test_nonrel_mixed_reaches_fp64_energy(n, naux, nocc, seed):
     s = synth.nonrel_system(n, naux, nocc, seed=seed)
     r64 = _run(s)
-    rm = _run(s, precision="mixed", mixed_switch=1e-5)
-    assert r64["converged"] and rm["converged"]
-    assert rm["mixed_iterations"] >= 1 and rm["fp64_iterations"] >= 1
-    assert abs(rm["energy"] - r64["energy"]) <= 1e-8
+    for switch in (0.0, 1e-5):  # incremental only / one FP64 re-seed of the accumulated exchange
+        rm = _run(s, precision="mixed", mixed_switch=switch)
+        assert r64["converged"] and rm["converged"]
+        assert rm["mixed_iterations"] >= 1
+        # the first build, the optional re-seed and the final build are the FP64 ones
+        assert rm["fp64_iterations"] == (2 if switch == 0.0 else rm["fp64_iterations"]) <= 3
+        assert rm["iterations"] == rm["mixed_iterations"] + rm["fp64_iterations"]
+        assert abs(rm["energy"] - r64["energy"]) <= 1e-8
 
 
 def _run_x2c(sysd, **kw):
