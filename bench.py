@@ -167,7 +167,7 @@ def x2c_batch_block(want_cpu: bool, count: int = 64, workers: int = 16):
         systems.append(sysd)
         probs.append(dict(eri=src, h_x2c=sysd["h"], x_large=sysd["X"], initial_density=sysd["P0"],
                           n_electrons=sysd["n_electrons"]))
-    scf.runX2CHartreeFockScfBatch(probs[:4], workers=4)  # warm-up
+    scf.runX2CHartreeFockScfBatch(probs, workers=workers)  # warm-up: every handle's first-call allocations
     t0 = time.perf_counter()
     seq = scf.runX2CHartreeFockScfBatch(probs, workers=1)
     t_seq = time.perf_counter() - t0

@@ -115,7 +115,7 @@ __global__ void fill_test_matrix_kernel(double* G, int64_t count) {
 //    (A[i][k] -= A[i][j] conj(A[k][j]) / d_j, spread over all threads) and, in the same phase,
 //    finishes column j-1 (scale by 1/sqrt(d), set the diagonal), which nothing reads any more;
 //  * the inverse is forward elimination on X = I with the same one-phase-per-row scheme.
-constexpr int CHOL_THREADS = 256;
+constexpr int CHOL_THREADS = 1024;
 
 template <int PL>
 __global__ void __launch_bounds__(CHOL_THREADS) chol_block_kernel(const double* M, int r, double* out,

@@ -404,6 +404,28 @@ struct PhaseTimer {
   }
 };
 
+// ---- DHF window deflation ----
+
+// F += (b[1] - b[0]) Pi over `cnt` doubles (interleaved complex): the states of the projector Pi move
+// up by the width of the spectral interval b, i.e. above every other eigenvalue of F in b.
+__global__ void deflate_kernel(double* F, const double* Pi, const double* b, int64_t cnt) {
+  const double sigma = b[1] - b[0];
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < cnt;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    F[i] += sigma * Pi[i];
+}
+
+// Stage 1 of Re tr(A B) = Re sum_ij A_ij conj(B_ij) for Hermitian A, B (interleaved complex).
+__global__ void herm_dot_partial_kernel(const double* A, const double* B, int64_t n2, double* part) {
+  __shared__ double red[32];
+  int64_t beg, end;
+  chunk_of(n2, beg, end);
+  double acc = 0.0;
+  for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) acc += A[2 * i] * B[2 * i] + A[2 * i + 1] * B[2 * i + 1];
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
 // ---- tight spectral bounds for SP2 (block Krylov Ritz values) ----
 
 // K[:, 0:m] (n rows, row pitch ldk) = deterministic pseudo-random numbers in [-1, 1) (splitmix64).
@@ -914,10 +936,30 @@ void scf_rel(rr_ri_store* h, int kind, const double* hc, const double* v_total, 
     a.mirror = 1;  // X^dagger F X is Hermitian
     gemm(a, s, wk(), wcap());
     // window projector in the orthonormal basis
-    sp2_projector(h, Fo, n_eff, nlo + n_electrons, Pi, T2, scal + 8, s, true);
     if (nlo > 0) {
+      // DHF: the negative-energy projector first (a wide gap: few SP2 steps), then those states are
+      // moved above the whole spectrum (F' = F + sigma Pi_neg, sigma = width of the interval SP2
+      // used) and the window is the lowest n_electrons states of F', whose spectral interval no
+      // longer spans the negative-energy continuum.  tr(Pi Pi_neg) ~ 0 confirms that no shifted
+      // state stayed below the window; otherwise the window is Pi_{nlo + n_e}(F) - Pi_{nlo}(F).
       sp2_projector(h, Fo, n_eff, nlo, Pi2, T2, scal + 8, s, true);
-      axpby(Pi, Pi2, -1.0, 1.0, ee, s);
+      RR_CUDA(cudaMemcpyAsync(tmp, Fo, sizeof(double) * ee, cudaMemcpyDeviceToDevice, s));
+      deflate_kernel<<<blocks_for(ee), 256, 0, s>>>(Fo, Pi2, scal + 8, ee);
+      RR_LAUNCH_CHECK();
+      sp2_projector(h, Fo, n_eff, n_electrons, Pi, T2, scal + 8, s, true);
+      herm_dot_partial_kernel<<<RED_CTAS, 256, 0, s>>>(Pi, Pi2, n_eff * n_eff, red);
+      RR_LAUNCH_CHECK();
+      reduce_partials_kernel<0><<<1, 256, 0, s>>>(red, RED_CTAS, 1.0, scal + 16);
+      RR_LAUNCH_CHECK();
+      double leak = 0.0;
+      RR_CUDA(cudaMemcpyAsync(&leak, scal + 16, sizeof(double), cudaMemcpyDeviceToHost, s));
+      RR_CUDA(cudaStreamSynchronize(s));
+      if (!(std::fabs(leak) < 1e-6)) {
+        sp2_projector(h, tmp, n_eff, nlo + n_electrons, Pi, T2, scal + 8, s, true);
+        axpby(Pi, Pi2, -1.0, 1.0, ee, s);
+      }
+    } else {
+      sp2_projector(h, Fo, n_eff, nlo + n_electrons, Pi, T2, scal + 8, s, true);
     }
     // P_new = X Pi X^dagger (Kramers-projected)
     GemmDesc b;
