@@ -186,5 +186,5 @@ def test_learned_preconditioner_cuts_macro_iterations():
                 e[mode] = r["energy"]
                 prob.close()
             assert abs(e["learned"] - e["plain"]) <= 1e-7
-    assert tot["learned"] <= 0.85 * tot["plain"], tot
+    assert tot["learned"] <= 0.70 * tot["plain"], tot  # at least 30 % fewer macro-iterations
     net.close()
