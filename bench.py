@@ -470,7 +470,9 @@ def run_case(args):
     mixed_exchange  the split-BF16 tcgen05 exchange K = sum_P (Ct B^P)^T (Ct B^P) at n=400, naux=1600,
                   nocc=40 (rr_ri_jk_occupied, RR_PREC_MIXED; J stays FP64);
     rkb_mixed     the 4c RKB Fock build of the Kramers-restricted DHF shapes with the split-BF16 exchange,
-                  full then incremental (nl=200, ns=600, naux=1000, 40 spinors)."""
+                  full then incremental (nl=200, ns=600, naux=1000, 40 spinors);
+    x2c_mixed     the X2C Fock build with the split-BF16 exchange, full then incremental (nl=200,
+                  naux=1000, 80 electrons)."""
     import ctypes
 
     import torch
@@ -536,6 +538,24 @@ def run_case(args):
         out.update(workload=f"mixed rkbFockMatrix nl={NL4} ns={NS4} naux={NAUX4} nocc={NOCC4}", ms_full=full,
                    ms_incremental=incr)
         store.sync()
+    elif args.case == "x2c_mixed":
+        s = synth.x2c_system(X2C_NL, X2C_NAUX, X2C_NE, seed=SEED + 21, box=20.0, gap=X2C_GAP)
+        dev = {k: torch.from_numpy(np.ascontiguousarray(s[k])).cuda() for k in ("B", "h", "S", "X", "P0")}
+        store = ri.RiX2cEriSource(X2C_NL, dev["B"], dev["X"], dev["S"]).store
+        n = 2 * X2C_NL
+        F = torch.empty((n, n), dtype=torch.complex128, device="cuda")
+        X = dev["X"]
+
+        def step(incremental):
+            o = L.opts(L.RR_MEM_DEVICE, precision=L.RR_PREC_MIXED, stream=stream, sync=0, incremental=incremental)
+            L.check(lib.rr_ri_fock_x2c(store.handle, dev["h"].data_ptr(), dev["P0"].data_ptr(), dev["S"].data_ptr(),
+                                       X.data_ptr(), X.shape[1], F.data_ptr(), ctypes.byref(o)))
+
+        full = timed(lambda: step(0), args.steps, args.warmup)
+        incr = timed(lambda: step(1), args.steps, args.warmup)
+        out.update(workload=f"mixed x2cFockMatrix nl={X2C_NL} naux={X2C_NAUX} {X2C_NE} electrons", ms_full=full,
+                   ms_incremental=incr)
+        store.sync()
     print(json.dumps(out))
 
 
@@ -546,7 +566,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", default=None, choices=["headline", "mixed_exchange", "rkb_mixed"],
+    ap.add_argument("--case", default=None, choices=["headline", "mixed_exchange", "rkb_mixed", "x2c_mixed"],
                     help="run one workload for profiling instead of the bench line")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)

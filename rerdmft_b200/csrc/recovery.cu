@@ -115,20 +115,32 @@ __global__ void fill_test_matrix_kernel(double* G, int64_t count) {
 //    (A[i][k] -= A[i][j] conj(A[k][j]) / d_j, spread over all threads) and, in the same phase,
 //    finishes column j-1 (scale by 1/sqrt(d), set the diagonal), which nothing reads any more;
 //  * the inverse is forward elimination on X = I with the same one-phase-per-row scheme.
-constexpr int CHOL_THREADS = 1024;
+constexpr int CHOL_THREADS = 256;  // 16 x 16: the element updates use a 2-D thread grid
 
-template <int PL>
+// SMEM selects the buffer at compile time, so the shared-memory variant addresses it with
+// shared-memory instructions (a pointer that may be either compiles to slower generic accesses).
+template <int PL, bool SMEM>
 __global__ void __launch_bounds__(CHOL_THREADS) chol_block_kernel(const double* M, int r, double* out,
                                                                   int want_inverse, int* status, double* gbuf) {
   extern __shared__ double sm[];
-  double* A = gbuf ? gbuf : sm;   // r x r, factor in the lower triangle
+  double* A = SMEM ? sm : gbuf;   // r x r, factor in the lower triangle
   double* X = A + r * r * PL;     // r x r, L^{-1}
   double* piv = X + r * r * PL;   // r pivots d_j before the square root
-  const int t = threadIdx.x;
+  const int t = threadIdx.x, ty = t >> 4, tx = t & 15;  // 16 x 16 grid for the element updates
   for (int e = t; e < r * r * PL; e += CHOL_THREADS) A[e] = M[e];
+  if (want_inverse)
+    for (int e = t; e < r * r; e += CHOL_THREADS) {
+      X[e * PL] = (e / r == e % r) ? 1.0 : 0.0;
+      if (PL == 2) X[e * PL + 1] = 0.0;
+    }
   __syncthreads();
-  for (int j = 0; j <= r; ++j) {
-    if (j > 0) {  // finish column j-1 (its pivot was saved in step j-1; nothing reads the column now)
+  // Phase j runs factorisation step j and, when the inverse is wanted, inverse step j - 2, whose
+  // column of L was finished in phase j - 1: r + 3 barriers instead of 2 r + 2.  The two steps touch
+  // disjoint data (the factorisation writes columns j - 1 and > j of A, the inverse step reads
+  // columns j - 2 and j - 3 of A and writes X).
+  const int last = want_inverse ? r + 2 : r;
+  for (int j = 0; j <= last; ++j) {
+    if (j > 0 && j <= r) {  // finish column j-1 (its pivot was saved in step j-1; nothing reads the column now)
       const int c = j - 1;
       double d = piv[c];
       if (!(d > 0.0)) d = 1e-300;
@@ -148,16 +160,40 @@ __global__ void __launch_bounds__(CHOL_THREADS) chol_block_kernel(const double* 
       if (t == 0) piv[j] = d;
       if (!(d > 0.0)) d = 1e-300;
       const double inv_d = 1.0 / d;
-      const int m = r - j - 1;  // trailing triangle rows j+1..r-1, element (i, k) with k <= i
-      // square sweep of the m x m trailing block (upper half skipped): integer index math only
-      for (int e = t; e < m * m; e += CHOL_THREADS) {
-        const int a = e / m, b = e - a * m;
-        if (b > a) continue;
-        const int i = j + 1 + a, k = j + 1 + b;
-        const double ar = A[(i * r + j) * PL], ai = PL == 2 ? A[(i * r + j) * PL + 1] : 0.0;
-        const double br = A[(k * r + j) * PL], bi = PL == 2 ? A[(k * r + j) * PL + 1] : 0.0;
-        A[(i * r + k) * PL] -= (ar * br + ai * bi) * inv_d;
-        if (PL == 2) A[(i * r + k) * PL + 1] -= (ai * br - ar * bi) * inv_d;
+      // trailing triangle rows j+1..r-1, element (i, k) with k <= i: a 16 x 16 thread grid strides
+      // over rows (ty) and columns (tx), no index division
+      for (int i = j + 1 + ty; i < r; i += 16) {
+        const double ar = A[(i * r + j) * PL] * inv_d, ai = PL == 2 ? A[(i * r + j) * PL + 1] * inv_d : 0.0;
+        for (int k = j + 1 + tx; k <= i; k += 16) {
+          const double br = A[(k * r + j) * PL], bi = PL == 2 ? A[(k * r + j) * PL + 1] : 0.0;
+          A[(i * r + k) * PL] -= ar * br + ai * bi;
+          if (PL == 2) A[(i * r + k) * PL + 1] -= ai * br - ar * bi;
+        }
+      }
+    }
+    // Inverse step q = j - 2 (forward elimination on X = I): row q of X is final once divided by
+    // L[q][q]; rows i > q subtract L[i][q] / L[q][q] times the undivided row q (columns c <= q), and
+    // row q-1 is divided in the same step.
+    const int q = j - 2;
+    if (want_inverse && q >= 0) {
+      if (q > 0) {
+        const int p1 = q - 1;
+        const double inv = 1.0 / A[(p1 * r + p1) * PL];
+        for (int c = t; c <= p1; c += CHOL_THREADS) {
+          X[(p1 * r + c) * PL] *= inv;
+          if (PL == 2) X[(p1 * r + c) * PL + 1] *= inv;
+        }
+      }
+      if (q < r) {
+        const double inv = 1.0 / A[(q * r + q) * PL];
+        for (int i = q + 1 + ty; i < r; i += 16) {
+          const double lr = A[(i * r + q) * PL] * inv, li = PL == 2 ? A[(i * r + q) * PL + 1] * inv : 0.0;
+          for (int c = tx; c <= q; c += 16) {
+            const double xr = X[(q * r + c) * PL], xi = PL == 2 ? X[(q * r + c) * PL + 1] : 0.0;
+            X[(i * r + c) * PL] -= lr * xr - li * xi;
+            if (PL == 2) X[(i * r + c) * PL + 1] -= lr * xi + li * xr;
+          }
+        }
       }
     }
     __syncthreads();
@@ -169,35 +205,6 @@ __global__ void __launch_bounds__(CHOL_THREADS) chol_block_kernel(const double* 
       if (PL == 2) out[e * PL + 1] = k <= i ? A[e * PL + 1] : 0.0;
     }
     return;
-  }
-  for (int e = t; e < r * r; e += CHOL_THREADS) {
-    X[e * PL] = (e / r == e % r) ? 1.0 : 0.0;
-    if (PL == 2) X[e * PL + 1] = 0.0;
-  }
-  __syncthreads();
-  // Row j of X is final once divided by L[j][j]; rows i > j subtract L[i][j] / L[j][j] times the
-  // undivided row j (columns c <= j), and row j-1 is divided in the same phase.
-  for (int j = 0; j <= r; ++j) {
-    if (j > 0) {
-      const int q = j - 1;
-      const double inv = 1.0 / A[(q * r + q) * PL];
-      for (int c = t; c <= q; c += CHOL_THREADS) {
-        X[(q * r + c) * PL] *= inv;
-        if (PL == 2) X[(q * r + c) * PL + 1] *= inv;
-      }
-    }
-    if (j < r) {
-      const double inv = 1.0 / A[(j * r + j) * PL];
-      const int rows = r - j - 1, cols = j + 1;
-      for (int e = t; e < rows * cols; e += CHOL_THREADS) {
-        const int i = j + 1 + e / cols, c = e % cols;
-        const double lr = A[(i * r + j) * PL] * inv, li = PL == 2 ? A[(i * r + j) * PL + 1] * inv : 0.0;
-        const double xr = X[(j * r + c) * PL], xi = PL == 2 ? X[(j * r + c) * PL + 1] : 0.0;
-        X[(i * r + c) * PL] -= lr * xr - li * xi;
-        if (PL == 2) X[(i * r + c) * PL + 1] -= lr * xi + li * xr;
-      }
-    }
-    __syncthreads();
   }
   // out = (L^{-1})^dagger: out[c][i] = conj(X[i][c])
   for (int e = t; e < r * r; e += CHOL_THREADS) {
@@ -247,16 +254,10 @@ void projector_ct(rr_ri_store* h, const double* A, const double* Pe, const doubl
   gemm(y, s, wk, wcap);
   auto chol = [&](const double* mat, int inverse) {
     const int sm = chol_in_smem ? static_cast<int>(block_smem) : 0;
-    double* gb = chol_in_smem ? nullptr : gw;
-    if (cplx) {
-      auto k = chol_block_kernel<2>;
-      if (sm > 48 * 1024) RR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-      k<<<1, CHOL_THREADS, sm, s>>>(mat, static_cast<int>(r), Wt, inverse, h->status.p + 1, gb);
-    } else {
-      auto k = chol_block_kernel<1>;
-      if (sm > 48 * 1024) RR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-      k<<<1, CHOL_THREADS, sm, s>>>(mat, static_cast<int>(r), Wt, inverse, h->status.p + 1, gb);
-    }
+    auto k = cplx ? (chol_in_smem ? chol_block_kernel<2, true> : chol_block_kernel<2, false>)
+                  : (chol_in_smem ? chol_block_kernel<1, true> : chol_block_kernel<1, false>);
+    if (sm > 48 * 1024) RR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    k<<<1, CHOL_THREADS, sm, s>>>(mat, static_cast<int>(r), Wt, inverse, h->status.p + 1, chol_in_smem ? nullptr : gw);
     RR_LAUNCH_CHECK();
   };
   GemmDesc gm;  // M = Y^dagger Y
