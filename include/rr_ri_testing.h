@@ -21,6 +21,12 @@ int rr_test_gemm_f64(int64_t M, int64_t N, int64_t K, const double* A, int64_t l
 /* gamma = B vec(D) and J = B^T gamma through the TMA streaming passes (B: naux x n2, dense). */
 int rr_test_j_passes(const double* B, int64_t naux, int64_t n2, const double* D, double* gamma, double* J);
 
+/* The same passes over the packed upper triangles of the n x n rows of B (the store's J path when
+ * every B^P is symmetric to a few ulps): *packed = 1 when B passed the symmetry test and the packed
+ * passes ran, 0 when the dense passes ran instead (D, J: n x n). */
+int rr_test_j_passes_packed(const double* B, int64_t naux, int64_t n, const double* D, double* gamma, double* J,
+                            int32_t* packed);
+
 /* K = sum_P (Ct B^P)^T (Ct B^P) through the split-BF16 tcgen05 exchange (B: naux x n*n dense,
  * Ct: nocc x n, K: n x n; all FP64 device pointers). */
 int rr_test_mixed_exchange(const double* B, int64_t naux, int64_t n, const double* Ct, int64_t nocc, double* K);

@@ -137,6 +137,7 @@ _SIGS = {
     "rr_test_mixed_exchange": (ctypes.c_int, [_vp, _i64, _i64, _vp, _i64, _vp]),
     "rr_test_mixed_exchange_delta": (ctypes.c_int, [_vp, _i64, _i64, _vp, _vp, _i64, _vp]),
     "rr_test_j_passes": (ctypes.c_int, [_vp, _i64, _i64, _vp, _vp, _vp]),
+    "rr_test_j_passes_packed": (ctypes.c_int, [_vp, _i64, _i64, _vp, _vp, _vp, _vp]),
 }
 
 _lib = None

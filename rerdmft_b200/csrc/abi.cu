@@ -125,6 +125,7 @@ int rr_ri_create(const double* B, int64_t naux, int64_t n, int32_t mem, rr_ri_ha
       h->status.alloc(2);
       RR_CUDA(cudaMemsetAsync(h->status.p, 0, 2 * sizeof(int), h->ctx.main));
       upload_tensor(h->B[0], &h->pitch[0], B, naux, n * n, mem == RR_MEM_HOST, h->ctx.main);
+      rr::pack_for_j(h, 0, n, h->ctx.main);
       RR_CUDA(cudaStreamSynchronize(h->ctx.main));
     } catch (...) {
       h->ctx.destroy();
@@ -154,6 +155,8 @@ int rr_ri_create_4c(const double* B_LL, const double* B_SS, int64_t naux, int64_
       RR_CUDA(cudaMemsetAsync(h->status.p, 0, 2 * sizeof(int), h->ctx.main));
       upload_tensor(h->B[0], &h->pitch[0], B_LL, naux, nl * nl, mem == RR_MEM_HOST, h->ctx.main);
       upload_tensor(h->B[1], &h->pitch[1], B_SS, naux, ns * ns, mem == RR_MEM_HOST, h->ctx.main);
+      rr::pack_for_j(h, 0, nl, h->ctx.main);
+      rr::pack_for_j(h, 1, ns, h->ctx.main);
       RR_CUDA(cudaStreamSynchronize(h->ctx.main));
     } catch (...) {
       h->ctx.destroy();
@@ -612,5 +615,45 @@ extern "C" int rr_test_j_passes(const double* B, int64_t naux, int64_t n2, const
     int e = 0;
     RR_CUDA(cudaMemcpy(&e, err.p, sizeof(int), cudaMemcpyDeviceToHost));
     RR_REQUIRE(e == 0, RR_ERR_TIMEOUT, "rr_test_j_passes: device wait bound expired");
+  });
+}
+
+extern "C" int rr_test_j_passes_packed(const double* B, int64_t naux, int64_t n, const double* D, double* gamma,
+                                       double* J, int32_t* packed) {
+  return api([&] {
+    RR_REQUIRE(naux >= 1 && n >= 1 && packed != nullptr, RR_ERR_ARG, "rr_test_j_passes_packed: bad arguments");
+    const int64_t n2 = n * n;
+    const int64_t pitch = rr::round_up(std::max<int64_t>(n2, 2), 32);
+    rr::DevBuf<double> Bp(static_cast<size_t>(naux * pitch)), Bpk, Dpk(static_cast<size_t>(rr::tri_len(n) + 1));
+    rr::DevBuf<double> Dp(static_cast<size_t>(pitch));  // zero-padded copy for the dense passes
+    rr::DevBuf<int> err(1);
+    RR_CUDA(cudaMemset(Bp.p, 0, sizeof(double) * Bp.n));
+    RR_CUDA(cudaMemset(Dp.p, 0, sizeof(double) * Dp.n));
+    RR_CUDA(cudaMemcpy(Dp.p, D, sizeof(double) * n2, cudaMemcpyDeviceToDevice));
+    RR_CUDA(cudaMemset(err.p, 0, sizeof(int)));
+    RR_CUDA(cudaMemcpy2D(Bp.p, sizeof(double) * pitch, B, sizeof(double) * n2, sizeof(double) * n2, naux,
+                         cudaMemcpyDeviceToDevice));
+    int64_t pitch_pk = 0;
+    const bool ok = rr::j_pack_upper(Bp.p, pitch, naux, n, Bpk, pitch_pk, nullptr);
+    *packed = ok ? 1 : 0;
+    rr::JTensor t;
+    t.J = J;
+    if (ok) {
+      rr::j_fold_density(D, n, Dpk.p, nullptr);
+      t.B = Bpk.p; t.pitch = pitch_pk; t.len = rr::tri_len(n); t.tri_n = n; t.D = Dpk.p;
+    } else {
+      t.B = Bp.p; t.pitch = pitch; t.len = n2; t.D = Dp.p;
+    }
+    rr::JPlan pl = rr::j_plan(1, &t, naux);
+    rr::DevBuf<double> gp(static_cast<size_t>(std::max<int64_t>(pl.gpart_doubles, 1)));
+    rr::DevBuf<double> jp(static_cast<size_t>(std::max<int64_t>(pl.jpart_doubles, 1)));
+    rr::j_pass1(pl, gp.p, err.p, nullptr);
+    rr::j_gamma(pl, gp.p, gamma, nullptr);
+    rr::j_pass2(pl, gp.p, jp.p, err.p, nullptr);
+    rr::j_finish(pl, jp.p, 1.0, nullptr);
+    RR_CUDA(cudaDeviceSynchronize());
+    int e = 0;
+    RR_CUDA(cudaMemcpy(&e, err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    RR_REQUIRE(e == 0, RR_ERR_TIMEOUT, "rr_test_j_passes_packed: device wait bound expired");
   });
 }

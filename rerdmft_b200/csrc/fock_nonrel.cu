@@ -79,40 +79,44 @@ void exchange_nonrel(rr_ri_store* h, const double* Ct, int64_t ldct, bool ct_tra
   gemm(sk, s, h->work.p, static_cast<int64_t>(h->work.n));
 }
 
-// Launches the J passes for the pitched density Dp on the side stream, forked from / joined to s.
-void coulomb_async(rr_ri_store* h, const double* Dp, double* J, double scale, cudaStream_t s) {
-  JTensor t;
-  t.B = h->B[0].p;
-  t.pitch = h->pitch[0];
-  t.len = h->n * h->n;
-  t.D = Dp;
-  t.J = J;
-  JPlan pl = j_plan(1, &t, h->naux, 1);
-  h->jscr.ensure(static_cast<size_t>(round_up(pl.gpart_doubles, 32) + pl.jpart_doubles + 32));
-  double* gpart = h->jscr.p;
-  double* jpart = h->jscr.p + round_up(pl.gpart_doubles, 32);
-  auto& c = h->ctx;
-  RR_CUDA(cudaEventRecord(c.fork, s));
-  RR_CUDA(cudaStreamWaitEvent(c.side, c.fork, 0));
-  prof_mark(h, 5, c.side);
-  j_pass1(pl, gpart, h->status.p, c.side);
-  j_pass2(pl, gpart, jpart, h->status.p, c.side);
-  j_finish(pl, jpart, scale, c.side);
-  prof_mark(h, 6, c.side);
-  RR_CUDA(cudaEventRecord(c.join, c.side));
+void pack_for_j(rr_ri_store* h, int t, int64_t n, cudaStream_t s) {
+  h->Bpk[t].release();
+  h->pitch_pk[t] = 0;
+  if (h->naux == 0 || n < 2) return;
+  size_t free_b = 0, total_b = 0;
+  RR_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  const double bytes = 8.0 * static_cast<double>(h->naux) * static_cast<double>(round_up(tri_len(n), 32));
+  if (bytes > 0.5 * static_cast<double>(free_b)) return;
+  j_pack_upper(h->B[t].p, h->pitch[t], h->naux, n, h->Bpk[t], h->pitch_pk[t], s);
+}
+
+JTensor j_tensor(rr_ri_store* h, int t, int64_t n, const double* D, double* J, int64_t doff, cudaStream_t s) {
+  JTensor jt;
+  jt.J = J;
+  if (h->Bpk[t].p) {
+    RR_REQUIRE(static_cast<int64_t>(h->dfold.n) >= doff + tri_len(n) + 1, RR_ERR_ARG, "j_tensor: fold buffer too small");
+    j_fold_density(D, n, h->dfold.p + doff, s);
+    jt.B = h->Bpk[t].p;
+    jt.pitch = h->pitch_pk[t];
+    jt.len = tri_len(n);
+    jt.tri_n = n;
+    jt.D = h->dfold.p + doff;
+  } else {
+    jt.B = h->B[t].p;
+    jt.pitch = h->pitch[t];
+    jt.len = n * n;
+    jt.D = D;
+  }
+  return jt;
 }
 
 // Same for one or two tensors sharing gamma (4c: LL and SS); Dp[t] pitched, J[t] dense outputs.
 void coulomb_async_multi(rr_ri_store* h, int ntens, const double* const* Dp, double* const* J, cudaStream_t s) {
   JTensor t[2];
   const int64_t nn[2] = {h->n, h->ns};
-  for (int i = 0; i < ntens; ++i) {
-    t[i].B = h->B[i].p;
-    t[i].pitch = h->pitch[i];
-    t[i].len = nn[i] * nn[i];
-    t[i].D = Dp[i];
-    t[i].J = J[i];
-  }
+  const int64_t doff1 = round_up(tri_len(nn[0]) + 1, 32);
+  h->dfold.ensure(static_cast<size_t>(doff1 + (ntens > 1 ? tri_len(nn[1]) + 1 : 0)));
+  for (int i = 0; i < ntens; ++i) t[i] = j_tensor(h, i, nn[i], Dp[i], J[i], i ? doff1 : 0, s);
   JPlan pl = j_plan(ntens, t, h->naux, 1);
   h->jscr.ensure(static_cast<size_t>(round_up(pl.gpart_doubles, 32) + pl.jpart_doubles + 32));
   double* gpart = h->jscr.p;
@@ -172,12 +176,8 @@ __global__ void density_flag_kernel(const double* m, int* flag) { flag[0] = m[0]
 void coulomb_after_ht(rr_ri_store* h, const double* Dp, const double* Ct, int64_t nocc, double* J,
                       const double* tgam, int tseg, cudaStream_t s) {
   const int64_t n = h->n, naux = h->naux, n2 = n * n;
-  JTensor t;
-  t.B = h->B[0].p;
-  t.pitch = h->pitch[0];
-  t.len = n2;
-  t.D = Dp;
-  t.J = J;
+  h->dfold.ensure(static_cast<size_t>(tri_len(n) + 1));
+  JTensor t = j_tensor(h, 0, n, Dp, J, 0, s);
   JPlan pl = j_plan(1, &t, naux, 3);
   const int64_t goff = round_up(pl.gpart_doubles, 32), joff = goff + round_up(pl.jpart_doubles, 32);
   const int64_t toff = joff + round_up(n2, 32);

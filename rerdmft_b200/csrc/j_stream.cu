@@ -1,6 +1,7 @@
 // Coulomb streaming passes (see j_stream.cuh).  One producer warp issues 16 KB TMA bulk copies
 // into a 4-stage shared-memory ring; 8 consumer warps read them with 128-bit shared loads.
 #include <atomic>
+#include <cfloat>
 #include "j_stream.cuh"
 #include "tma_util.cuh"
 
@@ -221,16 +222,76 @@ __global__ void __launch_bounds__(THREADS) j_pass2_kernel(const P2 p) {
   }
 }
 
+__host__ __device__ inline int64_t out_len(const JTensor& t) { return t.tri_n ? t.tri_n * t.tri_n : t.len; }
+
+// J[t][k] from the pass-2 partials of entry k (packed rows: of entry tri_index(min, max), so both
+// triangles get the same sum, added in the same order).
 __global__ void j_finish_kernel(JTensor t0, JTensor t1, int ntens, int nrange, int64_t jstride, const double* jpart,
                                 double scale) {
-  const int64_t total = t0.len + (ntens > 1 ? t1.len : 0);
+  const int64_t out0 = out_len(t0);
+  const int64_t total = out0 + (ntens > 1 ? out_len(t1) : 0);
   for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < total;
        k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const bool second = k >= out0;
+    const JTensor& t = second ? t1 : t0;
+    const int64_t kk = second ? k - out0 : k;
+    int64_t src = second ? t0.len : 0;
+    if (t.tri_n) {
+      const int64_t q = kk / t.tri_n, a = kk - q * t.tri_n;
+      src += q <= a ? tri_index(q, a, t.tri_n) : tri_index(a, q, t.tri_n);
+    } else {
+      src += kk;
+    }
     double s = 0.0;
-    for (int r = 0; r < nrange; ++r) s += jpart[r * jstride + k];
-    if (k < t0.len) t0.J[k] = scale * s;
-    else t1.J[k - t0.len] = scale * s;
+    for (int r = 0; r < nrange; ++r) s += jpart[r * jstride + src];
+    t.J[kk] = scale * s;
   }
+}
+
+// Packs the upper triangle of each B^P through 32 x 32 tile pairs (ti <= tj) in shared memory, so
+// both the tile and its mirror are read with coalesced loads; *asym = 1 when an element and its
+// mirror differ by more than 8 eps of the larger.
+__global__ void __launch_bounds__(256) j_pack_kernel(const double* __restrict__ B, int64_t pitch, int64_t naux,
+                                                     int64_t n, double* __restrict__ out, int64_t pitch_out,
+                                                     int* asym) {
+  __shared__ double tu[32][33], tl[32][33];
+  const int ntile = static_cast<int>((n + 31) / 32);
+  const int ti = static_cast<int>(blockIdx.x) / ntile, tj = static_cast<int>(blockIdx.x) % ntile;
+  if (ti > tj) return;
+  const int c = threadIdx.x & 31, r0 = threadIdx.x >> 5;
+  bool bad = false;
+  for (int64_t P = blockIdx.y; P < naux; P += gridDim.y) {
+    const double* b = B + P * pitch;
+    for (int r = r0; r < 32; r += 8) {
+      const int64_t q = ti * 32 + r, a = tj * 32 + c;  // upper tile (q, a)
+      tu[r][c] = q < n && a < n ? b[q * n + a] : 0.0;
+      const int64_t q2 = tj * 32 + r, a2 = ti * 32 + c;  // mirror tile (a, q), stored transposed
+      tl[c][r] = q2 < n && a2 < n ? b[q2 * n + a2] : 0.0;
+    }
+    __syncthreads();
+    double* o = out + P * pitch_out;
+    for (int r = r0; r < 32; r += 8) {
+      const int64_t q = ti * 32 + r, a = tj * 32 + c;
+      if (q < n && a < n && a >= q) {
+        const double x = tu[r][c], y = tl[r][c];
+        if (!(fabs(x - y) <= 8.0 * DBL_EPSILON * fmax(fabs(x), fabs(y)))) bad = true;
+        o[tri_index(q, a, n)] = x;
+      }
+    }
+    __syncthreads();
+  }
+  if (bad) atomicOr(asym, 1);
+}
+
+__global__ void j_fold_kernel(const double* __restrict__ D, int64_t n, double* __restrict__ Dpk) {
+  const int64_t n2 = n * n;
+  for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n2;
+       k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t q = k / n, a = k - q * n;
+    if (a < q) continue;
+    Dpk[tri_index(q, a, n)] = a == q ? D[k] : D[k] + D[a * n + q];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && (tri_len(n) & 1)) Dpk[tri_len(n)] = 0.0;
 }
 
 __global__ void j_gamma_kernel(const double* gpart, int64_t naux, int segtot, double* gamma) {
@@ -342,19 +403,48 @@ void j_pass2(const JPlan& pl, const double* gpart, double* jpart, int* err, cuda
 }
 
 void j_finish(const JPlan& pl, const double* jpart, double scale, cudaStream_t s) {
-  const int64_t total = pl.t[0].len + (pl.ntens > 1 ? pl.t[1].len : 0);
+  const int64_t jstride = pl.t[0].len + (pl.ntens > 1 ? pl.t[1].len : 0);
+  const int64_t total = out_len(pl.t[0]) + (pl.ntens > 1 ? out_len(pl.t[1]) : 0);
   if (total == 0) return;
-  const int64_t jstride = total;
   // nrange actually used by pass 2 (ranges past naux produce no rows and are never read).
   const int64_t rp = (pl.naux + pl.nrange - 1) / std::max(pl.nrange, 1);
   const int used = pl.naux ? static_cast<int>((pl.naux + rp - 1) / rp) : 0;
   const int blocks = static_cast<int>(std::min<int64_t>(4LL * sm_count(), (total + 255) / 256));
   if (used == 0) {
-    RR_CUDA(cudaMemsetAsync(pl.t[0].J, 0, sizeof(double) * pl.t[0].len, s));
-    if (pl.ntens > 1) RR_CUDA(cudaMemsetAsync(pl.t[1].J, 0, sizeof(double) * pl.t[1].len, s));
+    RR_CUDA(cudaMemsetAsync(pl.t[0].J, 0, sizeof(double) * out_len(pl.t[0]), s));
+    if (pl.ntens > 1) RR_CUDA(cudaMemsetAsync(pl.t[1].J, 0, sizeof(double) * out_len(pl.t[1]), s));
     return;
   }
   j_finish_kernel<<<blocks, 256, 0, s>>>(pl.t[0], pl.t[1], pl.ntens, used, jstride, jpart, scale);
+  RR_LAUNCH_CHECK();
+}
+
+bool j_pack_upper(const double* B, int64_t pitch, int64_t naux, int64_t n, DevBuf<double>& out, int64_t& pitch_out,
+                  cudaStream_t s) {
+  RR_REQUIRE(n >= 1 && naux >= 1 && pitch >= n * n, RR_ERR_ARG, "j_pack_upper: bad shape");
+  pitch_out = round_up(tri_len(n), 32);
+  out.alloc(static_cast<size_t>(naux * pitch_out));
+  RR_CUDA(cudaMemsetAsync(out.p, 0, sizeof(double) * out.n, s));
+  DevBuf<int> asym(1);
+  RR_CUDA(cudaMemsetAsync(asym.p, 0, sizeof(int), s));
+  const int64_t ntile = (n + 31) / 32;
+  const dim3 grid(static_cast<unsigned>(ntile * ntile), static_cast<unsigned>(std::min<int64_t>(naux, 65535)));
+  j_pack_kernel<<<grid, 256, 0, s>>>(B, pitch, naux, n, out.p, pitch_out, asym.p);
+  RR_LAUNCH_CHECK();
+  int h = 0;
+  RR_CUDA(cudaMemcpyAsync(&h, asym.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  RR_CUDA(cudaStreamSynchronize(s));
+  if (h) {
+    out.release();
+    pitch_out = 0;
+    return false;
+  }
+  return true;
+}
+
+void j_fold_density(const double* D, int64_t n, double* Dpk, cudaStream_t s) {
+  const int blocks = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(2LL * sm_count(), (n * n + 255) / 256)));
+  j_fold_kernel<<<blocks, 256, 0, s>>>(D, n, Dpk);
   RR_LAUNCH_CHECK();
 }
 

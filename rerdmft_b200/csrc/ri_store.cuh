@@ -12,12 +12,17 @@ struct rr_ri_store {
   int ntens = 1;
   rr::DevBuf<double> B[2];  // resident tensors, row pitch `pitch` doubles (256-byte aligned rows)
   int64_t pitch[2] = {0, 0};
+  // Packed upper triangles of B[t] (rr::j_pack_upper), built at creation when every B^P is
+  // symmetric and the copy fits in half of the free memory; the J passes then stream these.
+  rr::DevBuf<double> Bpk[2];
+  int64_t pitch_pk[2] = {0, 0};
   rr::DevBuf<int> status;   // device status word written by bounded waits
   // Scratch, grown on demand and reused across calls.
   rr::DevBuf<double> mats;  // per-call matrices (inputs, outputs, intermediates)
   rr::DevBuf<double> T;     // half-transformed exchange intermediate
   rr::DevBuf<double> work;  // split-K partial products
   rr::DevBuf<double> jscr;  // J pass-1/pass-2 partial sums
+  rr::DevBuf<double> dfold; // densities folded onto the packed triangles
   rr::DevBuf<double> tgam;  // gamma partials from the half-transform epilogue
   rr::DevBuf<double> solver_a;  // eigen-problem matrix / eigenvectors
   rr::DevBuf<double> solver_w;  // eigenvalues
@@ -73,6 +78,11 @@ struct RelBuild {
 };
 
 cudaStream_t call_stream(rr_ri_store* h, const rr_opts* o);
+// Builds h->Bpk[t] from h->B[t] (n x n rows) when it fits; synchronises s.
+void pack_for_j(rr_ri_store* h, int t, int64_t n, cudaStream_t s);
+// JTensor of tensor t (n x n rows) over the packed copy when there is one (D folded into dfold at
+// offset doff doubles) or over B[t] itself (D used as is).
+JTensor j_tensor(rr_ri_store* h, int t, int64_t n, const double* D, double* J, int64_t doff, cudaStream_t s);
 // Records profiling event i on stream s when profiling is on.
 void prof_mark(rr_ri_store* h, int i, cudaStream_t s);
 int64_t launches();

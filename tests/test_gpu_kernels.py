@@ -106,3 +106,38 @@ def test_j_passes(naux, n2):
     Jref = B.T @ gref
     assert np.abs(_np(g) - gref).max() <= 1e-12 * np.sqrt(n2) * np.abs(gref).max()
     assert np.abs(_np(J) - Jref).max() <= 1e-12 * np.sqrt(naux * n2) * np.abs(Jref).max()
+
+
+@pytest.mark.parametrize("naux,n,kind", [(1, 1, "sym"), (5, 2, "sym"), (37, 33, "sym"), (129, 64, "roundoff"),
+                                         (200, 97, "roundoff"), (64, 150, "sym"), (40, 31, "asym")])
+def test_j_passes_packed(naux, n, kind):
+    """Packed upper-triangle passes: exact-symmetric and roundoff-symmetric B take them and match the
+    dense formula; a B that is not symmetric falls back to the dense passes."""
+    rng = np.random.default_rng(naux + n)
+    g = rng.uniform(0.5, 1.5, size=(naux, n))
+    c = rng.standard_normal((naux, n, n))
+    c = c + c.transpose(0, 2, 1)
+    if kind == "sym":
+        B = c
+    elif kind == "roundoff":  # (c g_q) g_a against (c g_a) g_q: symmetric to an ulp or two
+        B = c * g[:, :, None] * g[:, None, :]
+    else:
+        B = c + 1e-6 * rng.standard_normal((naux, n, n))
+    B = np.ascontiguousarray(B.reshape(naux, n * n))
+    D = rng.standard_normal((n, n))
+    dB, dD = _dev(B), _dev(D.reshape(-1))
+    gam = torch.empty(naux, dtype=torch.float64, device="cuda")
+    J = torch.empty(n * n, dtype=torch.float64, device="cuda")
+    packed = ctypes.c_int32(-1)
+    L.check(L.lib().rr_test_j_passes_packed(dB.data_ptr(), naux, n, dD.data_ptr(), gam.data_ptr(), J.data_ptr(),
+                                            ctypes.byref(packed)))
+    assert packed.value == (0 if kind == "asym" else 1)
+    gref = B @ D.reshape(-1)
+    Jref = B.T @ gref
+    n2 = n * n
+    assert np.abs(_np(gam) - gref).max() <= 1e-12 * np.sqrt(n2) * np.abs(gref).max()
+    Jg = _np(J)
+    assert np.abs(Jg - Jref).max() <= 1e-12 * np.sqrt(naux * n2) * np.abs(Jref).max()
+    if kind != "asym":
+        Jm = Jg.reshape(n, n)
+        assert np.array_equal(Jm, Jm.T)
