@@ -31,7 +31,7 @@ void density_from_occupied(double* Dp, const double* C, int64_t n, int64_t nocc,
 // Exchange K' = sum_P (Ct B^P)^T (Ct B^P) for a given Ct (nocc x n, row-major with leading
 // dimension ldct, or its transpose when ct_transposed: Ct = C^T with C stored n x nocc).
 void coulomb_after_ht(rr_ri_store* h, const double* Dp, const double* Ct, int64_t nocc, double* J,
-                      const double* tgam, int tseg, cudaStream_t s);
+                      const double* tgam, int tseg, cudaStream_t s, bool overlap = false);
 
 // With Dp given, the Coulomb matrix J (from the pitched density Dp) is queued on the side stream
 // right after the half-transform (coulomb_after_ht) and lands in Jout; join with coulomb_join.
@@ -66,7 +66,7 @@ void exchange_nonrel(rr_ri_store* h, const double* Ct, int64_t ldct, bool ct_tra
   }
   gemm(ht, s);
   prof_mark(h, 2, s);
-  if (Dp) coulomb_after_ht(h, Dp, Ct, nocc, Jout, tgam, tseg, s);
+  if (Dp) coulomb_after_ht(h, Dp, Ct, nocc, Jout, tgam, tseg, s, true);
 
   GemmDesc sk;
   sk.M = n; sk.N = n; sk.K = naux * nocc;
@@ -171,14 +171,24 @@ __global__ void density_flag_kernel(const double* m, int* flag) { flag[0] = m[0]
 // whenever D = 2 Ct^T Ct.  Here, on the side stream after the half-transform (event `mid`), that
 // identity is checked on the device (Drec = 2 Ct^T Ct vs D); pass 1 streams B only when it fails
 // (the kernel is launched either way and exits at once when not needed); pass 2 streams B once.
-// The passes run on `s` itself with the whole GPU (3 CTAs per SM): measured on B200, sharing the SMs
-// with the SYRK halved both.  tgam: naux * tseg partials from the half-transform.
+// Without overlap the passes run on `s` itself with the whole GPU (3 CTAs per SM).  With overlap
+// they run on the side stream, forked from s here, with one CTA per SM, next to the exchange SYRK
+// that s runs meanwhile: the J kernels are held to 48 registers so that one of them and two SYRK
+// CTAs (2 x 25.6k registers) fit on an SM together.  Either way the caller joins with coulomb_join.
+// tgam: naux * tseg partials from the half-transform.
 void coulomb_after_ht(rr_ri_store* h, const double* Dp, const double* Ct, int64_t nocc, double* J,
-                      const double* tgam, int tseg, cudaStream_t s) {
+                      const double* tgam, int tseg, cudaStream_t s_in, bool overlap) {
   const int64_t n = h->n, naux = h->naux, n2 = n * n;
+  auto& c = h->ctx;
+  cudaStream_t s = s_in;
+  if (overlap) {
+    RR_CUDA(cudaEventRecord(c.fork, s_in));
+    RR_CUDA(cudaStreamWaitEvent(c.side, c.fork, 0));
+    s = c.side;
+  }
   h->dfold.ensure(static_cast<size_t>(tri_len(n) + 1));
   JTensor t = j_tensor(h, 0, n, Dp, J, 0, s);
-  JPlan pl = j_plan(1, &t, naux, 3);
+  JPlan pl = j_plan(1, &t, naux, overlap ? 1 : 3);
   const int64_t goff = round_up(pl.gpart_doubles, 32), joff = goff + round_up(pl.jpart_doubles, 32);
   const int64_t toff = joff + round_up(n2, 32);
   h->jscr.ensure(static_cast<size_t>(toff + 64));
@@ -187,7 +197,6 @@ void coulomb_after_ht(rr_ri_store* h, const double* Dp, const double* Ct, int64_
   double* Drec = h->jscr.p + joff;
   double* mm = h->jscr.p + toff;
   int* flag = reinterpret_cast<int*>(mm + 4);
-  auto& c = h->ctx;
   prof_mark(h, 5, s);
   if (nocc > 0 && naux > 0 && tgam) {
     GemmDesc g;  // Drec = 2 Ct^T Ct

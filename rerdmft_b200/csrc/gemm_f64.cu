@@ -321,6 +321,9 @@ void launch_cfg_v(const Params& p, dim3 grid, cudaStream_t s) {
   static std::atomic<bool> attr{false};  // host threads may race here: the attribute is idempotent
   if (!attr) {
     RR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, CF::SMEM_BYTES));
+    // Largest shared-memory carveout: an SM only takes CTAs of another kernel when its carveout
+    // fits them too, and the J passes run beside the exchange SYRK.
+    RR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
     attr = true;
   }
   kern<<<grid, CF::THREADS, CF::SMEM_BYTES, s>>>(p);

@@ -14,6 +14,8 @@ constexpr int CWARPS = 8;
 constexpr int CT = 32 * CWARPS;
 constexpr int THREADS = CT + 32;
 constexpr int SMEM = NST * CW * 8 + 2 * NST * 8 + CWARPS * 8;
+// The pass kernels are held to 48 registers (a few bytes of spills outside the ring loops): one CTA
+// then fits on an SM beside two CTAs of the exchange SYRK.
 constexpr int ERR_P1_PROD = 1 << 0, ERR_P1_CONS = 1 << 1, ERR_P2_PROD = 1 << 2, ERR_P2_CONS = 1 << 3;
 
 struct P1 {
@@ -65,7 +67,7 @@ __device__ __forceinline__ void decode1(const P1& p, int64_t it, int& tau, int64
   ke = min64(p.t[tau].len, kb + p.seglen[tau]);
 }
 
-__global__ void __launch_bounds__(THREADS) j_pass1_kernel(const P1 p) {
+__global__ void __maxnreg__(48) j_pass1_kernel(const P1 p) {
   if (p.skip && *p.skip) return;
   extern __shared__ __align__(128) unsigned char sm[];
   double* ring = reinterpret_cast<double*>(sm);
@@ -139,7 +141,7 @@ __global__ void __launch_bounds__(THREADS) j_pass1_kernel(const P1 p) {
   }
 }
 
-__global__ void __launch_bounds__(THREADS) j_pass2_kernel(const P2 p) {
+__global__ void __maxnreg__(48) j_pass2_kernel(const P2 p) {
   extern __shared__ __align__(128) unsigned char sm[];
   double* ring = reinterpret_cast<double*>(sm);
   uint64_t* full = reinterpret_cast<uint64_t*>(sm + NST * CW * 8);
@@ -323,6 +325,9 @@ void set_smem_attr() {
   if (!done) {
     RR_CUDA(cudaFuncSetAttribute(j_pass1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
     RR_CUDA(cudaFuncSetAttribute(j_pass2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
+    // same carveout as the GEMMs they run beside, so an SM can hold both
+    RR_CUDA(cudaFuncSetAttribute(j_pass1_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
+    RR_CUDA(cudaFuncSetAttribute(j_pass2_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
     done = true;
   }
 }
