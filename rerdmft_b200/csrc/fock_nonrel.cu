@@ -31,10 +31,14 @@ void density_from_occupied(double* Dp, const double* C, int64_t n, int64_t nocc,
 // Exchange K' = sum_P (Ct B^P)^T (Ct B^P) for a given Ct (nocc x n, row-major with leading
 // dimension ldct, or its transpose when ct_transposed: Ct = C^T with C stored n x nocc).
 void coulomb_after_ht(rr_ri_store* h, const double* Dp, const double* Ct, int64_t nocc, double* J,
-                      const double* tgam, int tseg, cudaStream_t s, bool overlap = false);
+                      const double* tgam, int tseg, cudaStream_t s);
+void coulomb_prep(rr_ri_store* h, const double* Dp, const double* Ct, int64_t nocc, double* J, bool have_tgam,
+                  cudaStream_t s, bool overlap);
+void coulomb_run(rr_ri_store* h, const double* tgam, int tseg, cudaStream_t s);
 
-// With Dp given, the Coulomb matrix J (from the pitched density Dp) is queued on the side stream
-// right after the half-transform (coulomb_after_ht) and lands in Jout; join with coulomb_join.
+// With Dp given, the Coulomb matrix J (from the pitched density Dp) is prepared on the side stream
+// beside the half-transform and streamed beside the SYRK (coulomb_prep / coulomb_run); it lands in
+// Jout; join with coulomb_join.
 // The exchange reads c_t as Ct (nocc x n, ld ldct) or, when ct_transposed, as C^T of C (n x ldct).
 void exchange_nonrel(rr_ri_store* h, const double* Ct, int64_t ldct, bool ct_transposed, int64_t nocc, double* K,
                      cudaStream_t s, const double* Dp = nullptr, double* Jout = nullptr) {
@@ -63,10 +67,11 @@ void exchange_nonrel(rr_ri_store* h, const double* Ct, int64_t ldct, bool ct_tra
     ht.edot_ld = n;
     ht.edot_scale = 2.0;
     ht.edot_out = tgam;
+    coulomb_prep(h, Dp, Ct, nocc, Jout, true, s, true);  // side stream, beside the half-transform
   }
   gemm(ht, s);
   prof_mark(h, 2, s);
-  if (Dp) coulomb_after_ht(h, Dp, Ct, nocc, Jout, tgam, tseg, s, true);
+  if (Dp) coulomb_run(h, tgam, tseg, s);  // side stream, beside the SYRK
 
   GemmDesc sk;
   sk.M = n; sk.N = n; sk.K = naux * nocc;
@@ -166,18 +171,19 @@ __global__ void density_flag_kernel(const double* m, int* flag) { flag[0] = m[0]
 
 }  // namespace
 
-// Coulomb for the nonrelativistic build.  The half-transform GEMM already produced, in its
-// epilogue, gamma partials from T:  gamma_P = sum_mn B^P_mn D_mn = 2 sum_{i,a} T[P](i,a) Ct(i,a)
-// whenever D = 2 Ct^T Ct.  Here, on the side stream after the half-transform (event `mid`), that
-// identity is checked on the device (Drec = 2 Ct^T Ct vs D); pass 1 streams B only when it fails
-// (the kernel is launched either way and exits at once when not needed); pass 2 streams B once.
-// Without overlap the passes run on `s` itself with the whole GPU (3 CTAs per SM).  With overlap
-// they run on the side stream, forked from s here, with one CTA per SM, next to the exchange SYRK
-// that s runs meanwhile: the J kernels are held to 48 registers so that one of them and two SYRK
-// CTAs (2 x 25.6k registers) fit on an SM together.  Either way the caller joins with coulomb_join.
-// tgam: naux * tseg partials from the half-transform.
-void coulomb_after_ht(rr_ri_store* h, const double* Dp, const double* Ct, int64_t nocc, double* J,
-                      const double* tgam, int tseg, cudaStream_t s_in, bool overlap) {
+// Coulomb for the nonrelativistic build.  The half-transform GEMM produces, in its epilogue,
+// gamma partials from T:  gamma_P = sum_mn B^P_mn D_mn = 2 sum_{i,a} T[P](i,a) Ct(i,a) whenever
+// D = 2 Ct^T Ct.  coulomb_prep checks that identity on the device (Drec = 2 Ct^T Ct vs D) and folds D
+// onto the packed triangles; coulomb_run (after the half-transform) launches pass 1, which streams B
+// only when the check failed (it is launched either way and exits at once when not needed), pass 2
+// and the finish.
+// Without overlap everything runs on `s` itself and the passes use the whole GPU (3 CTAs per SM).
+// With overlap the preparation runs on the side stream beside the half-transform and the passes,
+// with one CTA per SM, beside the exchange SYRK that s runs after it: the J kernels are held to 48
+// registers so that one of them and two SYRK CTAs (2 x 25.6k registers) fit on an SM together.
+// Either way the caller joins with coulomb_join.  have_tgam: the half-transform writes the partials.
+void coulomb_prep(rr_ri_store* h, const double* Dp, const double* Ct, int64_t nocc, double* J, bool have_tgam,
+                  cudaStream_t s_in, bool overlap) {
   const int64_t n = h->n, naux = h->naux, n2 = n * n;
   auto& c = h->ctx;
   cudaStream_t s = s_in;
@@ -192,13 +198,11 @@ void coulomb_after_ht(rr_ri_store* h, const double* Dp, const double* Ct, int64_
   const int64_t goff = round_up(pl.gpart_doubles, 32), joff = goff + round_up(pl.jpart_doubles, 32);
   const int64_t toff = joff + round_up(n2, 32);
   h->jscr.ensure(static_cast<size_t>(toff + 64));
-  double* gpart = h->jscr.p;
-  double* jpart = h->jscr.p + goff;
   double* Drec = h->jscr.p + joff;
   double* mm = h->jscr.p + toff;
   int* flag = reinterpret_cast<int*>(mm + 4);
   prof_mark(h, 5, s);
-  if (nocc > 0 && naux > 0 && tgam) {
+  if (nocc > 0 && naux > 0 && have_tgam) {
     GemmDesc g;  // Drec = 2 Ct^T Ct
     g.M = n; g.N = n; g.K = nocc;
     g.A = Ct; g.lda = n; g.opA = Op::T;
@@ -212,11 +216,35 @@ void coulomb_after_ht(rr_ri_store* h, const double* Dp, const double* Ct, int64_
   } else {
     RR_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s));
   }
-  j_pass1(pl, gpart, h->status.p, s, flag);
-  j_pass2(pl, gpart, jpart, h->status.p, s, tgam, tseg, flag);
-  j_finish(pl, jpart, 1.0, s);
+  auto& jp = h->jpend;
+  jp.pl = pl;
+  jp.gpart = h->jscr.p;
+  jp.jpart = h->jscr.p + goff;
+  jp.flag = flag;
+  jp.s = s;
+  jp.overlap = overlap;
+}
+
+// s_in: the stream that ran the half-transform (the one coulomb_prep was given).
+void coulomb_run(rr_ri_store* h, const double* tgam, int tseg, cudaStream_t s_in) {
+  auto& c = h->ctx;
+  auto& jp = h->jpend;
+  const cudaStream_t s = jp.s;
+  if (jp.overlap) {
+    RR_CUDA(cudaEventRecord(c.mid, s_in));
+    RR_CUDA(cudaStreamWaitEvent(s, c.mid, 0));
+  }
+  j_pass1(jp.pl, jp.gpart, h->status.p, s, jp.flag);
+  j_pass2(jp.pl, jp.gpart, jp.jpart, h->status.p, s, tgam, tseg, jp.flag);
+  j_finish(jp.pl, jp.jpart, 1.0, s);
   prof_mark(h, 6, s);
-  RR_CUDA(cudaEventRecord(c.join, s));  // coulomb_join is then a no-op wait on the same stream
+  RR_CUDA(cudaEventRecord(c.join, s));  // without overlap coulomb_join is a no-op wait on the same stream
+}
+
+void coulomb_after_ht(rr_ri_store* h, const double* Dp, const double* Ct, int64_t nocc, double* J,
+                      const double* tgam, int tseg, cudaStream_t s) {
+  coulomb_prep(h, Dp, Ct, nocc, J, tgam != nullptr, s, false);
+  coulomb_run(h, tgam, tseg, s);
 }
 
 void coulomb_join(rr_ri_store* h, cudaStream_t s) { RR_CUDA(cudaStreamWaitEvent(s, h->ctx.join, 0)); }

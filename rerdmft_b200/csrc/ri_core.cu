@@ -31,6 +31,7 @@ void Context::init(cudaStream_t user_stream) {
   RR_CUDA(cudaStreamCreateWithPriority(&side, cudaStreamNonBlocking, hi));
   RR_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
   RR_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+  RR_CUDA(cudaEventCreateWithFlags(&mid, cudaEventDisableTiming));
   RR_SOLVER(cusolverDnCreate(&solver));
 }
 

@@ -23,6 +23,14 @@ struct rr_ri_store {
   rr::DevBuf<double> work;  // split-K partial products
   rr::DevBuf<double> jscr;  // J pass-1/pass-2 partial sums
   rr::DevBuf<double> dfold; // densities folded onto the packed triangles
+  // Coulomb passes prepared by coulomb_prep and launched by coulomb_run.
+  struct {
+    rr::JPlan pl;
+    double *gpart = nullptr, *jpart = nullptr;
+    int* flag = nullptr;
+    cudaStream_t s = nullptr;
+    bool overlap = false;
+  } jpend;
   rr::DevBuf<double> tgam;  // gamma partials from the half-transform epilogue
   rr::DevBuf<double> solver_a;  // eigen-problem matrix / eigenvectors
   rr::DevBuf<double> solver_w;  // eigenvalues

@@ -27,7 +27,7 @@ namespace rr {
 void exchange_nonrel(rr_ri_store* h, const double* Ct, int64_t ldct, bool ct_transposed, int64_t nocc, double* K,
                      cudaStream_t s, const double* Dp, double* Jout);
 void coulomb_after_ht(rr_ri_store* h, const double* Dp, const double* Ct, int64_t nocc, double* J, const double* tgam,
-                      int tseg, cudaStream_t s, bool overlap = false);
+                      int tseg, cudaStream_t s);
 void coulomb_join(rr_ri_store* h, cudaStream_t s);
 void fock_nonrel(rr_ri_store* h, const double* hc, const double* D, const double* S, const double* X, int64_t n_eff,
                  double* F, const rr_opts* o);
