@@ -406,7 +406,8 @@ int pick_splits(const GemmDesc& d, Shape sh, int64_t* kchunk) {
   // Enough CTAs for several waves (load balance across SMs), K chunks of at least 128.
   const int64_t target = 8LL * num_sms();
   int splits = 1;
-  if (cplx_tile32(d)) {
+  if (cplx_tile32(d) || (sh.bm == 32 && sh.bn == 32 && tiles < 2LL * num_sms())) {
+    // small square products (recovery, SCF): one wave of 32 x 32 tiles at most, so split K up to 4
     splits = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(4, d.K / (4 * KT))));
   } else if (!(sh.bm == 32 && sh.bn == 32) && tiles < 2LL * num_sms() && d.K >= 8 * KT) {
     splits = static_cast<int>(std::min<int64_t>((target + tiles - 1) / tiles, d.K / (8 * KT)));

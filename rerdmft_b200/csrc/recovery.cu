@@ -315,11 +315,10 @@ int64_t occupied_ct(rr_ri_store* h, const double* X, const double* S, const doub
                     double scale, bool cplx, bool weighted, double* Ct, cudaStream_t s) {
   const int PL = cplx ? 2 : 1;
   if (n_eff == 0) return 0;
-  double *SD, *SDS, *Y, *Pe, *A, *T, *A2, *F, *res;
+  double *SD, *Y, *Pe, *A, *T, *A2, *F, *res;
   int* rank;
   Arena ar(&h->solver_a);
-  ar.request(&SD, n * n * PL);
-  ar.request(&SDS, n * n * PL);
+  ar.request(&SD, n * n_eff * PL);
   ar.request(&Y, n * n_eff * PL);
   ar.request(&Pe, n_eff * n_eff * PL);
   ar.request(&A, n_eff * n_eff * PL);
@@ -335,20 +334,19 @@ int64_t occupied_ct(rr_ri_store* h, const double* X, const double* S, const doub
   h->work.ensure(static_cast<size_t>(std::max<int64_t>(static_cast<int64_t>(h->work.n), 8 * n * n * PL)));
   double* wk = h->work.p;
   const int64_t wcap = static_cast<int64_t>(h->work.n);
-  // P_eff = X^dagger (S D S * scale) X
+  // P_eff = X^dagger (S D S * scale) X = Z^dagger D Z * scale with Z = S X (S is Hermitian): three
+  // products instead of four.
   GemmDesc g;
   g.cplx = cplx;
-  g.M = n; g.N = n; g.K = n;
-  g.A = S; g.lda = n; g.B = Dp; g.ldb = n; g.C = SD; g.ldc = n;
+  g.M = n; g.N = n_eff; g.K = n;
+  g.A = S; g.lda = n; g.B = X; g.ldb = n_eff; g.C = SD; g.ldc = n_eff;  // Z (n x n_eff) in SD
   gemm(g, s, wk, wcap);
-  g.A = SD; g.B = S; g.C = SDS;
-  gemm(g, s, wk, wcap);
-  g.N = n_eff; g.A = SDS; g.B = X; g.ldb = n_eff; g.C = Y; g.ldc = n_eff;
+  g.A = Dp; g.B = SD; g.C = Y;  // Y = D Z
   gemm(g, s, wk, wcap);
   GemmDesc pe;
   pe.cplx = cplx;
   pe.M = n_eff; pe.N = n_eff; pe.K = n;
-  pe.A = X; pe.lda = n_eff; pe.opA = Op::T; pe.conjA = cplx;
+  pe.A = SD; pe.lda = n_eff; pe.opA = Op::T; pe.conjA = cplx;
   pe.B = Y; pe.ldb = n_eff; pe.C = Pe; pe.ldc = n_eff; pe.alpha = scale;
   gemm(pe, s, wk, wcap);
 
