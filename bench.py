@@ -31,7 +31,7 @@ sys.path.insert(0, str(ROOT))
 N_AO, N_AUX, N_OCC, SEED = 400, 1600, 40, 2024
 # DRAM bytes (read + write) of one half-transform launch at this workload, from the ncu capture in
 # profiles/dgemm_half_transform_n400_naux1600_nocc40.md (B read once, T written once).
-HT_TRAFFIC_BYTES = 2.048573e9 + 0.198356e9
+HT_TRAFFIC_BYTES = 2.048888e9 + 0.194917e9
 METRIC = "RI J+K Fock builds/s"
 UNIT = "builds/s"
 

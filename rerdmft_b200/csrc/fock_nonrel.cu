@@ -201,7 +201,6 @@ void coulomb_prep(rr_ri_store* h, const double* Dp, const double* Ct, int64_t no
   double* Drec = h->jscr.p + joff;
   double* mm = h->jscr.p + toff;
   int* flag = reinterpret_cast<int*>(mm + 4);
-  prof_mark(h, 5, s);
   if (nocc > 0 && naux > 0 && have_tgam) {
     GemmDesc g;  // Drec = 2 Ct^T Ct
     g.M = n; g.N = n; g.K = nocc;
@@ -234,6 +233,7 @@ void coulomb_run(rr_ri_store* h, const double* tgam, int tseg, cudaStream_t s_in
     RR_CUDA(cudaEventRecord(c.mid, s_in));
     RR_CUDA(cudaStreamWaitEvent(s, c.mid, 0));
   }
+  prof_mark(h, 5, s);  // J phase = the passes (the preparation overlaps the half-transform)
   j_pass1(jp.pl, jp.gpart, h->status.p, s, jp.flag);
   j_pass2(jp.pl, jp.gpart, jp.jpart, h->status.p, s, tgam, tseg, jp.flag);
   j_finish(jp.pl, jp.jpart, 1.0, s);
