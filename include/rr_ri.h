@@ -166,7 +166,7 @@ typedef struct rr_scf_result {
   int64_t fp64_iterations;  /* Fock builds in FP64 */
   double seconds;           /* wall time of the loop, inputs on the device to density out */
   /* Device time per phase, summed over the iterations (only when rr_ri_set_profiling is on, else 0):
-   * Fock builds (the final FP64 build of a mixed loop not included), energy + DIIS, density step
+   * Fock builds (the final FP64 build of a mixed loop included), energy + DIIS, density step
    * (orthogonal transform, SP2 projector(s), back-transform, density change). */
   double build_ms, diis_ms, density_ms;
 } rr_scf_result;

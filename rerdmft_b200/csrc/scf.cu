@@ -397,6 +397,13 @@ struct PhaseTimer {
       ms[i] += t;
     }
   }
+  // the final FP64 build of a mixed loop (marks 0 and 1 around it, after the stream has passed 1)
+  void accumulate_build() {
+    if (!on) return;
+    float t = 0.f;
+    RR_CUDA(cudaEventElapsedTime(&t, ev[0], ev[1]));
+    ms[0] += t;
+  }
   void store(rr_scf_result* r) const {
     r->build_ms = ms[0];
     r->diis_ms = ms[1];
@@ -760,9 +767,11 @@ void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff
         // last iteration in FP64: the FP64 Fock matrix of the newest density and its energy
         if (mixing_on) axpby(Pn, P, 1.0 - so->mixing, so->mixing, n2, s);
         std::swap(P, Pn);
+        pt.mark(0, s);
         exchange_nonrel(h, Ct, n, false, nocc, K, s, P, J);
         coulomb_join(h, s);
         fock_combine(F, hd, J, K, n2, s);
+        pt.mark(1, s);
         ++n_fp64;
         energy_partial_kernel<1><<<RED_CTAS, 256, 0, s>>>(P, hd, F, n, red);
         RR_LAUNCH_CHECK();
@@ -771,6 +780,7 @@ void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff
         double ev = 0.0;
         RR_CUDA(cudaMemcpyAsync(&ev, scal, sizeof(double), cudaMemcpyDeviceToHost, s));
         RR_CUDA(cudaStreamSynchronize(s));
+        pt.accumulate_build();
         res->electronic_energy = ev;
         if (it < so->max_iterations) {
           ++it;
@@ -994,12 +1004,15 @@ void scf_rel(rr_ri_store* h, int kind, const double* hc, const double* v_total, 
         if (mixing_on) axpby(Pn, P, 1.0 - so->mixing, so->mixing, c2, s);
         have_proj = !mixing_on;
         std::swap(P, Pn);
+        pt.mark(0, s);
         build(nullptr);
+        pt.mark(1, s);
         ++n_fp64;
         energy_of_f();
         double ev = 0.0;
         RR_CUDA(cudaMemcpyAsync(&ev, scal, sizeof(double), cudaMemcpyDeviceToHost, s));
         RR_CUDA(cudaStreamSynchronize(s));
+        pt.accumulate_build();
         res->electronic_energy = ev;
         if (it < so->max_iterations) {
           ++it;
