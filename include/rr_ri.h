@@ -74,7 +74,10 @@ int rr_version(void);
 /* Uploads the (naux, n*n) RI tensor once and keeps it resident in HBM.
  * Replaces constructing RiNonRelEriSource / RiX2cEriSource (src/NON_REL/NonRelFockMatrixRi.h:30,
  * src/X2C_DHF/X2C_FockMatrixRi.h:29): both hold eri3_L of this shape.  mem: RR_MEM_HOST or
- * RR_MEM_DEVICE for B.  The handle binds to the current CUDA device. */
+ * RR_MEM_DEVICE for B.  The handle binds to the current CUDA device.  When every B^P is symmetric
+ * to a few ulps and there is room (at most half of the free device memory), the handle also keeps
+ * the packed upper triangles (naux * n(n+1)/2 doubles) for the Coulomb passes, which then stream
+ * half of B; otherwise J streams B itself. */
 int rr_ri_create(const double* B, int64_t naux, int64_t n, int32_t mem, rr_ri_handle* out);
 
 /* 4-component variant: eri3_LL (naux, nl*nl) and eri3_SS (naux, ns*ns) sharing the aux index
