@@ -249,8 +249,6 @@ void coulomb_after_ht(rr_ri_store* h, const double* Dp, const double* Ct, int64_
 
 void coulomb_join(rr_ri_store* h, cudaStream_t s) { RR_CUDA(cudaStreamWaitEvent(s, h->ctx.join, 0)); }
 
-int64_t occupied_ct(rr_ri_store* h, const double* X, const double* S, const double* Dp, int64_t n, int64_t n_eff,
-                    double scale, bool cplx, bool weighted, double* Ct, cudaStream_t s);
 
 void fock_nonrel(rr_ri_store* h, const double* hc, const double* D, const double* S, const double* X, int64_t n_eff,
                  double* F, const rr_opts* o) {
@@ -277,19 +275,36 @@ void fock_nonrel(rr_ri_store* h, const double* hc, const double* D, const double
   if (!host) { hd = const_cast<double*>(hc); Sd = const_cast<double*>(S); Xd = const_cast<double*>(X); Fd = F; }
 
   prof_mark(h, 0, s);
-  copy_in_padded(Dp, pitch, D, n2, host, s);
+  cudaEvent_t d_ready = nullptr, h_ready = nullptr;
   if (host) {
-    copy_in(hd, hc, n2, true, s);
-    copy_in(Sd, S, n2, true, s);
-    copy_in(Xd, X, n * n_eff, true, s);
+    // Host inputs arrive on the side stream in the order they are read: S and X (the recovery's
+    // first product is S X), then D, then h (read only by the final combine), so the later copies
+    // overlap the recovery.
+    auto& c = h->ctx;
+    RR_CUDA(cudaEventRecord(c.fork, s));
+    RR_CUDA(cudaStreamWaitEvent(c.side, c.fork, 0));
+    copy_in(Sd, S, n2, true, c.side);
+    copy_in(Xd, X, n * n_eff, true, c.side);
+    RR_CUDA(cudaEventRecord(c.upl[0], c.side));
+    copy_in_padded(Dp, pitch, D, n2, true, c.side);
+    RR_CUDA(cudaEventRecord(c.upl[1], c.side));
+    copy_in(hd, hc, n2, true, c.side);
+    RR_CUDA(cudaEventRecord(c.upl[2], c.side));
+    RR_CUDA(cudaStreamWaitEvent(s, c.upl[0], 0));
+    d_ready = c.upl[1];
+    h_ready = c.upl[2];
+  } else {
+    copy_in_padded(Dp, pitch, D, n2, false, s);
   }
   // Occupied recovery (X^T (S D S / 2) X, eigenvalues > 0.5) as c_t = F^T X^T; the exchange queues
   // the Coulomb passes on the side stream after its half-transform.
-  const int64_t nocc = occupied_ct(h, Xd, Sd, Dp, n, n_eff, 0.5, false, false, Ct, s);
+  const int64_t nocc = occupied_ct(h, Xd, Sd, Dp, n, n_eff, 0.5, false, false, Ct, s, d_ready);
+  if (d_ready) RR_CUDA(cudaStreamWaitEvent(s, d_ready, 0));  // (n_eff = 0 skips the products)
   prof_mark(h, 1, s);
   exchange_nonrel(h, Ct, n, false, nocc, K, s, Dp, J);
   prof_mark(h, 3, s);
   coulomb_join(h, s);
+  if (h_ready) RR_CUDA(cudaStreamWaitEvent(s, h_ready, 0));
   fock_combine(Fd, hd, J, K, n2, s);
   if (host) copy_out(F, Fd, n2, true, s);
   prof_mark(h, 4, s);

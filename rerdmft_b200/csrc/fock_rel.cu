@@ -16,8 +16,6 @@
 
 namespace rr {
 
-int64_t occupied_ct(rr_ri_store* h, const double* X, const double* S, const double* Dp, int64_t n, int64_t n_eff,
-                    double scale, bool cplx, bool weighted, double* Ct, cudaStream_t s);
 void projector_ct(rr_ri_store* h, const double* A, const double* Pe, const double* X, int64_t n, int64_t n_eff,
                   int64_t r, bool cplx, double* Ct, cudaStream_t s);
 void prof_mark(rr_ri_store* h, int i, cudaStream_t s);

@@ -310,9 +310,10 @@ void projector_ct(rr_ri_store* h, const double* A, const double* Pe, const doubl
 
 // Recovers c_t (r x n, row-major) from the density.  cplx selects interleaved complex matrices;
 // weighted multiplies the projector by P_eff (sqrt(occupation) weighting of X2C / 4c).
-// Dp: density (n x n, ld n); S (n x n); X (n x n_eff).  Returns r.
+// Dp: density (n x n, ld n); S (n x n); X (n x n_eff).  d_ready (optional): event s waits on
+// before the first product that reads Dp.  Returns r.
 int64_t occupied_ct(rr_ri_store* h, const double* X, const double* S, const double* Dp, int64_t n, int64_t n_eff,
-                    double scale, bool cplx, bool weighted, double* Ct, cudaStream_t s) {
+                    double scale, bool cplx, bool weighted, double* Ct, cudaStream_t s, cudaEvent_t d_ready) {
   const int PL = cplx ? 2 : 1;
   if (n_eff == 0) return 0;
   double *SD, *Y, *Pe, *A, *T, *A2, *F, *res;
@@ -341,6 +342,7 @@ int64_t occupied_ct(rr_ri_store* h, const double* X, const double* S, const doub
   g.M = n; g.N = n_eff; g.K = n;
   g.A = S; g.lda = n; g.B = X; g.ldb = n_eff; g.C = SD; g.ldc = n_eff;  // Z (n x n_eff) in SD
   gemm(g, s, wk, wcap);
+  if (d_ready) RR_CUDA(cudaStreamWaitEvent(s, d_ready, 0));  // D may still be arriving from the host
   g.A = Dp; g.B = SD; g.C = Y;  // Y = D Z
   gemm(g, s, wk, wcap);
   GemmDesc pe;

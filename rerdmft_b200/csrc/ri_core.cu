@@ -32,6 +32,7 @@ void Context::init(cudaStream_t user_stream) {
   RR_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
   RR_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
   RR_CUDA(cudaEventCreateWithFlags(&mid, cudaEventDisableTiming));
+  for (auto& e : upl) RR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   RR_SOLVER(cusolverDnCreate(&solver));
 }
 
@@ -40,6 +41,10 @@ void Context::destroy() {
   if (fork) cudaEventDestroy(fork);
   if (join) cudaEventDestroy(join);
   if (mid) cudaEventDestroy(mid);
+  for (auto& e : upl) {
+    if (e) cudaEventDestroy(e);
+    e = nullptr;
+  }
   if (side) cudaStreamDestroy(side);
   if (own_main && main) cudaStreamDestroy(main);
   solver = nullptr;

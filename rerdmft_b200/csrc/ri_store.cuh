@@ -86,6 +86,10 @@ struct RelBuild {
 };
 
 cudaStream_t call_stream(rr_ri_store* h, const rr_opts* o);
+// Occupied-orbital recovery (recovery.cu): c_t (r x n) from the density; returns r.  d_ready
+// (optional): event s waits on before the first product that reads Dp.
+int64_t occupied_ct(rr_ri_store* h, const double* X, const double* S, const double* Dp, int64_t n, int64_t n_eff,
+                    double scale, bool cplx, bool weighted, double* Ct, cudaStream_t s, cudaEvent_t d_ready = nullptr);
 // Builds h->Bpk[t] from h->B[t] (n x n rows) when it fits; synchronises s.
 void pack_for_j(rr_ri_store* h, int t, int64_t n, cudaStream_t s);
 // JTensor of tensor t (n x n rows) over the packed copy when there is one (D folded into dfold at

@@ -92,6 +92,7 @@ struct Context {
   cudaStream_t side = nullptr;
   bool own_main = false;
   cudaEvent_t fork = nullptr, join = nullptr, mid = nullptr;
+  cudaEvent_t upl[3] = {nullptr, nullptr, nullptr};  // host-input uploads on the side stream
   cusolverDnHandle_t solver = nullptr;
   DevBuf<double> solver_work;
   DevBuf<int> solver_info;
