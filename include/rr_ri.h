@@ -81,7 +81,9 @@ int rr_version(void);
 int rr_ri_create(const double* B, int64_t naux, int64_t n, int32_t mem, rr_ri_handle* out);
 
 /* 4-component variant: eri3_LL (naux, nl*nl) and eri3_SS (naux, ns*ns) sharing the aux index
- * (src/UKB/UkbFockMatrixRi.h:84 RiDirectEriSource). */
+ * (src/UKB/UkbFockMatrixRi.h:84 RiDirectEriSource).  Every B^P is taken to be symmetric, as an RI
+ * tensor is: the relativistic builds write F's lower triangle from its upper one (F Hermitian), so a
+ * B^P with asymmetry d changes F at order d. */
 int rr_ri_create_4c(const double* B_LL, const double* B_SS, int64_t naux, int64_t nl, int64_t ns, int32_t mem,
                     rr_ri_handle* out);
 

@@ -40,6 +40,27 @@ def test_vs_oracle(n, naux, nocc):
     assert np.abs(F - Fo).max() <= TOL
 
 
+@pytest.mark.parametrize("kind", ["exact", "asym"])
+def test_store_symmetry_paths(kind):
+    """The store streams packed upper triangles for J when every B^P is symmetric to a few ulps and
+    the dense tensor otherwise: both agree with the reference formula (J_qa = sum_P gamma_P B^P_qa
+    with the full, possibly non-symmetric, B)."""
+    n, naux, nocc = 33, 97, 5
+    s = synth.nonrel_system(n, naux, nocc, seed=11)
+    Bn = s["B"].reshape(naux, n, n)
+    if kind == "exact":
+        B = 0.5 * (Bn + Bn.transpose(0, 2, 1))
+    else:
+        rng = np.random.default_rng(12)
+        A = rng.standard_normal(Bn.shape)
+        B = Bn + 1e-7 * np.abs(Bn).max() * (A - A.transpose(0, 2, 1))
+    B = np.ascontiguousarray(B.reshape(naux, n * n))
+    src = ri.RiNonRelEriSource(n, B, s["X"], s["S"])
+    F = ri.nonRelFockMatrix(s["h"], src, s["D0"])
+    Fo = o.nonrel_fock(s["h"], B, s["D0"], s["S"], s["X"])
+    assert np.abs(F - Fo).max() <= TOL
+
+
 def test_device_pointers_and_determinism():
     g = golden("nonrel_fock_n24_naux129")
     dev = {k: torch.from_numpy(v).cuda() for k, v in g.items()}

@@ -56,6 +56,23 @@ def test_rkb_vs_oracle(nl, ns, naux, ne):
     assert np.abs(F - Fo).max() <= TOL * max(1.0, np.abs(Fo).max())
 
 
+def test_rkb_one_tensor_packed_one_dense():
+    """Symmetric B_LL (packed J triangles) next to a B_SS whose asymmetry (1e-12 of its largest
+    element) fails the few-ulp symmetry test (dense J passes) in one store: the shared gamma and
+    both J blocks still follow the reference formula.  (A relativistic build forms F's lower
+    triangle from its upper one, so B^P must be symmetric to within the tolerance of the result.)"""
+    nl, ns, naux, ne = 12, 25, 60, 4
+    k = synth.rkb_system(nl, ns, naux, ne, seed=31)
+    rng = np.random.default_rng(32)
+    bss = k["B_SS"].reshape(naux, ns, ns)
+    A = rng.standard_normal(bss.shape)
+    B_SS = np.ascontiguousarray((bss + 1e-12 * np.abs(bss).max() * (A - A.transpose(0, 2, 1))).reshape(naux, ns * ns))
+    src = ri.RiDirectEriSource(nl, ns, k["B_LL"], B_SS, k["v_total"], k["s_full"], k["x_full"])
+    F = ri.rkbFockMatrix(k["h"], src, k["P0"])
+    Fo = o.rkb_fock(k["h"], nl, ns, k["B_LL"], B_SS, k["v_total"], k["s_full"], k["x_full"], k["P0"])
+    assert np.abs(F - Fo).max() <= TOL * max(1.0, np.abs(Fo).max())
+
+
 def test_ukb_device_mode_and_errors():
     g = golden("rkb_fock_nl5_ns9")
     src = ri.RiDirectEriSource(5, 9, g["B_LL"], g["B_SS"], g["v_total"], g["s_full"], g["x_full"])
