@@ -286,7 +286,8 @@ typedef struct rr_x2c_instance {
 } rr_x2c_instance;
 
 /* A batch of independent X2C-HF SCF problems of uneven size (a geometry scan) run concurrently:
- * `workers` host threads take the instances in order, each instance running rr_scf_run_x2c on its
+ * `workers` host threads take the instances largest store first (naux * n^2, the cost of a build),
+ * each instance running rr_scf_run_x2c on its
  * handle's own stream, so the small per-instance kernels of different instances overlap on the
  * GPU.  Host pointers.  Returns RR_OK when every instance succeeded, else the first failing
  * instance's code (all instances run; each reports its own status). */

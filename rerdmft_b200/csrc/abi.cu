@@ -1,5 +1,6 @@
 // extern "C" boundary of librr_ri (declared in include/rr_ri.h).  Every entry point converts
 // rr::Error (and any other exception) into a status code plus rr_last_error().
+#include <algorithm>
 #include <atomic>
 #include <new>
 #include <thread>
@@ -292,12 +293,24 @@ int rr_scf_run_x2c_batch(rr_x2c_instance* instances, int64_t count, const rr_scf
   return api([&] {
     RR_REQUIRE(count >= 0 && (instances || count == 0) && scf, RR_ERR_ARG, "rr_scf_run_x2c_batch: null argument");
     RR_REQUIRE(workers >= 1, RR_ERR_ARG, "rr_scf_run_x2c_batch: workers < 1");
+    // Largest first (by the store's naux * n^2, which sets the cost of a build), so that no large
+    // instance starts last and leaves the other workers idle.
+    std::vector<int64_t> order(static_cast<size_t>(count));
+    std::vector<double> cost(static_cast<size_t>(count), 0.0);
+    for (int64_t i = 0; i < count; ++i) {
+      order[i] = i;
+      if (instances[i].h) {
+        const rr_ri_store* st = instances[i].h;
+        cost[i] = static_cast<double>(st->naux) * static_cast<double>(st->n) * static_cast<double>(st->n);
+      }
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return cost[a] > cost[b]; });
     std::atomic<int64_t> next{0};
     auto work = [&] {
       for (;;) {
-        const int64_t i = next.fetch_add(1);
-        if (i >= count) return;
-        rr_x2c_instance& in = instances[i];
+        const int64_t k = next.fetch_add(1);
+        if (k >= count) return;
+        rr_x2c_instance& in = instances[order[k]];
         in.status = rr_scf_run_x2c(in.h, in.h_x2c, in.X, in.n_eff, in.S, in.P0, in.n_electrons, scf, &in.result,
                                    in.P_out, in.energy_history, nullptr);
       }
