@@ -64,6 +64,27 @@ __global__ void place_block_kernel(double* G, int64_t ntot, int64_t of, int64_t 
   }
 }
 
+// Gauss (3M) planes of one flavour's half-transform T = [Re (kk x fs) | Im (kk x fs)]:
+// minus = Re - Im and plus = Re + Im (either may be null).
+__global__ void plane_pm_kernel(const double* T, int64_t cnt, double* minus, double* plus) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < cnt;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double re = T[i], im = T[cnt + i];
+    if (minus) minus[i] = re - im;
+    if (plus) plus[i] = re + im;
+  }
+}
+
+// 3M combine: Re K = P1 + P2, Im K = P3 - P1 + P2 with P1 in Kre, P2 in K2, P3 in Kim.
+__global__ void combine_3m_kernel(double* Kre, double* Kim, const double* K2, int64_t count) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < count;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double p1 = Kre[i], p2 = K2[i];
+    Kim[i] = Kim[i] - p1 + p2;
+    Kre[i] = p1 + p2;
+  }
+}
+
 // G = -K (count doubles).
 __global__ void neg_copy_kernel(double* G, const double* K, int64_t count) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < count;
@@ -124,8 +145,10 @@ void two_electron_rel(rr_ri_store* h, const Flavours& fl, int64_t ntot, const do
   Arena ar(&h->mats);
   for (int t = 0; t < ntens; ++t) ar.request(&J[t], nt[t] * nt[t]);
   for (int f = 0; f < fl.nf; ++f) ar.request(&Cs[f], 2 * std::max<int64_t>(r, 1) * fl.fs[f]);
+  double* K2;
   ar.request(&Kre, fsmax * fsmax);
   ar.request(&Kim, fsmax * fsmax);
+  ar.request(&K2, fsmax * fsmax);
   ar.commit();
   coulomb_async_multi(h, ntens, Dp, J, s);
   if (rb) {
@@ -149,14 +172,21 @@ void two_electron_rel(rr_ri_store* h, const Flavours& fl, int64_t ntot, const do
   const bool fp64_k = !rb || !rb->mixed;
   double* Gk = rb ? h->inc_k.p : G;  // where the FP64 blocks land
   if (fp64_k) RR_CUDA(cudaMemsetAsync(Gk, 0, sizeof(double) * 2 * ntot * ntot, s));
-  // T planes: flavour f occupies [Re (naux*r*fs) | Im (naux*r*fs)]
-  std::array<double*, 4> T{};
+  // T planes: flavour f occupies [Re (naux*r*fs) | Im (naux*r*fs)]; the off-diagonal blocks (f < u)
+  // use Gauss's three products, with Re - Im of every flavour that is an f and Re + Im of every
+  // flavour that is a u of such a block.
+  std::array<double*, 4> T{}, Tm{}, Tp{};
   int64_t tsize = 0;
   for (int f = 0; f < fl.nf; ++f) tsize += 2 * naux * r * fl.fs[f];
+  for (int f = 0; f < fl.nf; ++f) tsize += (f + 1 < fl.nf ? naux * r * fl.fs[f] : 0) + (f > 0 ? naux * r * fl.fs[f] : 0);
   if (fp64_k && r > 0 && naux > 0) {
     h->T.ensure(static_cast<size_t>(tsize));
     int64_t o = 0;
     for (int f = 0; f < fl.nf; ++f) { T[f] = h->T.p + o; o += 2 * naux * r * fl.fs[f]; }
+    for (int f = 0; f < fl.nf; ++f) {
+      if (f + 1 < fl.nf) { Tm[f] = h->T.p + o; o += naux * r * fl.fs[f]; }
+      if (f > 0) { Tp[f] = h->T.p + o; o += naux * r * fl.fs[f]; }
+    }
     for (int f = 0; f < fl.nf; ++f) {
       split_rows_kernel<<<blocks_for(2 * r * fl.fs[f]), 256, 0, s>>>(Cs[f], Ct, r, ntot, fl.off[f], fl.fs[f]);
       RR_LAUNCH_CHECK();
@@ -170,6 +200,11 @@ void two_electron_rel(rr_ri_store* h, const Flavours& fl, int64_t ntot, const do
       ht.batch = naux;
       gemm(ht, s);
     }
+    for (int f = 0; f < fl.nf && fl.nf > 1; ++f) {
+      const int64_t cnt = naux * r * fl.fs[f];
+      plane_pm_kernel<<<blocks_for(cnt), 256, 0, s>>>(T[f], cnt, Tm[f], Tp[f]);
+      RR_LAUNCH_CHECK();
+    }
   }
   if (fp64_k) prof_mark(h, 2, s);
   for (int f = 0; f < fl.nf && fp64_k; ++f)
@@ -180,17 +215,32 @@ void two_electron_rel(rr_ri_store* h, const Flavours& fl, int64_t ntot, const do
         GemmDesc g;
         g.M = ff; g.N = fu;
         g.opA = Op::T; g.lda = ff; g.ldb = fu; g.ldc = fu;
-        // Re K = [Re; Im]_f^T [Re; Im]_u
-        g.K = 2 * kk; g.A = T[f]; g.B = T[u]; g.C = Kre; g.mirror = f == u ? 1 : 0;
-        int64_t want = gemm_work_doubles(g);
-        h->work.ensure(static_cast<size_t>(std::max<int64_t>(want, 1)));
-        gemm(g, s, h->work.p, static_cast<int64_t>(h->work.n));
-        // Im K = Re_f^T Im_u - Im_f^T Re_u
-        g.K = kk; g.A = T[f]; g.B = T[u] + kk * fu; g.C = Kim; g.alpha = 1.0; g.beta = 0.0;
-        g.mirror = f == u ? -1 : 0;
-        gemm(g, s, h->work.p, static_cast<int64_t>(h->work.n));
-        g.A = T[f] + kk * ff; g.B = T[u]; g.alpha = -1.0; g.beta = 1.0;
-        gemm(g, s, h->work.p, static_cast<int64_t>(h->work.n));
+        if (f == u) {
+          // Hermitian diagonal block, upper tiles: Re K = [Re; Im]^T [Re; Im] (symmetric),
+          // Im K = Re^T Im - Im^T Re (antisymmetric)
+          g.K = 2 * kk; g.A = T[f]; g.B = T[u]; g.C = Kre; g.mirror = 1;
+          int64_t want = gemm_work_doubles(g);
+          h->work.ensure(static_cast<size_t>(std::max<int64_t>(want, 1)));
+          gemm(g, s, h->work.p, static_cast<int64_t>(h->work.n));
+          g.K = kk; g.A = T[f]; g.B = T[u] + kk * fu; g.C = Kim; g.alpha = 1.0; g.beta = 0.0;
+          g.mirror = -1;
+          gemm(g, s, h->work.p, static_cast<int64_t>(h->work.n));
+          g.A = T[f] + kk * ff; g.B = T[u]; g.alpha = -1.0; g.beta = 1.0;
+          gemm(g, s, h->work.p, static_cast<int64_t>(h->work.n));
+        } else {
+          // Gauss: P1 = Re_f^T Re_u, P2 = Im_f^T Im_u, P3 = (Re - Im)_f^T (Re + Im)_u;
+          // Re K = P1 + P2, Im K = P3 - P1 + P2 (three products instead of four)
+          g.K = kk; g.A = T[f]; g.B = T[u]; g.C = Kre;
+          int64_t want = gemm_work_doubles(g);
+          h->work.ensure(static_cast<size_t>(std::max<int64_t>(want, 1)));
+          gemm(g, s, h->work.p, static_cast<int64_t>(h->work.n));
+          g.A = T[f] + kk * ff; g.B = T[u] + kk * fu; g.C = K2;
+          gemm(g, s, h->work.p, static_cast<int64_t>(h->work.n));
+          g.A = Tm[f]; g.B = Tp[u]; g.C = Kim;
+          gemm(g, s, h->work.p, static_cast<int64_t>(h->work.n));
+          combine_3m_kernel<<<blocks_for(ff * fu), 256, 0, s>>>(Kre, Kim, K2, ff * fu);
+          RR_LAUNCH_CHECK();
+        }
       } else {
         RR_CUDA(cudaMemsetAsync(Kre, 0, sizeof(double) * ff * fu, s));
         RR_CUDA(cudaMemsetAsync(Kim, 0, sizeof(double) * ff * fu, s));
