@@ -47,6 +47,8 @@ void j_pass2(const JPlan& plan, const double* gpart, double* jpart, int* err, cu
 // J[t][k] = scale * sum_r jpart[r][t][k]   (fixed order over r)
 void j_finish(const JPlan& plan, const double* jpart, double scale, cudaStream_t s);
 
+// The reference's three-centre tensor is symmetric in its two AO indices
+// (src/AO_ints/ThreeCenterIntegrals.cpp:177-178), so half of each row carries all of it.
 // Packs the upper triangles of the naux n x n rows of B (row pitch `pitch`) into `out`, row pitch
 // pitch_out = round_up(tri_len(n), 32), zero padded.  Every B^P must be symmetric to a few ulps
 // (|B_qa - B_aq| <= 8 eps max(|B_qa|, |B_aq|)): then gamma_P = sum_{q<=a} B^P_qa (D_qa + D_aq [a != q])
