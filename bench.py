@@ -673,8 +673,8 @@ def main():
     ht_flops = 2.0 * N_AUX * N_OCC * N_AO * N_AO
     syrk_flops = 2.0 * N_AUX * N_OCC * N_AO * N_AO
     j_bytes = 2.0 * N_AUX * N_AO * N_AO * 8  # algorithmic: two passes over B
-    # gamma comes from the half-transform epilogue; pass 2 streams the packed upper triangles of B
-    j_bytes_streamed = 1.0 * N_AUX * (-(-(N_AO * (N_AO + 1) // 2) // 32) * 32) * 8
+    # both passes stream the packed upper triangles of B (from the top of the build, beside the recovery)
+    j_bytes_streamed = 2.0 * N_AUX * (-(-(N_AO * (N_AO + 1) // 2) // 32) * 32) * 8
     phases = {k: round(v, 4) for k, v in acc.items()}
     ht_tf = ht_flops / (acc["half_transform_ms"] / 1e3) / 1e12 if acc.get("half_transform_ms") else None
     ex_tf = syrk_flops / (acc["exchange_ms"] / 1e3) / 1e12 if acc.get("exchange_ms") else None
@@ -716,9 +716,9 @@ def main():
         coulomb={"bound": "hbm", "achieved": j_gbs, "peak": hbm_peak, "unit": "GB/s",
                  "frac": (j_gbs / hbm_peak) if j_gbs else None, "peak_source": hbm_src,
                  "algorithmic": "2*naux*n^2*8 bytes per build (two passes over B)",
-                 "streamed": "naux*n(n+1)/2*8 bytes: pass 1 (gamma) comes from the half-transform epilogue when "
-                             "D = 2 C C^T, and pass 2 streams the packed upper triangles of the symmetric B^P; "
-                             "achieved counts the streamed bytes",
+                 "streamed": "2*naux*n(n+1)/2*8 bytes: both passes stream the packed upper triangles of the "
+                             "symmetric B^P, on a side stream from the top of the build (beside the occupied "
+                             "recovery and the half-transform, one CTA per SM); achieved counts the streamed bytes",
                  "algorithmic_rate_gbs": (j_bytes / (acc["coulomb_ms"] / 1e3) / 1e9) if acc.get("coulomb_ms") else None},
         kernels={"half_transform_tflops": ht_tf, "syrk_tflops_full_count": ex_tf},
         phases_ms=phases, clocks=clk, e2e=e2e, gpu_launches=int(launches), cpu_baseline=cpu,

@@ -247,6 +247,27 @@ void coulomb_after_ht(rr_ri_store* h, const double* Dp, const double* Ct, int64_
   coulomb_run(h, tgam, tseg, s);
 }
 
+// Both J passes from the density alone, on the side stream from the current point of s: the
+// drop-in build starts them before the occupied recovery, whose small products leave most of the
+// GPU idle.  Join with coulomb_join.
+void coulomb_early(rr_ri_store* h, const double* Dp, double* J, cudaStream_t s, int ctas_per_sm) {
+  const int64_t n = h->n, naux = h->naux;
+  auto& c = h->ctx;
+  RR_CUDA(cudaEventRecord(c.fork, s));
+  RR_CUDA(cudaStreamWaitEvent(c.side, c.fork, 0));
+  h->dfold.ensure(static_cast<size_t>(tri_len(n) + 1));
+  JTensor t = j_tensor(h, 0, n, Dp, J, 0, c.side);
+  JPlan pl = j_plan(1, &t, naux, ctas_per_sm);
+  const int64_t goff = round_up(pl.gpart_doubles, 32);
+  h->jscr.ensure(static_cast<size_t>(goff + pl.jpart_doubles + 32));
+  prof_mark(h, 5, c.side);
+  j_pass1(pl, h->jscr.p, h->status.p, c.side);
+  j_pass2(pl, h->jscr.p, h->jscr.p + goff, h->status.p, c.side);
+  j_finish(pl, h->jscr.p + goff, 1.0, c.side);
+  prof_mark(h, 6, c.side);
+  RR_CUDA(cudaEventRecord(c.join, c.side));
+}
+
 void coulomb_join(rr_ri_store* h, cudaStream_t s) { RR_CUDA(cudaStreamWaitEvent(s, h->ctx.join, 0)); }
 
 
@@ -278,8 +299,8 @@ void fock_nonrel(rr_ri_store* h, const double* hc, const double* D, const double
   cudaEvent_t d_ready = nullptr, h_ready = nullptr;
   if (host) {
     // Host inputs arrive on the side stream in the order they are read: S and X (the recovery's
-    // first product is S X), then D, then h (read only by the final combine), so the later copies
-    // overlap the recovery.
+    // first product is S X), then D (then the J passes and h, below), so the later copies overlap
+    // the recovery.
     auto& c = h->ctx;
     RR_CUDA(cudaEventRecord(c.fork, s));
     RR_CUDA(cudaStreamWaitEvent(c.side, c.fork, 0));
@@ -288,20 +309,29 @@ void fock_nonrel(rr_ri_store* h, const double* hc, const double* D, const double
     RR_CUDA(cudaEventRecord(c.upl[0], c.side));
     copy_in_padded(Dp, pitch, D, n2, true, c.side);
     RR_CUDA(cudaEventRecord(c.upl[1], c.side));
-    copy_in(hd, hc, n2, true, c.side);
-    RR_CUDA(cudaEventRecord(c.upl[2], c.side));
     RR_CUDA(cudaStreamWaitEvent(s, c.upl[0], 0));
     d_ready = c.upl[1];
-    h_ready = c.upl[2];
   } else {
     copy_in_padded(Dp, pitch, D, n2, false, s);
   }
-  // Occupied recovery (X^T (S D S / 2) X, eigenvalues > 0.5) as c_t = F^T X^T; the exchange queues
-  // the Coulomb passes on the side stream after its half-transform.
+  // J from the density on the side stream (after the upload of D there), beside the occupied
+  // recovery (X^T (S D S / 2) X, eigenvalues > 0.5) as c_t = F^T X^T on s, then the exchange.
+  // One J CTA per SM: it shares the SMs with the recovery and then the half-transform (measured at
+  // cfg 2: 1.67 ms per build with one, 1.70 with two, 1.81 with three).
+  constexpr int j_ctas = 1;
+  if (host) {
+    auto& c = h->ctx;
+    coulomb_early(h, Dp, J, c.side, j_ctas);
+    copy_in(hd, hc, n2, true, c.side);  // read only by the final combine
+    RR_CUDA(cudaEventRecord(c.upl[2], c.side));
+    h_ready = c.upl[2];
+  } else {
+    coulomb_early(h, Dp, J, s, j_ctas);
+  }
   const int64_t nocc = occupied_ct(h, Xd, Sd, Dp, n, n_eff, 0.5, false, false, Ct, s, d_ready);
   if (d_ready) RR_CUDA(cudaStreamWaitEvent(s, d_ready, 0));  // (n_eff = 0 skips the products)
   prof_mark(h, 1, s);
-  exchange_nonrel(h, Ct, n, false, nocc, K, s, Dp, J);
+  exchange_nonrel(h, Ct, n, false, nocc, K, s);
   prof_mark(h, 3, s);
   coulomb_join(h, s);
   if (h_ready) RR_CUDA(cudaStreamWaitEvent(s, h_ready, 0));
