@@ -471,6 +471,7 @@ def run_case(args):
                   nocc=40 (rr_ri_jk_occupied, RR_PREC_MIXED; J stays FP64);
     rkb_mixed     the 4c RKB Fock build of the Kramers-restricted DHF shapes with the split-BF16 exchange,
                   full then incremental (nl=200, ns=600, naux=1000, 40 spinors);
+    rkb_fp64      the same 4c RKB Fock build in FP64 (the 4c Fock-build workload of the bench line);
     x2c_mixed     the X2C Fock build with the split-BF16 exchange, full then incremental (nl=200,
                   naux=1000, 80 electrons)."""
     import ctypes
@@ -517,7 +518,7 @@ def run_case(args):
                                                              K.data_ptr(), ctypes.byref(o))), args.steps, args.warmup)
             out.update(workload=f"split-BF16 J/K n={N_AO} naux={N_AUX} nocc={N_OCC}", ms_per_call=ms)
         store.sync()
-    elif args.case == "rkb_mixed":
+    elif args.case in ("rkb_mixed", "rkb_fp64"):
         s = synth.rkb_system(NL4, NS4, NAUX4, 2 * (NOCC4 // 2), seed=SEED + 11, box=20.0)
         dev = {k: torch.from_numpy(np.ascontiguousarray(s[k])).cuda()
                for k in ("B_LL", "B_SS", "v_total", "s_full", "x_full", "h", "P0")}
@@ -533,10 +534,18 @@ def run_case(args):
                                        dev["s_full"].data_ptr(), x.data_ptr(), x.shape[1], dev["P0"].data_ptr(),
                                        F.data_ptr(), ctypes.byref(o)))
 
-        full = timed(lambda: step(0), args.steps, args.warmup)
-        incr = timed(lambda: step(1), args.steps, args.warmup)
-        out.update(workload=f"mixed rkbFockMatrix nl={NL4} ns={NS4} naux={NAUX4} nocc={NOCC4}", ms_full=full,
-                   ms_incremental=incr)
+        if args.case == "rkb_fp64":
+            o64 = L.opts(L.RR_MEM_DEVICE, stream=stream, sync=0)
+            ms = timed(lambda: L.check(lib.rr_ri_fock_rkb(store.handle, dev["h"].data_ptr(), dev["v_total"].data_ptr(),
+                                                          n_rkb, dev["s_full"].data_ptr(), x.data_ptr(), x.shape[1],
+                                                          dev["P0"].data_ptr(), F.data_ptr(), ctypes.byref(o64))),
+                       args.steps, args.warmup)
+            out.update(workload=f"FP64 rkbFockMatrix nl={NL4} ns={NS4} naux={NAUX4} nocc={NOCC4}", ms_per_build=ms)
+        else:
+            full = timed(lambda: step(0), args.steps, args.warmup)
+            incr = timed(lambda: step(1), args.steps, args.warmup)
+            out.update(workload=f"mixed rkbFockMatrix nl={NL4} ns={NS4} naux={NAUX4} nocc={NOCC4}", ms_full=full,
+                       ms_incremental=incr)
         store.sync()
     elif args.case == "x2c_mixed":
         s = synth.x2c_system(X2C_NL, X2C_NAUX, X2C_NE, seed=SEED + 21, box=20.0, gap=X2C_GAP)
@@ -566,7 +575,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", default=None, choices=["headline", "mixed_exchange", "rkb_mixed", "x2c_mixed"],
+    ap.add_argument("--case", default=None, choices=["headline", "mixed_exchange", "rkb_mixed", "rkb_fp64", "x2c_mixed"],
                     help="run one workload for profiling instead of the bench line")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)

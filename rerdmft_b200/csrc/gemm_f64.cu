@@ -364,12 +364,22 @@ bool use_tile80(int64_t M, int64_t N, int64_t K) {
   return K >= 8192 && p80 < p64;
 }
 
+// Batched half-transforms of 49..128 coefficient rows (the relativistic [Re; Im] rows, 2 r = 80 at
+// 40 spinors): the batch fills the GPU at any tile size, so the tile that pads M x N least wins;
+// 80 x 80 when it pads less than 64 x 64 and 32 x 32 (80 x 600: 80 x 640 instead of 128 x 640).
+bool batched_tile80(int64_t M, int64_t N, int64_t batch) {
+  if (M <= 48 || M > 128 || batch < num_sms()) return false;
+  auto pad = [&](int64_t t) { return static_cast<int64_t>(ceil_div(M, t)) * t * ceil_div(N, t) * t; };
+  return pad(80) < pad(64) && pad(80) < pad(32);
+}
+
 // Small square products (SP2 purification, DIIS, recovery at n <= 512): 32 x 32 tiles without
 // split-K: more CTAs and no reduction launch; measured 14 us instead of 20 us at n = 400.
 bool use_tile32(int64_t M, int64_t N, int64_t K) { return M > 48 && M <= 512 && N <= 512 && K <= 2048; }
 
 template <bool AK, bool BKM>
 void launch_real(const Params& p, dim3 grid, cudaStream_t s) {
+  if (batched_tile80(p.M, p.N, p.batch)) return launch_cfg<5, 5, 2, 2, AK, BKM, false>(p, grid, s);
   if (use_tile32(p.M, p.N, p.K)) return launch_cfg<2, 2, 2, 2, AK, BKM, false>(p, grid, s);
   if (p.M <= 48) {
     switch ((p.M + 7) / 8) {
@@ -392,6 +402,7 @@ bool cplx_tile32(const GemmDesc& d) { return d.cplx && d.M <= 1024 && d.N <= 102
 Shape pick_shape(const GemmDesc& d) {
   if (cplx_tile32(d)) return {32, 32};
   if (d.cplx) return {32, 64};
+  if (batched_tile80(d.M, d.N, d.batch)) return {80, 80};
   if (use_tile32(d.M, d.N, d.K)) return {32, 32};
   // 33..40 rows (the half-transform at 40 occupied orbitals): 40 x 80 tiles of five 40 x 16 warps,
   // measured 847 instead of 901 us at n = 400, naux = 1600 (80 divides typical n exactly).
