@@ -175,6 +175,7 @@ int rr_ri_destroy(rr_ri_handle h) {
     cudaDeviceSynchronize();
     for (auto& e : h->ev)
       if (e) cudaEventDestroy(e);
+    if (h->wait_ev) cudaEventDestroy(h->wait_ev);
     h->ctx.destroy();
     delete h;
   });
@@ -316,10 +317,20 @@ int rr_scf_run_x2c_batch(rr_x2c_instance* instances, int64_t count, const rr_scf
       }
     };
     const int nw = static_cast<int>(std::min<int64_t>(workers, std::max<int64_t>(count, 1)));
+    // With several workers the SCF host waits sleep instead of spinning (the threads would otherwise
+    // compete for the host cores while their GPU work runs); restored afterwards.
+    std::vector<char> was(static_cast<size_t>(count), 0);
+    for (int64_t i = 0; i < count; ++i)
+      if (instances[i].h) {
+        was[i] = instances[i].h->blocking_wait ? 1 : 0;
+        instances[i].h->blocking_wait = nw > 1;
+      }
     std::vector<std::thread> pool;
     for (int w = 1; w < nw; ++w) pool.emplace_back(work);
     work();
     for (auto& t : pool) t.join();
+    for (int64_t i = 0; i < count; ++i)
+      if (instances[i].h) instances[i].h->blocking_wait = was[i] != 0;
     for (int64_t i = 0; i < count; ++i)
       if (instances[i].status != RR_OK)
         throw rr::Error(instances[i].status, "rr_scf_run_x2c_batch: instance " + std::to_string(i) + " failed");

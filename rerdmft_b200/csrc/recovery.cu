@@ -371,7 +371,7 @@ int64_t occupied_ct(rr_ri_store* h, const double* X, const double* S, const doub
     else ns_residual_kernel<1><<<static_cast<int>(std::min<int64_t>(n_eff, 592)), 256, 0, s>>>(T, A, n_eff, res);
     RR_LAUNCH_CHECK();
     RR_CUDA(cudaMemcpyAsync(hres, res, 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
-    RR_CUDA(cudaStreamSynchronize(s));
+    host_wait(h, s);
     if (it == 0 && hres[1] > 2.5) {
       // ||A||_2 <= sqrt(||A^2||_inf): scale into the convergence region of the iteration
       axpby(A, A, 0.0, 1.0 / std::sqrt(hres[1]), n_eff * n_eff * PL, s);

@@ -64,11 +64,21 @@ void prof_mark(rr_ri_store* h, int i, cudaStream_t s) {
   h->ev_used[i] = true;
 }
 
+void host_wait(rr_ri_store* h, cudaStream_t s) {
+  if (h && h->blocking_wait) {
+    if (!h->wait_ev) RR_CUDA(cudaEventCreateWithFlags(&h->wait_ev, cudaEventBlockingSync | cudaEventDisableTiming));
+    RR_CUDA(cudaEventRecord(h->wait_ev, s));
+    RR_CUDA(cudaEventSynchronize(h->wait_ev));
+  } else {
+    RR_CUDA(cudaStreamSynchronize(s));
+  }
+}
+
 void check_status(rr_ri_store* h, cudaStream_t s) {
   // word 0: bounded-wait expiries (TMA pipelines); word 1: numerical failures (recovery Cholesky)
   int word[2] = {0, 0};
   RR_CUDA(cudaMemcpyAsync(word, h->status.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
-  RR_CUDA(cudaStreamSynchronize(s));
+  host_wait(h, s);
   if (word[0] != 0 || word[1] != 0) {
     RR_CUDA(cudaMemsetAsync(h->status.p, 0, 2 * sizeof(int), s));
     RR_CUDA(cudaStreamSynchronize(s));

@@ -33,6 +33,10 @@ struct rr_ri_store {
   } jpend;
   rr::DevBuf<double> tgam;  // gamma partials from the half-transform epilogue
   rr::DevBuf<double> solver_a;  // eigen-problem matrix / eigenvectors
+  // SCF loop state (matrices, DIIS history), grown on demand and kept with the handle, so that
+  // repeated SCF runs allocate nothing (a cudaFree would synchronise the whole device, and with
+  // it every other thread's handle).
+  rr::DevBuf<double> scf_buf, diis_err, diis_val, diis_dots;
   rr::DevBuf<double> solver_w;  // eigenvalues
   std::vector<double> host_w;
   // Split-BF16 copies of B[t] for RR_PREC_MIXED (built on first use) and their call scratch.
@@ -43,6 +47,10 @@ struct rr_ri_store {
   // inc_ld entries).
   rr::DevBuf<double> inc_k, inc_ct;
   int64_t inc_r = -1, inc_ld = 0;
+  // Host waits of the SCF loops: blocking (the waiting thread sleeps on an event) when many host
+  // threads drive handles at once (rr_scf_run_x2c_batch), spinning stream syncs otherwise.
+  bool blocking_wait = false;
+  cudaEvent_t wait_ev = nullptr;
   // Profiling events: 0 start, 1 recovery done, 2 half-transform done, 3 exchange done, 4 end
   // (main stream); 5 J start, 6 J end (side stream).
   bool profiling = false;
@@ -101,6 +109,8 @@ int64_t launches();
 void sp2_projector(rr_ri_store* h, const double* F, int64_t n, int64_t nocc, double* Pi, double* T, double* scal,
                    cudaStream_t s, bool cplx = false);
 void check_status(rr_ri_store* h, cudaStream_t s);  // syncs s, throws RR_ERR_TIMEOUT on a set word
+// Waits on the host for everything queued on s (see rr_ri_store::blocking_wait).
+void host_wait(rr_ri_store* h, cudaStream_t s);
 void copy_in(double* dst, const double* src, int64_t count, bool host, cudaStream_t s);
 void copy_out(double* dst, const double* src, int64_t count, bool host, cudaStream_t s);
 // Pitched copy of a flat n2-vector into a zero-padded buffer of `pitch` doubles.

@@ -305,18 +305,22 @@ bool solve_dense(std::vector<double> m, std::vector<double> rhs, size_t n, doubl
 // Device-resident DIIS history (src/Utils/DIIS.cpp:79-131): slots hold (error, value) pairs; the
 // newest-first order and the B matrix are kept on the host.
 struct DeviceDiis {
+  rr_ri_store* h;  // owns the history buffers; also for host_wait
   int max_vectors = 0;
   int64_t len = 0;
-  DevBuf<double> err, val, dots;
+  DevBuf<double>& err;
+  DevBuf<double>& val;
+  DevBuf<double>& dots;
   std::vector<int> order;  // slot indices, newest first
   std::vector<std::vector<double>> bmat;  // bmat[slot][slot]
+  explicit DeviceDiis(rr_ri_store* owner) : h(owner), err(owner->diis_err), val(owner->diis_val), dots(owner->diis_dots) {}
   void init(int maxv, int64_t length) {
     max_vectors = maxv;
     len = length;
     const int slots = std::max(maxv, 1);
-    err.alloc(static_cast<size_t>(slots * length));
-    val.alloc(static_cast<size_t>(slots * length));
-    dots.alloc(DIIS_MAX * (RED_CTAS + 1));
+    err.ensure(static_cast<size_t>(slots * length));
+    val.ensure(static_cast<size_t>(slots * length));
+    dots.ensure(DIIS_MAX * (RED_CTAS + 1));
     order.clear();
     bmat.assign(slots, std::vector<double>(slots, 0.0));
   }
@@ -346,7 +350,7 @@ struct DeviceDiis {
     RR_LAUNCH_CHECK();
     std::vector<double> d(a.count);
     RR_CUDA(cudaMemcpyAsync(d.data(), dots.p, sizeof(double) * a.count, cudaMemcpyDeviceToHost, s));
-    RR_CUDA(cudaStreamSynchronize(s));
+    host_wait(h, s);
     for (int k = 0; k < a.count; ++k) bmat[slot][order[k]] = bmat[order[k]][slot] = d[k];
     const size_t total = order.size();
     for (size_t m = total; m >= 2; --m) {
@@ -595,7 +599,7 @@ void sp2_projector(rr_ri_store* h, const double* F, int64_t n, int64_t nocc, dou
     if (it % 4 == 3) {
       double tr[2];
       RR_CUDA(cudaMemcpyAsync(tr, scal + 2, sizeof(tr), cudaMemcpyDeviceToHost, s));
-      RR_CUDA(cudaStreamSynchronize(s));
+      host_wait(h, s);
       // idempotency measure of the pre-update X: |tr X - tr X^2| (sum of lambda (1 - lambda))
       if (std::fabs(tr[0] - tr[1]) < 1e-11 * std::max<double>(1.0, N) && std::fabs(tr[0] - N) < 1e-6) return;
       // With every eigenvalue of X in [0, 1], tr X^2 <= tr X; otherwise the Ritz interval missed part
@@ -624,8 +628,7 @@ void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff
   cudaStream_t s = call_stream(h, o);
   const auto t_start = std::chrono::steady_clock::now();
   const int64_t pitch = round_up(std::max<int64_t>(n2, 2), 32);
-  DevBuf<double> buf;
-  Arena ar(&buf);
+  Arena ar(&h->scf_buf);
   double *hd, *Xd, *Sd, *P, *Pn, *F, *J, *K, *Fs, *e, *PS, *SP, *tmp, *Fo, *Pi, *T2, *Ct, *scal, *red;
   ar.request(&hd, n2);
   ar.request(&Xd, n * n_eff);
@@ -659,7 +662,7 @@ void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff
   const bool mixed = so->precision == RR_PREC_MIXED;
   bool reseed = false, reseeded = false;
   h->inc_r = -1;
-  DeviceDiis diis;
+  DeviceDiis diis(h);
   const bool use_diis = so->diis_size >= 2;
   diis.init(use_diis ? so->diis_size : 0, n2);
   RR_REQUIRE(so->diis_size <= DIIS_MAX, RR_ERR_ARG, "rr_scf_run_nonrel: diis_size too large");
@@ -754,7 +757,7 @@ void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff
     pt.mark(3, s);
     double hv[2];
     RR_CUDA(cudaMemcpyAsync(hv, scal, sizeof(hv), cudaMemcpyDeviceToHost, s));
-    RR_CUDA(cudaStreamSynchronize(s));
+    host_wait(h, s);
     pt.accumulate();
     const double energy = hv[0], dP = hv[1], dE = std::fabs(energy - prev);
     if (hist) hist[it - 1] = energy;
@@ -779,7 +782,7 @@ void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff
         RR_LAUNCH_CHECK();
         double ev = 0.0;
         RR_CUDA(cudaMemcpyAsync(&ev, scal, sizeof(double), cudaMemcpyDeviceToHost, s));
-        RR_CUDA(cudaStreamSynchronize(s));
+        host_wait(h, s);
         pt.accumulate_build();
         res->electronic_energy = ev;
         if (it < so->max_iterations) {
@@ -800,7 +803,7 @@ void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff
   if (it > so->max_iterations) it = so->max_iterations;
   check_status(h, s);
   copy_out(P_out, P, n2, host, s);
-  RR_CUDA(cudaStreamSynchronize(s));
+  host_wait(h, s);
   res->iterations = it;
   res->converged = converged ? 1 : 0;
   res->mixed_iterations = n_mixed;
@@ -828,8 +831,7 @@ void scf_rel(rr_ri_store* h, int kind, const double* hc, const double* v_total, 
   cudaStream_t s = call_stream(h, o);
   const auto t_start = std::chrono::steady_clock::now();
   const int64_t nu = dhf ? 2 * h->n + 2 * h->ns : 0;
-  DevBuf<double> buf;
-  Arena ar(&buf);
+  Arena ar(&h->scf_buf);
   double *hd, *Xd, *Sd, *vd = nullptr, *P, *Pn, *F, *Fs, *e, *PS, *SP, *tmp, *Fo, *Pi, *Pi2, *T2, *scal, *red;
   ar.request(&hd, c2);
   ar.request(&Xd, ce);
@@ -863,7 +865,7 @@ void scf_rel(rr_ri_store* h, int kind, const double* hc, const double* v_total, 
   } else {
     copy_in(P, P0, c2, host, s);
   }
-  DeviceDiis diis;
+  DeviceDiis diis(h);
   const bool use_diis = so->diis_size >= 2;
   RR_REQUIRE(so->diis_size <= DIIS_MAX, RR_ERR_ARG, "SCF: diis_size too large");
   diis.init(use_diis ? so->diis_size : 0, c2);
@@ -963,7 +965,7 @@ void scf_rel(rr_ri_store* h, int kind, const double* hc, const double* v_total, 
       RR_LAUNCH_CHECK();
       double leak = 0.0;
       RR_CUDA(cudaMemcpyAsync(&leak, scal + 16, sizeof(double), cudaMemcpyDeviceToHost, s));
-      RR_CUDA(cudaStreamSynchronize(s));
+      host_wait(h, s);
       if (!(std::fabs(leak) < 1e-6)) {
         sp2_projector(h, tmp, n_eff, nlo + n_electrons, Pi, T2, scal + 8, s, true);
         axpby(Pi, Pi2, -1.0, 1.0, ee, s);
@@ -991,7 +993,7 @@ void scf_rel(rr_ri_store* h, int kind, const double* hc, const double* v_total, 
     pt.mark(3, s);
     double hv[2];
     RR_CUDA(cudaMemcpyAsync(hv, scal, sizeof(hv), cudaMemcpyDeviceToHost, s));
-    RR_CUDA(cudaStreamSynchronize(s));
+    host_wait(h, s);
     pt.accumulate();
     const double energy = hv[0], dP = hv[1], dE = std::fabs(energy - prev);
     if (hist) hist[it - 1] = energy;
@@ -1011,7 +1013,7 @@ void scf_rel(rr_ri_store* h, int kind, const double* hc, const double* v_total, 
         energy_of_f();
         double ev = 0.0;
         RR_CUDA(cudaMemcpyAsync(&ev, scal, sizeof(double), cudaMemcpyDeviceToHost, s));
-        RR_CUDA(cudaStreamSynchronize(s));
+        host_wait(h, s);
         pt.accumulate_build();
         res->electronic_energy = ev;
         if (it < so->max_iterations) {
@@ -1030,7 +1032,7 @@ void scf_rel(rr_ri_store* h, int kind, const double* hc, const double* v_total, 
   if (it > so->max_iterations) it = so->max_iterations;
   check_status(h, s);
   copy_out(P_out, P, c2, host, s);
-  RR_CUDA(cudaStreamSynchronize(s));
+  host_wait(h, s);
   res->iterations = it;
   res->converged = converged ? 1 : 0;
   res->mixed_iterations = n_mixed;
