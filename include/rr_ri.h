@@ -18,6 +18,9 @@
  *    the same condition returns RR_ERR_ARG.  No C++ exception crosses this boundary.
  *  - Pointer arguments live in host memory unless rr_opts.mem == RR_MEM_DEVICE (then they are
  *    device pointers on the handle's device).  Host outputs are complete on return.
+ *  - A handle keeps its scratch (and the SCF loops' state) between calls, so one handle serves one
+ *    call at a time; different handles may be used from different host threads at once (as
+ *    rr_scf_run_x2c_batch does).
  */
 #ifndef RR_RI_H
 #define RR_RI_H

@@ -92,7 +92,15 @@ void pack_for_j(rr_ri_store* h, int t, int64_t n, cudaStream_t s) {
   RR_CUDA(cudaMemGetInfo(&free_b, &total_b));
   const double bytes = 8.0 * static_cast<double>(h->naux) * static_cast<double>(round_up(tri_len(n), 32));
   if (bytes > 0.5 * static_cast<double>(free_b)) return;
-  j_pack_upper(h->B[t].p, h->pitch[t], h->naux, n, h->Bpk[t], h->pitch_pk[t], s);
+  try {
+    j_pack_upper(h->B[t].p, h->pitch[t], h->naux, n, h->Bpk[t], h->pitch_pk[t], s);
+  } catch (const Error& e) {
+    if (e.code != RR_ERR_CUDA) throw;
+    // the packed copy is optional: without it J streams B itself (an out-of-memory is not sticky)
+    cudaGetLastError();
+    h->Bpk[t].release();
+    h->pitch_pk[t] = 0;
+  }
 }
 
 JTensor j_tensor(rr_ri_store* h, int t, int64_t n, const double* D, double* J, int64_t doff, cudaStream_t s) {
