@@ -127,7 +127,7 @@ def orbital_optimization_block():
     the shipped learned preconditioner: a LiH-sized system (11 spatial orbitals, naux 48; two seeds
     standing in for the 1.6 / 4.0 Angstrom geometries) and a synthetic one with 120 spatial orbitals
     (naux 480), iterations and wall time to |dE| < 1e-8 Ha between macro-iterations.  The learned
-    runs finish with plain ADAM (polish), so both energies are judged by the plain method; their
+    runs finish with plain ADAM (polish), so both energies come from the plain method; their
     macro-iteration counts include the polishing runs."""
     from rerdmft_b200 import orbopt, synth
 

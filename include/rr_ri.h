@@ -38,7 +38,7 @@ extern "C" {
 #define RR_ERR_TIMEOUT 4     /* a bounded device-side wait expired (kernel status word) */
 #define RR_ERR_NOMEM 5       /* device allocation failed */
 #define RR_ERR_STATE 6       /* handle in the wrong state for this call */
-#define RR_ERR_UNSUPPORTED 7 /* option not supported by this build */
+#define RR_ERR_UNSUPPORTED 7 /* option not supported by the library */
 
 #define RR_MEM_HOST 0
 #define RR_MEM_DEVICE 1

@@ -212,7 +212,7 @@ def run_full_optimization(problem: RotationProblem, tol: float = 1e-8, max_macro
     two successive runs' best energies differ by less than `tol` and the optimiser asked for no
     restart.  With a preconditioner (or exact_hessian) the pair scales are refreshed before every
     run from the current orbitals; with `polish` the plain method then continues from the
-    preconditioned result until it meets the same rule, so plain ADAM judges the converged energy
+    preconditioned result until it meets the same rule, so plain ADAM settles the converged energy
     (the rescaled runs only move the start).  Iterations of both phases are counted.  The scales use the
     90th percentile of the (predicted) curvature as reference (hessian_scales): on the synthetic
     functional-stage problems the median reference saved 19 % of the macro-iterations, the 90th
