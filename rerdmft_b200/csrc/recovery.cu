@@ -7,7 +7,7 @@
 // so any factor F with F F^dagger = W gives the same K.  Here:
 //   1. Pi = step(P_eff - 1/2), the spectral projector onto eigenvalues > 1/2, by the Newton-Schulz
 //      sign iteration A <- A (3 - A^2)/2 on A = 2 P_eff - 1 (FP64 DMMA GEMMs only; for an
-//      idempotent density A^2 = 1 already and one refinement step is all that runs);
+//      idempotent density A^2 = 1 already to rounding and the iteration stops at its first check);
 //   2. W = Pi (NON_REL) or Pi P_eff Pi (weighted);
 //   3. an orthonormal basis Q of range(Pi) (rank r = trace Pi = number of eigenvalues > 1/2) by
 //      CholeskyQR2 of Pi G for a fixed pseudo-random G (deterministic), and F = Q for NON_REL or
@@ -377,7 +377,9 @@ int64_t occupied_ct(rr_ri_store* h, const double* X, const double* S, const doub
       axpby(A, A, 0.0, 1.0 / std::sqrt(hres[1]), n_eff * n_eff * PL, s);
       continue;
     }
-    // A <- 1.5 A - 0.5 A T (always at least one refinement step)
+    // A density that is a projector to rounding (an SCF density) gives A^2 = I already: A is the
+    // sign, and a refinement would only move it by rounding.  Otherwise A <- 1.5 A - 0.5 A T.
+    if (hres[0] < 1e-13) { converged = true; break; }
     sq.A = A; sq.B = T; sq.C = A2; sq.alpha = 1.0;
     gemm(sq, s, wk, wcap);
     axpby(A, A2, -0.5, 1.5, n_eff * n_eff * PL, s);
