@@ -414,8 +414,10 @@ Shape pick_shape(const GemmDesc& d) {
 int pick_splits(const GemmDesc& d, Shape sh, int64_t* kchunk) {
   int64_t tiles = static_cast<int64_t>(ceil_div(d.M, sh.bm)) * ceil_div(d.N, sh.bn) * d.batch;
   if (d.mirror) tiles = (tiles + ceil_div(d.M, sh.bm) * d.batch) / 2;
-  // Enough CTAs for several waves (load balance across SMs), K chunks of at least 128.
-  const int64_t target = 8LL * num_sms();
+  // Enough CTAs for several waves (load balance across SMs), K chunks of at least 128: eight waves
+  // for upper-tile products (the exchange SYRK: 4 or 16 measured slower), sixteen for full ones
+  // (the 4c exchange blocks: 24.3 -> 23.5 ms per build against eight).
+  const int64_t target = (d.mirror ? 8LL : 16LL) * num_sms();
   int splits = 1;
   if (cplx_tile32(d) || (sh.bm == 32 && sh.bn == 32 && tiles < 2LL * num_sms())) {
     // small square products (recovery, SCF): one wave of 32 x 32 tiles at most, so split K up to 4
