@@ -28,18 +28,19 @@ void density_from_occupied(double* Dp, const double* C, int64_t n, int64_t nocc,
 
 }  // namespace
 
-// Exchange K' = sum_P (Ct B^P)^T (Ct B^P) for a given Ct (nocc x n, row-major with leading
-// dimension ldct, or its transpose when ct_transposed: Ct = C^T with C stored n x nocc).
+// The Coulomb passes of the nonrelativistic builds (defined below).
 void coulomb_after_ht(rr_ri_store* h, const double* Dp, const double* Ct, int64_t nocc, double* J,
                       const double* tgam, int tseg, cudaStream_t s);
 void coulomb_prep(rr_ri_store* h, const double* Dp, const double* Ct, int64_t nocc, double* J, bool have_tgam,
                   cudaStream_t s, bool overlap);
 void coulomb_run(rr_ri_store* h, const double* tgam, int tseg, cudaStream_t s);
 
-// With Dp given, the Coulomb matrix J (from the pitched density Dp) is prepared on the side stream
-// beside the half-transform and streamed beside the SYRK (coulomb_prep / coulomb_run); it lands in
-// Jout; join with coulomb_join.
-// The exchange reads c_t as Ct (nocc x n, ld ldct) or, when ct_transposed, as C^T of C (n x ldct).
+// Exchange K' = sum_P (Ct B^P)^T (Ct B^P) for a given Ct (nocc x n, row-major with leading
+// dimension ldct, or its transpose when ct_transposed: Ct = C^T with C stored n x nocc).
+// With Dp given (the SCF loop's FP64 build), the Coulomb matrix J of the pitched density Dp is
+// prepared on the side stream beside the half-transform and streamed beside the SYRK
+// (coulomb_prep / coulomb_run, gamma from the half-transform epilogue); it lands in Jout; join with
+// coulomb_join.  The drop-in build starts its J passes itself (coulomb_early) and passes no Dp.
 void exchange_nonrel(rr_ri_store* h, const double* Ct, int64_t ldct, bool ct_transposed, int64_t nocc, double* K,
                      cudaStream_t s, const double* Dp = nullptr, double* Jout = nullptr) {
   const int64_t n = h->n, naux = h->naux;
