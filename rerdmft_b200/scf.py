@@ -109,9 +109,11 @@ def runX2CHartreeFockScfBatch(problems, workers: int = 16, diis_size: int = 5, m
                               kramers_restricted: bool = True, precision: str = "fp64",
                               mixed_switch: float = 0.0) -> list:
     """A batch of independent X2C-HF problems (a geometry scan of uneven sizes) run concurrently
-    (rr_scf_run_x2c_batch: `workers` host threads, one stream per problem's handle).  Each problem is
-    a dict with eri (RiX2cEriSource), h_x2c, x_large, initial_density, n_electrons and optionally
-    overlap.  Returns one result dict per problem, as runX2CHartreeFockScf."""
+    (rr_scf_run_x2c_batch: `workers` host threads take the problems largest store first, one stream
+    per problem's handle; with more than one worker the host waits sleep instead of spinning).  Each
+    problem is a dict with eri (RiX2cEriSource), h_x2c, x_large, initial_density, n_electrons and
+    optionally overlap; each needs its own handle.  Returns one result dict per problem, as
+    runX2CHartreeFockScf."""
     keep, insts = [], (L.X2cInstance * len(problems))()
     outs = []
     for i, pr in enumerate(problems):
