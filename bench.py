@@ -36,6 +36,23 @@ METRIC = "RI J+K Fock builds/s"
 UNIT = "builds/s"
 
 
+def bench_config(world_size: int) -> dict:
+    """The workload description both arms print (the GPU arm and --impl reference)."""
+    return {"workload": f"nonrel RI J+K Fock build n={N_AO} naux={N_AUX} nocc={N_OCC} (FP64, occupied recovery "
+                        f"included)", "parallelism": f"replicas x{world_size}", "precision": "fp64",
+            "l2": "inputs larger than L2 (B = 2.05 GB)"}
+
+
+def cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def make_inputs():
     from rerdmft_b200 import synth
 
@@ -113,10 +130,13 @@ def rkb_fock_times(torch, fp64_peak, want_cpu: bool, steps: int = 10):
         if ref.available():
             ref.set_threads(os.cpu_count() or 1)
             t0 = time.perf_counter()
-            ref.rkb_fock(s["h"], NL4, NS4, s["B_LL"], s["B_SS"], s["v_total"], s["s_full"], s["x_full"], s["P0"])
+            F_ref = ref.rkb_fock(s["h"], NL4, NS4, s["B_LL"], s["B_SS"], s["v_total"], s["s_full"], s["x_full"],
+                                 s["P0"])
             dt = time.perf_counter() - t0
-            out["reference_cpu"] = dict(seconds_per_build=dt, cores=os.cpu_count() or 1,
+            out["reference_cpu"] = dict(seconds_per_build=dt, cores=os.cpu_count() or 1, cpu_model=cpu_model(),
                                         sample="one full-size call of the reference rkbFockMatrix")
+            out["parity"] = dict(max_abs_F_minus_reference=float(np.abs(F.cpu().numpy() - F_ref).max()),
+                                 tolerance=1e-10, inputs="the timed build's inputs")
     del dev, src, store, F
     torch.cuda.empty_cache()
     return out
@@ -414,11 +434,11 @@ def cpu_reference_rate(inp, seconds: float = 15.0):
     from oracle import ref
 
     if not ref.available():
-        return None
+        return None, None
     cores = os.cpu_count() or 1
     ref.set_threads(cores)
     t0 = time.perf_counter()
-    ref.nonrel_fock(inp["h"], inp["B"], inp["D"], inp["S"], inp["X"])
+    F_ref = ref.nonrel_fock(inp["h"], inp["B"], inp["D"], inp["S"], inp["X"])
     first = time.perf_counter() - t0
     reps = max(1, min(20, int(seconds / max(first, 1e-3))))
     best = first
@@ -426,18 +446,16 @@ def cpu_reference_rate(inp, seconds: float = 15.0):
         t0 = time.perf_counter()
         ref.nonrel_fock(inp["h"], inp["B"], inp["D"], inp["S"], inp["X"])
         best = min(best, time.perf_counter() - t0)
-    return dict(value=1.0 / best, unit=UNIT, cores=cores, kind="reference",
+    return dict(value=1.0 / best, unit=UNIT, cores=cores, cpu_model=cpu_model(), kind="reference",
                 sample=f"full workload (n={N_AO}, naux={N_AUX}, nocc={N_OCC}), best of {reps + 1} calls of the "
-                       f"reference nonRelFockMatrix compiled from its sources, OMP_NUM_THREADS={cores}")
+                       f"reference nonRelFockMatrix compiled from its sources, OMP_NUM_THREADS={cores}"), F_ref
 
 
 def run_reference(args):
     ws, rank, _ = dist_env()
     base = dict(metric=METRIC, unit=UNIT, n_gpus=args.gpus, steps=args.steps, warmup=args.warmup,
                 higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64", data="synthetic",
-                impl="reference",
-                config={"workload": f"nonrel RI J+K Fock build n={N_AO} naux={N_AUX} nocc={N_OCC}",
-                        "precision": "fp64", "l2": "inputs larger than L2"})
+                impl="reference", config=bench_config(args.gpus))
     if rank != 0:
         return
     from oracle import ref
@@ -448,18 +466,26 @@ def run_reference(args):
     inp = make_inputs()
     cores = os.cpu_count() or 1
     ref.set_threads(cores)
-    for _ in range(max(0, min(args.warmup, 1))):
+    # Every warm-up and timed step is one full-size call; if one call is so slow that the run would
+    # exceed about four minutes, fewer steps run and the line says how many.
+    t0 = time.perf_counter()
+    ref.nonrel_fock(inp["h"], inp["B"], inp["D"], inp["S"], inp["X"])
+    first = time.perf_counter() - t0
+    budget = max(1, int(240.0 / max(first, 1e-3)))
+    warmup = max(0, min(args.warmup - 1, budget // 4))
+    steps = max(1, min(args.steps, budget - warmup - 1))
+    for _ in range(warmup):
         ref.nonrel_fock(inp["h"], inp["B"], inp["D"], inp["S"], inp["X"])
-    steps = max(1, min(args.steps, 5))
     t0 = time.perf_counter()
     for _ in range(steps):
         ref.nonrel_fock(inp["h"], inp["B"], inp["D"], inp["S"], inp["X"])
     dt = time.perf_counter() - t0
     v = steps / dt
-    base.update(value=v, ms_per_step=1e3 * dt / steps,
-                cpu_baseline=dict(value=v, unit=UNIT, cores=cores, kind="reference",
-                                  sample=f"{steps} full-size calls (warm-up {min(args.warmup, 1)}) of the reference "
-                                         f"nonRelFockMatrix compiled from its sources, OMP_NUM_THREADS={cores}"),
+    base.update(steps=steps, warmup=warmup + 1, value=v, ms_per_step=1e3 * dt / steps,
+                cpu_baseline=dict(value=v, unit=UNIT, cores=cores, cpu_model=cpu_model(), kind="reference",
+                                  sample=f"{steps} timed full-size calls after {warmup + 1} warm-up calls of the "
+                                         f"reference nonRelFockMatrix compiled from its sources, "
+                                         f"OMP_NUM_THREADS={cores}"),
                 e2e=dict(value=v, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
     print(json.dumps(base))
 
@@ -680,7 +706,11 @@ def main():
     hbm_peak, hbm_src = measured_peaks()
     fp64_peak = fp64_gemm_peak(torch) if rank == 0 else None
     ht_flops = 2.0 * N_AUX * N_OCC * N_AO * N_AO
-    syrk_flops = 2.0 * N_AUX * N_OCC * N_AO * N_AO
+    # The exchange SYRK computes only the upper 80 x 80 output tiles of the symmetric K (15 of 25 at
+    # n = 400) and mirrors the rest: executed flops, not the full 2*naux*nocc*n^2 count.
+    syrk_tile = 80
+    syrk_nt = -(-N_AO // syrk_tile)
+    syrk_flops = 2.0 * N_AUX * N_OCC * (syrk_nt * (syrk_nt + 1) // 2) * syrk_tile * syrk_tile
     j_bytes = 2.0 * N_AUX * N_AO * N_AO * 8  # algorithmic: two passes over B
     # both passes stream the packed upper triangles of B (from the top of the build, beside the recovery)
     j_bytes_streamed = 2.0 * N_AUX * (-(-(N_AO * (N_AO + 1) // 2) // 32) * 32) * 8
@@ -695,7 +725,12 @@ def main():
         if pg:
             pg.destroy_process_group()
         return
-    cpu = None if args.no_cpu_baseline else cpu_reference_rate(inp)
+    F_gpu = F.cpu().numpy()
+    cpu, F_ref = (None, None) if args.no_cpu_baseline else cpu_reference_rate(inp)
+    parity = None
+    if F_ref is not None:
+        parity = dict(max_abs_F_minus_reference=float(np.abs(F_gpu - F_ref).max()), tolerance=1e-10,
+                      reference="nonRelFockMatrix compiled from the reference's sources, on the timed build's inputs")
     del dev, src, store
     torch.cuda.empty_cache()
     scf_block = scf_times(torch, want_cpu=not args.no_cpu_baseline)
@@ -708,9 +743,7 @@ def main():
         metric=METRIC, value=value, unit=UNIT, n_gpus=ws, steps=args.steps, warmup=args.warmup,
         ms_per_step=1e3 * t / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
         data="synthetic",
-        config={"workload": f"nonrel RI J+K Fock build n={N_AO} naux={N_AUX} nocc={N_OCC} (FP64, occupied recovery "
-                            f"included)", "parallelism": f"replicas x{ws}", "precision": "fp64",
-                "l2": "inputs larger than L2 (B = 2.05 GB)"},
+        config=bench_config(ws),
         roofline={"bound": "tensor", "kernel": "dgemm_kernel half-transform T^P = Ct B^P (FP64 DMMA, 45% of a build)",
                   "achieved": ht_tf, "peak": fp64_peak, "unit": "TFLOP/s",
                   "frac": (ht_tf / fp64_peak) if (ht_tf and fp64_peak) else None, "traffic": HT_TRAFFIC_BYTES,
@@ -721,7 +754,8 @@ def main():
                   "algorithmic": "2*naux*nocc*n^2 flops per launch (one launch per build)"},
         exchange={"bound": "tensor", "kernel": "half-transform + SYRK (FP64 DMMA)", "achieved": k_tf,
                   "peak": fp64_peak, "unit": "TFLOP/s", "frac": (k_tf / fp64_peak) if (k_tf and fp64_peak) else None,
-                  "algorithmic": "4*naux*nocc*n^2 flops per build (half-transform + full-count SYRK)"},
+                  "algorithmic": "2*naux*nocc*n^2 (half-transform) + 2*naux*nocc*15*80*80 (the SYRK's executed "
+                                 "upper tiles) flops per build"},
         coulomb={"bound": "hbm", "achieved": j_gbs, "peak": hbm_peak, "unit": "GB/s",
                  "frac": (j_gbs / hbm_peak) if j_gbs else None, "peak_source": hbm_src,
                  "algorithmic": "2*naux*n^2*8 bytes per build (two passes over B)",
@@ -729,8 +763,8 @@ def main():
                              "symmetric B^P, on a side stream from the top of the build (beside the occupied "
                              "recovery and the half-transform, one CTA per SM); achieved counts the streamed bytes",
                  "algorithmic_rate_gbs": (j_bytes / (acc["coulomb_ms"] / 1e3) / 1e9) if acc.get("coulomb_ms") else None},
-        kernels={"half_transform_tflops": ht_tf, "syrk_tflops_full_count": ex_tf},
-        phases_ms=phases, clocks=clk, e2e=e2e, gpu_launches=int(launches), cpu_baseline=cpu,
+        kernels={"half_transform_tflops": ht_tf, "syrk_tflops_executed": ex_tf},
+        phases_ms=phases, clocks=clk, e2e=e2e, gpu_launches=int(launches), cpu_baseline=cpu, parity=parity,
         time_to_1e8_ha=scf_block,
         time_to_1e8_ha_relativistic=rel_block,
         rkb_fock_4c=rkb_block,

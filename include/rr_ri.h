@@ -177,6 +177,17 @@ typedef struct rr_scf_result {
    * Fock builds (the final FP64 build of a mixed loop included), energy + DIIS, density step
    * (orthogonal transform, SP2 projector(s), back-transform, density change). */
   double build_ms, diis_ms, density_ms;
+  /* Optional outputs, as the reference's SCF results carry them (src/NON_REL/NonRelHartreeFock.h:28-38,
+   * src/X2C_DHF/X2C_HF.h:28-37, src/C4_DHF/C4_DHF.h:28-36).  The caller sets the pointers before the
+   * call (NULL: not wanted; host or device memory as opts->mem says); the loop fills them from its last
+   * iteration: orbital_energies (n_eff doubles, ascending) and c_matrix (C = X U, n x n_eff; complex for
+   * X2C / DHF) from X^dagger F X = U diag(w) U^dagger, and fock_matrix (n x n) = that F: the
+   * DIIS-extrapolated F of the last iteration, or, for a converged RR_PREC_MIXED loop, the FP64 Fock
+   * matrix of the final density.  Eigenvectors are determined up to a phase per vector (and a rotation
+   * within a degenerate level, e.g. a Kramers pair), as LAPACK's are. */
+  double* orbital_energies;
+  double* c_matrix;
+  double* fock_matrix;
 } rr_scf_result;
 
 /* Restricted nonrelativistic SCF with the RI Fock build, DIIS on e = FPS - SPF and the aufbau

@@ -51,6 +51,19 @@ int rr_test_adam_run_quadratic(int64_t n, const double* a, const double* b, doub
                                double* energy_best, int32_t* iterations, int32_t* restart, double* rate,
                                double* x_out);
 
+/* Number of device allocations (cudaMalloc of the library's own buffers) made by this process so far:
+ * a call that allocates nothing leaves it unchanged. */
+int64_t rr_test_device_allocations(void);
+
+/* Failure detection without a fault: one CTA of `threads` threads waits on an mbarrier that nothing
+ * arrives on (and no bulk copy is in flight) through the bounded wait every TMA pipeline of the library
+ * uses, with `spin_limit` polls (1 .. 4,194,304, the pipelines' own limit).  The wait expires, records
+ * its code in the status word and returns; the hook then returns RR_ERR_TIMEOUT, as a pipeline call
+ * does.  status_word: the recorded code; elapsed_ms: the launch's device time (CUDA events);
+ * cycles: SM clock cycles thread 0 spent in the wait. */
+int rr_test_wait_expiry(uint32_t spin_limit, int32_t threads, int32_t* status_word, double* elapsed_ms,
+                        double* cycles);
+
 #ifdef __cplusplus
 }
 #endif

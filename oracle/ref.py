@@ -236,18 +236,31 @@ def canonical_orth(S, thr=1e-10):
     return X[: n * n_eff.value].reshape(n, n_eff.value)
 
 
+def _orbital_outputs(n, n_eff, cplx):
+    dt = np.complex128 if cplx else np.float64
+    return dict(orbital_energies=np.empty(n_eff), c_matrix=np.empty((n, n_eff), dtype=dt),
+                fock_matrix=np.empty((n, n), dtype=dt))
+
+
+def _orb_ptrs(o):
+    return _p(o["orbital_energies"]), _p(o["c_matrix"]), _p(o["fock_matrix"])
+
+
 def nonrel_scf(sysd, diis_size=5, max_iter=100, e_tol=1e-8, d_tol=1e-6):
+    """runNonRelativisticHartreeFock (RI overload): energy, iterations, converged, density, energy history
+    and the result's orbital_energies, c_matrix and fock_matrix."""
     n, B = sysd["n"], _d(sysd["B"])
     X = _d(sysd["X"])
     res = ScfResult()
     P = np.empty((n, n))
     hist = np.full(max_iter, np.nan)
+    orb = _orbital_outputs(n, X.shape[1], False)
     _check(lib().rrref_nonrel_scf(_i64(n), _i64(B.shape[0]), _p(B), _p(_d(sysd["h"])), _p(X), _i64(X.shape[1]),
                                   _p(_d(sysd["S"])), _p(_d(sysd["D0"])), ctypes.c_int(sysd["n_electrons"]),
                                   ctypes.c_int(diis_size), ctypes.c_int(max_iter), ctypes.c_double(e_tol),
-                                  ctypes.c_double(d_tol), ctypes.byref(res), _p(P), _p(hist)))
+                                  ctypes.c_double(d_tol), ctypes.byref(res), _p(P), _p(hist), *_orb_ptrs(orb)))
     return dict(energy=res.electronic_energy, iterations=res.iterations, converged=bool(res.converged), P=P,
-                history=hist[: res.iterations].copy())
+                history=hist[: res.iterations].copy(), **orb)
 
 
 def x2c_scf(sysd, diis_size=5, max_iter=100, e_tol=1e-8, d_tol=1e-6, kramers=True):
@@ -256,13 +269,14 @@ def x2c_scf(sysd, diis_size=5, max_iter=100, e_tol=1e-8, d_tol=1e-6, kramers=Tru
     res = ScfResult()
     P = np.empty((2 * nl, 2 * nl), dtype=np.complex128)
     hist = np.full(max_iter, np.nan)
+    orb = _orbital_outputs(2 * nl, X.shape[1], True)
     _check(lib().rrref_x2c_scf(_i64(nl), _i64(B.shape[0]), _p(B), _p(_c(sysd["h"])), _p(X), _i64(X.shape[1]),
                                _p(_c(sysd["S"])), _p(_c(sysd["P0"])), ctypes.c_int(sysd["n_electrons"]),
                                ctypes.c_int(diis_size), ctypes.c_int(max_iter), ctypes.c_double(e_tol),
                                ctypes.c_double(d_tol), ctypes.c_int(1 if kramers else 0), ctypes.byref(res), _p(P),
-                               _p(hist)))
+                               _p(hist), *_orb_ptrs(orb)))
     return dict(energy=res.electronic_energy, iterations=res.iterations, converged=bool(res.converged), P=P,
-                history=hist[: res.iterations].copy())
+                history=hist[: res.iterations].copy(), **orb)
 
 
 def dhf_scf(sysd, diis_size=5, max_iter=100, e_tol=1e-8, d_tol=1e-6, kramers=True):
@@ -272,14 +286,15 @@ def dhf_scf(sysd, diis_size=5, max_iter=100, e_tol=1e-8, d_tol=1e-6, kramers=Tru
     res = ScfResult()
     P = np.empty((n_rkb, n_rkb), dtype=np.complex128)
     hist = np.full(max_iter, np.nan)
+    orb = _orbital_outputs(n_rkb, x_full.shape[1], True)
     _check(lib().rrref_dhf_scf(_i64(nl), _i64(ns), _i64(sysd["B_LL"].shape[0]), _p(_d(sysd["B_LL"])),
                                _p(_d(sysd["B_SS"])), _p(_c(sysd["v_total"])), _i64(n_rkb), _p(_c(sysd["s_full"])),
                                _p(x_full), _i64(x_full.shape[1]), _p(_c(sysd["h"])), _p(_c(sysd["P0"])),
                                ctypes.c_int(sysd["n_electrons"]), ctypes.c_int(diis_size), ctypes.c_int(max_iter),
                                ctypes.c_double(e_tol), ctypes.c_double(d_tol), ctypes.c_int(1 if kramers else 0),
-                               ctypes.byref(res), _p(P), _p(hist)))
+                               ctypes.byref(res), _p(P), _p(hist), *_orb_ptrs(orb)))
     return dict(energy=res.electronic_energy, iterations=res.iterations, converged=bool(res.converged), P=P,
-                history=hist[: res.iterations].copy())
+                history=hist[: res.iterations].copy(), **orb)
 
 
 # ---------------------------------------------------------------- orbital-rotation optimisation

@@ -370,11 +370,27 @@ static void copyHistory(const std::vector<double>& e, double* hist, i64 max_iter
   for (std::size_t i = 0; i < e.size() && static_cast<i64>(i) < max_iter; ++i) hist[i] = e[i];
 }
 
+// The result's orbital_energies, coefficients and Fock matrix, into the optional (nullable) outputs.
+static void copyOrbitalsReal(const std::vector<double>& w, const rerdmft::Matrix<double>& c,
+                             const rerdmft::Matrix<double>& f, double* w_out, double* c_out, double* f_out) {
+  if (w_out) std::memcpy(w_out, w.data(), sizeof(double) * w.size());
+  if (c_out) fromMatrix(c, c_out);
+  if (f_out) fromMatrix(f, f_out);
+}
+static void copyOrbitalsComplex(const std::vector<double>& w, const rerdmft::Matrix<std::complex<double>>& c,
+                                const rerdmft::Matrix<std::complex<double>>& f, double* w_out, double* c_out,
+                                double* f_out) {
+  if (w_out) std::memcpy(w_out, w.data(), sizeof(double) * w.size());
+  if (c_out) fromCMatrix(c, c_out);
+  if (f_out) fromCMatrix(f, f_out);
+}
+
 // src/NON_REL/NonRelHartreeFock.cpp:219 runNonRelativisticHartreeFock(RiNonRelEriSource, ...) with an
 // empty geometry (nuclear repulsion 0).  energy_history gets one electronic energy per iteration.
 int rrref_nonrel_scf(i64 n, i64 naux, const double* B, const double* h, const double* X, i64 n_eff,
                      const double* S, const double* P0, int n_electrons, int diis_size, int max_iter, double e_tol,
-                     double d_tol, rrref_scf_result* res, double* P_out, double* energy_history) {
+                     double d_tol, rrref_scf_result* res, double* P_out, double* energy_history, double* w_out,
+                     double* c_out, double* f_out) {
   return guard([&] {
     rerdmft::RiNonRelEriSource src;
     src.nl = static_cast<std::size_t>(n);
@@ -388,6 +404,7 @@ int rrref_nonrel_scf(i64 n, i64 naux, const double* B, const double* h, const do
     res->iterations = r.iterations;
     res->converged = r.converged ? 1 : 0;
     fromMatrix(r.density_matrix, P_out);
+    copyOrbitalsReal(r.orbital_energies, r.c_matrix, r.fock_matrix, w_out, c_out, f_out);
     std::vector<double> e;
     for (const auto& rec : r.history) e.push_back(rec.energy);
     copyHistory(e, energy_history, max_iter);
@@ -397,7 +414,8 @@ int rrref_nonrel_scf(i64 n, i64 naux, const double* B, const double* h, const do
 // src/X2C_DHF/X2C_HF.cpp:175 runX2CHartreeFockScf(h_x2c, RiX2cEriSource, ...)
 int rrref_x2c_scf(i64 nl, i64 naux, const double* B, const double* h, const double* X, i64 n_eff, const double* S,
                   const double* P0, int n_electrons, int diis_size, int max_iter, double e_tol, double d_tol,
-                  int kramers, rrref_scf_result* res, double* P_out, double* energy_history) {
+                  int kramers, rrref_scf_result* res, double* P_out, double* energy_history, double* w_out,
+                  double* c_out, double* f_out) {
   return guard([&] {
     rerdmft::RiX2cEriSource src;
     src.nl = static_cast<std::size_t>(nl);
@@ -411,6 +429,7 @@ int rrref_x2c_scf(i64 nl, i64 naux, const double* B, const double* h, const doub
     res->iterations = r.iterations;
     res->converged = r.converged ? 1 : 0;
     fromCMatrix(r.density_matrix, P_out);
+    copyOrbitalsComplex(r.orbital_energies, r.c_matrix, r.fock_matrix, w_out, c_out, f_out);
     std::vector<double> e;
     for (const auto& rec : r.history) e.push_back(rec.energy);
     copyHistory(e, energy_history, max_iter);
@@ -421,7 +440,8 @@ int rrref_x2c_scf(i64 nl, i64 naux, const double* B, const double* h, const doub
 int rrref_dhf_scf(i64 nl, i64 ns, i64 naux, const double* B_LL, const double* B_SS, const double* v_total,
                   i64 n_rkb, const double* s_full, const double* x_full, i64 n_eff, const double* h,
                   const double* P0, int n_electrons, int diis_size, int max_iter, double e_tol, double d_tol,
-                  int kramers, rrref_scf_result* res, double* P_out, double* energy_history) {
+                  int kramers, rrref_scf_result* res, double* P_out, double* energy_history, double* w_out,
+                  double* c_out, double* f_out) {
   return guard([&] {
     auto src = makeDirect(nl, ns, naux, B_LL, B_SS, v_total, n_rkb, s_full, x_full, n_eff);
     auto r = rerdmft::runDiracHartreeFockScf(toCMatrix(h, n_rkb, n_rkb), src, src.x_full,
@@ -431,6 +451,7 @@ int rrref_dhf_scf(i64 nl, i64 ns, i64 naux, const double* B_LL, const double* B_
     res->iterations = r.iterations;
     res->converged = r.converged ? 1 : 0;
     fromCMatrix(r.density_matrix, P_out);
+    copyOrbitalsComplex(r.orbital_energies, r.c_dhf, r.fock_matrix, w_out, c_out, f_out);
     std::vector<double> e;
     for (const auto& rec : r.history) e.push_back(rec.energy);
     copyHistory(e, energy_history, max_iter);

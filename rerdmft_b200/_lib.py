@@ -65,7 +65,8 @@ class AdamResult(ctypes.Structure):
 class ScfResult(ctypes.Structure):
     _fields_ = [("electronic_energy", _d), ("iterations", _i64), ("converged", _i64),
                 ("mixed_iterations", _i64), ("fp64_iterations", _i64), ("seconds", _d),
-                ("build_ms", _d), ("diis_ms", _d), ("density_ms", _d)]
+                ("build_ms", _d), ("diis_ms", _d), ("density_ms", _d),
+                ("orbital_energies", _vp), ("c_matrix", _vp), ("fock_matrix", _vp)]
 
 
 class X2cInstance(ctypes.Structure):
@@ -138,6 +139,9 @@ _SIGS = {
     "rr_test_mixed_exchange_delta": (ctypes.c_int, [_vp, _i64, _i64, _vp, _vp, _i64, _vp]),
     "rr_test_j_passes": (ctypes.c_int, [_vp, _i64, _i64, _vp, _vp, _vp]),
     "rr_test_j_passes_packed": (ctypes.c_int, [_vp, _i64, _i64, _vp, _vp, _vp, _vp]),
+    "rr_test_device_allocations": (ctypes.c_int64, []),
+    "rr_test_wait_expiry": (ctypes.c_int, [ctypes.c_uint32, _i32, ctypes.POINTER(_i32), ctypes.POINTER(_d),
+                                           ctypes.POINTER(_d)]),
 }
 
 _lib = None

@@ -303,29 +303,19 @@ __global__ void mirror_kernel(double* C, int64_t n, int64_t ldc, int64_t strideC
   }
 }
 
-int num_sms() {
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (sms <= 0) sms = 148;
-  }
-  return sms;
-}
+int num_sms() { return sm_count_current(); }
 
 template <int MT, int NT, int WM, int WN, bool AK, bool BKM, bool CPLX, int V, bool EDOT = false>
 void launch_cfg_v(const Params& p, dim3 grid, cudaStream_t s) {
   using CF = Cfg<MT, NT, WM, WN, AK, BKM, CPLX>;
   auto kern = dgemm_kernel<MT, NT, WM, WN, AK, BKM, CPLX, V, EDOT>;
-  static std::atomic<bool> attr{false};  // host threads may race here: the attribute is idempotent
-  if (!attr) {
+  static std::atomic<bool> attr[kMaxDevices];
+  once_per_device(attr, [&] {
     RR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, CF::SMEM_BYTES));
     // Largest shared-memory carveout: an SM only takes CTAs of another kernel when its carveout
     // fits them too, and the J passes run beside the exchange SYRK.
     RR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
-    attr = true;
-  }
+  });
   kern<<<grid, CF::THREADS, CF::SMEM_BYTES, s>>>(p);
   RR_LAUNCH_CHECK();
 }

@@ -305,31 +305,21 @@ __global__ void j_gamma_kernel(const double* gpart, int64_t naux, int segtot, do
   }
 }
 
-int sm_count() {
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (sms <= 0) sms = 148;
-  }
-  return sms;
-}
+int sm_count() { return sm_count_current(); }
 
 int grid_size(int64_t items, int ctas_per_sm) {
   return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(items, static_cast<int64_t>(ctas_per_sm) * sm_count())));
 }
 
 void set_smem_attr() {
-  static std::atomic<bool> done{false};  // host threads may race here: the attribute is idempotent
-  if (!done) {
+  static std::atomic<bool> done[kMaxDevices];
+  once_per_device(done, [] {
     RR_CUDA(cudaFuncSetAttribute(j_pass1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
     RR_CUDA(cudaFuncSetAttribute(j_pass2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
     // same carveout as the GEMMs they run beside, so an SM can hold both
     RR_CUDA(cudaFuncSetAttribute(j_pass1_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
     RR_CUDA(cudaFuncSetAttribute(j_pass2_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
-    done = true;
-  }
+  });
 }
 
 }  // namespace

@@ -523,16 +523,7 @@ CUtensorMap make_map(const void* base, int rank, const uint64_t* dims, const uin
   return m;
 }
 
-int sm_count() {
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (sms <= 0) sms = 148;
-  }
-  return sms;
-}
+int sm_count() { return sm_count_current(); }
 
 int64_t round8(int64_t x) { return (x + 7) / 8 * 8; }
 int grid_for(int64_t count) { return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((count + 255) / 256, 1184))); }
@@ -542,11 +533,8 @@ void launch_ht_bn(const CUtensorMap& a_hi, const CUtensorMap& a_lo, const CUtens
                   const HtEpi& e, int M, int nkb, int mtiles, int naux, int* err, cudaStream_t s) {
   using HC = HCfg<BN, STAGES>;
   auto kern = umma_ht_persistent_kernel<BN, STAGES>;
-  static std::atomic<bool> attr{false};  // host threads may race here: the attribute is idempotent
-  if (!attr) {
-    RR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, HC::SMEM));
-    attr = true;
-  }
+  static std::atomic<bool> attr[kMaxDevices];
+  once_per_device(attr, [&] { RR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, HC::SMEM)); });
   const int64_t items = static_cast<int64_t>(mtiles) * naux;
   const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(items, sm_count())));
   kern<<<grid, HT_THREADS, HC::SMEM, s>>>(a_hi, a_lo, b_hi, b_lo, e, M, nkb, mtiles, naux, err);
@@ -622,11 +610,10 @@ void launch_gemm(const BlockPlan& bp, const uint16_t* a_hi, const uint16_t* a_lo
   p.upper = bp.upper ? 1 : 0;
   p.work = work;
   p.err = err;
-  static std::atomic<bool> attr{false};  // host threads may race here: the attribute is idempotent
-  if (!attr) {
+  static std::atomic<bool> attr[kMaxDevices];
+  once_per_device(attr, [] {
     RR_CUDA(cudaFuncSetAttribute(umma_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, GCfg::SMEM));
-    attr = true;
-  }
+  });
   umma_gemm_kernel<<<dim3(static_cast<unsigned>(bp.tiles), static_cast<unsigned>(bp.splits)), 128, GCfg::SMEM, s>>>(
       mah, mal, mbh, mbl, p);
   RR_LAUNCH_CHECK();

@@ -24,7 +24,6 @@ namespace {
 //   [pass-1 partials: round_up(naux * nseg, 32)] [pass-2 partials: nrange * n^2]
 // nrange (the aux ranges pass 2 splits over) shrinks to what fits; at least one must fit.
 constexpr int64_t kScratchDoubles = 4LL << 20;
-constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 

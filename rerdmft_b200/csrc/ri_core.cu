@@ -15,6 +15,26 @@ static std::atomic<int64_t> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 int64_t launches() { return g_launches.load(std::memory_order_relaxed); }
 
+static std::atomic<int64_t> g_device_allocs{0};
+void count_device_alloc() { g_device_allocs.fetch_add(1, std::memory_order_relaxed); }
+int64_t device_allocations() { return g_device_allocs.load(std::memory_order_relaxed); }
+
+int current_device() {
+  int dev = 0;
+  RR_CUDA(cudaGetDevice(&dev));
+  return dev;
+}
+
+int sm_count_current() {
+  static std::atomic<int> cache[kMaxDevices];
+  const int dev = current_device();
+  int sms = (dev >= 0 && dev < kMaxDevices) ? cache[dev].load(std::memory_order_relaxed) : 0;
+  if (sms > 0) return sms;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+  if (dev >= 0 && dev < kMaxDevices) cache[dev].store(sms, std::memory_order_relaxed);
+  return sms;
+}
+
 void Context::init(cudaStream_t user_stream) {
   RR_CUDA(cudaGetDevice(&device));
   if (user_stream) {

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <cusolverDn.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -55,6 +56,9 @@ void count_launch();
     ::rr::count_launch();                                                                           \
   } while (0)
 
+// Counts the device allocations the library makes (DevBuf::alloc); read by a test hook.
+void count_device_alloc();
+
 // Owning device allocation (cudaMalloc/cudaFree), move-only.
 template <typename T>
 struct DevBuf {
@@ -72,7 +76,10 @@ struct DevBuf {
   ~DevBuf() { release(); }
   void alloc(size_t count) {
     release();
-    if (count) RR_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    if (count) {
+      RR_CUDA(cudaMalloc(&p, count * sizeof(T)));
+      count_device_alloc();
+    }
     n = count;
   }
   // Grow-only: keeps the allocation when it is already large enough.
@@ -100,6 +107,28 @@ struct Context {
   void destroy();
   void set_stream(cudaStream_t s);
 };
+
+// CUDA keeps kernel attributes per device context.  One-time settings (dynamic shared-memory size,
+// carveout) and the SM count are therefore kept per device ordinal, so one process may drive
+// several GPUs (a handle binds to the device current at its creation).
+constexpr int kMaxDevices = 64;
+int current_device();
+// Multiprocessor count of the current device (cached per device).
+int sm_count_current();
+// Runs f() once per device for this flag array (on the first call with that device current).
+// Host threads may race into f() together for one device: the attributes it sets are idempotent.
+template <class F>
+void once_per_device(std::atomic<bool> (&done)[kMaxDevices], F&& f) {
+  const int d = current_device();
+  if (d < 0 || d >= kMaxDevices) {
+    f();
+    return;
+  }
+  if (!done[d].load(std::memory_order_acquire)) {
+    f();
+    done[d].store(true, std::memory_order_release);
+  }
+}
 
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 inline int ceil_div(int64_t a, int64_t b) { return static_cast<int>((a + b - 1) / b); }

@@ -616,6 +616,53 @@ void sp2_projector(rr_ri_store* h, const double* F, int64_t n, int64_t nocc, dou
   throw Error(RR_ERR_SOLVER, "SCF: density purification did not converge (no gap at the Fermi level?)");
 }
 
+// Orbital energies, coefficients and Fock matrix of an SCF loop's last iteration, as the reference's
+// SCF results carry them (src/NON_REL/NonRelHartreeFock.h:28-38, src/X2C_DHF/X2C_HF.h:28-37,
+// src/C4_DHF/C4_DHF.h:28-36; filled at NonRelHartreeFock.cpp:146-151): w and U from
+// X^dagger F X = U diag(w) U^dagger (cuSOLVER syevd / heevd on the device, w ascending), C = X U, and
+// F itself.  Only the outputs whose pointers the caller set are formed.
+void scf_result_outputs(rr_ri_store* h, const double* F, const double* Xd, int64_t n, int64_t n_eff, bool cplx,
+                        const rr_scf_result* res, bool host, cudaStream_t s) {
+  const int PL = cplx ? 2 : 1;
+  if (res->fock_matrix) copy_out(res->fock_matrix, F, n * n * PL, host, s);
+  if (!res->orbital_energies && !res->c_matrix) return;
+  double *FX, *A, *w, *C;
+  Arena ar(&h->solver_a);
+  ar.request(&FX, n * n_eff * PL);
+  ar.request(&A, n_eff * n_eff * PL);
+  ar.request(&w, n_eff);
+  ar.request(&C, n * n_eff * PL);
+  ar.commit();
+  auto wk = [h] { return h->work.p; };
+  auto wcap = [h] { return static_cast<int64_t>(h->work.n); };
+  GemmDesc a;
+  a.cplx = cplx;
+  a.M = n; a.N = n_eff; a.K = n; a.A = F; a.lda = n; a.B = Xd; a.ldb = n_eff; a.C = FX; a.ldc = n_eff;
+  gemm(a, s, wk(), wcap());
+  a.M = n_eff; a.N = n_eff; a.K = n; a.A = Xd; a.lda = n_eff; a.opA = Op::T; a.conjA = cplx; a.B = FX; a.ldb = n_eff;
+  a.C = A; a.ldc = n_eff;
+  a.mirror = 1;  // X^dagger F X is Hermitian
+  gemm(a, s, wk(), wcap());
+  // row j of A: eigenvector j (conjugated for the complex solver, which sees the row-major matrix as
+  // its transpose)
+  if (cplx) eigh_herm(h, A, n_eff, w, s);
+  else eigh_sym(h, A, n_eff, w, s);
+  int info = 0;
+  RR_CUDA(cudaMemcpyAsync(&info, h->ctx.solver_info.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  host_wait(h, s);
+  RR_REQUIRE(info == 0, RR_ERR_SOLVER,
+             "SCF result: the eigensolver of X^dagger F X did not converge (info " + std::to_string(info) + ")");
+  if (res->orbital_energies) copy_out(res->orbital_energies, w, n_eff, host, s);
+  if (res->c_matrix) {
+    GemmDesc c;  // C = X U, U = A^dagger (complex) or A^T (real)
+    c.cplx = cplx;
+    c.M = n; c.N = n_eff; c.K = n_eff; c.A = Xd; c.lda = n_eff; c.B = A; c.ldb = n_eff; c.opB = Op::T;
+    c.conjB = cplx; c.C = C; c.ldc = n_eff;
+    gemm(c, s, wk(), wcap());
+    copy_out(res->c_matrix, C, n * n_eff * PL, host, s);
+  }
+}
+
 void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff, const double* S, const double* P0,
                 int n_electrons, const rr_scf_opts* so, rr_scf_result* res, double* P_out, double* hist,
                 const rr_opts* o) {
@@ -801,6 +848,9 @@ void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff
     std::swap(P, Pn);
   }
   if (it > so->max_iterations) it = so->max_iterations;
+  // the converged mixed loop's last Fock matrix is the FP64 build of the final density (no DIIS step
+  // follows it); otherwise the last iteration's DIIS-extrapolated F, as the reference reports
+  scf_result_outputs(h, mixed && converged ? F : Fs, Xd, n, n_eff, false, res, host, s);
   check_status(h, s);
   copy_out(P_out, P, n2, host, s);
   host_wait(h, s);
@@ -1030,6 +1080,7 @@ void scf_rel(rr_ri_store* h, int kind, const double* hc, const double* v_total, 
     std::swap(P, Pn);
   }
   if (it > so->max_iterations) it = so->max_iterations;
+  scf_result_outputs(h, mixed && converged ? F : Fs, Xd, n, n_eff, true, res, host, s);
   check_status(h, s);
   copy_out(P_out, P, c2, host, s);
   host_wait(h, s);

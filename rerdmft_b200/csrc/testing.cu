@@ -1,0 +1,94 @@
+// Test hooks for the library's failure detection and allocation behaviour (declared in
+// include/rr_ri_testing.h).  No reference counterpart.
+#include <algorithm>
+
+#include "ri_store.cuh"
+#include "tma_util.cuh"
+
+namespace rr {
+int64_t device_allocations();
+
+namespace {
+
+constexpr int kExpiryCode = 0x40;
+
+// One CTA.  Thread 0 initialises an mbarrier that expects one arrival; nothing ever arrives and no
+// bulk copy is issued, so every thread's bounded wait (the same mbar_wait the TMA pipelines use)
+// polls `limit` times, records kExpiryCode in *err and returns false.  out[0]: SM cycles thread 0
+// spent in the wait; out[1]: 1 if any wait returned true (it must not).
+__global__ void wait_expiry_kernel(uint32_t limit, int* err, long long* out) {
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int completed;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_barrier_init();
+    completed = 0;
+  }
+  __syncthreads();
+  const long long t0 = clock64();
+  bool dead = false;
+  const bool ok = mbar_wait(&bar, 0, err, kExpiryCode, dead, limit);
+  const long long t1 = clock64();
+  if (ok) atomicOr(&completed, 1);
+  // a dead thread skips later waits at once: the second wait must return false without polling
+  const bool again = mbar_wait(&bar, 0, err, kExpiryCode, dead, limit);
+  if (again) atomicOr(&completed, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    out[0] = t1 - t0;
+    out[1] = completed;
+  }
+}
+
+}  // namespace
+}  // namespace rr
+
+extern "C" {
+
+int64_t rr_test_device_allocations(void) { return rr::device_allocations(); }
+
+int rr_test_wait_expiry(uint32_t spin_limit, int32_t threads, int32_t* status_word, double* elapsed_ms,
+                        double* cycles) {
+  try {
+    rr::set_last_error("");
+    RR_REQUIRE(spin_limit >= 1 && spin_limit <= rr::kSpinLimit, RR_ERR_ARG,
+               "rr_test_wait_expiry: spin_limit must be in [1, 4194304]");
+    RR_REQUIRE(threads >= 32 && threads <= 1024 && threads % 32 == 0, RR_ERR_ARG,
+               "rr_test_wait_expiry: threads must be a multiple of 32 in [32, 1024]");
+    rr::DevBuf<int> err(1);
+    rr::DevBuf<long long> out(2);
+    RR_CUDA(cudaMemset(err.p, 0, sizeof(int)));
+    RR_CUDA(cudaMemset(out.p, 0, 2 * sizeof(long long)));
+    cudaEvent_t e0, e1;
+    RR_CUDA(cudaEventCreate(&e0));
+    RR_CUDA(cudaEventCreate(&e1));
+    RR_CUDA(cudaEventRecord(e0, nullptr));
+    rr::wait_expiry_kernel<<<1, threads>>>(spin_limit, err.p, out.p);
+    RR_LAUNCH_CHECK();
+    RR_CUDA(cudaEventRecord(e1, nullptr));
+    RR_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    RR_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int word = 0;
+    long long o[2] = {0, 0};
+    RR_CUDA(cudaMemcpy(&word, err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    RR_CUDA(cudaMemcpy(o, out.p, sizeof(o), cudaMemcpyDeviceToHost));
+    if (status_word) *status_word = word;
+    if (elapsed_ms) *elapsed_ms = ms;
+    if (cycles) *cycles = static_cast<double>(o[0]);
+    RR_REQUIRE(o[1] == 0, RR_ERR_STATE, "rr_test_wait_expiry: a wait on a barrier nobody arrives on completed");
+    // The pipelines report an expired wait as RR_ERR_TIMEOUT; so does this hook.
+    if (word != 0) throw rr::Error(RR_ERR_TIMEOUT, "device wait bound expired (status word 0x" + std::to_string(word) + ")");
+    return RR_OK;
+  } catch (const rr::Error& e) {
+    rr::set_last_error(e.what());
+    return e.code;
+  } catch (const std::exception& e) {
+    rr::set_last_error(e.what());
+    return RR_ERR_CUDA;
+  }
+}
+
+}  // extern "C"

@@ -45,10 +45,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 
 // Bounded wait; on expiry records `code` into *err, marks the calling thread `dead` and returns
 // false.  A dead thread skips every later wait at once (its results are discarded by the host,
-// which sees the status word), so a pipeline that lost a barrier drains in bounded time.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code, bool& dead) {
+// which sees the status word), so a pipeline that lost a barrier drains in bounded time.  The
+// pipelines use the default limit; a test hook passes a small one to make a wait expire.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code, bool& dead,
+                                          uint32_t limit = kSpinLimit) {
   if (dead) return false;
-  for (uint32_t i = 0; i < kSpinLimit; ++i)
+  for (uint32_t i = 0; i < limit; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   if (err) atomicOr(err, code);
   dead = true;

@@ -25,22 +25,39 @@ def _opts(diis_size, max_iterations, energy_tolerance, density_tolerance, precis
                      mixed_switch, mixing)
 
 
-def _result(res, P, hist):
+def _result(res, P, hist, orbitals=None):
     it = int(res.iterations)
-    return dict(energy=res.electronic_energy, iterations=it, converged=bool(res.converged), P=P,
-                history=hist[:it].copy(), seconds=res.seconds, mixed_iterations=int(res.mixed_iterations),
-                fp64_iterations=int(res.fp64_iterations),
-                phase_ms=dict(build=res.build_ms, diis=res.diis_ms, density=res.density_ms))
+    out = dict(energy=res.electronic_energy, iterations=it, converged=bool(res.converged), P=P,
+               history=hist[:it].copy(), seconds=res.seconds, mixed_iterations=int(res.mixed_iterations),
+               fp64_iterations=int(res.fp64_iterations),
+               phase_ms=dict(build=res.build_ms, diis=res.diis_ms, density=res.density_ms))
+    if orbitals is not None:
+        out.update(orbitals)
+    return out
+
+
+def _request_orbitals(res, n, n_eff, cplx):
+    """Host arrays for the loop's optional outputs (the reference's orbital_energies, c_matrix and
+    fock_matrix), their pointers set in the result struct."""
+    dt = np.complex128 if cplx else np.float64
+    o = dict(orbital_energies=np.empty(n_eff), c_matrix=np.empty((n, n_eff), dtype=dt),
+             fock_matrix=np.empty((n, n), dtype=dt))
+    res.orbital_energies = o["orbital_energies"].ctypes.data
+    res.c_matrix = o["c_matrix"].ctypes.data
+    res.fock_matrix = o["fock_matrix"].ctypes.data
+    return o
 
 
 def runNonRelativisticHartreeFock(eri: RiNonRelEriSource, h_core, x_large, initial_density, n_electrons: int,
                                   diis_size: int = 5, max_iterations: int = 100, energy_tolerance: float = 1e-8,
                                   density_tolerance: float = 1e-6, precision: str = "fp64",
-                                  mixed_switch: float = 0.0) -> dict:
+                                  mixed_switch: float = 0.0, orbitals: bool = False) -> dict:
     """RHF SCF on the GPU; returns energy (electronic), iterations, converged, density P, the
     per-iteration energy history, wall seconds and the mixed / FP64 build counts.  precision="mixed":
     FP64 first build, then incremental split-BF16 exchange, one FP64 build of the final density;
-    mixed_switch > 0 re-seeds the accumulated exchange once in FP64 when |dE| < mixed_switch."""
+    mixed_switch > 0 re-seeds the accumulated exchange once in FP64 when |dE| < mixed_switch.
+    orbitals=True also returns the reference result's orbital_energies, c_matrix and fock_matrix
+    (one device diagonalisation of X^T F X at the end of the loop)."""
     n = eri.nl
     h = _host(h_core, np.float64)
     X = _host(x_large, np.float64)
@@ -48,21 +65,22 @@ def runNonRelativisticHartreeFock(eri: RiNonRelEriSource, h_core, x_large, initi
     P0 = _host(initial_density, np.float64)
     so = _opts(diis_size, max_iterations, energy_tolerance, density_tolerance, precision, mixed_switch)
     res = L.ScfResult()
+    orb = _request_orbitals(res, n, X.shape[1], False) if orbitals else None
     P = np.empty((n, n))
     hist = np.full(max_iterations, np.nan)
     L.check(L.lib().rr_scf_run_nonrel(eri.store.handle, _ptr(h), _ptr(X), X.shape[1], _ptr(S), _ptr(P0), n_electrons,
                                       ctypes.byref(so), ctypes.byref(res), _ptr(P), _ptr(hist), ctypes.byref(L.opts())))
-    return _result(res, P, hist)
+    return _result(res, P, hist, orb)
 
 
 def runX2CHartreeFockScf(h_x2c, eri: RiX2cEriSource, x_large, initial_density, n_electrons: int, overlap=None,
                          diis_size: int = 5, max_iterations: int = 100, energy_tolerance: float = 1e-8,
                          density_tolerance: float = 1e-6, kramers_restricted: bool = True, mixing: float = 1.0,
-                         precision: str = "fp64", mixed_switch: float = 0.0) -> dict:
+                         precision: str = "fp64", mixed_switch: float = 0.0, orbitals: bool = False) -> dict:
     """X2C-HF on the GPU (rr_scf_run_x2c).  `overlap` defaults to the source's overlap.
     precision="mixed": incremental split-BF16 exchange, the last iteration an FP64 build of the
     converged density; mixed_switch > 0 re-seeds the accumulated exchange once in FP64 when
-    |dE| < mixed_switch."""
+    |dE| < mixed_switch.  orbitals as for runNonRelativisticHartreeFock."""
     n = 2 * eri.nl
     S = _host(eri.overlap if overlap is None else overlap, np.complex128)
     h = _host(h_x2c, np.complex128)
@@ -73,19 +91,21 @@ def runX2CHartreeFockScf(h_x2c, eri: RiX2cEriSource, x_large, initial_density, n
     so = _opts(diis_size, max_iterations, energy_tolerance, density_tolerance, precision, mixed_switch,
                kramers_restricted, mixing)
     res = L.ScfResult()
+    orb = _request_orbitals(res, n, X.shape[1], True) if orbitals else None
     P = np.empty((n, n), dtype=np.complex128)
     hist = np.full(max_iterations, np.nan)
     L.check(L.lib().rr_scf_run_x2c(eri.store.handle, _ptr(h), _ptr(X), X.shape[1], _ptr(S), _ptr(P0), n_electrons,
                                    ctypes.byref(so), ctypes.byref(res), _ptr(P), _ptr(hist), ctypes.byref(L.opts())))
-    return _result(res, P, hist)
+    return _result(res, P, hist, orb)
 
 
 def runDiracHartreeFockScf(h_rkb, eri: RiDirectEriSource, x_full, initial_density, n_electrons: int, overlap=None,
                            diis_size: int = 5, max_iterations: int = 100, energy_tolerance: float = 1e-8,
                            density_tolerance: float = 1e-6, kramers_restricted: bool = True,
-                           mixing: float = 1.0, precision: str = "fp64", mixed_switch: float = 0.0) -> dict:
-    """4c-DHF on the GPU (rr_scf_run_dhf).  `overlap` defaults to the source's s_full.  precision and
-    mixed_switch as for runX2CHartreeFockScf."""
+                           mixing: float = 1.0, precision: str = "fp64", mixed_switch: float = 0.0,
+                           orbitals: bool = False) -> dict:
+    """4c-DHF on the GPU (rr_scf_run_dhf).  `overlap` defaults to the source's s_full.  precision,
+    mixed_switch and orbitals as for runX2CHartreeFockScf."""
     h = _host(h_rkb, np.complex128)
     n = h.shape[0]
     S = _host(eri.s_full if overlap is None else overlap, np.complex128)
@@ -97,11 +117,12 @@ def runDiracHartreeFockScf(h_rkb, eri: RiDirectEriSource, x_full, initial_densit
     so = _opts(diis_size, max_iterations, energy_tolerance, density_tolerance, precision, mixed_switch,
                kramers_restricted, mixing)
     res = L.ScfResult()
+    orb = _request_orbitals(res, n, X.shape[1], True) if orbitals else None
     P = np.empty((n, n), dtype=np.complex128)
     hist = np.full(max_iterations, np.nan)
     L.check(L.lib().rr_scf_run_dhf(eri.store.handle, _ptr(h), _ptr(v), n, _ptr(S), _ptr(X), _ptr(P0), n_electrons,
                                    ctypes.byref(so), ctypes.byref(res), _ptr(P), _ptr(hist), ctypes.byref(L.opts())))
-    return _result(res, P, hist)
+    return _result(res, P, hist, orb)
 
 
 def runX2CHartreeFockScfBatch(problems, workers: int = 16, diis_size: int = 5, max_iterations: int = 100,

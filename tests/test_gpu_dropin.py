@@ -33,6 +33,16 @@ def _cases():
             assert np.abs(ref.nonrel_fock(g["h"], g["B"], g["D"], g["S"], g["X"]) - g["F"]).max() <= TOL, p.stem
         if "D_mix" in g:
             assert np.abs(ref.nonrel_fock(g["h"], g["B"], g["D_mix"], g["S"], g["X"]) - g["F_mix"]).max() <= TOL
+    # B rewritten in the same host buffer (one symmetric pair of entries of one aux row changed): the
+    # resident-tensor cache must see the new contents and upload them
+    from oracle import ri_oracle
+    g = golden("nonrel_fock_n24_naux129")
+    B2 = g["B"].copy()
+    B2[77, 5 * 24 + 17] += 0.25
+    B2[77, 17 * 24 + 5] += 0.25
+    F2 = ref.nonrel_fock(g["h"], B2, g["D"], g["S"], g["X"])
+    assert np.abs(F2 - ri_oracle.nonrel_fock(g["h"], B2, g["D"], g["S"], g["X"])).max() <= TOL
+    assert np.abs(F2 - g["F"]).max() > 1e-6
     for p in sorted(GOLDEN.glob("x2c_fock_*.npz")):
         g = golden(p.stem)
         assert np.abs(ref.x2c_fock(g["h"], g["B"], g["P"], g["S"], g["X"]) - g["F"]).max() <= TOL, p.stem

@@ -113,7 +113,7 @@ def test_nonrel_incremental_exchange_matches_difference():
 
 
 @pytest.mark.parametrize("kind", ["x2c", "dhf"])
-def test_mixed_scf_reaches_fp64_energy(kind):
+def test_mixed_scf_reaches_fp64_energy(ref_lib, kind):
     if kind == "x2c":
         s = synth.x2c_system(40, 160, 10, seed=22)
 
@@ -126,6 +126,10 @@ def test_mixed_scf_reaches_fp64_energy(kind):
             return scf.runDiracHartreeFockScf(s["h"], _rkb_src(s), s["x_full"], s["P0"], int(s["n_electrons"]), **kw)
     r64 = run()
     rm = run(precision="mixed")
+    # the reference's own FP64 loop (compiled from its sources) is the judge of the mixed energy
+    rr = ref_lib.x2c_scf(s) if kind == "x2c" else ref_lib.dhf_scf(s)
+    assert rr["converged"]
+    assert abs(rm["energy"] - rr["energy"]) <= 1e-8
     assert r64["converged"] and rm["converged"]
     assert rm["mixed_iterations"] >= 2 and rm["fp64_iterations"] == 1
     assert rm["iterations"] == rm["mixed_iterations"] + 1
@@ -134,3 +138,4 @@ def test_mixed_scf_reaches_fp64_energy(kind):
     rs = run(precision="mixed", mixed_switch=1e-4)  # one FP64 re-seed of the accumulated exchange
     assert rs["converged"] and rs["fp64_iterations"] in (1, 2)  # the re-seed happens only if |dE| gets below 1e-4 first
     assert abs(rs["energy"] - r64["energy"]) <= 1e-8
+    assert abs(rs["energy"] - rr["energy"]) <= 1e-8

@@ -53,9 +53,9 @@ def test_nonrel_vs_oracle(n, naux):
     src = ri.RiNonRelEriSource(n, B, np.eye(n), np.eye(n))
     m = mo.buildRiNonRelSpinMoEri(src, n, C)
     ref = o.nonrel_mo_build(B, C)
-    assert np.abs(m.b() - ref).max() <= TOL * max(1.0, np.abs(ref).max())
+    assert np.abs(m.b() - ref).max() <= TOL
     U = np.kron(np.eye(2), synth.random_orthogonal(n, rng))
-    assert np.abs(m.rotated(U).b() - o.nonrel_mo_rotated(ref, n, U)).max() <= TOL * max(1.0, np.abs(ref).max())
+    assert np.abs(m.rotated(U).b() - o.nonrel_mo_rotated(ref, n, U)).max() <= TOL
     po = (np.arange(2 * n) + n) % (2 * n)
     J, K, Lm = m.jkl(po)
     quads = np.array([[i, j, i, j] for i in range(2 * n) for j in range(2 * n)])
@@ -64,8 +64,7 @@ def test_nonrel_vs_oracle(n, naux):
     Ke = o.nonrel_mo_eri(ref, n, quads).reshape(2 * n, 2 * n)
     quads = np.array([[po[i], j, j, po[i]] for i in range(2 * n) for j in range(2 * n)])
     Le = o.nonrel_mo_eri(ref, n, quads).reshape(2 * n, 2 * n)
-    sc = max(1.0, np.abs(Je).max())
-    assert np.abs(J - Je).max() <= TOL * sc and np.abs(K - Ke).max() <= TOL * sc and np.abs(Lm - Le).max() <= TOL * sc
+    assert np.abs(J - Je).max() <= TOL and np.abs(K - Ke).max() <= TOL and np.abs(Lm - Le).max() <= TOL
 
 
 @pytest.mark.parametrize("nl,ns,naux,nt", [(3, 5, 11, 7), (10, 20, 60, 24), (25, 40, 100, 60)])
@@ -77,15 +76,13 @@ def test_ukb_vs_oracle(nl, ns, naux, nt):
     src = ri.RiDirectEriSource(nl, ns, B_LL, B_SS)
     m = mo.buildRiMoEri(src, c)
     ref = o.ri_mo_build(nl, ns, B_LL, B_SS, c)
-    sc = max(1.0, np.abs(ref).max())
-    assert np.abs(m.b() - ref).max() <= TOL * sc
+    assert np.abs(m.b() - ref).max() <= TOL
     U = synth.random_unitary(nt, rng)
-    assert np.abs(m.rotated(U).b() - o.ri_mo_rotated(ref, nt, U)).max() <= TOL * sc
+    assert np.abs(m.rotated(U).b() - o.ri_mo_rotated(ref, nt, U)).max() <= TOL
     po = np.arange(nt) ^ 1 if nt % 2 == 0 else np.arange(nt)
     J, K, Lm = m.jkl(po)
     Jo, Ko, Lo = o.jkl_matrices(ref, nt, po)
-    s2 = max(1.0, np.abs(Jo).max())
-    assert np.abs(J - Jo).max() <= TOL * s2 and np.abs(K - Ko).max() <= TOL * s2 and np.abs(Lm - Lo).max() <= TOL * s2
+    assert np.abs(J - Jo).max() <= TOL and np.abs(K - Ko).max() <= TOL and np.abs(Lm - Lo).max() <= TOL
 
 
 def test_hx_fock_golden():
@@ -112,7 +109,7 @@ def test_hx_fock_vs_oracle(n, naux):
     m = mo.RiMoEri.from_tensor(B, n)
     F = mo.hartreeExchangeFockMatrix(h, m, occ, h2, x2, po, l1, l2)
     Fo = o.hx_fock(h, B, occ, h2, x2, po, l1, l2)
-    assert np.abs(F - Fo).max() <= TOL * max(1.0, np.abs(Fo).max())
+    assert np.abs(F - Fo).max() <= TOL
 
 
 def test_errors_like_reference():

@@ -185,6 +185,6 @@ def test_learned_preconditioner_cuts_macro_iterations():
                 tot[mode] += r["macro_iterations"]
                 e[mode] = r["energy"]
                 prob.close()
-            assert abs(e["learned"] - e["plain"]) <= 1e-7
+            assert abs(e["learned"] - e["plain"]) <= 1e-8
     assert tot["learned"] <= 0.70 * tot["plain"], tot  # at least 30 % fewer macro-iterations
     net.close()

@@ -38,9 +38,11 @@ def test_nonrel_vs_oracle(n, naux, nocc, seed):
 
 
 @pytest.mark.parametrize("n,naux,nocc,seed", [(60, 200, 8, 4), (128, 400, 16, 5)])
-def test_nonrel_mixed_reaches_fp64_energy(n, naux, nocc, seed):
+def test_nonrel_mixed_reaches_fp64_energy(ref_lib, n, naux, nocc, seed):
     s = synth.nonrel_system(n, naux, nocc, seed=seed)
     r64 = _run(s)
+    rr = ref_lib.nonrel_scf(s)  # the reference's own FP64 loop
+    assert rr["converged"] and abs(r64["energy"] - rr["energy"]) <= 1e-8
     for switch in (0.0, 1e-5):  # incremental only / one FP64 re-seed of the accumulated exchange
         rm = _run(s, precision="mixed", mixed_switch=switch)
         assert r64["converged"] and rm["converged"]
@@ -49,6 +51,7 @@ def test_nonrel_mixed_reaches_fp64_energy(n, naux, nocc, seed):
         assert rm["fp64_iterations"] == (2 if switch == 0.0 else rm["fp64_iterations"]) <= 3
         assert rm["iterations"] == rm["mixed_iterations"] + rm["fp64_iterations"]
         assert abs(rm["energy"] - r64["energy"]) <= 1e-8
+        assert abs(rm["energy"] - rr["energy"]) <= 1e-8
 
 
 def _run_x2c(sysd, **kw):

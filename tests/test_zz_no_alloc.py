@@ -87,11 +87,15 @@ def test_noalloc_leaves_free_memory_unchanged():
     dJ = torch.empty((n, n), dtype=torch.float64, device="cuda")
     _noalloc_dev(store, dD, dJ)  # first call on the device: address lookup
     torch.cuda.synchronize()
+    allocs0 = L.lib().rr_test_device_allocations()
     free0, _ = torch.cuda.mem_get_info()
     for _ in range(3):
         _noalloc_dev(store, dD, dJ)
     torch.cuda.synchronize()
     free1, _ = torch.cuda.mem_get_info()
+    # the library's own count of its cudaMalloc calls is the primary check; free device memory (a
+    # device-wide reading that other activity could move) is the secondary one
+    assert L.lib().rr_test_device_allocations() == allocs0
     assert free1 == free0
     store.close()
 
