@@ -92,6 +92,47 @@ int rr_ri_create_4c(const double* B_LL, const double* B_SS, int64_t naux, int64_
 
 int rr_ri_destroy(rr_ri_handle h);
 
+/* ---------------- one-time set-up on the device ---------------- */
+
+/* RankReductionReport (src/Linear_Algebra/LinearAlgebra.h). */
+typedef struct rr_rank_report {
+  int64_t n_kept, n_dropped;
+  double smallest_kept, largest_dropped; /* 0 when nothing was kept / dropped (or all dropped are <= 0) */
+} rr_rank_report;
+
+/* canonicalOrthogonalize (hermitian = 0, real S) / canonicalOrthogonalizeHermitian (hermitian = 1,
+ * interleaved complex S), src/Linear_Algebra/LinearAlgebra.cpp:267-349, on the device (cuSOLVER
+ * eigensolver): the eigenvectors of S (of D^-1 S D^-1, D = diag(sqrt(Re S_ii)), for the Hermitian
+ * form) whose eigenvalues exceed `threshold` (X_LIN_DEP_THRS_L / _S; 1e-10 for the aux metric), scaled
+ * by 1/sqrt(eigenvalue) (and D^-1): X^dagger S X = I.  When nothing is dropped the real form returns
+ * the symmetric S^-1/2 = U w^-1/2 U^T, as the reference does.  X must hold n*n elements; on return its
+ * first n * n_eff elements are the n x n_eff matrix (row-major).  report may be NULL.  The reference
+ * uses it for the AO overlaps (main.cpp:4476, 4544, 4584) and for the aux metric (X_metric,
+ * src/AO_ints/ThreeCenterIntegrals.cpp:185-189).  Columns are determined up to sign / phase (and a
+ * rotation inside a degenerate eigenvalue), as LAPACK's are. */
+int rr_canonical_orthogonalize(const double* S, int64_t n, int32_t hermitian, double threshold, double* X,
+                               int64_t* n_eff, rr_rank_report* report, const rr_opts* opts);
+
+/* B = metric_x^T raw (naux_kept x n2): the metric contraction of riThreeCenterTensor,
+ * src/AO_ints/ThreeCenterIntegrals.cpp:219-236, on the FP64 tensor cores.  raw: (naux_raw, n2) raw
+ * 3-centre integrals (libcint's, from the host); metric_x: naux_raw x naux_kept (e.g. from
+ * rr_canonical_orthogonalize of the aux metric). */
+int rr_ri_three_center_tensor(const double* raw, int64_t naux_raw, int64_t n2, const double* metric_x,
+                              int64_t naux_kept, double* B, const rr_opts* opts);
+
+/* transformRiThreeCenterAoLegs, src/AO_ints/ThreeCenterIntegrals.cpp:191-217: B_out^P = t^T B_in^P t
+ * per aux row (B_in: naux x n_ao^2, t: n_ao x n_out, B_out: naux x n_out^2), e.g. Cartesian ->
+ * spherical / LOWGEN legs. */
+int rr_ri_transform_ao_legs(const double* B_in, int64_t naux, int64_t n_ao, const double* t, int64_t n_out,
+                            double* B_out, const rr_opts* opts);
+
+/* A resident RI handle built on the device from the raw 3-centre integrals, as the reference builds its
+ * source tensor (main.cpp:1108, 4922): B = metric_x^T raw (rr_ri_three_center_tensor), then, when t is
+ * not NULL, t^T B^P t (rr_ri_transform_ao_legs; n = n_out), else n = n_ao.  The result is the handle
+ * rr_ri_create would give for that B; mem applies to raw, metric_x and t. */
+int rr_ri_create_raw(const double* raw, int64_t naux_raw, int64_t n_ao, const double* metric_x, int64_t naux_kept,
+                     const double* t, int64_t n_out, int32_t mem, rr_ri_handle* out);
+
 /* naux, n (nl for 4c) and ns (0 for a single-tensor handle). */
 int rr_ri_info(rr_ri_handle h, int64_t* naux, int64_t* n, int64_t* ns);
 
@@ -306,6 +347,87 @@ typedef struct rr_x2c_instance {
  * GPU.  Host pointers.  Returns RR_OK when every instance succeeded, else the first failing
  * instance's code (all instances run; each reports its own status). */
 int rr_scf_run_x2c_batch(rr_x2c_instance* instances, int64_t count, const rr_scf_opts* scf, int32_t workers);
+
+/* ---------------- RESTART files and the hand-over between runs of a scan ----------------
+ * The reference's binary RESTART format (src/Utils/Restart.h:14-70), byte for byte: a file written by
+ * rr_restart_write is read by the reference's readRestart and the other way round.  Strings are
+ * NUL-terminated; vectors are pointer + count; coefficients are rows x cols row-major (interleaved
+ * complex when complex_coefficients).  Version 3 is written; versions 2 and 3 are read. */
+typedef struct rr_restart {
+  const char* method;     /* "NON_REL" | "X2C" | "4C" */
+  const char* functional; /* the FUNCTIONAL keyword */
+  const char* kind;       /* "OCCUPATIONS" | "GAMMAS" | "PCCD" | "CASSCF" */
+  uint64_t basis_fingerprint;
+  int64_t n_electrons, pnof_subspaces, pnof_coupling, n_core, jk_frozen_pairs, jk_active_pairs;
+  double total_energy;
+  int32_t orbitals_optimized, converged;
+  const double* occupations;
+  int64_t n_occupations;
+  const double* gammas;
+  int64_t n_gammas;
+  const double* amplitudes;
+  int64_t n_amplitudes;
+  int32_t complex_coefficients;
+  int64_t rows, cols;
+  const double* coefficients;
+  int64_t cas_electrons, cas_spinors;
+  const double* cas_state;
+  int64_t n_cas_state;
+} rr_restart;
+
+/* writeRestart, src/Utils/Restart.cpp:94-145 (the same checks and messages).  Host only, no GPU. */
+int rr_restart_write(const char* path, const rr_restart* data);
+/* readRestart, src/Utils/Restart.cpp:147-197: fills *out with library-owned strings and arrays, which
+ * rr_restart_release frees.  Host only, no GPU. */
+int rr_restart_read(const char* path, rr_restart* out);
+int rr_restart_release(rr_restart* data);
+/* restartCoefficients, src/Utils/Restart.cpp:199-206: C = C_scf U on the GPU (C_scf rows x n_mo, U
+ * n_mo x n_mo; U NULL = identity).  cplx: interleaved complex operands. */
+int rr_restart_coefficients(const double* c_scf, int64_t rows, int64_t n_mo, const double* u, int32_t cplx,
+                            double* c_out, const rr_opts* opts);
+/* The starting density of the next run of a scan from a RESTART file's orbitals: P = C diag(occ) C^dagger
+ * (rows x rows) on the GPU; for the SCF loops' conventions pass occupations 2 (RHF, spatial orbitals) or
+ * 1 (spinors) on the occupied columns.  No counterpart in the reference, whose READ_RESTART path builds
+ * the density on the host. */
+int rr_density_from_orbitals(const double* C, int64_t rows, int64_t cols, const double* occupations, int32_t cplx,
+                             double* P, const rr_opts* opts);
+
+/* ---------------- RI sigma-vector Hessian-vector primitives (NEO orbital Hessian) ----------------
+ * The GEMM engine behind the reference's RI Hessian-vector products (src/Hessian_opt/RiSigmaGemm.h,
+ * src/Hessian_opt/RiSigmaHessianToolkit.h).  Tensors are (naux, n^2) row-major, element [P, i n + j];
+ * cplx = 1: interleaved complex (RiMoEri's tensors), 0: real.  The real matrices (K, w, post, Wm) multiply
+ * the complex values unconjugated, as in the reference.  All pointers host or device as opts->mem says. */
+
+/* One operand of pairContract (RiSigmaGemm.h:21-41, PairOp): value(P, t, x) = [s ? s(P, idx[t n + x]) : 1]
+ * * [w ? w[t n + x] : 1] * [row ? row(P, t) : 1], right-multiplied by `post` when given:
+ * value(P, t, x) = sum_a v(P, t, a) post(a, x). */
+typedef struct rr_pair_op {
+  const double* s;      /* naux x n^2 (complex when cplx) or NULL */
+  const uint32_t* idx;  /* n^2 indices into one row of s (needed with s) */
+  const double* w;      /* n^2 real weights or NULL */
+  const double* row;    /* naux x n (complex when cplx) or NULL */
+  const double* post;   /* real n x n or NULL */
+} rr_pair_op;
+
+/* buildRiSigmaHessianToolkit(n, B, K), src/Hessian_opt/RiSigmaHessianToolkit.cpp:24-55: KB1[P] = K B^P,
+ * KB2[P] = B^P K (naux x n^2 each) and Bdiag, KB1diag, KB2diag (naux x n each); K real n x n. */
+int rr_sigma_toolkit(const double* B, int64_t n, int64_t naux, int32_t cplx, const double* K, double* kb1, double* kb2,
+                     double* bdiag, double* kb1diag, double* kb2diag, const rr_opts* opts);
+
+/* pairContract, src/Hessian_opt/RiSigmaGemm.cpp:65-95: target(x, y) += sign sum_{P,t} F(P,t,x) G(P,t,y)
+ * (target n x n, in and out). */
+int rr_sigma_pair_contract(double* target, double sign, int64_t n, int64_t naux, int32_t cplx, const rr_pair_op* f,
+                           const rr_pair_op* g, const rr_opts* opts);
+
+/* diagContract, src/Hessian_opt/RiSigmaGemm.cpp:97-114: target(a, b) += sum_P S(P, b n + a)
+ * (Ua(P, a) + Ub(P, b)); Ua / Ub (naux x n) may be NULL. */
+int rr_sigma_diag_contract(double* target, int64_t n, int64_t naux, int32_t cplx, const double* S, const double* Ua,
+                           const double* Ub, const rr_opts* opts);
+
+/* accumU, src/Hessian_opt/RiSigmaGemm.cpp:116-126: U(P, x) += alpha sum_t D[P n + t] Wm(x, t)
+ * (U, D: naux x n; Wm real n x n). */
+int rr_sigma_accum_u(double* U, double alpha, int64_t n, int64_t naux, int32_t cplx, const double* D, const double* Wm,
+                     const rr_opts* opts);
 
 /* ---------------- orbital-rotation optimisation (functional stage) ---------------- */
 

@@ -246,6 +246,31 @@ def _orb_ptrs(o):
     return _p(o["orbital_energies"]), _p(o["c_matrix"]), _p(o["fock_matrix"])
 
 
+def canonical_orth_report(S, thr=1e-10):
+    """canonicalOrthogonalize{,Hermitian} with its RankReductionReport (n_kept, n_dropped, smallest_kept,
+    largest_dropped)."""
+    n = S.shape[0]
+    herm = np.iscomplexobj(S)
+    n_eff = _i64(0)
+    X = np.zeros((n * n,), dtype=np.complex128 if herm else np.float64)
+    rep = np.zeros(4)
+    Sc = _c(S) if herm else _d(S)
+    _check(lib().rrref_canonical_orth_report(_i64(n), _p(Sc), ctypes.c_int(1 if herm else 0), ctypes.c_double(thr),
+                                             _p(X), ctypes.byref(n_eff), _p(rep)))
+    return X[: n * n_eff.value].reshape(n, n_eff.value), dict(n_kept=int(rep[0]), n_dropped=int(rep[1]),
+                                                              smallest_kept=rep[2], largest_dropped=rep[3])
+
+
+def transform_ao_legs(B, n_ao, t):
+    """transformRiThreeCenterAoLegs (src/AO_ints/ThreeCenterIntegrals.cpp:191-217): t^T B^P t per aux row."""
+    B = _d(B)
+    t = _d(t)
+    naux, n_out = B.shape[0], t.shape[1]
+    out = np.empty((naux, n_out * n_out))
+    _check(lib().rrref_transform_ao_legs(_i64(naux), _i64(n_ao), _p(B), _i64(n_out), _p(t), _p(out)))
+    return out
+
+
 def nonrel_scf(sysd, diis_size=5, max_iter=100, e_tol=1e-8, d_tol=1e-6):
     """runNonRelativisticHartreeFock (RI overload): energy, iterations, converged, density, energy history
     and the result's orbital_energies, c_matrix and fock_matrix."""
@@ -373,3 +398,80 @@ def hx_energy_nonrel(Bmo_spatial, n_sp, h, occ, h2, x2, pair_of=None, l1=None, l
                                         None if po is None else _p(_d(l1)), None if po is None else _p(_d(l2)),
                                         ctypes.byref(E)))
     return E.value
+
+
+# ---------------------------------------------------------------- RI sigma-vector Hessian-vector primitives
+# src/Hessian_opt/RiSigmaGemm.cpp (pairContract, diagContract, accumU) and RiSigmaHessianToolkit.cpp.
+
+
+def _cplx_of(*arrs):
+    return any(a is not None and np.iscomplexobj(a) for a in arrs)
+
+
+def _cv(a, cplx):
+    return None if a is None else (_c(a) if cplx else _d(a))
+
+
+def sigma_toolkit(B, n, K):
+    """buildRiSigmaHessianToolkit(n, B, K): KB1[P] = K B^P, KB2[P] = B^P K and the three diagonals."""
+    cplx = np.iscomplexobj(B)
+    naux = B.shape[0]
+    dt = np.complex128 if cplx else np.float64
+    kb1, kb2 = np.empty((naux, n * n), dtype=dt), np.empty((naux, n * n), dtype=dt)
+    bd, k1d, k2d = (np.empty((naux, n), dtype=dt) for _ in range(3))
+    _check(lib().rrref_sigma_toolkit(_i64(n), _i64(naux), ctypes.c_int(1 if cplx else 0), _p(_cv(B, cplx)),
+                                     _p(_d(K)), _p(kb1), _p(kb2), _p(bd), _p(k1d), _p(k2d)))
+    return dict(kb1=kb1, kb2=kb2, bdiag=bd, kb1diag=k1d, kb2diag=k2d)
+
+
+def _op_ptrs(op, cplx):
+    s = op.get("s")
+    idx = None if s is None else np.ascontiguousarray(op["idx"], dtype=np.uint32)
+    keep = [_cv(s, cplx), idx, _cv(op.get("w"), False), _cv(op.get("row"), cplx), _cv(op.get("post"), False)]
+    return keep, [None if a is None else _p(a) for a in keep]
+
+
+def sigma_pair_contract(target, sign, n, naux, f, g):
+    """pairContract: target(x,y) + sign sum_{P,t} F(P,t,x) G(P,t,y); an operand is a dict with optional
+    s (naux x n^2), idx (n^2 indices into an s row), w (n^2), row (naux x n), post (real n x n)."""
+    cplx = _cplx_of(target, f.get("s"), g.get("s"), f.get("row"), g.get("row"))
+    out = np.array(target, dtype=np.complex128 if cplx else np.float64, copy=True, order="C")
+    kf, pf = _op_ptrs(f, cplx)
+    kg, pg = _op_ptrs(g, cplx)
+    _check(lib().rrref_sigma_pair_contract(_i64(n), _i64(naux), ctypes.c_int(1 if cplx else 0),
+                                           ctypes.c_double(sign), _p(out), *pf, *pg))
+    return out
+
+
+def sigma_diag_contract(target, n, naux, S, Ua=None, Ub=None):
+    """diagContract: target(a,b) + sum_P S(P, b n + a) (Ua(P,a) + Ub(P,b))."""
+    cplx = _cplx_of(target, S, Ua, Ub)
+    out = np.array(target, dtype=np.complex128 if cplx else np.float64, copy=True, order="C")
+    ua, ub = _cv(Ua, cplx), _cv(Ub, cplx)
+    _check(lib().rrref_sigma_diag_contract(_i64(n), _i64(naux), ctypes.c_int(1 if cplx else 0), _p(out),
+                                           _p(_cv(S, cplx)), None if ua is None else _p(ua),
+                                           None if ub is None else _p(ub)))
+    return out
+
+
+def sigma_accum_u(U, alpha, n, naux, D, Wm):
+    """accumU: U(P,x) + alpha sum_t D[P n + t] Wm(x,t)."""
+    cplx = _cplx_of(U, D)
+    out = np.array(U, dtype=np.complex128 if cplx else np.float64, copy=True, order="C")
+    _check(lib().rrref_sigma_accum_u(_i64(n), _i64(naux), ctypes.c_int(1 if cplx else 0), _p(out),
+                                     ctypes.c_double(alpha), _p(_cv(D, cplx)), _p(_d(Wm))))
+    return out
+
+
+# ---------------------------------------------------------------- RESTART files (src/Utils/Restart.cpp)
+
+
+def restart_write(path, fields):
+    """The reference's writeRestart from an rr_restart record (rerdmft_b200._lib.Restart, a plain carrier
+    of the same fields)."""
+    _check(lib().rrref_restart_write(str(path).encode(), ctypes.byref(fields)))
+
+
+def restart_rewrite(in_path, out_path):
+    """The reference's readRestart of in_path written back with its writeRestart to out_path."""
+    _check(lib().rrref_restart_rewrite(str(in_path).encode(), str(out_path).encode()))

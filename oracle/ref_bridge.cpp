@@ -34,6 +34,10 @@
 #include "HartreeExchangeHessian.h"
 #include "OrbitalGradient.h"
 #include "SpinorRotation.h"
+#include "ThreeCenterIntegrals.h"
+#include "RiSigmaHessianToolkit.h"
+#include "Restart.h"
+#include "../include/rr_ri.h"
 
 extern "C" void scipy_openblas_set_num_threads(int n);
 
@@ -333,6 +337,205 @@ int rrref_canonical_orth(i64 n, const double* S, double thr, double* X_out, i64*
     auto x = rerdmft::canonicalOrthogonalize(toMatrix(S, n, n), thr);
     *n_eff = static_cast<i64>(x.cols());
     fromMatrix(x, X_out);
+  });
+}
+// canonicalOrthogonalize / canonicalOrthogonalizeHermitian with the RankReductionReport
+// (src/Linear_Algebra/LinearAlgebra.cpp:267 and :312): report = {n_kept, n_dropped, smallest_kept,
+// largest_dropped}.
+int rrref_canonical_orth_report(i64 n, const double* S, int hermitian, double thr, double* X_out, i64* n_eff,
+                                double* report) {
+  return guard([&] {
+    rerdmft::RankReductionReport r;
+    if (hermitian) {
+      auto x = rerdmft::canonicalOrthogonalizeHermitian(toCMatrix(S, n, n), thr, &r);
+      *n_eff = static_cast<i64>(x.cols());
+      fromCMatrix(x, X_out);
+    } else {
+      auto x = rerdmft::canonicalOrthogonalize(toMatrix(S, n, n), thr, &r);
+      *n_eff = static_cast<i64>(x.cols());
+      fromMatrix(x, X_out);
+    }
+    report[0] = static_cast<double>(r.n_kept);
+    report[1] = static_cast<double>(r.n_dropped);
+    report[2] = r.smallest_kept;
+    report[3] = r.largest_dropped;
+  });
+}
+}  // extern "C": the helpers below are templates
+
+// ---- RI sigma-vector Hessian-vector primitives (src/Hessian_opt/RiSigmaGemm.cpp,
+// src/Hessian_opt/RiSigmaHessianToolkit.cpp).  Complex operands are interleaved (cplx = 1).
+
+template <typename T>
+static rerdmft::Matrix<T> sigmaMat(const double* p, i64 r, i64 c) {
+  if constexpr (std::is_same_v<T, double>) return toMatrix(p, r, c);
+  else return toCMatrix(p, r, c);
+}
+template <typename T>
+static void sigmaOut(const rerdmft::Matrix<T>& m, double* out) {
+  if constexpr (std::is_same_v<T, double>) fromMatrix(m, out);
+  else fromCMatrix(m, out);
+}
+template <typename T>
+static void sigmaVecOut(const std::vector<T>& v, double* out) {
+  std::memcpy(out, v.data(), sizeof(T) * v.size());
+}
+
+template <typename T>
+static void sigmaToolkit(i64 n, i64 naux, const double* B, const double* K, double* kb1, double* kb2, double* bdiag,
+                         double* kb1diag, double* kb2diag) {
+  auto b = sigmaMat<T>(B, naux, n * n);
+  auto t = rerdmft::buildRiSigmaHessianToolkit<T>(static_cast<std::size_t>(n), b, toMatrix(K, n, n));
+  sigmaOut(t.kb1, kb1);
+  sigmaOut(t.kb2, kb2);
+  sigmaVecOut(t.bdiag, bdiag);
+  sigmaVecOut(t.kb1diag, kb1diag);
+  sigmaVecOut(t.kb2diag, kb2diag);
+}
+
+// One PairOp from flat tables: s (naux x n^2, nullable), idx (n^2 uint32), w (n^2, nullable), row
+// (naux x n, nullable), post (real n x n, nullable).
+template <typename T>
+struct SigmaOp {
+  rerdmft::Matrix<T> s, row;
+  rerdmft::Matrix<double> post;
+  rerdmft::risigma::PairOp<T> op;
+  SigmaOp(i64 n, i64 naux, const double* sp, const std::uint32_t* idx, const double* w, const double* rowp,
+          const double* postp) {
+    const std::size_t n2 = static_cast<std::size_t>(n * n);
+    if (sp) {
+      s = sigmaMat<T>(sp, naux, n * n);
+      op.s = &s;
+      op.idx.assign(idx, idx + n2);
+    }
+    if (w) op.w.assign(w, w + n2);
+    if (rowp) {
+      row = sigmaMat<T>(rowp, naux, n);
+      op.row = &row;
+    }
+    if (postp) {
+      post = toMatrix(postp, n, n);
+      op.post = &post;
+    }
+  }
+};
+
+template <typename T>
+static void sigmaPair(i64 n, i64 naux, double sign, double* target, const double* fs, const std::uint32_t* fidx,
+                      const double* fw, const double* frow, const double* fpost, const double* gs,
+                      const std::uint32_t* gidx, const double* gw, const double* grow, const double* gpost) {
+  auto tgt = sigmaMat<T>(target, n, n);
+  SigmaOp<T> f(n, naux, fs, fidx, fw, frow, fpost), g(n, naux, gs, gidx, gw, grow, gpost);
+  rerdmft::risigma::pairContract<T>(tgt, sign, static_cast<std::size_t>(n), static_cast<std::size_t>(naux), f.op,
+                                    g.op);
+  sigmaOut(tgt, target);
+}
+
+template <typename T>
+static void sigmaDiag(i64 n, i64 naux, double* target, const double* S, const double* Ua, const double* Ub) {
+  auto tgt = sigmaMat<T>(target, n, n);
+  auto s = sigmaMat<T>(S, naux, n * n);
+  rerdmft::Matrix<T> ua, ub;
+  if (Ua) ua = sigmaMat<T>(Ua, naux, n);
+  if (Ub) ub = sigmaMat<T>(Ub, naux, n);
+  rerdmft::risigma::diagContract<T>(tgt, static_cast<std::size_t>(n), static_cast<std::size_t>(naux), s,
+                                    Ua ? &ua : nullptr, Ub ? &ub : nullptr);
+  sigmaOut(tgt, target);
+}
+
+template <typename T>
+static void sigmaAccum(i64 n, i64 naux, double* U, double alpha, const double* D, const double* Wm) {
+  auto u = sigmaMat<T>(U, naux, n);
+  std::vector<T> d(static_cast<std::size_t>(naux * n));
+  std::memcpy(d.data(), D, sizeof(T) * d.size());
+  rerdmft::risigma::accumU<T>(u, alpha, static_cast<std::size_t>(n), static_cast<std::size_t>(naux), d,
+                              toMatrix(Wm, n, n));
+  sigmaOut(u, U);
+}
+
+extern "C" {
+
+int rrref_sigma_toolkit(i64 n, i64 naux, int cplx, const double* B, const double* K, double* kb1, double* kb2,
+                        double* bdiag, double* kb1diag, double* kb2diag) {
+  return guard([&] {
+    if (cplx) sigmaToolkit<std::complex<double>>(n, naux, B, K, kb1, kb2, bdiag, kb1diag, kb2diag);
+    else sigmaToolkit<double>(n, naux, B, K, kb1, kb2, bdiag, kb1diag, kb2diag);
+  });
+}
+
+int rrref_sigma_pair_contract(i64 n, i64 naux, int cplx, double sign, double* target, const double* fs,
+                              const std::uint32_t* fidx, const double* fw, const double* frow, const double* fpost,
+                              const double* gs, const std::uint32_t* gidx, const double* gw, const double* grow,
+                              const double* gpost) {
+  return guard([&] {
+    if (cplx)
+      sigmaPair<std::complex<double>>(n, naux, sign, target, fs, fidx, fw, frow, fpost, gs, gidx, gw, grow, gpost);
+    else
+      sigmaPair<double>(n, naux, sign, target, fs, fidx, fw, frow, fpost, gs, gidx, gw, grow, gpost);
+  });
+}
+
+int rrref_sigma_diag_contract(i64 n, i64 naux, int cplx, double* target, const double* S, const double* Ua,
+                              const double* Ub) {
+  return guard([&] {
+    if (cplx) sigmaDiag<std::complex<double>>(n, naux, target, S, Ua, Ub);
+    else sigmaDiag<double>(n, naux, target, S, Ua, Ub);
+  });
+}
+
+int rrref_sigma_accum_u(i64 n, i64 naux, int cplx, double* U, double alpha, const double* D, const double* Wm) {
+  return guard([&] {
+    if (cplx) sigmaAccum<std::complex<double>>(n, naux, U, alpha, D, Wm);
+    else sigmaAccum<double>(n, naux, U, alpha, D, Wm);
+  });
+}
+
+// src/Utils/Restart.cpp:94 writeRestart from the fields of an rr_restart record (the library's C
+// struct, used here only as a carrier of the same fields).
+int rrref_restart_write(const char* path, const rr_restart* r) {
+  return guard([&] {
+    rerdmft::RestartData d;
+    d.method = r->method ? r->method : "";
+    d.functional = r->functional ? r->functional : "";
+    d.kind = r->kind ? r->kind : "";
+    d.basis_fingerprint = r->basis_fingerprint;
+    d.n_electrons = r->n_electrons;
+    d.pnof_subspaces = r->pnof_subspaces;
+    d.pnof_coupling = r->pnof_coupling;
+    d.n_core = r->n_core;
+    d.jk_frozen_pairs = r->jk_frozen_pairs;
+    d.jk_active_pairs = r->jk_active_pairs;
+    d.total_energy = r->total_energy;
+    d.orbitals_optimized = r->orbitals_optimized != 0;
+    d.converged = r->converged != 0;
+    auto vec = [](const double* p, i64 n) { return p && n > 0 ? std::vector<double>(p, p + n) : std::vector<double>(); };
+    d.occupations = vec(r->occupations, r->n_occupations);
+    d.gammas = vec(r->gammas, r->n_gammas);
+    d.amplitudes = vec(r->amplitudes, r->n_amplitudes);
+    d.complex_coefficients = r->complex_coefficients != 0;
+    d.rows = static_cast<std::uint64_t>(r->rows);
+    d.cols = static_cast<std::uint64_t>(r->cols);
+    d.coefficients = vec(r->coefficients, r->rows * r->cols * (r->complex_coefficients ? 2 : 1));
+    d.cas_electrons = r->cas_electrons;
+    d.cas_spinors = r->cas_spinors;
+    d.cas_state = vec(r->cas_state, r->n_cas_state);
+    rerdmft::writeRestart(path, d);
+  });
+}
+
+// src/Utils/Restart.cpp:147 readRestart then :94 writeRestart: in_path parsed by the reference's reader
+// and written back by its writer (a byte-identical out_path shows the reader took every field).
+int rrref_restart_rewrite(const char* in_path, const char* out_path) {
+  return guard([&] { rerdmft::writeRestart(out_path, rerdmft::readRestart(in_path)); });
+}
+
+// src/AO_ints/ThreeCenterIntegrals.cpp:191 transformRiThreeCenterAoLegs: out (naux, n_out^2) =
+// t^T B^P t per aux row, t is n_ao x n_out.
+int rrref_transform_ao_legs(i64 naux, i64 n_ao, const double* B, i64 n_out, const double* t, double* out) {
+  return guard([&] {
+    auto r = rerdmft::transformRiThreeCenterAoLegs(toMatrix(B, naux, n_ao * n_ao), static_cast<std::size_t>(n_ao),
+                                                   toMatrix(t, n_ao, n_out));
+    fromMatrix(r, out);
   });
 }
 // src/Linear_Algebra/LinearAlgebra.cpp:312 canonicalOrthogonalizeHermitian; X_out holds n*n complex.

@@ -46,6 +46,26 @@ def canonical_orthogonalize_hermitian(s: np.ndarray, threshold: float = 1e-10) -
     return (u[:, keep] / np.sqrt(w[keep])) / d[:, None]
 
 
+def three_center_tensor(raw: np.ndarray, metric_x: np.ndarray) -> np.ndarray:
+    """src/AO_ints/ThreeCenterIntegrals.cpp:219-236 (riThreeCenterTensor after the libcint integrals):
+    B = metric_x^T raw, (naux_kept, n^2)."""
+    if raw.shape[0] != metric_x.shape[0]:
+        raise ValueError("riThreeCenterTensor: metric_x row count does not match the raw aux basis size")
+    return metric_x.T @ raw
+
+
+def transform_ao_legs(eri3_in: np.ndarray, n_ao: int, t: np.ndarray) -> np.ndarray:
+    """src/AO_ints/ThreeCenterIntegrals.cpp:191-217 (transformRiThreeCenterAoLegs): per aux row P,
+    u = t^T B^P, out_P = u t."""
+    if eri3_in.shape[1] != n_ao * n_ao:
+        raise ValueError("transformRiThreeCenterAoLegs: eri3_in column count does not match n_ao^2")
+    if t.shape[0] != n_ao:
+        raise ValueError("transformRiThreeCenterAoLegs: t row count does not match n_ao")
+    naux, n_out = eri3_in.shape[0], t.shape[1]
+    b = eri3_in.reshape(naux, n_ao, n_ao)
+    return np.einsum("ai,Pab,bj->Pij", t, b, t, optimize=True).reshape(naux, n_out * n_out)
+
+
 # --------------------------------------------------------------------------- occupied recovery
 
 
@@ -647,3 +667,60 @@ class AdamOptimizerNumpy:
             self.extra += o["inc"]
         prob.restore_best()
         return dict(iterations=t, energy_best=e_best, restart_requested=self.restart)
+
+
+# --------------------------------------------------------------------------- RI sigma-vector primitives
+
+
+def sigma_toolkit(B: np.ndarray, n: int, K: np.ndarray) -> dict:
+    """src/Hessian_opt/RiSigmaHessianToolkit.cpp:24-55: KB1[P] = K B^P, KB2[P] = B^P K (K real, applied
+    unconjugated) and the diagonals of B, KB1, KB2."""
+    naux = B.shape[0]
+    b = B.reshape(naux, n, n)
+    kb1 = np.einsum("as,Psb->Pab", K, b, optimize=True)
+    kb2 = np.einsum("Par,rb->Pab", b, K, optimize=True)
+    d = np.arange(n)
+    return dict(kb1=kb1.reshape(naux, n * n), kb2=kb2.reshape(naux, n * n), bdiag=b[:, d, d], kb1diag=kb1[:, d, d],
+                kb2diag=kb2[:, d, d])
+
+
+def _sigma_values(op: dict, n: int, naux: int, dtype) -> np.ndarray:
+    """value(P,t,x) of a PairOp (src/Hessian_opt/RiSigmaGemm.h:21-26, fillOp RiSigmaGemm.cpp:38-61):
+    s(P, idx(t,x)) * w(t,x) * row(P,t), then right-multiplied by post when given."""
+    v = np.ones((naux, n, n), dtype=dtype)
+    if op.get("s") is not None:
+        v = v * op["s"][:, np.asarray(op["idx"], dtype=np.int64)].reshape(naux, n, n)
+    if op.get("w") is not None:
+        v = v * np.asarray(op["w"]).reshape(n, n)[None]
+    if op.get("row") is not None:
+        v = v * op["row"][:, :, None]
+    if op.get("post") is not None:
+        v = v @ op["post"]
+    return v
+
+
+def sigma_pair_contract(target, sign, n, naux, f, g):
+    """pairContract (RiSigmaGemm.cpp:65-95): target(x,y) + sign sum_{P,t} F(P,t,x) G(P,t,y), no
+    conjugation (the reference's GEMM is A^T B)."""
+    cplx = any(np.iscomplexobj(a) for a in (target, f.get("s"), g.get("s"), f.get("row"), g.get("row"))
+               if a is not None)
+    dt = np.complex128 if cplx else np.float64
+    F = _sigma_values(f, n, naux, dt)
+    G = _sigma_values(g, n, naux, dt)
+    return target + sign * np.einsum("Ptx,Pty->xy", F, G, optimize=True)
+
+
+def sigma_diag_contract(target, n, naux, S, Ua=None, Ub=None):
+    """diagContract (RiSigmaGemm.cpp:97-114): target(a,b) + sum_P S(P, b n + a) (Ua(P,a) + Ub(P,b))."""
+    s = S.reshape(naux, n, n)  # s[P, b, a]
+    u = np.zeros((naux, n, n), dtype=np.result_type(S, target))  # [P, b, a]
+    if Ua is not None:
+        u = u + Ua[:, None, :]
+    if Ub is not None:
+        u = u + Ub[:, :, None]
+    return target + np.einsum("Pba,Pba->ab", s, u, optimize=True)
+
+
+def sigma_accum_u(U, alpha, n, naux, D, Wm):
+    """accumU (RiSigmaGemm.cpp:116-126): U(P,x) + alpha sum_t D[P n + t] Wm(x,t)."""
+    return U + alpha * (np.asarray(D).reshape(naux, n) @ Wm.T)

@@ -69,6 +69,25 @@ class ScfResult(ctypes.Structure):
                 ("orbital_energies", _vp), ("c_matrix", _vp), ("fock_matrix", _vp)]
 
 
+class RankReport(ctypes.Structure):
+    _fields_ = [("n_kept", _i64), ("n_dropped", _i64), ("smallest_kept", _d), ("largest_dropped", _d)]
+
+
+class PairOp(ctypes.Structure):
+    _fields_ = [("s", _vp), ("idx", _vp), ("w", _vp), ("row", _vp), ("post", _vp)]
+
+
+class Restart(ctypes.Structure):
+    _fields_ = [("method", ctypes.c_char_p), ("functional", ctypes.c_char_p), ("kind", ctypes.c_char_p),
+                ("basis_fingerprint", ctypes.c_uint64), ("n_electrons", _i64), ("pnof_subspaces", _i64),
+                ("pnof_coupling", _i64), ("n_core", _i64), ("jk_frozen_pairs", _i64), ("jk_active_pairs", _i64),
+                ("total_energy", _d), ("orbitals_optimized", _i32), ("converged", _i32),
+                ("occupations", _vp), ("n_occupations", _i64), ("gammas", _vp), ("n_gammas", _i64),
+                ("amplitudes", _vp), ("n_amplitudes", _i64), ("complex_coefficients", _i32), ("rows", _i64),
+                ("cols", _i64), ("coefficients", _vp), ("cas_electrons", _i64), ("cas_spinors", _i64),
+                ("cas_state", _vp), ("n_cas_state", _i64)]
+
+
 class X2cInstance(ctypes.Structure):
     _fields_ = [("h", _vp), ("h_x2c", _vp), ("X", _vp), ("n_eff", _i64), ("S", _vp), ("P0", _vp),
                 ("n_electrons", _i32), ("status", _i32), ("P_out", _vp), ("energy_history", _vp),
@@ -104,6 +123,21 @@ _SIGS = {
     "rr_ri_create": (ctypes.c_int, [_vp, _i64, _i64, _i32, ctypes.POINTER(_vp)]),
     "rr_ri_create_4c": (ctypes.c_int, [_vp, _vp, _i64, _i64, _i64, _i32, ctypes.POINTER(_vp)]),
     "rr_ri_destroy": (ctypes.c_int, [_vp]),
+    "rr_canonical_orthogonalize": (ctypes.c_int, [_vp, _i64, _i32, _d, _vp, ctypes.POINTER(_i64),
+                                                  ctypes.POINTER(RankReport), ctypes.POINTER(Opts)]),
+    "rr_ri_three_center_tensor": (ctypes.c_int, [_vp, _i64, _i64, _vp, _i64, _vp, ctypes.POINTER(Opts)]),
+    "rr_ri_transform_ao_legs": (ctypes.c_int, [_vp, _i64, _i64, _vp, _i64, _vp, ctypes.POINTER(Opts)]),
+    "rr_restart_write": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(Restart)]),
+    "rr_restart_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(Restart)]),
+    "rr_restart_release": (ctypes.c_int, [ctypes.POINTER(Restart)]),
+    "rr_restart_coefficients": (ctypes.c_int, [_vp, _i64, _i64, _vp, _i32, _vp, ctypes.POINTER(Opts)]),
+    "rr_density_from_orbitals": (ctypes.c_int, [_vp, _i64, _i64, _vp, _i32, _vp, ctypes.POINTER(Opts)]),
+    "rr_sigma_toolkit": (ctypes.c_int, [_vp, _i64, _i64, _i32, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(Opts)]),
+    "rr_sigma_pair_contract": (ctypes.c_int, [_vp, _d, _i64, _i64, _i32, ctypes.POINTER(PairOp), ctypes.POINTER(PairOp),
+                                              ctypes.POINTER(Opts)]),
+    "rr_sigma_diag_contract": (ctypes.c_int, [_vp, _i64, _i64, _i32, _vp, _vp, _vp, ctypes.POINTER(Opts)]),
+    "rr_sigma_accum_u": (ctypes.c_int, [_vp, _d, _i64, _i64, _i32, _vp, _vp, ctypes.POINTER(Opts)]),
+    "rr_ri_create_raw": (ctypes.c_int, [_vp, _i64, _i64, _vp, _i64, _vp, _i64, _i32, ctypes.POINTER(_vp)]),
     "rr_ri_info": (ctypes.c_int, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     "rr_ri_sync": (ctypes.c_int, [_vp]),
     "rr_ri_fock_nonrel": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _i64, _vp, ctypes.POINTER(Opts)]),

@@ -34,6 +34,7 @@ void coulomb_after_ht(rr_ri_store* h, const double* Dp, const double* Ct, int64_
 void coulomb_prep(rr_ri_store* h, const double* Dp, const double* Ct, int64_t nocc, double* J, bool have_tgam,
                   cudaStream_t s, bool overlap);
 void coulomb_run(rr_ri_store* h, const double* tgam, int tseg, cudaStream_t s);
+void coulomb_join(rr_ri_store* h, cudaStream_t s);
 
 // Exchange K' = sum_P (Ct B^P)^T (Ct B^P) for a given Ct (nocc x n, row-major with leading
 // dimension ldct, or its transpose when ct_transposed: Ct = C^T with C stored n x nocc).
@@ -42,10 +43,10 @@ void coulomb_run(rr_ri_store* h, const double* tgam, int tseg, cudaStream_t s);
 // (coulomb_prep / coulomb_run, gamma from the half-transform epilogue); it lands in Jout; join with
 // coulomb_join.  The drop-in build starts its J passes itself (coulomb_early) and passes no Dp.
 void exchange_nonrel(rr_ri_store* h, const double* Ct, int64_t ldct, bool ct_transposed, int64_t nocc, double* K,
-                     cudaStream_t s, const double* Dp = nullptr, double* Jout = nullptr) {
+                     cudaStream_t s, const double* Dp = nullptr, double* Jout = nullptr, bool half_only = false) {
   const int64_t n = h->n, naux = h->naux;
   if (nocc == 0 || naux == 0) {
-    RR_CUDA(cudaMemsetAsync(K, 0, sizeof(double) * n * n, s));
+    if (K) RR_CUDA(cudaMemsetAsync(K, 0, sizeof(double) * n * n, s));
     if (Dp) coulomb_after_ht(h, Dp, Ct, 0, Jout, nullptr, 0, s);
     return;
   }
@@ -73,6 +74,7 @@ void exchange_nonrel(rr_ri_store* h, const double* Ct, int64_t ldct, bool ct_tra
   gemm(ht, s);
   prof_mark(h, 2, s);
   if (Dp) coulomb_run(h, tgam, tseg, s);  // side stream, beside the SYRK
+  if (half_only) return;  // the caller uses T itself (energy-only evaluation)
 
   GemmDesc sk;
   sk.M = n; sk.N = n; sk.K = naux * nocc;
@@ -83,6 +85,32 @@ void exchange_nonrel(rr_ri_store* h, const double* Ct, int64_t ldct, bool ct_tra
   const int64_t want = gemm_work_doubles(sk);
   h->work.ensure(static_cast<size_t>(std::max<int64_t>(want, 1)));
   gemm(sk, s, h->work.p, static_cast<int64_t>(h->work.n));
+}
+
+// Energy-only FP64 evaluation of the nonrelativistic build for D = 2 Ct^T Ct (Ct: nocc x n, row-major):
+// J from the same passes as the build (J written to Jout) and the half-transform T^P = Ct B^P, then
+// energy[0] = 1/2 <D, J> and energy[1] = sum_P ||T^P Ct^T||_F^2 = Tr[D K'] / 2 (F = h + J - K'), so
+// 1/2 Tr[D (h + F)] = Tr[D h] + energy[0] - energy[1], without the n x n exchange product.
+void energy_nonrel(rr_ri_store* h, const double* Ct, int64_t nocc, const double* Dp, double* Jout, double* energy,
+                   cudaStream_t s) {
+  const int64_t n = h->n, naux = h->naux;
+  exchange_nonrel(h, Ct, n, false, nocc, nullptr, s, Dp, Jout, true);
+  h->work.ensure(static_cast<size_t>(std::max<int64_t>(static_cast<int64_t>(h->work.n), naux * nocc * nocc + 256)));
+  double* part = h->work.p + naux * nocc * nocc;
+  if (nocc > 0 && naux > 0) {
+    GemmDesc q;  // Q^P = T^P Ct^T (nocc x nocc)
+    q.M = nocc; q.N = nocc; q.K = n;
+    q.A = h->T.p; q.lda = n; q.strideA = nocc * n;
+    q.B = Ct; q.ldb = n; q.opB = Op::T; q.strideB = 0;
+    q.C = h->work.p; q.ldc = nocc; q.strideC = nocc * nocc;
+    q.batch = naux;
+    gemm(q, s);
+    dot_sum(h->work.p, nullptr, naux * nocc * nocc, 1.0, energy + 1, false, part, s);
+  } else {
+    RR_CUDA(cudaMemsetAsync(energy + 1, 0, sizeof(double), s));
+  }
+  coulomb_join(h, s);
+  dot_sum(Dp, Jout, n * n, 0.5, energy, false, part, s);
 }
 
 void pack_for_j(rr_ri_store* h, int t, int64_t n, cudaStream_t s) {

@@ -119,6 +119,59 @@ __global__ void add_kernel(double* out, const double* h, const double* G, int64_
     out[i] = h[i] + G[i];
 }
 
+// Deterministic two-stage sums for the energy-only evaluation: EN_CTAS CTAs write one partial each
+// over fixed chunks, one CTA adds them in order.
+constexpr int EN_CTAS = 256;
+
+__device__ __forceinline__ double en_block_sum(double v) {
+  __shared__ double red[32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) t += red[w];
+  __syncthreads();
+  return t;
+}
+
+// part[b] = this CTA's share of sum_P sum_ij (Q11 + Q22)_ij^2 + (Q21 - Q12)_ij^2, Q^P = [Qtop; Qbot]
+// (2r x 2r per aux row: Qtop = [Re T Cr^T | Re T Ci^T], Qbot = [Im T Cr^T | Im T Ci^T]), i.e.
+// ||M^P||_F^2 with M^P = sum_f c_f B^P c_f^dagger = (Q11 + Q22) + i (Q21 - Q12).
+__global__ void exchange_energy_partial_kernel(const double* Q, int64_t naux, int64_t r, double* part) {
+  const int64_t cnt = naux * r * r, per = (cnt + gridDim.x - 1) / gridDim.x;
+  const int64_t beg = blockIdx.x * per, end = beg + per < cnt ? beg + per : cnt;
+  double acc = 0.0;
+  for (int64_t idx = beg + threadIdx.x; idx < end; idx += blockDim.x) {
+    const int64_t P = idx / (r * r), e = idx % (r * r), i = e / r, j = e % r;
+    const double* q = Q + P * 4 * r * r;
+    const double q11 = q[i * 2 * r + j], q12 = q[i * 2 * r + r + j];
+    const double q21 = q[(r + i) * 2 * r + j], q22 = q[(r + i) * 2 * r + r + j];
+    const double re = q11 + q22, im = q21 - q12;
+    acc += re * re + im * im;
+  }
+  acc = en_block_sum(acc);
+  if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
+// part[b] = this CTA's share of sum_k D[k] J[k] over cnt entries (sum of D[k]^2 when J is null).
+__global__ void dot_partial_kernel(const double* D, const double* J, int64_t cnt, double* part) {
+  const int64_t per = (cnt + gridDim.x - 1) / gridDim.x;
+  const int64_t beg = blockIdx.x * per, end = beg + per < cnt ? beg + per : cnt;
+  double acc = 0.0;
+  for (int64_t idx = beg + threadIdx.x; idx < end; idx += blockDim.x) acc += D[idx] * (J ? J[idx] : D[idx]);
+  acc = en_block_sum(acc);
+  if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
+// out[0] = scale * sum of the `np` partials (one CTA, fixed order); with accumulate, out[0] += that.
+__global__ void sum_partials_kernel(const double* part, int np, double scale, double* out, int accumulate) {
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) acc += part[i];
+  acc = en_block_sum(acc);
+  if (threadIdx.x == 0) out[0] = (accumulate ? out[0] : 0.0) + scale * acc;
+}
+
 struct Flavours {
   int nf = 0;
   std::array<int64_t, 4> off{}, fs{};
@@ -128,6 +181,14 @@ struct Flavours {
 }  // namespace
 
 void coulomb_async_multi(rr_ri_store* h, int ntens, const double* const* Dp, double* const* J, cudaStream_t s);
+
+void dot_sum(const double* a, const double* b, int64_t cnt, double scale, double* out, bool accumulate, double* part,
+             cudaStream_t s) {
+  dot_partial_kernel<<<EN_CTAS, 256, 0, s>>>(a, b, cnt, part);
+  RR_LAUNCH_CHECK();
+  sum_partials_kernel<<<1, 256, 0, s>>>(part, EN_CTAS, scale, out, accumulate ? 1 : 0);
+  RR_LAUNCH_CHECK();
+}
 
 // Two-electron matrix G (complex ntot x ntot) = J - K for the given flavours from Ct (r x ntot,
 // complex), the reference's c_t of all flavours side by side.  Pdens: pitched real spin-summed
@@ -151,7 +212,9 @@ void two_electron_rel(rr_ri_store* h, const Flavours& fl, int64_t ntot, const do
   ar.request(&K2, fsmax * fsmax);
   ar.commit();
   coulomb_async_multi(h, ntens, Dp, J, s);
-  if (rb) {
+  const bool energy_only = rb && rb->energy;
+  RR_REQUIRE(!energy_only || !rb->mixed, RR_ERR_STATE, "two_electron_rel: the energy-only evaluation is FP64");
+  if (rb && !energy_only) {
     h->inc_k.ensure(static_cast<size_t>(2 * ntot * ntot));
     if (rb->mixed) {
       const bool incr = rb->incremental && h->inc_r == r && h->inc_ld == ntot && r > 0;
@@ -171,16 +234,19 @@ void two_electron_rel(rr_ri_store* h, const Flavours& fl, int64_t ntot, const do
   }
   const bool fp64_k = !rb || !rb->mixed;
   double* Gk = rb ? h->inc_k.p : G;  // where the FP64 blocks land
-  if (fp64_k) RR_CUDA(cudaMemsetAsync(Gk, 0, sizeof(double) * 2 * ntot * ntot, s));
+  if (fp64_k && !energy_only) RR_CUDA(cudaMemsetAsync(Gk, 0, sizeof(double) * 2 * ntot * ntot, s));
   // T planes: flavour f occupies [Re (naux*r*fs) | Im (naux*r*fs)]; the off-diagonal blocks (f < u)
   // use Gauss's three products, with Re - Im of every flavour that is an f and Re + Im of every
   // flavour that is a u of such a block.
   std::array<double*, 4> T{}, Tm{}, Tp{};
   int64_t tsize = 0;
   for (int f = 0; f < fl.nf; ++f) tsize += 2 * naux * r * fl.fs[f];
-  for (int f = 0; f < fl.nf; ++f) tsize += (f + 1 < fl.nf ? naux * r * fl.fs[f] : 0) + (f > 0 ? naux * r * fl.fs[f] : 0);
+  if (!energy_only)
+    for (int f = 0; f < fl.nf; ++f) tsize += (f + 1 < fl.nf ? naux * r * fl.fs[f] : 0) + (f > 0 ? naux * r * fl.fs[f] : 0);
+  // energy-only: the 2r x 2r products Q^P of every aux row follow the planes
+  const int64_t qsize = energy_only ? round_up(naux * 4 * r * r, 32) : 0;
   if (fp64_k && r > 0 && naux > 0) {
-    h->T.ensure(static_cast<size_t>(tsize));
+    h->T.ensure(static_cast<size_t>(round_up(tsize, 32) + qsize + EN_CTAS));
     int64_t o = 0;
     for (int f = 0; f < fl.nf; ++f) { T[f] = h->T.p + o; o += 2 * naux * r * fl.fs[f]; }
     for (int f = 0; f < fl.nf; ++f) {
@@ -200,11 +266,42 @@ void two_electron_rel(rr_ri_store* h, const Flavours& fl, int64_t ntot, const do
       ht.batch = naux;
       gemm(ht, s);
     }
-    for (int f = 0; f < fl.nf && fl.nf > 1; ++f) {
+    for (int f = 0; f < fl.nf && fl.nf > 1 && !energy_only; ++f) {
       const int64_t cnt = naux * r * fl.fs[f];
       plane_pm_kernel<<<blocks_for(cnt), 256, 0, s>>>(T[f], cnt, Tm[f], Tp[f]);
       RR_LAUNCH_CHECK();
     }
+  }
+  if (energy_only) {
+    // E_K = sum_P ||sum_f (c_f B^P) c_f^dagger||_F^2 from the half-transform planes: per flavour
+    // Qtop^P += Re T_f^P Cs_f^T and Qbot^P += Im T_f^P Cs_f^T (Cs_f = [Re c_f; Im c_f]), r x 2r each
+    double* part = h->T.p + round_up(tsize, 32) + qsize;
+    if (r > 0 && naux > 0) {
+      double* Q = h->T.p + round_up(tsize, 32);
+      for (int f = 0; f < fl.nf; ++f)
+        for (int plane = 0; plane < 2; ++plane) {
+          GemmDesc q;
+          q.M = r; q.N = 2 * r; q.K = fl.fs[f];
+          q.A = T[f] + plane * naux * r * fl.fs[f]; q.lda = fl.fs[f]; q.strideA = r * fl.fs[f];
+          q.B = Cs[f]; q.ldb = fl.fs[f]; q.opB = Op::T; q.strideB = 0;
+          q.C = Q + plane * r * 2 * r; q.ldc = 2 * r; q.strideC = 4 * r * r;
+          q.batch = naux;
+          q.beta = f > 0 ? 1.0 : 0.0;
+          gemm(q, s);
+        }
+      exchange_energy_partial_kernel<<<EN_CTAS, 256, 0, s>>>(Q, naux, r, part);
+      RR_LAUNCH_CHECK();
+      sum_partials_kernel<<<1, 256, 0, s>>>(part, EN_CTAS, 1.0, rb->energy + 1, 0);
+      RR_LAUNCH_CHECK();
+    } else {
+      RR_CUDA(cudaMemsetAsync(rb->energy + 1, 0, sizeof(double), s));
+    }
+    // E_J = 1/2 sum_t <D_t, J_t> once the J passes are done
+    RR_CUDA(cudaStreamWaitEvent(s, h->ctx.join, 0));
+    h->work.ensure(static_cast<size_t>(std::max<int64_t>(static_cast<int64_t>(h->work.n), EN_CTAS)));
+    double* jpart = h->work.p;
+    for (int t = 0; t < ntens; ++t) dot_sum(Dp[t], J[t], nt[t] * nt[t], 0.5, rb->energy, t > 0, jpart, s);
+    return;
   }
   if (fp64_k) prof_mark(h, 2, s);
   for (int f = 0; f < fl.nf && fp64_k; ++f)
@@ -319,9 +416,11 @@ void fock_x2c(rr_ri_store* h, const double* hc, const double* P, const double* S
   fl.tens = {0, 0, 0, 0};
   const double* dps[1] = {Dp};
   two_electron_rel(h, fl, n, Ct, r, dps, G, s, rb);
-  add_kernel<<<blocks_for(nn2), 256, 0, s>>>(Fd, hd, G, nn2);
-  RR_LAUNCH_CHECK();
-  if (host) copy_out(F, Fd, nn2, true, s);
+  if (!(rb && rb->energy)) {
+    add_kernel<<<blocks_for(nn2), 256, 0, s>>>(Fd, hd, G, nn2);
+    RR_LAUNCH_CHECK();
+    if (host) copy_out(F, Fd, nn2, true, s);
+  }
   prof_mark(h, 4, s);
   if (host || (o && o->sync)) check_status(h, s);
 }
@@ -468,6 +567,11 @@ void fock_rkb(rr_ri_store* h, const double* hc, const double* v, int64_t n_rkb, 
   fl.tens = {0, 0, 1, 1};
   const double* dps[2] = {DL, DS};
   two_electron_rel(h, fl, nu, Ct_ukb, r, dps, G, s, rb);
+  if (rb && rb->energy) {  // energy-only evaluation: no F
+    prof_mark(h, 4, s);
+    if (host || (o && o->sync)) check_status(h, s);
+    return;
+  }
   // F = h + v^dagger G v
   GemmDesc b;
   b.cplx = true;

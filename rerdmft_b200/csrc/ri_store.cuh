@@ -88,9 +88,14 @@ struct Arena {
 //                    same rank) only the exchange of c_t - c_t(previous) is added to inc_k, so the
 //                    rounding error scales with the density change;
 //   otherwise:       FP64 exchange that (re)seeds inc_k.
+// energy (device, 2 doubles; not with mixed): energy-only FP64 evaluation, no G and no F: J in FP64 and
+// the FP64 half-transform only, energy[0] = E_J = 1/2 sum_t <D_t, J_t> (spin-summed densities) and
+// energy[1] = E_K = sum_P || sum_f c_f B^P c_f^dagger ||_F^2 = Re Tr[c_t^dagger c_t K], so that
+// 1/2 Re Tr[P (h + F)] = Re Tr[P h] + E_J - E_K / 2 for P = c_t^dagger c_t; inc_k is left untouched.
 struct RelBuild {
   bool mixed = false;
   bool incremental = false;
+  double* energy = nullptr;
 };
 
 cudaStream_t call_stream(rr_ri_store* h, const rr_opts* o);
@@ -120,6 +125,10 @@ void copy_in_padded(double* dst, int64_t pitch, const double* src, int64_t n2, b
 void axpby(double* y, const double* x, double a, double b, int64_t n, cudaStream_t s);  // y = a x + b y
 // out (cols x rows) = in^T for a real row-major rows x cols matrix.
 void transpose(double* out, const double* in, int64_t rows, int64_t cols, cudaStream_t s);
+// out[0] (device) = scale * sum_k a[k] b[k] over cnt entries (sum of a[k]^2 when b is null), or
+// out[0] += that with accumulate; deterministic (fixed-order two-stage sum), part: 256 doubles of scratch.
+void dot_sum(const double* a, const double* b, int64_t cnt, double scale, double* out, bool accumulate, double* part,
+             cudaStream_t s);
 // F = h + J - K (real, n2 entries).
 void fock_combine(double* F, const double* h, const double* J, const double* K, int64_t n2, cudaStream_t s);
 // Symmetric eigensolver (cuSOLVER dsyevd) in place on a (n x n) row-major symmetric matrix:

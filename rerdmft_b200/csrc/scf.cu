@@ -25,7 +25,9 @@
 namespace rr {
 
 void exchange_nonrel(rr_ri_store* h, const double* Ct, int64_t ldct, bool ct_transposed, int64_t nocc, double* K,
-                     cudaStream_t s, const double* Dp, double* Jout);
+                     cudaStream_t s, const double* Dp, double* Jout, bool half_only = false);
+void energy_nonrel(rr_ri_store* h, const double* Ct, int64_t nocc, const double* Dp, double* Jout, double* energy,
+                   cudaStream_t s);
 void coulomb_after_ht(rr_ri_store* h, const double* Dp, const double* Ct, int64_t nocc, double* J, const double* tgam,
                       int tseg, cudaStream_t s);
 void coulomb_join(rr_ri_store* h, cudaStream_t s);
@@ -815,20 +817,38 @@ void scf_nonrel(rr_ri_store* h, const double* hc, const double* X, int64_t n_eff
     if (conv) {
       if (mixed) {
         // last iteration in FP64: the FP64 Fock matrix of the newest density and its energy
+        // Unless the caller asked for the Fock matrix or orbitals, only the FP64 energy is formed: J and
+        // the half-transform give 1/2 Tr[D (h + F)] = Tr[D h] + E_J - E_K without the exchange SYRK.
         if (mixing_on) axpby(Pn, P, 1.0 - so->mixing, so->mixing, n2, s);
         std::swap(P, Pn);
+        // (with linear mixing the density is not 2 Ct^T Ct, so the full build gives its energy)
+        const bool full_fock = res->fock_matrix || res->c_matrix || res->orbital_energies || mixing_on;
         pt.mark(0, s);
-        exchange_nonrel(h, Ct, n, false, nocc, K, s, P, J);
-        coulomb_join(h, s);
-        fock_combine(F, hd, J, K, n2, s);
-        pt.mark(1, s);
-        ++n_fp64;
-        energy_partial_kernel<1><<<RED_CTAS, 256, 0, s>>>(P, hd, F, n, red);
-        RR_LAUNCH_CHECK();
-        reduce_partials_kernel<0><<<1, 256, 0, s>>>(red, RED_CTAS, 0.5, scal);
-        RR_LAUNCH_CHECK();
         double ev = 0.0;
-        RR_CUDA(cudaMemcpyAsync(&ev, scal, sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (full_fock) {
+          exchange_nonrel(h, Ct, n, false, nocc, K, s, P, J);
+          coulomb_join(h, s);
+          fock_combine(F, hd, J, K, n2, s);
+          pt.mark(1, s);
+          energy_partial_kernel<1><<<RED_CTAS, 256, 0, s>>>(P, hd, F, n, red);
+          RR_LAUNCH_CHECK();
+          reduce_partials_kernel<0><<<1, 256, 0, s>>>(red, RED_CTAS, 0.5, scal);
+          RR_LAUNCH_CHECK();
+          RR_CUDA(cudaMemcpyAsync(&ev, scal, sizeof(double), cudaMemcpyDeviceToHost, s));
+        } else {
+          energy_nonrel(h, Ct, nocc, P, J, scal + 24, s);
+          pt.mark(1, s);
+          // Tr[D h] = 1/2 sum_ij D_ij (h + h)_ji
+          energy_partial_kernel<1><<<RED_CTAS, 256, 0, s>>>(P, hd, hd, n, red);
+          RR_LAUNCH_CHECK();
+          reduce_partials_kernel<0><<<1, 256, 0, s>>>(red, RED_CTAS, 0.5, scal + 26);
+          RR_LAUNCH_CHECK();
+          double e3[3];
+          RR_CUDA(cudaMemcpyAsync(e3, scal + 24, sizeof(e3), cudaMemcpyDeviceToHost, s));
+          host_wait(h, s);
+          ev = e3[2] + e3[0] - e3[1];
+        }
+        ++n_fp64;
         host_wait(h, s);
         pt.accumulate_build();
         res->electronic_energy = ev;
@@ -1052,17 +1072,37 @@ void scf_rel(rr_ri_store* h, int kind, const double* hc, const double* v_total, 
     prev = energy;
     if (conv) {
       if (mixed) {
-        // last iteration in FP64: the FP64 Fock matrix of the newest density and its energy
+        // last iteration in FP64: the FP64 energy of the newest density.  Unless the caller asked for
+        // the Fock matrix or orbitals, only the energy is formed: J in FP64 and the FP64 half-transform
+        // give 1/2 Re Tr[P (h + F)] = Re Tr[P h] + E_J - E_K / 2 without the exchange products.
         if (mixing_on) axpby(Pn, P, 1.0 - so->mixing, so->mixing, c2, s);
         have_proj = !mixing_on;
         std::swap(P, Pn);
+        // (with linear mixing the density is not c_t^dagger c_t, so the full build gives its energy)
+        const bool full_fock = res->fock_matrix || res->c_matrix || res->orbital_energies || mixing_on;
         pt.mark(0, s);
-        build(nullptr);
-        pt.mark(1, s);
-        ++n_fp64;
-        energy_of_f();
         double ev = 0.0;
-        RR_CUDA(cudaMemcpyAsync(&ev, scal, sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (full_fock) {
+          build(nullptr);
+          pt.mark(1, s);
+          energy_of_f();
+          RR_CUDA(cudaMemcpyAsync(&ev, scal, sizeof(double), cudaMemcpyDeviceToHost, s));
+        } else {
+          RelBuild rb;
+          rb.energy = scal + 24;
+          build(&rb);
+          pt.mark(1, s);
+          // Re Tr[P h] = 1/2 sum_ij P_ij (h + h)_ji
+          energy_partial_kernel<2><<<RED_CTAS, 256, 0, s>>>(P, hd, hd, n, red);
+          RR_LAUNCH_CHECK();
+          reduce_partials_kernel<0><<<1, 256, 0, s>>>(red, RED_CTAS, 0.5, scal + 26);
+          RR_LAUNCH_CHECK();
+          double e3[3];
+          RR_CUDA(cudaMemcpyAsync(e3, scal + 24, sizeof(e3), cudaMemcpyDeviceToHost, s));
+          host_wait(h, s);
+          ev = e3[2] + e3[0] - 0.5 * e3[1];
+        }
+        ++n_fp64;
         host_wait(h, s);
         pt.accumulate_build();
         res->electronic_energy = ev;

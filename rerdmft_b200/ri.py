@@ -264,3 +264,108 @@ def rkbFockMatrix(h_rkb, eri: RiDirectEriSource, density_matrix, stream: int | N
     L.check(L.lib().rr_ri_fock_rkb(store.handle, _ptr(h), _ptr(v), n_rkb, _ptr(s), _ptr(x), x.shape[1], _ptr(P),
                                    _ptr(F), ctypes.byref(o)))
     return F
+
+
+# ---------------------------------------------------------------- one-time set-up on the device
+
+
+def _setup_call(args_host):
+    """Host (numpy) or device (CUDA torch) call of a set-up entry point: all arguments one kind."""
+    dev = any(_is_dev(a) for a in args_host if a is not None)
+    return dev, L.opts(L.RR_MEM_DEVICE if dev else L.RR_MEM_HOST)
+
+
+def _canonical_orth(s, threshold, hermitian, report):
+    dev = _is_dev(s)
+    dtype = np.complex128 if hermitian else np.float64
+    S = _dev(s, dtype) if dev else _host(s, dtype)
+    n = S.shape[0]
+    if tuple(S.shape) != (n, n):
+        raise RrError(L.RR_ERR_ARG, "canonicalOrthogonalize: matrix is not square")
+    if dev:
+        X = torch.empty(n * n, dtype=torch.complex128 if hermitian else torch.float64, device=S.device)
+    else:
+        X = np.empty(n * n, dtype=dtype)
+    n_eff = ctypes.c_int64(0)
+    rep = L.RankReport()
+    o = L.opts(L.RR_MEM_DEVICE if dev else L.RR_MEM_HOST)
+    L.check(L.lib().rr_canonical_orthogonalize(_ptr(S), n, 1 if hermitian else 0, float(threshold), _ptr(X),
+                                               ctypes.byref(n_eff), ctypes.byref(rep), ctypes.byref(o)))
+    X = X[: n * n_eff.value].reshape(n, n_eff.value)
+    if report:
+        return X, dict(n_kept=rep.n_kept, n_dropped=rep.n_dropped, smallest_kept=rep.smallest_kept,
+                       largest_dropped=rep.largest_dropped)
+    return X
+
+
+def canonicalOrthogonalize(s, threshold: float, report: bool = False):
+    """canonicalOrthogonalize (src/Linear_Algebra/LinearAlgebra.cpp:267-310) on the device: X (n x n_eff)
+    with X^T S X = I from the eigenvectors of S above `threshold`; the symmetric S^-1/2 when nothing is
+    dropped.  report=True also returns the RankReductionReport fields."""
+    return _canonical_orth(s, threshold, False, report)
+
+
+def canonicalOrthogonalizeHermitian(s, threshold: float, report: bool = False):
+    """canonicalOrthogonalizeHermitian (LinearAlgebra.cpp:312-349) on the device, with the Jacobi scaling
+    D = diag(sqrt(Re S_ii)) applied before the threshold."""
+    return _canonical_orth(s, threshold, True, report)
+
+
+def riThreeCenterTensor(raw, metric_x):
+    """riThreeCenterTensor's contraction (src/AO_ints/ThreeCenterIntegrals.cpp:219-236) on the device:
+    B = metric_x^T raw for the raw 3-centre integrals (naux_raw, n^2) the host computed."""
+    dev, o = _setup_call([raw, metric_x])
+    conv = _dev if dev else _host
+    raw = conv(raw, np.float64)
+    mx = conv(metric_x, np.float64)
+    if mx.shape[0] != raw.shape[0]:
+        raise RrError(L.RR_ERR_ARG, "riThreeCenterTensor: metric_x row count does not match the raw aux basis size")
+    naux_kept, n2 = mx.shape[1], raw.shape[1]
+    out = (torch.empty((naux_kept, n2), dtype=torch.float64, device=raw.device) if dev
+           else np.empty((naux_kept, n2)))
+    L.check(L.lib().rr_ri_three_center_tensor(_ptr(raw), raw.shape[0], n2, _ptr(mx), naux_kept, _ptr(out),
+                                              ctypes.byref(o)))
+    return out
+
+
+def transformRiThreeCenterAoLegs(eri3_in, n_ao: int, t):
+    """transformRiThreeCenterAoLegs (src/AO_ints/ThreeCenterIntegrals.cpp:191-217) on the device:
+    t^T B^P t per aux row."""
+    dev, o = _setup_call([eri3_in, t])
+    conv = _dev if dev else _host
+    B = conv(eri3_in, np.float64)
+    t = conv(t, np.float64)
+    if B.shape[1] != n_ao * n_ao:
+        raise RrError(L.RR_ERR_ARG, "transformRiThreeCenterAoLegs: eri3_in column count does not match n_ao^2")
+    if t.shape[0] != n_ao:
+        raise RrError(L.RR_ERR_ARG, "transformRiThreeCenterAoLegs: t row count does not match n_ao")
+    naux, n_out = B.shape[0], t.shape[1]
+    out = (torch.empty((naux, n_out * n_out), dtype=torch.float64, device=B.device) if dev
+           else np.empty((naux, n_out * n_out)))
+    L.check(L.lib().rr_ri_transform_ao_legs(_ptr(B), naux, n_ao, _ptr(t), n_out, _ptr(out), ctypes.byref(o)))
+    return out
+
+
+def store_from_raw(raw, n_ao: int, metric_x, t=None) -> RiStore:
+    """A resident RiStore built on the device from the raw 3-centre integrals (rr_ri_create_raw): the
+    metric contraction, then the AO-leg transform when t is given, as the reference builds its source
+    tensor (main.cpp:1108 then :4922)."""
+    dev = any(_is_dev(a) for a in (raw, metric_x, t) if a is not None)
+    conv = _dev if dev else _host
+    raw = conv(raw, np.float64)
+    mx = conv(metric_x, np.float64)
+    if raw.shape[1] != n_ao * n_ao:
+        raise RrError(L.RR_ERR_ARG, "riThreeCenterTensor: raw column count does not match n_ao^2")
+    if mx.shape[0] != raw.shape[0]:
+        raise RrError(L.RR_ERR_ARG, "riThreeCenterTensor: metric_x row count does not match the raw aux basis size")
+    tt = conv(t, np.float64) if t is not None else None
+    if tt is not None and tt.shape[0] != n_ao:
+        raise RrError(L.RR_ERR_ARG, "transformRiThreeCenterAoLegs: t row count does not match n_ao")
+    n_out = tt.shape[1] if tt is not None else n_ao
+    st = RiStore.__new__(RiStore)
+    st.handle = ctypes.c_void_p()
+    L.check(L.lib().rr_ri_create_raw(_ptr(raw), raw.shape[0], n_ao, _ptr(mx), mx.shape[1],
+                                     _ptr(tt) if tt is not None else None, n_out,
+                                     L.RR_MEM_DEVICE if dev else L.RR_MEM_HOST, ctypes.byref(st.handle)))
+    st.n, st.ns, st.naux = n_out, 0, mx.shape[1]
+    return st

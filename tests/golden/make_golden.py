@@ -6,7 +6,8 @@ from ``rerdmft_b200.synth``.  The fixtures pin the numpy restatement (``oracle/r
 and the CUDA path; they travel with the repository, so tests on a machine without the
 reference tree still compare against the reference's numbers.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # every fixture
+    python tests/golden/make_golden.py ri_setup   # only ri_setup.npz (the device set-up path)
 """
 from __future__ import annotations
 
@@ -29,7 +30,45 @@ def save(name, **arrays):
     print(f"  {name}.npz")
 
 
+def aux_metric_stand_in(naux, seed):
+    """A Gaussian-overlap stand-in for the aux metric (P|Q) (the real one needs libcint): exp(-|r_P -
+    r_Q|^2 / 2) over seeded centres, two of them coincident, so the canonical orthogonalisation drops
+    one direction as LOWGEN does for a near-dependent aux basis."""
+    rng = np.random.default_rng(seed)
+    r = rng.uniform(0.0, 6.0, size=(naux, 3))
+    r[1] = r[0]
+    d2 = ((r[:, None, :] - r[None, :, :]) ** 2).sum(-1)
+    return np.exp(-0.5 * d2)
+
+
+def make_setup():
+    """The device set-up path: canonical orthogonalisation with its report (LinearAlgebra.cpp:267, :312),
+    the metric contraction (ThreeCenterIntegrals.cpp:219-236: restated, since the reference function
+    runs only after libcint integrals) and the AO-leg transform (ThreeCenterIntegrals.cpp:191-217,
+    the reference's own function)."""
+    ref.set_threads(4)
+    n_ao, naux_raw, n_out = 10, 60, 8
+    M = aux_metric_stand_in(naux_raw, 31)
+    Xm, rep = ref.canonical_orth_report(M, 1e-10)
+    raw = synth.ri_tensor(n_ao, naux_raw, 32, box=6.0)
+    B = Xm.T @ raw
+    rng = np.random.default_rng(33)
+    t = rng.standard_normal((n_ao, n_out))
+    B_legs = ref.transform_ao_legs(B, n_ao, t)
+    k = synth.rkb_system(8, 14, 40, 4, seed=23)
+    Xh, reph = ref.canonical_orth_report(k["s_full"], 1e-10)
+    Sfull = synth.nonrel_system(12, 30, 3, seed=34)["S"]
+    Xf, repf = ref.canonical_orth_report(Sfull, 1e-10)
+    save("ri_setup", metric=M, metric_x=Xm, metric_report=np.array([rep["n_kept"], rep["n_dropped"],
+                                                                     rep["smallest_kept"], rep["largest_dropped"]]),
+         raw=raw, B=B, t=t, B_legs=B_legs, s_full=k["s_full"], XXh=Xh @ Xh.conj().T,
+         s_full_report=np.array([reph["n_kept"], reph["n_dropped"], reph["smallest_kept"], reph["largest_dropped"]]),
+         S_full_rank=Sfull, X_full_rank=Xf)
+
+
 def main():
+    if sys.argv[1:] == ["ri_setup"]:
+        return make_setup()
     ref.set_threads(4)
     # --- nonrelativistic Fock builds (NonRelFockMatrixRi.cpp:71) ---
     for n, naux, nocc, seed in [(1, 3, 1, 11), (7, 20, 2, 12), (13, 37, 3, 13), (24, 129, 5, 14), (33, 70, 7, 15)]:
@@ -156,6 +195,7 @@ def main():
     Xs = ref.canonical_orth(S, 1e-6)
     Xh = ref.canonical_orth(k["s_full"], 1e-10)
     save("orth", S=S, X=Xs, s_full=k["s_full"], XXh=Xh @ Xh.conj().T)
+    make_setup()
 
 
 if __name__ == "__main__":

@@ -122,3 +122,19 @@ def test_orthogonalisation():
     assert np.abs(X @ X.T - g["X"] @ g["X"].T).max() < 1e-9
     Xh = o.canonical_orthogonalize_hermitian(g["s_full"], 1e-10)
     assert np.abs(Xh @ Xh.conj().T - g["XXh"]).max() < 1e-10
+
+
+def test_setup_path_restatements():
+    """The numpy restatements of the metric contraction and the AO-leg transform against the fixture
+    (the AO legs from the reference's own transformRiThreeCenterAoLegs), and of the canonical
+    orthogonalisation against the reference's X and report."""
+    g = golden("ri_setup")
+    assert np.abs(o.three_center_tensor(g["raw"], g["metric_x"]) - g["B"]).max() < 1e-12
+    n_ao = g["t"].shape[0]
+    assert np.abs(o.transform_ao_legs(g["B"], n_ao, g["t"]) - g["B_legs"]).max() < 1e-12
+    X = o.canonical_orthogonalize(g["metric"], 1e-10)
+    assert X.shape == g["metric_x"].shape and int(g["metric_report"][1]) == 1
+    assert np.abs(X @ X.T - g["metric_x"] @ g["metric_x"].T).max() < 1e-8
+    assert np.abs(o.canonical_orthogonalize(g["S_full_rank"], 1e-10) - g["X_full_rank"]).max() < 1e-12
+    Xh = o.canonical_orthogonalize_hermitian(g["s_full"], 1e-10)
+    assert np.abs(Xh @ Xh.conj().T - g["XXh"]).max() < 1e-10
