@@ -142,6 +142,115 @@ def rkb_fock_times(torch, fp64_peak, want_cpu: bool, steps: int = 10):
     return out
 
 
+def mo_transform_block(torch, fp64_peak, want_cpu: bool, reps: int = 5):
+    """MO three-index transforms of the functional stage: buildRiNonRelSpinMoEri at the headline shape
+    (n = 400, naux = 1600, C a full 400 x 400 orthogonal matrix: 4 naux n^3 = 409.6 GFLOP) and buildRiMoEri
+    at the 4-component shapes (nl = 200, ns = 600, naux = 1000, 400 positive-energy spinors), each call timed on the
+    host around the synchronous library call (the new tensor's allocation included), against the
+    reference's own functions on the host cores (one call each)."""
+    import ctypes
+
+    from rerdmft_b200 import _lib as L
+    from rerdmft_b200 import synth
+
+    lib = L.lib()
+    out = {}
+    inp = make_inputs()
+    rng = np.random.default_rng(SEED + 5)
+    C = np.ascontiguousarray(synth.random_orthogonal(N_AO, rng))
+    dB = torch.from_numpy(inp["B"]).cuda()
+    from rerdmft_b200.ri import RiStore
+
+    st = RiStore(dB, nl=N_AO)
+    dC = torch.from_numpy(C).cuda()
+    o = L.opts(L.RR_MEM_DEVICE, sync=1)
+
+    def build_nonrel():
+        h = ctypes.c_void_p()
+        L.check(lib.rr_mo_build_nonrel(st.handle, dC.data_ptr(), ctypes.byref(h), ctypes.byref(o)))
+        return h
+
+    h = build_nonrel()
+    L.check(lib.rr_mo_destroy(h))
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        h = build_nonrel()
+        times.append(time.perf_counter() - t0)
+        L.check(lib.rr_mo_destroy(h))
+    best = min(times)
+    flops = 4.0 * N_AUX * N_AO ** 3
+    out["nonrel_spin"] = dict(workload=f"buildRiNonRelSpinMoEri n={N_AO} naux={N_AUX} (full C, FP64)",
+                              seconds_per_build=best, algorithmic_gflop=flops / 1e9,
+                              achieved_tflops=flops / best / 1e12,
+                              frac_of_dgemm=(flops / best / 1e12 / fp64_peak) if fp64_peak else None,
+                              note="host wall time of the synchronous call, the 2.05 GB output allocation included")
+    if want_cpu:
+        from oracle import ref
+
+        if ref.available():
+            ref.set_threads(os.cpu_count() or 1)
+            t0 = time.perf_counter()
+            Bref = ref.nonrel_mo_build(inp["B"], C)
+            dt = time.perf_counter() - t0
+            h = build_nonrel()
+            got = np.empty((N_AUX, N_AO * N_AO))
+            L.check(lib.rr_mo_copy_tensor(h, got.ctypes.data, ctypes.byref(L.opts())))
+            L.check(lib.rr_mo_destroy(h))
+            out["nonrel_spin"]["reference_cpu"] = dict(seconds_per_build=dt, cores=os.cpu_count() or 1,
+                                                       cpu_model=cpu_model(),
+                                                       sample="one full-size call of the reference "
+                                                              "buildRiNonRelSpinMoEri")
+            out["nonrel_spin"]["parity"] = dict(max_abs_minus_reference=float(np.abs(got - Bref).max()),
+                                                tolerance=1e-10)
+            del Bref, got
+    st.close()
+    del dB, dC, inp
+    torch.cuda.empty_cache()
+
+    s = synth.rkb_system(NL4, NS4, NAUX4, 2 * (NOCC4 // 2), seed=SEED + 11, box=20.0)
+    # the functional stage's MO space: the positive-energy half of the RKB basis (no-pair), 400 spinors
+    nt = s["n_rkb"] // 2
+    c_ukb = np.ascontiguousarray(s["v_total"] @ synth.random_unitary(s["n_rkb"], rng)[:, :nt])
+    st4 = RiStore(torch.from_numpy(s["B_LL"]).cuda(), torch.from_numpy(s["B_SS"]).cuda(), nl=NL4, ns=NS4)
+    dc = torch.from_numpy(c_ukb).cuda()
+
+    def build_ukb():
+        h = ctypes.c_void_p()
+        L.check(lib.rr_mo_build_ukb(st4.handle, dc.data_ptr(), nt, ctypes.byref(h), ctypes.byref(o)))
+        return h
+
+    h = build_ukb()
+    L.check(lib.rr_mo_destroy(h))
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        h = build_ukb()
+        times.append(time.perf_counter() - t0)
+        L.check(lib.rr_mo_destroy(h))
+    best = min(times)
+    # per flavour f: T = c_f^dagger B_f^P (2 real products, 2 nt fs^2 each) and T c_f (complex, 8 nt^2 fs)
+    fl = [NL4, NL4, NS4, NS4]
+    flops = NAUX4 * sum(4.0 * nt * f * f + 8.0 * nt * nt * f for f in fl)
+    out["ukb_4c"] = dict(workload=f"buildRiMoEri nl={NL4} ns={NS4} naux={NAUX4} n_total={nt} (complex, FP64)",
+                         seconds_per_build=best, algorithmic_gflop=flops / 1e9, achieved_tflops=flops / best / 1e12,
+                         frac_of_dgemm=(flops / best / 1e12 / fp64_peak) if fp64_peak else None,
+                         note="host wall time of the synchronous call, the 2.56 GB output allocation included")
+    if want_cpu:
+        from oracle import ref
+
+        if ref.available():
+            t0 = time.perf_counter()
+            ref.ri_mo_build(NL4, NS4, s["B_LL"], s["B_SS"], c_ukb)
+            out["ukb_4c"]["reference_cpu"] = dict(seconds_per_build=time.perf_counter() - t0,
+                                                  cores=os.cpu_count() or 1, cpu_model=cpu_model(),
+                                                  sample="one full-size call of the reference buildRiMoEri")
+    st4.close()
+    del dc
+    torch.cuda.empty_cache()
+    return out
+
+
 def orbital_optimization_block():
     """Functional-stage orbital optimisation (ADAM macro loop at fixed occupations) with and without
     the shipped learned preconditioner: a LiH-sized system (11 spatial orbitals, naux 48; two seeds
@@ -735,6 +844,7 @@ def main():
     torch.cuda.empty_cache()
     scf_block = scf_times(torch, want_cpu=not args.no_cpu_baseline)
     rkb_block = rkb_fock_times(torch, fp64_peak, want_cpu=not args.no_cpu_baseline)
+    mo_block = mo_transform_block(torch, fp64_peak, want_cpu=not args.no_cpu_baseline)
     orb_block = orbital_optimization_block()
     x2c_block = x2c_batch_block(want_cpu=not args.no_cpu_baseline)
     rel_block = rel_scf_times(not args.no_cpu_baseline,
@@ -768,6 +878,7 @@ def main():
         time_to_1e8_ha=scf_block,
         time_to_1e8_ha_relativistic=rel_block,
         rkb_fock_4c=rkb_block,
+        mo_transform=mo_block,
         orbital_optimization=orb_block,
         x2c_batch=x2c_block,
     )

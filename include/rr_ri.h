@@ -324,6 +324,20 @@ int rr_mo_hx_fock(rr_mo_handle m, const double* h, const double* occupations, co
                   const double* two_rdm_x, const int64_t* pair_of, const double* two_rdm_l1, const double* two_rdm_l2,
                   double* F, const rr_opts* opts);
 
+/* The CASSCF RI operators (src/MCSCF/CasFock.cpp:246-262) on an MO tensor; d = 2n for RR_MO_NONREL_SPIN
+ * (the reference works on embeddedB()), n for RR_MO_COMPLEX; complex matrices interleaved.
+ * casTwoElectronOperator: G (d x d) = J(rho) - K(rho) for a one-particle density rho (d x d), with K from
+ * rho's eigen-decomposition (eigenvalues |w| > 1e-14, CasFock.cpp:74-113). */
+int rr_mo_cas_two_electron(rr_mo_handle m, const double* rho, double* G, const rr_opts* opts);
+/* casActiveCumulantFock (CasFock.cpp:116-133): F (d x n_active) = sum_r sum_P B(P, act[r], p)
+ * T[P](r, q), T = Bact lambda with lambda[s, t, r, q] (n_active^4 entries); active: n_active indices in [0, d). */
+int rr_mo_cas_cumulant_fock(rr_mo_handle m, int64_t n_active, const int64_t* active, const double* lambda, double* F,
+                            const rr_opts* opts);
+/* casActiveIntegrals (CasFock.cpp:136-147): (tu|vw) = sum_P B(P, t u) B(P, v w) over the active list,
+ * n_active^4 values. */
+int rr_mo_cas_active_integrals(rr_mo_handle m, int64_t n_active, const int64_t* active, double* out,
+                               const rr_opts* opts);
+
 /* One X2C-HF problem of a batch (its own 2-component handle and inputs, as for rr_scf_run_x2c);
  * result and status are outputs (status: RR_OK or the error code of this instance). */
 typedef struct rr_x2c_instance {

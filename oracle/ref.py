@@ -475,3 +475,37 @@ def restart_write(path, fields):
 def restart_rewrite(in_path, out_path):
     """The reference's readRestart of in_path written back with its writeRestart to out_path."""
     _check(lib().rrref_restart_rewrite(str(in_path).encode(), str(out_path).encode()))
+
+
+# ---------------------------------------------------------------- CASSCF RI operators (src/MCSCF/CasFock.cpp)
+
+
+def cas_two_electron(Bmo, n, rho):
+    """casTwoElectronOperator on RiNonRelSpinMoEri (real Bmo, n spatial orbitals, rho 2n x 2n) or RiMoEri
+    (complex Bmo, n spinors)."""
+    cplx = np.iscomplexobj(Bmo)
+    d = n if cplx else 2 * n
+    G = np.empty((d, d), dtype=np.complex128 if cplx else np.float64)
+    _check(lib().rrref_cas_two_electron(ctypes.c_int(1 if cplx else 0), _i64(n), _i64(Bmo.shape[0]),
+                                        _p(_cv(Bmo, cplx)), _p(_cv(rho, cplx)), _p(G)))
+    return G
+
+
+def cas_cumulant_fock(Bmo, n, active, lam):
+    cplx = np.iscomplexobj(Bmo)
+    d = n if cplx else 2 * n
+    act = np.ascontiguousarray(active, dtype=np.int64)
+    F = np.empty((d, act.size), dtype=np.complex128 if cplx else np.float64)
+    _check(lib().rrref_cas_cumulant_fock(ctypes.c_int(1 if cplx else 0), _i64(n), _i64(Bmo.shape[0]),
+                                         _p(_cv(Bmo, cplx)), _i64(act.size), _p(act),
+                                         _p(_cv(np.asarray(lam).reshape(-1), cplx)), _p(F)))
+    return F
+
+
+def cas_active_integrals(Bmo, n, active):
+    cplx = np.iscomplexobj(Bmo)
+    act = np.ascontiguousarray(active, dtype=np.int64)
+    out = np.empty(act.size ** 4, dtype=np.complex128 if cplx else np.float64)
+    _check(lib().rrref_cas_active_integrals(ctypes.c_int(1 if cplx else 0), _i64(n), _i64(Bmo.shape[0]),
+                                            _p(_cv(Bmo, cplx)), _i64(act.size), _p(act), _p(out)))
+    return out

@@ -37,6 +37,7 @@
 #include "ThreeCenterIntegrals.h"
 #include "RiSigmaHessianToolkit.h"
 #include "Restart.h"
+#include "CasFock.h"
 #include "../include/rr_ri.h"
 
 extern "C" void scipy_openblas_set_num_threads(int n);
@@ -487,6 +488,52 @@ int rrref_sigma_accum_u(i64 n, i64 naux, int cplx, double* U, double alpha, cons
   return guard([&] {
     if (cplx) sigmaAccum<std::complex<double>>(n, naux, U, alpha, D, Wm);
     else sigmaAccum<double>(n, naux, U, alpha, D, Wm);
+  });
+}
+
+// The CASSCF RI overloads (src/MCSCF/CasFock.cpp:246-262) on an MO tensor: kind 0 = RiNonRelSpinMoEri
+// (real spatial tensor of n orbitals, accessor dimension 2n), 1 = RiMoEri (complex, n spinors).
+// casTwoElectronOperator: G (d x d) from rho (d x d).
+int rrref_cas_two_electron(int kind, i64 n, i64 naux, const double* Bmo, const double* rho, double* G) {
+  return guard([&] {
+    if (kind == 0) {
+      rerdmft::RiNonRelSpinMoEri eri(static_cast<std::size_t>(n), toMatrix(Bmo, naux, n * n));
+      fromMatrix(rerdmft::casTwoElectronOperator(eri, toMatrix(rho, 2 * n, 2 * n)), G);
+    } else {
+      rerdmft::RiMoEri eri(static_cast<std::size_t>(n), toCMatrix(Bmo, naux, n * n));
+      fromCMatrix(rerdmft::casTwoElectronOperator(eri, toCMatrix(rho, n, n)), G);
+    }
+  });
+}
+// casActiveCumulantFock: F (d x a) from the active list and lambda (a^4, [s,t,r,q]).
+int rrref_cas_cumulant_fock(int kind, i64 n, i64 naux, const double* Bmo, i64 a, const i64* active,
+                            const double* lambda, double* F) {
+  return guard([&] {
+    std::vector<std::size_t> act(active, active + a);
+    const std::size_t a4 = static_cast<std::size_t>(a * a * a * a);
+    if (kind == 0) {
+      rerdmft::RiNonRelSpinMoEri eri(static_cast<std::size_t>(n), toMatrix(Bmo, naux, n * n));
+      fromMatrix(rerdmft::casActiveCumulantFock(eri, act, std::vector<double>(lambda, lambda + a4)), F);
+    } else {
+      rerdmft::RiMoEri eri(static_cast<std::size_t>(n), toCMatrix(Bmo, naux, n * n));
+      const auto* lc = reinterpret_cast<const std::complex<double>*>(lambda);
+      fromCMatrix(rerdmft::casActiveCumulantFock(eri, act, std::vector<std::complex<double>>(lc, lc + a4)), F);
+    }
+  });
+}
+// casActiveIntegrals: (tu|vw) over the active list, a^4 values.
+int rrref_cas_active_integrals(int kind, i64 n, i64 naux, const double* Bmo, i64 a, const i64* active, double* out) {
+  return guard([&] {
+    std::vector<std::size_t> act(active, active + a);
+    if (kind == 0) {
+      rerdmft::RiNonRelSpinMoEri eri(static_cast<std::size_t>(n), toMatrix(Bmo, naux, n * n));
+      auto v = rerdmft::casActiveIntegrals(eri, act);
+      std::memcpy(out, v.data(), sizeof(double) * v.size());
+    } else {
+      rerdmft::RiMoEri eri(static_cast<std::size_t>(n), toCMatrix(Bmo, naux, n * n));
+      auto v = rerdmft::casActiveIntegrals(eri, act);
+      std::memcpy(out, v.data(), sizeof(std::complex<double>) * v.size());
+    }
   });
 }
 

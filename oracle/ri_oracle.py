@@ -724,3 +724,54 @@ def sigma_diag_contract(target, n, naux, S, Ua=None, Ub=None):
 def sigma_accum_u(U, alpha, n, naux, D, Wm):
     """accumU (RiSigmaGemm.cpp:116-126): U(P,x) + alpha sum_t D[P n + t] Wm(x,t)."""
     return U + alpha * (np.asarray(D).reshape(naux, n) @ Wm.T)
+
+
+# --------------------------------------------------------------------------- CASSCF RI operators
+
+
+def _cas_operand(Bmo, n):
+    """The tensor the CASSCF RI operators act on (src/MCSCF/CasFock.cpp:246-262): embeddedB for a real
+    spatial tensor (NonRelSpinRiMoEri.h:77-89), the tensor itself for a complex one; returns (B, d)."""
+    if np.iscomplexobj(Bmo):
+        return Bmo, n
+    naux = Bmo.shape[0]
+    b = Bmo.reshape(naux, n, n)
+    e = np.zeros((naux, 2 * n, 2 * n))
+    e[:, :n, :n] = b
+    e[:, n:, n:] = b
+    return e.reshape(naux, 4 * n * n), 2 * n
+
+
+def cas_two_electron(Bmo, n, rho):
+    """riTwoElectronOperator (CasFock.cpp:74-113): G = J - K, c_P = sum_st rho_st B(P,st), J = B^T c,
+    K = sum_P B_P conj(rho~) B_P with rho~ = rho's eigen-decomposition without |w| <= 1e-14."""
+    B, d = _cas_operand(Bmo, n)
+    naux = B.shape[0]
+    c = B @ rho.reshape(-1)
+    J = (B.T @ c).reshape(d, d)
+    w, u = np.linalg.eigh(rho)
+    k = np.abs(w) > 1e-14
+    rt = (np.conj(u[:, k]) * w[k]) @ u[:, k].T  # conj(U) diag(w) U^T
+    b = B.reshape(naux, d, d)
+    K = np.einsum("Prt,ts,Psp->rp", b, rt, b, optimize=True)
+    return J - K
+
+
+def cas_cumulant_fock(Bmo, n, active, lam):
+    """riActiveCumulantFock (CasFock.cpp:116-133)."""
+    B, d = _cas_operand(Bmo, n)
+    naux, a = B.shape[0], len(active)
+    b = B.reshape(naux, d, d)
+    act = np.asarray(active)
+    bact = b[:, act][:, :, act].reshape(naux, a * a)
+    T = (bact @ np.asarray(lam).reshape(a * a, a * a)).reshape(naux, a, a)  # [P, r, q]
+    return np.einsum("Prp,Prq->pq", b[:, act, :], T, optimize=True)
+
+
+def cas_active_integrals(Bmo, n, active):
+    """riActiveIntegrals (CasFock.cpp:136-147): (tu|vw) = sum_P B(P,tu) B(P,vw), flat [t,u,v,w]."""
+    B, d = _cas_operand(Bmo, n)
+    naux, a = B.shape[0], len(active)
+    act = np.asarray(active)
+    ba = B.reshape(naux, d, d)[:, act][:, :, act].reshape(naux, a * a)
+    return (ba.T @ ba).reshape(-1)

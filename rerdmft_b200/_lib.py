@@ -148,6 +148,9 @@ _SIGS = {
     "rr_ri_fock_rkb": (ctypes.c_int, [_vp, _vp, _vp, _i64, _vp, _vp, _i64, _vp, _vp, ctypes.POINTER(Opts)]),
     "rr_mo_build_nonrel": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(_vp), ctypes.POINTER(Opts)]),
     "rr_mo_build_ukb": (ctypes.c_int, [_vp, _vp, _i64, ctypes.POINTER(_vp), ctypes.POINTER(Opts)]),
+    "rr_mo_cas_two_electron": (ctypes.c_int, [_vp, _vp, _vp, ctypes.POINTER(Opts)]),
+    "rr_mo_cas_cumulant_fock": (ctypes.c_int, [_vp, _i64, _vp, _vp, _vp, ctypes.POINTER(Opts)]),
+    "rr_mo_cas_active_integrals": (ctypes.c_int, [_vp, _i64, _vp, _vp, ctypes.POINTER(Opts)]),
     "rr_mo_from_tensor": (ctypes.c_int, [_vp, _i64, _i64, _i32, _i32, ctypes.POINTER(_vp)]),
     "rr_mo_destroy": (ctypes.c_int, [_vp]),
     "rr_mo_info": (ctypes.c_int, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i32)]),

@@ -421,6 +421,39 @@ int rr_mo_build_ukb(rr_ri_handle ri4c, const double* c_ukb, int64_t n_total, rr_
   });
 }
 
+int rr_mo_cas_two_electron(rr_mo_handle mh, const double* rho, double* G, const rr_opts* opts) {
+  return api([&] {
+    auto* m = checked_mo(mh);
+    RR_REQUIRE(rho && G, RR_ERR_ARG, "casTwoElectronOperator: null matrix");
+    cudaStream_t st = rr::mo_stream(m, opts);
+    rr::cas_two_electron(m, rho, G, host_mem(opts), st);
+    if (host_mem(opts) || (opts && opts->sync)) RR_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int rr_mo_cas_cumulant_fock(rr_mo_handle mh, int64_t n_active, const int64_t* active, const double* lambda, double* F,
+                            const rr_opts* opts) {
+  return api([&] {
+    auto* m = checked_mo(mh);
+    RR_REQUIRE(n_active >= 0 && (n_active == 0 || (active && lambda)) && F, RR_ERR_ARG,
+               "casActiveCumulantFock: bad arguments");
+    cudaStream_t st = rr::mo_stream(m, opts);
+    rr::cas_cumulant_fock(m, n_active, active, lambda, F, host_mem(opts), st);
+    if (host_mem(opts) || (opts && opts->sync)) RR_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int rr_mo_cas_active_integrals(rr_mo_handle mh, int64_t n_active, const int64_t* active, double* out,
+                               const rr_opts* opts) {
+  return api([&] {
+    auto* m = checked_mo(mh);
+    RR_REQUIRE(n_active >= 0 && (n_active == 0 || (active && out)), RR_ERR_ARG, "casActiveIntegrals: bad arguments");
+    cudaStream_t st = rr::mo_stream(m, opts);
+    rr::cas_active_integrals(m, n_active, active, out, host_mem(opts), st);
+    if (host_mem(opts) || (opts && opts->sync)) RR_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
 int rr_mo_from_tensor(const double* Bmo, int64_t naux, int64_t n, int32_t kind, int32_t mem, rr_mo_handle* out) {
   return api([&] {
     RR_REQUIRE(out && naux >= 0 && n >= 0 && (Bmo || naux * n == 0), RR_ERR_ARG, "rr_mo_from_tensor: bad argument");

@@ -388,6 +388,21 @@ void mo_positive_block(rr_mo_store* src, int64_t off, rr_mo_store* dst, cudaStre
   RR_LAUNCH_CHECK();
 }
 
+const double* mo_operand(rr_mo_store* m, cudaStream_t s, int64_t* d) {
+  if (m->cplx) {
+    *d = m->n;
+    return m->B.p;
+  }
+  const int64_t dd = 4 * m->n * m->n;
+  *d = 2 * m->n;
+  m->emb.ensure(static_cast<size_t>(std::max<int64_t>(m->naux * dd, 1)));
+  if (m->naux * dd) {
+    embed_kernel<<<blocks_for(m->naux * dd), 256, 0, s>>>(m->emb.p, m->B.p, m->naux, m->n);
+    RR_LAUNCH_CHECK();
+  }
+  return m->emb.p;
+}
+
 void mo_embedded(rr_mo_store* m, double* out, bool host, cudaStream_t s) {
   const int64_t n = m->n, naux = m->naux, cnt = naux * 4 * n * n;
   double* dst = out;

@@ -21,6 +21,14 @@ void mo_positive_block(rr_mo_store* src, int64_t off, rr_mo_store* dst, cudaStre
 void mo_embedded(rr_mo_store* m, double* out, bool host, cudaStream_t s);
 void mo_eri(rr_mo_store* m, int64_t count, const int64_t* quads, double* out, bool host, cudaStream_t s);
 void mo_jkl(rr_mo_store* m, const int64_t* pair_of, double* J, double* K, double* L, bool host, cudaStream_t s);
+// The tensor the functional-stage operators act on: B itself (RiMoEri, d = n) or the block-diagonal
+// embedded spin-orbital tensor in m->emb (RiNonRelSpinMoEri, d = 2n, the reference's embeddedB()).
+const double* mo_operand(rr_mo_store* m, cudaStream_t s, int64_t* d);
+// CASSCF RI operators (cas.cu).
+void cas_two_electron(rr_mo_store* m, const double* rho, double* G, bool host, cudaStream_t s);
+void cas_cumulant_fock(rr_mo_store* m, int64_t a, const int64_t* active, const double* lambda, double* F, bool host,
+                       cudaStream_t s);
+void cas_active_integrals(rr_mo_store* m, int64_t a, const int64_t* active, double* out, bool host, cudaStream_t s);
 void mo_hx_fock(rr_mo_store* m, const double* h, const double* occ, const double* h2, const double* x2,
                 const int64_t* pair_of, const double* l1, const double* l2, double* F, bool host, cudaStream_t s);
 }  // namespace rr

@@ -167,9 +167,8 @@ void fock_combine(double* F, const double* h, const double* J, const double* K, 
   RR_LAUNCH_CHECK();
 }
 
-void eigh_sym(rr_ri_store* h, double* a, int64_t n, double* w, cudaStream_t s) {
+void eigh_sym_ctx(Context& c, double* a, int64_t n, double* w, cudaStream_t s) {
   if (n == 0) return;
-  auto& c = h->ctx;
   RR_SOLVER(cusolverDnSetStream(c.solver, s));
   int lwork = 0;
   RR_SOLVER(cusolverDnDsyevd_bufferSize(c.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, static_cast<int>(n),
@@ -180,9 +179,8 @@ void eigh_sym(rr_ri_store* h, double* a, int64_t n, double* w, cudaStream_t s) {
                              static_cast<int>(n), w, c.solver_work.p, lwork, c.solver_info.p));
 }
 
-void eigh_herm(rr_ri_store* h, double* a, int64_t n, double* w, cudaStream_t s) {
+void eigh_herm_ctx(Context& c, double* a, int64_t n, double* w, cudaStream_t s) {
   if (n == 0) return;
-  auto& c = h->ctx;
   RR_SOLVER(cusolverDnSetStream(c.solver, s));
   int lwork = 0;
   auto* az = reinterpret_cast<cuDoubleComplex*>(a);
@@ -194,5 +192,9 @@ void eigh_herm(rr_ri_store* h, double* a, int64_t n, double* w, cudaStream_t s) 
                              static_cast<int>(n), w, reinterpret_cast<cuDoubleComplex*>(c.solver_work.p), lwork,
                              c.solver_info.p));
 }
+
+void eigh_sym(rr_ri_store* h, double* a, int64_t n, double* w, cudaStream_t s) { eigh_sym_ctx(h->ctx, a, n, w, s); }
+
+void eigh_herm(rr_ri_store* h, double* a, int64_t n, double* w, cudaStream_t s) { eigh_herm_ctx(h->ctx, a, n, w, s); }
 
 }  // namespace rr

@@ -136,5 +136,9 @@ void fock_combine(double* F, const double* h, const double* J, const double* K, 
 void eigh_sym(rr_ri_store* h, double* a, int64_t n, double* w, cudaStream_t s);
 // Hermitian (interleaved complex) version, cuSOLVER zheevd; row j of `a` holds conj(eigenvector j).
 void eigh_herm(rr_ri_store* h, double* a, int64_t n, double* w, cudaStream_t s);
+// The same on any execution context (its cuSOLVER handle and scratch); the info word is left in
+// c.solver_info.
+void eigh_sym_ctx(Context& c, double* a, int64_t n, double* w, cudaStream_t s);
+void eigh_herm_ctx(Context& c, double* a, int64_t n, double* w, cudaStream_t s);
 
 }  // namespace rr

@@ -176,3 +176,46 @@ def hartreeExchangeFockMatrix(h, eri: _MoBase, occupations, two_rdm_h, two_rdm_x
 def jkOnlyFockMatrix(h, eri: _MoBase, occupations, two_rdm_h, two_rdm_x):
     """src/Hessian_opt/RiGemmFock.cpp:186 / :194: the pair-free special case."""
     return hartreeExchangeFockMatrix(h, eri, occupations, two_rdm_h, two_rdm_x)
+
+
+# ---------------------------------------------------------------- CASSCF RI operators (src/MCSCF/CasFock.cpp:246-262)
+
+
+def _dim_dtype(eri):
+    return eri.dim(), (np.complex128 if eri._kind == L.RR_MO_COMPLEX else np.float64)
+
+
+def casTwoElectronOperator(eri, rho):
+    """G = J(rho) - K(rho) over the accessor dimension (CasFock.cpp:74-113; embeddedB for the nonrelativistic
+    tensor), with K from rho's eigen-decomposition on the device."""
+    d, dt = _dim_dtype(eri)
+    r = np.ascontiguousarray(rho, dtype=dt)
+    if r.shape != (d, d):
+        raise RrError(L.RR_ERR_ARG, "casTwoElectronOperator: rho dimension does not match the MO tensor")
+    G = np.empty((d, d), dtype=dt)
+    L.check(L.lib().rr_mo_cas_two_electron(eri.handle, r.ctypes.data, G.ctypes.data, ctypes.byref(L.opts())))
+    return G
+
+
+def casActiveCumulantFock(eri, active, lam):
+    """casActiveCumulantFock (CasFock.cpp:116-133): F (d x a) from the active list and lambda[s,t,r,q]."""
+    d, dt = _dim_dtype(eri)
+    act = np.ascontiguousarray(active, dtype=np.int64)
+    a = act.size
+    lm = np.ascontiguousarray(lam, dtype=dt).reshape(-1)
+    if lm.size != a ** 4:
+        raise RrError(L.RR_ERR_ARG, "casActiveCumulantFock: lambda must hold n_active^4 values")
+    F = np.empty((d, a), dtype=dt)
+    L.check(L.lib().rr_mo_cas_cumulant_fock(eri.handle, a, act.ctypes.data, lm.ctypes.data, F.ctypes.data,
+                                            ctypes.byref(L.opts())))
+    return F
+
+
+def casActiveIntegrals(eri, active):
+    """casActiveIntegrals (CasFock.cpp:136-147): (tu|vw) over the active list, a^4 values (flat, [t,u,v,w])."""
+    _, dt = _dim_dtype(eri)
+    act = np.ascontiguousarray(active, dtype=np.int64)
+    out = np.empty(act.size ** 4, dtype=dt)
+    L.check(L.lib().rr_mo_cas_active_integrals(eri.handle, act.size, act.ctypes.data, out.ctypes.data,
+                                               ctypes.byref(L.opts())))
+    return out
