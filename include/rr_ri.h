@@ -324,6 +324,20 @@ int rr_mo_hx_fock(rr_mo_handle m, const double* h, const double* occupations, co
                   const double* two_rdm_x, const int64_t* pair_of, const double* two_rdm_l1, const double* two_rdm_l2,
                   double* F, const rr_opts* opts);
 
+/* hartreeExchangeJointHessianDiagonal (src/Hessian_opt/HartreeExchangeHessian.cpp:653-711, the RiMoEri
+ * instantiation) on a complex MO tensor (RR_MO_COMPLEX, n spinors): out (2 n_pairs) = the diagonal of the
+ * joint [real; imaginary] orbital-rotation Hessian for each pair (pairs: n_pairs x 2 int64 (p, q), p != q),
+ * from h (complex n x n), the occupations, two_rdm_h / two_rdm_x (real n x n), fock (complex n x n, the
+ * generalized Fock matrix of rr_mo_hx_fock) and optionally pair_of (n int64) with two_rdm_l1 / two_rdm_l2.
+ * With a PNOF functional's full two-RDM (buildPnofFullTwoRdm / buildPnofPairOf) this is
+ * pnofJointHessianDiagonal (src/Hessian_opt/PnofHessian.cpp:171-181).  The labels of the learned
+ * preconditioner for complex orbitals.  A real tensor returns RR_ERR_UNSUPPORTED (no reference form). */
+int rr_mo_hx_joint_hessian_diagonal(rr_mo_handle m, const double* h, const double* occupations,
+                                    const double* two_rdm_h, const double* two_rdm_x, const double* fock,
+                                    int64_t n_pairs, const int64_t* pairs, const int64_t* pair_of,
+                                    const double* two_rdm_l1, const double* two_rdm_l2, double* out,
+                                    const rr_opts* opts);
+
 /* The CASSCF RI operators (src/MCSCF/CasFock.cpp:246-262) on an MO tensor; d = 2n for RR_MO_NONREL_SPIN
  * (the reference works on embeddedB()), n for RR_MO_COMPLEX; complex matrices interleaved.
  * casTwoElectronOperator: G (d x d) = J(rho) - K(rho) for a one-particle density rho (d x d), with K from

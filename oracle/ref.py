@@ -509,3 +509,31 @@ def cas_active_integrals(Bmo, n, active):
     _check(lib().rrref_cas_active_integrals(ctypes.c_int(1 if cplx else 0), _i64(n), _i64(Bmo.shape[0]),
                                             _p(_cv(Bmo, cplx)), _i64(act.size), _p(act), _p(out)))
     return out
+
+
+# ---------------------------------------------------------------- joint Hessian diagonal, PNOF two-RDM
+
+
+def hx_joint_hessian_diag(Bmo, n, h, occ, h2, x2, fock, pairs, pair_of=None, l1=None, l2=None):
+    """hartreeExchangeJointHessianDiagonal on a RiMoEri (HartreeExchangeHessian.cpp:653-711)."""
+    pr = np.ascontiguousarray(pairs, dtype=np.int64).reshape(-1, 2)
+    out = np.empty(2 * pr.shape[0])
+    po = None if pair_of is None else np.ascontiguousarray(pair_of, dtype=np.int64)
+    _check(lib().rrref_hx_joint_hessian_diag(_i64(n), _i64(Bmo.shape[0]), _p(_c(Bmo)), _p(_c(h)), _p(_d(occ)),
+                                             _p(_d(h2)), _p(_d(x2)), _p(_c(fock)), _i64(pr.shape[0]), _p(pr),
+                                             None if po is None else _p(po), None if l1 is None else _p(_d(l1)),
+                                             None if l2 is None else _p(_d(l2)), _p(out)))
+    return out
+
+
+def pnof_full_two_rdm(functional, geminals, occ, n_total, relativistic=True):
+    """buildPnofFullTwoRdm + buildPnofPairOf (PnofFock.cpp:29, :139); functional in PNOF5, PNOF7, PNOF7S, GNOF;
+    geminals: rows (i, ibar, subspace_id, is_principal)."""
+    f = {"PNOF5": 0, "PNOF7": 1, "PNOF7S": 2, "GNOF": 3}[functional]
+    g = np.ascontiguousarray(geminals, dtype=np.int64).reshape(-1, 4)
+    h2, x2, l1, l2 = (np.empty((n_total, n_total)) for _ in range(4))
+    po = np.empty(n_total, dtype=np.int64)
+    _check(lib().rrref_pnof_full_two_rdm(ctypes.c_int(f), _i64(g.shape[0]), _p(g), _p(_d(occ)), _i64(n_total),
+                                         ctypes.c_int(1 if relativistic else 0), _p(h2), _p(x2), _p(l1), _p(l2),
+                                         _p(po)))
+    return dict(two_rdm_h=h2, two_rdm_x=x2, two_rdm_l1=l1, two_rdm_l2=l2, pair_of=po)

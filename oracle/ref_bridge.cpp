@@ -38,6 +38,7 @@
 #include "RiSigmaHessianToolkit.h"
 #include "Restart.h"
 #include "CasFock.h"
+#include "PnofFock.h"
 #include "../include/rr_ri.h"
 
 extern "C" void scipy_openblas_set_num_threads(int n);
@@ -488,6 +489,53 @@ int rrref_sigma_accum_u(i64 n, i64 naux, int cplx, double* U, double alpha, cons
   return guard([&] {
     if (cplx) sigmaAccum<std::complex<double>>(n, naux, U, alpha, D, Wm);
     else sigmaAccum<double>(n, naux, U, alpha, D, Wm);
+  });
+}
+
+// src/Hessian_opt/HartreeExchangeHessian.cpp:653 hartreeExchangeJointHessianDiagonal, RiMoEri instantiation
+// (:705-711): out (2 npairs); pairs npairs x 2; pair_of null = no pair terms.
+int rrref_hx_joint_hessian_diag(i64 n, i64 naux, const double* Bmo, const double* h, const double* occ,
+                                const double* h2, const double* x2, const double* fock, i64 npairs, const i64* pairs,
+                                const i64* pair_of, const double* l1, const double* l2, double* out) {
+  return guard([&] {
+    rerdmft::RiMoEri eri(static_cast<std::size_t>(n), toCMatrix(Bmo, naux, n * n));
+    std::vector<std::pair<std::size_t, std::size_t>> pr(static_cast<std::size_t>(npairs));
+    for (i64 i = 0; i < npairs; ++i) pr[i] = {static_cast<std::size_t>(pairs[2 * i]), static_cast<std::size_t>(pairs[2 * i + 1])};
+    std::vector<std::size_t> po;
+    rerdmft::Matrix<double> L1, L2;
+    if (pair_of) {
+      po.assign(pair_of, pair_of + n);
+      L1 = toMatrix(l1, n, n);
+      L2 = toMatrix(l2, n, n);
+    }
+    auto d = rerdmft::hartreeExchangeJointHessianDiagonal(toCMatrix(h, n, n), eri, std::vector<double>(occ, occ + n),
+                                                          toMatrix(h2, n, n), toMatrix(x2, n, n), toCMatrix(fock, n, n),
+                                                          pr, po, L1, L2);
+    std::memcpy(out, d.data(), sizeof(double) * d.size());
+  });
+}
+
+// src/Hessian_opt/PnofFock.cpp:29 buildPnofFullTwoRdm and :139 buildPnofPairOf: functional 0..3 = PNOF5,
+// PNOF7, PNOF7s, GNOF; geminals n_gem x 4 (i, ibar, subspace_id, is_principal).
+int rrref_pnof_full_two_rdm(int functional, i64 n_gem, const i64* gem, const double* occ, i64 n_total,
+                            int relativistic, double* h2, double* x2, double* l1, double* l2, i64* pair_of) {
+  return guard([&] {
+    std::vector<rerdmft::PnofGeminal> g(static_cast<std::size_t>(n_gem));
+    for (i64 k = 0; k < n_gem; ++k)
+      g[k] = rerdmft::PnofGeminal{static_cast<std::size_t>(gem[4 * k]), static_cast<std::size_t>(gem[4 * k + 1]),
+                                  static_cast<std::size_t>(gem[4 * k + 2]), gem[4 * k + 3] != 0};
+    const rerdmft::PnofFunctional f = functional == 0 ? rerdmft::PnofFunctional::kPnof5
+                                      : functional == 1 ? rerdmft::PnofFunctional::kPnof7
+                                      : functional == 2 ? rerdmft::PnofFunctional::kPnof7s
+                                                        : rerdmft::PnofFunctional::kGnof;
+    auto full = rerdmft::buildPnofFullTwoRdm(f, g, std::vector<double>(occ, occ + n_total),
+                                             static_cast<std::size_t>(n_total), relativistic != 0);
+    fromMatrix(full.two_rdm_h, h2);
+    fromMatrix(full.two_rdm_x, x2);
+    fromMatrix(full.two_rdm_l1, l1);
+    fromMatrix(full.two_rdm_l2, l2);
+    auto po = rerdmft::buildPnofPairOf(g, static_cast<std::size_t>(n_total));
+    for (i64 i = 0; i < n_total; ++i) pair_of[i] = static_cast<i64>(po[i]);
   });
 }
 

@@ -148,6 +148,8 @@ _SIGS = {
     "rr_ri_fock_rkb": (ctypes.c_int, [_vp, _vp, _vp, _i64, _vp, _vp, _i64, _vp, _vp, ctypes.POINTER(Opts)]),
     "rr_mo_build_nonrel": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(_vp), ctypes.POINTER(Opts)]),
     "rr_mo_build_ukb": (ctypes.c_int, [_vp, _vp, _i64, ctypes.POINTER(_vp), ctypes.POINTER(Opts)]),
+    "rr_mo_hx_joint_hessian_diagonal": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp,
+                                                       ctypes.POINTER(Opts)]),
     "rr_mo_cas_two_electron": (ctypes.c_int, [_vp, _vp, _vp, ctypes.POINTER(Opts)]),
     "rr_mo_cas_cumulant_fock": (ctypes.c_int, [_vp, _i64, _vp, _vp, _vp, ctypes.POINTER(Opts)]),
     "rr_mo_cas_active_integrals": (ctypes.c_int, [_vp, _i64, _vp, _vp, ctypes.POINTER(Opts)]),

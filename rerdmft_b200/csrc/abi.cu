@@ -421,6 +421,24 @@ int rr_mo_build_ukb(rr_ri_handle ri4c, const double* c_ukb, int64_t n_total, rr_
   });
 }
 
+int rr_mo_hx_joint_hessian_diagonal(rr_mo_handle mh, const double* h, const double* occupations,
+                                    const double* two_rdm_h, const double* two_rdm_x, const double* fock,
+                                    int64_t n_pairs, const int64_t* pairs, const int64_t* pair_of,
+                                    const double* two_rdm_l1, const double* two_rdm_l2, double* out,
+                                    const rr_opts* opts) {
+  return api([&] {
+    auto* m = checked_mo(mh);
+    RR_REQUIRE(h && occupations && two_rdm_h && two_rdm_x && fock && out && n_pairs >= 0 && (pairs || n_pairs == 0),
+               RR_ERR_ARG, "hartreeExchangeJointHessianDiagonal: null argument");
+    RR_REQUIRE(!pair_of || (two_rdm_l1 && two_rdm_l2), RR_ERR_ARG,
+               "hartreeExchangeJointHessianDiagonal: pair_of/two_rdm_l1/two_rdm_l2 must be given together");
+    cudaStream_t st = rr::mo_stream(m, opts);
+    rr::mo_hx_joint_hessian_diagonal(m, h, occupations, two_rdm_h, two_rdm_x, fock, n_pairs, pairs, pair_of,
+                                     two_rdm_l1, two_rdm_l2, out, host_mem(opts), st);
+    if (host_mem(opts) || (opts && opts->sync)) RR_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
 int rr_mo_cas_two_electron(rr_mo_handle mh, const double* rho, double* G, const rr_opts* opts) {
   return api([&] {
     auto* m = checked_mo(mh);

@@ -29,6 +29,11 @@ void cas_two_electron(rr_mo_store* m, const double* rho, double* G, bool host, c
 void cas_cumulant_fock(rr_mo_store* m, int64_t a, const int64_t* active, const double* lambda, double* F, bool host,
                        cudaStream_t s);
 void cas_active_integrals(rr_mo_store* m, int64_t a, const int64_t* active, double* out, bool host, cudaStream_t s);
+// hartreeExchangeJointHessianDiagonal on a complex tensor (hessian_joint.cu).
+void mo_hx_joint_hessian_diagonal(rr_mo_store* m, const double* h, const double* occ, const double* h2,
+                                  const double* x2, const double* fock, int64_t npairs, const int64_t* pairs,
+                                  const int64_t* pair_of, const double* l1, const double* l2, double* out, bool host,
+                                  cudaStream_t s);
 void mo_hx_fock(rr_mo_store* m, const double* h, const double* occ, const double* h2, const double* x2,
                 const int64_t* pair_of, const double* l1, const double* l2, double* F, bool host, cudaStream_t s);
 }  // namespace rr

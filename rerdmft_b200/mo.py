@@ -219,3 +219,33 @@ def casActiveIntegrals(eri, active):
     L.check(L.lib().rr_mo_cas_active_integrals(eri.handle, act.size, act.ctypes.data, out.ctypes.data,
                                                ctypes.byref(L.opts())))
     return out
+
+
+def hartreeExchangeJointHessianDiagonal(h, eri, occupations, two_rdm_h, two_rdm_x, fock, pair_indices, pair_of=None,
+                                        two_rdm_l1=None, two_rdm_l2=None):
+    """hartreeExchangeJointHessianDiagonal on a complex RiMoEri (src/Hessian_opt/HartreeExchangeHessian.cpp:653-711)
+    on the GPU: 2 * len(pair_indices) values, the [real; imaginary] diagonal of the joint orbital Hessian.  With
+    a PNOF functional's full two-RDM and pair_of this is pnofJointHessianDiagonal (PnofHessian.cpp:171-181)."""
+    if eri._kind != L.RR_MO_COMPLEX:
+        raise RrError(L.RR_ERR_UNSUPPORTED, "hartreeExchangeJointHessianDiagonal: needs a complex RiMoEri")
+    n = eri.n
+    hh = np.ascontiguousarray(h, dtype=np.complex128)
+    F = np.ascontiguousarray(fock, dtype=np.complex128)
+    occ = np.ascontiguousarray(occupations, dtype=np.float64)
+    h2 = np.ascontiguousarray(two_rdm_h, dtype=np.float64)
+    x2 = np.ascontiguousarray(two_rdm_x, dtype=np.float64)
+    if hh.shape != (n, n) or F.shape != (n, n) or occ.size != n or h2.shape != (n, n) or x2.shape != (n, n):
+        raise RrError(L.RR_ERR_ARG, "hartreeExchangeJointHessianDiagonal: dimensions inconsistent with the MO tensor")
+    pairs = np.ascontiguousarray(pair_indices, dtype=np.int64).reshape(-1, 2)
+    po = l1 = l2 = None
+    if pair_of is not None:
+        po = np.ascontiguousarray(pair_of, dtype=np.int64)
+        l1 = np.ascontiguousarray(two_rdm_l1, dtype=np.float64)
+        l2 = np.ascontiguousarray(two_rdm_l2, dtype=np.float64)
+    out = np.empty(2 * pairs.shape[0])
+    L.check(L.lib().rr_mo_hx_joint_hessian_diagonal(
+        eri.handle, hh.ctypes.data, occ.ctypes.data, h2.ctypes.data, x2.ctypes.data, F.ctypes.data, pairs.shape[0],
+        pairs.ctypes.data if pairs.size else None, None if po is None else po.ctypes.data,
+        None if l1 is None else l1.ctypes.data, None if l2 is None else l2.ctypes.data, out.ctypes.data,
+        ctypes.byref(L.opts())))
+    return out
