@@ -96,6 +96,17 @@ void with_new_mo(rr_mo_handle* out, rr_mo_store* m, F&& f) {
 }
 
 
+// Clears an SCF result record for a new run, keeping the output pointers the caller set in it.
+void keep_outputs_reset(rr_scf_result* r) {
+  double* w = r->orbital_energies;
+  double* c = r->c_matrix;
+  double* f = r->fock_matrix;
+  *r = rr_scf_result{};
+  r->orbital_energies = w;
+  r->c_matrix = c;
+  r->fock_matrix = f;
+}
+
 rr_ri_store* checked(rr_ri_handle h) {
   if (!h) throw rr::Error(RR_ERR_ARG, "null handle");
   RR_CUDA(cudaSetDevice(h->ctx.device));
@@ -268,7 +279,7 @@ int rr_scf_run_nonrel(rr_ri_handle h, const double* h_core, const double* X, int
     RR_REQUIRE(scf->max_iterations >= 1, RR_ERR_ARG, "rr_scf_run_nonrel: max_iterations < 1");
     RR_REQUIRE(scf->precision == RR_PREC_FP64 || scf->precision == RR_PREC_MIXED, RR_ERR_UNSUPPORTED,
                "rr_scf_run_nonrel: unknown precision");
-    *result = rr_scf_result{};
+    keep_outputs_reset(result);
     rr::scf_nonrel(s, h_core, X, n_eff, S, P0, n_electrons, scf, result, P_out, energy_history, opts);
   });
 }
@@ -284,7 +295,7 @@ int rr_scf_run_x2c(rr_ri_handle h, const double* h_x2c, const double* X, int64_t
     RR_REQUIRE(scf->max_iterations >= 1, RR_ERR_ARG, "rr_scf_run_x2c: max_iterations < 1");
     RR_REQUIRE(scf->precision == RR_PREC_FP64 || scf->precision == RR_PREC_MIXED, RR_ERR_UNSUPPORTED,
                "rr_scf_run_x2c: precision");
-    *result = rr_scf_result{};
+    keep_outputs_reset(result);
     rr::scf_rel(s, 0, h_x2c, nullptr, 2 * s->n, X, n_eff, S, P0, n_electrons, scf, result, P_out, energy_history,
                 opts);
   });
@@ -350,7 +361,7 @@ int rr_scf_run_dhf(rr_ri_handle h, const double* h_rkb, const double* v_total, i
     RR_REQUIRE(scf->max_iterations >= 1, RR_ERR_ARG, "rr_scf_run_dhf: max_iterations < 1");
     RR_REQUIRE(scf->precision == RR_PREC_FP64 || scf->precision == RR_PREC_MIXED, RR_ERR_UNSUPPORTED,
                "rr_scf_run_dhf: precision");
-    *result = rr_scf_result{};
+    keep_outputs_reset(result);
     rr::scf_rel(s, 1, h_rkb, v_total, n_rkb, x_full, n_rkb, s_full, P0, n_electrons, scf, result, P_out,
                 energy_history, opts);
   });

@@ -57,4 +57,13 @@ void gemm(const GemmDesc& d, cudaStream_t stream, double* work = nullptr, int64_
 // Doubles of scratch gemm() would like for split-K on this descriptor.
 int64_t gemm_work_doubles(const GemmDesc& d);
 
+// T[P] = Ct B^P for P < naux on the m16n8k8 FP64 shape (ht_dmma16.cu): Ct nocc x n (row pitch n), B^P
+// n x n in rows of `pitch` doubles, T[P] at T + P nocc n (row pitch n).  Returns false (nothing launched)
+// when the operands do not meet its 16-byte alignment rule.
+bool half_transform_m16(const double* Ct, int64_t nocc, const double* B, int64_t pitch, int64_t naux, int64_t n,
+                        double* T, cudaStream_t s);
+// Which half-transform the nonrelativistic exchange uses: 0 = the general DMMA GEMM (m8n8k4),
+// 1 = half_transform_m16.  RR_HALF_TRANSFORM=m8|m16 overrides the default.
+int half_transform_kind();
+
 }  // namespace rr

@@ -3,6 +3,7 @@
 #include <algorithm>
 
 #include "ri_store.cuh"
+#include "gemm_f64.cuh"
 #include "tma_util.cuh"
 
 namespace rr {
@@ -46,6 +47,34 @@ __global__ void wait_expiry_kernel(uint32_t limit, int* err, long long* out) {
 extern "C" {
 
 int64_t rr_test_device_allocations(void) { return rr::device_allocations(); }
+
+int rr_test_half_transform(const double* Ct, int64_t nocc, const double* B, int64_t naux, int64_t n, double* T,
+                           int32_t variant) {
+  try {
+    rr::set_last_error("");
+    RR_REQUIRE(variant == 0 || variant == 1, RR_ERR_ARG, "rr_test_half_transform: variant must be 0 or 1");
+    if (variant == 1) {
+      RR_REQUIRE(rr::half_transform_m16(Ct, nocc, B, n * n, naux, n, T, nullptr), RR_ERR_UNSUPPORTED,
+                 "rr_test_half_transform: operands not supported by the m16n8k8 kernel");
+    } else {
+      rr::GemmDesc g;
+      g.M = nocc; g.N = n; g.K = n;
+      g.A = Ct; g.lda = n; g.strideA = 0;
+      g.B = B; g.ldb = n; g.strideB = n * n;
+      g.C = T; g.ldc = n; g.strideC = nocc * n;
+      g.batch = naux;
+      rr::gemm(g, nullptr);
+    }
+    RR_CUDA(cudaDeviceSynchronize());
+    return RR_OK;
+  } catch (const rr::Error& e) {
+    rr::set_last_error(e.what());
+    return e.code;
+  } catch (const std::exception& e) {
+    rr::set_last_error(e.what());
+    return RR_ERR_CUDA;
+  }
+}
 
 int rr_test_wait_expiry(uint32_t spin_limit, int32_t threads, int32_t* status_word, double* elapsed_ms,
                         double* cycles) {
