@@ -485,15 +485,22 @@ int rr_adam_default_options(rr_adam_options* out);
 
 /* The ADAM orbital-rotation problem of FULL_OPTIMIZATION (RotationProblem,
  * src/Full_opt/FullOptimization.cpp:1330-1548, with AdamOptimizer, src/Utils/ADAM.cpp:133-213) for a
- * nonrelativistic RI MO tensor m (rr_mo_build_nonrel / RR_MO_NONREL_SPIN) and a fixed-occupation
- * hartree-exchange functional, all on the GPU.  The handle takes a copy of m's tensor.  Host
- * arguments: h (n x n spatial one-electron matrix in m's MO basis), occupations (2n spin
- * orbitals), two_rdm_h / two_rdm_x (2n x 2n), optional pair_of (2n) with two_rdm_l1 / two_rdm_l2
- * (2n x 2n); options NULL = the reference defaults.  Pairs are adamPairIndices(2n) (p > q); the
- * spin-twin pairs get the averaged gradient, so every rotation is spin restricted. */
+ * fixed-occupation hartree-exchange functional, all on the GPU.  The handle takes a copy of m's tensor.
+ * Nonrelativistic m (RR_MO_NONREL_SPIN): h is the n x n spatial one-electron matrix in m's MO basis,
+ * occupations span the 2n spin orbitals, two_rdm_h / two_rdm_x are 2n x 2n, optional pair_of (2n)
+ * with two_rdm_l1 / two_rdm_l2 (2n x 2n); pairs are adamPairIndices(2n) (p > q) and the spin-twin
+ * pairs get the averaged gradient, so every rotation is spin restricted.
+ * Complex m (RR_MO_COMPLEX, n spinors): h is n x n complex (interleaved), occupations n, the two-RDM
+ * factors n x n real, optional pair_of (n) with l1 / l2; pairs are adamPairIndices(n) (p > q),
+ * gradients, steps and rotations complex (RotationProblem<std::complex<double>>).
+ * options NULL = the reference defaults. */
 int rr_orbopt_create(rr_mo_handle m, const double* h, const double* occupations, const double* two_rdm_h,
                      const double* two_rdm_x, const int64_t* pair_of, const double* two_rdm_l1,
                      const double* two_rdm_l2, const rr_adam_options* options, rr_orbopt_handle* out);
+/* Complex problems only: drop every pair that touches one of the first n_negative spinors (the
+ * negative-energy branch of a 4-component basis) from the rotation (RotationProblem's n_negative,
+ * excludeNegative, FullOptimization.cpp:83-92).  Clears the scales of rr_orbopt_set_scales. */
+int rr_orbopt_exclude_negative(rr_orbopt_handle h, int64_t n_negative);
 int rr_orbopt_destroy(rr_orbopt_handle h);
 int rr_orbopt_info(rr_orbopt_handle h, int64_t* n_pairs, int64_t* n_spatial, int64_t* naux);
 /* One AdamOptimizer::run: ADAM steps from the current orbitals until the gradient or energy
@@ -501,7 +508,8 @@ int rr_orbopt_info(rr_orbopt_handle h, int64_t* n_pairs, int64_t* n_spatial, int
  * rate, the extra-iteration allowance and the restart flag persist between runs, as in the
  * reference. */
 int rr_orbopt_run(rr_orbopt_handle h, rr_adam_result* result);
-/* Energy 1/2 sum_q [n_q h_qq + F_qq] and the pair gradient (n_pairs) at the current orbitals. */
+/* Energy 1/2 sum_q [n_q Re h_qq + Re F_qq] and the pair gradient (n_pairs entries, interleaved complex
+ * for a complex problem) at the current orbitals. */
 int rr_orbopt_energy(rr_orbopt_handle h, double* energy);
 int rr_orbopt_gradient(rr_orbopt_handle h, double* gradient);
 /* Per-pair preconditioning scales s (n_pairs, positive; NULL = plain ADAM): ADAM sees g / sqrt(s)
@@ -509,13 +517,16 @@ int rr_orbopt_gradient(rr_orbopt_handle h, double* gradient);
  * (FullOptimization.cpp:1362-1369).  No counterpart for the learned use in the reference. */
 int rr_orbopt_set_scales(rr_orbopt_handle h, const double* scales);
 /* hartreeExchangeHessianElement(p,q,p,q) per pair at the current orbitals
- * (src/Hessian_opt/HartreeExchangeHessian.cpp:221), the labels of the learned preconditioner. */
+ * (src/Hessian_opt/HartreeExchangeHessian.cpp:221), the labels of the learned preconditioner; for a
+ * complex problem the joint [t; y] diagonal of hartreeExchangeJointHessianDiagonal over the pairs
+ * (2 n_pairs entries). */
 int rr_orbopt_hessian_diagonal(rr_orbopt_handle h, double* out);
 /* Preconditioner inputs per pair (i = q, a = p): F_ii, F_aa, n_i, n_a, J_ia, K_ia, J_ii, J_aa
- * (n_pairs x 8 floats; F the generalized Fock matrix, J/K the MO Coulomb and exchange integrals). */
+ * (n_pairs x 8 floats; F the generalized Fock matrix, J/K the MO Coulomb and exchange integrals;
+ * real parts for a complex problem). */
 int rr_orbopt_features(rr_orbopt_handle h, float* out);
-/* Current accumulated spatial rotation (n x n), rotated h (n x n) and MO tensor (naux x n^2);
- * any pointer may be NULL. */
+/* Current accumulated rotation (n x n), rotated h (n x n) and MO tensor (naux x n^2), interleaved
+ * complex for a complex problem; any pointer may be NULL. */
 int rr_orbopt_state(rr_orbopt_handle h, double* rotation, double* h_out, double* Bmo_out);
 
 /* ---------------- learned preconditioner (no counterpart in the reference) ----------------

@@ -45,6 +45,10 @@ int rr_test_adam_steps(int64_t n, int32_t cplx, int64_t nsteps, double lr, doubl
  * orbital optimiser uses (src/Hessian_opt/SpinorRotation.cpp:17 computes the same matrix). */
 int rr_test_rotation_matrix(int64_t n, const double* kappa, double* U);
 
+/* The same for an anti-Hermitian complex kappa (interleaved n x n host matrices in and out), the
+ * route of the complex orbital optimiser. */
+int rr_test_rotation_matrix_complex(int64_t n, const double* kappa, double* U);
+
 /* AdamOptimizer<double>::run `runs` times (ADAM.cpp:140-213) on E(x) = sum (a x^2 / 2 + b x) +
  * c (sum x^2)^2 with x += step, driven by the device ADAM and the library's run logic. */
 int rr_test_adam_run_quadratic(int64_t n, const double* a, const double* b, double c, const double* x0, int32_t runs,

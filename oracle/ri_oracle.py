@@ -621,8 +621,51 @@ class RotationProblemNumpy:
         self.B, self.h = self.best[0].copy(), self.best[1].copy()
 
 
+class RotationProblemComplexNumpy:
+    """RotationProblem<std::complex<double>, RiMoEri> (src/Full_opt/FullOptimization.cpp:1330-1548) for a
+    fixed-occupation hartree-exchange functional: pairs excludeNegative(adamPairIndices(n), n_negative)
+    (FullOptimization.cpp:83-92), complex gradient 2 (F_qp - conj F_pq), kappa_pq = step,
+    kappa_qp = -conj(step) (ADAM.cpp:106-128), rotations U = exp(-kappa) through the eigenvectors of
+    i kappa (SpinorRotation.cpp:17-90) applied as U^dagger B^P U and U^dagger h U, energy from the
+    generalized-Fock identity."""
+
+    def __init__(self, Bmo, h, occ, h2, x2, pair_of=None, l1=None, l2=None, n_negative=0):
+        self.n = h.shape[0]
+        self.B, self.h = np.array(Bmo, dtype=complex), np.array(h, dtype=complex)
+        self.occ, self.h2, self.x2 = occ, h2, x2
+        self.po, self.l1, self.l2 = pair_of, l1, l2
+        self.pairs = [(p, q) for p, q in pair_indices(self.n) if p >= n_negative and q >= n_negative]
+        self.u = np.eye(self.n, dtype=complex)
+        self.best = None
+
+    def fock(self):
+        return hx_fock(self.h, self.B, self.occ, self.h2, self.x2, self.po, self.l1, self.l2)
+
+    def energy(self):
+        return hx_energy_from_fock(self.h, self.occ, self.fock())
+
+    def gradient(self):
+        F = self.fock()
+        return np.array([2.0 * (F[q, p] - np.conj(F[p, q])) for p, q in self.pairs], dtype=complex)
+
+    def rotate(self, step):
+        u = rotation_matrix(kappa_matrix(self.n, self.pairs, np.asarray(step, dtype=complex)))
+        b3 = self.B.reshape(-1, self.n, self.n)
+        self.B = np.einsum("ai,Pab,bj->Pij", u.conj(), b3, u, optimize=True).reshape(b3.shape[0], -1)
+        self.h = u.conj().T @ self.h @ u
+        self.u = self.u @ u
+
+    def save_best(self):
+        self.best = (self.B.copy(), self.h.copy(), self.u.copy())
+
+    def restore_best(self):
+        self.B, self.h, self.u = (x.copy() for x in self.best)
+
+
 class AdamOptimizerNumpy:
-    """AdamOptimizer<double>::run (src/Utils/ADAM.cpp:140-213) with the AdamOptions defaults."""
+    """AdamOptimizer<T>::run (src/Utils/ADAM.cpp:140-213) with the AdamOptions defaults; complex
+    gradients take a complex first moment and the second moment of |g|^2 (Adam<complex>::step,
+    ADAM.cpp:33-51)."""
 
     def __init__(self, lr=0.01, rate_factor=0.2, base=10, inc=20, limit=200, gtol=1e-5, etol=1e-9):
         self.opt = dict(lr=lr, rate_factor=rate_factor, base=base, inc=inc, limit=limit, gtol=gtol, etol=etol)
@@ -635,20 +678,23 @@ class AdamOptimizerNumpy:
         if max_calls > o["limit"]:
             max_calls = o["base"]
         n = len(prob.pairs) if hasattr(prob, "pairs") else prob.dim
-        m1, m2, mx, t = np.zeros(n), np.zeros(n), np.zeros(n), 0
+        m1, m2, mx, t = None, np.zeros(n), np.zeros(n), 0
         e_old = prob.energy()
         e_best = e_old
         prob.save_best()
         improved, ediff = False, 0.0
         while True:
             g = prob.gradient()
+            if m1 is None:
+                m1 = np.zeros(n, dtype=g.dtype)
             if np.abs(g).max() < o["gtol"]:
                 self.lr, self.extra = o["lr"], 0
                 break
             t += 1
             c1, c2 = 1 - 0.7 ** t, 1 - 0.9 ** t
             m1 = 0.7 * m1 + 0.3 * g
-            m2 = 0.9 * m2 + 0.1 * g * g
+            sq = g.real * g.real + g.imag * g.imag if np.iscomplexobj(g) else g * g
+            m2 = 0.9 * m2 + 0.1 * sq
             mx = np.maximum(mx, m2 / c2)
             prob.rotate(-self.lr * (m1 / c1) / (np.sqrt(mx) + 1e-15))
             e = prob.energy()

@@ -100,6 +100,7 @@ _SIGS = {
     "rr_orbopt_create": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(AdamOptions),
                                         ctypes.POINTER(_vp)]),
     "rr_orbopt_destroy": (ctypes.c_int, [_vp]),
+    "rr_orbopt_exclude_negative": (ctypes.c_int, [_vp, _i64]),
     "rr_orbopt_info": (ctypes.c_int, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     "rr_orbopt_run": (ctypes.c_int, [_vp, ctypes.POINTER(AdamResult)]),
     "rr_orbopt_energy": (ctypes.c_int, [_vp, ctypes.POINTER(_d)]),
@@ -117,6 +118,7 @@ _SIGS = {
     "rr_mlp_set_params": (ctypes.c_int, [_vp, _vp]),
     "rr_test_adam_steps": (ctypes.c_int, [_i64, _i32, _i64, _d, _d, _d, _d, _vp, _vp]),
     "rr_test_rotation_matrix": (ctypes.c_int, [_i64, _vp, _vp]),
+    "rr_test_rotation_matrix_complex": (ctypes.c_int, [_i64, _vp, _vp]),
     "rr_test_adam_run_quadratic": (ctypes.c_int, [_i64, _vp, _vp, _d, _vp, _i32, _vp, _vp, _vp, _vp, _vp]),
     "rr_last_error": (ctypes.c_char_p, []),
     "rr_version": (ctypes.c_int, []),

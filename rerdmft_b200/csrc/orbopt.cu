@@ -1,18 +1,22 @@
 // Orbital-rotation optimisation of the functional stage on the GPU (reference: src/Utils/ADAM.cpp,
 // the ADAM branch of the orbital optimisation, and the RotationProblem of
-// src/Full_opt/FullOptimization.cpp:1330-1548) for the nonrelativistic spin-orbital RI tensor
-// (RiNonRelSpinMoEri) with a fixed-occupation hartree-exchange functional (two_rdm_h / two_rdm_x and
-// the optional pair terms two_rdm_l1 / two_rdm_l2).
+// src/Full_opt/FullOptimization.cpp:1330-1548) with a fixed-occupation hartree-exchange functional
+// (two_rdm_h / two_rdm_x and the optional pair terms two_rdm_l1 / two_rdm_l2), for either MO tensor:
+// the nonrelativistic spin-orbital RiNonRelSpinMoEri (RotationProblem<double, ...>) or the complex
+// spinor RiMoEri of X2C / 4c (RotationProblem<complex<double>, ...>).
 //
 // Per ADAM step, all on the device:
-//   g_I = 2 (F_qp - F_pq) over the pairs (p > q) of the 2n spin orbitals, twin pairs (the same
-//         spatial pair in the other spin) averaged            (OrbitalGradient.h, FullOptimization.cpp:1410)
-//   step = Adam<double>::step(g)                              (ADAM.cpp:33-51, exact IEEE operation order)
-//   u = exp(-kappa) of the spatial block of kappa(step)       (SpinorRotation.cpp: eigen route there;
+//   g_I = 2 (F_qp - conj F_pq) over the pairs (p > q): for the spin-orbital kind the 2n spin
+//         orbitals with twin pairs (the same spatial pair in the other spin) averaged; for the
+//         complex kind the n spinors minus the pairs touching the first n_negative ones
+//         (excludeNegative, C4_DHF)                        (OrbitalGradient.h, FullOptimization.cpp:1410)
+//   step = Adam<T>::step(g)                                   (ADAM.cpp:33-51, exact IEEE operation order)
+//   u = exp(-kappa), kappa_pq = step_I, kappa_qp = -conj step_I (ADAM.cpp:92-128); the spatial block
+//         for the spin-orbital kind                        (SpinorRotation.cpp: eigen route there;
 //         scaling and squaring of a Taylor series here, both equal to ~1e-15)
-//   B^P <- u^T B^P u, h <- u^T h u, U_total <- U_total u     (RiNonRelSpinMoEri::rotated)
+//   B^P <- u^dagger B^P u, h <- u^dagger h u, U_total <- U_total u   (RiNonRelSpinMoEri / RiMoEri ::rotated)
 //   F = riHxFockGemm(h, B, occupations, two-RDMs)              (mo_hx_fock)
-//   E = 1/2 sum_q [n_q h_qq + F_qq]                            (FullOptimization.cpp:1383)
+//   E = 1/2 sum_q [n_q Re h_qq + Re F_qq]                      (FullOptimization.cpp:1383)
 // The run / restart / learning-rate logic of AdamOptimizer::run (ADAM.cpp:140-213) is host code.
 //
 // A learned preconditioner enters exactly where the reference's min-max stage rescales its pairs
@@ -281,6 +285,122 @@ __global__ void features_kernel(const double* F, const double* occ, const double
   }
 }
 
+// ---- complex (RiMoEri) problem: explicit pair table pq[2I] = p, pq[2I+1] = q (p > q), interleaved
+// complex matrices.
+
+// g_I = 2 (F_qp - conj F_pq) (orbitalGradient, src/Hessian_opt/OrbitalGradient.h), divided by
+// sqrt(scale_I) on both components.
+__global__ void pair_gradient_c_kernel(const double* F, int64_t d, int64_t npairs, const int64_t* pq,
+                                       const double* scale, double* g) {
+  for (int64_t I = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; I < npairs;
+       I += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t p = pq[2 * I], q = pq[2 * I + 1];
+    double re = 2.0 * (F[2 * (q * d + p)] - F[2 * (p * d + q)]);
+    double im = 2.0 * (F[2 * (q * d + p) + 1] + F[2 * (p * d + q) + 1]);
+    if (scale) {
+      const double r = sqrt(scale[I]);
+      re /= r;
+      im /= r;
+    }
+    g[2 * I] = re;
+    g[2 * I + 1] = im;
+  }
+}
+
+// out[0] = max |g_I| (complex modulus; one CTA)
+__global__ void absmax_c_kernel(const double* g, int64_t n, double* out) {
+  __shared__ double red[32];
+  double m = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, hypot(g[2 * i], g[2 * i + 1]));
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
+    out[0] = m;
+  }
+}
+
+// adamKappaMatrix (src/Utils/ADAM.cpp:106-128) over the pair table: kappa_pq = step_I / sqrt(scale_I),
+// kappa_qp = -conj(kappa_pq); kappa zeroed beforehand.
+__global__ void kappa_c_scatter_kernel(const double* step, const double* scale, const int64_t* pq, int64_t npairs,
+                                       int64_t n, double* kappa) {
+  for (int64_t I = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; I < npairs;
+       I += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t p = pq[2 * I], q = pq[2 * I + 1];
+    double re = step[2 * I], im = step[2 * I + 1];
+    if (scale) {
+      const double r = sqrt(scale[I]);
+      re /= r;
+      im /= r;
+    }
+    kappa[2 * (p * n + q)] = re;
+    kappa[2 * (p * n + q) + 1] = im;
+    kappa[2 * (q * n + p)] = -re;
+    kappa[2 * (q * n + p) + 1] = im;
+  }
+}
+
+// out[0] = max_i sum_j |kappa_ij| (complex modulus; one CTA)
+__global__ void row_norm_c_kernel(const double* kappa, int64_t n, double* out) {
+  __shared__ double red[32];
+  double m = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+    double r = 0.0;
+    for (int64_t j = 0; j < n; ++j) r += hypot(kappa[2 * (i * n + j)], kappa[2 * (i * n + j) + 1]);
+    m = fmax(m, r);
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
+    out[0] = m;
+  }
+}
+
+// Y = I + c X (n x n, interleaved complex, c real)
+__global__ void eye_plus_c_kernel(double* Y, const double* X, double c, int64_t n) {
+  for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < n * n;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    Y[2 * idx] = (idx / n == idx % n ? 1.0 : 0.0) + c * X[2 * idx];
+    Y[2 * idx + 1] = c * X[2 * idx + 1];
+  }
+}
+
+// out[0] = 1/2 sum_q [n_q Re H_qq + Re F_qq] (FullOptimization.cpp:1383; one CTA, interleaved complex)
+__global__ void energy_trace_c_kernel(const double* H, const double* F, const double* occ, int64_t d, double* out) {
+  __shared__ double red[32];
+  double a = 0.0;
+  for (int64_t q = threadIdx.x; q < d; q += blockDim.x) a += occ[q] * H[2 * (q * d + q)] + F[2 * (q * d + q)];
+  for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = a;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) t += red[w];
+    out[0] = 0.5 * t;
+  }
+}
+
+// Preconditioner inputs of the complex problem (real parts of the complex F, J, K), FP32.
+__global__ void features_c_kernel(const double* F, const double* occ, const double* J, const double* K, int64_t d,
+                                  int64_t npairs, const int64_t* pq, float* out) {
+  for (int64_t I = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; I < npairs;
+       I += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t p = pq[2 * I], q = pq[2 * I + 1];
+    float* o = out + I * 8;
+    o[0] = static_cast<float>(F[2 * (q * d + q)]);
+    o[1] = static_cast<float>(F[2 * (p * d + p)]);
+    o[2] = static_cast<float>(occ[q]);
+    o[3] = static_cast<float>(occ[p]);
+    o[4] = static_cast<float>(J[2 * (q * d + p)]);
+    o[5] = static_cast<float>(K[2 * (q * d + p)]);
+    o[6] = static_cast<float>(J[2 * (q * d + q)]);
+    o[7] = static_cast<float>(J[2 * (p * d + p)]);
+  }
+}
+
 // Quadratic test problem E(x) = sum (a x^2/2 + b x) + c (sum x^2)^2 (one CTA each).
 __global__ void quad_energy_kernel(const double* x, const double* a, const double* b, double c, int64_t n, double* out) {
   __shared__ double red[2][32];
@@ -358,6 +478,7 @@ struct DeviceAdam {
 struct OptProblem {
   virtual ~OptProblem() = default;
   virtual int64_t dim() const = 0;
+  virtual int pl() const { return 1; }           // 2: complex parameters (interleaved)
   virtual double energy() = 0;                   // trial point
   virtual double gradient(double* g) = 0;        // g on the device; returns max |g|
   virtual void rotate(const double* step) = 0;   // step on the device
@@ -398,9 +519,10 @@ rr_adam_result adam_run(OptState& st, OptProblem& prob) {
   int max_calls = st.opt.base_iterations + st.extra;
   if (max_calls > st.opt.max_iterations_limit) max_calls = st.opt.base_iterations;
   const int64_t n = prob.dim();
-  st.g.ensure(static_cast<size_t>(std::max<int64_t>(n, 1)));
-  st.step.ensure(static_cast<size_t>(std::max<int64_t>(n, 1)));
-  st.adam.init(n, 1, st.opt, st.lr, s);
+  const int PL = prob.pl();
+  st.g.ensure(static_cast<size_t>(std::max<int64_t>(PL * n, 1)));
+  st.step.ensure(static_cast<size_t>(std::max<int64_t>(PL * n, 1)));
+  st.adam.init(n, PL, st.opt, st.lr, s);
   res.learning_rate = st.lr;
   double e_old = prob.energy();
   double e_best = e_old;
@@ -446,10 +568,13 @@ rr_adam_result adam_run(OptState& st, OptProblem& prob) {
   return res;
 }
 
-// U = exp(-kappa) for a real antisymmetric n x n kappa (device), by scaling and squaring of the
-// Taylor series in Horner form: after scaling ||A|| <= 1/2 (norm = a 1-norm bound of kappa) and the
-// degree is the smallest m with ||A||^(m+1) / (m+1)! < 2^-60.  Ta, Tb: n x n scratch.
-void expm_neg(const double* kap, double norm, int64_t n, double* U, double* Ta, double* Tb, cudaStream_t s) {
+// U = exp(-kappa) for an anti-symmetric (real) or anti-Hermitian (complex, interleaved) n x n kappa
+// on the device, by scaling and squaring of the Taylor series in Horner form: after scaling
+// ||A|| <= 1/2 (norm = a 1-norm bound of kappa) and the degree is the smallest m with
+// ||A||^(m+1) / (m+1)! < 2^-60.  Ta, Tb: n x n scratch of the same element kind.
+// (src/Hessian_opt/SpinorRotation.cpp:17 forms the same matrix through the eigenvectors of i kappa.)
+void expm_neg(const double* kap, double norm, int64_t n, double* U, double* Ta, double* Tb, cudaStream_t s,
+              bool cplx) {
   int sq = 0;
   double a = norm;
   while (a > 0.5) { a *= 0.5; ++sq; }
@@ -461,23 +586,28 @@ void expm_neg(const double* kap, double norm, int64_t n, double* U, double* Ta, 
     ++m;
   }
   const double scale = -std::ldexp(1.0, -sq);  // A = -kappa / 2^sq
+  auto eye_plus = [&](double* Y, const double* X, double c) {
+    if (cplx) eye_plus_c_kernel<<<blocks_for(n * n), 256, 0, s>>>(Y, X, c, n);
+    else eye_plus_kernel<<<blocks_for(n * n), 256, 0, s>>>(Y, X, c, n);
+    RR_LAUNCH_CHECK();
+  };
   GemmDesc g;
+  g.cplx = cplx;
   g.M = n; g.N = n; g.K = n; g.A = kap; g.lda = n; g.ldb = n; g.ldc = n;
-  eye_plus_kernel<<<blocks_for(n * n), 256, 0, s>>>(Ta, kap, scale / m, n);  // T = I + A/m
-  RR_LAUNCH_CHECK();
+  eye_plus(Ta, kap, scale / m);  // T = I + A/m
   for (int k = m - 1; k >= 1; --k) {  // T = I + (A T) / k
     g.B = Ta; g.C = Tb; g.alpha = scale / k; g.beta = 0.0;
     gemm(g, s);
-    eye_plus_kernel<<<blocks_for(n * n), 256, 0, s>>>(Ta, Tb, 1.0, n);
-    RR_LAUNCH_CHECK();
+    eye_plus(Ta, Tb, 1.0);
   }
   for (int i = 0; i < sq; ++i) {
     GemmDesc q;
+    q.cplx = cplx;
     q.M = n; q.N = n; q.K = n; q.A = Ta; q.lda = n; q.B = Ta; q.ldb = n; q.C = Tb; q.ldc = n;
     gemm(q, s);
     std::swap(Ta, Tb);
   }
-  RR_CUDA(cudaMemcpyAsync(U, Ta, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, s));
+  RR_CUDA(cudaMemcpyAsync(U, Ta, sizeof(double) * (cplx ? 2 : 1) * n * n, cudaMemcpyDeviceToDevice, s));
 }
 
 }  // namespace rr
@@ -485,9 +615,15 @@ void expm_neg(const double* kap, double norm, int64_t n, double* U, double* Ta, 
 
 struct rr_orbopt_store : rr::OptProblem {
   rr::Context ctx;
-  int64_t n = 0, d = 0, naux = 0, npairs = 0;
+  // cplx 0: RiNonRelSpinMoEri (n spatial orbitals, d = 2n spin orbitals, pairs adamPairIndices(2n) by
+  // formula, spin-restricted rotations of the spatial block); cplx 1: RiMoEri (d = n spinors, the
+  // pair table pqd = adamPairIndices(n) without the pairs that touch the first n_negative spinors,
+  // unitary rotations).
+  int cplx = 0, PL = 1;
+  int64_t n = 0, d = 0, naux = 0, npairs = 0, n_negative = 0;
   rr_mo_store mo;  // trial tensor (mo.B) and the MO kernels' scratch
   rr::DevBuf<double> Bbest, Bwork, mats;
+  rr::DevBuf<int64_t> pqd;
   double *h_t = nullptr, *h_b = nullptr, *u_t = nullptr, *u_b = nullptr, *H = nullptr, *F = nullptr;
   double *occ = nullptr, *h2 = nullptr, *x2 = nullptr, *l1 = nullptr, *l2 = nullptr, *scal = nullptr;
   double *kap = nullptr, *U = nullptr, *Ta = nullptr, *Tb = nullptr, *scales = nullptr, *J = nullptr, *K = nullptr;
@@ -498,16 +634,40 @@ struct rr_orbopt_store : rr::OptProblem {
   rr::OptState state;
 
   int64_t dim() const override { return npairs; }
+  int pl() const override { return PL; }
   cudaStream_t stream() const override { return ctx.main; }
+
+  // excludeNegative(adamPairIndices(n), n_negative) (FullOptimization.cpp:83-92) into pqd.
+  void set_pairs(int64_t nneg) {
+    std::vector<int64_t> t;
+    t.reserve(static_cast<size_t>(n * (n - 1)));
+    for (int64_t p = 0; p < n; ++p)
+      for (int64_t q = 0; q < p; ++q)
+        if (p >= nneg && q >= nneg) {
+          t.push_back(p);
+          t.push_back(q);
+        }
+    n_negative = nneg;
+    npairs = static_cast<int64_t>(t.size() / 2);
+    pqd.ensure(std::max<size_t>(t.size(), 2));
+    if (!t.empty())
+      RR_CUDA(cudaMemcpyAsync(pqd.p, t.data(), sizeof(int64_t) * t.size(), cudaMemcpyHostToDevice, ctx.main));
+    RR_CUDA(cudaStreamSynchronize(ctx.main));
+  }
 
   // F and E at the trial orbitals (cached until the next rotation).
   void build_fock() {
     if (fock_valid) return;
     cudaStream_t s = ctx.main;
-    rr::spin_block_kernel<<<rr::blocks_for(d * d), 256, 0, s>>>(h_t, n, H);
-    RR_LAUNCH_CHECK();
-    rr::mo_hx_fock(&mo, H, occ, h2, x2, have_l ? po : nullptr, l1, l2, F, false, s);
-    rr::energy_trace_kernel<<<1, 256, 0, s>>>(H, F, occ, d, scal);
+    if (cplx) {
+      rr::mo_hx_fock(&mo, h_t, occ, h2, x2, have_l ? po : nullptr, l1, l2, F, false, s);
+      rr::energy_trace_c_kernel<<<1, 256, 0, s>>>(h_t, F, occ, d, scal);
+    } else {
+      rr::spin_block_kernel<<<rr::blocks_for(d * d), 256, 0, s>>>(h_t, n, H);
+      RR_LAUNCH_CHECK();
+      rr::mo_hx_fock(&mo, H, occ, h2, x2, have_l ? po : nullptr, l1, l2, F, false, s);
+      rr::energy_trace_kernel<<<1, 256, 0, s>>>(H, F, occ, d, scal);
+    }
     RR_LAUNCH_CHECK();
     double e;
     RR_CUDA(cudaMemcpyAsync(&e, scal, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -522,9 +682,18 @@ struct rr_orbopt_store : rr::OptProblem {
   double gradient(double* g) override {
     build_fock();
     cudaStream_t s = ctx.main;
-    rr::pair_gradient_kernel<<<rr::blocks_for(npairs), 256, 0, s>>>(F, n, npairs, have_scales ? scales : nullptr, g);
-    RR_LAUNCH_CHECK();
-    rr::absmax_kernel<<<1, 512, 0, s>>>(g, npairs, scal + 1);
+    const double* sc = have_scales ? scales : nullptr;
+    if (cplx) {
+      if (npairs) {
+        rr::pair_gradient_c_kernel<<<rr::blocks_for(npairs), 256, 0, s>>>(F, d, npairs, pqd.p, sc, g);
+        RR_LAUNCH_CHECK();
+      }
+      rr::absmax_c_kernel<<<1, 512, 0, s>>>(g, npairs, scal + 1);
+    } else {
+      rr::pair_gradient_kernel<<<rr::blocks_for(npairs), 256, 0, s>>>(F, n, npairs, sc, g);
+      RR_LAUNCH_CHECK();
+      rr::absmax_kernel<<<1, 512, 0, s>>>(g, npairs, scal + 1);
+    }
     RR_LAUNCH_CHECK();
     double m;
     RR_CUDA(cudaMemcpyAsync(&m, scal + 1, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -533,45 +702,59 @@ struct rr_orbopt_store : rr::OptProblem {
   }
   void rotate(const double* step) override {
     cudaStream_t s = ctx.main;
-    rr::kappa_kernel<<<1, 256, 0, s>>>(step, have_scales ? scales : nullptr, n, kap, scal + 2);
+    const double* sc = have_scales ? scales : nullptr;
+    if (cplx) {
+      RR_CUDA(cudaMemsetAsync(kap, 0, sizeof(double) * 2 * n * n, s));
+      if (npairs) {
+        rr::kappa_c_scatter_kernel<<<rr::blocks_for(npairs), 256, 0, s>>>(step, sc, pqd.p, npairs, n, kap);
+        RR_LAUNCH_CHECK();
+      }
+      rr::row_norm_c_kernel<<<1, 256, 0, s>>>(kap, n, scal + 2);
+    } else {
+      rr::kappa_kernel<<<1, 256, 0, s>>>(step, sc, n, kap, scal + 2);
+    }
     RR_LAUNCH_CHECK();
     double norm;
     RR_CUDA(cudaMemcpyAsync(&norm, scal + 2, sizeof(double), cudaMemcpyDeviceToHost, s));
     RR_CUDA(cudaStreamSynchronize(s));
-    rr::expm_neg(kap, norm, n, U, Ta, Tb, s);
+    rr::expm_neg(kap, norm, n, U, Ta, Tb, s, cplx != 0);
     const int64_t nn = n * n;
-    rr::GemmDesc a;  // W^P = u^T B^P
+    // real: u^T (.) u; complex: U^dagger (.) U (RiNonRelSpinMoEri::rotated / RiMoEri::rotated)
+    rr::GemmDesc a;  // W^P = u^dagger B^P
+    a.cplx = cplx; a.conjA = cplx;
     a.M = n; a.N = n; a.K = n; a.A = U; a.lda = n; a.opA = rr::Op::T;
     a.B = mo.B.p; a.ldb = n; a.strideB = nn; a.C = Bwork.p; a.ldc = n; a.strideC = nn; a.batch = naux;
     rr::gemm(a, s);
     rr::GemmDesc b;  // B^P = W^P u
+    b.cplx = cplx;
     b.M = n; b.N = n; b.K = n; b.A = Bwork.p; b.lda = n; b.strideA = nn; b.B = U; b.ldb = n;
     b.C = mo.B.p; b.ldc = n; b.strideC = nn; b.batch = naux;
     rr::gemm(b, s);
-    rr::GemmDesc c;  // h = u^T h u
+    rr::GemmDesc c;  // h = u^dagger h u
+    c.cplx = cplx; c.conjA = cplx;
     c.M = n; c.N = n; c.K = n; c.A = U; c.lda = n; c.opA = rr::Op::T; c.B = h_t; c.ldb = n; c.C = Ta; c.ldc = n;
     rr::gemm(c, s);
-    c.opA = rr::Op::N; c.A = Ta; c.B = U; c.C = h_t;
+    c.opA = rr::Op::N; c.conjA = 0; c.A = Ta; c.B = U; c.C = h_t;
     rr::gemm(c, s);
     c.A = u_t; c.B = U; c.C = Ta;  // U_total <- U_total u
     rr::gemm(c, s);
-    RR_CUDA(cudaMemcpyAsync(u_t, Ta, sizeof(double) * nn, cudaMemcpyDeviceToDevice, s));
+    RR_CUDA(cudaMemcpyAsync(u_t, Ta, sizeof(double) * PL * nn, cudaMemcpyDeviceToDevice, s));
     fock_valid = false;
   }
   void save_best() override {
     cudaStream_t s = ctx.main;
-    RR_CUDA(cudaMemcpyAsync(Bbest.p, mo.B.p, sizeof(double) * naux * n * n, cudaMemcpyDeviceToDevice, s));
-    RR_CUDA(cudaMemcpyAsync(h_b, h_t, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, s));
-    RR_CUDA(cudaMemcpyAsync(u_b, u_t, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, s));
+    RR_CUDA(cudaMemcpyAsync(Bbest.p, mo.B.p, sizeof(double) * PL * naux * n * n, cudaMemcpyDeviceToDevice, s));
+    RR_CUDA(cudaMemcpyAsync(h_b, h_t, sizeof(double) * PL * n * n, cudaMemcpyDeviceToDevice, s));
+    RR_CUDA(cudaMemcpyAsync(u_b, u_t, sizeof(double) * PL * n * n, cudaMemcpyDeviceToDevice, s));
   }
   void restore_best() override {
     cudaStream_t s = ctx.main;
-    RR_CUDA(cudaMemcpyAsync(mo.B.p, Bbest.p, sizeof(double) * naux * n * n, cudaMemcpyDeviceToDevice, s));
-    RR_CUDA(cudaMemcpyAsync(h_t, h_b, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, s));
-    RR_CUDA(cudaMemcpyAsync(u_t, u_b, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, s));
+    RR_CUDA(cudaMemcpyAsync(mo.B.p, Bbest.p, sizeof(double) * PL * naux * n * n, cudaMemcpyDeviceToDevice, s));
+    RR_CUDA(cudaMemcpyAsync(h_t, h_b, sizeof(double) * PL * n * n, cudaMemcpyDeviceToDevice, s));
+    RR_CUDA(cudaMemcpyAsync(u_t, u_b, sizeof(double) * PL * n * n, cudaMemcpyDeviceToDevice, s));
     fock_valid = false;
   }
-  // J, K (2n x 2n, spin rule) and M1 = two_rdm_h (K - J) at the current orbitals (F built too).
+  // J, K (2n x 2n, spin rule) and M1 = two_rdm_h (K - J) at the current orbitals (F built too; real kind).
   void jk_m1() {
     cudaStream_t s = ctx.main;
     build_fock();
@@ -663,63 +846,66 @@ int rr_orbopt_create(rr_mo_handle m, const double* h, const double* occupations,
                      const double* two_rdm_l2, const rr_adam_options* options, rr_orbopt_handle* out) {
   return guarded([&] {
     RR_REQUIRE(m && out && h && occupations && two_rdm_h && two_rdm_x, RR_ERR_ARG, "rr_orbopt_create: null argument");
-    RR_REQUIRE(m->cplx == 0, RR_ERR_UNSUPPORTED,
-               "rr_orbopt_create: only the nonrelativistic spin-orbital tensor (RiNonRelSpinMoEri) is supported");
     RR_REQUIRE(!pair_of || (two_rdm_l1 && two_rdm_l2), RR_ERR_ARG,
                "rr_orbopt_create: pair_of needs two_rdm_l1 and two_rdm_l2");
     RR_CUDA(cudaSetDevice(m->ctx.device));
     *out = nullptr;
-    const int64_t n = m->n, d = 2 * n, nn = n * n, dd = d * d;
+    const int cplx = m->cplx ? 1 : 0, PL = cplx ? 2 : 1;
+    const int64_t n = m->n, d = cplx ? n : 2 * n, nn = n * n, dd = d * d;
     if (pair_of)
       for (int64_t i = 0; i < d; ++i)
         RR_REQUIRE(pair_of[i] >= 0 && pair_of[i] < d, RR_ERR_ARG, "rr_orbopt_create: pair_of out of range");
     auto* o = new rr_orbopt_store();
     try {
       o->ctx.init(nullptr);
+      o->cplx = cplx;
+      o->PL = PL;
       o->n = n;
       o->d = d;
       o->naux = m->naux;
-      o->npairs = d * (d - 1) / 2;
       o->state.opt = options ? *options : rr::default_adam_options();
       o->state.lr = o->state.opt.learning_rate;
       cudaStream_t s = o->ctx.main;
-      o->mo.cplx = 0;
+      if (cplx) o->set_pairs(0);
+      else o->npairs = d * (d - 1) / 2;
+      o->mo.cplx = cplx;
       o->mo.naux = o->naux;
       o->mo.n = n;
-      const size_t bsz = static_cast<size_t>(std::max<int64_t>(o->naux * nn, 1));
+      const size_t bsz = static_cast<size_t>(std::max<int64_t>(PL * o->naux * nn, 1));
       o->mo.B.alloc(bsz);
       o->Bbest.alloc(bsz);
       o->Bwork.alloc(bsz);
-      RR_CUDA(cudaMemcpyAsync(o->mo.B.p, m->B.p, sizeof(double) * o->naux * nn, cudaMemcpyDeviceToDevice, s));
+      RR_CUDA(cudaMemcpyAsync(o->mo.B.p, m->B.p, sizeof(double) * PL * o->naux * nn, cudaMemcpyDeviceToDevice, s));
+      const int64_t mat = PL * nn, big = std::max(PL * nn, dd);
       rr::Arena ar(&o->mats);
-      ar.request(&o->h_t, nn);
-      ar.request(&o->h_b, nn);
-      ar.request(&o->u_t, nn);
-      ar.request(&o->u_b, nn);
-      ar.request(&o->kap, nn);
-      ar.request(&o->U, nn);
-      ar.request(&o->Ta, std::max(nn, dd));
-      ar.request(&o->Tb, std::max(nn, dd));
+      ar.request(&o->h_t, mat);
+      ar.request(&o->h_b, mat);
+      ar.request(&o->u_t, mat);
+      ar.request(&o->u_b, mat);
+      ar.request(&o->kap, mat);
+      ar.request(&o->U, mat);
+      ar.request(&o->Ta, big);
+      ar.request(&o->Tb, big);
       ar.request(&o->H, dd);
-      ar.request(&o->F, dd);
-      ar.request(&o->J, dd);
-      ar.request(&o->K, dd);
+      ar.request(&o->F, PL * dd);
+      ar.request(&o->J, PL * dd);
+      ar.request(&o->K, PL * dd);
       ar.request(&o->M1, dd);
       ar.request(&o->occ, d);
       ar.request(&o->h2, dd);
       ar.request(&o->x2, dd);
       ar.request(&o->l1, dd);
       ar.request(&o->l2, dd);
-      ar.request(&o->scales, o->npairs);
+      ar.request(&o->scales, std::max<int64_t>(o->npairs, d * (d - 1) / 2));
       double* pob;
       ar.request(&pob, d);
       ar.request(&o->scal, 64);
       ar.commit();
       o->po = reinterpret_cast<int64_t*>(pob);
-      rr::copy_in(o->h_t, h, nn, true, s);
-      std::vector<double> eye(static_cast<size_t>(nn), 0.0);
-      for (int64_t i = 0; i < n; ++i) eye[static_cast<size_t>(i * n + i)] = 1.0;
-      rr::copy_in(o->u_t, eye.data(), nn, true, s);
+      rr::copy_in(o->h_t, h, mat, true, s);
+      std::vector<double> eye(static_cast<size_t>(mat), 0.0);
+      for (int64_t i = 0; i < n; ++i) eye[static_cast<size_t>(PL * (i * n + i))] = 1.0;
+      rr::copy_in(o->u_t, eye.data(), mat, true, s);
       rr::copy_in(o->occ, occupations, d, true, s);
       rr::copy_in(o->h2, two_rdm_h, dd, true, s);
       rr::copy_in(o->x2, two_rdm_x, dd, true, s);
@@ -736,6 +922,17 @@ int rr_orbopt_create(rr_mo_handle m, const double* h, const double* occupations,
       throw;
     }
     *out = o;
+  });
+}
+
+int rr_orbopt_exclude_negative(rr_orbopt_handle h, int64_t n_negative) {
+  return guarded([&] {
+    auto* o = checked_opt(h);
+    RR_REQUIRE(o->cplx, RR_ERR_UNSUPPORTED,
+               "rr_orbopt_exclude_negative: the negative-energy branch exists for the complex (4-component) tensor only");
+    RR_REQUIRE(n_negative >= 0 && n_negative <= o->n, RR_ERR_ARG, "rr_orbopt_exclude_negative: n_negative out of range");
+    o->set_pairs(n_negative);
+    o->have_scales = false;
   });
 }
 
@@ -794,9 +991,9 @@ int rr_orbopt_gradient(rr_orbopt_handle h, double* g) {
   return guarded([&] {
     auto* o = checked_opt(h);
     RR_REQUIRE(g, RR_ERR_ARG, "rr_orbopt_gradient: null output");
-    rr::DevBuf<double> gd(static_cast<size_t>(std::max<int64_t>(o->npairs, 1)));
+    rr::DevBuf<double> gd(static_cast<size_t>(std::max<int64_t>(o->PL * o->npairs, 1)));
     o->gradient(gd.p);
-    rr::copy_out(g, gd.p, o->npairs, true, o->ctx.main);
+    rr::copy_out(g, gd.p, o->PL * o->npairs, true, o->ctx.main);
     RR_CUDA(cudaStreamSynchronize(o->ctx.main));
   });
 }
@@ -806,6 +1003,16 @@ int rr_orbopt_hessian_diagonal(rr_orbopt_handle h, double* out) {
     auto* o = checked_opt(h);
     RR_REQUIRE(out, RR_ERR_ARG, "rr_orbopt_hessian_diagonal: null output");
     cudaStream_t s = o->ctx.main;
+    if (o->cplx) {
+      // hartreeExchangeJointHessianDiagonal over the pair table: 2 n_pairs entries
+      o->build_fock();
+      rr::DevBuf<double> od(static_cast<size_t>(std::max<int64_t>(2 * o->npairs, 1)));
+      rr::mo_hx_joint_hessian_diagonal(&o->mo, o->h_t, o->occ, o->h2, o->x2, o->F, o->npairs, o->pqd.p,
+                                       o->have_l ? o->po : nullptr, o->l1, o->l2, od.p, false, s);
+      rr::copy_out(out, od.p, 2 * o->npairs, true, s);
+      RR_CUDA(cudaStreamSynchronize(s));
+      return;
+    }
     o->jk_m1();
     rr::spin_block_kernel<<<rr::blocks_for(o->d * o->d), 256, 0, s>>>(o->h_t, o->n, o->H);
     RR_LAUNCH_CHECK();
@@ -830,8 +1037,14 @@ int rr_orbopt_features(rr_orbopt_handle h, float* out) {
     o->build_fock();
     rr::mo_jkl(&o->mo, nullptr, o->J, o->K, nullptr, false, s);
     rr::DevBuf<float> fd(static_cast<size_t>(std::max<int64_t>(8 * o->npairs, 1)));
-    rr::features_kernel<<<rr::blocks_for(o->npairs), 256, 0, s>>>(o->F, o->occ, o->J, o->K, o->d, o->npairs, fd.p);
-    RR_LAUNCH_CHECK();
+    if (o->npairs) {
+      if (o->cplx)
+        rr::features_c_kernel<<<rr::blocks_for(o->npairs), 256, 0, s>>>(o->F, o->occ, o->J, o->K, o->d, o->npairs,
+                                                                         o->pqd.p, fd.p);
+      else
+        rr::features_kernel<<<rr::blocks_for(o->npairs), 256, 0, s>>>(o->F, o->occ, o->J, o->K, o->d, o->npairs, fd.p);
+      RR_LAUNCH_CHECK();
+    }
     RR_CUDA(cudaMemcpyAsync(out, fd.p, sizeof(float) * 8 * o->npairs, cudaMemcpyDeviceToHost, s));
     RR_CUDA(cudaStreamSynchronize(s));
   });
@@ -841,9 +1054,9 @@ int rr_orbopt_state(rr_orbopt_handle h, double* rotation, double* h_out, double*
   return guarded([&] {
     auto* o = checked_opt(h);
     cudaStream_t s = o->ctx.main;
-    if (rotation) rr::copy_out(rotation, o->u_t, o->n * o->n, true, s);
-    if (h_out) rr::copy_out(h_out, o->h_t, o->n * o->n, true, s);
-    if (Bmo_out) rr::copy_out(Bmo_out, o->mo.B.p, o->naux * o->n * o->n, true, s);
+    if (rotation) rr::copy_out(rotation, o->u_t, o->PL * o->n * o->n, true, s);
+    if (h_out) rr::copy_out(h_out, o->h_t, o->PL * o->n * o->n, true, s);
+    if (Bmo_out) rr::copy_out(Bmo_out, o->mo.B.p, o->PL * o->naux * o->n * o->n, true, s);
     RR_CUDA(cudaStreamSynchronize(s));
   });
 }
@@ -880,8 +1093,24 @@ int rr_test_rotation_matrix(int64_t n, const double* kappa, double* U) {
     }
     rr::DevBuf<double> k(static_cast<size_t>(std::max<int64_t>(n * n, 1))), u(k.n), a(k.n), b(k.n);
     RR_CUDA(cudaMemcpy(k.p, kappa, sizeof(double) * n * n, cudaMemcpyHostToDevice));
-    rr::expm_neg(k.p, norm, n, u.p, a.p, b.p, nullptr);
+    rr::expm_neg(k.p, norm, n, u.p, a.p, b.p, nullptr, false);
     RR_CUDA(cudaMemcpy(U, u.p, sizeof(double) * n * n, cudaMemcpyDeviceToHost));
+  });
+}
+
+int rr_test_rotation_matrix_complex(int64_t n, const double* kappa, double* U) {
+  return guarded([&] {
+    double norm = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+      double r = 0.0;
+      for (int64_t j = 0; j < n; ++j) r += std::hypot(kappa[2 * (i * n + j)], kappa[2 * (i * n + j) + 1]);
+      norm = std::max(norm, r);
+    }
+    const size_t cnt = static_cast<size_t>(std::max<int64_t>(2 * n * n, 2));
+    rr::DevBuf<double> k(cnt), u(cnt), a(cnt), b(cnt);
+    RR_CUDA(cudaMemcpy(k.p, kappa, sizeof(double) * 2 * n * n, cudaMemcpyHostToDevice));
+    rr::expm_neg(k.p, norm, n, u.p, a.p, b.p, nullptr, true);
+    RR_CUDA(cudaMemcpy(U, u.p, sizeof(double) * 2 * n * n, cudaMemcpyDeviceToHost));
   });
 }
 

@@ -12,7 +12,8 @@
 
 The functional is a fixed-occupation hartree-exchange form (two_rdm_h, two_rdm_x and optionally the
 pair terms pair_of / two_rdm_l1 / two_rdm_l2) over the nonrelativistic spin-orbital RI tensor
-(``mo.RiNonRelSpinMoEri``), as in the reference's RI FULL_OPTIMIZATION.
+(``mo.RiNonRelSpinMoEri``) or the complex spinor tensor (``mo.RiMoEri``, X2C / 4c), as in the
+reference's RI FULL_OPTIMIZATION.
 """
 from __future__ import annotations
 
@@ -36,22 +37,29 @@ def adam_default_options() -> L.AdamOptions:
 
 
 class RotationProblem:
-    """ADAM orbital-rotation problem on the GPU for `eri` (RiNonRelSpinMoEri, n spatial orbitals).
+    """ADAM orbital-rotation problem on the GPU (RotationProblem<T, Eri>) for `eri`:
 
-    h: n x n spatial one-electron matrix in eri's MO basis; occupations: 2n; two_rdm_h / two_rdm_x:
-    2n x 2n; optional pair_of (2n) with two_rdm_l1 / two_rdm_l2 (2n x 2n)."""
+    * ``RiNonRelSpinMoEri`` (n spatial orbitals): h is the n x n spatial one-electron matrix in eri's
+      MO basis; occupations 2n; two_rdm_h / two_rdm_x 2n x 2n; optional pair_of (2n) with
+      two_rdm_l1 / two_rdm_l2 (2n x 2n).  Pairs adamPairIndices(2n), spin-twin averaged gradient.
+    * ``RiMoEri`` (n spinors, complex): h complex n x n; occupations n; two-RDM factors n x n;
+      optional pair_of (n) with l1 / l2; ``n_negative`` drops the pairs touching the first
+      n_negative spinors (excludeNegative, FullOptimization.cpp:83-92).  Complex gradient and steps."""
 
     def __init__(self, eri, h, occupations, two_rdm_h, two_rdm_x, pair_of=None, two_rdm_l1=None, two_rdm_l2=None,
-                 options: L.AdamOptions | None = None):
+                 options: L.AdamOptions | None = None, n_negative: int = 0):
         n = eri.n
-        d = 2 * n
-        h = _d(h)
+        self.complex = getattr(eri, "_kind", L.RR_MO_NONREL_SPIN) == L.RR_MO_COMPLEX
+        d = n if self.complex else 2 * n
+        h = np.ascontiguousarray(h, dtype=np.complex128) if self.complex else _d(h)
         if h.shape != (n, n):
-            raise RrError(L.RR_ERR_ARG, "RotationProblem: h must be the n x n spatial matrix")
+            raise RrError(L.RR_ERR_ARG, "RotationProblem: h must be n x n in the tensor's MO basis")
         occ = _d(occupations)
         h2, x2 = _d(two_rdm_h), _d(two_rdm_x)
         if occ.shape != (d,) or h2.shape != (d, d) or x2.shape != (d, d):
-            raise RrError(L.RR_ERR_ARG, "RotationProblem: occupations / two-RDMs must span the 2n spin orbitals")
+            raise RrError(L.RR_ERR_ARG, "RotationProblem: occupations / two-RDMs must span the %d accessor orbitals" % d)
+        if n_negative and not self.complex:
+            raise RrError(L.RR_ERR_UNSUPPORTED, "RotationProblem: n_negative needs the complex RiMoEri tensor")
         po = None if pair_of is None else np.ascontiguousarray(pair_of, dtype=np.int64)
         l1 = None if po is None else _d(two_rdm_l1)
         l2 = None if po is None else _d(two_rdm_l2)
@@ -61,12 +69,20 @@ class RotationProblem:
                                          None if po is None else l1.ctypes.data,
                                          None if po is None else l2.ctypes.data,
                                          None if options is None else ctypes.byref(options), ctypes.byref(self.handle)))
-        self.n, self.d = n, d
-        self.n_pairs = d * (d - 1) // 2
-        p = np.array([pp for pp in range(d) for _ in range(pp)])
-        q = np.array([qq for pp in range(d) for qq in range(pp)])
-        self.pairs = np.stack([p, q], axis=1) if self.n_pairs else np.zeros((0, 2), dtype=int)
-        self.cross_spin = (p >= n) != (q >= n) if self.n_pairs else np.zeros(0, dtype=bool)
+        if n_negative:
+            L.check(L.lib().rr_orbopt_exclude_negative(self.handle, int(n_negative)))
+        self.n, self.d, self.n_negative = n, d, int(n_negative)
+        pq = [(pp, qq) for pp in range(d) for qq in range(pp) if pp >= self.n_negative and qq >= self.n_negative]
+        self.n_pairs = len(pq)
+        self.pairs = np.array(pq, dtype=int).reshape(-1, 2)
+        if self.complex:
+            self.cross_spin = np.zeros(self.n_pairs, dtype=bool)
+        else:
+            self.cross_spin = (self.pairs[:, 0] >= n) != (self.pairs[:, 1] >= n)
+
+    @property
+    def _dt(self):
+        return np.complex128 if self.complex else np.float64
 
     def close(self):
         if self.handle and self.handle.value:
@@ -90,12 +106,13 @@ class RotationProblem:
         return e.value
 
     def gradient(self) -> np.ndarray:
-        g = np.empty(self.n_pairs)
+        g = np.empty(self.n_pairs, dtype=self._dt)
         L.check(L.lib().rr_orbopt_gradient(self.handle, g.ctypes.data))
         return g
 
     def hessian_diagonal(self) -> np.ndarray:
-        h = np.empty(self.n_pairs)
+        """Per-pair diagonal Hessian; the joint [t; y] diagonal (2 n_pairs) for a complex problem."""
+        h = np.empty(2 * self.n_pairs if self.complex else self.n_pairs)
         L.check(L.lib().rr_orbopt_hessian_diagonal(self.handle, h.ctypes.data))
         return h
 
@@ -114,12 +131,12 @@ class RotationProblem:
         L.check(L.lib().rr_orbopt_set_scales(self.handle, s.ctypes.data))
 
     def state(self, with_tensor: bool = False):
-        """(accumulated spatial rotation, rotated h, rotated MO tensor or None)."""
-        u = np.empty((self.n, self.n))
-        h = np.empty((self.n, self.n))
+        """(accumulated rotation, rotated h, rotated MO tensor or None)."""
+        u = np.empty((self.n, self.n), dtype=self._dt)
+        h = np.empty((self.n, self.n), dtype=self._dt)
         naux = ctypes.c_int64()
         L.check(L.lib().rr_orbopt_info(self.handle, None, None, ctypes.byref(naux)))
-        b = np.empty((naux.value, self.n * self.n)) if with_tensor else None
+        b = np.empty((naux.value, self.n * self.n), dtype=self._dt) if with_tensor else None
         L.check(L.lib().rr_orbopt_state(self.handle, u.ctypes.data, h.ctypes.data, None if b is None else b.ctypes.data))
         return u, h, b
 
@@ -131,6 +148,8 @@ def hessian_scales(problem: RotationProblem, hdiag, clip: float = 16.0, quantile
     pairs as well cost more iterations than it saved on the synthetic functional-stage problems);
     cross-spin pairs (zero gradient) keep 1."""
     h = np.abs(np.asarray(hdiag, dtype=float))
+    if h.shape[0] == 2 * problem.n_pairs and problem.complex:  # joint [t; y] diagonal: one scale per pair
+        h = 0.5 * (h[: problem.n_pairs] + h[problem.n_pairs:])
     same = ~problem.cross_spin
     med = np.quantile(h[same], quantile) if same.any() else 1.0
     if not med > 0:
@@ -279,11 +298,16 @@ PARAMS_FILE = __import__("pathlib").Path(__file__).resolve().parent / "data" / "
 
 
 def problem_from_system(sysd: dict, options: L.AdamOptions | None = None):
-    """(RotationProblem, MO tensor) for a dict of rerdmft_b200.synth.functional_system's form."""
-    from .mo import RiNonRelSpinMoEri
+    """(RotationProblem, MO tensor) for a dict of rerdmft_b200.synth.functional_system's form (or
+    functional_system_complex's, which carries the complex spinor tensor and n_negative)."""
+    from .mo import RiMoEri, RiNonRelSpinMoEri
 
-    eri = RiNonRelSpinMoEri.from_tensor(sysd["Bmo"], sysd["ns"])
     extra = {k: sysd[k] for k in ("pair_of", "two_rdm_l1", "two_rdm_l2") if k in sysd}
+    if np.iscomplexobj(sysd["Bmo"]):
+        eri = RiMoEri.from_tensor(sysd["Bmo"], sysd["n"])
+        extra["n_negative"] = sysd.get("n_negative", 0)
+    else:
+        eri = RiNonRelSpinMoEri.from_tensor(sysd["Bmo"], sysd["ns"])
     prob = RotationProblem(eri, sysd["h"], sysd["occupations"], sysd["two_rdm_h"], sysd["two_rdm_x"],
                            options=options, **extra)
     return prob, eri

@@ -234,3 +234,39 @@ def functional_system(ns: int, naux: int, seed: int, nocc: int | None = None, wi
         out["two_rdm_l1"] = 0.01 * rng.standard_normal((d, d))
         out["two_rdm_l2"] = 0.01 * rng.standard_normal((d, d))
     return out
+
+
+def functional_system_complex(n: int, naux: int, seed: int, nocc: int | None = None, with_pairs: bool = False,
+                              n_negative: int = 0, box: float = 8.0) -> dict:
+    """Fixed-occupation functional-stage inputs for the complex spinor RI tensor (RiMoEri): the
+    cube/Gaussian recipe's tensor in a random unitary basis (every B^P Hermitian), a Hermitian h with
+    nocc low levels (not diagonal in that basis), spinor occupations (nocc near 1, the rest decaying
+    from 0.05) with two_rdm_h = n_p n_q, two_rdm_x = sqrt(n_p n_q), optionally small random pair terms,
+    and optionally n_negative leading spinors of a negative-energy branch (levels near -40, empty)."""
+    rng = np.random.default_rng(seed)
+    B = ri_tensor(n, naux, seed, box=box)
+    B *= 2.4 / max(1e-30, np.sqrt(np.abs(B).max() * np.sqrt(naux)))
+    u = random_unitary(n, rng)
+    Bmo = np.einsum("ai,Pab,bj->Pij", u.conj(), B.reshape(naux, n, n), u, optimize=True).reshape(naux, n * n)
+    npos = n - n_negative
+    nocc = max(1, npos // 4) if nocc is None else nocc
+    e = np.sort(np.concatenate([-3.0 + rng.random(nocc), 0.5 + 3 * rng.random(npos - nocc)]))
+    e = np.concatenate([-40.0 - rng.random(n_negative), e])
+    uu = random_unitary(n, rng)
+    # keep the negative branch on its own block of the spinor space so it stays separable
+    if n_negative:
+        uu[:n_negative, n_negative:] = 0.0
+        uu[n_negative:, :n_negative] = 0.0
+        uu[:n_negative, :n_negative] = random_unitary(n_negative, rng)
+        uu[n_negative:, n_negative:] = random_unitary(npos, rng)
+    h = (uu * e) @ uu.conj().T
+    h = 0.5 * (h + h.conj().T)
+    occ = np.concatenate([np.zeros(n_negative), 0.97 - 0.05 * rng.random(nocc),
+                          0.05 * np.exp(-np.arange(npos - nocc) / 2.0)])
+    out = dict(n=n, naux=naux, Bmo=Bmo, h=h, occupations=occ, two_rdm_h=np.outer(occ, occ),
+               two_rdm_x=np.sqrt(np.outer(occ, occ)), n_negative=n_negative)
+    if with_pairs:
+        out["pair_of"] = np.array([(i + 1) % n if i % 2 == 0 else i - 1 for i in range(n)])
+        out["two_rdm_l1"] = 0.01 * rng.standard_normal((n, n))
+        out["two_rdm_l2"] = 0.01 * rng.standard_normal((n, n))
+    return out

@@ -138,3 +138,54 @@ def test_setup_path_restatements():
     assert np.abs(o.canonical_orthogonalize(g["S_full_rank"], 1e-10) - g["X_full_rank"]).max() < 1e-12
     Xh = o.canonical_orthogonalize_hermitian(g["s_full"], 1e-10)
     assert np.abs(Xh @ Xh.conj().T - g["XXh"]).max() < 1e-10
+
+
+def test_complex_rotation_problem_restatement(ref_lib):
+    """The complex RotationProblem restatement against the reference's own pieces: its generalized
+    Fock and orbitalGradient give the pair gradient, its spinorRotationMatrix the rotation, its
+    Adam<complex>::step the steps of the optimiser's first iterations.  Without pair terms (random
+    l1 / l2 are not consistent with the trace form of the energy) the gradient is the derivative of
+    the energy along the real and imaginary parts of each pair's step."""
+    from rerdmft_b200 import synth
+
+    f = synth.functional_system_complex(8, 24, 11, with_pairs=True, n_negative=2)
+    args = (f["pair_of"], f["two_rdm_l1"], f["two_rdm_l2"])
+    pb = o.RotationProblemComplexNumpy(f["Bmo"], f["h"], f["occupations"], f["two_rdm_h"], f["two_rdm_x"], *args,
+                                       n_negative=2)
+    assert all(p >= 2 and q >= 2 for p, q in pb.pairs) and len(pb.pairs) == 15
+    F = ref_lib.hx_fock_complex(f["Bmo"], 8, f["h"], f["occupations"], f["two_rdm_h"], f["two_rdm_x"], *args)
+    assert np.abs(pb.fock() - F).max() <= 1e-12
+    G = ref_lib.orbital_gradient(F)
+    g = pb.gradient()
+    assert np.abs(g - np.array([G[p, q] for p, q in pb.pairs])).max() <= 1e-12
+    rng = np.random.default_rng(1)
+    step = 0.05 * (rng.standard_normal(len(pb.pairs)) + 1j * rng.standard_normal(len(pb.pairs)))
+    k = o.kappa_matrix(8, pb.pairs, step)
+    assert np.abs(o.rotation_matrix(k) - ref_lib.rotation_matrix(k)).max() <= 1e-13
+    gs = np.stack([g, 0.5 * g, -g])
+    ref_steps = ref_lib.adam_steps(gs)
+    m1, m2, mx = np.zeros_like(g), np.zeros(g.size), np.zeros(g.size)
+    for t in range(1, 4):
+        m1 = 0.7 * m1 + 0.3 * gs[t - 1]
+        m2 = 0.9 * m2 + 0.1 * (gs[t - 1].real ** 2 + gs[t - 1].imag ** 2)
+        mx = np.maximum(mx, m2 / (1 - 0.9 ** t))
+        st = -0.01 * (m1 / (1 - 0.7 ** t)) / (np.sqrt(mx) + 1e-15)
+        assert np.abs(st - ref_steps[t - 1]).max() <= 1e-15
+    f = synth.functional_system_complex(8, 24, 11, n_negative=2)
+    pb = o.RotationProblemComplexNumpy(f["Bmo"], f["h"], f["occupations"], f["two_rdm_h"], f["two_rdm_x"],
+                                       n_negative=2)
+    g = pb.gradient()
+    e0, eps = pb.energy(), 1e-6
+    for comp in (1.0, 1j):
+        d = np.zeros(len(pb.pairs), dtype=complex)
+        d[4] = eps * comp
+        pb.save_best()
+        pb.rotate(d)
+        ep = pb.energy()
+        pb.restore_best()
+        pb.rotate(-d)
+        em = pb.energy()
+        pb.restore_best()
+        want = g[4].real if comp == 1.0 else g[4].imag
+        assert abs((ep - em) / (2 * eps) - want) <= 1e-7 * max(1.0, abs(want))
+    assert abs(pb.energy() - e0) <= 1e-14
