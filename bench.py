@@ -29,9 +29,17 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 N_AO, N_AUX, N_OCC, SEED = 400, 1600, 40, 2024
-# DRAM bytes (read + write) of one half-transform launch at this workload, from the ncu capture in
-# profiles/dgemm_half_transform_n400_naux1600_nocc40.md (B read once, T written once).
-HT_TRAFFIC_BYTES = 2.048888e9 + 0.194917e9
+# The half-transform kernel of the nonrelativistic exchange (RR_HALF_TRANSFORM selects it; m16 is the
+# library default) with the DRAM bytes (read + write) of one launch at this workload from its ncu
+# capture (B read once, T written once), None where no capture exists.
+HT_KIND = os.environ.get("RR_HALF_TRANSFORM", "m16")
+HT_KERNELS = {
+    "m8": dict(kernel="dgemm_kernel half-transform T^P = Ct B^P (FP64 DMMA m8n8k4)",
+               traffic=2.048888e9 + 0.194917e9, profile="profiles/dgemm_half_transform_n400_naux1600_nocc40.md"),
+    "m16": dict(kernel="ht_dmma16_kernel half-transform T^P = Ct B^P (FP64 DMMA m16n8k8)", traffic=None,
+                profile="profiles/ht_dmma16_half_transform_n400_naux1600_nocc40.md"),
+}
+HT = HT_KERNELS[HT_KIND]
 METRIC = "RI J+K Fock builds/s"
 UNIT = "builds/s"
 
@@ -854,11 +862,11 @@ def main():
         ms_per_step=1e3 * t / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
         data="synthetic",
         config=bench_config(ws),
-        roofline={"bound": "tensor", "kernel": "dgemm_kernel half-transform T^P = Ct B^P (FP64 DMMA, 45% of a build)",
+        roofline={"bound": "tensor", "kernel": HT["kernel"],
                   "achieved": ht_tf, "peak": fp64_peak, "unit": "TFLOP/s",
-                  "frac": (ht_tf / fp64_peak) if (ht_tf and fp64_peak) else None, "traffic": HT_TRAFFIC_BYTES,
-                  "traffic_source": "dram read+write of one launch, ncu capture in "
-                                    "profiles/dgemm_half_transform_n400_naux1600_nocc40.md",
+                  "frac": (ht_tf / fp64_peak) if (ht_tf and fp64_peak) else None, "traffic": HT["traffic"],
+                  "traffic_source": ("dram read+write of one launch, ncu capture in " + HT["profile"])
+                  if HT["traffic"] else "no ncu capture of this kernel yet",
                   "algorithmic_bytes": 8.0 * N_AUX * (N_AO * N_AO + N_OCC * N_AO),
                   "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 has no entry in MEASURED_PEAKS.json)",
                   "algorithmic": "2*naux*nocc*n^2 flops per launch (one launch per build)"},

@@ -63,7 +63,7 @@ int64_t gemm_work_doubles(const GemmDesc& d);
 bool half_transform_m16(const double* Ct, int64_t nocc, const double* B, int64_t pitch, int64_t naux, int64_t n,
                         double* T, cudaStream_t s);
 // Which half-transform the nonrelativistic exchange uses: 0 = the general DMMA GEMM (m8n8k4),
-// 1 = half_transform_m16.  RR_HALF_TRANSFORM=m8|m16 overrides the default.
+// 1 = half_transform_m16 (the default).  RR_HALF_TRANSFORM=m8|m16 overrides the default.
 int half_transform_kind();
 
 }  // namespace rr
