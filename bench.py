@@ -288,11 +288,10 @@ def orbital_optimization_block():
     return out
 
 
-def x2c_batch_block(want_cpu: bool, count: int = 64, workers: int = 16):
-    """Batched X2C-HF geometry scan: `count` instances with uneven nl in [20, 120] (seeded), naux = 4 nl,
-    4 or 14 electrons (LiH- / CO-like) alternating, each converged to 1e-8 Ha; one handle per
-    instance, run one after another (workers = 1) and concurrently (rr_scf_run_x2c_batch)."""
-    from rerdmft_b200 import ri, scf, synth
+def x2c_batch_problems(count: int = 64):
+    """The batched X2C-HF geometry scan: `count` instances with uneven nl in [20, 120] (seeded), naux = 4 nl,
+    4 or 14 electrons (LiH- / CO-like) alternating, one handle each (uploaded here)."""
+    from rerdmft_b200 import ri, synth
 
     rng = np.random.default_rng(SEED + 44)
     sizes = rng.integers(20, 121, size=count)
@@ -304,6 +303,17 @@ def x2c_batch_block(want_cpu: bool, count: int = 64, workers: int = 16):
         systems.append(sysd)
         probs.append(dict(eri=src, h_x2c=sysd["h"], x_large=sysd["X"], initial_density=sysd["P0"],
                           n_electrons=sysd["n_electrons"]))
+    return sizes, probs, systems
+
+
+def x2c_batch_block(want_cpu: bool, count: int = 64, workers: int = 16):
+    """Batched X2C-HF geometry scan (x2c_batch_problems), each instance converged to 1e-8 Ha: one after
+    another (workers = 1), concurrently on host threads (rr_scf_run_x2c_batch), and in lockstep as one
+    grouped program (rr_scf_run_x2c_grouped: one grouped launch per phase per iteration for all instances,
+    autotuned tiles; the first run tunes the shapes, the timed run uses the cache)."""
+    from rerdmft_b200 import scf
+
+    sizes, probs, systems = x2c_batch_problems(count)
     scf.runX2CHartreeFockScfBatch(probs, workers=workers)  # warm-up: every handle's first-call allocations
     t0 = time.perf_counter()
     seq = scf.runX2CHartreeFockScfBatch(probs, workers=1)
@@ -311,12 +321,29 @@ def x2c_batch_block(want_cpu: bool, count: int = 64, workers: int = 16):
     t0 = time.perf_counter()
     par = scf.runX2CHartreeFockScfBatch(probs, workers=workers)
     t_par = time.perf_counter() - t0
+    tune = {}
+    scf.runX2CHartreeFockScfBatch(probs, mode="grouped", stats=tune)  # tunes every new shape
+    st = {}
+    t0 = time.perf_counter()
+    grp = scf.runX2CHartreeFockScfBatch(probs, mode="grouped", stats=st)
+    t_grp = time.perf_counter() - t0
     out = dict(workload=f"{count} X2C-HF instances, nl in [20, 120] (uneven), naux = 4 nl, 4 / 14 electrons, FP64",
                seconds_one_after_another=t_seq, seconds_concurrent=t_par, workers=workers,
                instances_per_s=count / t_par, converged=int(sum(r["converged"] for r in par)),
                iterations_total=int(sum(r["iterations"] for r in par)),
                max_energy_difference_sequential_vs_concurrent=float(max(abs(a["energy"] - b["energy"])
-                                                                      for a, b in zip(seq, par))))
+                                                                      for a, b in zip(seq, par))),
+               grouped=dict(seconds=t_grp, instances_per_s=count / t_grp,
+                            converged=int(sum(r["converged"] for r in grp)),
+                            lockstep_iterations=st["iterations"], launches_total=st["launches_total"],
+                            launches_setup=st["launches_setup"],
+                            launches_max_iteration=st["launches_max_iteration"],
+                            instances_first_iteration_grouped=st["grouped_instances_first"],
+                            max_energy_difference_vs_concurrent=float(max(abs(a["energy"] - b["energy"])
+                                                                          for a, b in zip(grp, par))),
+                            autotune=dict(seconds_first_run=tune["autotune_seconds"],
+                                          shapes_cached=st["autotune_entries"],
+                                          seconds_timed_run=st["autotune_seconds"])))
     if want_cpu:
         from oracle import ref
 
@@ -616,7 +643,8 @@ def run_case(args):
                   full then incremental (nl=200, ns=600, naux=1000, 40 spinors);
     rkb_fp64      the same 4c RKB Fock build in FP64 (the 4c Fock-build workload of the bench line);
     x2c_mixed     the X2C Fock build with the split-BF16 exchange, full then incremental (nl=200,
-                  naux=1000, 80 electrons)."""
+                  naux=1000, 80 electrons);
+    x2c_batch     the lockstep grouped X2C-HF scan (64 uneven instances), tuned then timed once."""
     import ctypes
 
     import torch
@@ -641,6 +669,20 @@ def run_case(args):
         return e0.elapsed_time(e1) / steps
 
     out = dict(case=args.case, steps=args.steps, warmup=args.warmup)
+    if args.case == "x2c_batch":
+        from rerdmft_b200 import scf
+
+        _, probs, _ = x2c_batch_problems()
+        tune, st = {}, {}
+        scf.runX2CHartreeFockScfBatch(probs, mode="grouped", stats=tune)
+        t0 = time.perf_counter()
+        res = scf.runX2CHartreeFockScfBatch(probs, mode="grouped", stats=st)
+        out.update(workload="64 X2C-HF instances, grouped lockstep", seconds=time.perf_counter() - t0,
+                   converged=int(sum(r["converged"] for r in res)), stats=st, tuning_run=tune)
+        for p in probs:
+            p["eri"].store.close()
+        print(json.dumps(out))
+        return
     if args.case in ("headline", "mixed_exchange"):
         inp = make_inputs()
         dev = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in inp.items()}
@@ -718,7 +760,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", default=None, choices=["headline", "mixed_exchange", "rkb_mixed", "rkb_fp64", "x2c_mixed"],
+    ap.add_argument("--case", default=None, choices=["headline", "mixed_exchange", "rkb_mixed", "rkb_fp64", "x2c_mixed",
+                                                    "x2c_batch"],
                     help="run one workload for profiling instead of the bench line")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)

@@ -376,6 +376,37 @@ typedef struct rr_x2c_instance {
  * instance's code (all instances run; each reports its own status). */
 int rr_scf_run_x2c_batch(rr_x2c_instance* instances, int64_t count, const rr_scf_opts* scf, int32_t workers);
 
+/* The same batch in lockstep on one stream (the config-4 geometry scan as one grouped program):
+ * every phase of an SCF iteration runs for all instances still iterating in one grouped launch
+ * (persistent grouped FP64 DMMA GEMMs whose tile shapes and split-K counts come from the library's
+ * autotuner, and grouped elementwise / reduction kernels), so the number of kernel launches per
+ * iteration does not grow with the number of instances.  The first iteration takes the occupied
+ * spinors from the caller's density in the same grouped form when that density is an idempotent
+ * projector of the instance's n_electrons spinors, else by the single-instance recovery.  SP2 runs
+ * from Gershgorin bounds.  FP64 only (RR_PREC_MIXED: RR_ERR_UNSUPPORTED); DIIS or linear mixing as
+ * scf says.  Each instance's result does not depend on which other instances share the batch.  Host
+ * pointers.  stats (optional) receives the batch's launch counts and times. */
+typedef struct rr_batch_stats {
+  int64_t iterations;             /* lockstep iterations (the largest instance count) */
+  int64_t launches_total;         /* kernels launched by the call (autotuning excluded) */
+  int64_t launches_setup;         /* of which before the first iteration's Fock build */
+  int64_t launches_max_iteration; /* the most launched in one iteration */
+  int64_t grouped_instances_first;/* instances whose first iteration ran grouped */
+  double seconds;                 /* wall time of the call */
+  double autotune_seconds;        /* of which spent timing new GEMM shapes */
+  int64_t autotune_entries;       /* shapes in the autotuner cache afterwards */
+} rr_batch_stats;
+
+int rr_scf_run_x2c_grouped(rr_x2c_instance* instances, int64_t count, const rr_scf_opts* scf, rr_batch_stats* stats);
+
+/* The grouped GEMM autotuner's cache: one line per problem shape ("<key> <configuration> <splits>
+ * <microseconds per problem>").  The first tuning loads the file named by RR_AUTOTUNE_CACHE when that
+ * variable is set, and rr_scf_run_x2c_grouped saves new entries there. */
+int rr_autotune_load(const char* path);
+int rr_autotune_save(const char* path);
+int rr_autotune_clear(void);
+int64_t rr_autotune_entries(void);
+
 /* ---------------- RESTART files and the hand-over between runs of a scan ----------------
  * The reference's binary RESTART format (src/Utils/Restart.h:14-70), byte for byte: a file written by
  * rr_restart_write is read by the reference's readRestart and the other way round.  Strings are

@@ -88,6 +88,16 @@ class Restart(ctypes.Structure):
                 ("cas_state", _vp), ("n_cas_state", _i64)]
 
 
+class BatchStats(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int64), ("launches_total", ctypes.c_int64),
+                ("launches_setup", ctypes.c_int64), ("launches_max_iteration", ctypes.c_int64),
+                ("grouped_instances_first", ctypes.c_int64), ("seconds", ctypes.c_double),
+                ("autotune_seconds", ctypes.c_double), ("autotune_entries", ctypes.c_int64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class X2cInstance(ctypes.Structure):
     _fields_ = [("h", _vp), ("h_x2c", _vp), ("X", _vp), ("n_eff", _i64), ("S", _vp), ("P0", _vp),
                 ("n_electrons", _i32), ("status", _i32), ("P_out", _vp), ("energy_history", _vp),
@@ -96,6 +106,12 @@ class X2cInstance(ctypes.Structure):
 
 _SIGS = {
     "rr_scf_run_x2c_batch": (ctypes.c_int, [ctypes.POINTER(X2cInstance), _i64, ctypes.POINTER(ScfOpts), _i32]),
+    "rr_scf_run_x2c_grouped": (ctypes.c_int, [ctypes.POINTER(X2cInstance), _i64, ctypes.POINTER(ScfOpts),
+                                              ctypes.POINTER(BatchStats)]),
+    "rr_autotune_load": (ctypes.c_int, [ctypes.c_char_p]),
+    "rr_autotune_save": (ctypes.c_int, [ctypes.c_char_p]),
+    "rr_autotune_clear": (ctypes.c_int, []),
+    "rr_autotune_entries": (_i64, []),
     "rr_adam_default_options": (ctypes.c_int, [ctypes.POINTER(AdamOptions)]),
     "rr_orbopt_create": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(AdamOptions),
                                         ctypes.POINTER(_vp)]),

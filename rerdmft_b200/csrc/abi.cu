@@ -6,6 +6,7 @@
 #include <thread>
 #include <vector>
 
+#include "grouped.cuh"
 #include "mo_store.cuh"
 
 namespace rr {
@@ -21,6 +22,7 @@ void fock_rkb(rr_ri_store*, const double*, const double*, int64_t, const double*
               int64_t = 0);
 void scf_nonrel(rr_ri_store*, const double*, const double*, int64_t, const double*, const double*, int,
                 const rr_scf_opts*, rr_scf_result*, double*, double*, const rr_opts*);
+void scf_x2c_grouped(rr_x2c_instance*, int64_t, const rr_scf_opts*, rr_batch_stats*);
 void scf_rel(rr_ri_store*, int, const double*, const double*, int64_t, const double*, int64_t, const double*,
              const double*, int, const rr_scf_opts*, rr_scf_result*, double*, double*, const rr_opts*);
 }  // namespace rr
@@ -300,6 +302,42 @@ int rr_scf_run_x2c(rr_ri_handle h, const double* h_x2c, const double* X, int64_t
                 opts);
   });
 }
+
+int rr_scf_run_x2c_grouped(rr_x2c_instance* instances, int64_t count, const rr_scf_opts* scf, rr_batch_stats* stats) {
+  return api([&] {
+    RR_REQUIRE(count >= 0 && (instances || count == 0) && scf, RR_ERR_ARG, "rr_scf_run_x2c_grouped: null argument");
+    if (stats) *stats = rr_batch_stats{};
+    if (count == 0) return;
+    RR_CUDA(cudaSetDevice(instances[0].h ? instances[0].h->ctx.device : 0));
+    for (int64_t i = 0; i < count; ++i)
+      RR_REQUIRE(!instances[i].h || instances[i].h->ctx.device == instances[0].h->ctx.device, RR_ERR_ARG,
+                 "rr_scf_run_x2c_grouped: every handle must live on one device");
+    rr::scf_x2c_grouped(instances, count, scf, stats);
+    for (int64_t i = 0; i < count; ++i)
+      if (instances[i].status != RR_OK)
+        throw rr::Error(instances[i].status, "rr_scf_run_x2c_grouped: instance " + std::to_string(i) + " failed");
+  });
+}
+
+int rr_autotune_load(const char* path) {
+  return api([&] {
+    RR_REQUIRE(path, RR_ERR_ARG, "rr_autotune_load: null path");
+    rr::autotune_load(path);
+  });
+}
+
+int rr_autotune_save(const char* path) {
+  return api([&] {
+    RR_REQUIRE(path, RR_ERR_ARG, "rr_autotune_save: null path");
+    rr::autotune_save(path);
+  });
+}
+
+int rr_autotune_clear(void) {
+  return api([&] { rr::autotune_clear(); });
+}
+
+int64_t rr_autotune_entries(void) { return rr::autotune_entries(); }
 
 int rr_scf_run_x2c_batch(rr_x2c_instance* instances, int64_t count, const rr_scf_opts* scf, int32_t workers) {
   return api([&] {

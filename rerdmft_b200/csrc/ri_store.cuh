@@ -114,6 +114,13 @@ int64_t launches();
 void sp2_projector(rr_ri_store* h, const double* F, int64_t n, int64_t nocc, double* Pi, double* T, double* scal,
                    cudaStream_t s, bool cplx = false);
 void check_status(rr_ri_store* h, cudaStream_t s);  // syncs s, throws RR_ERR_TIMEOUT on a set word
+// The DIIS bordered solve of the SCF loops (Gaussian elimination with partial pivoting; false when
+// min |pivot| / max |pivot| is not above tol).
+bool diis_solve(const std::vector<double>& m, const std::vector<double>& rhs, size_t n, double tol,
+                std::vector<double>& x);
+// Orbital energies, C and F of an SCF loop's last iteration into the result's output pointers.
+void scf_result_outputs(rr_ri_store* h, const double* F, const double* Xd, int64_t n, int64_t n_eff, bool cplx,
+                        const rr_scf_result* res, bool host, cudaStream_t s);
 // Waits on the host for everything queued on s (see rr_ri_store::blocking_wait).
 void host_wait(rr_ri_store* h, cudaStream_t s);
 void copy_in(double* dst, const double* src, int64_t count, bool host, cudaStream_t s);

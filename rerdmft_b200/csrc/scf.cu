@@ -489,6 +489,11 @@ __global__ void ritz_bounds_kernel(const double* w, int k, const int* info, doub
 
 }  // namespace
 
+bool diis_solve(const std::vector<double>& m, const std::vector<double>& rhs, size_t n, double tol,
+                std::vector<double>& x) {
+  return solve_dense(m, rhs, n, tol, x);
+}
+
 // Narrows the SP2 spectral interval b (device, [lo, hi], Gershgorin on entry) of the Hermitian n x n
 // F with the Ritz values of F on the block Krylov space [V, F V, F^2 V, F^3 V] (V: 8 fixed
 // pseudo-random vectors), widened by 10% of their spread: a generalized 32 x 32 eigenproblem

@@ -128,13 +128,15 @@ def runDiracHartreeFockScf(h_rkb, eri: RiDirectEriSource, x_full, initial_densit
 def runX2CHartreeFockScfBatch(problems, workers: int = 16, diis_size: int = 5, max_iterations: int = 100,
                               energy_tolerance: float = 1e-8, density_tolerance: float = 1e-6,
                               kramers_restricted: bool = True, precision: str = "fp64",
-                              mixed_switch: float = 0.0) -> list:
-    """A batch of independent X2C-HF problems (a geometry scan of uneven sizes) run concurrently
-    (rr_scf_run_x2c_batch: `workers` host threads take the problems largest store first, one stream
-    per problem's handle; with more than one worker the host waits sleep instead of spinning).  Each
-    problem is a dict with eri (RiX2cEriSource), h_x2c, x_large, initial_density, n_electrons and
-    optionally overlap; each needs its own handle.  Returns one result dict per problem, as
-    runX2CHartreeFockScf."""
+                              mixed_switch: float = 0.0, mode: str = "threads", stats: dict | None = None) -> list:
+    """A batch of independent X2C-HF problems (a geometry scan of uneven sizes).  Each problem is a dict
+    with eri (RiX2cEriSource), h_x2c, x_large, initial_density, n_electrons and optionally overlap; each
+    needs its own handle.  Returns one result dict per problem, as runX2CHartreeFockScf.
+
+    mode "threads": rr_scf_run_x2c_batch, `workers` host threads taking the problems largest store first,
+    one stream per problem's handle.  mode "grouped": rr_scf_run_x2c_grouped, all problems in lockstep
+    on one stream, every phase of an iteration one grouped launch for all of them (FP64 only); `stats`
+    (a dict) receives its launch counts and times."""
     keep, insts = [], (L.X2cInstance * len(problems))()
     outs = []
     for i, pr in enumerate(problems):
@@ -154,5 +156,25 @@ def runX2CHartreeFockScfBatch(problems, workers: int = 16, diis_size: int = 5, m
                                  int(pr["n_electrons"]), 0, _ptr(P), _ptr(hist), L.ScfResult())
     so = _opts(diis_size, max_iterations, energy_tolerance, density_tolerance, precision, mixed_switch,
                kramers_restricted, 1.0)
-    L.check(L.lib().rr_scf_run_x2c_batch(insts, len(problems), ctypes.byref(so), workers))
+    if mode == "grouped":
+        st = L.BatchStats()
+        L.check(L.lib().rr_scf_run_x2c_grouped(insts, len(problems), ctypes.byref(so), ctypes.byref(st)))
+        if stats is not None:
+            stats.update(st.as_dict())
+    elif mode == "threads":
+        L.check(L.lib().rr_scf_run_x2c_batch(insts, len(problems), ctypes.byref(so), workers))
+    else:
+        raise RrError(L.RR_ERR_ARG, "runX2CHartreeFockScfBatch: mode is 'threads' or 'grouped'")
     return [_result(insts[i].result, P, hist) for i, (P, hist) in enumerate(outs)]
+
+
+def autotune_cache(load: str | None = None, save: str | None = None, clear: bool = False) -> int:
+    """The grouped GEMM autotuner's cache (rr_autotune_*): optionally clear it, load a cache file, save
+    it to a file; returns the number of tuned shapes."""
+    if clear:
+        L.check(L.lib().rr_autotune_clear())
+    if load is not None:
+        L.check(L.lib().rr_autotune_load(str(load).encode()))
+    if save is not None:
+        L.check(L.lib().rr_autotune_save(str(save).encode()))
+    return int(L.lib().rr_autotune_entries())
