@@ -198,6 +198,7 @@ _SIGS = {
     "rr_test_j_passes_packed": (ctypes.c_int, [_vp, _i64, _i64, _vp, _vp, _vp, _vp]),
     "rr_test_device_allocations": (ctypes.c_int64, []),
     "rr_test_half_transform": (ctypes.c_int, [_vp, _i64, _vp, _i64, _i64, _vp, _i32]),
+    "rr_test_half_transform_time": (ctypes.c_int, [_vp, _i64, _vp, _i64, _i64, _vp, _i32, _i32, _vp]),
     "rr_test_wait_expiry": (ctypes.c_int, [ctypes.c_uint32, _i32, ctypes.POINTER(_i32), ctypes.POINTER(_d),
                                            ctypes.POINTER(_d)]),
 }

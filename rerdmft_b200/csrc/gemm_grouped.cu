@@ -413,6 +413,7 @@ void TableRing::reset() {
 }
 
 const void* TableRing::put(const void* src, size_t bytes, cudaStream_t s) {
+  RR_REQUIRE(src && bytes > 0, RR_ERR_ARG, "TableRing::put: empty table");
   const size_t need = (bytes + 15) & ~size_t{15};
   if (cap == 0) reserve(std::max<size_t>(size_t{4} << 20, 2 * need));
   else if (used + need > cap) reserve(std::max(2 * cap, 2 * need));

@@ -3,11 +3,11 @@
 //
 // The product is computed transposed, T[P]^T = B^P^T Ct^T: its M is the AO count n (16-row fragments
 // cover any n that is a multiple of 16 without padding, unlike the occupied count), N = nocc (8-column
-// fragments), K = n.  A CTA owns an 80 x 40 block of T[P]^T (five warps of 16 x 40: one A fragment and five
-// B fragments per k8 step) and stores it transposed into T[P] (nocc x n, row-major, the layout the
-// exchange SYRK reads).  A 3-stage cp.async ring stages 16-deep k tiles of B^P (rows k, AO columns
-// contiguous) and of Ct; the shared-memory pitches are 4 (mod 16) doubles, so the fragment loads of a
-// half-warp touch 16 distinct 8-byte bank pairs.
+// fragments), K = n.  The default CTA owns an 80 x 40 block of T[P]^T (five warps of 16 x 40: one A
+// fragment and five B fragments per k8 step) and stores it transposed into T[P] (nocc x n, row-major,
+// the layout the exchange SYRK reads).  A 3-stage cp.async ring stages 16-deep k tiles of B^P (rows k,
+// AO columns contiguous) and of Ct.  Other warp counts, k depths and ring depths are instantiated for
+// measurement (half_transform_m16's config).
 #include <algorithm>
 #include <cstdlib>
 #include <string>
@@ -16,12 +16,6 @@
 
 namespace rr {
 namespace {
-
-constexpr int HT_BM = 80, HT_BN = 40, HT_KT = 16, HT_STAGES = 3, HT_THREADS = 160;
-constexpr int HT_LDA = HT_BM + 4;  // sA[k][m]: 84 = 4 (mod 16), even (16-byte cp.async destinations)
-constexpr int HT_LDB = HT_KT + 4;  // sB[n][k]: 20 = 4 (mod 16)
-constexpr int HT_SA = HT_KT * HT_LDA, HT_SB = HT_BN * HT_LDB, HT_STAGE = HT_SA + HT_SB;
-constexpr int HT_SMEM = HT_STAGES * HT_STAGE * 8;
 
 __device__ __forceinline__ void cp16(uint32_t saddr, const void* g, int bytes) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(saddr), "l"(g), "r"(bytes));
@@ -48,36 +42,52 @@ struct HtArgs {
   int64_t n, nocc, pitch, p0;
 };
 
-__global__ void __launch_bounds__(HT_THREADS) ht_dmma16_kernel(const HtArgs a) {
+// WARPS warps per CTA, each a 16-row slice of the CTA's BM = 16 WARPS AO columns times 40 occupied
+// rows; KT-deep k tiles in a STAGES-deep ring.  Shared-memory pitches are 4 (mod 16) doubles, so the
+// fragment loads of a half-warp touch 16 distinct 8-byte bank pairs.
+template <int WARPS, int KT, int STAGES>
+struct HtCfg {
+  static constexpr int BM = 16 * WARPS, BN = 40, THREADS = 32 * WARPS;
+  static constexpr int LDA = BM + 4;  // sA[k][m]
+  static constexpr int LDB = KT + 4;  // sB[n][k]
+  static constexpr int SA = KT * LDA, SB = BN * LDB, STAGE = SA + SB;
+  static constexpr int SMEM = STAGES * STAGE * 8;
+  static_assert(LDA % 16 == 4 && LDB % 16 == 4, "pitches must be 4 (mod 16)");
+};
+
+template <int WARPS, int KT, int STAGES>
+__global__ void __launch_bounds__(32 * WARPS) ht_dmma16_kernel(const HtArgs a) {
+  using CF = HtCfg<WARPS, KT, STAGES>;
+  constexpr int BM = CF::BM, BN = CF::BN, THREADS = CF::THREADS, LDA = CF::LDA, LDB = CF::LDB;
   extern __shared__ __align__(16) double smem[];
-  const int64_t j0 = static_cast<int64_t>(blockIdx.x) * HT_BM;  // AO columns of B^P (rows of T^T)
-  const int64_t i0 = static_cast<int64_t>(blockIdx.y) * HT_BN;  // occupied rows of T
+  const int64_t j0 = static_cast<int64_t>(blockIdx.x) * BM;  // AO columns of B^P (rows of T^T)
+  const int64_t i0 = static_cast<int64_t>(blockIdx.y) * BN;  // occupied rows of T
   const int64_t P = a.p0 + blockIdx.z;
   const double* Bp = a.B + P * a.pitch;
   const int64_t n = a.n;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t = lane & 3;
   const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
-  const int ktiles = static_cast<int>((n + HT_KT - 1) / HT_KT);
+  const int ktiles = static_cast<int>((n + KT - 1) / KT);
 
   auto load = [&](int stage, int kt) {
-    const int64_t k0 = static_cast<int64_t>(kt) * HT_KT;
-    const uint32_t sa = sbase + static_cast<uint32_t>(stage * HT_STAGE * 8);
-    const uint32_t sb = sa + HT_SA * 8;
-    // B^P rows k0..k0+15, AO columns j0..j0+79: 640 16-byte chunks (two doubles each)
+    const int64_t k0 = static_cast<int64_t>(kt) * KT;
+    const uint32_t sa = sbase + static_cast<uint32_t>(stage * CF::STAGE * 8);
+    const uint32_t sb = sa + CF::SA * 8;
+    // B^P rows k0 .. k0+KT-1, AO columns j0 .. j0+BM-1 (16-byte chunks of two doubles)
 #pragma unroll
-    for (int e = tid; e < HT_KT * HT_BM / 2; e += HT_THREADS) {
-      const int r = e / (HT_BM / 2), c = 2 * (e % (HT_BM / 2));
+    for (int e = tid; e < KT * BM / 2; e += THREADS) {
+      const int r = e / (BM / 2), c = 2 * (e % (BM / 2));
       const int64_t k = k0 + r, j = j0 + c;
       const int nvalid = k < n ? static_cast<int>(max(int64_t(0), min(int64_t(2), n - j))) : 0;
-      cp16(sa + static_cast<uint32_t>((r * HT_LDA + c) * 8), nvalid ? Bp + k * n + j : Bp, nvalid * 8);
+      cp16(sa + static_cast<uint32_t>((r * LDA + c) * 8), nvalid ? Bp + k * n + j : Bp, nvalid * 8);
     }
-    // Ct rows i0..i0+39, columns k0..k0+15: 320 chunks
+    // Ct rows i0 .. i0+39, columns k0 .. k0+KT-1
 #pragma unroll
-    for (int e = tid; e < HT_BN * HT_KT / 2; e += HT_THREADS) {
-      const int r = e / (HT_KT / 2), c = 2 * (e % (HT_KT / 2));
+    for (int e = tid; e < BN * KT / 2; e += THREADS) {
+      const int r = e / (KT / 2), c = 2 * (e % (KT / 2));
       const int64_t i = i0 + r, k = k0 + c;
       const int nvalid = i < a.nocc ? static_cast<int>(max(int64_t(0), min(int64_t(2), n - k))) : 0;
-      cp16(sb + static_cast<uint32_t>((r * HT_LDB + c) * 8), nvalid ? a.Ct + i * n + k : a.Ct, nvalid * 8);
+      cp16(sb + static_cast<uint32_t>((r * LDB + c) * 8), nvalid ? a.Ct + i * n + k : a.Ct, nvalid * 8);
     }
   };
 
@@ -88,29 +98,29 @@ __global__ void __launch_bounds__(HT_THREADS) ht_dmma16_kernel(const HtArgs a) {
     for (int q = 0; q < 4; ++q) acc[jb][q] = 0.0;
 
 #pragma unroll
-  for (int s = 0; s < HT_STAGES - 1; ++s) {
+  for (int s = 0; s < STAGES - 1; ++s) {
     if (s < ktiles) load(s, s);
     cp_commit();
   }
   const int m = warp * 16 + g;  // this lane's A rows m and m + 8 within the tile
   for (int kt = 0; kt < ktiles; ++kt) {
-    cp_wait<HT_STAGES - 2>();
+    cp_wait<STAGES - 2>();
     __syncthreads();
-    const double* sA = smem + (kt % HT_STAGES) * HT_STAGE;
-    const double* sB = sA + HT_SA;
+    const double* sA = smem + (kt % STAGES) * CF::STAGE;
+    const double* sB = sA + CF::SA;
 #pragma unroll
-    for (int ks = 0; ks < HT_KT / 8; ++ks) {
+    for (int ks = 0; ks < KT / 8; ++ks) {
       const int k = ks * 8 + t;
-      const double a0 = sA[k * HT_LDA + m], a1 = sA[k * HT_LDA + m + 8];
-      const double a2 = sA[(k + 4) * HT_LDA + m], a3 = sA[(k + 4) * HT_LDA + m + 8];
+      const double a0 = sA[k * LDA + m], a1 = sA[k * LDA + m + 8];
+      const double a2 = sA[(k + 4) * LDA + m], a3 = sA[(k + 4) * LDA + m + 8];
 #pragma unroll
       for (int jb = 0; jb < 5; ++jb) {
-        const double b0 = sB[(jb * 8 + g) * HT_LDB + k], b1 = sB[(jb * 8 + g) * HT_LDB + k + 4];
+        const double b0 = sB[(jb * 8 + g) * LDB + k], b1 = sB[(jb * 8 + g) * LDB + k + 4];
         dmma16(acc[jb], a0, a1, a2, a3, b0, b1);
       }
     }
-    const int nk = kt + HT_STAGES - 1;
-    if (nk < ktiles) load(nk % HT_STAGES, nk);
+    const int nk = kt + STAGES - 1;
+    if (nk < ktiles) load(nk % STAGES, nk);
     cp_commit();
   }
   cp_wait<0>();
@@ -126,26 +136,42 @@ __global__ void __launch_bounds__(HT_THREADS) ht_dmma16_kernel(const HtArgs a) {
     }
 }
 
-}  // namespace
-
-bool half_transform_m16(const double* Ct, int64_t nocc, const double* B, int64_t pitch, int64_t naux, int64_t n,
-                        double* T, cudaStream_t s) {
-  // 16-byte cp.async sources: even n and pitch, 16-byte aligned bases
-  auto al = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
-  if (n % 2 != 0 || pitch % 2 != 0 || !al(Ct) || !al(B) || nocc <= 0 || n <= 0) return false;
+template <int WARPS, int KT, int STAGES>
+void launch_ht(const HtArgs& base, int64_t naux, cudaStream_t s) {
+  using CF = HtCfg<WARPS, KT, STAGES>;
+  auto kern = ht_dmma16_kernel<WARPS, KT, STAGES>;
   static std::atomic<bool> attr[kMaxDevices];
-  once_per_device(attr, [] {
-    RR_CUDA(cudaFuncSetAttribute(ht_dmma16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, HT_SMEM));
-    RR_CUDA(cudaFuncSetAttribute(ht_dmma16_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 cudaSharedmemCarveoutMaxShared));
+  once_per_device(attr, [&] {
+    RR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, CF::SMEM));
+    RR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
   });
   for (int64_t p0 = 0; p0 < naux; p0 += 65535) {
     const int64_t cnt = std::min<int64_t>(65535, naux - p0);
-    HtArgs a{Ct, B, T, n, nocc, pitch, p0};
-    dim3 grid(static_cast<unsigned>((n + HT_BM - 1) / HT_BM), static_cast<unsigned>((nocc + HT_BN - 1) / HT_BN),
+    HtArgs a = base;
+    a.p0 = p0;
+    dim3 grid(static_cast<unsigned>((a.n + CF::BM - 1) / CF::BM), static_cast<unsigned>((a.nocc + CF::BN - 1) / CF::BN),
               static_cast<unsigned>(cnt));
-    ht_dmma16_kernel<<<grid, HT_THREADS, HT_SMEM, s>>>(a);
+    kern<<<grid, CF::THREADS, CF::SMEM, s>>>(a);
     RR_LAUNCH_CHECK();
+  }
+}
+
+}  // namespace
+
+bool half_transform_m16(const double* Ct, int64_t nocc, const double* B, int64_t pitch, int64_t naux, int64_t n,
+                        double* T, cudaStream_t s, int config) {
+  // 16-byte cp.async sources: even n and pitch, 16-byte aligned bases
+  auto al = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
+  if (n % 2 != 0 || pitch % 2 != 0 || !al(Ct) || !al(B) || nocc <= 0 || n <= 0) return false;
+  HtArgs a{Ct, B, T, n, nocc, pitch, 0};
+  switch (config) {
+    case 1: launch_ht<1, 16, 4>(a, naux, s); break;
+    case 2: launch_ht<2, 16, 4>(a, naux, s); break;
+    case 3: launch_ht<5, 32, 2>(a, naux, s); break;
+    case 4: launch_ht<4, 16, 3>(a, naux, s); break;
+    case 5: launch_ht<1, 32, 3>(a, naux, s); break;
+    case 6: launch_ht<2, 32, 3>(a, naux, s); break;
+    default: launch_ht<5, 16, 3>(a, naux, s); break;
   }
   return true;
 }

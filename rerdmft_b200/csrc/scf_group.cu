@@ -496,8 +496,10 @@ struct Batch {
     for (size_t i = 0; i < gs.size(); ++i) t[i] = gs[i].d;
     return static_cast<const GDev*>(ring.put(t.data(), sizeof(GDev) * t.size(), s));
   }
+  // (nullptr for an empty list: nothing is launched over it)
   const int* upload_list(const std::vector<int>& a) {
-    return static_cast<const int*>(ring.put(a.data(), sizeof(int) * std::max<size_t>(a.size(), 1), s));
+    if (a.empty()) return nullptr;
+    return static_cast<const int*>(ring.put(a.data(), sizeof(int) * a.size(), s));
   }
   int64_t max_over(const std::vector<int>& a, int64_t (*f)(const GDev&)) const {
     int64_t m = 1;

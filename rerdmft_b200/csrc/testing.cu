@@ -52,9 +52,9 @@ int rr_test_half_transform(const double* Ct, int64_t nocc, const double* B, int6
                            int32_t variant) {
   try {
     rr::set_last_error("");
-    RR_REQUIRE(variant == 0 || variant == 1, RR_ERR_ARG, "rr_test_half_transform: variant must be 0 or 1");
-    if (variant == 1) {
-      RR_REQUIRE(rr::half_transform_m16(Ct, nocc, B, n * n, naux, n, T, nullptr), RR_ERR_UNSUPPORTED,
+    RR_REQUIRE(variant >= 0 && variant <= 7, RR_ERR_ARG, "rr_test_half_transform: variant must be in [0, 7]");
+    if (variant >= 1) {
+      RR_REQUIRE(rr::half_transform_m16(Ct, nocc, B, n * n, naux, n, T, nullptr, variant - 1), RR_ERR_UNSUPPORTED,
                  "rr_test_half_transform: operands not supported by the m16n8k8 kernel");
     } else {
       rr::GemmDesc g;
@@ -66,6 +66,45 @@ int rr_test_half_transform(const double* Ct, int64_t nocc, const double* B, int6
       rr::gemm(g, nullptr);
     }
     RR_CUDA(cudaDeviceSynchronize());
+    return RR_OK;
+  } catch (const rr::Error& e) {
+    rr::set_last_error(e.what());
+    return e.code;
+  } catch (const std::exception& e) {
+    rr::set_last_error(e.what());
+    return RR_ERR_CUDA;
+  }
+}
+
+int rr_test_half_transform_time(const double* Ct, int64_t nocc, const double* B, int64_t naux, int64_t n, double* T,
+                                int32_t variant, int32_t reps, double* ms) {
+  try {
+    rr::set_last_error("");
+    RR_REQUIRE(reps >= 1 && ms, RR_ERR_ARG, "rr_test_half_transform_time: reps >= 1 and an output are needed");
+    const int rc = rr_test_half_transform(Ct, nocc, B, naux, n, T, variant);  // warm-up, checks the variant
+    if (rc != RR_OK) return rc;
+    cudaEvent_t e0, e1;
+    RR_CUDA(cudaEventCreate(&e0));
+    RR_CUDA(cudaEventCreate(&e1));
+    RR_CUDA(cudaEventRecord(e0, nullptr));
+    for (int r = 0; r < reps; ++r) {
+      if (variant >= 1) {
+        rr::half_transform_m16(Ct, nocc, B, n * n, naux, n, T, nullptr, variant - 1);
+      } else {
+        rr::GemmDesc g;
+        g.M = nocc; g.N = n; g.K = n;
+        g.A = Ct; g.lda = n; g.B = B; g.ldb = n; g.strideB = n * n; g.C = T; g.ldc = n; g.strideC = nocc * n;
+        g.batch = naux;
+        rr::gemm(g, nullptr);
+      }
+    }
+    RR_CUDA(cudaEventRecord(e1, nullptr));
+    RR_CUDA(cudaEventSynchronize(e1));
+    float t = 0.f;
+    RR_CUDA(cudaEventElapsedTime(&t, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = t / reps;
     return RR_OK;
   } catch (const rr::Error& e) {
     rr::set_last_error(e.what());
