@@ -13,6 +13,7 @@
 #include <string>
 
 #include "gemm_f64.cuh"
+#include "tma_util.cuh"
 
 namespace rr {
 namespace {
@@ -136,6 +137,138 @@ __global__ void __launch_bounds__(32 * WARPS) ht_dmma16_kernel(const HtArgs a) {
     }
 }
 
+// Warp-specialised variant: the five compute warps of the default tiling plus one copy warp that fills
+// a STAGES-deep ring with 1-D bulk copies (one per B^P row segment of the tile and one per Ct row
+// segment, each into its padded shared-memory row), completing on the stage's `full` mbarrier; the
+// compute warps release a stage through its `empty` mbarrier.  No CTA-wide barrier in the main loop,
+// so a warp waits only for its data.  Every wait is bounded (status word, then the CTA drains).
+template <int STAGES>
+__global__ void __launch_bounds__(192, 1) ht_tma16_kernel(const HtArgs a, int* status) {
+  using CF = HtCfg<5, 16, STAGES>;
+  constexpr int BM = CF::BM, BN = CF::BN, KT = 16, LDA = CF::LDA, LDB = CF::LDB;
+  extern __shared__ __align__(16) double smem[];
+  __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES];
+  const int64_t j0 = static_cast<int64_t>(blockIdx.x) * BM;
+  const int64_t i0 = static_cast<int64_t>(blockIdx.y) * BN;
+  const int64_t P = a.p0 + blockIdx.z;
+  const double* Bp = a.B + P * a.pitch;
+  const int64_t n = a.n;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int ktiles = static_cast<int>((n + KT - 1) / KT);
+  if (tid == 0) {
+    for (int st = 0; st < STAGES; ++st) {
+      mbar_init(&full[st], 1);
+      mbar_init(&empty[st], 5);
+    }
+    fence_barrier_init();
+  }
+  __syncthreads();
+  bool dead = false;
+  // bounded wait: on expiry the status word records 0x10 and this thread skips every later wait
+  auto wait = [&](uint64_t* bar, uint32_t parity) -> bool {
+    if (dead) return false;
+    for (uint32_t i = 0; i < kSpinLimit; ++i)
+      if (mbar_try_wait(bar, parity)) return true;
+    atomicOr(status, 0x10);
+    dead = true;
+    return false;
+  };
+  if (warp == 5) {
+    // copy warp
+    const int rowsB = static_cast<int>(min(static_cast<int64_t>(BN), a.nocc - i0));
+    const uint32_t bytesA = static_cast<uint32_t>(min(static_cast<int64_t>(BM), n - j0) * 8);
+    for (int kt = 0; kt < ktiles && !dead; ++kt) {
+      const int st = kt % STAGES;
+      if (kt >= STAGES) {
+        bool ok = true;
+        if (lane == 0) ok = wait(&empty[st], ((kt / STAGES) - 1) & 1);
+        ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+        if (!ok) { dead = true; break; }
+      }
+      __syncwarp();
+      double* sA = smem + st * CF::STAGE;
+      double* sB = sA + CF::SA;
+      const int64_t k0 = static_cast<int64_t>(kt) * KT;
+      const int rowsA = static_cast<int>(min(static_cast<int64_t>(KT), n - k0));
+      const uint32_t bytesB = static_cast<uint32_t>(rowsA * 8);
+      // k rows past n (last tile): zeros in both operands
+      if (rowsA < KT) {
+        for (int e = lane; e < (KT - rowsA) * BM; e += 32) sA[(rowsA + e / BM) * LDA + e % BM] = 0.0;
+        for (int e = lane; e < BN * (KT - rowsA); e += 32) sB[(e / (KT - rowsA)) * LDB + rowsA + e % (KT - rowsA)] = 0.0;
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive_expect_tx(&full[st], rowsA * bytesA + rowsB * bytesB);
+      __syncwarp();
+      for (int c = lane; c < rowsA + rowsB; c += 32) {
+        if (c < rowsA) tma_load_1d(sA + c * LDA, Bp + (k0 + c) * n + j0, bytesA, &full[st]);
+        else tma_load_1d(sB + (c - rowsA) * LDB, a.Ct + (i0 + c - rowsA) * n + k0, bytesB, &full[st]);
+      }
+    }
+    // drain: the copies of the last stages have landed before the CTA may exit
+    if (lane == 0) {
+      dead = false;
+      for (int kt = max(0, ktiles - STAGES); kt < ktiles; ++kt) wait(&full[kt % STAGES], (kt / STAGES) & 1);
+    }
+    return;
+  }
+  const int g = lane >> 2, t = lane & 3;
+  double acc[5][4];
+#pragma unroll
+  for (int jb = 0; jb < 5; ++jb)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[jb][q] = 0.0;
+  const int m = warp * 16 + g;
+  for (int kt = 0; kt < ktiles; ++kt) {
+    const int st = kt % STAGES;
+    if (!wait(&full[st], (kt / STAGES) & 1)) break;
+    const double* sA = smem + st * CF::STAGE;
+    const double* sB = sA + CF::SA;
+#pragma unroll
+    for (int ks = 0; ks < KT / 8; ++ks) {
+      const int k = ks * 8 + t;
+      const double a0 = sA[k * LDA + m], a1 = sA[k * LDA + m + 8];
+      const double a2 = sA[(k + 4) * LDA + m], a3 = sA[(k + 4) * LDA + m + 8];
+#pragma unroll
+      for (int jb = 0; jb < 5; ++jb) {
+        const double b0 = sB[(jb * 8 + g) * LDB + k], b1 = sB[(jb * 8 + g) * LDB + k + 4];
+        dmma16(acc[jb], a0, a1, a2, a3, b0, b1);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[st]);
+  }
+  if (dead) return;
+  double* Tp = a.T + P * a.nocc * n;
+#pragma unroll
+  for (int jb = 0; jb < 5; ++jb)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int64_t j = j0 + warp * 16 + g + (q >= 2 ? 8 : 0);
+      const int64_t i = i0 + jb * 8 + 2 * t + (q & 1);
+      if (j < n && i < a.nocc) Tp[i * n + j] = acc[jb][q];
+    }
+}
+
+template <int STAGES>
+void launch_ht_tma(const HtArgs& base, int64_t naux, int* status, cudaStream_t s) {
+  using CF = HtCfg<5, 16, STAGES>;
+  auto kern = ht_tma16_kernel<STAGES>;
+  static std::atomic<bool> attr[kMaxDevices];
+  once_per_device(attr, [&] {
+    RR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, CF::SMEM));
+    RR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
+  });
+  for (int64_t p0 = 0; p0 < naux; p0 += 65535) {
+    const int64_t cnt = std::min<int64_t>(65535, naux - p0);
+    HtArgs a = base;
+    a.p0 = p0;
+    dim3 grid(static_cast<unsigned>((a.n + CF::BM - 1) / CF::BM), static_cast<unsigned>((a.nocc + CF::BN - 1) / CF::BN),
+              static_cast<unsigned>(cnt));
+    kern<<<grid, 192, CF::SMEM, s>>>(a, status);
+    RR_LAUNCH_CHECK();
+  }
+}
+
 template <int WARPS, int KT, int STAGES>
 void launch_ht(const HtArgs& base, int64_t naux, cudaStream_t s) {
   using CF = HtCfg<WARPS, KT, STAGES>;
@@ -159,7 +292,7 @@ void launch_ht(const HtArgs& base, int64_t naux, cudaStream_t s) {
 }  // namespace
 
 bool half_transform_m16(const double* Ct, int64_t nocc, const double* B, int64_t pitch, int64_t naux, int64_t n,
-                        double* T, cudaStream_t s, int config) {
+                        double* T, cudaStream_t s, int config, int* status) {
   // 16-byte cp.async sources: even n and pitch, 16-byte aligned bases
   auto al = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
   if (n % 2 != 0 || pitch % 2 != 0 || !al(Ct) || !al(B) || nocc <= 0 || n <= 0) return false;
@@ -171,6 +304,14 @@ bool half_transform_m16(const double* Ct, int64_t nocc, const double* B, int64_t
     case 4: launch_ht<4, 16, 3>(a, naux, s); break;
     case 5: launch_ht<1, 32, 3>(a, naux, s); break;
     case 6: launch_ht<2, 32, 3>(a, naux, s); break;
+    case 7:
+      if (!status) return false;
+      launch_ht_tma<4>(a, naux, status, s);
+      break;
+    case 8:
+      if (!status) return false;
+      launch_ht_tma<3>(a, naux, status, s);
+      break;
     default: launch_ht<5, 16, 3>(a, naux, s); break;
   }
   return true;

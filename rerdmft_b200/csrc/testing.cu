@@ -41,8 +41,32 @@ __global__ void wait_expiry_kernel(uint32_t limit, int* err, long long* out) {
   }
 }
 
+// Status word of the half-transform hooks (per device, zeroed on first use): a timed-out wait of the
+// bulk-copy pipeline sets it and the hook reports RR_ERR_TIMEOUT.
+int* test_status() {
+  static int* word[kMaxDevices] = {};
+  const int d = current_device();
+  if (!word[d]) {
+    RR_CUDA(cudaMalloc(&word[d], sizeof(int)));
+    RR_CUDA(cudaMemset(word[d], 0, sizeof(int)));
+  }
+  return word[d];
+}
+
+void check_test_status() {
+  int v = 0;
+  RR_CUDA(cudaMemcpy(&v, test_status(), sizeof(int), cudaMemcpyDeviceToHost));
+  if (v) {
+    RR_CUDA(cudaMemset(test_status(), 0, sizeof(int)));
+    throw Error(RR_ERR_TIMEOUT, "half-transform pipeline wait timed out (status " + std::to_string(v) + ")");
+  }
+}
+
 }  // namespace
 }  // namespace rr
+
+using rr::check_test_status;
+using rr::test_status;
 
 extern "C" {
 
@@ -52,9 +76,10 @@ int rr_test_half_transform(const double* Ct, int64_t nocc, const double* B, int6
                            int32_t variant) {
   try {
     rr::set_last_error("");
-    RR_REQUIRE(variant >= 0 && variant <= 7, RR_ERR_ARG, "rr_test_half_transform: variant must be in [0, 7]");
+    RR_REQUIRE(variant >= 0 && variant <= 9, RR_ERR_ARG, "rr_test_half_transform: variant must be in [0, 9]");
     if (variant >= 1) {
-      RR_REQUIRE(rr::half_transform_m16(Ct, nocc, B, n * n, naux, n, T, nullptr, variant - 1), RR_ERR_UNSUPPORTED,
+      RR_REQUIRE(rr::half_transform_m16(Ct, nocc, B, n * n, naux, n, T, nullptr, variant - 1, test_status()),
+                 RR_ERR_UNSUPPORTED,
                  "rr_test_half_transform: operands not supported by the m16n8k8 kernel");
     } else {
       rr::GemmDesc g;
@@ -66,6 +91,7 @@ int rr_test_half_transform(const double* Ct, int64_t nocc, const double* B, int6
       rr::gemm(g, nullptr);
     }
     RR_CUDA(cudaDeviceSynchronize());
+    check_test_status();
     return RR_OK;
   } catch (const rr::Error& e) {
     rr::set_last_error(e.what());
@@ -89,7 +115,7 @@ int rr_test_half_transform_time(const double* Ct, int64_t nocc, const double* B,
     RR_CUDA(cudaEventRecord(e0, nullptr));
     for (int r = 0; r < reps; ++r) {
       if (variant >= 1) {
-        rr::half_transform_m16(Ct, nocc, B, n * n, naux, n, T, nullptr, variant - 1);
+        rr::half_transform_m16(Ct, nocc, B, n * n, naux, n, T, nullptr, variant - 1, test_status());
       } else {
         rr::GemmDesc g;
         g.M = nocc; g.N = n; g.K = n;
@@ -104,6 +130,7 @@ int rr_test_half_transform_time(const double* Ct, int64_t nocc, const double* B,
     RR_CUDA(cudaEventElapsedTime(&t, e0, e1));
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    check_test_status();
     *ms = t / reps;
     return RR_OK;
   } catch (const rr::Error& e) {

@@ -145,14 +145,16 @@ def test_j_passes_packed(naux, n, kind):
 
 @pytest.mark.parametrize("nocc,n,naux", [(40, 400, 30), (17, 64, 7), (45, 82, 3), (1, 2, 1)])
 def test_half_transform_variants(nocc, n, naux):
-    """T[P] = Ct B^P through the general DMMA GEMM (m8n8k4) and the m16n8k8 half-transform, ragged tiles
-    included (n not a multiple of 80 or 16, nocc not a multiple of 40 or 8), against numpy."""
+    """T[P] = Ct B^P through the general DMMA GEMM (m8n8k4) and every tiling of the m16n8k8 half-transform
+    (the CTA-synchronous ring in its warp / depth / stage variants and the warp-specialised bulk-copy
+    pipeline), ragged tiles included (n not a multiple of 80 or 16, nocc not a multiple of 40 or 8),
+    against numpy."""
     rng = np.random.default_rng(n + nocc)
     Ct = rng.standard_normal((nocc, n))
     B = rng.standard_normal((naux, n * n))
     ref = np.einsum("ik,Pkj->Pij", Ct, B.reshape(naux, n, n), optimize=True)
     dC, dB = torch.from_numpy(Ct).cuda(), torch.from_numpy(B).cuda()
-    for variant in (0, 1):
+    for variant in range(10):
         T = torch.full((naux, nocc, n), float("nan"), dtype=torch.float64, device="cuda")
         L.check(L.lib().rr_test_half_transform(dC.data_ptr(), nocc, dB.data_ptr(), naux, n, T.data_ptr(), variant))
         err = np.abs(T.cpu().numpy() - ref).max()
