@@ -395,6 +395,10 @@ typedef struct rr_batch_stats {
   double seconds;                 /* wall time of the call */
   double autotune_seconds;        /* of which spent timing new GEMM shapes */
   int64_t autotune_entries;       /* shapes in the autotuner cache afterwards */
+  /* device time per phase summed over the iterations (CUDA events on the batch's stream): occupied
+   * spinors + Fock build + energy, DIIS, density step (X^dagger F X, SP2, back-transform, dP) */
+  double build_ms, diis_ms, density_ms;
+  int64_t sp2_steps_max;          /* the most SP2 steps of one iteration */
 } rr_batch_stats;
 
 int rr_scf_run_x2c_grouped(rr_x2c_instance* instances, int64_t count, const rr_scf_opts* scf, rr_batch_stats* stats);

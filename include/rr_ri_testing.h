@@ -61,7 +61,7 @@ int64_t rr_test_device_allocations(void);
 
 /* T[P] = Ct B^P for P < naux (Ct nocc x n, B naux x n^2, T naux x nocc x n; device pointers, synchronous)
  * through the general DMMA GEMM (variant 0, m8n8k4) or the m16n8k8 half-transform (variant 1: its default
- * tiling; 2-7: the alternative tilings kept for measurement). */
+ * tiling; 2-14: the alternative tilings kept for measurement). */
 int rr_test_half_transform(const double* Ct, int64_t nocc, const double* B, int64_t naux, int64_t n, double* T,
                            int32_t variant);
 /* The same, `reps` times after one warm-up; *ms = the average device time of one (CUDA events). */

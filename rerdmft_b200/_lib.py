@@ -92,7 +92,9 @@ class BatchStats(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int64), ("launches_total", ctypes.c_int64),
                 ("launches_setup", ctypes.c_int64), ("launches_max_iteration", ctypes.c_int64),
                 ("grouped_instances_first", ctypes.c_int64), ("seconds", ctypes.c_double),
-                ("autotune_seconds", ctypes.c_double), ("autotune_entries", ctypes.c_int64)]
+                ("autotune_seconds", ctypes.c_double), ("autotune_entries", ctypes.c_int64),
+                ("build_ms", ctypes.c_double), ("diis_ms", ctypes.c_double), ("density_ms", ctypes.c_double),
+                ("sp2_steps_max", ctypes.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

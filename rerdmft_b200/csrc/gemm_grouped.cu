@@ -278,11 +278,44 @@ int64_t bucket(int64_t x) {
   return round_up(x, 2048);
 }
 
-std::string key_of(const GemmDesc& d) {
-  std::ostringstream k;
-  k << "c" << (d.cplx ? 1 : 0) << "a" << static_cast<int>(d.opA) << "b" << static_cast<int>(d.opB) << "m" << d.mirror
-    << "_" << bucket(d.M) << "x" << bucket(d.N) << "x" << bucket(d.K) << "x" << bucket(d.batch);
-  return k.str();
+// Cache key: element kind, layout, mirror mode and the bucketed M, N, K, batch.
+struct ShapeKey {
+  int64_t v[8];
+  bool operator==(const ShapeKey& o) const {
+    for (int i = 0; i < 8; ++i)
+      if (v[i] != o.v[i]) return false;
+    return true;
+  }
+};
+
+struct ShapeKeyHash {
+  size_t operator()(const ShapeKey& k) const {
+    uint64_t h = 1469598103934665603ull;
+    for (int i = 0; i < 8; ++i) h = (h ^ static_cast<uint64_t>(k.v[i])) * 1099511628211ull;
+    return static_cast<size_t>(h);
+  }
+};
+
+ShapeKey shape_key(const GemmDesc& d) {
+  return ShapeKey{{d.cplx ? 1 : 0, static_cast<int64_t>(d.opA), static_cast<int64_t>(d.opB), d.mirror, bucket(d.M),
+                   bucket(d.N), bucket(d.K), bucket(d.batch)}};
+}
+
+// The cache file's text form of a key: c<kind>a<opA>b<opB>m<mirror>_<M>x<N>x<K>x<batch>.
+std::string key_text(const ShapeKey& k) {
+  std::ostringstream t;
+  t << "c" << k.v[0] << "a" << k.v[1] << "b" << k.v[2] << "m" << k.v[3] << "_" << k.v[4] << "x" << k.v[5] << "x" << k.v[6]
+    << "x" << k.v[7];
+  return t.str();
+}
+
+bool parse_key(const std::string& s, ShapeKey& k) {
+  long long v[8];
+  if (std::sscanf(s.c_str(), "c%llda%lldb%lldm%lld_%lldx%lldx%lldx%lld", &v[0], &v[1], &v[2], &v[3], &v[4], &v[5], &v[6],
+                  &v[7]) != 8)
+    return false;
+  for (int i = 0; i < 8; ++i) k.v[i] = v[i];
+  return true;
 }
 
 // Doubles spanned by the output of d (every batch entry, plane and mirrored triangle).
@@ -305,7 +338,7 @@ std::vector<int> candidate_cfgs(const GemmDesc& d) {
 
 struct Tuner {
   std::mutex mu;
-  std::unordered_map<std::string, std::pair<GemmChoice, double>> cache;
+  std::unordered_map<ShapeKey, std::pair<GemmChoice, double>, ShapeKeyHash> cache;
   bool env_loaded = false, dirty = false;
   TableRing ring;
   DevBuf<double> cbuf, wbuf;
@@ -326,18 +359,20 @@ void load_locked(Tuner& t, const std::string& path) {
   std::string line;
   while (std::getline(in, line)) {
     std::istringstream ls(line);
-    std::string key;
+    std::string text;
     GemmChoice c;
     double us = 0.0;
-    if (!(ls >> key >> c.cfg >> c.splits >> us)) continue;
+    ShapeKey key;
+    if (!(ls >> text >> c.cfg >> c.splits >> us) || !parse_key(text, key)) continue;
     if (c.cfg < 0 || c.cfg > 6 || c.splits < 1 || c.splits > 64) continue;
-    if (key.size() > 1 && key[1] == '1' && c.cfg > 1) continue;  // complex products have two configurations
+    if (key.v[0] == 1 && c.cfg > 1) continue;  // complex products have two configurations
     t.cache[key] = {c, us};
   }
 }
 
 void save_locked(Tuner& t, const std::string& path) {
-  std::map<std::string, std::pair<GemmChoice, double>> sorted(t.cache.begin(), t.cache.end());
+  std::map<std::string, std::pair<GemmChoice, double>> sorted;
+  for (auto& [k, v] : t.cache) sorted[key_text(k)] = v;
   const std::string tmp = path + ".tmp";
   {
     std::ofstream out(tmp, std::ios::trunc);
@@ -436,7 +471,7 @@ GemmChoice autotune_choice(const GemmDesc& d) {
   Tuner& t = tuner();
   std::lock_guard<std::mutex> lk(t.mu);
   env_load_locked(t);
-  const std::string key = key_of(d);
+  const ShapeKey key = shape_key(d);
   auto it = t.cache.find(key);
   if (it != t.cache.end()) return it->second.first;
   if (!t.s) {

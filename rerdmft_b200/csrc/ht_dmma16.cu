@@ -312,6 +312,11 @@ bool half_transform_m16(const double* Ct, int64_t nocc, const double* B, int64_t
       if (!status) return false;
       launch_ht_tma<3>(a, naux, status, s);
       break;
+    case 9: launch_ht<2, 16, 3>(a, naux, s); break;
+    case 10: launch_ht<2, 16, 5>(a, naux, s); break;
+    case 11: launch_ht<2, 16, 6>(a, naux, s); break;
+    case 12: launch_ht<4, 16, 4>(a, naux, s); break;
+    case 13: launch_ht<3, 16, 4>(a, naux, s); break;
     default: launch_ht<5, 16, 3>(a, naux, s); break;
   }
   return true;

@@ -773,7 +773,10 @@ void scf_x2c_grouped(rr_x2c_instance* ins, int64_t count, const rr_scf_opts* so,
     }
   }
   const int64_t launches_setup = own_launches() - launches0;
-  int64_t max_iter_launches = 0, lockstep = 0;
+  int64_t max_iter_launches = 0, lockstep = 0, sp2_max = 0;
+  cudaEvent_t ev[4];
+  for (auto& e : ev) RR_CUDA(cudaEventCreate(&e));
+  double phase_ms[3] = {0.0, 0.0, 0.0};
 
   // ---- lockstep iterations ----
   for (int64_t it = 1; it <= so->max_iterations; ++it) {
@@ -784,6 +787,7 @@ void scf_x2c_grouped(rr_x2c_instance* ins, int64_t count, const rr_scf_opts* so,
     lockstep = it;
     const int64_t l_it0 = own_launches();
     const int na = static_cast<int>(act.size());
+    RR_CUDA(cudaEventRecord(ev[0], b.s));
     if (it > 1) {
       // occupied spinors of the previous iteration's projector (with linear mixing the density is no
       // projector: single-instance recovery from P)
@@ -862,6 +866,7 @@ void scf_x2c_grouped(rr_x2c_instance* ins, int64_t count, const rr_scf_opts* so,
     // energy
     GLAUNCH(k_energy_part, GRC, na, tab, al);
     GLAUNCH(k_reduce<0>, 1, na, tab, al, P_E, GRC, GRC, 1, 0, 0.5);
+    RR_CUDA(cudaEventRecord(ev[1], b.s));
     // DIIS
     if (use_diis) {
       g.clear();
@@ -940,6 +945,7 @@ void scf_x2c_grouped(rr_x2c_instance* ins, int64_t count, const rr_scf_opts* so,
       al = b.upload_list(act);
     }
     GLAUNCH(k_diis_combine, mx([](const GDev& d) { return 2 * d.n * d.n; }), na, tab, al);
+    RR_CUDA(cudaEventRecord(ev[2], b.s));
     // Fo = X^dagger Fs X
     g.clear();
     for (int i : act) {
@@ -966,6 +972,7 @@ void scf_x2c_grouped(rr_x2c_instance* ins, int64_t count, const rr_scf_opts* so,
       std::vector<int> sp = act;
       const int* spl = al;
       for (int step = 0; step < 120 && !sp.empty(); ++step) {
+        sp2_max = std::max<int64_t>(sp2_max, step + 1);
         g.clear();
         for (int i : sp) {
           const GDev& d = b.gs[i].d;
@@ -1029,7 +1036,13 @@ void scf_x2c_grouped(rr_x2c_instance* ins, int64_t count, const rr_scf_opts* so,
     }
     GLAUNCH(k_maxdiff_part, GRC, na2, tab, al);
     GLAUNCH(k_reduce<2>, 1, na2, tab, al, P_D, GRC, GRC, 1, 1, 1.0);
+    RR_CUDA(cudaEventRecord(ev[3], b.s));
     b.sync_scalars();
+    for (int q = 0; q < 3; ++q) {
+      float t = 0.f;
+      RR_CUDA(cudaEventElapsedTime(&t, ev[q], ev[q + 1]));
+      phase_ms[q] += t;
+    }
     max_iter_launches = std::max(max_iter_launches, own_launches() - l_it0);
     // convergence (X2C_HF.cpp:120-134): dP < tolP or dE < tolE from the second iteration
     std::vector<int> mix;
@@ -1100,7 +1113,12 @@ void scf_x2c_grouped(rr_x2c_instance* ins, int64_t count, const rr_scf_opts* so,
     autotune_totals(&ts, &tl);
     stats->autotune_seconds = ts - tune_s0;
     stats->autotune_entries = autotune_entries();
+    stats->build_ms = phase_ms[0];
+    stats->diis_ms = phase_ms[1];
+    stats->density_ms = phase_ms[2];
+    stats->sp2_steps_max = sp2_max;
   }
+  for (auto& e : ev) cudaEventDestroy(e);
 }
 
 }  // namespace rr

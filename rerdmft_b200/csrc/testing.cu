@@ -76,7 +76,7 @@ int rr_test_half_transform(const double* Ct, int64_t nocc, const double* B, int6
                            int32_t variant) {
   try {
     rr::set_last_error("");
-    RR_REQUIRE(variant >= 0 && variant <= 9, RR_ERR_ARG, "rr_test_half_transform: variant must be in [0, 9]");
+    RR_REQUIRE(variant >= 0 && variant <= 14, RR_ERR_ARG, "rr_test_half_transform: variant must be in [0, 14]");
     if (variant >= 1) {
       RR_REQUIRE(rr::half_transform_m16(Ct, nocc, B, n * n, naux, n, T, nullptr, variant - 1, test_status()),
                  RR_ERR_UNSUPPORTED,

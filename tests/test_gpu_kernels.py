@@ -154,7 +154,7 @@ def test_half_transform_variants(nocc, n, naux):
     B = rng.standard_normal((naux, n * n))
     ref = np.einsum("ik,Pkj->Pij", Ct, B.reshape(naux, n, n), optimize=True)
     dC, dB = torch.from_numpy(Ct).cuda(), torch.from_numpy(B).cuda()
-    for variant in range(10):
+    for variant in range(15):
         T = torch.full((naux, nocc, n), float("nan"), dtype=torch.float64, device="cuda")
         L.check(L.lib().rr_test_half_transform(dC.data_ptr(), nocc, dB.data_ptr(), naux, n, T.data_ptr(), variant))
         err = np.abs(T.cpu().numpy() - ref).max()
