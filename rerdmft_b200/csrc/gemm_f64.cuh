@@ -35,7 +35,8 @@ struct GemmDesc {
   int64_t c_col_stride = 1;
   // Symmetric outputs: compute only tiles touching the upper triangle, then fill the strict
   // lower triangle from the upper one: +1 C[i][j] = C[j][i] (Hermitian conj for cplx),
-  // -1 C[i][j] = -C[j][i].  0 = full output.  Requires M == N.
+  // -1 C[i][j] = -C[j][i].  0 = full output.  Requires M == N.  2 (grouped GEMM only): the upper
+  // tiles and nothing else; the strict lower triangle is left for the consumer to read as the mirror.
   int mirror = 0;
   // Epilogue dot (real, no split-K): per output tile also
   //   edot_out[b * tiles + tile] = edot_scale * sum_{(m,n) in tile} C[b](m, n) * edot_E[m * edot_ld + n]
@@ -59,11 +60,11 @@ int64_t gemm_work_doubles(const GemmDesc& d);
 
 // T[P] = Ct B^P for P < naux on the m16n8k8 FP64 shape (ht_dmma16.cu): Ct nocc x n (row pitch n), B^P
 // n x n in rows of `pitch` doubles, T[P] at T + P nocc n (row pitch n).  Returns false (nothing launched)
-// when the operands do not meet its 16-byte alignment rule.  config 0 is the default tiling (5 warps,
-// 16-deep k tiles, 3 stages); 1-6 are the alternatives kept for measurement: (warps, k depth, stages) =
+// when the operands do not meet its 16-byte alignment rule.  config 0 is the default tiling (2 warps,
+// 16-deep k tiles, 5 stages); 1-6 are the alternatives kept for measurement: (warps, k depth, stages) =
 // (1,16,4), (2,16,4), (5,32,2), (4,16,3), (1,32,3), (2,32,3); 7 and 8 the warp-specialised bulk-copy
 // pipeline with 4 and 3 stages (they need `status`, the device word a timed-out wait sets); 9-13:
-// (2,16,3), (2,16,5), (2,16,6), (4,16,4), (3,16,4).
+// (2,16,3), (5,16,3), (2,16,6), (4,16,4), (3,16,4).
 bool half_transform_m16(const double* Ct, int64_t nocc, const double* B, int64_t pitch, int64_t naux, int64_t n,
                         double* T, cudaStream_t s, int config = 0, int* status = nullptr);
 // Which half-transform the nonrelativistic exchange uses: 0 = the general DMMA GEMM (m8n8k4),

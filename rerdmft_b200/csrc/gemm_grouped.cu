@@ -47,7 +47,7 @@ __device__ __forceinline__ int find_problem(const int64_t* off, int n, int64_t t
   return lo;
 }
 
-template <int MT, int NT, int WM, int WN, bool AK, bool BKM, bool CPLX>
+template <int MT, int NT, int WM, int WN, bool AK, bool BKM, bool CPLX, int V>
 __global__ void __launch_bounds__(32 * WM * WN) dgemm_grouped_kernel(const GroupArgs g) {
   using CF = Cfg<MT, NT, WM, WN, AK, BKM, CPLX>;
   extern __shared__ __align__(16) double smem[];
@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(32 * WM * WN) dgemm_grouped_kernel(const Group
     const int64_t bz = lt / (tx * ty), rem = lt % (tx * ty);
     const int64_t m0 = (rem / tx) * CF::BM, n0 = (rem % tx) * CF::BN;
     if (sp.upper_only && m0 > n0 + CF::BN - 1) continue;
-    dgemm_tile<MT, NT, WM, WN, AK, BKM, CPLX, 1, false>(sp, n0, m0, bz, smem, 0);
+    dgemm_tile<MT, NT, WM, WN, AK, BKM, CPLX, V, false>(sp, n0, m0, bz, smem, 0);
   }
 }
 
@@ -94,10 +94,10 @@ constexpr TileDims kReal[7] = {{32, 32}, {64, 64}, {80, 80}, {8, 128}, {16, 128}
 constexpr TileDims kCplx[2] = {{32, 32}, {32, 64}};
 TileDims dims_of(bool cplx, int cfg) { return cplx ? kCplx[cfg] : kReal[cfg]; }
 
-template <int MT, int NT, int WM, int WN, bool AK, bool BKM, bool CPLX>
+template <int MT, int NT, int WM, int WN, bool AK, bool BKM, bool CPLX, int V = 1>
 void launch_grouped(const GroupArgs& g, cudaStream_t s) {
   using CF = Cfg<MT, NT, WM, WN, AK, BKM, CPLX>;
-  auto kern = dgemm_grouped_kernel<MT, NT, WM, WN, AK, BKM, CPLX>;
+  auto kern = dgemm_grouped_kernel<MT, NT, WM, WN, AK, BKM, CPLX, V>;
   static std::atomic<bool> attr[kMaxDevices];
   static int occ[kMaxDevices];
   const int dev = current_device();
@@ -113,17 +113,23 @@ void launch_grouped(const GroupArgs& g, cudaStream_t s) {
   RR_LAUNCH_CHECK();
 }
 
-template <bool AK, bool BKM>
-void launch_real_cfg(int cfg, const GroupArgs& g, cudaStream_t s) {
+template <bool AK, bool BKM, int V>
+void launch_real_cfg_v(int cfg, const GroupArgs& g, cudaStream_t s) {
   switch (cfg) {
-    case 0: return launch_grouped<2, 2, 2, 2, AK, BKM, false>(g, s);
-    case 1: return launch_grouped<4, 4, 2, 2, AK, BKM, false>(g, s);
-    case 2: return launch_grouped<5, 5, 2, 2, AK, BKM, false>(g, s);
-    case 3: return launch_grouped<1, 4, 1, 4, AK, BKM, false>(g, s);
-    case 4: return launch_grouped<2, 4, 1, 4, AK, BKM, false>(g, s);
-    case 5: return launch_grouped<4, 4, 1, 4, AK, BKM, false>(g, s);
-    default: return launch_grouped<5, 2, 1, 5, AK, BKM, false>(g, s);
+    case 0: return launch_grouped<2, 2, 2, 2, AK, BKM, false, V>(g, s);
+    case 1: return launch_grouped<4, 4, 2, 2, AK, BKM, false, V>(g, s);
+    case 2: return launch_grouped<5, 5, 2, 2, AK, BKM, false, V>(g, s);
+    case 3: return launch_grouped<1, 4, 1, 4, AK, BKM, false, V>(g, s);
+    case 4: return launch_grouped<2, 4, 1, 4, AK, BKM, false, V>(g, s);
+    case 5: return launch_grouped<4, 4, 1, 4, AK, BKM, false, V>(g, s);
+    default: return launch_grouped<5, 2, 1, 5, AK, BKM, false, V>(g, s);
   }
+}
+
+template <bool AK, bool BKM>
+void launch_real_cfg(int cfg, bool vec2, const GroupArgs& g, cudaStream_t s) {
+  if (vec2) launch_real_cfg_v<AK, BKM, 2>(cfg, g, s);
+  else launch_real_cfg_v<AK, BKM, 1>(cfg, g, s);
 }
 
 template <bool AK, bool BKM>
@@ -132,23 +138,35 @@ void launch_cplx_cfg(int cfg, const GroupArgs& g, cudaStream_t s) {
   else launch_grouped<2, 4, 2, 2, AK, BKM, true>(g, s);
 }
 
-void launch_cfg(bool cplx, bool AK, bool BKM, int cfg, const GroupArgs& g, cudaStream_t s) {
+void launch_cfg(bool cplx, bool AK, bool BKM, int cfg, bool vec2, const GroupArgs& g, cudaStream_t s) {
   if (cplx) {
     if (AK && BKM) launch_cplx_cfg<true, true>(cfg, g, s);
     else if (AK) launch_cplx_cfg<true, false>(cfg, g, s);
     else if (BKM) launch_cplx_cfg<false, true>(cfg, g, s);
     else launch_cplx_cfg<false, false>(cfg, g, s);
   } else {
-    if (AK && BKM) launch_real_cfg<true, true>(cfg, g, s);
-    else if (AK) launch_real_cfg<true, false>(cfg, g, s);
-    else if (BKM) launch_real_cfg<false, true>(cfg, g, s);
-    else launch_real_cfg<false, false>(cfg, g, s);
+    if (AK && BKM) launch_real_cfg<true, true>(cfg, vec2, g, s);
+    else if (AK) launch_real_cfg<true, false>(cfg, vec2, g, s);
+    else if (BKM) launch_real_cfg<false, true>(cfg, vec2, g, s);
+    else launch_real_cfg<false, false>(cfg, vec2, g, s);
   }
+}
+
+// 16-byte loads (real products only): 16-byte aligned bases and batch strides, even leading dims, even
+// contiguous extents and an even k chunk, so that a pair of doubles never straddles a row end.
+bool vec2_ok(const GemmDesc& d, int64_t kchunk) {
+  if (d.cplx) return false;
+  auto al = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15) == 0; };
+  const bool AK = d.opA == Op::N, BKM = d.opB == Op::T;
+  const bool a = al(d.A) && d.lda % 2 == 0 && d.strideA % 2 == 0 && (AK ? d.K % 2 == 0 : d.M % 2 == 0);
+  const bool b = al(d.B) && d.ldb % 2 == 0 && d.strideB % 2 == 0 && (BKM ? d.K % 2 == 0 : d.N % 2 == 0);
+  return a && b && kchunk % 2 == 0;
 }
 
 void check_desc(const GemmDesc& d) {
   RR_REQUIRE(d.M >= 0 && d.N >= 0 && d.K >= 0 && d.batch >= 0, RR_ERR_ARG, "gemm_grouped: negative size");
   RR_REQUIRE(!d.mirror || d.M == d.N, RR_ERR_ARG, "gemm_grouped: mirror needs a square output");
+  RR_REQUIRE(d.mirror >= -1 && d.mirror <= 2, RR_ERR_ARG, "gemm_grouped: mirror must be -1, 0, 1 or 2");
   RR_REQUIRE(!d.mirror || (d.c_plane_rows == 0 && d.c_col_stride == 1), RR_ERR_ARG,
              "gemm_grouped: mirror with planar or strided output");
   RR_REQUIRE(d.c_col_stride >= 1 && (d.c_col_stride == 1 || !d.cplx), RR_ERR_ARG, "gemm_grouped: bad output column stride");
@@ -211,7 +229,8 @@ void grouped_run(const std::vector<GemmDesc>& descs, const std::vector<GemmChoic
   std::map<int, std::vector<size_t>> groups;
   for (size_t k = 0; k < items.size(); ++k) {
     const GemmDesc& d = descs[items[k].i];
-    const int key = (d.cplx ? 1000 : 0) + (d.opA == Op::N ? 100 : 0) + (d.opB == Op::T ? 10 : 0) + items[k].cfg;
+    const int key = (vec2_ok(d, items[k].kc) ? 10000 : 0) + (d.cplx ? 1000 : 0) + (d.opA == Op::N ? 100 : 0) +
+                    (d.opB == Op::T ? 10 : 0) + items[k].cfg;
     groups[key].push_back(k);
   }
   for (auto& [key, ks] : groups) {
@@ -231,8 +250,9 @@ void grouped_run(const std::vector<GemmDesc>& descs, const std::vector<GemmChoic
     g.off = static_cast<const int64_t*>(ring.put(off.data(), sizeof(int64_t) * off.size(), s));
     g.n = static_cast<int>(gp.size());
     g.total = total;
-    const bool cplx = key >= 1000, AK = (key / 100) % 10 == 1, BKM = (key / 10) % 10 == 1;
-    launch_cfg(cplx, AK, BKM, key % 10, g, s);
+    const bool vec2 = key >= 10000, cplx = (key / 1000) % 10 == 1, AK = (key / 100) % 10 == 1,
+               BKM = (key / 10) % 10 == 1;
+    launch_cfg(cplx, AK, BKM, key % 10, vec2, g, s);
     if (launches) ++*launches;
   }
   // split-K reductions, then mirrors of the one-pass upper-only products (the reduction mirrors its own)
@@ -244,7 +264,7 @@ void grouped_run(const std::vector<GemmDesc>& descs, const std::vector<GemmChoic
       for (size_t k = 0; k < items.size(); ++k) {
         const GemmDesc& d = descs[items[k].i];
         if ((d.cplx ? 2 : 1) != pl) continue;
-        const bool take = pass == 0 ? items[k].splits > 1 : (d.mirror != 0 && items[k].splits == 1);
+        const bool take = pass == 0 ? items[k].splits > 1 : ((d.mirror == 1 || d.mirror == -1) && items[k].splits == 1);
         if (!take) continue;
         gp.push_back(prm[k]);
         off.push_back(total);

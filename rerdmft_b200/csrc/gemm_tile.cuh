@@ -29,7 +29,7 @@ struct Params {
   int64_t c_plane_rows, c_plane_stride;
   int64_t ccs;  // output column stride
   int upper_only;
-  int mirror;  // split-K reduce of an upper-only product also writes the strict lower triangle (+1 / -1)
+  int mirror;  // split-K reduce of an upper-only product also writes the strict lower triangle (+1 / -1; 2: not)
   const double* eE;
   int64_t eld;
   double escale;
@@ -270,7 +270,7 @@ __device__ __forceinline__ void splitk_reduce_elem(const Params& p, int64_t idx)
     if (p.beta != 0.0) v[q] += p.beta * c[q];
     c[q] = v[q];
   }
-  if (p.upper_only && row < col) {
+  if (p.upper_only && row < col && p.mirror != 2) {
     // the strict lower triangle from the final upper value (mirror requires no plane split and a
     // unit column stride; the lower triangle is never read as beta input here)
     double* t = p.C + (b * p.strideC + col * p.ldc + row) * PL;

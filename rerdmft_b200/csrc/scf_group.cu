@@ -345,9 +345,9 @@ __global__ void k_sp2_init(const GDev* tab, const int* act) {
   }
 }
 
-// Trace-correcting SP2 step on X (Pi) with T2 = X^2: t1 = tr X, t2 = tr X^2 from the partials at pin;
-// X <- X^2 if that brings the trace closer to N = r, else 2X - X^2; scal[2..3] = (t1, t2); partials of
-// the new X at pout.
+// Trace-correcting SP2 step on X (Pi) with T2 = X^2 (its upper triangle; the lower one is read as the
+// Hermitian mirror): t1 = tr X, t2 = tr X^2 from the partials at pin; X <- X^2 if that brings the trace
+// closer to N = r, else 2X - X^2; scal[2..3] = (t1, t2); partials of the new X at pout.
 __global__ void k_sp2_step(const GDev* tab, const int* act, int pin, int pout) {
   const GDev& d = inst(tab, act);
   __shared__ int sq;
@@ -374,9 +374,11 @@ __global__ void k_sp2_step(const GDev* tab, const int* act, int pin, int pout) {
   double tr = 0.0, fro = 0.0;
   for (int64_t idx = beg + threadIdx.x; idx < end; idx += blockDim.x) {
     const int64_t i = idx / n, j = idx % n;
+    const int64_t u = i <= j ? idx : j * n + i;
+    const double t2[2] = {d.T2[2 * u], i <= j ? d.T2[2 * u + 1] : -d.T2[2 * u + 1]};
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
-      const double x = square ? d.T2[2 * idx + q] : 2.0 * d.Pi[2 * idx + q] - d.T2[2 * idx + q];
+      const double x = square ? t2[q] : 2.0 * d.Pi[2 * idx + q] - t2[q];
       d.Pi[2 * idx + q] = x;
       fro += x * x;
       if (q == 0 && i == j) tr += x;
@@ -445,6 +447,14 @@ __global__ void __launch_bounds__(CHOL_THREADS) k_chol(const GDev* tab, const in
   extern __shared__ double csm[];
   const GDev& d = tab[act[blockIdx.x]];
   chol_block_body<2>(d.Mm, static_cast<int>(d.r), d.Wt, inverse, d.status, csm);
+}
+
+// Occupied count r of the next Fock build, and the places that depend on it: the second spin block's
+// split rows and half-transform planes follow the first block's.
+void set_rank(GDev& d, int64_t r) {
+  d.r = r;
+  d.Cs1 = d.Cs0 + 2 * r * d.nl;
+  d.T1 = d.T0 + 2 * d.naux * r * d.nl;
 }
 
 int gblocks(int64_t per_inst) {
@@ -673,10 +683,8 @@ void scf_x2c_grouped(rr_x2c_instance* ins, int64_t count, const rr_scf_opts* so,
       ar.request(&d.gam, naux);
       ar.request(&d.J, nl * nl);
       ar.request(&d.Ct, 2 * rmax * n);
-      ar.request(&d.Cs0, 2 * rmax * nl);
-      ar.request(&d.Cs1, 2 * rmax * nl);
-      ar.request(&d.T0, 2 * naux * rmax * nl);
-      ar.request(&d.T1, 2 * naux * rmax * nl);
+      ar.request(&d.Cs0, 4 * rmax * nl);         // [Re c_0; Im c_0; Re c_1; Im c_1] (Cs1 follows Cs0)
+      ar.request(&d.T0, 4 * naux * rmax * nl);   // the four planes of both half-transforms (T1 follows T0)
       ar.request(&d.Tm0, naux * rmax * nl);
       ar.request(&d.Tp1, naux * rmax * nl);
       for (double** k : {&d.K00r, &d.K00i, &d.K11r, &d.K11i, &d.K01r, &d.K01i, &d.K2}) ar.request(k, nl * nl);
@@ -692,6 +700,7 @@ void scf_x2c_grouped(rr_x2c_instance* ins, int64_t count, const rr_scf_opts* so,
       ar.request(&d.val, slots * c2);
       ar.commit();
       d.h = hd; d.X = Xd; d.S = Sd;
+      set_rank(d, r);
       d.scal = b.scal_all.p + i * SCAL;
       d.status = b.status_all.p + i;
       d.kramers = so->kramers_restricted && in.n_electrons % 2 == 0;
@@ -764,8 +773,9 @@ void scf_x2c_grouped(rr_x2c_instance* ins, int64_t count, const rr_scf_opts* so,
     for (int i : fallback) {
       GHost& G = b.gs[i];
       try {
-        G.d.r = occupied_ct(G.h, G.d.X, G.d.S, G.d.P, G.d.n, G.d.ne, 1.0, true, true, G.d.Ct, b.s);
-        RR_REQUIRE(G.d.r <= G.d.ne, RR_ERR_SOLVER, "occupied recovery rank out of range");
+        const int64_t r = occupied_ct(G.h, G.d.X, G.d.S, G.d.P, G.d.n, G.d.ne, 1.0, true, true, G.d.Ct, b.s);
+        RR_REQUIRE(r <= G.d.ne, RR_ERR_SOLVER, "occupied recovery rank out of range");
+        set_rank(G.d, r);
       } catch (const Error& e) {
         G.in->status = e.code;
         G.ok = G.active = false;
@@ -792,12 +802,12 @@ void scf_x2c_grouped(rr_x2c_instance* ins, int64_t count, const rr_scf_opts* so,
       // occupied spinors of the previous iteration's projector (with linear mixing the density is no
       // projector: single-instance recovery from P)
       if (!mixing_on) {
-        for (int i : act) b.gs[i].d.r = b.gs[i].in->n_electrons;
+        for (int i : act) set_rank(b.gs[i].d, b.gs[i].in->n_electrons);
         grouped_ct(b, act, false);
       } else {
         for (int i : act) {
           GHost& G = b.gs[i];
-          G.d.r = occupied_ct(G.h, G.d.X, G.d.S, G.d.P, G.d.n, G.d.ne, 1.0, true, true, G.d.Ct, b.s);
+          set_rank(G.d, occupied_ct(G.h, G.d.X, G.d.S, G.d.P, G.d.n, G.d.ne, 1.0, true, true, G.d.Ct, b.s));
         }
       }
     }
@@ -810,19 +820,19 @@ void scf_x2c_grouped(rr_x2c_instance* ins, int64_t count, const rr_scf_opts* so,
     GLAUNCH(k_jmat, mx([](const GDev& d) { return d.nl * d.nl; }), na, tab, al);
     // K
     GLAUNCH(k_split, mx([](const GDev& d) { return 4 * d.r * d.nl; }), na, tab, al);
+    // one half-transform for both spin blocks (B^P read once): rows [Re c_0; Im c_0; Re c_1; Im c_1]
+    // into the planes [Re T_0 | Im T_0 | Re T_1 | Im T_1]
     std::vector<GemmDesc> g;
     for (int i : act) {
       const GDev& d = b.gs[i].d;
-      for (int f = 0; f < 2; ++f) {
-        GemmDesc ht;
-        ht.M = 2 * d.r; ht.N = d.nl; ht.K = d.nl;
-        ht.A = f ? d.Cs1 : d.Cs0; ht.lda = d.nl;
-        ht.B = d.B; ht.ldb = d.nl; ht.strideB = d.pitch;
-        ht.C = f ? d.T1 : d.T0; ht.ldc = d.nl; ht.strideC = d.r * d.nl;
-        ht.c_plane_rows = d.r; ht.c_plane_stride = d.naux * d.r * d.nl;
-        ht.batch = d.naux;
-        g.push_back(ht);
-      }
+      GemmDesc ht;
+      ht.M = 4 * d.r; ht.N = d.nl; ht.K = d.nl;
+      ht.A = d.Cs0; ht.lda = d.nl;
+      ht.B = d.B; ht.ldb = d.nl; ht.strideB = d.pitch;
+      ht.C = d.T0; ht.ldc = d.nl; ht.strideC = d.r * d.nl;
+      ht.c_plane_rows = d.r; ht.c_plane_stride = d.naux * d.r * d.nl;
+      ht.batch = d.naux;
+      g.push_back(ht);
     }
     b.gemms(g);
     GLAUNCH(k_plane_pm, mx([](const GDev& d) { return d.naux * d.r * d.nl; }), na, tab, al);
@@ -977,7 +987,7 @@ void scf_x2c_grouped(rr_x2c_instance* ins, int64_t count, const rr_scf_opts* so,
         for (int i : sp) {
           const GDev& d = b.gs[i].d;
           GemmDesc q = cg(d.ne, d.ne, d.ne, d.Pi, d.ne, d.Pi, d.ne, d.T2, d.ne);
-          q.mirror = 1;
+          q.mirror = 2;  // X^2 is Hermitian: upper tiles only, k_sp2_step reads the rest as the mirror
           g.push_back(q);
         }
         b.gemms(g);
