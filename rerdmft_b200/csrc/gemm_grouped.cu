@@ -173,9 +173,10 @@ void check_desc(const GemmDesc& d) {
   RR_REQUIRE(!d.edot_out, RR_ERR_ARG, "gemm_grouped: no epilogue dot");
 }
 
-// Runs descs[i] with choice[i] (the autotuner's, or a candidate it is timing).
-void grouped_run(const std::vector<GemmDesc>& descs, const std::vector<GemmChoice>& choice, cudaStream_t s,
-                 TableRing& ring, DevBuf<double>& work, int64_t* launches) {
+// Builds the launches of descs[i] with choice[i] (the autotuner's, or a candidate it is timing).
+void grouped_build(const std::vector<GemmDesc>& descs, const std::vector<GemmChoice>& choice, cudaStream_t s,
+                   TableRing& ring, DevBuf<double>& work, GroupedPlan& plan) {
+  plan.launches.clear();
   struct Item {
     size_t i;
     int cfg, splits;
@@ -245,15 +246,18 @@ void grouped_run(const std::vector<GemmDesc>& descs, const std::vector<GemmChoic
       off.push_back(total);
       total += items[k].tiles;
     }
-    GroupArgs g;
-    g.probs = static_cast<const Params*>(ring.put(gp.data(), sizeof(Params) * gp.size(), s));
-    g.off = static_cast<const int64_t*>(ring.put(off.data(), sizeof(int64_t) * off.size(), s));
-    g.n = static_cast<int>(gp.size());
-    g.total = total;
-    const bool vec2 = key >= 10000, cplx = (key / 1000) % 10 == 1, AK = (key / 100) % 10 == 1,
-               BKM = (key / 10) % 10 == 1;
-    launch_cfg(cplx, AK, BKM, key % 10, vec2, g, s);
-    if (launches) ++*launches;
+    GroupedLaunch L{};
+    L.kind = 0;
+    L.probs = ring.put(gp.data(), sizeof(Params) * gp.size(), s);
+    L.off = static_cast<const int64_t*>(ring.put(off.data(), sizeof(int64_t) * off.size(), s));
+    L.n = static_cast<int>(gp.size());
+    L.total = total;
+    L.vec2 = key >= 10000;
+    L.cplx = (key / 1000) % 10 == 1;
+    L.AK = (key / 100) % 10 == 1;
+    L.BKM = (key / 10) % 10 == 1;
+    L.cfg = key % 10;
+    plan.launches.push_back(L);
   }
   // split-K reductions, then mirrors of the one-pass upper-only products (the reduction mirrors its own)
   for (int pl = 1; pl <= 2; ++pl)
@@ -271,22 +275,46 @@ void grouped_run(const std::vector<GemmDesc>& descs, const std::vector<GemmChoic
         total += d.batch * d.M * d.N;
       }
       if (gp.empty()) continue;
-      GroupArgs g;
-      g.probs = static_cast<const Params*>(ring.put(gp.data(), sizeof(Params) * gp.size(), s));
-      g.off = static_cast<const int64_t*>(ring.put(off.data(), sizeof(int64_t) * off.size(), s));
-      g.n = static_cast<int>(gp.size());
-      g.total = total;
-      const int blocks = static_cast<int>(std::min<int64_t>(4LL * sm_count_current(), std::max<int64_t>(1, (total + 255) / 256)));
-      if (pass == 0) {
-        if (pl == 2) splitk_reduce_grouped_kernel<2><<<blocks, 256, 0, s>>>(g);
-        else splitk_reduce_grouped_kernel<1><<<blocks, 256, 0, s>>>(g);
+      GroupedLaunch L{};
+      L.kind = pass == 0 ? 1 : 2;
+      L.pl = pl;
+      L.probs = ring.put(gp.data(), sizeof(Params) * gp.size(), s);
+      L.off = static_cast<const int64_t*>(ring.put(off.data(), sizeof(int64_t) * off.size(), s));
+      L.n = static_cast<int>(gp.size());
+      L.total = total;
+      L.blocks = static_cast<int>(std::min<int64_t>(4LL * sm_count_current(), std::max<int64_t>(1, (total + 255) / 256)));
+      plan.launches.push_back(L);
+    }
+}
+
+void grouped_exec(const GroupedPlan& plan, cudaStream_t s, int64_t* launches) {
+  for (const GroupedLaunch& L : plan.launches) {
+    GroupArgs g;
+    g.probs = static_cast<const Params*>(L.probs);
+    g.off = L.off;
+    g.n = L.n;
+    g.total = L.total;
+    if (L.kind == 0) {
+      launch_cfg(L.cplx, L.AK, L.BKM, L.cfg, L.vec2, g, s);
+    } else {
+      if (L.kind == 1) {
+        if (L.pl == 2) splitk_reduce_grouped_kernel<2><<<L.blocks, 256, 0, s>>>(g);
+        else splitk_reduce_grouped_kernel<1><<<L.blocks, 256, 0, s>>>(g);
       } else {
-        if (pl == 2) mirror_grouped_kernel<2><<<blocks, 256, 0, s>>>(g);
-        else mirror_grouped_kernel<1><<<blocks, 256, 0, s>>>(g);
+        if (L.pl == 2) mirror_grouped_kernel<2><<<L.blocks, 256, 0, s>>>(g);
+        else mirror_grouped_kernel<1><<<L.blocks, 256, 0, s>>>(g);
       }
       RR_LAUNCH_CHECK();
-      if (launches) ++*launches;
     }
+    if (launches) ++*launches;
+  }
+}
+
+void grouped_run(const std::vector<GemmDesc>& descs, const std::vector<GemmChoice>& choice, cudaStream_t s,
+                 TableRing& ring, DevBuf<double>& work, int64_t* launches) {
+  GroupedPlan plan;
+  grouped_build(descs, choice, s, ring, work, plan);
+  grouped_exec(plan, s, launches);
 }
 
 // ------------------------------------------------------------------------------------ autotuner
@@ -478,6 +506,16 @@ const void* TableRing::put(const void* src, size_t bytes, cudaStream_t s) {
   used += need;
   return out;
 }
+
+void gemm_grouped_plan(const std::vector<GemmDesc>& descs, cudaStream_t s, TableRing& ring, DevBuf<double>& work,
+                       GroupedPlan& plan) {
+  std::vector<GemmChoice> ch(descs.size());
+  for (size_t i = 0; i < descs.size(); ++i)
+    if (descs[i].M > 0 && descs[i].N > 0 && descs[i].batch > 0) ch[i] = autotune_choice(descs[i]);
+  grouped_build(descs, ch, s, ring, work, plan);
+}
+
+void gemm_grouped_exec(const GroupedPlan& plan, cudaStream_t s, int64_t* launches) { grouped_exec(plan, s, launches); }
 
 void gemm_grouped(const std::vector<GemmDesc>& descs, cudaStream_t s, TableRing& ring, DevBuf<double>& work,
                   int64_t* launches) {

@@ -48,6 +48,26 @@ struct TableRing {
 void gemm_grouped(const std::vector<GemmDesc>& descs, cudaStream_t s, TableRing& ring, DevBuf<double>& work,
                   int64_t* launches);
 
+// A built grouped launch sequence: its tables live in the TableRing it was built with and its split-K
+// scratch in `work`, so it may be executed again (on the same stream) until the ring's next reset() or
+// the next growth of that scratch.  For loops that repeat the same products (SP2 steps).
+struct GroupedLaunch {
+  int kind;  // 0 GEMM tiles, 1 split-K reduction, 2 mirror
+  int cfg, pl;
+  bool cplx, AK, BKM, vec2;
+  const void* probs;
+  const int64_t* off;
+  int n;
+  int64_t total;
+  int blocks;
+};
+struct GroupedPlan {
+  std::vector<GroupedLaunch> launches;
+};
+void gemm_grouped_plan(const std::vector<GemmDesc>& descs, cudaStream_t s, TableRing& ring, DevBuf<double>& work,
+                       GroupedPlan& plan);
+void gemm_grouped_exec(const GroupedPlan& plan, cudaStream_t s, int64_t* launches);
+
 // The tuned choice for this problem shape: looked up in the cache, else measured on the spot (each
 // candidate configuration and split count timed as a grouped launch of enough copies of the problem
 // to fill the GPU, CUDA events, the fastest per problem kept).  The first call loads the file named by

@@ -820,19 +820,21 @@ void scf_x2c_grouped(rr_x2c_instance* ins, int64_t count, const rr_scf_opts* so,
     GLAUNCH(k_jmat, mx([](const GDev& d) { return d.nl * d.nl; }), na, tab, al);
     // K
     GLAUNCH(k_split, mx([](const GDev& d) { return 4 * d.r * d.nl; }), na, tab, al);
-    // one half-transform for both spin blocks (B^P read once): rows [Re c_0; Im c_0; Re c_1; Im c_1]
-    // into the planes [Re T_0 | Im T_0 | Re T_1 | Im T_1]
+    // the half-transforms of the two spin blocks, T_f[P] = [Re c_f; Im c_f] B^P, as two problems per
+    // instance (one product of all four row blocks measured slower: its 4r rows fit no skinny tile)
     std::vector<GemmDesc> g;
     for (int i : act) {
       const GDev& d = b.gs[i].d;
-      GemmDesc ht;
-      ht.M = 4 * d.r; ht.N = d.nl; ht.K = d.nl;
-      ht.A = d.Cs0; ht.lda = d.nl;
-      ht.B = d.B; ht.ldb = d.nl; ht.strideB = d.pitch;
-      ht.C = d.T0; ht.ldc = d.nl; ht.strideC = d.r * d.nl;
-      ht.c_plane_rows = d.r; ht.c_plane_stride = d.naux * d.r * d.nl;
-      ht.batch = d.naux;
-      g.push_back(ht);
+      for (int f = 0; f < 2; ++f) {
+        GemmDesc ht;
+        ht.M = 2 * d.r; ht.N = d.nl; ht.K = d.nl;
+        ht.A = f ? d.Cs1 : d.Cs0; ht.lda = d.nl;
+        ht.B = d.B; ht.ldb = d.nl; ht.strideB = d.pitch;
+        ht.C = f ? d.T1 : d.T0; ht.ldc = d.nl; ht.strideC = d.r * d.nl;
+        ht.c_plane_rows = d.r; ht.c_plane_stride = d.naux * d.r * d.nl;
+        ht.batch = d.naux;
+        g.push_back(ht);
+      }
     }
     b.gemms(g);
     GLAUNCH(k_plane_pm, mx([](const GDev& d) { return d.naux * d.r * d.nl; }), na, tab, al);
@@ -981,16 +983,23 @@ void scf_x2c_grouped(rr_x2c_instance* ins, int64_t count, const rr_scf_opts* so,
     {
       std::vector<int> sp = act;
       const int* spl = al;
+      // the same X^2 products every step: built once per stretch between read-backs, then re-launched
+      GroupedPlan sq;
+      bool sq_valid = false;
       for (int step = 0; step < 120 && !sp.empty(); ++step) {
         sp2_max = std::max<int64_t>(sp2_max, step + 1);
-        g.clear();
-        for (int i : sp) {
-          const GDev& d = b.gs[i].d;
-          GemmDesc q = cg(d.ne, d.ne, d.ne, d.Pi, d.ne, d.Pi, d.ne, d.T2, d.ne);
-          q.mirror = 2;  // X^2 is Hermitian: upper tiles only, k_sp2_step reads the rest as the mirror
-          g.push_back(q);
+        if (!sq_valid) {
+          g.clear();
+          for (int i : sp) {
+            const GDev& d = b.gs[i].d;
+            GemmDesc q = cg(d.ne, d.ne, d.ne, d.Pi, d.ne, d.Pi, d.ne, d.T2, d.ne);
+            q.mirror = 2;  // X^2 is Hermitian: upper tiles only, k_sp2_step reads the rest as the mirror
+            g.push_back(q);
+          }
+          gemm_grouped_plan(g, b.s, b.ring, b.work, sq);
+          sq_valid = true;
         }
-        b.gemms(g);
+        gemm_grouped_exec(sq, b.s, nullptr);
         const int pin = (step & 1) ? P_S1 : P_S0, pout = (step & 1) ? P_S0 : P_S1;
         GLAUNCH(k_sp2_step, GRC, sp.size(), tab, spl, pin, pout);
         if (step % 4 == 3) {
@@ -1003,6 +1012,7 @@ void scf_x2c_grouped(rr_x2c_instance* ins, int64_t count, const rr_scf_opts* so,
           }
           sp.swap(keep);
           spl = b.upload_list(sp);
+          sq_valid = false;  // the read-back reset the table space
         }
       }
       for (int i : sp) {  // no gap at the Fermi level
