@@ -399,6 +399,7 @@ typedef struct rr_batch_stats {
    * spinors + Fock build + energy, DIIS, density step (X^dagger F X, SP2, back-transform, dP) */
   double build_ms, diis_ms, density_ms;
   int64_t sp2_steps_max;          /* the most SP2 steps of one iteration */
+  double host_wait_ms;            /* wall time the host spent waiting for the stream at read-backs */
 } rr_batch_stats;
 
 int rr_scf_run_x2c_grouped(rr_x2c_instance* instances, int64_t count, const rr_scf_opts* scf, rr_batch_stats* stats);

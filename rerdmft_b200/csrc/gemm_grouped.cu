@@ -177,6 +177,7 @@ void check_desc(const GemmDesc& d) {
 void grouped_build(const std::vector<GemmDesc>& descs, const std::vector<GemmChoice>& choice, cudaStream_t s,
                    TableRing& ring, DevBuf<double>& work, GroupedPlan& plan) {
   plan.launches.clear();
+  plan.side = &ring.side;
   struct Item {
     size_t i;
     int cfg, splits;
@@ -288,6 +289,13 @@ void grouped_build(const std::vector<GemmDesc>& descs, const std::vector<GemmCho
 }
 
 void grouped_exec(const GroupedPlan& plan, cudaStream_t s, int64_t* launches) {
+  int ngemm = 0;
+  for (const GroupedLaunch& L : plan.launches) ngemm += L.kind == 0 ? 1 : 0;
+  SideStreams* ss = ngemm > 1 ? plan.side : nullptr;
+  if (ss) ss->make();
+  if (ss) RR_CUDA(cudaEventRecord(ss->fork, s));
+  int k = 0;
+  bool joined = ss == nullptr;
   for (const GroupedLaunch& L : plan.launches) {
     GroupArgs g;
     g.probs = static_cast<const Params*>(L.probs);
@@ -295,8 +303,21 @@ void grouped_exec(const GroupedPlan& plan, cudaStream_t s, int64_t* launches) {
     g.n = L.n;
     g.total = L.total;
     if (L.kind == 0) {
-      launch_cfg(L.cplx, L.AK, L.BKM, L.cfg, L.vec2, g, s);
+      cudaStream_t t = s;
+      if (ss) {
+        t = ss->st[k % SideStreams::kCount];
+        if (k < SideStreams::kCount) RR_CUDA(cudaStreamWaitEvent(t, ss->fork, 0));
+        ++k;
+      }
+      launch_cfg(L.cplx, L.AK, L.BKM, L.cfg, L.vec2, g, t);
     } else {
+      if (!joined) {  // the tile launches (all before the first reduction in a plan) are done first
+        for (int i = 0; i < std::min(k, SideStreams::kCount); ++i) {
+          RR_CUDA(cudaEventRecord(ss->done[i], ss->st[i]));
+          RR_CUDA(cudaStreamWaitEvent(s, ss->done[i], 0));
+        }
+        joined = true;
+      }
       if (L.kind == 1) {
         if (L.pl == 2) splitk_reduce_grouped_kernel<2><<<L.blocks, 256, 0, s>>>(g);
         else splitk_reduce_grouped_kernel<1><<<L.blocks, 256, 0, s>>>(g);
@@ -308,6 +329,11 @@ void grouped_exec(const GroupedPlan& plan, cudaStream_t s, int64_t* launches) {
     }
     if (launches) ++*launches;
   }
+  if (!joined)
+    for (int i = 0; i < std::min(k, SideStreams::kCount); ++i) {
+      RR_CUDA(cudaEventRecord(ss->done[i], ss->st[i]));
+      RR_CUDA(cudaStreamWaitEvent(s, ss->done[i], 0));
+    }
 }
 
 void grouped_run(const std::vector<GemmDesc>& descs, const std::vector<GemmChoice>& choice, cudaStream_t s,
@@ -470,6 +496,23 @@ double measure(Tuner& t, const GemmDesc& d, GemmChoice cand) {
 }
 
 }  // namespace
+
+SideStreams::~SideStreams() {
+  for (int i = 0; i < kCount; ++i) {
+    if (st[i]) cudaStreamDestroy(st[i]);
+    if (done[i]) cudaEventDestroy(done[i]);
+  }
+  if (fork) cudaEventDestroy(fork);
+}
+
+void SideStreams::make() {
+  if (fork) return;
+  for (int i = 0; i < kCount; ++i) {
+    RR_CUDA(cudaStreamCreateWithFlags(&st[i], cudaStreamNonBlocking));
+    RR_CUDA(cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming));
+  }
+  RR_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+}
 
 TableRing::~TableRing() {
   if (host) cudaFreeHost(host);

@@ -21,10 +21,24 @@ struct GemmChoice {
 // into a linear device buffer.  Space is handed out in order and recycled by reset(), which the
 // owner calls only after the stream has passed every launch that read earlier tables (a full wait);
 // when the buffer runs out, put() continues in a larger one and keeps the full one until reset().
+// Side streams of a caller's grouped launches: tile launches of different configurations run beside
+// each other, joined before the reductions (created on first use, on the device current then).
+struct SideStreams {
+  static constexpr int kCount = 4;
+  cudaStream_t st[kCount] = {};
+  cudaEvent_t fork = nullptr, done[kCount] = {};
+  SideStreams() = default;
+  SideStreams(const SideStreams&) = delete;
+  SideStreams& operator=(const SideStreams&) = delete;
+  ~SideStreams();
+  void make();
+};
+
 struct TableRing {
   DevBuf<char> dev;
   char* host = nullptr;
   size_t cap = 0, used = 0;
+  SideStreams side;  // the grouped launches that take their tables from this ring run their tiles here
   // buffers that filled up since the last reset(): kept until then, since tables in them may still
   // be read by queued launches
   std::vector<std::pair<DevBuf<char>, char*>> retired;
@@ -63,6 +77,7 @@ struct GroupedLaunch {
 };
 struct GroupedPlan {
   std::vector<GroupedLaunch> launches;
+  SideStreams* side = nullptr;  // of the ring the plan was built with
 };
 void gemm_grouped_plan(const std::vector<GemmDesc>& descs, cudaStream_t s, TableRing& ring, DevBuf<double>& work,
                        GroupedPlan& plan);

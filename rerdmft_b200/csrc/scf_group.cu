@@ -495,7 +495,7 @@ struct Batch {
   DevBuf<double> work, scal_all;
   DevBuf<int> status_all;
   std::vector<double> scal_host;
-  int64_t nlaunch_start = 0;
+  double wait_ms = 0.0;
   ~Batch() {
     if (s) cudaStreamDestroy(s);
   }
@@ -518,7 +518,9 @@ struct Batch {
   }
   void sync_scalars() {
     RR_CUDA(cudaMemcpyAsync(scal_host.data(), scal_all.p, sizeof(double) * scal_host.size(), cudaMemcpyDeviceToHost, s));
+    const auto w0 = std::chrono::steady_clock::now();
     RR_CUDA(cudaStreamSynchronize(s));
+    wait_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();
     ring.reset();
   }
   void gemms(const std::vector<GemmDesc>& g) { gemm_grouped(g, s, ring, work, nullptr); }
@@ -1137,6 +1139,7 @@ void scf_x2c_grouped(rr_x2c_instance* ins, int64_t count, const rr_scf_opts* so,
     stats->diis_ms = phase_ms[1];
     stats->density_ms = phase_ms[2];
     stats->sp2_steps_max = sp2_max;
+    stats->host_wait_ms = b.wait_ms;
   }
   for (auto& e : ev) cudaEventDestroy(e);
 }
