@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "chol.cuh"
@@ -466,7 +467,6 @@ int gblocks(int64_t per_inst) {
 struct GHost {
   rr_x2c_instance* in = nullptr;
   rr_ri_store* h = nullptr;
-  DevBuf<double> mem;
   GDev d{};
   double* scal_host = nullptr;  // its row of the gathered scalars
   bool ok = true, active = true, converged = false, grouped_first = false;
@@ -488,17 +488,44 @@ GemmDesc cg(int64_t M, int64_t N, int64_t K, const double* A, int64_t lda, const
   return g;
 }
 
-struct Batch {
-  std::vector<GHost> gs;
+// Batch-level resources kept per device between calls (a stream, the table space, split-K scratch, the
+// gathered scalars), so that a repeated scan allocates nothing; calls on one device take turns.
+struct GroupCtx {
+  std::mutex mu;
   cudaStream_t s = nullptr;
   TableRing ring;
   DevBuf<double> work, scal_all;
   DevBuf<int> status_all;
+  cudaEvent_t ev[4] = {};
+};
+
+GroupCtx& group_ctx() {
+  static GroupCtx* ctx[kMaxDevices] = {};
+  static std::mutex mk;
+  const int d = current_device();
+  std::lock_guard<std::mutex> lk(mk);
+  if (!ctx[d]) {
+    auto* c = new GroupCtx();  // kept for the process: its CUDA objects are never released at exit
+    RR_CUDA(cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking));
+    for (auto& e : c->ev) RR_CUDA(cudaEventCreate(&e));
+    c->ring.reserve(size_t{8} << 20);
+    ctx[d] = c;
+  }
+  return *ctx[d];
+}
+
+struct Batch {
+  GroupCtx& c;
+  std::vector<GHost> gs;
+  cudaStream_t s;
+  TableRing& ring;
+  DevBuf<double>& work;
+  DevBuf<double>& scal_all;
+  DevBuf<int>& status_all;
   std::vector<double> scal_host;
   double wait_ms = 0.0;
-  ~Batch() {
-    if (s) cudaStreamDestroy(s);
-  }
+  explicit Batch(GroupCtx& ctx)
+      : c(ctx), s(ctx.s), ring(ctx.ring), work(ctx.work), scal_all(ctx.scal_all), status_all(ctx.status_all) {}
 
   // table of every instance's descriptor, as it is now
   const GDev* upload_tab() {
@@ -615,15 +642,16 @@ void scf_x2c_grouped(rr_x2c_instance* ins, int64_t count, const rr_scf_opts* so,
   RR_REQUIRE(so->diis_size <= GDIIS, RR_ERR_ARG, "rr_scf_run_x2c_grouped: diis_size too large");
   const bool use_diis = so->diis_size >= 2;
   const bool mixing_on = !use_diis && so->mixing > 0.0 && so->mixing != 1.0;
-  Batch b;
+  GroupCtx& ctx = group_ctx();
+  std::lock_guard<std::mutex> ctx_lock(ctx.mu);
+  Batch b(ctx);
+  b.ring.reset();
   b.gs.resize(static_cast<size_t>(count));
-  RR_CUDA(cudaStreamCreateWithFlags(&b.s, cudaStreamNonBlocking));
-  b.scal_all.alloc(static_cast<size_t>(std::max<int64_t>(count, 1) * SCAL));
-  b.status_all.alloc(static_cast<size_t>(std::max<int64_t>(count, 1)));
+  b.scal_all.ensure(static_cast<size_t>(std::max<int64_t>(count, 1) * SCAL));
+  b.status_all.ensure(static_cast<size_t>(std::max<int64_t>(count, 1)));
   RR_CUDA(cudaMemsetAsync(b.status_all.p, 0, sizeof(int) * std::max<int64_t>(count, 1), b.s));
   RR_CUDA(cudaMemsetAsync(b.scal_all.p, 0, sizeof(double) * std::max<int64_t>(count, 1) * SCAL, b.s));
   b.scal_host.assign(static_cast<size_t>(std::max<int64_t>(count, 1) * SCAL), 0.0);
-  b.ring.reserve(size_t{8} << 20);
   double tune_s0 = 0.0;
   int64_t tune_l0 = 0;
   autotune_totals(&tune_s0, &tune_l0);
@@ -661,7 +689,7 @@ void scf_x2c_grouped(rr_x2c_instance* ins, int64_t count, const rr_scf_opts* so,
       const int64_t c2 = 2 * n * n, ce = 2 * n * ne, ee = 2 * ne * ne, naux = h->naux;
       // the occupied count can differ from n_electrons only for a fallback first iteration
       const int64_t rmax = ne;
-      Arena ar(&G.mem);
+      Arena ar(&h->scf_buf);  // the handle's SCF buffers, grown on demand and kept between runs
       GDev& d = G.d;
       d.nl = nl; d.n = n; d.ne = ne; d.r = r; d.naux = naux; d.pitch = h->pitch[0]; d.nb = nl;
       d.B = h->B[0].p;
@@ -786,8 +814,7 @@ void scf_x2c_grouped(rr_x2c_instance* ins, int64_t count, const rr_scf_opts* so,
   }
   const int64_t launches_setup = own_launches() - launches0;
   int64_t max_iter_launches = 0, lockstep = 0, sp2_max = 0;
-  cudaEvent_t ev[4];
-  for (auto& e : ev) RR_CUDA(cudaEventCreate(&e));
+  cudaEvent_t* ev = ctx.ev;
   double phase_ms[3] = {0.0, 0.0, 0.0};
 
   // ---- lockstep iterations ----
@@ -1141,7 +1168,7 @@ void scf_x2c_grouped(rr_x2c_instance* ins, int64_t count, const rr_scf_opts* so,
     stats->sp2_steps_max = sp2_max;
     stats->host_wait_ms = b.wait_ms;
   }
-  for (auto& e : ev) cudaEventDestroy(e);
+
 }
 
 }  // namespace rr
