@@ -400,6 +400,7 @@ typedef struct rr_batch_stats {
   double build_ms, diis_ms, density_ms;
   int64_t sp2_steps_max;          /* the most SP2 steps of one iteration */
   double host_wait_ms;            /* wall time the host spent waiting for the stream at read-backs */
+  double host_gemm_ms;            /* wall time the host spent building and enqueueing grouped GEMMs */
 } rr_batch_stats;
 
 int rr_scf_run_x2c_grouped(rr_x2c_instance* instances, int64_t count, const rr_scf_opts* scf, rr_batch_stats* stats);

@@ -94,7 +94,8 @@ class BatchStats(ctypes.Structure):
                 ("grouped_instances_first", ctypes.c_int64), ("seconds", ctypes.c_double),
                 ("autotune_seconds", ctypes.c_double), ("autotune_entries", ctypes.c_int64),
                 ("build_ms", ctypes.c_double), ("diis_ms", ctypes.c_double), ("density_ms", ctypes.c_double),
-                ("sp2_steps_max", ctypes.c_int64), ("host_wait_ms", ctypes.c_double)]
+                ("sp2_steps_max", ctypes.c_int64), ("host_wait_ms", ctypes.c_double),
+                ("host_gemm_ms", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

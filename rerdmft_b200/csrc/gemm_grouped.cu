@@ -228,13 +228,19 @@ void grouped_build(const std::vector<GemmDesc>& descs, const std::vector<GemmCho
   }
   // one launch per (element kind, layout, configuration); inside it the longest-K problems first, so
   // the fixed-stride walk spreads them over the grid
-  std::map<int, std::vector<size_t>> groups;
+  std::vector<std::pair<int, std::vector<size_t>>> groups;  // few keys: a sorted small vector
   for (size_t k = 0; k < items.size(); ++k) {
     const GemmDesc& d = descs[items[k].i];
     const int key = (vec2_ok(d, items[k].kc) ? 10000 : 0) + (d.cplx ? 1000 : 0) + (d.opA == Op::N ? 100 : 0) +
                     (d.opB == Op::T ? 10 : 0) + items[k].cfg;
-    groups[key].push_back(k);
+    auto it = std::find_if(groups.begin(), groups.end(), [&](const auto& g) { return g.first == key; });
+    if (it == groups.end()) {
+      groups.emplace_back(key, std::vector<size_t>{});
+      it = groups.end() - 1;
+    }
+    it->second.push_back(k);
   }
+  std::sort(groups.begin(), groups.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
   for (auto& [key, ks] : groups) {
     std::stable_sort(ks.begin(), ks.end(), [&](size_t a, size_t b) {
       return prm[a].kchunk * prm[a].M > prm[b].kchunk * prm[b].M;
@@ -552,9 +558,8 @@ const void* TableRing::put(const void* src, size_t bytes, cudaStream_t s) {
 
 void gemm_grouped_plan(const std::vector<GemmDesc>& descs, cudaStream_t s, TableRing& ring, DevBuf<double>& work,
                        GroupedPlan& plan) {
-  std::vector<GemmChoice> ch(descs.size());
-  for (size_t i = 0; i < descs.size(); ++i)
-    if (descs[i].M > 0 && descs[i].N > 0 && descs[i].batch > 0) ch[i] = autotune_choice(descs[i]);
+  std::vector<GemmChoice> ch;
+  autotune_choices(descs, ch);
   grouped_build(descs, ch, s, ring, work, plan);
 }
 
@@ -562,15 +567,31 @@ void gemm_grouped_exec(const GroupedPlan& plan, cudaStream_t s, int64_t* launche
 
 void gemm_grouped(const std::vector<GemmDesc>& descs, cudaStream_t s, TableRing& ring, DevBuf<double>& work,
                   int64_t* launches) {
-  std::vector<GemmChoice> ch(descs.size());
-  for (size_t i = 0; i < descs.size(); ++i)
-    if (descs[i].M > 0 && descs[i].N > 0 && descs[i].batch > 0) ch[i] = autotune_choice(descs[i]);
+  std::vector<GemmChoice> ch;
+  autotune_choices(descs, ch);
   grouped_run(descs, ch, s, ring, work, launches);
 }
+
+namespace {
+GemmChoice choice_locked(Tuner& t, const GemmDesc& d);
+}  // namespace
 
 GemmChoice autotune_choice(const GemmDesc& d) {
   Tuner& t = tuner();
   std::lock_guard<std::mutex> lk(t.mu);
+  return choice_locked(t, d);
+}
+
+void autotune_choices(const std::vector<GemmDesc>& descs, std::vector<GemmChoice>& out) {
+  out.assign(descs.size(), GemmChoice{});
+  Tuner& t = tuner();
+  std::lock_guard<std::mutex> lk(t.mu);
+  for (size_t i = 0; i < descs.size(); ++i)
+    if (descs[i].M > 0 && descs[i].N > 0 && descs[i].batch > 0) out[i] = choice_locked(t, descs[i]);
+}
+
+namespace {
+GemmChoice choice_locked(Tuner& t, const GemmDesc& d) {
   env_load_locked(t);
   const ShapeKey key = shape_key(d);
   auto it = t.cache.find(key);
@@ -601,6 +622,7 @@ GemmChoice autotune_choice(const GemmDesc& d) {
   t.launches += rr::launches() - l0;
   return best;
 }
+}  // namespace
 
 void autotune_load(const std::string& path) {
   Tuner& t = tuner();

@@ -88,6 +88,8 @@ void gemm_grouped_exec(const GroupedPlan& plan, cudaStream_t s, int64_t* launche
 // to fill the GPU, CUDA events, the fastest per problem kept).  The first call loads the file named by
 // RR_AUTOTUNE_CACHE when that variable is set.
 GemmChoice autotune_choice(const GemmDesc& d);
+// The same for every problem of descs (one lock for all; empty problems get the default).
+void autotune_choices(const std::vector<GemmDesc>& descs, std::vector<GemmChoice>& out);
 // Cache file: one line per shape, "<key> <cfg> <splits> <microseconds per problem>".
 void autotune_load(const std::string& path);
 void autotune_save(const std::string& path);

@@ -550,7 +550,12 @@ struct Batch {
     wait_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();
     ring.reset();
   }
-  void gemms(const std::vector<GemmDesc>& g) { gemm_grouped(g, s, ring, work, nullptr); }
+  double gemm_ms = 0.0;
+  void gemms(const std::vector<GemmDesc>& g) {
+    const auto t0 = std::chrono::steady_clock::now();
+    gemm_grouped(g, s, ring, work, nullptr);
+    gemm_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
 };
 
 #define GLAUNCH(kern, gx, nact, ...)                                                      \
@@ -1025,10 +1030,16 @@ void scf_x2c_grouped(rr_x2c_instance* ins, int64_t count, const rr_scf_opts* so,
             q.mirror = 2;  // X^2 is Hermitian: upper tiles only, k_sp2_step reads the rest as the mirror
             g.push_back(q);
           }
+          const auto t0 = std::chrono::steady_clock::now();
           gemm_grouped_plan(g, b.s, b.ring, b.work, sq);
+          b.gemm_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
           sq_valid = true;
         }
-        gemm_grouped_exec(sq, b.s, nullptr);
+        {
+          const auto t0 = std::chrono::steady_clock::now();
+          gemm_grouped_exec(sq, b.s, nullptr);
+          b.gemm_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        }
         const int pin = (step & 1) ? P_S1 : P_S0, pout = (step & 1) ? P_S0 : P_S1;
         GLAUNCH(k_sp2_step, GRC, sp.size(), tab, spl, pin, pout);
         if (step % 4 == 3) {
@@ -1167,6 +1178,7 @@ void scf_x2c_grouped(rr_x2c_instance* ins, int64_t count, const rr_scf_opts* so,
     stats->density_ms = phase_ms[2];
     stats->sp2_steps_max = sp2_max;
     stats->host_wait_ms = b.wait_ms;
+    stats->host_gemm_ms = b.gemm_ms;
   }
 
 }
