@@ -305,6 +305,52 @@ def orbital_optimization_block():
     return out
 
 
+def gnof_optimization_block():
+    """GNOF FULL_OPTIMIZATION (rerdmft_b200.pnof: device ADAM orbital runs, host occupation steps over
+    the gamma angles from the device J/K) on LiH-sized systems (11 spatial orbitals, naux 48, two
+    occupied pairs each coupled with three virtual pairs; two seeds): macro-iterations and wall time to
+    |dE| < 1e-8 Ha with plain ADAM and with the learned preconditioner, each at the reference's base
+    rate and at 2, 4, 8 x that rate (the best run that reaches the default plain energy to 1e-7 Ha is
+    reported beside the default)."""
+    from rerdmft_b200 import mo, orbopt, pnof, synth
+
+    net = orbopt.load_default_preconditioner()
+    out = {}
+    n, nocc, coupling = 11, 2, 4
+    for seed in (16, 40):
+        f = synth.functional_system(n, 48, seed, nocc=nocc)
+        gem = pnof.nonrel_geminals(n, nocc, coupling)
+        occ0 = pnof.occupations_of(gem, coupling, np.full(nocc * (coupling - 1), np.pi / 4), 2 * n)
+        two = pnof.full_two_rdm(pnof.FUNCTIONALS["GNOF"], gem, occ0, 2 * n)
+        runs = {"plain": {}, "learned": {}}
+        for mode in runs:
+            for factor in (1, 2, 4, 8):
+                opt = orbopt.adam_default_options()
+                opt.learning_rate = 0.01 * factor
+                eri = mo.RiNonRelSpinMoEri.from_tensor(f["Bmo"], n)
+                prob = orbopt.RotationProblem(eri, f["h"], occ0, two["two_rdm_h"], two["two_rdm_x"], two["pair_of"],
+                                              two["two_rdm_l1"], two["two_rdm_l2"], options=opt)
+                res = pnof.run_pnof_optimization(prob, "GNOF", gem, coupling,
+                                                 preconditioner=net if mode == "learned" else None)
+                prob.close()
+                eri.close()
+                runs[mode][factor] = dict(learning_rate=opt.learning_rate,
+                                          **{k: res[k] for k in ("macro_iterations", "scaled_macro_iterations",
+                                                                 "adam_steps", "seconds", "energy", "converged")})
+        r = {"plain": runs["plain"][1], "learned": runs["learned"][1]}
+        e_ref = r["plain"]["energy"]
+        for mode in runs:
+            ok = [v for v in runs[mode].values() if v["converged"] and abs(v["energy"] - e_ref) <= 1e-7]
+            r[mode + "_best_rate"] = min(ok, key=lambda v: v["macro_iterations"]) if ok else None
+        r["macro_reduction"] = 1.0 - r["learned"]["macro_iterations"] / r["plain"]["macro_iterations"]
+        if r["plain_best_rate"] and r["learned_best_rate"]:
+            r["macro_reduction_best_rates"] = (1.0 - r["learned_best_rate"]["macro_iterations"] /
+                                               r["plain_best_rate"]["macro_iterations"])
+        out[f"lih_sized_n11_seed{seed}"] = r
+    net.close()
+    return out
+
+
 def x2c_batch_problems(count: int = 64):
     """The batched X2C-HF geometry scan: `count` instances with uneven nl in [20, 120] (seeded), naux = 4 nl,
     4 or 14 electrons (LiH- / CO-like) alternating, one handle each (uploaded here)."""
@@ -915,6 +961,7 @@ def main():
     mo_block = mo_transform_block(torch, fp64_peak, want_cpu=not args.no_cpu_baseline)
     orb_block = orbital_optimization_block()
     x2c_block = x2c_batch_block(want_cpu=not args.no_cpu_baseline)
+    gnof_block = gnof_optimization_block()
     rel_block = rel_scf_times(not args.no_cpu_baseline,
                               (rkb_block.get("reference_cpu") or {}).get("seconds_per_build"))
     line = dict(
@@ -949,6 +996,7 @@ def main():
         mo_transform=mo_block,
         orbital_optimization=orb_block,
         x2c_batch=x2c_block,
+        gnof_optimization=gnof_block,
     )
     print(json.dumps(line))
     if pg:

@@ -539,6 +539,16 @@ int rr_orbopt_create(rr_mo_handle m, const double* h, const double* occupations,
  * excludeNegative, FullOptimization.cpp:83-92).  Clears the scales of rr_orbopt_set_scales. */
 int rr_orbopt_exclude_negative(rr_orbopt_handle h, int64_t n_negative);
 int rr_orbopt_destroy(rr_orbopt_handle h);
+/* New occupations and two-RDM factors (the same shapes as at creation) for the next runs, as the macro
+ * loop of FULL_OPTIMIZATION hands the re-optimised occupations to the orbital stage
+ * (FullOptimization.cpp:2822-2835); the orbitals, the ADAM state and the scales are kept. */
+int rr_orbopt_set_functional(rr_orbopt_handle h, const double* occupations, const double* two_rdm_h,
+                             const double* two_rdm_x, const int64_t* pair_of, const double* two_rdm_l1,
+                             const double* two_rdm_l2);
+/* J_ij = eri(i,j,i,j) and K_ij = eri(i,j,j,i) of the current (rotated) tensor over the accessor's
+ * dimension (2n spin orbitals, or n spinors, interleaved complex), host outputs: what the occupation
+ * step reads (RiMoEri.h:50-57). */
+int rr_orbopt_jk(rr_orbopt_handle h, double* J, double* K);
 int rr_orbopt_info(rr_orbopt_handle h, int64_t* n_pairs, int64_t* n_spatial, int64_t* naux);
 /* One AdamOptimizer::run: ADAM steps from the current orbitals until the gradient or energy
  * converges or the run's step budget ends; the best orbitals found become current.  The learning

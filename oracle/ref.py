@@ -537,3 +537,17 @@ def pnof_full_two_rdm(functional, geminals, occ, n_total, relativistic=True):
                                          ctypes.c_int(1 if relativistic else 0), _p(h2), _p(x2), _p(l1), _p(l2),
                                          _p(po)))
     return dict(two_rdm_h=h2, two_rdm_x=x2, two_rdm_l1=l1, two_rdm_l2=l2, pair_of=po)
+
+
+def pnof_energy_nonrel(functional, geminals, occ, Bmo_spatial, n_sp, h):
+    """pnofElectronicEnergy and pnofOccupationGradient (PNOFs.cpp:271, :463) of a non-relativistic
+    spin-orbital problem (h and occupations over the 2 n_sp spin orbitals); returns (energy, gradient
+    per geminal)."""
+    f = {"PNOF5": 0, "PNOF7": 1, "PNOF7S": 2, "GNOF": 3}[functional.upper()]
+    g = np.ascontiguousarray(geminals, dtype=np.int64).reshape(-1, 4)
+    e = ctypes.c_double()
+    grad = np.empty(g.shape[0])
+    _check(lib().rrref_pnof_energy_nonrel(ctypes.c_int(f), _i64(g.shape[0]), _p(g), _p(_d(occ)), _i64(n_sp),
+                                          _i64(Bmo_spatial.shape[0]), _p(_d(Bmo_spatial)), _p(_d(h)),
+                                          ctypes.byref(e), _p(grad)))
+    return e.value, grad

@@ -39,6 +39,8 @@
 #include "Restart.h"
 #include "CasFock.h"
 #include "PnofFock.h"
+#include "PNOFs.h"
+#include "Tensor4.h"
 #include "../include/rr_ri.h"
 
 extern "C" void scipy_openblas_set_num_threads(int n);
@@ -536,6 +538,39 @@ int rrref_pnof_full_two_rdm(int functional, i64 n_gem, const i64* gem, const dou
     fromMatrix(full.two_rdm_l2, l2);
     auto po = rerdmft::buildPnofPairOf(g, static_cast<std::size_t>(n_total));
     for (i64 i = 0; i < n_total; ++i) pair_of[i] = static_cast<i64>(po[i]);
+  });
+}
+
+// src/Occ_opt/PNOFs.cpp:271 pnofElectronicEnergy (with :212 buildPnofTwoRdm) and :463
+// pnofOccupationGradient for a non-relativistic spin-orbital problem: the RiNonRelSpinMoEri of Bmo (n_sp
+// spatial orbitals) expanded to the dense Tensor4<double> over its 2 n_sp accessors (the instantiations the
+// reference compiles), h 2n x 2n, occupations 2n; geminals n_gem x 4 as for rrref_pnof_full_two_rdm.
+int rrref_pnof_energy_nonrel(int functional, i64 n_gem, const i64* gem, const double* occ, i64 n_sp, i64 naux,
+                             const double* Bmo, const double* h, double* energy, double* grad) {
+  return guard([&] {
+    std::vector<rerdmft::PnofGeminal> g(static_cast<std::size_t>(n_gem));
+    for (i64 k = 0; k < n_gem; ++k)
+      g[k] = rerdmft::PnofGeminal{static_cast<std::size_t>(gem[4 * k]), static_cast<std::size_t>(gem[4 * k + 1]),
+                                  static_cast<std::size_t>(gem[4 * k + 2]), gem[4 * k + 3] != 0};
+    const rerdmft::PnofFunctional f = functional == 0 ? rerdmft::PnofFunctional::kPnof5
+                                      : functional == 1 ? rerdmft::PnofFunctional::kPnof7
+                                      : functional == 2 ? rerdmft::PnofFunctional::kPnof7s
+                                                        : rerdmft::PnofFunctional::kGnof;
+    rerdmft::RiNonRelSpinMoEri eri(static_cast<std::size_t>(n_sp), toMatrix(Bmo, naux, n_sp * n_sp));
+    const std::size_t d = static_cast<std::size_t>(2 * n_sp);
+    rerdmft::Tensor4<double> t(d, d, d, d);
+    for (std::size_t a = 0; a < d; ++a)
+      for (std::size_t b = 0; b < d; ++b)
+        for (std::size_t c = 0; c < d; ++c)
+          for (std::size_t e = 0; e < d; ++e) t(a, b, c, e) = eri(a, b, c, e);
+    const std::vector<double> o(occ, occ + d);
+    const auto H = toMatrix(h, static_cast<i64>(d), static_cast<i64>(d));
+    const auto two = rerdmft::buildPnofTwoRdm(f, g, o, false);
+    *energy = rerdmft::pnofElectronicEnergy(f, H, t, o, g, two, false);
+    if (grad) {
+      const auto gr = rerdmft::pnofOccupationGradient(f, H, t, o, g, false);
+      std::memcpy(grad, gr.data(), sizeof(double) * gr.size());
+    }
   });
 }
 

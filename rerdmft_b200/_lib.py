@@ -120,6 +120,8 @@ _SIGS = {
                                         ctypes.POINTER(_vp)]),
     "rr_orbopt_destroy": (ctypes.c_int, [_vp]),
     "rr_orbopt_exclude_negative": (ctypes.c_int, [_vp, _i64]),
+    "rr_orbopt_set_functional": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "rr_orbopt_jk": (ctypes.c_int, [_vp, _vp, _vp]),
     "rr_orbopt_info": (ctypes.c_int, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     "rr_orbopt_run": (ctypes.c_int, [_vp, ctypes.POINTER(AdamResult)]),
     "rr_orbopt_energy": (ctypes.c_int, [_vp, ctypes.POINTER(_d)]),

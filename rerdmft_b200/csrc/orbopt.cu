@@ -936,6 +936,42 @@ int rr_orbopt_exclude_negative(rr_orbopt_handle h, int64_t n_negative) {
   });
 }
 
+int rr_orbopt_set_functional(rr_orbopt_handle h, const double* occupations, const double* two_rdm_h,
+                             const double* two_rdm_x, const int64_t* pair_of, const double* two_rdm_l1,
+                             const double* two_rdm_l2) {
+  return guarded([&] {
+    auto* o = checked_opt(h);
+    RR_REQUIRE(occupations && two_rdm_h && two_rdm_x, RR_ERR_ARG, "rr_orbopt_set_functional: null argument");
+    RR_REQUIRE(!pair_of || (two_rdm_l1 && two_rdm_l2), RR_ERR_ARG,
+               "rr_orbopt_set_functional: pair_of needs two_rdm_l1 and two_rdm_l2");
+    const int64_t d = o->d, dd = d * d;
+    if (pair_of)
+      for (int64_t i = 0; i < d; ++i)
+        RR_REQUIRE(pair_of[i] >= 0 && pair_of[i] < d, RR_ERR_ARG, "rr_orbopt_set_functional: pair_of out of range");
+    cudaStream_t s = o->ctx.main;
+    rr::copy_in(o->occ, occupations, d, true, s);
+    rr::copy_in(o->h2, two_rdm_h, dd, true, s);
+    rr::copy_in(o->x2, two_rdm_x, dd, true, s);
+    o->have_l = pair_of != nullptr;
+    if (o->have_l) {
+      rr::copy_in(o->l1, two_rdm_l1, dd, true, s);
+      rr::copy_in(o->l2, two_rdm_l2, dd, true, s);
+      RR_CUDA(cudaMemcpyAsync(o->po, pair_of, sizeof(int64_t) * d, cudaMemcpyHostToDevice, s));
+    }
+    RR_CUDA(cudaStreamSynchronize(s));
+    o->fock_valid = false;
+  });
+}
+
+int rr_orbopt_jk(rr_orbopt_handle h, double* J, double* K) {
+  return guarded([&] {
+    auto* o = checked_opt(h);
+    RR_REQUIRE(J && K, RR_ERR_ARG, "rr_orbopt_jk: null output");
+    rr::mo_jkl(&o->mo, nullptr, J, K, nullptr, true, o->ctx.main);
+    RR_CUDA(cudaStreamSynchronize(o->ctx.main));
+  });
+}
+
 int rr_orbopt_destroy(rr_orbopt_handle h) {
   return guarded([&] {
     if (!h) return;

@@ -130,6 +130,36 @@ class RotationProblem:
             raise RrError(L.RR_ERR_ARG, "RotationProblem.set_scales: one scale per pair")
         L.check(L.lib().rr_orbopt_set_scales(self.handle, s.ctypes.data))
 
+    def set_functional(self, occupations, two_rdm_h, two_rdm_x, pair_of=None, two_rdm_l1=None, two_rdm_l2=None):
+        """New occupations and two-RDM factors for the next runs (orbitals, ADAM state and scales kept)."""
+        occ = _d(occupations)
+        h2, x2 = _d(two_rdm_h), _d(two_rdm_x)
+        if occ.shape != (self.d,) or h2.shape != (self.d, self.d) or x2.shape != (self.d, self.d):
+            raise RrError(L.RR_ERR_ARG, "RotationProblem.set_functional: shapes differ from the problem's")
+        po = None if pair_of is None else np.ascontiguousarray(pair_of, dtype=np.int64)
+        l1 = None if po is None else _d(two_rdm_l1)
+        l2 = None if po is None else _d(two_rdm_l2)
+        L.check(L.lib().rr_orbopt_set_functional(self.handle, occ.ctypes.data, h2.ctypes.data, x2.ctypes.data,
+                                                 None if po is None else po.ctypes.data,
+                                                 None if po is None else l1.ctypes.data,
+                                                 None if po is None else l2.ctypes.data))
+
+    def jk(self):
+        """J_ij = eri(i,j,i,j), K_ij = eri(i,j,j,i) of the current tensor (d x d)."""
+        J = np.empty((self.d, self.d), dtype=self._dt)
+        K = np.empty((self.d, self.d), dtype=self._dt)
+        L.check(L.lib().rr_orbopt_jk(self.handle, J.ctypes.data, K.ctypes.data))
+        return J, K
+
+    def jk_and_h_diag(self):
+        """(real J, real K, the diagonal of the current one-electron matrix over the d accessor orbitals)."""
+        J, K = self.jk()
+        _, h, _ = self.state()
+        hd = np.real(np.diag(h))
+        if not self.complex:
+            hd = np.concatenate([hd, hd])
+        return np.real(J), np.real(K), hd
+
     def state(self, with_tensor: bool = False):
         """(accumulated rotation, rotated h, rotated MO tensor or None)."""
         u = np.empty((self.n, self.n), dtype=self._dt)

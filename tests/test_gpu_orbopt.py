@@ -188,3 +188,45 @@ def test_learned_preconditioner_cuts_macro_iterations():
             assert abs(e["learned"] - e["plain"]) <= 1e-8
     assert tot["learned"] <= 0.70 * tot["plain"], tot  # at least 30 % fewer macro-iterations
     net.close()
+
+
+def _gnof_problem(n, nocc, coupling, seed, naux=24):
+    from rerdmft_b200 import pnof
+
+    f = synth.functional_system(n, naux, seed, nocc=nocc)
+    gem = pnof.nonrel_geminals(n, nocc, coupling)
+    occ0 = pnof.occupations_of(gem, coupling, np.full(nocc * (coupling - 1), np.pi / 4), 2 * n)
+    two = pnof.full_two_rdm(pnof.FUNCTIONALS["GNOF"], gem, occ0, 2 * n)
+    eri = mo.RiNonRelSpinMoEri.from_tensor(f["Bmo"], n)
+    prob = orbopt.RotationProblem(eri, f["h"], occ0, two["two_rdm_h"], two["two_rdm_x"], two["pair_of"],
+                                  two["two_rdm_l1"], two["two_rdm_l2"])
+    return f, gem, prob, eri
+
+
+def test_gnof_full_optimization_matches_reference_energy(ref_lib):
+    """GNOF FULL_OPTIMIZATION (device ADAM orbital runs, host occupation steps from the device J/K):
+    converged; the final energy is the reference's pnofElectronicEnergy at the final orbitals and
+    occupations, and the device rotation problem's energy (generalized-Fock trace with the full two-RDM)
+    is the same number; the learned preconditioner reaches the same energy."""
+    from rerdmft_b200 import pnof
+
+    n, nocc, coupling = 8, 2, 3
+    f, gem, prob, eri = _gnof_problem(n, nocc, coupling, 6)
+    r = pnof.run_pnof_optimization(prob, "GNOF", gem, coupling)
+    assert r["converged"]
+    u, hr, b = prob.state(with_tensor=True)
+    H = np.zeros((2 * n, 2 * n))
+    H[:n, :n] = hr
+    H[n:, n:] = hr
+    e_ref, _ = ref_lib.pnof_energy_nonrel("GNOF", gem, r["occupations"], b, n, H)
+    assert abs(r["energy"] - e_ref) <= 1e-10 * max(1.0, abs(e_ref))
+    assert abs(prob.energy() - e_ref) <= 1e-10 * max(1.0, abs(e_ref))
+    assert np.abs(prob.gradient()).max() < 1e-3
+    assert np.all(np.diff(r["history"][1:]) < 1e-7)  # macro-iteration energies do not rise
+    prob.close()
+    net = orbopt.load_default_preconditioner()
+    f, gem, prob, eri = _gnof_problem(n, nocc, coupling, 6)
+    rl = pnof.run_pnof_optimization(prob, "GNOF", gem, coupling, preconditioner=net)
+    assert rl["converged"] and abs(rl["energy"] - r["energy"]) <= 1e-7
+    prob.close()
+    net.close()
