@@ -32,7 +32,7 @@ N_AO, N_AUX, N_OCC, SEED = 400, 1600, 40, 2024
 # The half-transform kernel of the nonrelativistic exchange (RR_HALF_TRANSFORM selects it; m16 is the
 # library default) with the DRAM bytes (read + write) of one launch at this workload from its ncu
 # capture (B read once, T written once), None where no capture exists.
-HT_KIND = os.environ.get("RR_HALF_TRANSFORM", "m16")
+HT_KIND = os.environ.get("RR_HALF_TRANSFORM", "m16").split(":")[0]
 HT_KERNELS = {
     "m8": dict(kernel="dgemm_kernel half-transform T^P = Ct B^P (FP64 DMMA m8n8k4)",
                traffic=2.048888e9 + 0.194917e9, profile="profiles/dgemm_half_transform_n400_naux1600_nocc40.md"),

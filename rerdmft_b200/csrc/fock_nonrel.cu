@@ -72,7 +72,7 @@ void exchange_nonrel(rr_ri_store* h, const double* Ct, int64_t ldct, bool ct_tra
     coulomb_prep(h, Dp, Ct, nocc, Jout, true, s, true);  // side stream, beside the half-transform
   }
   if (!(tgam == nullptr && !ct_transposed && ldct == n && half_transform_kind() == 1 &&
-        half_transform_m16(Ct, nocc, h->B[0].p, h->pitch[0], naux, n, h->T.p, s)))
+        half_transform_m16(Ct, nocc, h->B[0].p, h->pitch[0], naux, n, h->T.p, s, half_transform_config())))
     gemm(ht, s);
   prof_mark(h, 2, s);
   if (Dp) coulomb_run(h, tgam, tseg, s);  // side stream, beside the SYRK

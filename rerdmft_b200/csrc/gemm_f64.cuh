@@ -70,5 +70,8 @@ bool half_transform_m16(const double* Ct, int64_t nocc, const double* B, int64_t
 // Which half-transform the nonrelativistic exchange uses: 0 = the general DMMA GEMM (m8n8k4),
 // 1 = half_transform_m16 (the default).  RR_HALF_TRANSFORM=m8|m16 overrides the default.
 int half_transform_kind();
+// The m16 tiling the exchange uses (config of half_transform_m16): 0 unless RR_HALF_TRANSFORM=m16:<config>
+// names another (for measurement).
+int half_transform_config();
 
 }  // namespace rr

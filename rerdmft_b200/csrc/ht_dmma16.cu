@@ -327,10 +327,21 @@ int half_transform_kind() {
   static const int kind = [] {
     const char* e = std::getenv("RR_HALF_TRANSFORM");
     if (e && std::string(e) == "m8") return 0;
-    if (e && std::string(e) == "m16") return 1;
-    return 1;  // 1.633 against 1.656 ms per n = 400, naux = 1600, nocc = 40 build (50 builds each)
+    return 1;  // m16 (two warps over a 5-stage ring: 1.633 against 1.656 ms per headline build for m8)
   }();
   return kind;
+}
+
+int half_transform_config() {
+  static const int cfg = [] {
+    const char* e = std::getenv("RR_HALF_TRANSFORM");
+    if (!e) return 0;
+    const std::string v(e);
+    if (v.rfind("m16:", 0) != 0) return 0;
+    const int c = std::atoi(v.c_str() + 4);
+    return c >= 0 && c <= 13 && c != 7 && c != 8 ? c : 0;  // 7 and 8 need a status word
+  }();
+  return cfg;
 }
 
 }  // namespace rr
