@@ -8,6 +8,8 @@
 //   join, F = h + J - K'   (K' = K/2 of the reference: its c_t carries sqrt(2)).
 #include <algorithm>
 
+#include <cstdlib>
+
 #include "ri_store.cuh"
 
 namespace rr {
@@ -356,8 +358,13 @@ void fock_nonrel(rr_ri_store* h, const double* hc, const double* D, const double
   // J from the density on the side stream (after the upload of D there), beside the occupied
   // recovery (X^T (S D S / 2) X, eigenvalues > 0.5) as c_t = F^T X^T on s, then the exchange.
   // One J CTA per SM: it shares the SMs with the recovery and then the half-transform (measured at
-  // n = 400, naux = 1600, nocc = 40: 1.67 ms per build with one, 1.70 with two, 1.81 with three).
-  constexpr int j_ctas = 1;
+  // n = 400, naux = 1600, nocc = 40: 1.67 ms per build with one, 1.70 with two, 1.81 with three);
+  // RR_J_CTAS=<k> sets another count for measurement.
+  static const int j_ctas = [] {
+    const char* e = std::getenv("RR_J_CTAS");
+    const int k = e ? std::atoi(e) : 1;
+    return k >= 1 && k <= 4 ? k : 1;
+  }();
   if (host) {
     auto& c = h->ctx;
     coulomb_early(h, Dp, J, c.side, j_ctas);
