@@ -61,10 +61,10 @@ int64_t gemm_work_doubles(const GemmDesc& d);
 // T[P] = Ct B^P for P < naux on the m16n8k8 FP64 shape (ht_dmma16.cu): Ct nocc x n (row pitch n), B^P
 // n x n in rows of `pitch` doubles, T[P] at T + P nocc n (row pitch n).  Returns false (nothing launched)
 // when the operands do not meet its 16-byte alignment rule.  config 0 is the default tiling (2 warps,
-// 16-deep k tiles, 5 stages); 1-6 are the alternatives kept for measurement: (warps, k depth, stages) =
+// 16-deep k tiles, 3 stages); 1-6 are the alternatives kept for measurement: (warps, k depth, stages) =
 // (1,16,4), (2,16,4), (5,32,2), (4,16,3), (1,32,3), (2,32,3); 7 and 8 the warp-specialised bulk-copy
 // pipeline with 4 and 3 stages (they need `status`, the device word a timed-out wait sets); 9-13:
-// (2,16,3), (5,16,3), (2,16,6), (4,16,4), (3,16,4).
+// (2,16,5), (5,16,3), (2,16,6), (4,16,4), (3,16,4).
 bool half_transform_m16(const double* Ct, int64_t nocc, const double* B, int64_t pitch, int64_t naux, int64_t n,
                         double* T, cudaStream_t s, int config = 0, int* status = nullptr);
 // Which half-transform the nonrelativistic exchange uses: 0 = the general DMMA GEMM (m8n8k4),

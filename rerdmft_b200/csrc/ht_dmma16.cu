@@ -5,10 +5,13 @@
 // cover any n that is a multiple of 16 without padding, unlike the occupied count), N = nocc (8-column
 // fragments), K = n.  Each warp owns a 16 x 40 block of T[P]^T (one A fragment and five B fragments per
 // k8 step) and stores it transposed into T[P] (nocc x n, row-major, the layout the exchange SYRK reads).
-// The default CTA is two such warps (32 AO columns) over a 5-stage cp.async ring of 16-deep k tiles of
-// B^P (rows k, AO columns contiguous) and of Ct: at n = 400, naux = 1600, nocc = 40 it measured 0.723 ms
-// against 0.824 ms for five warps over 3 stages and 0.76-1.19 ms for the other tilings kept for
-// measurement (half_transform_m16's config), the warp-specialised bulk-copy pipeline included.
+// The default CTA is two such warps (32 AO columns) over a 3-stage cp.async ring of 16-deep k tiles of
+// B^P (rows k, AO columns contiguous) and of Ct.  Timed alone at n = 400, naux = 1600, nocc = 40 a
+// 5-stage ring is the fastest tiling (0.723 ms against 0.824 ms for five warps over 3 stages and
+// 0.76-1.19 ms for the others kept for measurement, half_transform_m16's config, the warp-specialised
+// bulk-copy pipeline included); inside the Fock build, where the exchange overlaps the Coulomb passes on
+// another stream, the 3-stage ring (27 KB of shared memory a CTA against 45 KB) gave 1.565 ms a build
+// against 1.636 ms for the 5-stage one and 1.615-1.619 ms for (4,16,4) and (2,16,4).
 #include <algorithm>
 #include <cstdlib>
 #include <string>
@@ -313,12 +316,12 @@ bool half_transform_m16(const double* Ct, int64_t nocc, const double* B, int64_t
       if (!status) return false;
       launch_ht_tma<3>(a, naux, status, s);
       break;
-    case 9: launch_ht<2, 16, 3>(a, naux, s); break;
+    case 9: launch_ht<2, 16, 5>(a, naux, s); break;
     case 10: launch_ht<5, 16, 3>(a, naux, s); break;
     case 11: launch_ht<2, 16, 6>(a, naux, s); break;
     case 12: launch_ht<4, 16, 4>(a, naux, s); break;
     case 13: launch_ht<3, 16, 4>(a, naux, s); break;
-    default: launch_ht<2, 16, 5>(a, naux, s); break;
+    default: launch_ht<2, 16, 3>(a, naux, s); break;
   }
   return true;
 }
@@ -327,7 +330,7 @@ int half_transform_kind() {
   static const int kind = [] {
     const char* e = std::getenv("RR_HALF_TRANSFORM");
     if (e && std::string(e) == "m8") return 0;
-    return 1;  // m16 (two warps over a 5-stage ring: 1.633 against 1.656 ms per headline build for m8)
+    return 1;  // m16 (1.565 ms per headline build against 1.656 ms for m8)
   }();
   return kind;
 }
