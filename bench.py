@@ -37,7 +37,7 @@ HT_KERNELS = {
     "m8": dict(kernel="dgemm_kernel half-transform T^P = Ct B^P (FP64 DMMA m8n8k4)",
                traffic=2.048888e9 + 0.194917e9, profile="profiles/dgemm_half_transform_n400_naux1600_nocc40.md"),
     "m16": dict(kernel="ht_dmma16_kernel half-transform T^P = Ct B^P (FP64 DMMA m16n8k8)",
-                traffic=2.048240e9 + 0.196934e9,
+                traffic=2.048169e9 + 0.197358e9,
                 profile="profiles/ht_dmma16_half_transform_n400_naux1600_nocc40.md"),
 }
 HT = HT_KERNELS[HT_KIND]
