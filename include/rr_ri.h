@@ -133,6 +133,41 @@ int rr_ri_transform_ao_legs(const double* B_in, int64_t naux, int64_t n_ao, cons
 int rr_ri_create_raw(const double* raw, int64_t naux_raw, int64_t n_ao, const double* metric_x, int64_t naux_kept,
                      const double* t, int64_t n_out, int32_t mem, rr_ri_handle* out);
 
+/* A list of contracted Cartesian Gaussian functions, the reference's std::vector<BasisFunction>
+ * (src/AO_basis/MolecularBasis.h:13-22) flattened, in host memory: function i sits at center[3i..3i+2]
+ * (bohr) with Cartesian exponents lxyz[3i..3i+2] (l = lx + ly + lz <= 6) and the primitives
+ * [prim_offset[i], prim_offset[i+1]) of exponents / coefficients.  Coefficients are in libcint's
+ * convention, as normalizeCartesianBasis (src/AO_ints/Integrals.cpp:140-187) leaves them: the function is
+ * sum_p coefficient_p * f(l) * x^lx y^ly z^lz exp(-exponent_p r^2), f(0) = 1/sqrt(4 pi),
+ * f(1) = sqrt(3/(4 pi)), f(l >= 2) = 1.  Runs of consecutive functions forming one shell in libcint's
+ * component order (equal centre, l, exponents, proportional coefficients) are evaluated together. */
+typedef struct rr_basis {
+  int64_t n;
+  const double* center;
+  const int32_t* lxyz;
+  const int64_t* prim_offset; /* n + 1 entries, prim_offset[0] = 0 */
+  const double* exponents;
+  const double* coefficients;
+} rr_basis;
+
+/* The aux metric (P|Q), naux x naux: auxMetric, src/AO_ints/ThreeCenterIntegrals.cpp:140-161 (libcint
+ * cint2c2e_cart per shell pair there), on the GPU (McMurchie-Davidson, FP64).  opts->mem applies to
+ * `metric`. */
+int rr_int_aux_metric(const rr_basis* aux, double* metric, const rr_opts* opts);
+
+/* The raw 3-centre integrals raw[P, p n + q] = (pq|P), naux x n^2: threeCenterIntegralsRaw,
+ * src/AO_ints/ThreeCenterIntegrals.cpp:163-184 (libcint cint3c2e_cart there), on the GPU.  opts->mem
+ * applies to `raw` (RR_MEM_DEVICE keeps the naux n^2 doubles on the device, e.g. for rr_ri_create_raw). */
+int rr_int_three_center_raw(const rr_basis* basis, const rr_basis* aux, double* raw, const rr_opts* opts);
+
+/* A resident RI handle from the basis sets alone, everything on the device: the aux metric, its canonical
+ * orthogonalisation at metric_threshold (auxMetricOrthogonalization, ThreeCenterIntegrals.cpp:185-189;
+ * the reference passes 1e-10, main.cpp:1085), the raw 3-centre integrals and riThreeCenterTensor's
+ * contraction (:219-236), then t^T B^P t when t (host, n x n_out) is given, as rr_ri_create_raw.
+ * naux_kept (may be NULL): the aux functions kept; report (may be NULL): the metric's rank report. */
+int rr_ri_create_basis(const rr_basis* basis, const rr_basis* aux, double metric_threshold, const double* t,
+                       int64_t n_out, rr_ri_handle* out, int64_t* naux_kept, rr_rank_report* report);
+
 /* naux, n (nl for 4c) and ns (0 for a single-tensor handle). */
 int rr_ri_info(rr_ri_handle h, int64_t* naux, int64_t* n, int64_t* ns);
 

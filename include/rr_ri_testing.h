@@ -77,6 +77,10 @@ int rr_test_half_transform_time(const double* Ct, int64_t nocc, const double* B,
 int rr_test_wait_expiry(uint32_t spin_limit, int32_t threads, int32_t* status_word, double* elapsed_ms,
                         double* cycles);
 
+/* The device Boys function of the integral kernels: out[i (nmax+1) + n] = F_n(T[i]) for n <= nmax <= 18
+ * (host arrays). */
+int rr_test_boys(const double* T, int64_t count, int32_t nmax, double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -73,6 +73,12 @@ class RankReport(ctypes.Structure):
     _fields_ = [("n_kept", _i64), ("n_dropped", _i64), ("smallest_kept", _d), ("largest_dropped", _d)]
 
 
+class Basis(ctypes.Structure):
+    """rr_basis: a flattened BasisFunction list (host arrays)."""
+    _fields_ = [("n", _i64), ("center", _vp), ("lxyz", _vp), ("prim_offset", _vp), ("exponents", _vp),
+                ("coefficients", _vp)]
+
+
 class PairOp(ctypes.Structure):
     _fields_ = [("s", _vp), ("idx", _vp), ("w", _vp), ("row", _vp), ("post", _vp)]
 
@@ -161,6 +167,12 @@ _SIGS = {
     "rr_sigma_diag_contract": (ctypes.c_int, [_vp, _i64, _i64, _i32, _vp, _vp, _vp, ctypes.POINTER(Opts)]),
     "rr_sigma_accum_u": (ctypes.c_int, [_vp, _d, _i64, _i64, _i32, _vp, _vp, ctypes.POINTER(Opts)]),
     "rr_ri_create_raw": (ctypes.c_int, [_vp, _i64, _i64, _vp, _i64, _vp, _i64, _i32, ctypes.POINTER(_vp)]),
+    "rr_int_aux_metric": (ctypes.c_int, [ctypes.POINTER(Basis), _vp, ctypes.POINTER(Opts)]),
+    "rr_int_three_center_raw": (ctypes.c_int, [ctypes.POINTER(Basis), ctypes.POINTER(Basis), _vp,
+                                               ctypes.POINTER(Opts)]),
+    "rr_ri_create_basis": (ctypes.c_int, [ctypes.POINTER(Basis), ctypes.POINTER(Basis), _d, _vp, _i64,
+                                          ctypes.POINTER(_vp), ctypes.POINTER(_i64), ctypes.POINTER(RankReport)]),
+    "rr_test_boys": (ctypes.c_int, [_vp, _i64, _i32, _vp]),
     "rr_ri_info": (ctypes.c_int, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     "rr_ri_sync": (ctypes.c_int, [_vp]),
     "rr_ri_fock_nonrel": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _i64, _vp, ctypes.POINTER(Opts)]),

@@ -147,5 +147,9 @@ void eigh_herm(rr_ri_store* h, double* a, int64_t n, double* w, cudaStream_t s);
 // c.solver_info.
 void eigh_sym_ctx(Context& c, double* a, int64_t n, double* w, cudaStream_t s);
 void eigh_herm_ctx(Context& c, double* a, int64_t n, double* w, cudaStream_t s);
+// canonicalOrthogonalize(Hermitian) on the device (tensor_build.cu): X (n x n_eff, caller's n x n buffer),
+// opts->mem for S and X, opts->stream (or a private stream) for the work.
+void canonical_orthogonalize(const double* S, int64_t n, bool herm, double threshold, double* X, int64_t* n_eff_out,
+                             rr_rank_report* report, const rr_opts* o);
 
 }  // namespace rr

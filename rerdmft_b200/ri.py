@@ -94,14 +94,17 @@ class RiStore:
 
 
 class RiNonRelEriSource:
-    """src/NON_REL/NonRelFockMatrixRi.h:30: nl, eri3_L (n_aux, nl*nl), x_large, overlap."""
+    """src/NON_REL/NonRelFockMatrixRi.h:30: nl, eri3_L (n_aux, nl*nl), x_large, overlap.  store: an
+    already resident RiStore of the same tensor (e.g. integrals.store_from_basis) in place of eri3_L."""
 
-    def __init__(self, nl, eri3_L, x_large, overlap):
+    def __init__(self, nl, eri3_L, x_large, overlap, store: RiStore | None = None):
         self.nl = int(nl)
         self.eri3_L = eri3_L
         self.x_large = x_large
         self.overlap = overlap
-        self._store = None
+        self._store = store
+        if eri3_L is None and (store is None or store.n != self.nl or store.ns != 0):
+            raise RrError(L.RR_ERR_ARG, "RiNonRelEriSource: need eri3_L or a single-tensor store of nl functions")
 
     @property
     def store(self) -> RiStore:
@@ -117,7 +120,7 @@ def nonRelFockMatrix(h_core, eri: RiNonRelEriSource, density_matrix, stream: int
     nl = eri.nl
     if tuple(density_matrix.shape) != (nl, nl):
         raise RrError(L.RR_ERR_ARG, "nonRelFockMatrix (RI): density_matrix dimension does not match nl")
-    if eri.eri3_L.shape[1] != nl * nl:
+    if eri.eri3_L is not None and eri.eri3_L.shape[1] != nl * nl:
         raise RrError(L.RR_ERR_ARG, "nonRelFockMatrix (RI): eri3_L column count does not match nl^2")
     store = eri.store
     dev = _is_dev(density_matrix)
