@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -53,10 +54,12 @@ struct IntArgs {
   const double* map_sc;
   const int2* pairs;   // bra shell pairs (A, B); B = the unit shell for the metric
   int64_t npairs;
-  int c0, nc;          // ket shells [c0, c0 + nc)
+  const int* cidx;     // ket shells
+  int64_t nc;
   int metric;          // 1: (A|C) with C >= A, out = M (naux x naux); 0: (AB|C), out = raw (naux x n^2)
   int64_t n;           // orbital function count (raw) or aux count (metric)
   double* out;
+  const double* boys;  // Boys function table (boys_table)
   int la_max, lab_max, lc_max, L_max;  // shared-memory sizing
 };
 
@@ -106,6 +109,56 @@ __device__ void boys_eval(int nmax, double T, double* F) {
   for (int n = nmax - 1; n >= 0; --n) F[n] = (2.0 * T * F[n + 1] + e) / (2 * n + 1);
 }
 
+// Boys function table: F_n(T_k) for T_k = k / 20 (k = 0 .. 720, T_k <= 36) and n = 0 .. kMaxLSum + 6, from
+// the series above.  Between grid points F_n(T) = sum_{j=0}^{6} F_{n+j}(T_k) (T_k - T)^j / j! (dF_n/dT =
+// -F_{n+1}) at the nearest T_k (|T - T_k| <= 1/40: the remainder is below 1.3e-15 F_n), then the downward
+// recurrence; above T = 36 the asymptotic F_0 and the upward recurrence.
+constexpr int kBoysOrders = kMaxLSum + 7;
+constexpr int kBoysPoints = 721;
+constexpr double kBoysPerUnit = 20.0;
+
+__global__ void boys_table_kernel(double* tab) {
+  double F[kBoysOrders];
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < kBoysPoints; k += gridDim.x * blockDim.x) {
+    boys_eval(kBoysOrders - 1, k / kBoysPerUnit, F);
+    for (int n = 0; n < kBoysOrders; ++n) tab[k * kBoysOrders + n] = F[n];
+  }
+}
+
+__device__ __forceinline__ double boys_taylor(const double* row, double d) {
+  return row[0] + d * (row[1] + d * (1.0 / 2) * (row[2] + d * (1.0 / 3) * (row[3] + d * (1.0 / 4) *
+         (row[4] + d * (1.0 / 5) * (row[5] + d * (1.0 / 6) * row[6])))));
+}
+
+__device__ void boys_table_eval(int nmax, double T, const double* tab, double* F) {
+  const double e = exp(-T);
+  if (T >= 36.0) {
+    F[0] = 0.5 * sqrt(M_PI / T);
+    const double inv2t = 0.5 / T;
+    for (int n = 0; n < nmax; ++n) F[n + 1] = ((2 * n + 1) * F[n] - e) * inv2t;
+    return;
+  }
+  const int k = __double2int_rn(T * kBoysPerUnit);
+  F[nmax] = boys_taylor(tab + k * kBoysOrders + nmax, k / kBoysPerUnit - T);
+  for (int n = nmax - 1; n >= 0; --n) F[n] = (2.0 * T * F[n + 1] + e) / (2 * n + 1);
+}
+
+template <int N>
+__device__ __forceinline__ void boys_fixed(double T, const double* tab, double (&F)[N + 1]) {
+  const double e = exp(-T);
+  if (T >= 36.0) {
+    F[0] = 0.5 * sqrt(M_PI / T);
+    const double inv2t = 0.5 / T;
+#pragma unroll
+    for (int n = 0; n < N; ++n) F[n + 1] = ((2 * n + 1) * F[n] - e) * inv2t;
+    return;
+  }
+  const int k = __double2int_rn(T * kBoysPerUnit);
+  F[N] = boys_taylor(tab + k * kBoysOrders + N, k / kBoysPerUnit - T);
+#pragma unroll
+  for (int n = N - 1; n >= 0; --n) F[n] = (2.0 * T * F[n + 1] + e) * (1.0 / (2 * n + 1));
+}
+
 // E[i][j][t] (flat ((i (lb+1) + j) (la+lb+1) + t)) of one dimension, without K_AB.
 __device__ void e_table(double* E, int la, int lb, double p, double xpa, double xpb) {
   const int lt = la + lb + 1;
@@ -152,7 +205,7 @@ __global__ void __launch_bounds__(kIntThreads) eri_kernel(IntArgs a) {
   for (int64_t item = static_cast<int64_t>(blockIdx.x) * nwarp + warp; item < items;
        item += static_cast<int64_t>(gridDim.x) * nwarp) {
     const int2 pr = a.pairs[item / a.nc];
-    const int ic_sh = a.c0 + static_cast<int>(item % a.nc);
+    const int ic_sh = a.cidx[item % a.nc];
     if (a.metric && ic_sh < pr.x) continue;  // (P|Q) for Q >= P only
     const DShell A = a.sh[pr.x], B = a.sh[pr.y], C = a.sh[ic_sh];
     const bool sym = a.metric ? (ic_sh == pr.x) : (pr.x == pr.y);
@@ -181,7 +234,7 @@ __global__ void __launch_bounds__(kIntThreads) eri_kernel(IntArgs a) {
             const double alpha = p * ga / (p + ga);
             const double X = Px - C.x, Y = Py - C.y, Z = Pz - C.z;
             __syncwarp();
-            if (lane == 3) boys_eval(L, alpha * (X * X + Y * Y + Z * Z), F);
+            if (lane == 3) boys_table_eval(L, alpha * (X * X + Y * Y + Z * Z), a.boys, F);
             if (lane == 4) {  // single-centre Hermite expansion of the aux factor: Ec[i][t]
               const double inv2q = 0.5 / ga;
               for (int ii = 0; ii <= C.l; ++ii)
@@ -290,14 +343,260 @@ __global__ void __launch_bounds__(kIntThreads) eri_kernel(IntArgs a) {
   }
 }
 
-// Test hook kernel: F_n(T) for every T of a list.
-__global__ void boys_kernel(const double* T, int64_t count, int nmax, double* out) {
+// Test hook kernel: F_n(T) for every T of a list, as the integral kernels evaluate it (table path).
+__global__ void boys_kernel(const double* T, int64_t count, int nmax, const double* tab, double* out) {
   double F[kMaxLSum + 1];
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < count;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    boys_eval(nmax, T[i], F);
+    boys_table_eval(nmax, T[i], tab, F);
     for (int n = 0; n <= nmax; ++n) out[i * (nmax + 1) + n] = F[n];
   }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Thread-per-item kernels for the low angular-momentum classes, where most primitive triples are:
+// one thread computes every output of one (orbital shell pair, aux shell), all tables in registers,
+// every loop over components and Hermite indices unrolled at compile time.
+
+template <int L>
+struct Cart {
+  static constexpr int N = (L + 1) * (L + 2) / 2;
+  int x[N], y[N], z[N];
+  constexpr Cart() : x(), y(), z() {
+    int k = 0;
+    for (int a = L; a >= 0; --a)
+      for (int b = L - a; b >= 0; --b) {
+        x[k] = a;
+        y[k] = b;
+        z[k] = L - a - b;
+        ++k;
+      }
+  }
+};
+
+__host__ __device__ constexpr int rix(int t, int u, int v) {
+  return (t + u + v) * (t + u + v + 1) * (t + u + v + 2) / 6 + (u + v) * (u + v + 1) / 2 + v;
+}
+
+struct ClassArgs {
+  const DShell* sh;
+  const double* ex;
+  const double* co;
+  const int* map_fn;
+  const double* map_sc;
+  const int2* pairs;  // (A, B) with l_A >= l_B
+  int64_t npairs;
+  const int* cidx;    // aux shells of the class's l
+  int64_t ncs;
+  int64_t n;
+  double* out;
+  const double* boys;
+};
+
+// E^ab of one dimension for the compile-time (LA, LB): E[i][j][t].
+template <int LA, int LB>
+__device__ __forceinline__ void e_fixed(double (&E)[LA + 1][LB + 1][LA + LB + 1], double inv2p, double xpa,
+                                       double xpb) {
+#pragma unroll
+  for (int i = 0; i <= LA; ++i)
+#pragma unroll
+    for (int j = 0; j <= LB; ++j)
+#pragma unroll
+      for (int t = 0; t <= LA + LB; ++t) {
+        double v;
+        if (i == 0 && j == 0) {
+          v = t == 0 ? 1.0 : 0.0;
+        } else if (t > i + j) {
+          v = 0.0;
+        } else if (i > 0) {
+          v = xpa * E[i - 1][j][t];
+          if (t > 0) v += inv2p * E[i - 1][j][t - 1];
+          if (t + 1 <= i + j - 1) v += (t + 1) * E[i - 1][j][t + 1];
+        } else {
+          v = xpb * E[i][j - 1][t];
+          if (t > 0) v += inv2p * E[i][j - 1][t - 1];
+          if (t + 1 <= i + j - 1) v += (t + 1) * E[i][j - 1][t + 1];
+        }
+        E[i][j][t] = v;
+      }
+}
+
+template <int LA, int LB, int LC>
+__global__ void __launch_bounds__(128) eri_class_kernel(ClassArgs a) {
+  constexpr int NA = Cart<LA>::N, NB = Cart<LB>::N, NC = Cart<LC>::N;
+  constexpr int LAB = LA + LB, L = LAB + LC;
+  constexpr int NR = (L + 1) * (L + 2) * (L + 3) / 6, NG = (LAB + 1) * (LAB + 2) * (LAB + 3) / 6;
+  constexpr Cart<LA> ca{};
+  constexpr Cart<LB> cb{};
+  constexpr Cart<LC> cc{};
+  const double two_pi25 = 2.0 * M_PI * M_PI * sqrt(M_PI);
+  const int64_t total = a.npairs * a.ncs;
+  for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < total;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int2 pr = a.pairs[idx % a.npairs];
+    const int csh = a.cidx[idx / a.npairs];
+    const DShell A = a.sh[pr.x], B = a.sh[pr.y], C = a.sh[csh];
+    double acc[NA * NB * NC];
+#pragma unroll
+    for (int q = 0; q < NA * NB * NC; ++q) acc[q] = 0.0;
+    const double ab[3] = {A.x - B.x, A.y - B.y, A.z - B.z};
+    const double ab2 = ab[0] * ab[0] + ab[1] * ab[1] + ab[2] * ab[2];
+    for (int i = 0; i < A.nprim; ++i) {
+      const double al = a.ex[A.prim0 + i], cA = a.co[A.prim0 + i];
+      for (int j = 0; j < B.nprim; ++j) {
+        const double be = a.ex[B.prim0 + j], cB = a.co[B.prim0 + j];
+        const double p = al + be, ip = 1.0 / p;
+        const double P[3] = {(al * A.x + be * B.x) * ip, (al * A.y + be * B.y) * ip, (al * A.z + be * B.z) * ip};
+        const double K = exp(-al * be * ip * ab2);
+        double E[3][LA + 1][LB + 1][LAB + 1];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) e_fixed<LA, LB>(E[d], 0.5 * ip, -be * ip * ab[d], al * ip * ab[d]);
+        for (int k = 0; k < C.nprim; ++k) {
+          const double ga = a.ex[C.prim0 + k], cC = a.co[C.prim0 + k];
+          const double alpha = p * ga / (p + ga);
+          const double X = P[0] - C.x, Y = P[1] - C.y, Z = P[2] - C.z;
+          double F[L + 1];
+          boys_fixed<L>(alpha * (X * X + Y * Y + Z * Z), a.boys, F);
+          double pw[L + 1];
+          pw[0] = 1.0;
+#pragma unroll
+          for (int n = 1; n <= L; ++n) pw[n] = pw[n - 1] * (-2.0 * alpha);
+          double R[NR];
+          R[0] = pw[L] * F[L];
+#pragma unroll
+          for (int n = L - 1; n >= 0; --n) {
+#pragma unroll
+            for (int sl = L - n; sl >= 1; --sl)
+#pragma unroll
+              for (int m = 0; m <= sl; ++m)
+#pragma unroll
+                for (int v = 0; v <= m; ++v) {
+                  const int u = m - v, t = sl - m;
+                  double val;
+                  if (t > 0) {
+                    val = X * R[rix(t - 1, u, v)];
+                    if (t > 1) val += (t - 1) * R[rix(t - 2, u, v)];
+                  } else if (u > 0) {
+                    val = Y * R[rix(t, u - 1, v)];
+                    if (u > 1) val += (u - 1) * R[rix(t, u - 2, v)];
+                  } else {
+                    val = Z * R[rix(t, u, v - 1)];
+                    if (v > 1) val += (v - 1) * R[rix(t, u, v - 2)];
+                  }
+                  R[rix(t, u, v)] = val;
+                }
+            R[0] = pw[n] * F[n];
+          }
+          // single-centre Hermite coefficients of the aux factor, Ec[i][t] (t = i, i - 2, ...)
+          double Ec[LC + 1][LC + 1];
+          const double inv2q = 0.5 / ga;
+#pragma unroll
+          for (int ii = 0; ii <= LC; ++ii)
+#pragma unroll
+            for (int t = 0; t <= LC; ++t) {
+              double v = 0.0;
+              if (ii == 0) {
+                v = t == 0 ? 1.0 : 0.0;
+              } else {
+                if (t > 0) v += inv2q * Ec[ii - 1][t - 1];
+                if (t + 1 <= LC) v += (t + 1) * Ec[ii - 1][t + 1];
+              }
+              Ec[ii][t] = v;
+            }
+          const double w = cA * cB * cC * two_pi25 / (p * ga * sqrt(p + ga)) * K;
+#pragma unroll
+          for (int ic = 0; ic < NC; ++ic) {
+            const int cx = cc.x[ic], cy = cc.y[ic], cz = cc.z[ic];
+            double G[NG];
+#pragma unroll
+            for (int sl = 0; sl <= LAB; ++sl)
+#pragma unroll
+              for (int m = 0; m <= sl; ++m)
+#pragma unroll
+                for (int v = 0; v <= m; ++v) {
+                  const int u = m - v, t = sl - m;
+                  double g = 0.0;
+#pragma unroll
+                  for (int tau = cx & 1; tau <= cx; tau += 2)
+#pragma unroll
+                    for (int nu = cy & 1; nu <= cy; nu += 2)
+#pragma unroll
+                      for (int phi = cz & 1; phi <= cz; phi += 2) {
+                        const double ec = Ec[cx][tau] * Ec[cy][nu] * Ec[cz][phi];
+                        const double r = R[rix(t + tau, u + nu, v + phi)];
+                        g += ((tau + nu + phi) & 1) ? -ec * r : ec * r;
+                      }
+                  G[rix(t, u, v)] = g;
+                }
+#pragma unroll
+            for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+              for (int ib = 0; ib < NB; ++ib) {
+                const int ax = ca.x[ia], ay = ca.y[ia], az = ca.z[ia], bx = cb.x[ib], by = cb.y[ib], bz = cb.z[ib];
+                double val = 0.0;
+#pragma unroll
+                for (int t = 0; t <= ax + bx; ++t)
+#pragma unroll
+                  for (int u = 0; u <= ay + by; ++u)
+#pragma unroll
+                    for (int v = 0; v <= az + bz; ++v)
+                      val += E[0][ax][bx][t] * E[1][ay][by][u] * E[2][az][bz][v] * G[rix(t, u, v)];
+                acc[(ia * NB + ib) * NC + ic] += w * val;
+              }
+          }
+        }
+      }
+    }
+    const bool sym = pr.x == pr.y;
+#pragma unroll
+    for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+      for (int ib = 0; ib < NB; ++ib) {
+        if (sym && ia > ib) continue;
+        const int fa = a.map_fn[A.map0 + ia], fb = a.map_fn[B.map0 + ib];
+        if (fa < 0 || fb < 0) continue;
+        const double sab = a.map_sc[A.map0 + ia] * a.map_sc[B.map0 + ib];
+#pragma unroll
+        for (int ic = 0; ic < NC; ++ic) {
+          const int fc = a.map_fn[C.map0 + ic];
+          if (fc < 0) continue;
+          const double v = acc[(ia * NB + ib) * NC + ic] * sab * a.map_sc[C.map0 + ic];
+          const int64_t row = static_cast<int64_t>(fc) * a.n * a.n;
+          a.out[row + static_cast<int64_t>(fa) * a.n + fb] = v;
+          a.out[row + static_cast<int64_t>(fb) * a.n + fa] = v;
+        }
+      }
+  }
+}
+
+// The classes with a thread-per-item kernel (l_A >= l_B): the s and p pairs with aux s .. f, (pp| s, p),
+// (ds| s, p).  The others (more outputs, few primitives) take the warp kernel.
+template <int LA, int LB, int LC>
+void launch_class(const ClassArgs& a, cudaStream_t s) {
+  auto kern = eri_class_kernel<LA, LB, LC>;
+  static int per_sm[kMaxDevices] = {};
+  const int dev = current_device();
+  if (!per_sm[dev]) RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[dev], kern, 128, 0));
+  int sms = 0;
+  RR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int64_t total = a.npairs * a.ncs;
+  const int grid = static_cast<int>(std::max<int64_t>(
+      1, std::min<int64_t>((total + 127) / 128, static_cast<int64_t>(sms) * std::max(per_sm[dev], 1) * 8)));
+  kern<<<grid, 128, 0, s>>>(a);
+  RR_LAUNCH_CHECK();
+}
+
+bool launch_class_any(int la, int lb, int lc, const ClassArgs& a, cudaStream_t s) {
+#define RR_CLASS(A, B, C)                  \
+  if (la == A && lb == B && lc == C) {     \
+    launch_class<A, B, C>(a, s);           \
+    return true;                           \
+  }
+  RR_CLASS(0, 0, 0) RR_CLASS(0, 0, 1) RR_CLASS(0, 0, 2) RR_CLASS(0, 0, 3)
+  RR_CLASS(1, 0, 0) RR_CLASS(1, 0, 1) RR_CLASS(1, 0, 2) RR_CLASS(1, 0, 3)
+  RR_CLASS(1, 1, 0) RR_CLASS(1, 1, 1) RR_CLASS(2, 0, 0) RR_CLASS(2, 0, 1)
+#undef RR_CLASS
+  return false;
 }
 
 double common_factor(int l) {
@@ -420,33 +719,55 @@ void upload(DevBuf<T>& d, const std::vector<T>& h, cudaStream_t s) {
   if (!h.empty()) RR_CUDA(cudaMemcpyAsync(d.p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, s));
 }
 
-// Launches eri_kernel over pairs x ket shells [c0, c0 + nc) of the combined table.
-void launch_eri(const HostShells& all, const std::vector<int2>& pairs, int c0, int nc, int la_max, int lc_max,
-                bool metric, int64_t n, double* out, cudaStream_t s) {
-  if (pairs.empty() || nc == 0) return;
-  DevBuf<DShell> dsh;
-  DevBuf<double> dex, dco, dsc;
-  DevBuf<int> dfn;
-  DevBuf<int2> dpairs;
-  upload(dsh, all.sh, s);
-  upload(dex, all.ex, s);
-  upload(dco, all.co, s);
-  upload(dsc, all.sc, s);
-  upload(dfn, all.fn, s);
-  upload(dpairs, pairs, s);
+// The Boys table of the current device, built once (kept until exit, 144 KB).
+const double* boys_table(cudaStream_t s) {
+  static double* tab[kMaxDevices] = {};
+  static std::mutex mu;
+  const int dev = current_device();
+  std::lock_guard<std::mutex> lock(mu);
+  if (!tab[dev]) {
+    double* t = nullptr;
+    RR_CUDA(cudaMalloc(&t, sizeof(double) * kBoysPoints * kBoysOrders));
+    boys_table_kernel<<<(kBoysPoints + 127) / 128, 128, 0, s>>>(t);
+    RR_LAUNCH_CHECK();
+    RR_CUDA(cudaStreamSynchronize(s));
+    tab[dev] = t;
+  }
+  return tab[dev];
+}
+
+// Device copy of the combined shell table.
+struct DevShells {
+  DevBuf<DShell> sh;
+  DevBuf<double> ex, co, sc;
+  DevBuf<int> fn;
+  DevShells(const HostShells& all, cudaStream_t s) {
+    upload(sh, all.sh, s);
+    upload(ex, all.ex, s);
+    upload(co, all.co, s);
+    upload(sc, all.sc, s);
+    upload(fn, all.fn, s);
+  }
+};
+
+// Launches eri_kernel (warp per item) over pairs x the ket shells `cidx` (device list of nc).
+void launch_eri(const DevShells& d, const int2* pairs, int64_t npairs, const int* cidx, int64_t nc, int la_max,
+                int lc_max, bool metric, int64_t n, double* out, const double* boys, cudaStream_t s) {
+  if (npairs == 0 || nc == 0) return;
   IntArgs a{};
-  a.sh = dsh.p;
-  a.ex = dex.p;
-  a.co = dco.p;
-  a.map_fn = dfn.p;
-  a.map_sc = dsc.p;
-  a.pairs = dpairs.p;
-  a.npairs = static_cast<int64_t>(pairs.size());
-  a.c0 = c0;
+  a.sh = d.sh.p;
+  a.ex = d.ex.p;
+  a.co = d.co.p;
+  a.map_fn = d.fn.p;
+  a.map_sc = d.sc.p;
+  a.pairs = pairs;
+  a.npairs = npairs;
+  a.cidx = cidx;
   a.nc = nc;
   a.metric = metric ? 1 : 0;
   a.n = n;
   a.out = out;
+  a.boys = boys;
   a.la_max = la_max;
   a.lab_max = 2 * la_max;
   a.lc_max = lc_max;
@@ -458,16 +779,16 @@ void launch_eri(const HostShells& all, const std::vector<int2>& pairs, int c0, i
   const size_t smem = sizeof(double) * per_warp * (kIntThreads / 32);
   RR_REQUIRE(smem <= 227 * 1024, RR_ERR_ARG, "integrals: angular momenta too high for the shared-memory tables");
   RR_CUDA(cudaFuncSetAttribute(eri_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-  int sms = 0, dev = 0, per_sm = 0;
-  RR_CUDA(cudaGetDevice(&dev));
+  int sms = 0, per_sm = 0;
+  const int dev = current_device();
   RR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eri_kernel, kIntThreads, smem));
-  const int64_t items = a.npairs * nc;
+  const int64_t items = npairs * nc;
   const int64_t want = (items + kIntThreads / 32 - 1) / (kIntThreads / 32);
-  const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(want, static_cast<int64_t>(sms) * std::max(per_sm, 1) * 4)));
+  const int grid = static_cast<int>(
+      std::max<int64_t>(1, std::min<int64_t>(want, static_cast<int64_t>(sms) * std::max(per_sm, 1) * 4)));
   eri_kernel<<<grid, kIntThreads, smem, s>>>(a);
   RR_LAUNCH_CHECK();
-  RR_CUDA(cudaStreamSynchronize(s));  // the tables are freed on return
 }
 
 struct IntCtx {
@@ -494,10 +815,11 @@ void aux_metric_device(const rr_basis* aux, double* M, cudaStream_t s) {
   group_shells(aux, "auxMetric", hs);
   const int na = static_cast<int>(hs.sh.size());
   if (na == 0) return;
+  const double* boys = boys_table(s);
   // the constant function 1 as the second bra factor: one primitive of exponent 0, coefficient 1
+  // (beta = 0 makes its centre irrelevant: P = A, K = 1)
   HostShells unit;
-  DShell u{0.0, 0.0, 0.0, 0, 1, 0, 0};
-  unit.sh.push_back(u);
+  unit.sh.push_back(DShell{0.0, 0.0, 0.0, 0, 1, 0, 0});
   unit.ex.push_back(0.0);
   unit.co.push_back(1.0);
   unit.fn.push_back(-1);
@@ -506,9 +828,18 @@ void aux_metric_device(const rr_basis* aux, double* M, cudaStream_t s) {
   const int iu = static_cast<int>(all.sh.size());
   append_shells(all, unit);
   std::vector<int2> pairs(na);
-  for (int i = 0; i < na; ++i) pairs[i] = make_int2(i, iu);
-  // the unit shell sits at each bra's own centre: P = A, K = 1 (beta = 0 makes the centre irrelevant)
-  launch_eri(all, pairs, 0, na, hs.lmax, hs.lmax, true, aux->n, M, s);
+  std::vector<int> cidx(na);
+  for (int i = 0; i < na; ++i) {
+    pairs[i] = make_int2(i, iu);
+    cidx[i] = i;
+  }
+  DevShells d(all, s);
+  DevBuf<int2> dp;
+  DevBuf<int> dc;
+  upload(dp, pairs, s);
+  upload(dc, cidx, s);
+  launch_eri(d, dp.p, na, dc.p, na, hs.lmax, hs.lmax, true, aux->n, M, boys, s);
+  RR_CUDA(cudaStreamSynchronize(s));  // the tables are freed on return
 }
 
 void three_center_raw_device(const rr_basis* orb, const rr_basis* aux, double* raw, cudaStream_t s) {
@@ -517,13 +848,57 @@ void three_center_raw_device(const rr_basis* orb, const rr_basis* aux, double* r
   group_shells(aux, "threeCenterIntegralsRaw (aux basis)", ha);
   const int no = static_cast<int>(ho.sh.size()), na = static_cast<int>(ha.sh.size());
   if (no == 0 || na == 0) return;
+  const double* boys = boys_table(s);
   HostShells all = ho;
   append_shells(all, ha);
-  std::vector<int2> pairs;
-  pairs.reserve(static_cast<size_t>(no) * (no + 1) / 2);
+  // pairs (i <= j) by class (l_A >= l_B after a swap: both halves of the pq symmetry are written),
+  // within a class by primitive count (threads of a warp loop alike); aux shells by l
+  std::vector<std::vector<int2>> by_class((kMaxL + 1) * (kMaxL + 1));
   for (int i = 0; i < no; ++i)
-    for (int j = i; j < no; ++j) pairs.push_back(make_int2(i, j));
-  launch_eri(all, pairs, no, na, ho.lmax, ha.lmax, false, orb->n, raw, s);
+    for (int j = i; j < no; ++j) {
+      int a = i, b = j;
+      if (ho.sh[a].l < ho.sh[b].l) std::swap(a, b);
+      by_class[ho.sh[a].l * (kMaxL + 1) + ho.sh[b].l].push_back(make_int2(a, b));
+    }
+  std::vector<std::vector<int>> aux_by_l(kMaxL + 1);
+  for (int c = 0; c < na; ++c) aux_by_l[ha.sh[c].l].push_back(no + c);
+  std::vector<int2> pairs;
+  std::vector<int> cidx;
+  struct Range { int la, lb; int64_t p0, np; };
+  std::vector<Range> ranges;
+  for (int la = 0; la <= kMaxL; ++la)
+    for (int lb = 0; lb <= la; ++lb) {
+      auto& v = by_class[la * (kMaxL + 1) + lb];
+      if (v.empty()) continue;
+      std::stable_sort(v.begin(), v.end(), [&](int2 x, int2 y) {
+        return ho.sh[x.x].nprim * ho.sh[x.y].nprim > ho.sh[y.x].nprim * ho.sh[y.y].nprim;
+      });
+      ranges.push_back(Range{la, lb, static_cast<int64_t>(pairs.size()), static_cast<int64_t>(v.size())});
+      pairs.insert(pairs.end(), v.begin(), v.end());
+    }
+  std::vector<int64_t> c0(kMaxL + 2, 0);
+  for (int l = 0; l <= kMaxL; ++l) {
+    c0[l + 1] = c0[l] + static_cast<int64_t>(aux_by_l[l].size());
+    cidx.insert(cidx.end(), aux_by_l[l].begin(), aux_by_l[l].end());
+  }
+  DevShells d(all, s);
+  DevBuf<int2> dp;
+  DevBuf<int> dc;
+  upload(dp, pairs, s);
+  upload(dc, cidx, s);
+  ClassArgs ca{d.sh.p, d.ex.p, d.co.p, d.fn.p, d.sc.p, nullptr, 0, nullptr, 0, orb->n, raw, boys};
+  for (const Range& r : ranges)
+    for (int lc = 0; lc <= kMaxL; ++lc) {
+      const int64_t nc = c0[lc + 1] - c0[lc];
+      if (nc == 0) continue;
+      ca.pairs = dp.p + r.p0;
+      ca.npairs = r.np;
+      ca.cidx = dc.p + c0[lc];
+      ca.ncs = nc;
+      if (!launch_class_any(r.la, r.lb, lc, ca, s))
+        launch_eri(d, dp.p + r.p0, r.np, dc.p + c0[lc], nc, ho.lmax, ha.lmax, false, orb->n, raw, boys, s);
+    }
+  RR_CUDA(cudaStreamSynchronize(s));  // the tables are freed on return
 }
 
 template <typename F>
@@ -633,7 +1008,9 @@ int rr_test_boys(const double* T, int64_t count, int32_t nmax, double* out) {
     if (count == 0) return;
     rr::DevBuf<double> dT(static_cast<size_t>(count)), dF(static_cast<size_t>(count * (nmax + 1)));
     RR_CUDA(cudaMemcpy(dT.p, T, sizeof(double) * count, cudaMemcpyHostToDevice));
-    rr::boys_kernel<<<static_cast<int>(std::min<int64_t>((count + 127) / 128, 1184)), 128>>>(dT.p, count, nmax, dF.p);
+    const double* tab = rr::boys_table(nullptr);
+    rr::boys_kernel<<<static_cast<int>(std::min<int64_t>((count + 127) / 128, 1184)), 128>>>(dT.p, count, nmax, tab,
+                                                                                          dF.p);
     RR_LAUNCH_CHECK();
     RR_CUDA(cudaMemcpy(out, dF.p, sizeof(double) * count * (nmax + 1), cudaMemcpyDeviceToHost));
   });
