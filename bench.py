@@ -351,6 +351,31 @@ def gnof_optimization_block():
     return out
 
 
+def water_cluster(waters: int):
+    """(H2O)_waters / cc-pVDZ (Cartesian) on a cubic grid 3 Angstrom apart, with its PAUTO aux basis: the
+    orbital basis, the aux basis (both normalised as the reference normalises them) and the geometry.
+    The basis data are the fixture tests/golden/water_ccpvdz.npz (the reference's example basis file)."""
+    from rerdmft_b200 import basis as bs
+
+    z = np.load(ROOT / "tests" / "golden" / "water_ccpvdz.npz")
+    sets, off = {}, 0
+    for el, l, npr in zip(z["shell_element"], z["shell_l"], z["shell_nprim"]):
+        sets.setdefault(str(el), []).append(bs.Shell(int(l), [float(v) for v in z["exponents"][off:off + npr]],
+                                                     [float(v) for v in z["coefficients"][off:off + npr]]))
+        off += int(npr)
+    mol = [(str(s), *map(float, xyz)) for s, xyz in zip(z["atom_symbol"], z["atom_xyz"])]
+    k = int(np.ceil(waters ** (1.0 / 3.0) - 1e-9))
+    geo = []
+    for i in range(waters):
+        sh = np.array([i % k, (i // k) % k, i // (k * k)]) * 3.0 * bs.ANGSTROM_TO_BOHR
+        geo += [bs.Atom(s, x + sh[0], y + sh[1], zz + sh[2]) for s, x, y, zz in mol]
+    orb = bs.build_molecular_basis(geo, sets)
+    bs.normalize_cartesian_basis(orb)
+    aux = bs.build_auto_auxiliary_basis(orb, "PAUTO")
+    bs.normalize_cartesian_basis(aux)
+    return orb, aux, geo
+
+
 def x2c_batch_problems(count: int = 64):
     """The batched X2C-HF geometry scan: `count` instances with uneven nl in [20, 120] (seeded), naux = 4 nl,
     4 or 14 electrons (LiH- / CO-like) alternating, one handle each (uploaded here)."""
@@ -707,7 +732,9 @@ def run_case(args):
     rkb_fp64      the same 4c RKB Fock build in FP64 (the 4c Fock-build workload of the bench line);
     x2c_mixed     the X2C Fock build with the split-BF16 exchange, full then incremental (nl=200,
                   naux=1000, 80 electrons);
-    x2c_batch     the lockstep grouped X2C-HF scan (64 uneven instances), tuned then timed once."""
+    x2c_batch     the lockstep grouped X2C-HF scan (64 uneven instances), tuned then timed once;
+    integrals     the raw 3-centre integrals and the aux metric of (H2O)_8 / cc-pVDZ with its PAUTO aux basis
+                  (n = 200, naux = 2856; RR_WATERS=<k> for another cluster), device outputs."""
     import ctypes
 
     import torch
@@ -732,6 +759,25 @@ def run_case(args):
         return e0.elapsed_time(e1) / steps
 
     out = dict(case=args.case, steps=args.steps, warmup=args.warmup)
+    if args.case == "integrals":
+        from rerdmft_b200 import integrals as gi
+
+        waters = int(os.environ.get("RR_WATERS", "8"))
+        orb, aux, _ = water_cluster(waters)
+        n, na = len(orb), len(aux)
+        co, ca = gi._CBasis(orb), gi._CBasis(aux)
+        raw = torch.empty((na, n * n), dtype=torch.float64, device="cuda")
+        M = torch.empty((na, na), dtype=torch.float64, device="cuda")
+        o = L.opts(L.RR_MEM_DEVICE, stream=stream)
+        ms_raw = timed(lambda: L.check(lib.rr_int_three_center_raw(ctypes.byref(co.c), ctypes.byref(ca.c),
+                                                                   raw.data_ptr(), ctypes.byref(o))),
+                       args.steps, args.warmup)
+        ms_m = timed(lambda: L.check(lib.rr_int_aux_metric(ctypes.byref(ca.c), M.data_ptr(), ctypes.byref(o))),
+                     args.steps, args.warmup)
+        out.update(workload=f"(H2O)_{waters} cc-pVDZ raw 3-centre integrals n={n} naux={na}", ms_raw=ms_raw,
+                   ms_metric=ms_m, raw_gb=na * n * n * 8 / 1e9)
+        print(json.dumps(out))
+        return
     if args.case == "x2c_batch":
         from rerdmft_b200 import scf
 
@@ -824,7 +870,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--case", default=None, choices=["headline", "mixed_exchange", "rkb_mixed", "rkb_fp64", "x2c_mixed",
-                                                    "x2c_batch"],
+                                                    "x2c_batch", "integrals"],
                     help="run one workload for profiling instead of the bench line")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)

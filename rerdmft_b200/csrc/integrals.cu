@@ -361,18 +361,19 @@ __global__ void boys_kernel(const double* T, int64_t count, int nmax, const doub
 template <int L>
 struct Cart {
   static constexpr int N = (L + 1) * (L + 2) / 2;
-  int x[N], y[N], z[N];
-  constexpr Cart() : x(), y(), z() {
-    int k = 0;
-    for (int a = L; a >= 0; --a)
-      for (int b = L - a; b >= 0; --b) {
-        x[k] = a;
-        y[k] = b;
-        z[k] = L - a - b;
-        ++k;
-      }
-  }
 };
+
+// Exponent d (0: x, 1: y, 2: z) of Cartesian component k of angular momentum l in libcint's order; a
+// plain function, correct whether the compiler folds it or evaluates it at run time.
+__host__ __device__ constexpr int cart_comp(int l, int k, int d) {
+  int idx = 0;
+  for (int a = l; a >= 0; --a)
+    for (int b = l - a; b >= 0; --b) {
+      if (idx == k) return d == 0 ? a : (d == 1 ? b : l - a - b);
+      ++idx;
+    }
+  return 0;
+}
 
 __host__ __device__ constexpr int rix(int t, int u, int v) {
   return (t + u + v) * (t + u + v + 1) * (t + u + v + 2) / 6 + (u + v) * (u + v + 1) / 2 + v;
@@ -421,24 +422,99 @@ __device__ __forceinline__ void e_fixed(double (&E)[LA + 1][LB + 1][LA + LB + 1]
       }
 }
 
-template <int LA, int LB, int LC>
+__host__ __device__ constexpr int n_herm(int l) { return (l + 1) * (l + 2) * (l + 3) / 6; }
+
+// acc[(ia NB + ib) STRIDE] += w (a b | component IC of c) for one primitive triple, from the E tables of the
+// pair, the Hermite Coulomb integrals R and the aux factor's Hermite coefficients Ec; every index is a
+// compile-time constant.
+template <int LA, int LB, int LC, int IC, int STRIDE>
+__device__ __forceinline__ void accum_comp(double* acc, const double (&E)[3][LA + 1][LB + 1][LA + LB + 1],
+                                           const double (&R)[n_herm(LA + LB + LC)],
+                                           const double (&Ec)[LC + 1][LC + 1], double w) {
+  constexpr int NA = Cart<LA>::N, NB = Cart<LB>::N, LAB = LA + LB;
+  constexpr int cx = cart_comp(LC, IC, 0), cy = cart_comp(LC, IC, 1), cz = cart_comp(LC, IC, 2);
+  double G[n_herm(LAB)];
+#pragma unroll
+  for (int sl = 0; sl <= LAB; ++sl)
+#pragma unroll
+    for (int m = 0; m <= sl; ++m)
+#pragma unroll
+      for (int v = 0; v <= m; ++v) {
+        const int u = m - v, t = sl - m;
+        double g = 0.0;
+#pragma unroll
+        for (int tau = cx & 1; tau <= cx; tau += 2)
+#pragma unroll
+          for (int nu = cy & 1; nu <= cy; nu += 2)
+#pragma unroll
+            for (int phi = cz & 1; phi <= cz; phi += 2) {
+              const double ec = Ec[cx][tau] * Ec[cy][nu] * Ec[cz][phi];
+              const double r = R[rix(t + tau, u + nu, v + phi)];
+              g += ((tau + nu + phi) & 1) ? -ec * r : ec * r;
+            }
+        G[rix(t, u, v)] = g;
+      }
+#pragma unroll
+  for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+    for (int ib = 0; ib < NB; ++ib) {
+      const int ax = cart_comp(LA, ia, 0), ay = cart_comp(LA, ia, 1), az = cart_comp(LA, ia, 2);
+      const int bx = cart_comp(LB, ib, 0), by = cart_comp(LB, ib, 1), bz = cart_comp(LB, ib, 2);
+      double val = 0.0;
+#pragma unroll
+      for (int t = 0; t <= ax + bx; ++t)
+#pragma unroll
+        for (int u = 0; u <= ay + by; ++u)
+#pragma unroll
+          for (int v = 0; v <= az + bz; ++v)
+            val += E[0][ax][bx][t] * E[1][ay][by][u] * E[2][az][bz][v] * G[rix(t, u, v)];
+      acc[(ia * NB + ib) * STRIDE] += w * val;
+    }
+}
+
+// Every component, acc[(ia NB + ib) NC + ic].
+template <int LA, int LB, int LC, int IC>
+__device__ __forceinline__ void comp_all(double* acc, const double (&E)[3][LA + 1][LB + 1][LA + LB + 1],
+                                         const double (&R)[n_herm(LA + LB + LC)],
+                                         const double (&Ec)[LC + 1][LC + 1], double w) {
+  if constexpr (IC < Cart<LC>::N) {
+    accum_comp<LA, LB, LC, IC, Cart<LC>::N>(acc + IC, E, R, Ec, w);
+    comp_all<LA, LB, LC, IC + 1>(acc, E, R, Ec, w);
+  }
+}
+
+// The thread's one component `ic`, acc[ia NB + ib].
+template <int LA, int LB, int LC, int IC>
+__device__ __forceinline__ void comp_dispatch(int ic, double* acc, const double (&E)[3][LA + 1][LB + 1][LA + LB + 1],
+                                              const double (&R)[n_herm(LA + LB + LC)],
+                                              const double (&Ec)[LC + 1][LC + 1], double w) {
+  if constexpr (IC < Cart<LC>::N) {
+    if (ic == IC)
+      accum_comp<LA, LB, LC, IC, 1>(acc, E, R, Ec, w);
+    else
+      comp_dispatch<LA, LB, LC, IC + 1>(ic, acc, E, R, Ec, w);
+  }
+}
+
+// SPLIT: one thread per (pair, aux shell, aux component) for the classes with many outputs; the component
+// is selected among compile-time branches, so every table index stays static.
+template <int LA, int LB, int LC, bool SPLIT>
 __global__ void __launch_bounds__(128) eri_class_kernel(ClassArgs a) {
-  constexpr int NA = Cart<LA>::N, NB = Cart<LB>::N, NC = Cart<LC>::N;
+  constexpr int NA = Cart<LA>::N, NB = Cart<LB>::N, NC = Cart<LC>::N, NCA = SPLIT ? 1 : NC;
   constexpr int LAB = LA + LB, L = LAB + LC;
-  constexpr int NR = (L + 1) * (L + 2) * (L + 3) / 6, NG = (LAB + 1) * (LAB + 2) * (LAB + 3) / 6;
-  constexpr Cart<LA> ca{};
-  constexpr Cart<LB> cb{};
-  constexpr Cart<LC> cc{};
+  constexpr int NR = n_herm(L);
   const double two_pi25 = 2.0 * M_PI * M_PI * sqrt(M_PI);
-  const int64_t total = a.npairs * a.ncs;
+  const int64_t total = a.npairs * a.ncs * (SPLIT ? NC : 1);
   for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < total;
        idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int2 pr = a.pairs[idx % a.npairs];
-    const int csh = a.cidx[idx / a.npairs];
+    const int64_t rest = idx / a.npairs;
+    const int icsel = SPLIT ? static_cast<int>(rest % NC) : 0;
+    const int csh = a.cidx[SPLIT ? rest / NC : rest];
     const DShell A = a.sh[pr.x], B = a.sh[pr.y], C = a.sh[csh];
-    double acc[NA * NB * NC];
+    double acc[NA * NB * NCA];
 #pragma unroll
-    for (int q = 0; q < NA * NB * NC; ++q) acc[q] = 0.0;
+    for (int q = 0; q < NA * NB * NCA; ++q) acc[q] = 0.0;
     const double ab[3] = {A.x - B.x, A.y - B.y, A.z - B.z};
     const double ab2 = ab[0] * ab[0] + ab[1] * ab[1] + ab[2] * ab[2];
     for (int i = 0; i < A.nprim; ++i) {
@@ -504,45 +580,10 @@ __global__ void __launch_bounds__(128) eri_class_kernel(ClassArgs a) {
               Ec[ii][t] = v;
             }
           const double w = cA * cB * cC * two_pi25 / (p * ga * sqrt(p + ga)) * K;
-#pragma unroll
-          for (int ic = 0; ic < NC; ++ic) {
-            const int cx = cc.x[ic], cy = cc.y[ic], cz = cc.z[ic];
-            double G[NG];
-#pragma unroll
-            for (int sl = 0; sl <= LAB; ++sl)
-#pragma unroll
-              for (int m = 0; m <= sl; ++m)
-#pragma unroll
-                for (int v = 0; v <= m; ++v) {
-                  const int u = m - v, t = sl - m;
-                  double g = 0.0;
-#pragma unroll
-                  for (int tau = cx & 1; tau <= cx; tau += 2)
-#pragma unroll
-                    for (int nu = cy & 1; nu <= cy; nu += 2)
-#pragma unroll
-                      for (int phi = cz & 1; phi <= cz; phi += 2) {
-                        const double ec = Ec[cx][tau] * Ec[cy][nu] * Ec[cz][phi];
-                        const double r = R[rix(t + tau, u + nu, v + phi)];
-                        g += ((tau + nu + phi) & 1) ? -ec * r : ec * r;
-                      }
-                  G[rix(t, u, v)] = g;
-                }
-#pragma unroll
-            for (int ia = 0; ia < NA; ++ia)
-#pragma unroll
-              for (int ib = 0; ib < NB; ++ib) {
-                const int ax = ca.x[ia], ay = ca.y[ia], az = ca.z[ia], bx = cb.x[ib], by = cb.y[ib], bz = cb.z[ib];
-                double val = 0.0;
-#pragma unroll
-                for (int t = 0; t <= ax + bx; ++t)
-#pragma unroll
-                  for (int u = 0; u <= ay + by; ++u)
-#pragma unroll
-                    for (int v = 0; v <= az + bz; ++v)
-                      val += E[0][ax][bx][t] * E[1][ay][by][u] * E[2][az][bz][v] * G[rix(t, u, v)];
-                acc[(ia * NB + ib) * NC + ic] += w * val;
-              }
+          if constexpr (SPLIT) {
+            comp_dispatch<LA, LB, LC, 0>(icsel, acc, E, R, Ec, w);
+          } else {
+            comp_all<LA, LB, LC, 0>(acc, E, R, Ec, w);
           }
         }
       }
@@ -558,9 +599,10 @@ __global__ void __launch_bounds__(128) eri_class_kernel(ClassArgs a) {
         const double sab = a.map_sc[A.map0 + ia] * a.map_sc[B.map0 + ib];
 #pragma unroll
         for (int ic = 0; ic < NC; ++ic) {
+          if (SPLIT && ic != icsel) continue;  // ic compile-time, icsel the thread's component
           const int fc = a.map_fn[C.map0 + ic];
           if (fc < 0) continue;
-          const double v = acc[(ia * NB + ib) * NC + ic] * sab * a.map_sc[C.map0 + ic];
+          const double v = acc[(ia * NB + ib) * NCA + (SPLIT ? 0 : ic)] * sab * a.map_sc[C.map0 + ic];
           const int64_t row = static_cast<int64_t>(fc) * a.n * a.n;
           a.out[row + static_cast<int64_t>(fa) * a.n + fb] = v;
           a.out[row + static_cast<int64_t>(fb) * a.n + fa] = v;
@@ -569,17 +611,18 @@ __global__ void __launch_bounds__(128) eri_class_kernel(ClassArgs a) {
   }
 }
 
-// The classes with a thread-per-item kernel (l_A >= l_B): the s and p pairs with aux s .. f, (pp| s, p),
-// (ds| s, p).  The others (more outputs, few primitives) take the warp kernel.
-template <int LA, int LB, int LC>
+// The classes with a thread-per-item kernel (l_A >= l_B <= 2, aux l <= 3): one thread per item for the s
+// and p pairs with aux s .. f, (pp| s, p) and (ds| s, p); one thread per aux component for the rest.
+// Higher angular momenta take the warp kernel.
+template <int LA, int LB, int LC, bool SPLIT>
 void launch_class(const ClassArgs& a, cudaStream_t s) {
-  auto kern = eri_class_kernel<LA, LB, LC>;
+  auto kern = eri_class_kernel<LA, LB, LC, SPLIT>;
   static int per_sm[kMaxDevices] = {};
   const int dev = current_device();
   if (!per_sm[dev]) RR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[dev], kern, 128, 0));
   int sms = 0;
   RR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  const int64_t total = a.npairs * a.ncs;
+  const int64_t total = a.npairs * a.ncs * (SPLIT ? Cart<LC>::N : 1);
   const int grid = static_cast<int>(std::max<int64_t>(
       1, std::min<int64_t>((total + 127) / 128, static_cast<int64_t>(sms) * std::max(per_sm[dev], 1) * 8)));
   kern<<<grid, 128, 0, s>>>(a);
@@ -587,14 +630,15 @@ void launch_class(const ClassArgs& a, cudaStream_t s) {
 }
 
 bool launch_class_any(int la, int lb, int lc, const ClassArgs& a, cudaStream_t s) {
-#define RR_CLASS(A, B, C)                  \
+#define RR_CLASS(A, B, C, SPLIT)           \
   if (la == A && lb == B && lc == C) {     \
-    launch_class<A, B, C>(a, s);           \
+    launch_class<A, B, C, SPLIT>(a, s);    \
     return true;                           \
   }
-  RR_CLASS(0, 0, 0) RR_CLASS(0, 0, 1) RR_CLASS(0, 0, 2) RR_CLASS(0, 0, 3)
-  RR_CLASS(1, 0, 0) RR_CLASS(1, 0, 1) RR_CLASS(1, 0, 2) RR_CLASS(1, 0, 3)
-  RR_CLASS(1, 1, 0) RR_CLASS(1, 1, 1) RR_CLASS(2, 0, 0) RR_CLASS(2, 0, 1)
+  RR_CLASS(0, 0, 0, false) RR_CLASS(0, 0, 1, false) RR_CLASS(0, 0, 2, false) RR_CLASS(0, 0, 3, false)
+  RR_CLASS(1, 0, 0, false) RR_CLASS(1, 0, 1, false) RR_CLASS(1, 0, 2, false) RR_CLASS(1, 0, 3, false)
+  RR_CLASS(1, 1, 0, false) RR_CLASS(1, 1, 1, false) RR_CLASS(2, 0, 0, false) RR_CLASS(2, 0, 1, false)
+  RR_CLASS(1, 1, 2, true) RR_CLASS(1, 1, 3, true) RR_CLASS(2, 0, 2, true) RR_CLASS(2, 0, 3, true)
 #undef RR_CLASS
   return false;
 }
