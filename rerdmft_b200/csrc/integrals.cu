@@ -16,12 +16,16 @@
 // return for the same basis-function lists: a function is coefficient * f(l) * x^lx y^ly z^lz exp(-a r^2)
 // with f(0) = 1/sqrt(4 pi), f(1) = sqrt(3/(4 pi)) and f(l >= 2) = 1.
 //
-// GPU mapping: one warp per work item (orbital shell pair, aux shell) or (aux shell, aux shell), a
-// grid-stride loop over items.  Per primitive pair the warp's first three lanes build the three E tables
-// in shared memory; per aux primitive lane 0 evaluates the Boys function and the warp builds the R table
-// level by level (in place, one __syncwarp per level); each lane then accumulates its share of the
-// (component a, component b, component c) outputs, in chunks of 32 x kOutPerLane.  Every output element
-// is written exactly once (both halves of the (pq) symmetry from one value), so nothing is zeroed.
+// GPU mapping.  Work items are (orbital shell pair, aux shell), grouped by angular-momentum class
+// (l_A >= l_B after swapping the pair).  The low classes, where most primitive triples are (s and p pairs
+// with long contractions), run one thread per item (or per item and aux component) in kernels templated
+// on (l_A, l_B, l_C): E, R and the accumulators in registers, every component and Hermite loop unrolled.
+// The other classes and the metric run one warp per item: per primitive pair lanes 0-2 build the three E
+// tables in shared memory; per aux primitive lane 3 evaluates the Boys function and the warp builds the R
+// table level by level (in place, one __syncwarp per level); each lane then accumulates its share of the
+// (component a, component b, component c) outputs, in chunks of 32 x kOutPerLane.  The Boys function
+// comes from a table of F_n at T = k/20 and a 7-term Taylor step.  Every output element is written exactly
+// once (both halves of the (pq) symmetry from one value), so nothing is zeroed.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -611,9 +615,10 @@ __global__ void __launch_bounds__(128) eri_class_kernel(ClassArgs a) {
   }
 }
 
-// The classes with a thread-per-item kernel (l_A >= l_B <= 2, aux l <= 3): one thread per item for the s
-// and p pairs with aux s .. f, (pp| s, p) and (ds| s, p); one thread per aux component for the rest.
-// Higher angular momenta take the warp kernel.
+// The classes with a thread-per-item kernel (l_A >= l_B, aux l <= 3): one thread per item for the s and p
+// pairs with aux s .. f, (pp| s, p) and (ds| s, p); one thread per aux component for (pp| d, f) and
+// (ds| d, f).  The rest take the warp kernel; (dp| s .. f) are 7.6 of the 12.2 ms of the (H2O)_8 / cc-pVDZ
+// raw tensor there, but as templates this file compiled for 16 minutes, so they stay in the warp kernel.
 template <int LA, int LB, int LC, bool SPLIT>
 void launch_class(const ClassArgs& a, cudaStream_t s) {
   auto kern = eri_class_kernel<LA, LB, LC, SPLIT>;
