@@ -358,11 +358,8 @@ def water_cluster(waters: int):
     from rerdmft_b200 import basis as bs
 
     z = np.load(ROOT / "tests" / "golden" / "water_ccpvdz.npz")
-    sets, off = {}, 0
-    for el, l, npr in zip(z["shell_element"], z["shell_l"], z["shell_nprim"]):
-        sets.setdefault(str(el), []).append(bs.Shell(int(l), [float(v) for v in z["exponents"][off:off + npr]],
-                                                     [float(v) for v in z["coefficients"][off:off + npr]]))
-        off += int(npr)
+    sets = bs.basis_set_from_arrays(z["shell_element"], z["shell_l"], z["shell_nprim"], z["exponents"],
+                                    z["coefficients"])
     mol = [(str(s), *map(float, xyz)) for s, xyz in zip(z["atom_symbol"], z["atom_xyz"])]
     k = int(np.ceil(waters ** (1.0 / 3.0) - 1e-9))
     geo = []
@@ -374,6 +371,105 @@ def water_cluster(waters: int):
     aux = bs.build_auto_auxiliary_basis(orb, "PAUTO")
     bs.normalize_cartesian_basis(aux)
     return orb, aux, geo
+
+
+def lih_631g():
+    """LiH / 6-31G at 1.5949 Angstrom with its PAUTO aux basis, and the RI Hartree-Fock energy the reference
+    printed for it (fixture tests/golden/lih_631g.npz)."""
+    from rerdmft_b200 import basis as bs
+
+    z = np.load(ROOT / "tests" / "golden" / "lih_631g.npz")
+    sets = bs.basis_set_from_arrays(z["shell_element"], z["shell_l"], z["shell_nprim"], z["exponents"],
+                                    z["coefficients"])
+    geo = [bs.Atom(str(s), *map(float, xyz)) for s, xyz in zip(z["atom_symbol"], z["atom_xyz"])]
+    orb = bs.build_molecular_basis(geo, sets)
+    bs.normalize_cartesian_basis(orb)
+    aux = bs.build_auto_auxiliary_basis(orb, "PAUTO")
+    bs.normalize_cartesian_basis(aux)
+    return orb, aux, geo, int(z["nelec"]), float(z["e_hf_ri"])
+
+
+def integrals_block(torch, hbm_peak, want_cpu: bool, waters: int = 8, reps: int = 3):
+    """The device integral engine: the raw 3-centre integrals and the aux metric of (H2O)_waters / cc-pVDZ
+    (PAUTO aux basis), device outputs, CUDA events; and, in the CPU leg, LiH / 6-31G against the numpy
+    restatement (time and max relative difference) and its RI Hartree-Fock energy from device integrals and
+    the device SCF loop against the reference's printed value."""
+    import ctypes
+
+    from rerdmft_b200 import _lib as L
+    from rerdmft_b200 import basis as bs
+    from rerdmft_b200 import integrals as gi
+
+    lib = L.lib()
+    orb, aux, _ = water_cluster(waters)
+    n, na = len(orb), len(aux)
+    co, ca = gi._CBasis(orb), gi._CBasis(aux)
+    raw = torch.empty((na, n * n), dtype=torch.float64, device="cuda")
+    M = torch.empty((na, na), dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    o = L.opts(L.RR_MEM_DEVICE, stream=stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    ms_raw = timed(lambda: L.check(lib.rr_int_three_center_raw(ctypes.byref(co.c), ctypes.byref(ca.c), raw.data_ptr(),
+                                                               ctypes.byref(o))))
+    ms_m = timed(lambda: L.check(lib.rr_int_aux_metric(ctypes.byref(ca.c), M.data_ptr(), ctypes.byref(o))))
+    shells_o = [(orb[f].l, len(orb[f].exponents)) for f, _ in bs.group_into_shells(orb)]
+    shells_a = [(aux[f].l, len(aux[f].exponents)) for f, _ in bs.group_into_shells(aux)]
+    prim_a = sum(p for _, p in shells_a)
+    triples = sum(shells_o[i][1] * shells_o[j][1] for i in range(len(shells_o)) for j in range(i, len(shells_o))) * prim_a
+    raw_bytes = 8.0 * na * n * n
+    out = dict(workload=f"(H2O)_{waters} / cc-pVDZ (Cartesian), PAUTO aux basis: raw (pq|P) and (P|Q), FP64",
+               n=n, naux=na, raw_gb=raw_bytes / 1e9, ms_raw=ms_raw, ms_metric=ms_m,
+               primitive_triples=triples, primitive_triples_per_s=triples / (ms_raw / 1e3),
+               raw_write_gbs=raw_bytes / (ms_raw / 1e3) / 1e9,
+               write_floor_ms=(raw_bytes / (hbm_peak * 1e9) * 1e3) if hbm_peak else None,
+               note="compute-bound (FP64 Hermite recurrences); the write floor is the raw tensor at measured HBM")
+    del raw, M
+    torch.cuda.empty_cache()
+    if want_cpu:
+        sys.path.insert(0, str(ROOT))
+        from oracle import integrals_oracle as io
+        from oracle import ri_oracle as ro
+        from rerdmft_b200 import ri, scf
+
+        lorb, laux, geo, nelec, e_ref = lih_631g()
+        t0 = time.perf_counter()
+        raw_ref = io.three_center_raw(lorb, laux)
+        cpu_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        raw_dev = gi.threeCenterIntegralsRaw(lorb, laux)
+        dev_s = time.perf_counter() - t0
+        S = io.overlap_matrix(lorb)
+        ch = [(bs.atomic_number(a.symbol), (a.x, a.y, a.z)) for a in geo]
+        h = io.kinetic_matrix(lorb) + io.nuclear_attraction_matrix(lorb, ch)
+        X = ro.canonical_orthogonalize(S, 1e-6)
+        store, rep = gi.store_from_basis(lorb, laux, 1e-10)
+        src = ri.RiNonRelEriSource(len(lorb), None, X, S, store=store)
+        w, u = np.linalg.eigh(X.T @ h @ X)
+        c = X @ u[:, :nelec // 2]
+        r = scf.runNonRelativisticHartreeFock(src, h, X, 2.0 * c @ c.T, nelec)
+        e = r["energy"] + bs.nuclear_repulsion(geo)
+        store.close()
+        out["parity"] = dict(
+            workload="LiH / 6-31G (n = 11) with its PAUTO aux basis (naux = 106)",
+            raw_max_rel_vs_restatement=float(np.abs(raw_dev - raw_ref).max() / np.abs(raw_ref).max()),
+            ri_hf_energy=e, reference_energy=e_ref, energy_minus_reference=e - e_ref,
+            reference="the reference's printed RI-HF energy (libcint integrals), examples/reference.yaml",
+            metric_kept=rep["n_kept"], metric_dropped=rep["n_dropped"])
+        out["cpu_baseline"] = dict(kind="port", cores=1, seconds=cpu_s, device_call_seconds=dev_s,
+                                   sample="LiH / 6-31G raw tensor by the numpy McMurchie-Davidson restatement (the "
+                                          "reference's libcint is not available here)")
+    return out
 
 
 def x2c_batch_problems(count: int = 64):
@@ -1008,6 +1104,7 @@ def main():
     orb_block = orbital_optimization_block()
     x2c_block = x2c_batch_block(want_cpu=not args.no_cpu_baseline)
     gnof_block = gnof_optimization_block()
+    int_block = integrals_block(torch, hbm_peak, want_cpu=not args.no_cpu_baseline)
     rel_block = rel_scf_times(not args.no_cpu_baseline,
                               (rkb_block.get("reference_cpu") or {}).get("seconds_per_build"))
     line = dict(
@@ -1043,6 +1140,7 @@ def main():
         orbital_optimization=orb_block,
         x2c_batch=x2c_block,
         gnof_optimization=gnof_block,
+        integrals=int_block,
     )
     print(json.dumps(line))
     if pg:

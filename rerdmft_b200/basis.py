@@ -128,6 +128,19 @@ def read_basis_set(path: str) -> dict:
     return out
 
 
+def basis_set_from_arrays(shell_element, shell_l, shell_nprim, exponents, coefficients) -> dict:
+    """{ELEMENT: [Shell, ...]} from flat per-shell arrays (element, l, primitive count) and the concatenated
+    exponents and coefficients, the inverse of listing read_basis_set's shells in order."""
+    out: dict = {}
+    off = 0
+    for el, l, npr in zip(shell_element, shell_l, shell_nprim):
+        npr = int(npr)
+        out.setdefault(str(el).upper(), []).append(
+            Shell(int(l), [float(v) for v in exponents[off:off + npr]], [float(v) for v in coefficients[off:off + npr]]))
+        off += npr
+    return out
+
+
 def build_molecular_basis(geometry: list, basis_set: dict) -> list:
     """Copies each atom's shells to its position, one BasisFunction per Cartesian component."""
     fns = []

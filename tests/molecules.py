@@ -12,12 +12,8 @@ def load(name: str, aux_kind: str = "PAUTO") -> dict:
     """geometry (bohr), the normalised orbital basis, the normalised automatic aux basis, nelec and the
     reference energies stored with the fixture."""
     z = golden(name)
-    sets: dict = {}
-    off = 0
-    for el, l, npr in zip(z["shell_element"], z["shell_l"], z["shell_nprim"]):
-        sets.setdefault(str(el), []).append(bs.Shell(int(l), [float(v) for v in z["exponents"][off:off + npr]],
-                                                     [float(v) for v in z["coefficients"][off:off + npr]]))
-        off += int(npr)
+    sets = bs.basis_set_from_arrays(z["shell_element"], z["shell_l"], z["shell_nprim"], z["exponents"],
+                                    z["coefficients"])
     geo = [bs.Atom(str(s), *map(float, xyz)) for s, xyz in zip(z["atom_symbol"], z["atom_xyz"])]
     orb = bs.build_molecular_basis(geo, sets)
     bs.normalize_cartesian_basis(orb)
