@@ -88,6 +88,7 @@ struct ClassArgs {
   int64_t n;
   double* out;
   const double* boys;
+  int metric;  // 1: pairs are (A, the constant function), out = (P|Q) (n x n), items with C < A skipped
 };
 
 // E^ab of one dimension for the compile-time (LA, LB): E[i][j][t].
@@ -207,6 +208,7 @@ __global__ void __launch_bounds__(128) eri_class_kernel(ClassArgs a) {
     const int64_t rest = idx / a.npairs;
     const int icsel = SPLIT ? static_cast<int>(rest % NC) : 0;
     const int csh = a.cidx[SPLIT ? rest / NC : rest];
+    if (a.metric && csh < pr.x) continue;  // (P|Q) for Q >= P only
     const DShell A = a.sh[pr.x], B = a.sh[pr.y], C = a.sh[csh];
     double acc[NA * NB * NCA];
 #pragma unroll
@@ -283,6 +285,22 @@ __global__ void __launch_bounds__(128) eri_class_kernel(ClassArgs a) {
           }
         }
       }
+    }
+    if (a.metric) {  // B is the constant function (l_B = 0): out[P][Q] and out[Q][P]
+      const bool same = csh == pr.x;
+#pragma unroll
+      for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+        for (int ic = 0; ic < NC; ++ic) {
+          if (SPLIT && ic != icsel) continue;
+          if (same && ia > ic) continue;
+          const int fa = a.map_fn[A.map0 + ia], fc = a.map_fn[C.map0 + ic];
+          if (fa < 0 || fc < 0) continue;
+          const double v = acc[ia * NB * NCA + (SPLIT ? 0 : ic)] * a.map_sc[A.map0 + ia] * a.map_sc[C.map0 + ic];
+          a.out[static_cast<int64_t>(fa) * a.n + fc] = v;
+          a.out[static_cast<int64_t>(fc) * a.n + fa] = v;
+        }
+      continue;
     }
     const bool sym = pr.x == pr.y;
 #pragma unroll

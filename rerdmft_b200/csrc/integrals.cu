@@ -560,18 +560,37 @@ void aux_metric_device(const rr_basis* aux, double* M, cudaStream_t s) {
   HostShells all = hs;
   const int iu = static_cast<int>(all.sh.size());
   append_shells(all, unit);
-  std::vector<int2> pairs(na);
-  std::vector<int> cidx(na);
-  for (int i = 0; i < na; ++i) {
-    pairs[i] = make_int2(i, iu);
-    cidx[i] = i;
+  // bra shells (A, unit) and ket shells, both by angular momentum; a (l_A, 0 | l_C) class kernel in
+  // metric mode where one exists (items with C < A skipped there), else the warp kernel
+  std::vector<int2> pairs;
+  std::vector<int> cidx;
+  std::vector<int64_t> p0(kMaxL + 2, 0), c0(kMaxL + 2, 0);
+  for (int l = 0; l <= kMaxL; ++l) {
+    for (int i = 0; i < na; ++i)
+      if (hs.sh[i].l == l) {
+        pairs.push_back(make_int2(i, iu));
+        cidx.push_back(i);
+      }
+    p0[l + 1] = static_cast<int64_t>(pairs.size());
+    c0[l + 1] = static_cast<int64_t>(cidx.size());
   }
   DevShells d(all, s);
   DevBuf<int2> dp;
   DevBuf<int> dc;
   upload(dp, pairs, s);
   upload(dc, cidx, s);
-  launch_eri(d, dp.p, na, dc.p, na, hs.lmax, hs.lmax, true, aux->n, M, boys, s);
+  ClassArgs ca{d.sh.p, d.ex.p, d.co.p, d.fn.p, d.sc.p, nullptr, 0, nullptr, 0, aux->n, M, boys, 1};
+  for (int la = 0; la <= kMaxL; ++la)
+    for (int lc = 0; lc <= kMaxL; ++lc) {
+      const int64_t np = p0[la + 1] - p0[la], nc = c0[lc + 1] - c0[lc];
+      if (np == 0 || nc == 0) continue;
+      ca.pairs = dp.p + p0[la];
+      ca.npairs = np;
+      ca.cidx = dc.p + c0[lc];
+      ca.ncs = nc;
+      if (!launch_class_any(la, 0, lc, ca, s))
+        launch_eri(d, dp.p + p0[la], np, dc.p + c0[lc], nc, hs.lmax, hs.lmax, true, aux->n, M, boys, s);
+    }
   RR_CUDA(cudaStreamSynchronize(s));  // the tables are freed on return
 }
 
@@ -619,7 +638,7 @@ void three_center_raw_device(const rr_basis* orb, const rr_basis* aux, double* r
   DevBuf<int> dc;
   upload(dp, pairs, s);
   upload(dc, cidx, s);
-  ClassArgs ca{d.sh.p, d.ex.p, d.co.p, d.fn.p, d.sc.p, nullptr, 0, nullptr, 0, orb->n, raw, boys};
+  ClassArgs ca{d.sh.p, d.ex.p, d.co.p, d.fn.p, d.sc.p, nullptr, 0, nullptr, 0, orb->n, raw, boys, 0};
   for (const Range& r : ranges)
     for (int lc = 0; lc <= kMaxL; ++lc) {
       const int64_t nc = c0[lc + 1] - c0[lc];
