@@ -365,16 +365,24 @@ void fock_nonrel(rr_ri_store* h, const double* hc, const double* D, const double
     const int k = e ? std::atoi(e) : 1;
     return k >= 1 && k <= 4 ? k : 1;
   }();
+  // RR_J_AFTER_RECOVERY=1 (device pointers, for measurement): the J passes start after the recovery
+  // instead, beside the half-transform and the SYRK only: 1.630 / 1.748 / 1.818 ms per build with 1 / 2 / 3
+  // J CTAs per SM, against 1.565 / 1.584 / 1.708 ms from the top of the build.
+  static const bool j_late = [] {
+    const char* e = std::getenv("RR_J_AFTER_RECOVERY");
+    return e && std::atoi(e) == 1;
+  }();
   if (host) {
     auto& c = h->ctx;
     coulomb_early(h, Dp, J, c.side, j_ctas);
     copy_in(hd, hc, n2, true, c.side);  // read only by the final combine
     RR_CUDA(cudaEventRecord(c.upl[2], c.side));
     h_ready = c.upl[2];
-  } else {
+  } else if (!j_late) {
     coulomb_early(h, Dp, J, s, j_ctas);
   }
   const int64_t nocc = occupied_ct(h, Xd, Sd, Dp, n, n_eff, 0.5, false, false, Ct, s, d_ready);
+  if (!host && j_late) coulomb_early(h, Dp, J, s, j_ctas);
   if (d_ready) RR_CUDA(cudaStreamWaitEvent(s, d_ready, 0));  // (n_eff = 0 skips the products)
   prof_mark(h, 1, s);
   exchange_nonrel(h, Ct, n, false, nocc, K, s);
