@@ -7,6 +7,7 @@
 //         K' = sum_P T[P]^T T[P] (split-K DMMA SYRK, upper tiles + mirror)        [FP64 tensor]
 //   join, F = h + J - K'   (K' = K/2 of the reference: its c_t carries sqrt(2)).
 #include <algorithm>
+#include <vector>
 
 #include <cstdlib>
 
@@ -38,6 +39,59 @@ void coulomb_prep(rr_ri_store* h, const double* Dp, const double* Ct, int64_t no
 void coulomb_run(rr_ri_store* h, const double* tgam, int tseg, cudaStream_t s);
 void coulomb_join(rr_ri_store* h, cudaStream_t s);
 
+namespace {
+
+// K = sum_c parts[c] in the order c = 0, 1, ... (n2 entries each).
+__global__ void sum_parts_kernel(double* K, const double* parts, int nparts, int64_t n2) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n2;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double v = parts[i];
+    for (int c = 1; c < nparts; ++c) v += parts[c * n2 + i];
+    K[i] = v;
+  }
+}
+
+}  // namespace
+
+// The exchange with the half-transform and the SYRK pipelined over `chunks` ranges of aux indices: the
+// main stream half-transforms range c + 1 while the handle's second compute stream runs the SYRK of
+// range c into its own partial K_c; K = sum_c K_c in a fixed order.  Needs the m16 half-transform's
+// operands (even n and pitch, 16-byte aligned Ct).
+void exchange_pipelined(rr_ri_store* h, const double* Ct, int64_t nocc, double* K, cudaStream_t s, int chunks) {
+  const int64_t n = h->n, naux = h->naux, n2 = n * n;
+  auto& c = h->ctx;
+  h->T.ensure(static_cast<size_t>(naux * nocc * n));
+  h->kpart.ensure(static_cast<size_t>(chunks * n2));
+  std::vector<GemmDesc> sk(chunks);
+  std::vector<int64_t> p0(chunks + 1);
+  int64_t want = 1;
+  for (int ci = 0; ci <= chunks; ++ci) p0[ci] = naux * ci / chunks;
+  for (int ci = 0; ci < chunks; ++ci) {
+    GemmDesc& g = sk[ci];
+    g.M = n; g.N = n; g.K = (p0[ci + 1] - p0[ci]) * nocc;
+    g.A = h->T.p + p0[ci] * nocc * n; g.lda = n; g.opA = Op::T;
+    g.B = g.A; g.ldb = n; g.opB = Op::N;
+    g.C = h->kpart.p + ci * n2; g.ldc = n;
+    g.mirror = 1;
+    want = std::max(want, gemm_work_doubles(g));
+  }
+  h->work.ensure(static_cast<size_t>(want));
+  for (int ci = 0; ci < chunks; ++ci) {
+    RR_REQUIRE(half_transform_m16(Ct, nocc, h->B[0].p + p0[ci] * h->pitch[0], h->pitch[0], p0[ci + 1] - p0[ci], n,
+                                  h->T.p + p0[ci] * nocc * n, s, half_transform_config()),
+               RR_ERR_STATE, "exchange_pipelined: operands not supported by the m16 half-transform");
+    RR_CUDA(cudaEventRecord(c.pipe_ev[ci], s));
+    RR_CUDA(cudaStreamWaitEvent(c.pipe_stream, c.pipe_ev[ci], 0));
+    gemm(sk[ci], c.pipe_stream, h->work.p, static_cast<int64_t>(h->work.n));
+  }
+  prof_mark(h, 2, s);
+  RR_CUDA(cudaEventRecord(c.pipe_ev[chunks], c.pipe_stream));
+  RR_CUDA(cudaStreamWaitEvent(s, c.pipe_ev[chunks], 0));
+  sum_parts_kernel<<<static_cast<int>(std::min<int64_t>((n2 + 255) / 256, 1184)), 256, 0, s>>>(K, h->kpart.p, chunks,
+                                                                                               n2);
+  RR_LAUNCH_CHECK();
+}
+
 // Exchange K' = sum_P (Ct B^P)^T (Ct B^P) for a given Ct (nocc x n, row-major with leading
 // dimension ldct, or its transpose when ct_transposed: Ct = C^T with C stored n x nocc).
 // With Dp given (the SCF loop's FP64 build), the Coulomb matrix J of the pitched density Dp is
@@ -59,6 +113,21 @@ void exchange_nonrel(rr_ri_store* h, const double* Ct, int64_t ldct, bool ct_tra
   ht.B = h->B[0].p; ht.ldb = n; ht.opB = Op::N; ht.strideB = h->pitch[0];
   ht.C = h->T.p; ht.ldc = n; ht.strideC = nocc * n;
   ht.batch = naux;
+  // RR_HT_PIPELINE=<chunks> (2 .. 8, for measurement): the drop-in build's half-transform and SYRK
+  // pipelined over that many ranges of aux indices (exchange_pipelined).  Both are DMMA-bound, so running
+  // them side by side gains nothing and the smaller per-chunk SYRKs cost: at n = 400, naux = 1600,
+  // nocc = 40, 1.609 / 1.627 / 1.672 / 1.723 ms per build with 2 / 3 / 4 / 6 chunks against 1.566 ms.
+  static const int pipe_chunks = [] {
+    const char* e = std::getenv("RR_HT_PIPELINE");
+    const int k = e ? std::atoi(e) : 0;
+    return k >= 2 && k <= Context::kPipeMax ? k : 0;
+  }();
+  auto al16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
+  if (pipe_chunks && !Dp && !half_only && K && !ct_transposed && ldct == n && half_transform_kind() == 1 &&
+      n % 2 == 0 && h->pitch[0] % 2 == 0 && al16(Ct) && naux >= 8 * pipe_chunks) {
+    exchange_pipelined(h, Ct, nocc, K, s, pipe_chunks);
+    return;
+  }
   double* tgam = nullptr;
   int tseg = 0;
   if (Dp) {

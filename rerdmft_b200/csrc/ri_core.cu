@@ -53,6 +53,8 @@ void Context::init(cudaStream_t user_stream) {
   RR_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
   RR_CUDA(cudaEventCreateWithFlags(&mid, cudaEventDisableTiming));
   for (auto& e : upl) RR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  RR_CUDA(cudaStreamCreateWithFlags(&pipe_stream, cudaStreamNonBlocking));
+  for (auto& e : pipe_ev) RR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   RR_SOLVER(cusolverDnCreate(&solver));
 }
 
@@ -65,6 +67,12 @@ void Context::destroy() {
     if (e) cudaEventDestroy(e);
     e = nullptr;
   }
+  for (auto& e : pipe_ev) {
+    if (e) cudaEventDestroy(e);
+    e = nullptr;
+  }
+  if (pipe_stream) cudaStreamDestroy(pipe_stream);
+  pipe_stream = nullptr;
   if (side) cudaStreamDestroy(side);
   if (own_main && main) cudaStreamDestroy(main);
   solver = nullptr;

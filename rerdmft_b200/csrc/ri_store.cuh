@@ -20,6 +20,7 @@ struct rr_ri_store {
   // Scratch, grown on demand and reused across calls.
   rr::DevBuf<double> mats;  // per-call matrices (inputs, outputs, intermediates)
   rr::DevBuf<double> T;     // half-transformed exchange intermediate
+  rr::DevBuf<double> kpart; // per-chunk exchange partials of the pipelined half-transform / SYRK
   rr::DevBuf<double> work;  // split-K partial products
   rr::DevBuf<double> jscr;  // J pass-1/pass-2 partial sums
   rr::DevBuf<double> dfold; // densities folded onto the packed triangles

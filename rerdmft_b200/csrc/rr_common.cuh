@@ -100,6 +100,11 @@ struct Context {
   bool own_main = false;
   cudaEvent_t fork = nullptr, join = nullptr, mid = nullptr;
   cudaEvent_t upl[3] = {nullptr, nullptr, nullptr};  // host-input uploads on the side stream
+  // Second compute stream and its events: the exchange SYRK of one chunk of aux indices runs there
+  // while the main stream half-transforms the next chunk.
+  static constexpr int kPipeMax = 8;
+  cudaStream_t pipe_stream = nullptr;
+  cudaEvent_t pipe_ev[kPipeMax + 1] = {};
   cusolverDnHandle_t solver = nullptr;
   DevBuf<double> solver_work;
   DevBuf<int> solver_info;
