@@ -12,6 +12,8 @@
                               radial normalisation, then each Cartesian component scaled to unit
                               self-overlap, the overlap carrying libcint's s / p factor)
 * ``build_auto_auxiliary_basis``  src/AO_basis/AuxiliaryBasis.cpp:116-190 (the AUTO / PAUTO recipe)
+* ``build_spherical_transform``  src/Utils/SphericalTransform.cpp:60-165 (per l: the Laplacian's null space on
+                              the monomials, Loewdin-orthonormalised in the normalised Cartesian overlap)
 * ``ANGSTROM_TO_BOHR``        src/Input/Input.cpp:23
 
 A basis is a list of :class:`BasisFunction` (the reference's struct of the same name); ``flatten``
@@ -344,3 +346,68 @@ def nuclear_repulsion(geometry: list) -> float:
             r = math.sqrt((a.x - b.x) ** 2 + (a.y - b.y) ** 2 + (a.z - b.z) ** 2)
             e += atomic_number(a.symbol) * atomic_number(b.symbol) / r
     return e
+
+
+def _laplacian(l: int) -> np.ndarray:
+    """(n(l-2), n(l)): the Laplacian of each degree-l monomial in degree-(l-2) monomials."""
+    src, dst = cartesian_components(l), cartesian_components(l - 2)
+    out = np.zeros((len(dst), len(src)))
+    for s, (lx, ly, lz) in enumerate(src):
+        for d, (a, b, c) in enumerate(((lx - 2, ly, lz), (lx, ly - 2, lz), (lx, ly, lz - 2))):
+            if min(a, b, c) >= 0:
+                out[dst.index((a, b, c)), s] += (lx, ly, lz)[d] * ((lx, ly, lz)[d] - 1)
+    return out
+
+
+def cartesian_to_spherical_block(l: int) -> np.ndarray:
+    """(n(l) x (2l + 1)) block of src/Utils/SphericalTransform.cpp:60-130: the null space of the Laplacian
+    on degree-l monomials (eigenvectors of L^T L with zero eigenvalue), Loewdin-orthonormalised in the
+    overlap of the normalised Cartesian components (canonical orthogonalisation at 1e-8), expressed in the
+    Cartesian components.  The span is unique; the orientation inside it is the eigensolver's."""
+    nf, ns = len(cartesian_components(l)), 2 * l + 1
+    if nf == ns:
+        return np.eye(nf)
+    lap = _laplacian(l)
+    w, u = np.linalg.eigh(lap.T @ lap)
+    null = u[:, :ns]
+    comps = cartesian_components(l)
+    raw = np.array([[cartesian_self_overlap_pair(l, ci, cj) for cj in comps] for ci in comps])
+    d = 1.0 / np.sqrt(np.diag(raw))
+    s_norm = raw * d[:, None] * d[None, :]
+    m = null.T @ s_norm @ null
+    ev, ec = np.linalg.eigh(m)
+    keep = ev > 1e-8
+    if keep.sum() != ns:
+        raise ValueError(f"cartesian_to_spherical_block: l={l}: rank {int(keep.sum())} of {ns}")
+    x = ec[:, keep] / np.sqrt(ev[keep])
+    if keep.all():
+        x = x @ ec.T  # the symmetric form when nothing is dropped, as canonical orthogonalisation gives
+    return null @ x
+
+
+def cartesian_self_overlap_pair(l: int, ci: tuple, cj: tuple, a: float = 1.0) -> float:
+    """<x^ci exp(-a r^2) | x^cj exp(-a r^2)> at one centre (unit coefficients, no libcint factor)."""
+    v = 1.0
+    for p, q in zip(ci, cj):
+        k = p + q
+        if k % 2:
+            return 0.0
+        v *= _double_factorial_odd(k // 2) / (4.0 * a) ** (k // 2) * math.sqrt(math.pi / (2.0 * a))
+    return v
+
+
+def build_spherical_transform(functions: list) -> tuple:
+    """The block-diagonal Cartesian-to-spherical transform of a normalised Cartesian basis
+    (src/Utils/SphericalTransform.cpp:132-165): (T (n_cart x n_sph), [(l, cartesian offset, spherical
+    offset)]), shells as consecutive runs of len(cartesian_components(l)) functions."""
+    shells, i, n_sph = [], 0, 0
+    while i < len(functions):
+        l = functions[i].l
+        shells.append((l, i, n_sph))
+        n_sph += 2 * l + 1
+        i += len(cartesian_components(l))
+    T = np.zeros((len(functions), n_sph))
+    for l, co, so in shells:
+        blk = cartesian_to_spherical_block(l)
+        T[co:co + blk.shape[0], so:so + blk.shape[1]] = blk
+    return T, shells

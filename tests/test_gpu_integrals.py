@@ -156,3 +156,24 @@ def test_device_outputs_stay_on_device():
     _close(M.cpu().numpy(), io.aux_metric(m["aux"]))
     _close(raw.cpu().numpy(), io.three_center_raw(m["basis"], m["aux"]))
     del torch
+
+
+def test_spherical_store_from_basis():
+    """rr_ri_create_basis with the Cartesian-to-spherical transform (the reference's CARTESIAN FALSE and
+    relativistic large-component basis): the Fock matrix of the device store against the oracle's
+    t^T B^P t of the restated integrals."""
+    m = molecules.load("water_ccpvdz")
+    T, _ = bs.build_spherical_transform(m["basis"])
+    S = io.overlap_matrix(m["basis"])
+    ch = [(bs.atomic_number(a.symbol), (a.x, a.y, a.z)) for a in m["geometry"]]
+    h = io.kinetic_matrix(m["basis"]) + io.nuclear_attraction_matrix(m["basis"], ch)
+    Ss, hs = T.T @ S @ T, T.T @ h @ T
+    Xs = ro.canonical_orthogonalize(Ss, 1e-6)
+    store, rep = gi.store_from_basis(m["basis"], m["aux"], 1e-10, t=T)
+    ns = T.shape[1]
+    src = ri.RiNonRelEriSource(ns, None, Xs, Ss, store=store)
+    Mx = ro.canonical_orthogonalize(io.aux_metric(m["aux"]), 1e-10)
+    B = ro.transform_ao_legs(Mx.T @ io.three_center_raw(m["basis"], m["aux"]), len(m["basis"]), T)
+    D = molecules.core_guess(hs, Xs, m["nelec"] // 2)
+    F = ri.nonRelFockMatrix(hs, src, D)
+    assert np.abs(F - ro.nonrel_fock(hs, B, D, Ss, Xs)).max() < 1e-10

@@ -165,3 +165,27 @@ def test_lih_stretched_lowest_state_matches_reference():
     m = molecules.load("lih_631g_5a")
     e, _ = _ri_hf(m, lambda h, X: molecules.random_guesses(X, m["nelec"] // 2, seed=0, count=12))
     assert abs(min(e) - m["e_hf_ri"]) < m["tolerance"], min(e) - m["e_hf_ri"]
+
+
+@pytest.mark.parametrize("l", range(7))
+def test_spherical_blocks(l):
+    """Each block (src/Utils/SphericalTransform.cpp:60-130) spans the Laplacian's null space on degree-l
+    monomials and is orthonormal in the overlap of the normalised Cartesian components."""
+    blk = bs.cartesian_to_spherical_block(l)
+    comps = bs.cartesian_components(l)
+    assert blk.shape == (len(comps), 2 * l + 1)
+    raw = np.array([[bs.cartesian_self_overlap_pair(l, a, b) for b in comps] for a in comps])
+    d = 1.0 / np.sqrt(np.diag(raw))
+    s_norm = raw * d[:, None] * d[None, :]
+    assert np.abs(blk.T @ s_norm @ blk - np.eye(2 * l + 1)).max() < 1e-12
+    if l >= 2:
+        assert np.abs(bs._laplacian(l) @ blk).max() < 1e-12 * max(1.0, np.abs(blk).max())
+
+
+def test_spherical_transform_of_a_basis():
+    m = molecules.load("water_ccpvdz")
+    T, shells = bs.build_spherical_transform(m["basis"])
+    assert T.shape == (25, 24) and len(shells) == 12
+    S = io.overlap_matrix(m["basis"])
+    Ss = T.T @ S @ T
+    assert np.abs(np.diag(Ss) - 1.0).max() < 1e-12  # the transformed functions stay normalised
