@@ -194,6 +194,54 @@ def mo_transform_block(torch, fp64_peak, want_cpu: bool, reps: int = 5):
                               achieved_tflops=flops / best / 1e12,
                               frac_of_dgemm=(flops / best / 1e12 / fp64_peak) if fp64_peak else None,
                               note="host wall time of the synchronous call, the 2.05 GB output allocation included")
+
+    # Device time of the same build into an existing tensor (rr_mo_build_nonrel_into: no allocation), CUDA
+    # events on the call's stream; B (2.05 GB) and the output are far larger than L2, so no flush.
+    stream = torch.cuda.current_stream()
+    od = L.opts(L.RR_MEM_DEVICE, sync=0, stream=stream.cuda_stream)
+    hm = build_nonrel()
+
+    def device_seconds(prec, n_rep):
+        od.precision = prec
+        L.check(lib.rr_mo_build_nonrel_into(st.handle, dC.data_ptr(), hm, ctypes.byref(od)))
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(n_rep):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            L.check(lib.rr_mo_build_nonrel_into(st.handle, dC.data_ptr(), hm, ctypes.byref(od)))
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1) / 1e3)
+        return float(np.median(ts))
+
+    t64 = device_seconds(L.RR_PREC_FP64, reps)
+    out["nonrel_spin"]["device_seconds_per_rebuild"] = t64
+    out["nonrel_spin"]["device_frac_of_dgemm"] = (flops / t64 / 1e12 / fp64_peak) if fp64_peak else None
+    b64 = np.empty((N_AUX, N_AO * N_AO))
+    L.check(lib.rr_mo_copy_tensor(hm, b64.ctypes.data, ctypes.byref(L.opts())))
+    tmx = device_seconds(L.RR_PREC_MIXED, 3 * reps)
+    bmx = np.empty_like(b64)
+    L.check(lib.rr_mo_copy_tensor(hm, bmx.ctypes.data, ctypes.byref(L.opts())))
+    L.check(lib.rr_mo_destroy(hm))
+    hbm, _ = measured_peaks()
+    pk = ROOT / "MEASURED_PEAKS.json"
+    bf16_peak = json.loads(pk.read_text()).get("bf16_tflops", 1590.0) if pk.exists() else 1590.0
+    ldq = (N_AO + 7) // 8 * 8
+    # bytes: the split copy of B read, the split intermediate written and read, the FP64 tensor written
+    moved = N_AUX * N_AO * ldq * 2 * 2 * 3 + N_AUX * N_AO * N_AO * 8
+    tc_flops = 3 * flops  # three BF16 products per FP64-equivalent product
+    err = float(np.abs(bmx - b64).max())
+    out["nonrel_spin_mixed"] = dict(
+        workload=f"buildRiNonRelSpinMoEri n={N_AO} naux={N_AUX} (full C, split-BF16 tcgen05, RR_PREC_MIXED)",
+        device_seconds_per_rebuild=tmx, speedup_over_fp64_device=t64 / tmx,
+        tensor_tflops=tc_flops / tmx / 1e12,
+        frac_of_bf16_peak=(tc_flops / tmx / 1e12 / bf16_peak) if bf16_peak else None,
+        hbm_gbs=moved / tmx / 1e9, frac_of_hbm=(moved / tmx / 1e9 / hbm) if hbm else None,
+        algorithmic_bytes=moved, bf16_mma_flops=tc_flops,
+        max_abs_minus_fp64=err, rel_to_max=err / float(np.abs(b64).max()),
+        kernel="umma_mo_kernel (two launches: B^P C split, then C^T (B^P C) in FP64)")
+    del b64, bmx
     if want_cpu:
         from oracle import ref
 
@@ -830,7 +878,9 @@ def run_case(args):
                   naux=1000, 80 electrons);
     x2c_batch     the lockstep grouped X2C-HF scan (64 uneven instances), tuned then timed once;
     integrals     the raw 3-centre integrals and the aux metric of (H2O)_8 / cc-pVDZ with its PAUTO aux basis
-                  (n = 200, naux = 2856; RR_WATERS=<k> for another cluster), device outputs."""
+                  (n = 200, naux = 2856; RR_WATERS=<k> for another cluster), device outputs;
+    mo_mixed      the split-BF16 MO transform B_mo^P = C^T B^P C rebuilt into one tensor (n = 400, naux = 1600;
+                  RR_MO_NAUX=<k> for fewer aux rows), and the FP64 build of the same tensor (mo_fp64)."""
     import ctypes
 
     import torch
@@ -872,6 +922,25 @@ def run_case(args):
                      args.steps, args.warmup)
         out.update(workload=f"(H2O)_{waters} cc-pVDZ raw 3-centre integrals n={n} naux={na}", ms_raw=ms_raw,
                    ms_metric=ms_m, raw_gb=na * n * n * 8 / 1e9)
+        print(json.dumps(out))
+        return
+    if args.case in ("mo_mixed", "mo_fp64"):
+        na = int(os.environ.get("RR_MO_NAUX", str(N_AUX)))
+        B = synth.ri_tensor(N_AO, na, SEED, box=20.0)
+        C = synth.random_orthogonal(N_AO, np.random.default_rng(SEED + 5))
+        st = ri.RiStore(torch.from_numpy(B).cuda(), nl=N_AO)
+        dC = torch.from_numpy(C).cuda()
+        prec = L.RR_PREC_MIXED if args.case == "mo_mixed" else L.RR_PREC_FP64
+        h = ctypes.c_void_p()
+        L.check(lib.rr_mo_build_nonrel(st.handle, dC.data_ptr(), ctypes.byref(h),
+                                       ctypes.byref(L.opts(L.RR_MEM_DEVICE, precision=prec))))
+        o = L.opts(L.RR_MEM_DEVICE, precision=prec, stream=stream, sync=0)
+        ms = timed(lambda: L.check(lib.rr_mo_build_nonrel_into(st.handle, dC.data_ptr(), h, ctypes.byref(o))),
+                   args.steps, args.warmup)
+        L.check(lib.rr_mo_destroy(h))
+        st.close()
+        out.update(workload=f"buildRiNonRelSpinMoEri n={N_AO} naux={na} ({args.case})", ms_per_build=ms,
+                   gflop_fp64_equivalent=4.0 * na * N_AO ** 3 / 1e9)
         print(json.dumps(out))
         return
     if args.case == "x2c_batch":
@@ -966,7 +1035,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--case", default=None, choices=["headline", "mixed_exchange", "rkb_mixed", "rkb_fp64", "x2c_mixed",
-                                                    "x2c_batch", "integrals"],
+                                                    "x2c_batch", "integrals", "mo_mixed", "mo_fp64"],
                     help="run one workload for profiling instead of the bench line")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)

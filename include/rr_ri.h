@@ -314,8 +314,15 @@ typedef struct rr_mo_store* rr_mo_handle;
 #define RR_MO_COMPLEX 1     /* RiMoEri: complex tensor (naux, n*n) over n spinors */
 
 /* buildRiNonRelSpinMoEri(eri3_L, n, C), src/NON_REL/NonRelSpinRiMoEri.cpp:13: B_mo^P = C^T B^P C
- * with the handle's resident eri3_L; C is n x n (the spatial alpha half of the coefficients). */
+ * with the handle's resident eri3_L; C is n x n (the spatial alpha half of the coefficients).
+ * opts->precision = RR_PREC_MIXED: both products as split-BF16 tcgen05 MMAs (three BF16 products, FP32
+ * accumulation, the intermediate C^T B^P re-split to BF16 pairs), the tensor stored in FP64; relative
+ * error about 1e-5 of max|B_mo| (the FP64 build is the default). */
 int rr_mo_build_nonrel(rr_ri_handle ri, const double* C, rr_mo_handle* out, const rr_opts* opts);
+/* The same build into an existing RR_MO_NONREL_SPIN tensor of the handle's naux and n, overwritten in
+ * place (a functional-stage loop that rebuilds the tensor for new orbitals allocates nothing after the
+ * first build); NonRelSpinRiMoEri.cpp:13-43 re-run on an existing object. */
+int rr_mo_build_nonrel_into(rr_ri_handle ri, const double* C, rr_mo_handle mo, const rr_opts* opts);
 
 /* buildRiMoEri(RiDirectEriSource, c_ukb), src/UKB/RiMoEri.cpp:64: B(P,p,q) = sum over the four UKB
  * blocks of sum conj(c(mu,p)) c(nu,q) (mu nu|P); c_ukb is n_ukb x n_total complex (n_ukb = 2nl+2ns

@@ -182,6 +182,7 @@ _SIGS = {
     "rr_ri_two_electron_ukb": (ctypes.c_int, [_vp, _vp, _vp, _i64, _vp, _vp, ctypes.POINTER(Opts)]),
     "rr_ri_fock_rkb": (ctypes.c_int, [_vp, _vp, _vp, _i64, _vp, _vp, _i64, _vp, _vp, ctypes.POINTER(Opts)]),
     "rr_mo_build_nonrel": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(_vp), ctypes.POINTER(Opts)]),
+    "rr_mo_build_nonrel_into": (ctypes.c_int, [_vp, _vp, _vp, ctypes.POINTER(Opts)]),
     "rr_mo_build_ukb": (ctypes.c_int, [_vp, _vp, _i64, ctypes.POINTER(_vp), ctypes.POINTER(Opts)]),
     "rr_mo_hx_joint_hessian_diagonal": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp,
                                                        ctypes.POINTER(Opts)]),

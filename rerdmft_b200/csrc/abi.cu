@@ -449,9 +449,33 @@ int rr_mo_build_nonrel(rr_ri_handle ri, const double* C, rr_mo_handle* out, cons
     auto* m = new_mo(0, s->naux, s->n);
     with_new_mo(out, m, [&] {
       cudaStream_t st = rr::call_stream(s, opts);
-      rr::mo_build_nonrel(s, C, m, host_mem(opts), st);
+      if (opts && opts->precision == RR_PREC_MIXED) {
+        rr::mo_build_nonrel_mixed(s, C, m, host_mem(opts), st);
+        rr::check_status(s, st);
+      } else {
+        rr::mo_build_nonrel(s, C, m, host_mem(opts), st);
+      }
       RR_CUDA(cudaStreamSynchronize(st));
     });
+  });
+}
+
+int rr_mo_build_nonrel_into(rr_ri_handle ri, const double* C, rr_mo_handle mo, const rr_opts* opts) {
+  return api([&] {
+    auto* s = checked(ri);
+    RR_REQUIRE(C, RR_ERR_ARG, "rr_mo_build_nonrel_into: null argument");
+    auto* m = checked_mo(mo);
+    RR_REQUIRE(s->ntens == 1, RR_ERR_STATE, "rr_mo_build_nonrel_into: needs a single-tensor handle");
+    RR_REQUIRE(!m->cplx && m->naux == s->naux && m->n == s->n, RR_ERR_ARG,
+               "rr_mo_build_nonrel_into: the MO handle is not a nonrelativistic tensor of the handle's naux and n");
+    cudaStream_t st = rr::call_stream(s, opts);
+    const bool mixed = opts && opts->precision == RR_PREC_MIXED;
+    if (mixed) rr::mo_build_nonrel_mixed(s, C, m, host_mem(opts), st);
+    else rr::mo_build_nonrel(s, C, m, host_mem(opts), st);
+    if (host_mem(opts) || (opts && opts->sync)) {
+      if (mixed) rr::check_status(s, st);
+      RR_CUDA(cudaStreamSynchronize(st));
+    }
   });
 }
 

@@ -1,6 +1,8 @@
 // Split-BF16 operands and the tcgen05 exchange (RR_PREC_MIXED); see mixed_tc.cu.
 #pragma once
 
+#include <cuda.h>
+
 #include "rr_common.cuh"
 
 namespace rr {
@@ -50,5 +52,10 @@ void mixed_exchange_general(const MixedOperands* ops, MixedScratch& scr, const E
 // ldct) on the device.
 void mixed_exchange(const MixedOperands& mo, MixedScratch& scr, const double* Ct, int64_t ldct, int64_t nocc, double* K,
                     int* err, cudaStream_t s);
+
+// BF16 tensor map with a 128- or 64-byte swizzle and zero fill out of bounds; dims / strides (bytes,
+// rank-1 entries) / box innermost first.
+CUtensorMap bf16_tensor_map(const void* base, int rank, const uint64_t* dims, const uint64_t* strides_bytes,
+                            const uint32_t* box, int swizzle_bytes = 128);
 
 }  // namespace rr

@@ -621,6 +621,21 @@ void launch_gemm(const BlockPlan& bp, const uint16_t* a_hi, const uint16_t* a_lo
 
 }  // namespace
 
+CUtensorMap bf16_tensor_map(const void* base, int rank, const uint64_t* dims, const uint64_t* strides_bytes,
+                            const uint32_t* box, int swizzle_bytes) {
+  RR_REQUIRE(swizzle_bytes == 128 || swizzle_bytes == 64, RR_ERR_ARG, "bf16_tensor_map: swizzle of 128 or 64 bytes");
+  if (swizzle_bytes == 128) return make_map(base, rank, dims, strides_bytes, box);
+  CUtensorMap m;
+  uint32_t elem[3] = {1, 1, 1};
+  const CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, static_cast<cuuint32_t>(rank), const_cast<void*>(base),
+                                 reinterpret_cast<const cuuint64_t*>(dims), reinterpret_cast<const cuuint64_t*>(strides_bytes),
+                                 reinterpret_cast<const cuuint32_t*>(box), reinterpret_cast<const cuuint32_t*>(elem),
+                                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  RR_REQUIRE(r == CUDA_SUCCESS, RR_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(static_cast<int>(r)) + ")");
+  return m;
+}
+
 // Resident split copy of B for the mixed path: Bt_hi/lo[P][a][q], row pitch ldq = round8(n).
 void mixed_prepare(MixedOperands& mo, const double* B, int64_t pitch, int64_t n, int64_t naux, cudaStream_t s) {
   if (mo.ready && mo.n == n && mo.naux == naux) return;

@@ -261,7 +261,7 @@ cudaStream_t mo_stream(rr_mo_store* m, const rr_opts* o) {
 // B_mo^P = C^T B^P C (real, n x n), chunked over P: T = C^T B^P, then T C.
 void mo_build_nonrel(rr_ri_store* ri, const double* C, rr_mo_store* m, bool host, cudaStream_t s) {
   const int64_t n = ri->n, naux = ri->naux;
-  m->B.alloc(static_cast<size_t>(std::max<int64_t>(naux * n * n, 1)));
+  m->B.ensure(static_cast<size_t>(std::max<int64_t>(naux * n * n, 1)));  // a rebuild keeps the tensor's memory
   m->scratch.ensure(static_cast<size_t>(round_up(n * n, 32)));
   double* Cd = m->scratch.p;
   copy_in(Cd, C, n * n, host, s);

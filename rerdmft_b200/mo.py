@@ -116,8 +116,12 @@ class RiMoEri(_MoBase):
         return RiMoEri(h)
 
 
-def buildRiNonRelSpinMoEri(eri: RiNonRelEriSource | RiStore, n_spatial: int, c_spatial) -> RiNonRelSpinMoEri:
-    """src/NON_REL/NonRelSpinRiMoEri.cpp:13 on the resident tensor of `eri`."""
+def buildRiNonRelSpinMoEri(eri: RiNonRelEriSource | RiStore, n_spatial: int, c_spatial,
+                           precision: int = L.RR_PREC_FP64, into: RiNonRelSpinMoEri | None = None) -> RiNonRelSpinMoEri:
+    """src/NON_REL/NonRelSpinRiMoEri.cpp:13 on the resident tensor of `eri`.
+
+    precision=RR_PREC_MIXED forms both products in split BF16 on the tensor cores (relative error about
+    1e-5 of max|B_mo|); `into` rebuilds an existing tensor of the same shape in place."""
     store = eri.store if isinstance(eri, RiNonRelEriSource) else eri
     if tuple(c_spatial.shape) != (n_spatial, n_spatial):
         raise RrError(L.RR_ERR_ARG, "buildRiNonRelSpinMoEri: c_spatial dimensions do not match n_spatial")
@@ -125,8 +129,11 @@ def buildRiNonRelSpinMoEri(eri: RiNonRelEriSource | RiStore, n_spatial: int, c_s
         raise RrError(L.RR_ERR_ARG, "buildRiNonRelSpinMoEri: eri3_L column count does not match n_spatial*n_spatial")
     dev = _is_dev(c_spatial)
     C = (_dev if dev else _host)(c_spatial, np.float64)
+    o = L.opts(L.RR_MEM_DEVICE if dev else L.RR_MEM_HOST, precision=precision)
+    if into is not None:
+        L.check(L.lib().rr_mo_build_nonrel_into(store.handle, _ptr(C), into.handle, ctypes.byref(o)))
+        return into
     h = ctypes.c_void_p()
-    o = L.opts(L.RR_MEM_DEVICE if dev else L.RR_MEM_HOST)
     L.check(L.lib().rr_mo_build_nonrel(store.handle, _ptr(C), ctypes.byref(h), ctypes.byref(o)))
     return RiNonRelSpinMoEri(h)
 
