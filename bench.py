@@ -293,6 +293,42 @@ def mo_transform_block(torch, fp64_peak, want_cpu: bool, reps: int = 5):
                          seconds_per_build=best, algorithmic_gflop=flops / 1e9, achieved_tflops=flops / best / 1e12,
                          frac_of_dgemm=(flops / best / 1e12 / fp64_peak) if fp64_peak else None,
                          note="host wall time of the synchronous call, the 2.56 GB output allocation included")
+    # split BF16 (RR_PREC_MIXED): same host-wall timing (new tensor each call), error against the FP64 build
+    om = L.opts(L.RR_MEM_DEVICE, precision=L.RR_PREC_MIXED, sync=1)
+
+    def build_ukb_mixed():
+        hh = ctypes.c_void_p()
+        L.check(lib.rr_mo_build_ukb(st4.handle, dc.data_ptr(), nt, ctypes.byref(hh), ctypes.byref(om)))
+        return hh
+
+    h = build_ukb()
+    b64 = np.empty((NAUX4, 2 * nt * nt))
+    L.check(lib.rr_mo_copy_tensor(h, b64.ctypes.data, ctypes.byref(L.opts())))
+    L.check(lib.rr_mo_destroy(h))
+    h = build_ukb_mixed()
+    L.check(lib.rr_mo_destroy(h))
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        h = build_ukb_mixed()
+        times.append(time.perf_counter() - t0)
+        if len(times) < 3:
+            L.check(lib.rr_mo_destroy(h))
+    bmx = np.empty_like(b64)
+    L.check(lib.rr_mo_copy_tensor(h, bmx.ctypes.data, ctypes.byref(L.opts())))
+    L.check(lib.rr_mo_destroy(h))
+    tm = min(times)
+    nu4 = 2 * NL4 + 2 * NS4
+    # BF16 MMA work: step 1 per flavour 2 fs^2 (2 nt) per aux index, step 2 2 nt (2 nt) (2 nu), 3 products each
+    mma = 3.0 * NAUX4 * (sum(2.0 * f * f * 2 * nt for f in fl) + 2.0 * nt * 2 * nt * 2 * nu4)
+    err = float(np.abs(bmx - b64).max())
+    out["ukb_4c_mixed"] = dict(
+        workload=f"buildRiMoEri nl={NL4} ns={NS4} naux={NAUX4} n_total={nt} (complex, split-BF16 tcgen05, "
+                 "RR_PREC_MIXED)",
+        seconds_per_build=tm, speedup_over_fp64=best / tm, bf16_mma_tflop=mma / 1e12,
+        tensor_tflops=mma / tm / 1e12, max_abs_minus_fp64=err, rel_to_max=err / float(np.abs(b64).max()),
+        note="host wall time of the synchronous call, the 2.56 GB output allocation included")
+    del b64, bmx
     if want_cpu:
         from oracle import ref
 

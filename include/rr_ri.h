@@ -326,7 +326,9 @@ int rr_mo_build_nonrel_into(rr_ri_handle ri, const double* C, rr_mo_handle mo, c
 
 /* buildRiMoEri(RiDirectEriSource, c_ukb), src/UKB/RiMoEri.cpp:64: B(P,p,q) = sum over the four UKB
  * blocks of sum conj(c(mu,p)) c(nu,q) (mu nu|P); c_ukb is n_ukb x n_total complex (n_ukb = 2nl+2ns
- * of a 4-component handle; an X2C handle is the ns = 0 case). */
+ * of a 4-component handle; an X2C handle is the ns = 0 case).  opts->precision = RR_PREC_MIXED: split-BF16
+ * tcgen05 products as for rr_mo_build_nonrel (the four blocks and the real and imaginary parts in one K
+ * range of 2 n_ukb), relative error about 1e-5 of max|B|. */
 int rr_mo_build_ukb(rr_ri_handle ri4c, const double* c_ukb, int64_t n_total, rr_mo_handle* out, const rr_opts* opts);
 
 /* Wraps an existing MO tensor (naux, n*n; kind RR_MO_NONREL_SPIN real or RR_MO_COMPLEX complex). */

@@ -488,7 +488,12 @@ int rr_mo_build_ukb(rr_ri_handle ri4c, const double* c_ukb, int64_t n_total, rr_
     auto* m = new_mo(1, s->naux, n_total);
     with_new_mo(out, m, [&] {
       cudaStream_t st = rr::call_stream(s, opts);
-      rr::mo_build_ukb(s, c_ukb, n_total, m, host_mem(opts), st);
+      if (opts && opts->precision == RR_PREC_MIXED) {
+        rr::mo_build_ukb_mixed(s, c_ukb, n_total, m, host_mem(opts), st);
+        rr::check_status(s, st);
+      } else {
+        rr::mo_build_ukb(s, c_ukb, n_total, m, host_mem(opts), st);
+      }
       RR_CUDA(cudaStreamSynchronize(st));
     });
   });

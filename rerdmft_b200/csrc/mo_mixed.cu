@@ -59,15 +59,19 @@ struct MoCfg {
   static_assert(SMEM <= 232448, "shared memory per CTA");
 };
 
-// Output of one step.  Row R of the flat product is (P, r) with P = R / n, r = R % n; column c < n.
-//   EPI 0: hi/lo[(P n + c) ldq + r] = split(value)      (Yt[P][c][r])
-//   EPI 1: out[R n + c] = value                          (B_mo[P][r][c])
+// Output of one step.  Row R of the flat product is (P, r) with P = R / rper, r = R % rper; column c < ncol.
+//   EPI 0: hi/lo[(P cmod + c % cmod) ldq + (c / cmod) chi + koff + r] = split(value), ncol <= 2 cmod
+//          (nonrelativistic: cmod = n, Yt[P][c][r]; complex: c = (Re | Im block, q), K index of r shifted by
+//          the flavour's UKB row offset koff and by chi = n_ukb for the imaginary block)
+//   EPI 1: out[R ldo + c] = value, negated for odd c when conj_odd (the imaginary parts of a conjugate)
 struct MoEpi {
-  int64_t rows;  // naux * n
-  int n;
-  int64_t ldq;
+  int64_t rows;
+  int rper, ncol, cmod;
+  int64_t chi, koff, ldq;
   __nv_bfloat16* hi;
   __nv_bfloat16* lo;
+  int64_t ldo;
+  int conj_odd;
   double* out;
 };
 
@@ -211,22 +215,24 @@ __global__ void __launch_bounds__(MO_THREADS, 1)
         const int64_t R = R0 + lane;
         const int n0 = static_cast<int>(item % ntn) * BN;
         const bool live = R < e.rows;
-        const int64_t P = live ? R / e.n : 0;
-        const int r = live ? static_cast<int>(R - P * e.n) : 0;
+        const int64_t P = live ? R / e.rper : 0;
+        const int r = live ? static_cast<int>(R - P * e.rper) : 0;
         // Fast paths write through the staging tile: EPI 0 as 16-byte runs of 8 consecutive r of one P (all 32
         // rows live and in one P, r 8-aligned), EPI 1 as whole 128- / 256-byte row segments (n even).
-        const int64_t P0 = R0 / e.n;
-        const int a0 = static_cast<int>(R0 - P0 * e.n);
+        const int64_t P0 = R0 / e.rper;
+        const int a0 = static_cast<int>(R0 - P0 * e.rper);
         const bool rows_ok = R0 + 31 < e.rows;
-        const bool fast0 = rows_ok && a0 + 31 < e.n && (a0 & 7) == 0 && (e.n & 7) == 0;
-        const bool fast1 = rows_ok && (e.n & 1) == 0;
-        for (int c0 = 0; c0 < BN && n0 + c0 < e.n; c0 += 32) {  // warp-uniform bounds
+        const bool fast0 = rows_ok && a0 + 31 < e.rper && ((e.koff + a0) & 7) == 0 && (e.chi & 7) == 0 &&
+                           (e.ldq & 7) == 0;
+        const bool fast1 = rows_ok && (e.ldo & 1) == 0;
+        const double sgn_odd = e.conj_odd ? -1.0 : 1.0;
+        for (int c0 = 0; c0 < BN && n0 + c0 < e.ncol; c0 += 32) {  // warp-uniform bounds
           const int W = c0 + 32 <= BN ? 32 : 16;                  // BN is a multiple of 16
           float v[32];
           if (W == 32) tmem_ld32(tmem + lane_base + b * CF::BNP + c0, v);
           else tmem_ld16(tmem + lane_base + b * CF::BNP + c0, v);
           const int cb = n0 + c0;
-          const int cw = min(W, e.n - cb);  // valid columns of this chunk
+          const int cw = min(W, e.ncol - cb);  // valid columns of this chunk
           __syncwarp();                     // the previous chunk's reads of the tile are done
 #pragma unroll
           for (int t = 0; t < 32; ++t)
@@ -244,7 +250,9 @@ __global__ void __launch_bounds__(MO_THREADS, 1)
                   h[k >> 1] = pack2_bf16(x0, x1);
                   l[k >> 1] = pack2_bf16(x0 - q0, x1 - q1);
                 }
-                const int64_t o = (P0 * e.n + cb + jc) * e.ldq + a0 + 8 * g;
+                const int col = cb + jc;
+                const int blk = col >= e.cmod ? 1 : 0;  // ncol <= 2 cmod
+                const int64_t o = (P0 * e.cmod + col - blk * e.cmod) * e.ldq + blk * e.chi + e.koff + a0 + 8 * g;
                 *reinterpret_cast<uint4*>(e.hi + o) = make_uint4(h[0], h[1], h[2], h[3]);
                 *reinterpret_cast<uint4*>(e.lo + o) = make_uint4(l[0], l[1], l[2], l[3]);
               }
@@ -252,7 +260,9 @@ __global__ void __launch_bounds__(MO_THREADS, 1)
 #pragma unroll
               for (int t = 0; t < 32; ++t) {
                 if (t >= cw) continue;
-                const int64_t o = (P * e.n + cb + t) * e.ldq + r;
+                const int col = cb + t;
+                const int blk = col >= e.cmod ? 1 : 0;
+                const int64_t o = (P * e.cmod + col - blk * e.cmod) * e.ldq + blk * e.chi + e.koff + r;
                 const __nv_bfloat16 hb = __float2bfloat16_rn(v[t]);
                 e.hi[o] = hb;
                 e.lo[o] = __float2bfloat16_rn(v[t] - __bfloat162float(hb));
@@ -266,20 +276,20 @@ __global__ void __launch_bounds__(MO_THREADS, 1)
                 const int rr0 = lane / lpr, cp = lane % lpr;
                 for (int rr = rr0; rr < 32; rr += rpi) {
                   const double2 d = make_double2(static_cast<double>(sw[rr * 33 + 2 * cp]),
-                                                 static_cast<double>(sw[rr * 33 + 2 * cp + 1]));
-                  *reinterpret_cast<double2*>(e.out + (R0 + rr) * e.n + cb + 2 * cp) = d;
+                                                 sgn_odd * static_cast<double>(sw[rr * 33 + 2 * cp + 1]));
+                  *reinterpret_cast<double2*>(e.out + (R0 + rr) * e.ldo + cb + 2 * cp) = d;
                 }
               } else {
 #pragma unroll
                 for (int t = 0; t < 32; t += 2)
                   if (t < cw)
-                    *reinterpret_cast<double2*>(e.out + R * e.n + cb + t) =
-                        make_double2(static_cast<double>(v[t]), static_cast<double>(v[t + 1]));
+                    *reinterpret_cast<double2*>(e.out + R * e.ldo + cb + t) =
+                        make_double2(static_cast<double>(v[t]), sgn_odd * static_cast<double>(v[t + 1]));
               }
             } else if (live) {
 #pragma unroll
               for (int t = 0; t < 32; ++t)
-                if (t < cw) e.out[R * e.n + cb + t] = static_cast<double>(v[t]);
+                if (t < cw) e.out[R * e.ldo + cb + t] = (((cb + t) & 1) ? sgn_odd : 1.0) * static_cast<double>(v[t]);
             }
           }
         }
@@ -320,7 +330,7 @@ void launch_mo(const CUtensorMap& a_hi, const CUtensorMap& a_lo, const CUtensorM
   static std::atomic<bool> attr[kMaxDevices];
   once_per_device(attr, [&] { RR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, CF::SMEM)); });
   const int64_t rtiles = (e.rows + BM - 1) / BM;
-  const int ntn = (e.n + BN - 1) / BN;
+  const int ntn = (e.ncol + BN - 1) / BN;
   const int64_t items = rtiles * ntn;
   const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(items, sm_count_current())));
   kern<<<grid, MO_THREADS, CF::SMEM, s>>>(a_hi, a_lo, b_hi, b_lo, e, nkb, rtiles, ntn, err);
@@ -345,6 +355,7 @@ int pick_bn(int64_t n) {
 template <int EPI>
 void launch_step(int bn, int swz, const CUtensorMap& a_hi, const CUtensorMap& a_lo, const CUtensorMap& b_hi,
                  const CUtensorMap& b_lo, const MoEpi& e, int nkb, int* err, cudaStream_t s) {
+  RR_REQUIRE(e.ncol <= 2 * static_cast<int64_t>(e.cmod) && e.rper > 0, RR_ERR_ARG, "MO transform: bad epilogue layout");
   if (swz == 128) {
     switch (bn) {
       case 128: return launch_mo<128, 3, EPI, 128>(a_hi, a_lo, b_hi, b_lo, e, nkb, err, s);
@@ -362,6 +373,65 @@ void launch_step(int bn, int swz, const CUtensorMap& a_hi, const CUtensorMap& a_
     default: return launch_mo<256, 4, EPI, 64>(a_hi, a_lo, b_hi, b_lo, e, nkb, err, s);
   }
 }
+
+// Column tile width and swizzle for a product of `ncol` columns (RR_MO_BN / RR_MO_SWZ force them for
+// measurement).  The 128-byte swizzle (64-deep K blocks) where it is instantiated; the 64-byte swizzle's deeper
+// ring measured slower at n = 400 (1.371 against 1.321 ms per build with BN = 208).
+void choose_tiles(int64_t ncol, int* bn_out, int* swz_out) {
+  int bn = pick_bn(ncol);
+  if (const char* v = std::getenv("RR_MO_BN")) {
+    const int f = std::atoi(v);
+    RR_REQUIRE(f == 32 || f == 64 || f == 112 || f == 128 || f == 144 || f == 208 || f == 256, RR_ERR_ARG,
+               "RR_MO_BN: one of 32, 64, 112, 128, 144, 208, 256");
+    bn = f;
+  }
+  int swz = (bn == 128 || bn == 144 || bn == 208) ? 128 : 64;
+  if (const char* v = std::getenv("RR_MO_SWZ")) {
+    swz = std::atoi(v);
+    RR_REQUIRE((swz == 64) || (swz == 128 && (bn == 128 || bn == 144 || bn == 208)), RR_ERR_ARG,
+               "RR_MO_SWZ: 64, or 128 with a column tile of 128, 144 or 208");
+  }
+  *bn_out = bn;
+  *swz_out = swz;
+}
+
+// Split rows of the complex transform's B operands (BF16 hi / lo, row pitch ld) from c (nu x nt complex,
+// interleaved, row-major):
+//   ct2 of a flavour block (rows [off, off + fs) of c):  ct2[j'][q] = Re c[off + q][j'] (j' < nt),
+//                                                         Im c[off + q][j' - nt] (j' >= nt);
+//   cc over all rows k of c (K = 2 nu):  cc[2p][k] = Re c[k][p], cc[2p][nu + k] = Im c[k][p],
+//                                         cc[2p + 1][k] = -Im c[k][p], cc[2p + 1][nu + k] = Re c[k][p].
+__global__ void ct2_split_kernel(const double* c, int64_t nt, int64_t off, int64_t fs, int64_t ld, __nv_bfloat16* hi,
+                                 __nv_bfloat16* lo) {
+  const int64_t cnt = 2 * nt * fs;
+  for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < cnt;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t jp = idx / fs, q = idx % fs;
+    const int part = jp >= nt ? 1 : 0;
+    const double x = c[((off + q) * nt + (jp - part * nt)) * 2 + part];
+    const __nv_bfloat16 h = __double2bfloat16(x);
+    hi[jp * ld + q] = h;
+    lo[jp * ld + q] = __double2bfloat16(x - static_cast<double>(__bfloat162float(h)));
+  }
+}
+
+__global__ void cc_split_kernel(const double* c, int64_t nt, int64_t nu, int64_t ld, __nv_bfloat16* hi,
+                                __nv_bfloat16* lo) {
+  const int64_t cnt = 2 * nt * 2 * nu;
+  for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < cnt;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t row = idx / (2 * nu), k = idx % (2 * nu);
+    const int64_t p = row >> 1;
+    const bool second = k >= nu;
+    const double* e = c + ((second ? k - nu : k) * nt + p) * 2;
+    const double x = (row & 1) ? (second ? e[0] : -e[1]) : (second ? e[1] : e[0]);
+    const __nv_bfloat16 h = __double2bfloat16(x);
+    hi[row * ld + k] = h;
+    lo[row * ld + k] = __double2bfloat16(x - static_cast<double>(__bfloat162float(h)));
+  }
+}
+
+int grid_of(int64_t count) { return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((count + 255) / 256, 1184))); }
 
 }  // namespace
 
@@ -388,21 +458,8 @@ void mo_build_nonrel_mixed(rr_ri_store* ri, const double* C, rr_mo_store* m, boo
                                                                                                  ldq, ct_hi, ct_lo);
   RR_LAUNCH_CHECK();
 
-  int bn = pick_bn(n);
-  if (const char* v = std::getenv("RR_MO_BN")) {  // measurement: force a column tile width
-    const int f = std::atoi(v);
-    RR_REQUIRE(f == 32 || f == 64 || f == 112 || f == 128 || f == 144 || f == 208 || f == 256, RR_ERR_ARG,
-               "RR_MO_BN: one of 32, 64, 112, 128, 144, 208, 256");
-    bn = f;
-  }
-  // 128-byte swizzle (64-deep K blocks) where it is instantiated; the 64-byte swizzle's deeper ring measured
-  // slower at n = 400 (1.371 against 1.321 ms per build with BN = 208).
-  int swz = (bn == 128 || bn == 144 || bn == 208) ? 128 : 64;
-  if (const char* v = std::getenv("RR_MO_SWZ")) {  // measurement: force the swizzle
-    swz = std::atoi(v);
-    RR_REQUIRE((swz == 64) || (swz == 128 && (bn == 128 || bn == 144 || bn == 208)), RR_ERR_ARG,
-               "RR_MO_SWZ: 64, or 128 with a column tile of 128, 144 or 208");
-  }
+  int bn = 0, swz = 0;
+  choose_tiles(n, &bn, &swz);
   const int BK = swz / 2;
   const int nkb = static_cast<int>((n + BK - 1) / BK);
   const uint64_t rows = static_cast<uint64_t>(naux * n);
@@ -420,13 +477,117 @@ void mo_build_nonrel_mixed(rr_ri_store* ri, const double* C, rr_mo_store* m, boo
 
   MoEpi e{};
   e.rows = naux * n;
-  e.n = static_cast<int>(n);
+  e.rper = e.ncol = e.cmod = static_cast<int>(n);
+  e.chi = 0;
+  e.koff = 0;
   e.ldq = ldq;
   e.hi = reinterpret_cast<__nv_bfloat16*>(scr.pl_hi.p);
   e.lo = reinterpret_cast<__nv_bfloat16*>(scr.pl_lo.p);
+  e.ldo = n;
+  e.conj_odd = 0;
   e.out = m->B.p;
   launch_step<0>(bn, swz, bt_hi, bt_lo, c_hi, c_lo, e, nkb, ri->status.p, s);  // Yt = (B^P^T C)^T, split
   launch_step<1>(bn, swz, y_hi, y_lo, c_hi, c_lo, e, nkb, ri->status.p, s);    // B_mo^P = C^T B^P C, FP64
+}
+
+// RR_PREC_MIXED buildRiMoEri (src/UKB/RiMoEri.cpp:20-86): B(P,p,q) = sum_f c_f^dagger B_f^P c_f over the four
+// UKB blocks, c = R + i I.  Step 1 per flavour f: Y_f = B_f^T [R_f | I_f] (real, 2 nt columns) written as
+// Yt[P][q][k] with k = off_f + a for the real block and nu + off_f + a for the imaginary one, so every flavour
+// lands in one K range of length 2 nu.  Step 2, one real GEMM with K = 2 nu over all flavours:
+//   M[p][q] = sum_f c_f^dagger (B_f^T c_f) = sum_k cc[2p][k] Yt[q][k] + i sum_k cc[2p + 1][k] Yt[q][k]
+// with the output row (P, q) and the interleaved column (p, Re / Im): stored as B[P][q][p] = conj(M[p][q]),
+// which is (c^dagger B c)[q][p] element for element (no symmetry of B_f^P needed).  Chunked over P so that
+// the split intermediate stays within 256 Mi elements a plane.
+void mo_build_ukb_mixed(rr_ri_store* ri, const double* c_ukb, int64_t nt, rr_mo_store* m, bool host, cudaStream_t s) {
+  const int64_t nl = ri->n, ns = ri->ns, naux = ri->naux, nu = 2 * nl + 2 * ns;
+  const int64_t off[4] = {0, nl, 2 * nl, 2 * nl + ns}, fs[4] = {nl, nl, ns, ns};
+  const int tens[4] = {0, 0, 1, 1};
+  const int64_t fsmax = std::max(nl, ns);
+  RR_REQUIRE(2 * nt <= 65535 && fsmax <= 65535 && naux * std::max(fsmax, nt) < (int64_t(1) << 31), RR_ERR_ARG,
+             "rr_mo_build_ukb (RR_PREC_MIXED): dimensions exceed the tensor-map limits");
+  m->B.ensure(static_cast<size_t>(std::max<int64_t>(2 * naux * nt * nt, 1)));
+  if (nt == 0 || naux == 0 || nu == 0) {
+    if (m->B.n) RR_CUDA(cudaMemsetAsync(m->B.p, 0, sizeof(double) * m->B.n, s));
+    return;
+  }
+  m->scratch.ensure(static_cast<size_t>(round_up(2 * nu * nt, 32)));
+  double* cd = m->scratch.p;
+  copy_in(cd, c_ukb, 2 * nu * nt, host, s);
+  for (int t = 0; t < 2; ++t) {
+    const int64_t ft = t == 0 ? nl : ns;
+    if (ft > 0) mixed_prepare(ri->mixed[t], ri->B[t].p, ri->pitch[t], ft, naux, s);
+  }
+  const int64_t K2 = 2 * nu, ldk = (K2 + 7) / 8 * 8;
+  // B operands: cc (2 nt x ldk) and one ct2 per flavour (2 nt x ldq of its tensor), 256-element aligned
+  int64_t ooff[5];
+  int64_t tot = round_up(2 * nt * ldk, 256);
+  for (int f = 0; f < 4; ++f) {
+    ooff[f] = tot;
+    tot += fs[f] > 0 ? round_up(2 * nt * ri->mixed[tens[f]].ldq, 256) : 0;
+  }
+  MixedScratch& scr = ri->mscr;
+  scr.coef_hi.ensure(static_cast<size_t>(tot));
+  scr.coef_lo.ensure(static_cast<size_t>(tot));
+  auto* ch = reinterpret_cast<__nv_bfloat16*>(scr.coef_hi.p);
+  auto* cl = reinterpret_cast<__nv_bfloat16*>(scr.coef_lo.p);
+  cc_split_kernel<<<grid_of(2 * nt * K2), 256, 0, s>>>(cd, nt, nu, ldk, ch, cl);
+  RR_LAUNCH_CHECK();
+  for (int f = 0; f < 4; ++f) {
+    if (fs[f] == 0) continue;
+    ct2_split_kernel<<<grid_of(2 * nt * fs[f]), 256, 0, s>>>(cd, nt, off[f], fs[f], ri->mixed[tens[f]].ldq, ch + ooff[f],
+                                                             cl + ooff[f]);
+    RR_LAUNCH_CHECK();
+  }
+  const int64_t pc = std::max<int64_t>(1, std::min<int64_t>(naux, (int64_t(1) << 28) / (nt * ldk)));
+  scr.pl_hi.ensure(static_cast<size_t>(pc * nt * ldk));
+  scr.pl_lo.ensure(static_cast<size_t>(pc * nt * ldk));
+  int bn = 0, swz = 0;
+  choose_tiles(2 * nt, &bn, &swz);
+  const int BK = swz / 2;
+  uint32_t boxA[2] = {static_cast<uint32_t>(BK), BM};
+  uint32_t boxB[2] = {static_cast<uint32_t>(BK), static_cast<uint32_t>(bn)};
+  uint64_t strk[1] = {static_cast<uint64_t>(ldk) * 2};
+  uint64_t dimsC[2] = {static_cast<uint64_t>(K2), static_cast<uint64_t>(2 * nt)};
+  const CUtensorMap cc_hi = bf16_tensor_map(ch, 2, dimsC, strk, boxB, swz);
+  const CUtensorMap cc_lo = bf16_tensor_map(cl, 2, dimsC, strk, boxB, swz);
+  for (int64_t P0 = 0; P0 < naux; P0 += pc) {
+    const int64_t cnt = std::min(pc, naux - P0);
+    for (int f = 0; f < 4; ++f) {  // step 1: Yt columns of flavour f
+      if (fs[f] == 0) continue;
+      const MixedOperands& mo = ri->mixed[tens[f]];
+      uint64_t dimsA[2] = {static_cast<uint64_t>(fs[f]), static_cast<uint64_t>(cnt * fs[f])};
+      uint64_t dimsB[2] = {static_cast<uint64_t>(fs[f]), static_cast<uint64_t>(2 * nt)};
+      uint64_t strq[1] = {static_cast<uint64_t>(mo.ldq) * 2};
+      const int64_t a_off = P0 * fs[f] * mo.ldq;
+      const CUtensorMap a_hi = bf16_tensor_map(mo.bt_hi.p + a_off, 2, dimsA, strq, boxA, swz);
+      const CUtensorMap a_lo = bf16_tensor_map(mo.bt_lo.p + a_off, 2, dimsA, strq, boxA, swz);
+      const CUtensorMap b_hi = bf16_tensor_map(ch + ooff[f], 2, dimsB, strq, boxB, swz);
+      const CUtensorMap b_lo = bf16_tensor_map(cl + ooff[f], 2, dimsB, strq, boxB, swz);
+      MoEpi e{};
+      e.rows = cnt * fs[f];
+      e.rper = static_cast<int>(fs[f]);
+      e.ncol = static_cast<int>(2 * nt);
+      e.cmod = static_cast<int>(nt);
+      e.chi = nu;
+      e.koff = off[f];
+      e.ldq = ldk;
+      e.hi = reinterpret_cast<__nv_bfloat16*>(scr.pl_hi.p);
+      e.lo = reinterpret_cast<__nv_bfloat16*>(scr.pl_lo.p);
+      launch_step<0>(bn, swz, a_hi, a_lo, b_hi, b_lo, e, static_cast<int>((fs[f] + BK - 1) / BK), ri->status.p, s);
+    }
+    uint64_t dimsY[2] = {static_cast<uint64_t>(K2), static_cast<uint64_t>(cnt * nt)};
+    const CUtensorMap y_hi = bf16_tensor_map(scr.pl_hi.p, 2, dimsY, strk, boxA, swz);
+    const CUtensorMap y_lo = bf16_tensor_map(scr.pl_lo.p, 2, dimsY, strk, boxA, swz);
+    MoEpi e{};
+    e.rows = cnt * nt;
+    e.rper = static_cast<int>(nt);
+    e.ncol = static_cast<int>(2 * nt);
+    e.cmod = static_cast<int>(nt);
+    e.ldo = 2 * nt;
+    e.conj_odd = 1;
+    e.out = m->B.p + P0 * nt * nt * 2;
+    launch_step<1>(bn, swz, y_hi, y_lo, cc_hi, cc_lo, e, static_cast<int>((K2 + BK - 1) / BK), ri->status.p, s);
+  }
 }
 
 }  // namespace rr

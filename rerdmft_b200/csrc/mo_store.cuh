@@ -17,6 +17,7 @@ cudaStream_t mo_stream(rr_mo_store* m, const rr_opts* o);
 void mo_build_nonrel(rr_ri_store* ri, const double* C, rr_mo_store* m, bool host, cudaStream_t s);
 // RR_PREC_MIXED: the same tensor from split-BF16 tcgen05 products (mo_mixed.cu).
 void mo_build_nonrel_mixed(rr_ri_store* ri, const double* C, rr_mo_store* m, bool host, cudaStream_t s);
+void mo_build_ukb_mixed(rr_ri_store* ri, const double* c_ukb, int64_t nt, rr_mo_store* m, bool host, cudaStream_t s);
 void mo_build_ukb(rr_ri_store* ri, const double* c_ukb, int64_t nt, rr_mo_store* m, bool host, cudaStream_t s);
 void mo_rotate(rr_mo_store* src, const double* U, rr_mo_store* dst, bool host, cudaStream_t s);
 void mo_positive_block(rr_mo_store* src, int64_t off, rr_mo_store* dst, cudaStream_t s);

@@ -138,15 +138,18 @@ def buildRiNonRelSpinMoEri(eri: RiNonRelEriSource | RiStore, n_spatial: int, c_s
     return RiNonRelSpinMoEri(h)
 
 
-def buildRiMoEri(eri: RiDirectEriSource, c_ukb) -> RiMoEri:
-    """src/UKB/RiMoEri.cpp:64 on the resident LL/SS tensors of `eri`."""
+def buildRiMoEri(eri: RiDirectEriSource, c_ukb, precision: int = L.RR_PREC_FP64) -> RiMoEri:
+    """src/UKB/RiMoEri.cpp:64 on the resident LL/SS tensors of `eri`.
+
+    precision=RR_PREC_MIXED forms the products in split BF16 on the tensor cores (relative error about
+    1e-5 of max|B_mo|)."""
     nu = 2 * eri.nl + 2 * eri.ns
     if c_ukb.shape[0] != nu:
         raise RrError(L.RR_ERR_ARG, "buildRiMoEri: c_ukb row count does not match 2*nLarge+2*nSmall")
     dev = _is_dev(c_ukb)
     c = (_dev if dev else _host)(c_ukb, np.complex128)
     h = ctypes.c_void_p()
-    o = L.opts(L.RR_MEM_DEVICE if dev else L.RR_MEM_HOST)
+    o = L.opts(L.RR_MEM_DEVICE if dev else L.RR_MEM_HOST, precision=precision)
     L.check(L.lib().rr_mo_build_ukb(eri.store.handle, _ptr(c), c.shape[1], ctypes.byref(h), ctypes.byref(o)))
     return RiMoEri(h)
 

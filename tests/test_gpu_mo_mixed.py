@@ -1,6 +1,7 @@
-"""The split-BF16 (RR_PREC_MIXED) MO three-index transform B_mo^P = C^T B^P C on the tensor cores,
-against the numpy restatement of buildRiNonRelSpinMoEri (src/NON_REL/NonRelSpinRiMoEri.cpp:13-43) and the
-FP64 device build, and the in-place rebuild of an existing MO tensor.
+"""The split-BF16 (RR_PREC_MIXED) MO three-index transforms on the tensor cores: B_mo^P = C^T B^P C against
+the numpy restatement of buildRiNonRelSpinMoEri (src/NON_REL/NonRelSpinRiMoEri.cpp:13-43) and the FP64 device
+build, the in-place rebuild of an existing MO tensor, and the complex buildRiMoEri (src/UKB/RiMoEri.cpp:20-86)
+against its restatement and the FP64 device build.
 
 Tolerance: three BF16 products with FP32 accumulation per product and the intermediate C^T B^P re-split
 to BF16 pairs give a relative error of about 1e-5 of max|B_mo| (a numpy emulation of the same rounding
@@ -95,3 +96,42 @@ def test_rebuild_into_rejects_other_shapes():
     other = mo.buildRiNonRelSpinMoEri(ri.RiNonRelEriSource(n, B[:30], np.eye(n), np.eye(n)), n, np.eye(n))
     with pytest.raises(L.RrError, match="rr_mo_build_nonrel_into"):
         mo.buildRiNonRelSpinMoEri(src, n, np.eye(n), into=other)
+
+
+@pytest.mark.parametrize("nl,ns,naux,nt", [(3, 5, 7, 4), (12, 20, 50, 17), (33, 70, 40, 64), (64, 130, 30, 100)])
+def test_mixed_ukb_build_vs_oracle(nl, ns, naux, nt):
+    rng = np.random.default_rng(nl + ns)
+    B_LL = synth.ri_tensor(nl, naux, nl, box=6.0)
+    B_SS = synth.ri_tensor(ns, naux, ns, box=6.0)
+    c = synth.random_unitary(2 * nl + 2 * ns, rng)[:, :nt]
+    src = ri.RiDirectEriSource(nl, ns, B_LL, B_SS)
+    got = mo.buildRiMoEri(src, c, precision=L.RR_PREC_MIXED).b()
+    ref = o.ri_mo_build(nl, ns, B_LL, B_SS, c)
+    err = float(np.abs(got - ref).max())
+    scale = float(np.abs(ref).max())
+    print(f"nl={nl} ns={ns} naux={naux} nt={nt}: max|B(mixed) - B(FP64 oracle)| = {err:.3e} ({err / scale:.2e} of max)")
+    assert err <= MIXED_REL * scale
+    # non-symmetric B^P blocks: the stored tensor is c^dagger B^P c element for element
+    Bn_LL, Bn_SS = rng.standard_normal((naux, nl * nl)), rng.standard_normal((naux, ns * ns))
+    srcn = ri.RiDirectEriSource(nl, ns, Bn_LL, Bn_SS)
+    gotn = mo.buildRiMoEri(srcn, c, precision=L.RR_PREC_MIXED).b()
+    refn = o.ri_mo_build(nl, ns, Bn_LL, Bn_SS, c)
+    bound = o.ri_mo_build(nl, ns, np.abs(Bn_LL), np.abs(Bn_SS), np.abs(c)).real  # sum of |terms| per element
+    assert np.all(np.abs(gotn - refn) <= MIXED_REL * bound)
+
+
+def test_mixed_ukb_build_large():
+    """nl = 100, ns = 300, naux = 200, 200 spinors: 2 nt = 400 columns (BN = 208), K = 2 n_ukb = 1600, against
+    the FP64 device build."""
+    nl, ns, naux, nt = 100, 300, 200, 200
+    rng = np.random.default_rng(11)
+    B_LL = synth.ri_tensor(nl, naux, 1, box=12.0)
+    B_SS = synth.ri_tensor(ns, naux, 2, box=12.0)
+    c = synth.random_unitary(2 * nl + 2 * ns, rng)[:, :nt]
+    src = ri.RiDirectEriSource(nl, ns, B_LL, B_SS)
+    a = mo.buildRiMoEri(src, c).b()
+    b = mo.buildRiMoEri(src, c, precision=L.RR_PREC_MIXED).b()
+    err = float(np.abs(a - b).max())
+    scale = float(np.abs(a).max())
+    print(f"nl=100 ns=300 naux=200 nt=200: max|B(mixed) - B(FP64)| = {err:.3e} ({err / scale:.2e} of max)")
+    assert err <= MIXED_REL * scale
