@@ -118,7 +118,7 @@ template <int BN, int STAGES, int EPI, int SWZ>
 __global__ void __launch_bounds__(MO_THREADS, 1)
     umma_mo_kernel(const __grid_constant__ CUtensorMap mapA_hi, const __grid_constant__ CUtensorMap mapA_lo,
                    const __grid_constant__ CUtensorMap mapB_hi, const __grid_constant__ CUtensorMap mapB_lo,
-                   const MoEpi e, int nkb, int64_t rtiles, int ntn, int* err) {
+                   const MoEpi e, int nkb, int kvalid, int64_t rtiles, int ntn, int* err) {
   using CF = MoCfg<BN, STAGES, SWZ>;
   constexpr int BK = CF::BK, A_TILE = CF::A_TILE;
   extern __shared__ unsigned char smem_raw[];
@@ -172,10 +172,12 @@ __global__ void __launch_bounds__(MO_THREADS, 1)
     }
   } else if (warp == 5) {
     if (lane == 0) {  // MMA issuer
-      constexpr uint32_t idesc = idesc_bf16_f32(BM, BN);
       uint32_t q = 0, j = 0;
       for (int64_t item = blockIdx.x; item < total; item += gridDim.x, ++j) {
         const uint32_t b = j & 1;
+        // the last column tile multiplies only its valid columns (rounded up to the UMMA N step of 16)
+        const int nv = min(BN, e.ncol - static_cast<int>(item % ntn) * BN);
+        const uint32_t idesc = idesc_bf16_f32(BM, (nv + 15) / 16 * 16);
         if (j >= 2) mbar_wait(&tempty[b], ((j >> 1) - 1) & 1, err, ERR_MO_TEMPTY, dead);
         tc_fence_after();
         const uint32_t d = tmem + b * CF::BNP;
@@ -187,8 +189,10 @@ __global__ void __launch_bounds__(MO_THREADS, 1)
             const uint32_t base = smem_u32(smem + s * CF::STAGE);
             const uint64_t ahi = sdesc_k<SWZ>(base), alo = sdesc_k<SWZ>(base + A_TILE);
             const uint64_t bhi = sdesc_k<SWZ>(base + 2 * A_TILE), blo = sdesc_k<SWZ>(base + 2 * A_TILE + CF::B_TILE);
+            const int nks = min(BK / 16, (kvalid - k * BK + 15) / 16);  // 16-deep steps holding data (zero fill beyond)
 #pragma unroll
             for (int kk = 0; kk < BK / 16; ++kk) {
+              if (kk >= nks) break;
               const uint64_t dk = static_cast<uint64_t>(kk * 32) >> 4;  // +32 bytes per 16-element step
               umma_bf16(d, ahi + dk, bhi + dk, idesc, (k > 0 || kk > 0) ? 1u : 0u);
               umma_bf16(d, ahi + dk, blo + dk, idesc, 1u);
@@ -324,7 +328,8 @@ __global__ void ct_split_kernel(const double* C, int n, int64_t ldq, __nv_bfloat
 
 template <int BN, int STAGES, int EPI, int SWZ>
 void launch_mo(const CUtensorMap& a_hi, const CUtensorMap& a_lo, const CUtensorMap& b_hi, const CUtensorMap& b_lo,
-               const MoEpi& e, int nkb, int* err, cudaStream_t s) {
+               const MoEpi& e, int kvalid, int* err, cudaStream_t s) {
+  const int nkb = (kvalid + KBlk<SWZ>::BK - 1) / KBlk<SWZ>::BK;
   using CF = MoCfg<BN, STAGES, SWZ>;
   auto kern = umma_mo_kernel<BN, STAGES, EPI, SWZ>;
   static std::atomic<bool> attr[kMaxDevices];
@@ -333,7 +338,7 @@ void launch_mo(const CUtensorMap& a_hi, const CUtensorMap& a_lo, const CUtensorM
   const int ntn = (e.ncol + BN - 1) / BN;
   const int64_t items = rtiles * ntn;
   const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(items, sm_count_current())));
-  kern<<<grid, MO_THREADS, CF::SMEM, s>>>(a_hi, a_lo, b_hi, b_lo, e, nkb, rtiles, ntn, err);
+  kern<<<grid, MO_THREADS, CF::SMEM, s>>>(a_hi, a_lo, b_hi, b_lo, e, nkb, kvalid, rtiles, ntn, err);
   RR_LAUNCH_CHECK();
 }
 
@@ -354,23 +359,23 @@ int pick_bn(int64_t n) {
 
 template <int EPI>
 void launch_step(int bn, int swz, const CUtensorMap& a_hi, const CUtensorMap& a_lo, const CUtensorMap& b_hi,
-                 const CUtensorMap& b_lo, const MoEpi& e, int nkb, int* err, cudaStream_t s) {
+                 const CUtensorMap& b_lo, const MoEpi& e, int kvalid, int* err, cudaStream_t s) {
   RR_REQUIRE(e.ncol <= 2 * static_cast<int64_t>(e.cmod) && e.rper > 0, RR_ERR_ARG, "MO transform: bad epilogue layout");
   if (swz == 128) {
     switch (bn) {
-      case 128: return launch_mo<128, 3, EPI, 128>(a_hi, a_lo, b_hi, b_lo, e, nkb, err, s);
-      case 144: return launch_mo<144, 3, EPI, 128>(a_hi, a_lo, b_hi, b_lo, e, nkb, err, s);
-      default: return launch_mo<208, 2, EPI, 128>(a_hi, a_lo, b_hi, b_lo, e, nkb, err, s);
+      case 128: return launch_mo<128, 3, EPI, 128>(a_hi, a_lo, b_hi, b_lo, e, kvalid, err, s);
+      case 144: return launch_mo<144, 3, EPI, 128>(a_hi, a_lo, b_hi, b_lo, e, kvalid, err, s);
+      default: return launch_mo<208, 2, EPI, 128>(a_hi, a_lo, b_hi, b_lo, e, kvalid, err, s);
     }
   }
   switch (bn) {
-    case 32: return launch_mo<32, 8, EPI, 64>(a_hi, a_lo, b_hi, b_lo, e, nkb, err, s);
-    case 64: return launch_mo<64, 8, EPI, 64>(a_hi, a_lo, b_hi, b_lo, e, nkb, err, s);
-    case 112: return launch_mo<112, 6, EPI, 64>(a_hi, a_lo, b_hi, b_lo, e, nkb, err, s);
-    case 128: return launch_mo<128, 6, EPI, 64>(a_hi, a_lo, b_hi, b_lo, e, nkb, err, s);
-    case 144: return launch_mo<144, 6, EPI, 64>(a_hi, a_lo, b_hi, b_lo, e, nkb, err, s);
-    case 208: return launch_mo<208, 4, EPI, 64>(a_hi, a_lo, b_hi, b_lo, e, nkb, err, s);
-    default: return launch_mo<256, 4, EPI, 64>(a_hi, a_lo, b_hi, b_lo, e, nkb, err, s);
+    case 32: return launch_mo<32, 8, EPI, 64>(a_hi, a_lo, b_hi, b_lo, e, kvalid, err, s);
+    case 64: return launch_mo<64, 8, EPI, 64>(a_hi, a_lo, b_hi, b_lo, e, kvalid, err, s);
+    case 112: return launch_mo<112, 6, EPI, 64>(a_hi, a_lo, b_hi, b_lo, e, kvalid, err, s);
+    case 128: return launch_mo<128, 6, EPI, 64>(a_hi, a_lo, b_hi, b_lo, e, kvalid, err, s);
+    case 144: return launch_mo<144, 6, EPI, 64>(a_hi, a_lo, b_hi, b_lo, e, kvalid, err, s);
+    case 208: return launch_mo<208, 4, EPI, 64>(a_hi, a_lo, b_hi, b_lo, e, kvalid, err, s);
+    default: return launch_mo<256, 4, EPI, 64>(a_hi, a_lo, b_hi, b_lo, e, kvalid, err, s);
   }
 }
 
@@ -461,7 +466,6 @@ void mo_build_nonrel_mixed(rr_ri_store* ri, const double* C, rr_mo_store* m, boo
   int bn = 0, swz = 0;
   choose_tiles(n, &bn, &swz);
   const int BK = swz / 2;
-  const int nkb = static_cast<int>((n + BK - 1) / BK);
   const uint64_t rows = static_cast<uint64_t>(naux * n);
   uint64_t dimsA[2] = {static_cast<uint64_t>(n), rows};
   uint64_t dimsB[2] = {static_cast<uint64_t>(n), static_cast<uint64_t>(n)};
@@ -486,8 +490,8 @@ void mo_build_nonrel_mixed(rr_ri_store* ri, const double* C, rr_mo_store* m, boo
   e.ldo = n;
   e.conj_odd = 0;
   e.out = m->B.p;
-  launch_step<0>(bn, swz, bt_hi, bt_lo, c_hi, c_lo, e, nkb, ri->status.p, s);  // Yt = (B^P^T C)^T, split
-  launch_step<1>(bn, swz, y_hi, y_lo, c_hi, c_lo, e, nkb, ri->status.p, s);    // B_mo^P = C^T B^P C, FP64
+  launch_step<0>(bn, swz, bt_hi, bt_lo, c_hi, c_lo, e, static_cast<int>(n), ri->status.p, s);  // Yt = (B^P^T C)^T, split
+  launch_step<1>(bn, swz, y_hi, y_lo, c_hi, c_lo, e, static_cast<int>(n), ri->status.p, s);    // B_mo^P = C^T B^P C
 }
 
 // RR_PREC_MIXED buildRiMoEri (src/UKB/RiMoEri.cpp:20-86): B(P,p,q) = sum_f c_f^dagger B_f^P c_f over the four
@@ -573,7 +577,7 @@ void mo_build_ukb_mixed(rr_ri_store* ri, const double* c_ukb, int64_t nt, rr_mo_
       e.ldq = ldk;
       e.hi = reinterpret_cast<__nv_bfloat16*>(scr.pl_hi.p);
       e.lo = reinterpret_cast<__nv_bfloat16*>(scr.pl_lo.p);
-      launch_step<0>(bn, swz, a_hi, a_lo, b_hi, b_lo, e, static_cast<int>((fs[f] + BK - 1) / BK), ri->status.p, s);
+      launch_step<0>(bn, swz, a_hi, a_lo, b_hi, b_lo, e, static_cast<int>(fs[f]), ri->status.p, s);
     }
     uint64_t dimsY[2] = {static_cast<uint64_t>(K2), static_cast<uint64_t>(cnt * nt)};
     const CUtensorMap y_hi = bf16_tensor_map(scr.pl_hi.p, 2, dimsY, strk, boxA, swz);
@@ -586,7 +590,7 @@ void mo_build_ukb_mixed(rr_ri_store* ri, const double* c_ukb, int64_t nt, rr_mo_
     e.ldo = 2 * nt;
     e.conj_odd = 1;
     e.out = m->B.p + P0 * nt * nt * 2;
-    launch_step<1>(bn, swz, y_hi, y_lo, cc_hi, cc_lo, e, static_cast<int>((K2 + BK - 1) / BK), ri->status.p, s);
+    launch_step<1>(bn, swz, y_hi, y_lo, cc_hi, cc_lo, e, static_cast<int>(K2), ri->status.p, s);
   }
 }
 
