@@ -1,5 +1,7 @@
-// Split-BF16 MO three-index transform on the 5th-generation tensor cores (RR_PREC_MIXED of
-// rr_mo_build_nonrel): B_mo^P = C^T B^P C for every aux index P.
+// Split-BF16 MO three-index transforms on the 5th-generation tensor cores (RR_PREC_MIXED of
+// rr_mo_build_nonrel and rr_mo_build_ukb).  Nonrelativistic: B_mo^P = C^T B^P C for every aux index P; the
+// complex four-block form (buildRiMoEri) reuses the same kernel with other operand rows and output maps
+// (mo_build_ukb_mixed below).
 //
 // The reference forms the two products per P in FP64 (src/NON_REL/NonRelSpinRiMoEri.cpp:13-43,
 // buildRiNonRelSpinMoEri).  Here both products run as split-BF16 tcgen05 MMAs (x y ~= hi hi + hi lo +
@@ -14,7 +16,9 @@
 // Neither step needs symmetry of B^P: the result is C^T B^P C element for element.
 // Kernel: one persistent CTA per SM walks (row tile, column tile) items with a continuous TMA ring and
 // two TMEM accumulators, so the epilogue of one item overlaps the MMAs of the next.  Roles: warps 0-3
-// drain TMEM (lanes 32 w .. 32 w + 31), warp 4 lane 0 issues the TMA ring, warp 5 lane 0 the MMAs.
+// drain TMEM (lanes 32 w .. 32 w + 31) through a per-warp shared-memory staging tile, so that the stores
+// are whole 16-byte BF16 runs or whole FP64 row segments; warp 4 lane 0 issues the TMA ring, warp 5 lane 0
+// the MMAs.
 // Every mbarrier wait is bounded; an expiry sets a status bit that the host reports as RR_ERR_TIMEOUT.
 #include <cuda.h>
 #include <cuda_bf16.h>
