@@ -75,3 +75,36 @@ def test_column_tile_cost_model():
     assert pick(400) == 208 and pick(800) == 208 and pick(24) == 32 and pick(130) == 144
     costs = {c: -(-400 // c) * (c + 64) for c in (208, 144, 256, 112, 128)}
     assert sorted(costs, key=costs.get) == [208, 144, 256, 112, 128]
+
+
+def _bf16(x):
+    """Round-to-nearest-even to BF16 (through FP32), as __float2bfloat16_rn / __double2bfloat16 do for these
+    magnitudes."""
+    u = np.asarray(x, np.float32).view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def _split_mm(A, B):
+    """Three BF16 products hi hi + hi lo + lo hi with FP32 accumulation."""
+    ah, bh = _bf16(A), _bf16(B)
+    al, bl = _bf16(A - ah), _bf16(B - bh)
+    f = lambda a, b: (a.astype(np.float32) @ b.astype(np.float32)).astype(np.float64)  # noqa: E731
+    return f(ah, bh) + f(ah, bl) + f(al, bh)
+
+
+@pytest.mark.parametrize("n,naux", [(24, 6), (64, 3)])
+def test_split_bf16_error_model(n, naux):
+    """The rounding model behind the GPU tolerance (3e-5 of max|B_mo|): step 1 in split BF16, its FP32 result
+    re-split, step 2 in split BF16.  The emulation stays well inside the bound (about 1e-5)."""
+    from rerdmft_b200 import synth
+
+    rng = np.random.default_rng(n)
+    B = synth.ri_tensor(n, naux, n, box=6.0)
+    C = synth.random_orthogonal(n, rng)
+    ref = o.nonrel_mo_build(B, C).reshape(naux, n, n)
+    for P in range(naux):
+        BP = B[P].reshape(n, n)
+        Y = _split_mm(BP.T, C).astype(np.float32).astype(np.float64)   # step 1, FP32 accumulator
+        got = _split_mm(Y.T, C)                                         # step 2: rows j, columns i, stored [j][i]
+        assert np.abs(got - ref[P]).max() <= 3e-5 * np.abs(ref).max()
